@@ -1,0 +1,934 @@
+// Test infrastructure only: the CPU oracle (see btam_oracle.h).
+//
+// A literal restatement of the reference's arithmetic for the mean-field ADP
+// path.  Every function names the reference file:line it follows.  It keeps
+// the reference's loop structure (pair loop, j1 <= j2 triplet loop, one
+// Gaussian measure per pair/triplet) and its occupancy-threshold quirks; it
+// only replaces the per-call heap allocations with stack arrays and the Eigen
+// temporaries with plain arrays, which does not change any arithmetic.
+// Build: oracle/Makefile (-O2 -ffp-contract=off, IEEE double).
+#include "btam_oracle.h"
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+// Constants of the reference (Macros.hpp:40-42, 846-871).
+const double kSqrt2 = 1.4142135623730951;
+const double kMinOcc = 5e-4;           // min_occupancy
+const double kHbar = 6.5821192815E-4;  // h_planck [eV ps]
+const double kUma = 103.4993333E-6;    // unit_change_uma
+const int kH = 1, kMg = 12;            // AtomicSpecie ordinals
+const int kErrNeighborOverflow = 3, kErrNoNeighbors = 4, kErrBoxTooSmall = 5,
+          kErrGhostOverflow = 9;
+
+// ---------------------------------------------------------------------------
+// Cubic splines (Macros.hpp:286-329; cubic-spline.cpp:84-128)
+struct Spline {
+  double dx = 0;
+  int n = 0;
+  std::vector<double> a, b, c, d, db, dc, dd, ddc, ddd;
+};
+
+double spline_val(const Spline &s, double x) {
+  int m = static_cast<int>(x / s.dx);
+  m = std::min(m, s.n - 1);
+  double p = m * s.dx;
+  p = x - p;
+  p = std::min(p, s.dx);
+  return s.a[m] + (s.b[m] + (s.c[m] + s.d[m] * p) * p) * p;
+}
+double spline_d1(const Spline &s, double x) {
+  int m = static_cast<int>(x / s.dx);
+  m = std::min(m, s.n - 1);
+  double p = m * s.dx;
+  p = x - p;
+  p = std::min(p, s.dx);
+  return s.db[m] + (s.dc[m] + s.dd[m] * p) * p;
+}
+double spline_d2(const Spline &s, double x) {
+  int m = static_cast<int>(x / s.dx);
+  m = std::min(m, s.n - 1);
+  double p = m * s.dx;
+  p = x - p;
+  p = std::min(p, s.dx);
+  return s.ddc[m] + s.ddd[m] * p;
+}
+
+// adpPotential (Macros.hpp:486-533)
+struct Potential {
+  double mass = 0, factor = 0, rcut = 0;
+  Spline rho, embed, pair, u, w;
+};
+Potential gMgMg, gHH, gMgH;
+double gMass[32];
+
+bool read_spline(FILE *f, Spline &s) {
+  if (fscanf(f, "%d %lf", &s.n, &s.dx) != 2) return false;
+  std::vector<double> *cols[9] = {&s.a, &s.b, &s.c, &s.d, &s.db,
+                                  &s.dc, &s.dd, &s.ddc, &s.ddd};
+  for (auto *c : cols) c->assign(s.n, 0.0);
+  for (int i = 0; i < s.n; ++i)
+    for (auto *c : cols)
+      if (fscanf(f, "%lf", &(*c)[i]) != 1) return false;
+  return true;
+}
+
+// init_adp_MgHx (MgHx-ADP.cpp:366-501): element files hold
+// "mass factor rcut", rho and embedding splines, then pair/u/w splines; the
+// alloy file holds "rcut" and the pair/u/w splines only.
+bool load_potential(const std::string &path, Potential &p, bool alloy) {
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return false;
+  bool ok = true;
+  if (!alloy) {
+    ok = fscanf(f, "%lf %lf %lf", &p.mass, &p.factor, &p.rcut) == 3;
+    ok = ok && read_spline(f, p.rho) && read_spline(f, p.embed);
+  } else {
+    ok = fscanf(f, "%lf", &p.rcut) == 1;
+  }
+  ok = ok && read_spline(f, p.pair) && read_spline(f, p.u) && read_spline(f, p.w);
+  fclose(f);
+  return ok;
+}
+
+const Spline *table_by_id(int id) {
+  switch (id) {
+  case 0: return &gMgMg.rho;
+  case 1: return &gHH.rho;
+  case 2: return &gMgMg.embed;
+  case 3: return &gHH.embed;
+  case 4: return &gMgMg.pair;
+  case 5: return &gHH.pair;
+  case 6: return &gMgH.pair;
+  case 7: return &gMgMg.u;
+  case 8: return &gHH.u;
+  case 9: return &gMgH.u;
+  case 10: return &gMgMg.w;
+  case 11: return &gHH.w;
+  case 12: return &gMgH.w;
+  }
+  return nullptr;
+}
+
+// Table choice: rho by the species of j (MgHx-ADP.cpp:535-540); pair, u, w:
+// Mg-Mg, H-H, else the Mg-H table (MgHx-ADP.cpp:881-888, 1247-1263).
+const Potential &pot_of(int si, int sj) {
+  if (si == kMg && sj == kMg) return gMgMg;
+  if (si == kH && sj == kH) return gHH;
+  return gMgH;
+}
+const Spline &rho_of(int sj) { return sj == kMg ? gMgMg.rho : gHH.rho; }
+const Spline &embed_of(int si) { return si == kMg ? gMgMg.embed : gHH.embed; }
+
+inline double sq(double a) { return a == 0.0 ? 0.0 : a * a; }  // DSQR
+
+// ---------------------------------------------------------------------------
+// ADP per-term functions.  Argument layout as potential_function
+// (Macros.hpp:252-278): n[] occupancies, q[] 3 coordinates per slot.
+
+// rho_ij (MgHx-ADP.cpp:526-553), d_rho_ij_dq (557-601), d_rho_ij_dn (815-844)
+double rho_F(const double *n, const double *q, const int *spc) {
+  double r2 = 0, r[3];
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sq(r[a]);
+  }
+  return n[1] * spline_val(rho_of(spc[1]), std::sqrt(r2));
+}
+void rho_dq(int dir, double *out, const double *n, const double *q,
+            const int *spc) {
+  double r2 = 0, r[3];
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sq(r[a]);
+  }
+  double nr = std::sqrt(r2), inv = 1.0 / nr;
+  double g = n[1] * spline_d1(rho_of(spc[1]), nr);
+  for (int a = 0; a < 3; ++a) out[a] = 0.0;
+  if (dir == 0)
+    for (int a = 0; a < 3; ++a) out[a] = g * inv * r[a];
+  if (dir == 1)
+    for (int a = 0; a < 3; ++a) out[a] = -g * inv * r[a];
+}
+double rho_dn(int dir, const double *n, const double *q, const int *spc) {
+  (void)n;
+  double r2 = 0, r[3];
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sq(r[a]);
+  }
+  return dir == 1 ? spline_val(rho_of(spc[1]), std::sqrt(r2)) : 0.0;
+}
+
+// V_pair_ij (869-900), dV_pair_ij_dq (904-949), dV_pair_ij_dn (1170-1209)
+double pair_F(const double *n, const double *q, const int *spc) {
+  double r2 = 0, r[3];
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sq(r[a]);
+  }
+  double phi = n[0] * n[1] * spline_val(pot_of(spc[0], spc[1]).pair, std::sqrt(r2));
+  return 0.5 * phi;
+}
+void pair_dq(int dir, double *out, const double *n, const double *q,
+             const int *spc) {
+  double r2 = 0, r[3];
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sq(r[a]);
+  }
+  double nr = std::sqrt(r2), inv = 1.0 / nr;
+  double g = n[0] * n[1] * spline_d1(pot_of(spc[0], spc[1]).pair, nr);
+  for (int a = 0; a < 3; ++a) out[a] = 0.0;
+  if (dir == 0)
+    for (int a = 0; a < 3; ++a) out[a] = 0.5 * g * inv * r[a];
+  if (dir == 1)
+    for (int a = 0; a < 3; ++a) out[a] = -0.5 * g * inv * r[a];
+}
+double pair_dn(int dir, const double *n, const double *q, const int *spc) {
+  double r2 = 0, r[3];
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sq(r[a]);
+  }
+  double phi = spline_val(pot_of(spc[0], spc[1]).pair, std::sqrt(r2));
+  if (dir == 0) return 0.5 * (n[1] * phi);
+  if (dir == 1) return 0.5 * (n[0] * phi);
+  return 0.0;
+}
+
+// Shared geometry of the triplet terms (i = slot 0, j1 = 1, j2 = 2).
+struct Tri {
+  double r1[3], r2[3], r1sq = 0, r2sq = 0, dot = 0, n1, n2;
+};
+Tri tri_geom(const double *q) {
+  Tri t;
+  for (int a = 0; a < 3; ++a) {
+    t.r1[a] = q[a] - q[3 + a];
+    t.r2[a] = q[a] - q[6 + a];
+    t.r1sq += sq(t.r1[a]);
+    t.r2sq += sq(t.r2[a]);
+    t.dot += t.r1[a] * t.r2[a];
+  }
+  t.n1 = std::sqrt(t.r1sq);
+  t.n2 = std::sqrt(t.r2sq);
+  return t;
+}
+
+// V_dipole_ij1j2 (1233-1281), dV_dipole_ij1j2_dq (1285-1371), _dn (1683-1758)
+double dip_F(const double *n, const double *q, const int *spc) {
+  Tri t = tri_geom(q);
+  double u1 = n[0] * n[1] * spline_val(pot_of(spc[0], spc[1]).u, t.n1);
+  double u2 = n[0] * n[2] * spline_val(pot_of(spc[0], spc[2]).u, t.n2);
+  return (1.0 / 2.0) * u1 * u2 * t.dot;
+}
+void dip_dq(int dir, double *out, const double *n, const double *q,
+            const int *spc) {
+  Tri t = tri_geom(q);
+  const Spline &s1 = pot_of(spc[0], spc[1]).u, &s2 = pot_of(spc[0], spc[2]).u;
+  double i1 = 1.0 / t.n1, i2 = 1.0 / t.n2;
+  double u1 = n[0] * n[1] * spline_val(s1, t.n1);
+  double u2 = n[0] * n[2] * spline_val(s2, t.n2);
+  double du1 = n[0] * n[1] * spline_d1(s1, t.n1);
+  double du2 = n[0] * n[2] * spline_d1(s2, t.n2);
+  for (int a = 0; a < 3; ++a) out[a] = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    if (dir == 0)
+      out[a] = 0.5 * (du1 * u2 * t.dot * i1 * t.r1[a] +
+                      u1 * du2 * t.dot * i2 * t.r2[a] +
+                      u1 * u2 * (t.r1[a] + t.r2[a]));
+    if (dir == 1)
+      out[a] = -0.5 * (du1 * u2 * t.dot * i1 * t.r1[a] + u1 * u2 * t.r2[a]);
+    if (dir == 2)
+      out[a] = -0.5 * (u1 * du2 * t.dot * i2 * t.r2[a] + u1 * u2 * t.r1[a]);
+  }
+}
+double dip_dn(int dir, const double *n, const double *q, const int *spc) {
+  Tri t = tri_geom(q);
+  double s1 = spline_val(pot_of(spc[0], spc[1]).u, t.n1);
+  double s2 = spline_val(pot_of(spc[0], spc[2]).u, t.n2);
+  if (dir == 0) {
+    double u1 = n[0] * n[1] * s1, u2 = n[0] * n[2] * s2;
+    double d1 = n[1] * s1, d2 = n[2] * s2;
+    return (1.0 / 2.0) * d1 * u2 * t.dot + (1.0 / 2.0) * u1 * d2 * t.dot;
+  }
+  if (dir == 1) return (1.0 / 2.0) * (n[0] * s1) * (n[0] * n[2] * s2) * t.dot;
+  if (dir == 2) return (1.0 / 2.0) * (n[0] * n[1] * s1) * (n[0] * s2) * t.dot;
+  return 0.0;
+}
+
+// V_quadrupole_ij1j2 (1781-1831), _dq (1835-1935), _dn (2352-2434)
+double quad_F(const double *n, const double *q, const int *spc) {
+  Tri t = tri_geom(q);
+  double w1 = n[0] * n[1] * spline_val(pot_of(spc[0], spc[1]).w, t.n1);
+  double w2 = n[0] * n[2] * spline_val(pot_of(spc[0], spc[2]).w, t.n2);
+  return (1.0 / 2.0) * w1 * w2 * sq(t.dot) -
+         (1.0 / 6.0) * w1 * w2 * t.r1sq * t.r2sq;
+}
+void quad_dq(int dir, double *out, const double *n, const double *q,
+             const int *spc) {
+  Tri t = tri_geom(q);
+  const Spline &s1 = pot_of(spc[0], spc[1]).w, &s2 = pot_of(spc[0], spc[2]).w;
+  double i1 = 1.0 / t.n1, i2 = 1.0 / t.n2, dd = sq(t.dot);
+  double w1 = n[0] * n[1] * spline_val(s1, t.n1);
+  double w2 = n[0] * n[2] * spline_val(s2, t.n2);
+  double dw1 = n[0] * n[1] * spline_d1(s1, t.n1);
+  double dw2 = n[0] * n[2] * spline_d1(s2, t.n2);
+  for (int a = 0; a < 3; ++a) out[a] = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    if (dir == 0)
+      out[a] = (1.0 / 2.0) * (dw1 * w2 * dd * i1 * t.r1[a] +
+                              w1 * dw2 * dd * i2 * t.r2[a] +
+                              w1 * w2 * 2 * t.dot * (t.r1[a] + t.r2[a])) -
+               (1.0 / 6.0) * (dw1 * w2 * t.n1 * t.r2sq * t.r1[a] +
+                              w1 * dw2 * t.r1sq * t.n2 * t.r2[a] +
+                              w1 * w2 * 2 * t.r2sq * t.r1[a] +
+                              w1 * w2 * 2 * t.r1sq * t.r2[a]);
+    if (dir == 1)
+      out[a] = -0.5 * (dw1 * w2 * dd * i1 * t.r1[a] +
+                       w1 * w2 * 2 * t.dot * t.r2[a]) +
+               (1.0 / 6.0) * (dw1 * w2 * t.n1 * t.r2sq * t.r1[a] +
+                              w1 * w2 * 2 * t.r2sq * t.r1[a]);
+    if (dir == 2)
+      out[a] = -0.5 * (w1 * dw2 * dd * i2 * t.r2[a] +
+                       w1 * w2 * 2 * t.dot * t.r1[a]) +
+               (1.0 / 6.0) * (w1 * dw2 * t.r1sq * t.n2 * t.r2[a] +
+                              w1 * w2 * 2 * t.r1sq * t.r2[a]);
+  }
+}
+double quad_dn(int dir, const double *n, const double *q, const int *spc) {
+  Tri t = tri_geom(q);
+  double s1 = spline_val(pot_of(spc[0], spc[1]).w, t.n1);
+  double s2 = spline_val(pot_of(spc[0], spc[2]).w, t.n2);
+  if (dir == 0) {
+    double w1 = n[0] * n[1] * s1, w2 = n[0] * n[2] * s2;
+    double d1 = n[1] * s1, d2 = n[2] * s2, dd = sq(t.dot);
+    return (1.0 / 2.0) * d1 * w2 * dd + (1.0 / 2.0) * w1 * d2 * dd -
+           (1.0 / 6.0) * d1 * w2 * t.r1sq * t.r2sq -
+           (1.0 / 6.0) * w1 * d2 * t.r1sq * t.r2sq;
+  }
+  if (dir == 1) {
+    double d1 = n[0] * s1, w2 = n[0] * n[2] * s2;
+    return (1.0 / 2.0) * d1 * w2 * sq(t.dot) -
+           (1.0 / 6.0) * d1 * w2 * t.r1sq * t.r2sq;
+  }
+  if (dir == 2) {
+    double w1 = n[0] * n[1] * s1, d2 = n[0] * s2;
+    return (1.0 / 2.0) * w1 * d2 * sq(t.dot) -
+           (1.0 / 6.0) * w1 * d2 * t.r1sq * t.r2sq;
+  }
+  return 0.0;
+}
+
+struct Term {
+  double (*F)(const double *, const double *, const int *);
+  void (*dq)(int, double *, const double *, const double *, const int *);
+  double (*dn)(int, const double *, const double *, const int *);
+};
+const Term kRho = {rho_F, rho_dq, rho_dn};
+const Term kPair = {pair_F, pair_dq, pair_dn};
+const Term kDip = {dip_F, dip_dq, dip_dn};
+const Term kQuad = {quad_F, quad_dq, quad_dn};
+
+// ---------------------------------------------------------------------------
+// Gaussian measure (Quadrature-Measure.cpp:30-109): reduce the dof table so
+// coincident sites form one group, then one integration row per axis of each
+// group.  board[row][3*site+axis] = 1 where that row moves that site.
+struct Measure {
+  int ns = 0, D = 0;
+  int board[9][9];
+  const double *mean, *sigma, *x;
+  const int *spc;
+};
+
+Measure make_measure(const double *mean, const double *sigma, const double *x,
+                     const int *spc, const int *dof, int ns) {
+  Measure m;
+  m.ns = ns;
+  m.mean = mean;
+  m.sigma = sigma;
+  m.x = x;
+  m.spc = spc;
+  int aux[3][3];
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j < ns; ++j) aux[i][j] = dof[i * ns + j];
+  for (int i = 0; i < ns; ++i)
+    for (int j = 0; j < ns; ++j)
+      if (j != i)
+        for (int k = 0; k < ns; ++k)
+          if (aux[j][k] == aux[i][k]) aux[j][k] = 0;
+  memset(m.board, 0, sizeof(m.board));
+  int row = 0;
+  for (int i = 0; i < ns; ++i) {
+    int cnt = 0;
+    for (int j = 0; j < ns; ++j) cnt += aux[i][j];
+    if (cnt <= 0) continue;
+    for (int j = 0; j < ns; ++j)
+      if (aux[i][j])
+        for (int k = 0; k < 3; ++k) m.board[row * 3 + k][j * 3 + k] = 1;
+    ++row;
+  }
+  m.D = row * 3;
+  return m;
+}
+
+// Degree-3 rule (Quadrature-Hermitian-3th.cpp:36-110): 2D points
+// q = mean +/- sqrt(2) sigma zeta board_l, zeta = sqrt(D)/sqrt(2), weight 1/(2D).
+void point(const Measure &m, int l, double sgn, double *ql) {
+  double zeta = std::sqrt((double)m.D) / kSqrt2;
+  for (int s = 0; s < m.ns; ++s)
+    for (int a = 0; a < 3; ++a) {
+      double off = kSqrt2 * m.sigma[s] * zeta * m.board[l][s * 3 + a];
+      ql[s * 3 + a] = sgn > 0 ? m.mean[s * 3 + a] + off : m.mean[s * 3 + a] - off;
+    }
+}
+
+double integ(const Term &f, const Measure &m) {
+  double W = 1.0 / (2.0 * m.D), acc = 0.0, ql[9];
+  for (double sgn : {1.0, -1.0})
+    for (int l = 0; l < m.D; ++l) {
+      point(m, l, sgn, ql);
+      acc += f.F(m.x, ql, m.spc) * W;
+    }
+  return acc;
+}
+
+// meanfield_integral_gh_3th_dmq (212-296)
+void integ_dmq(int dir, const Term &f, const Measure &m, double *out) {
+  double W = 1.0 / (2.0 * m.D), ql[9], g[3];
+  for (int a = 0; a < 3; ++a) out[a] = 0.0;
+  for (double sgn : {1.0, -1.0})
+    for (int l = 0; l < m.D; ++l) {
+      point(m, l, sgn, ql);
+      f.dq(dir, g, m.x, ql, m.spc);
+      for (int a = 0; a < 3; ++a) out[a] += g[a] * W;
+    }
+}
+
+// meanfield_integral_gh3th_dsq (114-208)
+double integ_dsq(int dir, const Term &f, const Measure &m) {
+  double W = 1.0 / (2.0 * m.D), ql[9], g[3], acc = 0.0;
+  double zeta = std::sqrt((double)m.D) / kSqrt2;
+  for (double sgn : {1.0, -1.0})
+    for (int l = 0; l < m.D; ++l) {
+      point(m, l, sgn, ql);
+      double dqds[3];
+      for (int a = 0; a < 3; ++a)
+        dqds[a] = sgn * kSqrt2 * zeta * m.board[l][dir * 3 + a];
+      f.dq(dir, g, m.x, ql, m.spc);
+      for (int a = 0; a < 3; ++a) acc += g[a] * dqds[a] * W;
+    }
+  return acc;
+}
+
+// meanfield_integral_gh_3th_dxi (300-378)
+double integ_dxi(int dir, const Term &f, const Measure &m) {
+  double W = 1.0 / (2.0 * m.D), ql[9], acc = 0.0;
+  for (double sgn : {1.0, -1.0})
+    for (int l = 0; l < m.D; ++l) {
+      point(m, l, sgn, ql);
+      acc += f.dn(dir, m.x, ql, m.spc) * W;
+    }
+  return acc;
+}
+
+// ---------------------------------------------------------------------------
+// Per-site drivers.
+struct View {
+  const double *q, *sigma, *x, *rho;
+  const int *spc, *offs, *idx;
+};
+
+struct PairCtx {
+  double mean[6], sig[2], xx[2];
+  int sp[2];
+  Measure m;
+};
+void pair_ctx(const View &v, int i, int j, PairCtx &c) {
+  for (int a = 0; a < 3; ++a) {
+    c.mean[a] = v.q[3 * i + a];
+    c.mean[3 + a] = v.q[3 * j + a];
+  }
+  c.sig[0] = v.sigma[i];
+  c.sig[1] = v.sigma[j];
+  c.xx[0] = v.x[i];
+  c.xx[1] = v.x[j];
+  c.sp[0] = v.spc[i];
+  c.sp[1] = v.spc[j];
+  static const int dof[4] = {1, 0, 0, 1};
+  c.m = make_measure(c.mean, c.sig, c.xx, c.sp, dof, 2);
+}
+
+struct TriCtx {
+  double mean[9], sig[3], xx[3];
+  int sp[3];
+  Measure m;
+};
+void tri_ctx(const View &v, int i, int j1, int j2, TriCtx &c) {
+  int s[3] = {i, j1, j2};
+  for (int k = 0; k < 3; ++k) {
+    for (int a = 0; a < 3; ++a) c.mean[3 * k + a] = v.q[3 * s[k] + a];
+    c.sig[k] = v.sigma[s[k]];
+    c.xx[k] = v.x[s[k]];
+    c.sp[k] = v.spc[s[k]];
+  }
+  int dof[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (j1 == j2) {  // MgHx-mf-V-bulk.cpp:892-895
+    dof[5] = 1;
+    dof[7] = 1;
+  }
+  c.m = make_measure(c.mean, c.sig, c.xx, c.sp, dof, 3);
+}
+
+// evaluate_mf_rho_i_adp_MgHx (MgHx-mf-V-bulk.cpp:708-787)
+double mf_rho_i(const View &v, int i) {
+  if (v.spc[i] == kH && v.x[i] < kMinOcc) return 0.0;
+  double acc = 0.0;
+  for (int k = v.offs[i]; k < v.offs[i + 1]; ++k) {
+    int j = v.idx[k];
+    if (v.spc[j] == kH && v.x[j] < kMinOcc) continue;
+    PairCtx c;
+    pair_ctx(v, i, j, c);
+    acc += integ(kRho, c.m);
+  }
+  return acc;
+}
+
+// Mean-field <V>_0 of site i (evaluate_V0_i_adp_MgHx, 791-953); `skip_any`
+// selects the any-species site test of evaluate_S0_i_adp_MgHx (1004).
+double V0_i(const View &v, int i) {
+  double xi = v.x[i];
+  double pair = 0, dip = 0, quad = 0;
+  int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    int j1 = v.idx[k1];
+    if (v.spc[j1] == kH && v.x[j1] < kMinOcc) continue;
+    PairCtx c;
+    pair_ctx(v, i, j1, c);
+    pair += integ(kPair, c.m);
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      int j2 = v.idx[k2];
+      if (v.x[j2] < kMinOcc) continue;
+      TriCtx t;
+      tri_ctx(v, i, j1, j2, t);
+      double f = (k2 == k1) ? 1.0 : 2.0;
+      dip += f * integ(kDip, t.m);
+      quad += f * integ(kQuad, t.m);
+    }
+  }
+  double emb = xi * spline_val(embed_of(v.spc[i]), v.rho[i]);
+  return emb + pair + dip + quad;
+}
+
+// evaluate_DV0_i_Dq_u_MgHx (1823-2098): (dV0_i/dmean_q_u, dV0_i/dsigma_u).
+void DV0_dq(const View &v, int u, int i, double *out4) {
+  for (int c = 0; c < 4; ++c) out4[c] = 0.0;
+  if (v.x[u] < kMinOcc) return;
+  if (v.x[i] < kMinOcc) return;
+  double drho_q[3] = {0, 0, 0}, pair_q[3] = {0, 0, 0};
+  double dip_q[3] = {0, 0, 0}, quad_q[3] = {0, 0, 0};
+  double drho_s = 0, pair_s = 0, dip_s = 0, quad_s = 0;
+  int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    int j1 = v.idx[k1];
+    if (v.x[j1] < kMinOcc) continue;
+    PairCtx c;
+    pair_ctx(v, i, j1, c);
+    int sites2[2] = {i, j1};
+    for (int dir = 0; dir < 2; ++dir) {
+      if (sites2[dir] != u) continue;
+      double g[3];
+      integ_dmq(dir, kRho, c.m, g);
+      for (int a = 0; a < 3; ++a) drho_q[a] += g[a];
+      integ_dmq(dir, kPair, c.m, g);
+      for (int a = 0; a < 3; ++a) pair_q[a] += g[a];
+      drho_s += integ_dsq(dir, kRho, c.m);
+      pair_s += integ_dsq(dir, kPair, c.m);
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      int j2 = v.idx[k2];
+      if (v.x[j2] <= kMinOcc) continue;
+      int sites3[3] = {i, j1, j2};
+      if (sites3[0] != u && sites3[1] != u && sites3[2] != u) continue;
+      TriCtx t;
+      tri_ctx(v, i, j1, j2, t);
+      double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        if (sites3[dir] != u) continue;
+        double g[3];
+        integ_dmq(dir, kDip, t.m, g);
+        for (int a = 0; a < 3; ++a) dip_q[a] += f * g[a];
+        integ_dmq(dir, kQuad, t.m, g);
+        for (int a = 0; a < 3; ++a) quad_q[a] += f * g[a];
+        dip_s += f * integ_dsq(dir, kDip, t.m);
+        quad_s += f * integ_dsq(dir, kQuad, t.m);
+      }
+    }
+  }
+  double dF = spline_d1(embed_of(v.spc[i]), v.rho[i]);
+  for (int a = 0; a < 3; ++a)
+    out4[a] = v.x[i] * dF * drho_q[a] + pair_q[a] + dip_q[a] + quad_q[a];
+  out4[3] = v.x[i] * dF * drho_s + pair_s + dip_s + quad_s;
+}
+
+// evaluate_DV0_i_Dxi_u_adp_MgHx (2102-2325)
+double DV0_dx(const View &v, int u, int i) {
+  if (v.x[u] < kMinOcc) return 0.0;
+  if (v.x[i] < kMinOcc) return 0.0;
+  double drho = 0, pair = 0, dip = 0, quad = 0;
+  int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    int j1 = v.idx[k1];
+    if (v.x[j1] < kMinOcc) continue;
+    PairCtx c;
+    pair_ctx(v, i, j1, c);
+    int sites2[2] = {i, j1};
+    for (int dir = 0; dir < 2; ++dir) {
+      if (sites2[dir] != u) continue;
+      drho += integ_dxi(dir, kRho, c.m);
+      pair += integ_dxi(dir, kPair, c.m);
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      int j2 = v.idx[k2];
+      if (v.x[j2] < kMinOcc) continue;
+      int sites3[3] = {i, j1, j2};
+      if (sites3[0] != u && sites3[1] != u && sites3[2] != u) continue;
+      TriCtx t;
+      tri_ctx(v, i, j1, j2, t);
+      double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        if (sites3[dir] != u) continue;
+        dip += f * integ_dxi(dir, kDip, t.m);
+        quad += f * integ_dxi(dir, kQuad, t.m);
+      }
+    }
+  }
+  double emb = 0.0;
+  int si = v.spc[i];
+  if (si == kH && i == u) emb = spline_val(gHH.embed, v.rho[i]);
+  if (si == kH && i != u) emb = v.x[i] * spline_d1(gHH.embed, v.rho[i]) * drho;
+  if (si == kMg) emb = spline_d1(gMgMg.embed, v.rho[i]) * drho;  // no x_i (2312-2315)
+  return emb + pair + dip + quad;
+}
+
+// evaluate_S0_i_adp_MgHx (957-1142)
+double S0_i(const View &v, int i, double beta, double gamma) {
+  double xi = v.x[i];
+  if (xi < kMinOcc) return 0.0;
+  double V0 = V0_i(v, i);
+  double m = kUma * xi * gMass[v.spc[i] < 32 ? v.spc[i] : 0];
+  double H0 = 1.0 / (2.0 * beta) + V0;
+  double logZ = 3.0 * std::log((v.sigma[i] * std::sqrt(m / beta)) / kHbar);
+  if (xi < 1.0) logZ += std::log(1.0 / (1.0 - xi));
+  double gx = 0.0;
+  if (v.spc[i] == kH) gx = gamma * (xi > 0.9999 ? 0.9999 : xi);
+  return -logZ + beta * H0 - gx;
+}
+
+// Parallel loop over independent sites (std::thread; BTAM_ORACLE_THREADS).
+void par_for(int n, const std::function<void(int)> &fn) {
+  const char *e = getenv("BTAM_ORACLE_THREADS");
+  int t = e ? atoi(e) : (int)std::thread::hardware_concurrency();
+  if (t < 1) t = 1;
+  if (t > n) t = n;
+  if (t <= 1) {
+    for (int k = 0; k < n; ++k) fn(k);
+    return;
+  }
+  std::vector<std::thread> th;
+  for (int w = 0; w < t; ++w)
+    th.emplace_back([&, w]() {
+      for (int k = w; k < n; k += t) fn(k);
+    });
+  for (auto &x : th) x.join();
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int orc_load_tables(const char *dir) {
+  std::string d(dir);
+  if (!load_potential(d + "/adpmg.dat", gMgMg, false)) return 1;
+  if (!load_potential(d + "/adph.dat", gHH, false)) return 1;
+  if (!load_potential(d + "/adpmgh.dat", gMgH, true)) return 1;
+  for (double &m : gMass) m = 0.0;
+  gMass[kMg] = gMgMg.mass;  // element_mass[] (MgHx-ADP.cpp:436)
+  gMass[kH] = gHH.mass;
+  return 0;
+}
+
+double orc_spline(int table, double r, int deriv) {
+  const Spline *s = table_by_id(table);
+  if (!s || s->n == 0) return 0.0;
+  if (deriv == 0) return spline_val(*s, r);
+  if (deriv == 1) return spline_d1(*s, r);
+  return spline_d2(*s, r);
+}
+
+int orc_table_info(int table, double *dx) {
+  const Spline *s = table_by_id(table);
+  if (!s) return 0;
+  *dx = s->dx;
+  return s->n;
+}
+
+double orc_mass(int species) { return (species >= 0 && species < 32) ? gMass[species] : 0.0; }
+
+// Periodic images.  Orthogonal cells follow the slab test of
+// DMSwarmCreateGhostAtoms (Ghosts.cpp:123-648, In_Out_Cell 913-941): for
+// direction d (x fastest, n0..n26 without n13) the site must satisfy
+// lo <= q < lo + rc (d = -1), hi - rc <= q < hi (d = +1), lo <= q < hi (d = 0)
+// on each axis, and the copy is shifted by -d times the box edge so that it
+// lies beyond the opposite face.  (The reference's own shift search,
+// Ghosts.cpp:768-794, tries the zero shift first and so leaves single-rank
+// copies unshifted; this is the shift it intends.)  Triclinic cells use the
+// same rule on fractional coordinates with slab width rc / (face spacing).
+int orc_ghosts(int n, const double *q, const double *origin, const double *cell,
+               const int *periodic, double rc, int max_ghosts, double *q_ghost,
+               int *owner, int *image, int *n_ghost) {
+  bool ortho = cell[1] == 0 && cell[2] == 0 && cell[3] == 0 && cell[5] == 0 &&
+               cell[6] == 0 && cell[7] == 0;
+  // Reciprocal rows: frac = (q - o) . b_a, with b = inverse(cell^T) rows.
+  double A[3][3], B[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) A[r][c] = cell[3 * r + c];
+  double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+               A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+               A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  if (det == 0.0) return kErrBoxTooSmall;
+  // b_a = (a_b x a_c) / det
+  for (int a = 0; a < 3; ++a) {
+    const double *p = A[(a + 1) % 3], *s = A[(a + 2) % 3];
+    B[a][0] = (p[1] * s[2] - p[2] * s[1]) / det;
+    B[a][1] = (p[2] * s[0] - p[0] * s[2]) / det;
+    B[a][2] = (p[0] * s[1] - p[1] * s[0]) / det;
+  }
+  double w[3], lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    double bn = std::sqrt(B[a][0] * B[a][0] + B[a][1] * B[a][1] + B[a][2] * B[a][2]);
+    double height = 1.0 / bn;
+    if (periodic[a] && height < 2.0 * rc) return kErrBoxTooSmall;
+    w[a] = rc * bn;
+    lo[a] = origin[a];
+    hi[a] = origin[a] + A[a][a];
+  }
+  int ng = 0;
+  for (int i = 0; i < n; ++i) {
+    double c[3];
+    if (ortho) {
+      for (int a = 0; a < 3; ++a) c[a] = q[3 * i + a];
+    } else {
+      for (int a = 0; a < 3; ++a) {
+        double dq0 = q[3 * i] - origin[0], dq1 = q[3 * i + 1] - origin[1],
+               dq2 = q[3 * i + 2] - origin[2];
+        c[a] = dq0 * B[a][0] + dq1 * B[a][1] + dq2 * B[a][2];
+      }
+    }
+    for (int dir = 0; dir < 27; ++dir) {
+      if (dir == 13) continue;
+      int d[3] = {dir % 3 - 1, (dir / 3) % 3 - 1, dir / 9 - 1};
+      bool in = true;
+      for (int a = 0; a < 3 && in; ++a) {
+        if (d[a] != 0 && !periodic[a]) in = false;
+        double l = ortho ? lo[a] : 0.0, h = ortho ? hi[a] : 1.0;
+        double wa = ortho ? rc : w[a];
+        if (d[a] == -1) in = in && c[a] >= l && c[a] < l + wa;
+        else if (d[a] == 1) in = in && c[a] >= h - wa && c[a] < h;
+        else in = in && c[a] >= l && c[a] < h;
+      }
+      if (!in) continue;
+      if (ng >= max_ghosts) return kErrGhostOverflow;
+      for (int a = 0; a < 3; ++a) {
+        double s = q[3 * i + a];
+        for (int b = 0; b < 3; ++b)
+          if (d[b] != 0) s = s + (double)(-d[b]) * A[b][a];
+        q_ghost[3 * ng + a] = s;
+        image[3 * ng + a] = -d[a];
+      }
+      owner[ng] = i;
+      ++ng;
+    }
+  }
+  *n_ghost = ng;
+  return 0;
+}
+
+// neighbors (Neighbors.cpp:39-134), brute force, ascending j.
+int orc_neighbors(int n, const double *q, double rc, int maxn, const int *query,
+                  int nquery, int *offs, int *idx, int idx_cap) {
+  int total = 0;
+  offs[0] = 0;
+  for (int k = 0; k < nquery; ++k) {
+    int i = query[k], cnt = 0;
+    for (int j = 0; j < n; ++j) {
+      if (j == i) continue;
+      double dx = q[3 * i] - q[3 * j], dy = q[3 * i + 1] - q[3 * j + 1],
+             dz = q[3 * i + 2] - q[3 * j + 2];
+      double r = std::sqrt((dx * dx + dy * dy) + dz * dz);
+      if (r <= rc) {
+        if (cnt == maxn) return kErrNeighborOverflow;
+        if (total >= idx_cap) return kErrNeighborOverflow;
+        idx[total++] = j;
+        ++cnt;
+      }
+    }
+    if (cnt <= 0) return kErrNoNeighbors;
+    offs[k + 1] = total;
+  }
+  return 0;
+}
+
+int orc_quadrature(int term, int mode, int slot, int nsites, int coincident,
+                   const double *q, const double *sigma, const double *x,
+                   const int *spc, double *out) {
+  const Term *t = term == 0 ? &kRho : term == 1 ? &kPair : term == 2 ? &kDip
+                : term == 3 ? &kQuad : nullptr;
+  if (!t) return 1;
+  int dof2[4] = {1, 0, 0, 1};
+  int dof3[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  if (coincident) {
+    dof3[5] = 1;
+    dof3[7] = 1;
+  }
+  Measure m = make_measure(q, sigma, x, spc, nsites == 2 ? dof2 : dof3, nsites);
+  if (mode == 0) out[0] = integ(*t, m);
+  else if (mode == 1) integ_dmq(slot, *t, m, out);
+  else if (mode == 2) out[0] = integ_dsq(slot, *t, m);
+  else out[0] = integ_dxi(slot, *t, m);
+  return 0;
+}
+
+void orc_mf_rho(int n, const double *q, const double *sigma, const double *x,
+                const int *spc, const int *offs, const int *idx,
+                const int *sites, int nsites, double *out) {
+  (void)n;
+  View v{q, sigma, x, nullptr, spc, offs, idx};
+  par_for(nsites, [&](int k) { out[k] = mf_rho_i(v, sites[k]); });
+}
+
+void orc_V0(int n, const double *q, const double *sigma, const double *x,
+            const int *spc, const double *rho, const int *offs,
+            const int *idx, const int *sites, int nsites, double *out) {
+  (void)n;
+  View v{q, sigma, x, rho, spc, offs, idx};
+  par_for(nsites, [&](int k) {
+    int i = sites[k];
+    // evaluate_V0_i_adp_MgHx skips empty H sites (832-834)
+    out[k] = (spc[i] == kH && x[i] < kMinOcc) ? 0.0 : V0_i(v, i);
+  });
+}
+
+void orc_S0(int n, const double *q, const double *sigma, const double *x,
+            const int *spc, const double *rho, const double *beta,
+            const double *gamma, const int *offs, const int *idx,
+            const int *sites, int nsites, double *out) {
+  (void)n;
+  View v{q, sigma, x, rho, spc, offs, idx};
+  par_for(nsites, [&](int k) {
+    int i = sites[k];
+    out[k] = S0_i(v, i, beta[i], gamma[i]);
+  });
+}
+
+void orc_DV0_pairs(int n, const double *q, const double *sigma,
+                   const double *x, const int *spc, const double *rho,
+                   const int *offs, const int *idx, const int *u_list,
+                   const int *i_list, int npairs, double *out4, double *out_x) {
+  (void)n;
+  View v{q, sigma, x, rho, spc, offs, idx};
+  par_for(npairs, [&](int k) {
+    if (out4) DV0_dq(v, u_list[k], i_list[k], out4 + 4 * k);
+    if (out_x) out_x[k] = DV0_dx(v, u_list[k], i_list[k]);
+  });
+}
+
+// evaluate_rho_i_adp_MgHx_kokkos (density.cpp:44-104)
+void orc_rho_nmf(int n, const double *q, const double *x, const int *spc,
+                 const int *offs, const int *idx, const int *sites, int nsites,
+                 double *out) {
+  (void)n;
+  par_for(nsites, [&](int k) {
+    int i = sites[k];
+    double acc = 0.0;
+    if (!(x[i] < kMinOcc)) {
+      for (int p = offs[i]; p < offs[i + 1]; ++p) {
+        int j = idx[p];
+        if (x[j] < kMinOcc) continue;
+        double qq[6] = {q[3 * i], q[3 * i + 1], q[3 * i + 2],
+                        q[3 * j], q[3 * j + 1], q[3 * j + 2]};
+        double nn[2] = {x[i], x[j]};
+        int sp[2] = {spc[i], spc[j]};
+        acc += rho_F(nn, qq, sp);
+      }
+    }
+    out[k] = acc;
+  });
+}
+
+void orc_residuals(int n, const double *q, const double *sigma,
+                   const double *x, const int *spc, const double *beta,
+                   const double *gamma, const double *rho, const int *owner,
+                   const int *image, const int *offs, const int *idx,
+                   const int *u_list, int nu, double *Rq, double *Rs,
+                   double *Rx) {
+  (void)n;
+  View v{q, sigma, x, rho, spc, offs, idx};
+  par_for(nu, [&](int k) {
+    int u = u_list[k];
+    double rq[3] = {0, 0, 0}, rs = 0, rx = 0;
+    if (!(x[u] < kMinOcc)) {
+      // centres: u itself, then every neighbour of u (real or image)
+      int ncen = 1 + offs[u + 1] - offs[u];
+      for (int c = 0; c < ncen; ++c) {
+        int ic = c == 0 ? u : idx[offs[u] + c - 1];
+        int o = owner[ic];
+        const int *T = image + 3 * ic;
+        int uu = u;  // u as seen from the owner's frame
+        if (T[0] != 0 || T[1] != 0 || T[2] != 0) {
+          uu = -1;
+          for (int p = offs[o]; p < offs[o + 1]; ++p) {
+            int cand = idx[p];
+            const int *Tc = image + 3 * cand;
+            if (owner[cand] == u && Tc[0] == -T[0] && Tc[1] == -T[1] &&
+                Tc[2] == -T[2]) {
+              uu = cand;
+              break;
+            }
+          }
+          if (uu < 0) continue;  // pair straddles rc by rounding only
+        }
+        double g4[4];
+        DV0_dq(v, uu, o, g4);
+        double gx = DV0_dx(v, uu, o);
+        double wgt = beta[o] / beta[u];
+        for (int a = 0; a < 3; ++a) rq[a] += wgt * g4[a];
+        rs += wgt * g4[3];
+        rx += wgt * gx;
+      }
+      rs -= 3.0 / (beta[u] * sigma[u]);
+      if (spc[u] == kH) {
+        double xu = x[u];
+        double dlogz = 3.0 / (2.0 * xu) + (xu < 1.0 ? 1.0 / (1.0 - xu) : 0.0);
+        rx -= dlogz / beta[u];
+        if (xu < 0.9999) rx -= gamma[u] / beta[u];
+      } else {
+        rx = 0.0;
+      }
+    }
+    for (int a = 0; a < 3; ++a) Rq[3 * k + a] = rq[a];
+    Rs[k] = rs;
+    Rx[k] = rx;
+  });
+}
+
+}  // extern "C"

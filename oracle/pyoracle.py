@@ -1,0 +1,220 @@
+"""Test infrastructure only: ctypes access to the CPU oracle.
+
+Loads ``oracle/_build/libbtam_oracle.so`` (the restated oracle, always
+buildable with g++) and, when present, ``oracle/_ref/libbtam_ref.so`` (the
+reference's own arithmetic files compiled unmodified; needs the reference
+tree at build time).  Both expose the same per-site entry points with the
+prefixes ``orc_`` and ``ref_``.  Only tests/, __graft_entry__.smoke() and the
+CPU-baseline leg of bench.py use this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "_build", "libbtam_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libbtam_ref.so")
+REF_FAST_SO = os.path.join(HERE, "_ref", "libbtam_ref_fast.so")
+TABLES = os.path.join(os.path.dirname(HERE), "bt-am_b200", "data")
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+
+
+def _d(a):
+    return a.ctypes.data_as(_D)
+
+
+def _i(a):
+    return a.ctypes.data_as(_I)
+
+
+def build_oracle():
+    """Compile the restated oracle if it is missing (g++ only)."""
+    if not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-s", "_build/libbtam_oracle.so"], cwd=HERE,
+                       check=True)
+    return ORACLE_SO
+
+
+class Lib:
+    """One of the two CPU libraries (restated oracle or reference build)."""
+
+    def __init__(self, path, prefix, tables=TABLES):
+        self.path = path
+        self.prefix = prefix
+        self.lib = ctypes.CDLL(path)
+        f = self._f
+        f("spline").restype = ctypes.c_double
+        f("spline").argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int]
+        f("load_tables").argtypes = [ctypes.c_char_p]
+        rc = f("load_tables")(tables.encode())
+        if rc != 0:
+            raise RuntimeError(f"{path}: cannot load ADP tables from {tables}")
+
+    def _f(self, name):
+        return getattr(self.lib, f"{self.prefix}_{name}")
+
+    def spline(self, table, r, deriv=0):
+        return self._f("spline")(table, float(r), deriv)
+
+    def quadrature(self, term, mode, slot, q, sigma, x, spc, coincident=0):
+        q = np.ascontiguousarray(q, np.float64).ravel()
+        sigma = np.ascontiguousarray(sigma, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        spc = np.ascontiguousarray(spc, np.int32)
+        out = np.zeros(3)
+        self._f("quadrature")(term, mode, slot, len(sigma), coincident, _d(q),
+                              _d(sigma), _d(x), _i(spc), _d(out))
+        return out if mode == 1 else out[0]
+
+    # --- per-site drivers over a system with CSR neighbour lists ----------
+    def mf_rho(self, s, offs, idx, sites):
+        sites = np.ascontiguousarray(sites, np.int32)
+        out = np.zeros(len(sites))
+        self._f("mf_rho")(len(s["x"]), _d(s["q"]), _d(s["sigma"]), _d(s["x"]),
+                          _i(s["species"]), _i(offs), _i(idx), _i(sites),
+                          len(sites), _d(out))
+        return out
+
+    def V0(self, s, rho, offs, idx, sites):
+        sites = np.ascontiguousarray(sites, np.int32)
+        out = np.zeros(len(sites))
+        self._f("V0")(len(s["x"]), _d(s["q"]), _d(s["sigma"]), _d(s["x"]),
+                      _i(s["species"]), _d(rho), _i(offs), _i(idx),
+                      _i(sites), len(sites), _d(out))
+        return out
+
+    def S0(self, s, rho, offs, idx, sites):
+        sites = np.ascontiguousarray(sites, np.int32)
+        out = np.zeros(len(sites))
+        self._f("S0")(len(s["x"]), _d(s["q"]), _d(s["sigma"]), _d(s["x"]),
+                      _i(s["species"]), _d(rho), _d(s["beta"]), _d(s["gamma"]),
+                      _i(offs), _i(idx), _i(sites), len(sites), _d(out))
+        return out
+
+    def DV0_pairs(self, s, rho, offs, idx, u_list, i_list):
+        u_list = np.ascontiguousarray(u_list, np.int32)
+        i_list = np.ascontiguousarray(i_list, np.int32)
+        out4 = np.zeros((len(u_list), 4))
+        outx = np.zeros(len(u_list))
+        self._f("DV0_pairs")(len(s["x"]), _d(s["q"]), _d(s["sigma"]),
+                             _d(s["x"]), _i(s["species"]), _d(rho), _i(offs),
+                             _i(idx), _i(u_list), _i(i_list), len(u_list),
+                             _d(out4), _d(outx))
+        return out4, outx
+
+    def rho_nmf(self, s, offs, idx, sites):
+        sites = np.ascontiguousarray(sites, np.int32)
+        out = np.zeros(len(sites))
+        self._f("rho_nmf")(len(s["x"]), _d(s["q"]), _d(s["x"]),
+                           _i(s["species"]), _i(offs), _i(idx), _i(sites),
+                           len(sites), _d(out))
+        return out
+
+
+class Oracle(Lib):
+    """The restated oracle plus its project-defined pieces."""
+
+    def __init__(self, tables=TABLES):
+        super().__init__(build_oracle(), "orc", tables)
+        self._f("mass").restype = ctypes.c_double
+
+    def mass(self, species):
+        return self._f("mass")(int(species))
+
+    def ghosts(self, s, rc=6.2934034034, max_ghosts=None):
+        n = len(s["x"])
+        max_ghosts = max_ghosts or 27 * n
+        qg = np.zeros((max_ghosts, 3))
+        owner = np.zeros(max_ghosts, np.int32)
+        image = np.zeros((max_ghosts, 3), np.int32)
+        ng = ctypes.c_int(0)
+        cell = np.ascontiguousarray(s["cell"], np.float64)
+        origin = np.ascontiguousarray(s["origin"], np.float64)
+        per = np.ascontiguousarray(s["periodic"], np.int32)
+        rc_ = self._f("ghosts")(n, _d(s["q"]), _d(origin), _d(cell), _i(per),
+                                ctypes.c_double(rc), max_ghosts, _d(qg),
+                                _i(owner), _i(image), ctypes.byref(ng))
+        if rc_ != 0:
+            raise RuntimeError(f"orc_ghosts failed with code {rc_}")
+        k = ng.value
+        return qg[:k].copy(), owner[:k].copy(), image[:k].copy()
+
+    def neighbors(self, q, query=None, rc=6.2934034034, maxn=250):
+        q = np.ascontiguousarray(q, np.float64)
+        n = len(q)
+        query = np.arange(n, dtype=np.int32) if query is None else \
+            np.ascontiguousarray(query, np.int32)
+        cap = max(1, len(query)) * maxn
+        offs = np.zeros(len(query) + 1, np.int32)
+        idx = np.zeros(cap, np.int32)
+        rc_ = self._f("neighbors")(n, _d(q), ctypes.c_double(rc), maxn,
+                                   _i(query), len(query), _i(offs), _i(idx), cap)
+        if rc_ != 0:
+            raise RuntimeError(f"orc_neighbors failed with code {rc_}")
+        return offs, idx[:offs[-1]].copy()
+
+    def residuals(self, s, rho, owner, image, offs, idx, u_list):
+        u_list = np.ascontiguousarray(u_list, np.int32)
+        nu = len(u_list)
+        Rq = np.zeros((nu, 3))
+        Rs = np.zeros(nu)
+        Rx = np.zeros(nu)
+        self._f("residuals")(len(s["x"]), _d(s["q"]), _d(s["sigma"]),
+                             _d(s["x"]), _i(s["species"]), _d(s["beta"]),
+                             _d(s["gamma"]), _d(rho), _i(owner), _i(image),
+                             _i(offs), _i(idx), _i(u_list), nu, _d(Rq),
+                             _d(Rs), _d(Rx))
+        return Rq, Rs, Rx
+
+
+def reference(fast=False, tables=TABLES):
+    """The reference's own arithmetic (shim build), or None if not built."""
+    path = REF_FAST_SO if fast else REF_SO
+    if not os.path.exists(path):
+        return None
+    return Lib(path, "ref", tables)
+
+
+def expand(sys_, oracle, rc=6.2934034034):
+    """Real sites + periodic images as one site array, with the owner/image
+    maps, as the oracle evaluates them.  Returns (all-sites dict, n_real,
+    owner, image)."""
+    n = len(sys_["x"])
+    if any(sys_["periodic"]):
+        qg, og, ig = oracle.ghosts(sys_, rc)
+    else:
+        qg = np.zeros((0, 3))
+        og = np.zeros(0, np.int32)
+        ig = np.zeros((0, 3), np.int32)
+    full = dict(sys_)
+    full["q"] = np.ascontiguousarray(np.concatenate([sys_["q"], qg]))
+    for k in ("sigma", "x", "beta", "gamma"):
+        full[k] = np.ascontiguousarray(np.concatenate([sys_[k], sys_[k][og]]))
+    full["species"] = np.ascontiguousarray(
+        np.concatenate([sys_["species"], sys_["species"][og]]).astype(np.int32))
+    owner = np.concatenate([np.arange(n, dtype=np.int32), og]).astype(np.int32)
+    image = np.concatenate([np.zeros((n, 3), np.int32), ig]).astype(np.int32)
+    return full, n, np.ascontiguousarray(owner), np.ascontiguousarray(image)
+
+
+def evaluate(sys_, oracle, sites=None, residual_sites=None, rc=6.2934034034):
+    """Full literal evaluation on the real sites of one system: per-site
+    mean-field rho, V0 and S0, and the residuals of ``residual_sites``
+    (default: all real sites)."""
+    full, n, owner, image = expand(sys_, oracle, rc)
+    offs, idx = oracle.neighbors(full["q"], rc=rc)
+    real = np.arange(n, dtype=np.int32) if sites is None else np.asarray(sites, np.int32)
+    rho_real = oracle.mf_rho(full, offs, idx, np.arange(n, dtype=np.int32))
+    rho = rho_real[owner]
+    V0 = oracle.V0(full, rho, offs, idx, real)
+    S0 = oracle.S0(full, rho, offs, idx, real)
+    us = real if residual_sites is None else np.asarray(residual_sites, np.int32)
+    Rq, Rs, Rx = oracle.residuals(full, rho, owner, image, offs, idx, us)
+    return dict(rho=rho_real, V0=V0, S0=S0, Rq=Rq, Rs=Rs, Rx=Rx, offs=offs,
+                idx=idx, full=full, owner=owner, image=image, n_real=n)
