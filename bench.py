@@ -1,0 +1,341 @@
+"""Benchmark: mean-field ADP residual evaluations per second.
+
+One step = one residual evaluation (rho-bar, V0, S0, R_q, R_sigma, R_x and the
+FP64 totals) of the plain drop-in workload: periodic hcp Mg 20x15x15
+hexagonal cells (9000 Mg) with H on all 18000 tetrahedral sites
+(x ~ U[0, 0.3]), positions jittered N(0, 0.02 A), sigma ~ U[0.08, 0.15] A,
+T = 400 K; synthetic, seeded.  Neighbour lists are built once before timing
+(the reference also builds them once, main-BT-AM.cpp:100-104).
+
+Default arm (--impl btam): the FP32-compensated form is the headline
+`value`; the plain FP64 drop-in on the same system is reported beside it.
+`e2e` times the same evaluation through the C ABI with host buffers
+(pinned), including the host->device state copy and the device->host
+residual read.  Reference arm (--impl reference): the reference's own CPU
+arithmetic (oracle/_ref, -Ofast, all host threads) on a bounded sample of the
+same workload, extrapolated to one full evaluation.
+
+Multi-GPU (torchrun): every rank evaluates its own replica (independent
+systems, no data-path collective); value = evaluations of all ranks / max
+rank time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "bt-am_b200"), os.path.join(ROOT, "oracle")]
+
+METRIC = "mean-field ADP residual evals/s & DMD jobs/s, p50/p99, vs plain FP64 on GPU"
+WORKLOAD = ("plain drop-in: periodic hcp Mg 20x15x15 hexagonal cells, 9000 Mg + 18000 "
+            "tetrahedral H sites (x~U[0,0.3]), jitter N(0,0.02 A), sigma~U[0.08,0.15] A, "
+            "T=400 K, seed 2")
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FLOP_PASS1, FLOP_PASS2 = 1000.0, 2000.0  # algorithmic flops per directed active pair
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device),
+                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
+                                     capture_output=True, text=True, timeout=5).stdout
+                f = [v.strip() for v in out.strip().split(",")]
+                if len(f) == 6:
+                    self.samples.append(f)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4)
+                          if s[2 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def active_pairs(sys_, offs, idx, owner):
+    x = sys_["x"]
+    n = len(x)
+    xa = x[owner]
+    act_i = np.repeat(x >= 5e-4, np.diff(offs[:n + 1]))
+    return int(np.sum(act_i & (xa[idx] >= 5e-4)))
+
+
+def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0):
+    """Times the reference's own arithmetic (oracle/_ref, -Ofast build, all
+    host threads) on a bounded sample of one evaluation and extrapolates.
+    Returns (evals_per_s, description)."""
+    import pyoracle
+    ref = pyoracle.reference(fast=True)
+    kind = "reference"
+    orc = pyoracle.Oracle()
+    if ref is None:
+        ref, kind = orc, "port"
+    os.environ["BTAM_REF_THREADS"] = str(threads)
+    os.environ["BTAM_ORACLE_THREADS"] = str(threads)
+    rng = np.random.default_rng(seed)
+    n = len(sys_["x"])
+    full, nr, owner, image = pyoracle.expand(sys_, orc)
+    # neighbour lists of the sampled sites and of their neighbours' owners
+    sample_rho = np.sort(rng.choice(n, 1200, replace=False)).astype(np.int32)
+    sample_v0 = sample_rho[::12]
+    sample_res = sample_rho[::100]
+    need = set(map(int, sample_rho))
+    o1, i1 = orc.neighbors(full["q"], query=sample_res)
+    for j in i1:
+        need.add(int(owner[j]))
+    query = np.array(sorted(need), np.int32)
+    oq, iq = orc.neighbors(full["q"], query=query)
+    counts = np.zeros(len(full["x"]), np.int64)
+    counts[query] = np.diff(oq)
+    offs = np.zeros(len(full["x"]) + 1, np.int32)
+    offs[1:] = np.cumsum(counts)
+    idx = np.zeros(offs[-1], np.int32)
+    for k, qi in enumerate(query):
+        idx[offs[qi]:offs[qi + 1]] = iq[oq[k]:oq[k + 1]]
+    t0 = time.perf_counter()
+    rho_q = ref.mf_rho(full, offs, idx, query)
+    t_rho = (time.perf_counter() - t0) / len(query)
+    rho_real = np.zeros(nr)
+    rho_real[query] = rho_q
+    rho = rho_real[owner]
+    t0 = time.perf_counter()
+    ref.V0(full, rho, offs, idx, sample_v0)
+    t_v0 = (time.perf_counter() - t0) / len(sample_v0)
+    # residual of a site: dV0_i/d(q,sigma) and dV0_i/dx over i in {u} U N(u)
+    us, is_ = [], []
+    for u in sample_res:
+        for i in [u, *idx[offs[u]:offs[u + 1]]]:
+            us.append(int(u))
+            is_.append(int(owner[i]) if int(owner[i]) == int(i) else int(owner[i]))
+    t0 = time.perf_counter()
+    ref.DV0_pairs(full, rho, offs, idx, us, is_)
+    t_res = (time.perf_counter() - t0) / len(sample_res)
+    t_full = n * (t_rho + t_v0 + t_res)
+    desc = (f"{kind} arithmetic on {threads} threads: rho-bar of {len(query)} sites, V0 of "
+            f"{len(sample_v0)} sites, residual assembly (dV0_i/d(q,sigma,x) over i in "
+            f"{{u}}+N(u)) of {len(sample_res)} sites, each scaled to all {n} sites")
+    return 1.0 / t_full, desc, kind, t_full
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    from btam import lattice
+    sys_ = lattice.config2()
+    threads = os.cpu_count() or 1
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, desc, kind, _ = cpu_reference_sample(sys_, threads, seed=k)
+        if k >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sites": len(sys_["x"])},
+            "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads,
+                             "kind": kind, "sample": desc},
+            "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_btam(args, ws, rank, local):
+    import torch
+    import btam
+    from btam import lattice
+
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    sys_ = lattice.config2()
+    n = len(sys_["x"])
+    tables = btam.Tables()
+    S = btam.System(tables, sys_)
+    S.build_neighbors()
+    nr, ng, npairs = S.info()
+    offs, idx = S.neighbors()
+    owner = np.concatenate([np.arange(n), S.ghosts()[1]]).astype(np.int64)
+    P = active_pairs(sys_, offs, idx, owner)
+    stream = torch.cuda.ExternalStream(S.stream)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed_steps(prec, k):
+        evs = []
+        for _ in range(k):
+            with torch.cuda.stream(stream):
+                flush.add_(1.0)  # evict the working set from L2 between steps
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                S.evaluate_async(prec)
+                b.record(stream)
+            evs.append((a, b))
+        S.sync()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    results = {}
+    clocks = None
+    for prec, name in ((btam.FP32C, "fp32c"), (btam.FP64, "fp64")):
+        timed_steps(prec, args.warmup)
+        barrier()
+        with ClockSampler(local) as cs:
+            ms = timed_steps(prec, args.steps)
+            barrier()
+        if name == "fp32c":
+            clocks = cs.summary()
+        step_ms = max_over_ranks(float(np.mean(ms)))
+        results[name] = dict(ms=step_ms, value=ws * 1e3 / step_ms)
+    # per-kernel times for the roofline (FP32C form)
+    prof = np.array([S.profile(btam.FP32C) for _ in range(5)])
+    prof64 = np.array([S.profile(btam.FP64) for _ in range(5)])
+    p1, p2, _ = np.median(prof, axis=0)
+    p1d, p2d, _ = np.median(prof64, axis=0)
+    fp32_peak = btam.probe_fma_peak(False, 0.5)
+    fp64_peak = btam.probe_fma_peak(True, 0.5)
+    dom = "pass2" if p2 >= p1 else "pass1"
+    dom_ms = max(p1, p2)
+    dom_flops = (FLOP_PASS2 if dom == "pass2" else FLOP_PASS1) * P
+    achieved = dom_flops / (dom_ms * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": f"{dom} (FP32C)", "achieved": achieved,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                "traffic": None,
+                "peak_source": "measured live: btam_probe_fma_peak FP32 FMA loop on all SMs",
+                "flops_per_launch": dom_flops,
+                "pass1_ms": p1, "pass2_ms": p2,
+                "fp64_form": {"pass1_ms": p1d, "pass2_ms": p2d, "fp64_peak": fp64_peak,
+                              "frac_pass2": FLOP_PASS2 * P / (p2d * 1e-3) / 1e12 / fp64_peak}}
+    # e2e through the C ABI with pinned host buffers
+    qh = torch.from_numpy(sys_["q"]).pin_memory().numpy()
+    sh = torch.from_numpy(sys_["sigma"]).pin_memory().numpy()
+    xh = torch.from_numpy(sys_["x"]).pin_memory().numpy()
+    outs = {k: torch.zeros(sh_, dtype=torch.float64).pin_memory().numpy()
+            for k, sh_ in (("Rq", (n, 3)), ("Rs", (n,)), ("Rx", (n,)), ("totals", (4,)))}
+    lib = btam.lib()
+
+    def e2e_step():
+        S.set_state(q=qh, sigma=sh, x=xh)
+        code = lib.btam_mf_eval(S.handle, btam.FP32C, None, None, None,
+                                btam._d(outs["Rq"]), btam._d(outs["Rs"]), btam._d(outs["Rx"]),
+                                btam._d(outs["totals"]))
+        if code:
+            raise btam.BtamError(code, "btam_mf_eval")
+
+    for _ in range(args.warmup):
+        e2e_step()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    barrier()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    h2d = n * (24 + 8 + 8)
+    d2h = n * (24 + 8 + 8) + 32
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
+        cpu = {"value": v, "unit": "evals/s", "cores": os.cpu_count() or 1, "kind": kind,
+               "sample": desc}
+    if rank == 0:
+        line = {"metric": METRIC, "value": results["fp32c"]["value"], "unit": "evals/s",
+                "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": results["fp32c"]["ms"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32c",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "sites": n, "images": ng,
+                           "directed_active_pairs": P, "precision": "fp32c",
+                           "l2": "flushed between steps (256 MiB write, outside step events)",
+                           "parallelism": f"{ws} independent replica(s), no collective"},
+                "fp64_drop_in": {"value": results["fp64"]["value"], "unit": "evals/s",
+                                 "ms_per_step": results["fp64"]["ms"]},
+                "fp32c_over_fp64": results["fp32c"]["value"] / results["fp64"]["value"],
+                "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": {"value": ws * 1e3 / e2e_ms, "unit": "evals/s",
+                        "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "ms_per_step": e2e_ms},
+                "gpu_launches": 3 * args.steps,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="btam", choices=["btam", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+    else:
+        run_btam(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,269 @@
+"""Python bindings of libbtam.so (the C ABI in include/btam.h).
+
+Thin ctypes wrappers: every call goes to the CUDA library; there is no
+Python or CPU implementation of the path.  Importing works without a GPU;
+creating tables or systems needs a CUDA device and the built library
+(``python bt-am_b200/build.py``), and raises otherwise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+LIB_PATH = os.path.join(PKG, "lib", "libbtam.so")
+TABLES_DIR = os.path.join(PKG, "data")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "btam.h")
+
+FP64 = 0
+FP32C = 1
+R_CUTOFF = 6.2934034034
+MAXNEIGH = 250
+MIN_OCCUPANCY = 5e-4
+
+STATUS = {
+    0: "BTAM_OK", 1: "BTAM_ERR_ARG", 2: "BTAM_ERR_IO",
+    3: "BTAM_ERR_NEIGHBOR_OVERFLOW", 4: "BTAM_ERR_NO_NEIGHBORS",
+    5: "BTAM_ERR_BOX_TOO_SMALL", 6: "BTAM_ERR_NONFINITE", 7: "BTAM_ERR_OOM",
+    8: "BTAM_ERR_CUDA", 9: "BTAM_ERR_GHOST_OVERFLOW", 10: "BTAM_ERR_OCCUPANCY",
+    11: "BTAM_ERR_SPECIES", 12: "BTAM_ERR_TIMEOUT", 13: "BTAM_ERR_NOT_BUILT",
+    14: "BTAM_ERR_OUT_OF_BOX",
+}
+
+
+class BtamError(RuntimeError):
+    def __init__(self, code, what=""):
+        self.code = code
+        super().__init__(f"{what}: {STATUS.get(code, code)}")
+
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I = ctypes.POINTER(ctypes.c_int)
+_V = ctypes.c_void_p
+
+_PROTOS = {
+    "btam_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "btam_version": (ctypes.c_int, []),
+    "btam_tables_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_V)]),
+    "btam_tables_destroy": (None, [_V]),
+    "btam_tables_mass": (ctypes.c_double, [_V, ctypes.c_int]),
+    "btam_tables_spline": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D, _D, _D]),
+    "btam_system_create": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _I, _D, _D, _D, _D,
+                                          _I, ctypes.POINTER(_V)]),
+    "btam_system_destroy": (None, [_V]),
+    "btam_system_set_state": (ctypes.c_int, [_V, _D, _D, _D]),
+    "btam_system_info": (ctypes.c_int, [_V, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_system_stream": (_V, [_V]),
+    "btam_neighbors_build": (ctypes.c_int, [_V, ctypes.c_int]),
+    "btam_neighbors_copy": (ctypes.c_int, [_V, _I, _I, ctypes.c_longlong]),
+    "btam_ghosts_copy": (ctypes.c_int, [_V, _D, _I, _I]),
+    "btam_mf_rho": (ctypes.c_int, [_V, ctypes.c_int, _D]),
+    "btam_mf_eval": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D]),
+    "btam_mf_eval_async": (ctypes.c_int, [_V, ctypes.c_int]),
+    "btam_results_copy": (ctypes.c_int, [_V, _D, _D, _D, _D, _D, _D, _D]),
+    "btam_system_sync": (ctypes.c_int, [_V]),
+    "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
+    "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
+    "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
+}
+
+_lib = None
+
+
+def lib():
+    """The loaded CUDA library.  Raises if it has not been built: there is no
+    fallback implementation."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing; build it with "
+                               "`python bt-am_b200/build.py` (needs nvcc)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def exported_symbols():
+    """Names declared in include/btam.h (for the symbol-export test)."""
+    import re
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(btam_[a-z0-9_]+)\s*\(", text)))
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_D)
+
+
+def _i(a):
+    return None if a is None else a.ctypes.data_as(_I)
+
+
+def _check(code, what):
+    if code != 0:
+        raise BtamError(code, what)
+
+
+def probe_fma_peak(fp64=False, seconds=0.5):
+    """Measured FMA throughput (TFLOP/s) of the current device."""
+    out = np.zeros(1)
+    _check(lib().btam_probe_fma_peak(int(fp64), float(seconds), _d(out)),
+           "btam_probe_fma_peak")
+    return float(out[0])
+
+
+class Tables:
+    """The ADP tables on the device (init_adp_MgHx for MgMg, HH and MgH)."""
+
+    def __init__(self, directory=TABLES_DIR):
+        h = _V()
+        _check(lib().btam_tables_load(directory.encode(), ctypes.byref(h)),
+               "btam_tables_load")
+        self.handle = h
+
+    def mass(self, species):
+        return lib().btam_tables_mass(self.handle, int(species))
+
+    def spline(self, table, r):
+        r = np.ascontiguousarray(r, np.float64)
+        v = np.zeros_like(r)
+        dv = np.zeros_like(r)
+        _check(lib().btam_tables_spline(self.handle, table, len(r), _d(r), _d(v), _d(dv)),
+               "btam_tables_spline")
+        return v, dv
+
+    def close(self):
+        if self.handle:
+            lib().btam_tables_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class System:
+    """One device-resident system (the reference's DMSwarm of sites)."""
+
+    def __init__(self, tables, sysdict):
+        s = sysdict
+        self.tables = tables
+        self.n = len(s["x"])
+        q = np.ascontiguousarray(s["q"], np.float64)
+        sigma = np.ascontiguousarray(s["sigma"], np.float64)
+        x = np.ascontiguousarray(s["x"], np.float64)
+        spc = np.ascontiguousarray(s["species"], np.int32)
+        beta = np.ascontiguousarray(s.get("beta"), np.float64) if s.get("beta") is not None else None
+        gamma = np.ascontiguousarray(s.get("gamma"), np.float64) if s.get("gamma") is not None else None
+        origin = np.ascontiguousarray(s["origin"], np.float64)
+        cell = np.ascontiguousarray(s["cell"], np.float64).reshape(9)
+        per = np.ascontiguousarray(s["periodic"], np.int32)
+        h = _V()
+        _check(lib().btam_system_create(tables.handle, self.n, _d(q), _d(sigma), _d(x),
+                                        _i(spc), _d(beta), _d(gamma), _d(origin), _d(cell),
+                                        _i(per), ctypes.byref(h)), "btam_system_create")
+        self.handle = h
+        self.all_sites = None
+
+    # -- state and topology
+    def set_state(self, q=None, sigma=None, x=None):
+        q = None if q is None else np.ascontiguousarray(q, np.float64)
+        sigma = None if sigma is None else np.ascontiguousarray(sigma, np.float64)
+        x = None if x is None else np.ascontiguousarray(x, np.float64)
+        _check(lib().btam_system_set_state(self.handle, _d(q), _d(sigma), _d(x)),
+               "btam_system_set_state")
+
+    def build_neighbors(self, all_sites=False):
+        _check(lib().btam_neighbors_build(self.handle, int(bool(all_sites))),
+               "btam_neighbors_build")
+        self.all_sites = bool(all_sites)
+
+    def info(self):
+        nr, ng, npairs = ctypes.c_int(), ctypes.c_int(), ctypes.c_longlong()
+        _check(lib().btam_system_info(self.handle, ctypes.byref(nr), ctypes.byref(ng),
+                                      ctypes.byref(npairs)), "btam_system_info")
+        return nr.value, ng.value, npairs.value
+
+    def neighbors(self):
+        nr, ng, npairs = self.info()
+        n_list = nr + ng if self.all_sites else nr
+        offs = np.zeros(n_list + 1, np.int32)
+        idx = np.zeros(max(npairs, 1), np.int32)
+        _check(lib().btam_neighbors_copy(self.handle, _i(offs), _i(idx), len(idx)),
+               "btam_neighbors_copy")
+        return offs, idx[:npairs]
+
+    def ghosts(self):
+        nr, ng, _ = self.info()
+        q = np.zeros((ng, 3))
+        owner = np.zeros(ng, np.int32)
+        image = np.zeros((ng, 3), np.int32)
+        if ng:
+            _check(lib().btam_ghosts_copy(self.handle, _d(q), _i(owner), _i(image)),
+                   "btam_ghosts_copy")
+        return q, owner, image
+
+    @property
+    def stream(self):
+        return lib().btam_system_stream(self.handle)
+
+    # -- evaluation
+    def mf_rho(self, precision=FP64):
+        out = np.zeros(self.n)
+        _check(lib().btam_mf_rho(self.handle, precision, _d(out)), "btam_mf_rho")
+        return out
+
+    def evaluate(self, precision=FP64):
+        n = self.n
+        out = dict(rho=np.zeros(n), V0=np.zeros(n), S0=np.zeros(n), Rq=np.zeros((n, 3)),
+                   Rs=np.zeros(n), Rx=np.zeros(n), totals=np.zeros(4))
+        _check(lib().btam_mf_eval(self.handle, precision, _d(out["rho"]), _d(out["V0"]),
+                                  _d(out["S0"]), _d(out["Rq"]), _d(out["Rs"]), _d(out["Rx"]),
+                                  _d(out["totals"])), "btam_mf_eval")
+        return out
+
+    def evaluate_async(self, precision=FP64):
+        _check(lib().btam_mf_eval_async(self.handle, precision), "btam_mf_eval_async")
+
+    def sync(self):
+        _check(lib().btam_system_sync(self.handle), "btam_system_sync")
+
+    def results(self, want=("V0", "Rq", "Rs", "Rx", "totals")):
+        n = self.n
+        shapes = dict(rho=(n,), V0=(n,), S0=(n,), Rq=(n, 3), Rs=(n,), Rx=(n,), totals=(4,))
+        out = {k: np.zeros(shapes[k]) for k in want}
+        args = [_d(out.get(k)) for k in ("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals")]
+        _check(lib().btam_results_copy(self.handle, *args), "btam_results_copy")
+        return out
+
+    def profile(self, precision=FP64):
+        """Per-kernel device times (ms) of one evaluation: pass 1, pass 2,
+        totals."""
+        ms = np.zeros(3)
+        _check(lib().btam_mf_eval_profile(self.handle, precision, _d(ms)),
+               "btam_mf_eval_profile")
+        return ms
+
+    def rho_nmf(self):
+        out = np.zeros(self.n)
+        _check(lib().btam_rho_nmf(self.handle, _d(out)), "btam_rho_nmf")
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().btam_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

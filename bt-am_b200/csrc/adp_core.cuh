@@ -1,0 +1,601 @@
+// Mean-field ADP arithmetic shared by the CUDA kernels (adp_kernels.cu).
+//
+// The reference evaluates, per site i, the degree-3 Gauss-Hermite average of
+// the ADP terms over its neighbours (MgHx-mf-V-bulk.cpp:708-953): the pair
+// terms rho and phi with the 12-point pair rule (dimension 6, offset
+// sqrt(6) sigma, weight 1/12) and the dipole/quadrupole terms over all
+// neighbour pairs j1 <= j2 with the 18-point triplet rule (dimension 9,
+// offset 3 sigma, weight 1/18) or, for j1 == j2, the merged 12-point rule.
+// Every quadrature point moves exactly one group along one axis, and the
+// angular terms are the symmetric bilinear form
+//     B(g1, g2) = 1/2 a1.a2 + 1/2 L1:L2 - 1/6 tr L1 tr L2
+// of the per-neighbour features g = (a, L) = x_i x_j (u(r) r, w(r) r (x) r)
+// (MgHx-ADP.cpp:1233-1281, 1781-1831).  So the O(N_nb^2) triplet sum is
+// exactly, up to rounding, a sum of O(N_nb) per-site moments:
+//   sum_{j1<=j2} f * <V_ang>  =  1/18 sum_d [B(G(d),G(d)) - sum_j B(g_j(d),g_j(d))]
+//                              + 2/18 [B(H, G0) - sum_j B(h_j, g_j(r0))]
+//                              + 1/12 sum_j sum_{12 pts} B(g_j, g_j)
+// with G0 = sum_j g_j(r0_j), G(d) = sum_j g_j(r0_j + d) for the six centre
+// displacements d = +-3 sigma_i e_k, h_j = sum of g_j over the six
+// neighbour displacements -+3 sigma_j e_k, H = sum_j h_j.  Gradients are the
+// exact derivatives of this closed form, which equals what the reference's
+// _dmq/_dsq/_dxi rules return (Quadrature-Hermitian-3th.cpp:114-378).
+//
+// Pass 1 (per centre site) accumulates rho-bar, the pair/diagonal energies
+// and the moments G0, G(d), H; pass 2 (per site u, over its neighbours j)
+// adds dV0_u/d(q_u, sigma_u) from u's moments and dV0_j/d(q_u, sigma_u, x_u)
+// from j's moments.  All functions here are per pair and templated on the
+// arithmetic type R (double: plain FP64 form; float: FP32 form whose callers
+// accumulate with compensated sums).
+#pragma once
+
+#if defined(__CUDACC__)
+#define BTAM_HD __host__ __device__ __forceinline__
+#else
+#define BTAM_HD inline
+#endif
+
+#include <cmath>
+#include <cstdint>
+
+namespace btam {
+
+// Degree-3 rule constants (Quadrature-Hermitian-3th.cpp:56-60).
+constexpr double kDelta9 = 3.0;                 // sqrt(9)
+constexpr double kDelta6 = 2.449489742783178;   // sqrt(6)
+constexpr double kW9 = 1.0 / 18.0;
+constexpr double kW6 = 1.0 / 12.0;
+constexpr double kMinOcc = 5e-4;                // min_occupancy (Macros.hpp:869)
+
+// Table slots in the packed table array.
+enum TableId : int {
+  T_RHO_MG = 0, T_RHO_H = 1, T_F_MG = 2, T_F_H = 3,
+  T_PHI = 4,   // + pair kind (0 MgMg, 1 HH, 2 MgH)
+  T_U = 7, T_W = 10, T_COUNT = 13
+};
+
+template <class R> struct Coef4 { R a, b, c, d; };
+
+// One uniform-knot cubic spline (cubic-spline.cpp:84-112): segment
+// m = min(floor(r/dx), n-1), p = min(r - m dx, dx), value a+(b+(c+d p)p)p,
+// derivative b+(2c+3d p)p (the reference's db/dc/dd columns equal b, 2c, 3d).
+template <class R> struct SplineView {
+  const Coef4<R> *c;
+  R dx, inv_dx;
+  int n;
+};
+
+template <class R> struct TablesView {
+  SplineView<R> t[T_COUNT];
+};
+
+template <class R> BTAM_HD R rmin(R a, R b) { return a < b ? a : b; }
+
+template <class R>
+BTAM_HD void spline_vd(const SplineView<R> &s, R r, R &v, R &dv) {
+  int m = (int)(r * s.inv_dx);
+  m = m < s.n - 1 ? m : s.n - 1;
+  R p = rmin(r - (R)m * s.dx, s.dx);
+#if defined(__CUDA_ARCH__)
+  Coef4<R> k;
+  if (sizeof(R) == 4) {
+    float4 t = __ldg(reinterpret_cast<const float4 *>(s.c) + m);
+    k.a = (R)t.x; k.b = (R)t.y; k.c = (R)t.z; k.d = (R)t.w;
+  } else {
+    const double2 *q = reinterpret_cast<const double2 *>(s.c) + 2 * m;
+    double2 t0 = __ldg(q), t1 = __ldg(q + 1);
+    k.a = (R)t0.x; k.b = (R)t0.y; k.c = (R)t1.x; k.d = (R)t1.y;
+  }
+#else
+  Coef4<R> k = s.c[m];
+#endif
+  v = k.a + (k.b + (k.c + k.d * p) * p) * p;
+  dv = k.b + ((R)2 * k.c + (R)3 * k.d * p) * p;
+}
+
+template <class R> BTAM_HD R spline_v(const SplineView<R> &s, R r) {
+  R v, dv;
+  spline_vd(s, r, v, dv);
+  return v;
+}
+
+template <class R> struct V3 {
+  R x, y, z;
+};
+template <class R> BTAM_HD V3<R> mk3(R x, R y, R z) { return V3<R>{x, y, z}; }
+template <class R> BTAM_HD R dot3(const V3<R> &a, const V3<R> &b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <class R> BTAM_HD R comp(const V3<R> &a, int k) {
+  return k == 0 ? a.x : (k == 1 ? a.y : a.z);
+}
+template <class R> BTAM_HD V3<R> disp(const V3<R> &r, int k, R amount) {
+  V3<R> o = r;
+  if (k == 0) o.x += amount;
+  else if (k == 1) o.y += amount;
+  else o.z += amount;
+  return o;
+}
+
+template <class R> BTAM_HD R my_sqrt(R v) { return std::sqrt(v); }
+#if defined(__CUDA_ARCH__)
+template <> __device__ __forceinline__ float my_sqrt<float>(float v) { return sqrtf(v); }
+#endif
+
+// A feature sum (a, L) with L symmetric stored (xx, yy, zz, xy, xz, yz).
+template <class R> struct Feat {
+  R a[3], l[6];
+};
+
+// A bilinear-form dual D of a feature sum X, stored as (Da, Lambda) with
+// Lambda the full symmetric matrix such that B(X, Y) = Da.Ya + Lambda:Y_L:
+//   Da = a/2, Lambda_kk = L_kk/2 - tr L/6, Lambda_kl = L_kl/2 (k != l).
+template <class R> struct Dual {
+  R a[3], d[3], o[3];  // d: xx,yy,zz; o: xy,xz,yz
+};
+
+template <class R, class S> BTAM_HD Dual<R> dual_of(const S *a, const S *l) {
+  Dual<R> D;
+  S tr = l[0] + l[1] + l[2];
+  for (int k = 0; k < 3; ++k) D.a[k] = (R)(0.5 * a[k]);
+  for (int k = 0; k < 3; ++k) D.d[k] = (R)(0.5 * l[k] - tr / 6.0);
+  for (int k = 0; k < 3; ++k) D.o[k] = (R)(0.5 * l[3 + k]);
+  return D;
+}
+
+// B(X, X) of a feature sum, evaluated in double.
+template <class S> BTAM_HD double bself(const S *a, const S *l) {
+  double aa = (double)a[0] * a[0] + (double)a[1] * a[1] + (double)a[2] * a[2];
+  double ll = (double)l[0] * l[0] + (double)l[1] * l[1] + (double)l[2] * l[2] +
+              2.0 * ((double)l[3] * l[3] + (double)l[4] * l[4] + (double)l[5] * l[5]);
+  double tr = (double)l[0] + l[1] + l[2];
+  return 0.5 * aa + 0.5 * ll - tr * tr / 6.0;
+}
+
+// B(X, Y) for two feature sums, in double.
+template <class S> BTAM_HD double bpair(const S *a, const S *l, const S *b, const S *m) {
+  double ab = (double)a[0] * b[0] + (double)a[1] * b[1] + (double)a[2] * b[2];
+  double lm = (double)l[0] * m[0] + (double)l[1] * m[1] + (double)l[2] * m[2] +
+              2.0 * ((double)l[3] * m[3] + (double)l[4] * m[4] + (double)l[5] * m[5]);
+  double t1 = (double)l[0] + l[1] + l[2], t2 = (double)m[0] + m[1] + m[2];
+  return 0.5 * ab + 0.5 * lm - t1 * t2 / 6.0;
+}
+
+// Lambda r
+template <class R> BTAM_HD V3<R> lam_r(const Dual<R> &D, const V3<R> &r) {
+  return mk3<R>(D.d[0] * r.x + D.o[0] * r.y + D.o[1] * r.z,
+                D.o[0] * r.x + D.d[1] * r.y + D.o[2] * r.z,
+                D.o[1] * r.x + D.o[2] * r.y + D.d[2] * r.z);
+}
+
+// Spline values at one displaced geometry.
+template <class R> struct Geo {
+  V3<R> r;
+  R s, inv_s;     // |r|, 1/|r|
+  R u, du, w, dw; // dipole and quadrupole splines and derivatives
+};
+
+template <class R>
+BTAM_HD void geo_eval(Geo<R> &g, const V3<R> &r, const SplineView<R> &tu,
+                      const SplineView<R> &tw) {
+  g.r = r;
+  R s2 = dot3(r, r);
+  g.s = my_sqrt(s2);
+  g.inv_s = (R)1 / g.s;
+  spline_vd(tu, g.s, g.u, g.du);
+  spline_vd(tw, g.s, g.w, g.dw);
+}
+
+// D . f(r) with f(r) = (u r, w r r^T):  u (Da.r) + w (r^T Lambda r)
+template <class R> BTAM_HD R dual_f(const Dual<R> &D, const Geo<R> &g) {
+  V3<R> Da = mk3<R>(D.a[0], D.a[1], D.a[2]);
+  V3<R> Lr = lam_r(D, g.r);
+  return g.u * dot3(Da, g.r) + g.w * dot3(g.r, Lr);
+}
+
+// D . J(r) with J = df/dr:  u Da + [(u'/s) Da.r + (w'/s) r^T Lambda r] r + 2 w Lambda r
+template <class R> BTAM_HD V3<R> dual_J(const Dual<R> &D, const Geo<R> &g) {
+  V3<R> Da = mk3<R>(D.a[0], D.a[1], D.a[2]);
+  V3<R> Lr = lam_r(D, g.r);
+  R c = (g.du * dot3(Da, g.r) + g.dw * dot3(g.r, Lr)) * g.inv_s;
+  R tw = (R)2 * g.w;
+  return mk3<R>(g.u * Da.x + c * g.r.x + tw * Lr.x,
+                g.u * Da.y + c * g.r.y + tw * Lr.y,
+                g.u * Da.z + c * g.r.z + tw * Lr.z);
+}
+
+// B(f, f) = u^2 s^2 / 2 + w^2 s^4 / 3 at one geometry, and its gradient
+// [u u' s + u^2 + 2/3 w w' s^3 + 4/3 w^2 s^2] r.
+template <class R> BTAM_HD R bff(const Geo<R> &g) {
+  R s2 = g.s * g.s;
+  return (R)0.5 * g.u * g.u * s2 + g.w * g.w * s2 * s2 / (R)3;
+}
+template <class R> BTAM_HD R bff_grad_coef(const Geo<R> &g) {
+  R s2 = g.s * g.s;
+  return g.u * g.du * g.s + g.u * g.u +
+         ((R)2 / (R)3) * g.w * g.dw * s2 * g.s + ((R)4 / (R)3) * g.w * g.w * s2;
+}
+
+// Dual of X f(r0) (one feature scaled by X).
+template <class R> BTAM_HD Dual<R> dual_feat(const Geo<R> &g, R X) {
+  Dual<R> D;
+  R hu = (R)0.5 * X * g.u, hw = (R)0.5 * X * g.w;
+  R s2 = g.s * g.s;
+  D.a[0] = hu * g.r.x; D.a[1] = hu * g.r.y; D.a[2] = hu * g.r.z;
+  R t = X * g.w * s2 / (R)6;
+  D.d[0] = hw * g.r.x * g.r.x - t;
+  D.d[1] = hw * g.r.y * g.r.y - t;
+  D.d[2] = hw * g.r.z * g.r.z - t;
+  D.o[0] = hw * g.r.x * g.r.y;
+  D.o[1] = hw * g.r.x * g.r.z;
+  D.o[2] = hw * g.r.y * g.r.z;
+  return D;
+}
+
+template <class R> BTAM_HD void feat_add(Feat<R> &F, const Geo<R> &g) {
+  F.a[0] += g.u * g.r.x; F.a[1] += g.u * g.r.y; F.a[2] += g.u * g.r.z;
+  F.l[0] += g.w * g.r.x * g.r.x; F.l[1] += g.w * g.r.y * g.r.y;
+  F.l[2] += g.w * g.r.z * g.r.z; F.l[3] += g.w * g.r.x * g.r.y;
+  F.l[4] += g.w * g.r.x * g.r.z; F.l[5] += g.w * g.r.y * g.r.z;
+}
+
+template <class R> BTAM_HD Dual<R> dual_sub(const Dual<R> &A, const Dual<R> &B) {
+  Dual<R> D;
+  for (int k = 0; k < 3; ++k) {
+    D.a[k] = A.a[k] - B.a[k];
+    D.d[k] = A.d[k] - B.d[k];
+    D.o[k] = A.o[k] - B.o[k];
+  }
+  return D;
+}
+template <class R> BTAM_HD Dual<R> dual_flip(const Dual<R> &A) {
+  Dual<R> D = A;
+  D.a[0] = -A.a[0]; D.a[1] = -A.a[1]; D.a[2] = -A.a[2];
+  return D;
+}
+
+// Per-site moment record written by pass 1 and read by pass 2.
+// Layout (R units): [0] x_i F'(rho_i), [1] (H ? x_i : 1) F'(rho_i) (the
+// occupancy-gradient embedding factor of MgHx-mf-V-bulk.cpp:2299-2315),
+// [2] beta_i, [3] pad, then 8 duals of 9: G0, H, G(d) for d = (k, s) in the
+// order (x+, x-, y+, y-, z+, z-).
+constexpr int kMomStride = 4 + 8 * 9;  // 76
+constexpr int kMomG0 = 4, kMomH = 13, kMomGd = 22;
+
+template <class R> BTAM_HD Dual<R> load_dual(const R *m) {
+  Dual<R> D;
+  for (int k = 0; k < 3; ++k) {
+    D.a[k] = m[k];
+    D.d[k] = m[3 + k];
+    D.o[k] = m[6 + k];
+  }
+  return D;
+}
+template <class R, class S> BTAM_HD void store_dual(R *m, const Dual<S> &D) {
+  for (int k = 0; k < 3; ++k) {
+    m[k] = (R)D.a[k];
+    m[3 + k] = (R)D.d[k];
+    m[6 + k] = (R)D.o[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pair kind for phi/u/w tables: Mg-Mg, H-H, else Mg-H (MgHx-ADP.cpp:881-888).
+// Species codes: 0 = Mg, 1 = H.
+BTAM_HD int pair_kind(int ci, int cj) { return ci == cj ? ci : 2; }
+
+// ---------------------------------------------------------------------------
+// Pass 1, part A: everything of pair (i, j) except the six centre-displaced
+// triplet moments.  Adds (unscaled by the caller's weights):
+//   rho   += x_j sum_{12 pair pts} rho_{s_j}(|r|)
+//   epair += 1/2 X sum_{12} phi                        (X = x_i x_j)
+//   ediag += X^2 sum_{12} B(f,f)
+//   g0    += X f(r0)
+//   hsum  += X sum_{6 j-displaced triplet pts} f
+//   cross += X^2 B(sum_{6} f, f(r0))
+template <class R> struct Pass1A {
+  R rho, epair, ediag, cross;
+  Feat<R> g0, hsum;
+};
+
+template <class R>
+BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
+                          R sig_j, R xi, R xj, int ci, int cj, Pass1A<R> &o) {
+  const int pk = pair_kind(ci, cj);
+  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
+                      &tp = T.t[T_PHI + pk], &tr = T.t[cj == 0 ? T_RHO_MG : T_RHO_H];
+  const R X = xi * xj;
+  R rho = 0, phi = 0, diag = 0;
+  // 12-point pair rule: centre moves +-sqrt6 sigma_i e_k, neighbour -+sqrt6 sigma_j e_k
+  for (int side = 0; side < 2; ++side) {
+    R amt = (side == 0 ? sig_i : -sig_j) * (R)kDelta6;
+    for (int k = 0; k < 3; ++k)
+      for (int sg = 0; sg < 2; ++sg) {
+        Geo<R> g;
+        geo_eval(g, disp(r0, k, sg ? -amt : amt), tu, tw);
+        rho += spline_v(tr, g.s);
+        phi += spline_v(tp, g.s);
+        diag += bff(g);
+      }
+  }
+  o.rho += xj * rho;
+  o.epair += (R)0.5 * X * phi;
+  o.ediag += X * X * diag;
+  // centre geometry
+  Geo<R> g0;
+  geo_eval(g0, r0, tu, tw);
+  Feat<R> f0{};
+  feat_add(f0, g0);
+  // neighbour-displaced triplet geometries
+  Feat<R> hs{};
+  for (int k = 0; k < 3; ++k)
+    for (int sg = 0; sg < 2; ++sg) {
+      Geo<R> g;
+      R amt = sig_j * (R)kDelta9;
+      geo_eval(g, disp(r0, k, sg ? amt : -amt), tu, tw);
+      feat_add(hs, g);
+    }
+  for (int c = 0; c < 3; ++c) {
+    o.g0.a[c] += X * f0.a[c];
+    o.hsum.a[c] += X * hs.a[c];
+  }
+  for (int c = 0; c < 6; ++c) {
+    o.g0.l[c] += X * f0.l[c];
+    o.hsum.l[c] += X * hs.l[c];
+  }
+  o.cross += X * X * (R)bpair(hs.a, hs.l, f0.a, f0.l);
+}
+
+// Pass 1, part B: one centre displacement d = (k, sg) of pair (i, j):
+//   gd    += X f(r0 + d),   sself += X^2 B(f, f)(r0 + d)
+template <class R>
+BTAM_HD void pass1_pair_B(const TablesView<R> &T, const V3<R> &r0, R sig_i,
+                          R X, int pk, int k, int sg, Feat<R> &gd, R &sself) {
+  Geo<R> g;
+  R amt = sig_i * (R)kDelta9;
+  geo_eval(g, disp(r0, k, sg ? -amt : amt), T.t[T_U + pk], T.t[T_W + pk]);
+  Feat<R> f{};
+  feat_add(f, g);
+  for (int c = 0; c < 3; ++c) gd.a[c] += X * f.a[c];
+  for (int c = 0; c < 6; ++c) gd.l[c] += X * f.l[c];
+  sself += X * X * bff(g);
+}
+
+// ---------------------------------------------------------------------------
+// Pass 2: contributions of neighbour j to the residuals of site u.
+// r0 = q_u - q_j.  mu, mj: moment records of u and of j's owner.
+// embq_u = x_u F'(rho_u); embq_j, embx_j likewise for j; omega = beta_j/beta_u.
+// Outputs (added):  gq (3): dS/dq_u / beta_u pieces, gs: d/dsigma_u,
+// gx: d/dx_u of V0_j (cross term only; the self occupancy term is per site).
+template <class R> struct Pass2Out {
+  R gq[3];
+  R gs;
+  R gx;
+};
+
+// Moment-record readers: plain loads (host, shared memory) or read-only
+// cached global loads (device, neighbour records).
+template <class R> BTAM_HD R ld_plain(const R *p) { return *p; }
+template <class R> BTAM_HD R ld_ro(const R *p) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+template <class R, bool RO> BTAM_HD Dual<R> dual_at(const R *m) {
+  Dual<R> D;
+  for (int k = 0; k < 3; ++k) {
+    D.a[k] = RO ? ld_ro(m + k) : ld_plain(m + k);
+    D.d[k] = RO ? ld_ro(m + 3 + k) : ld_plain(m + 3 + k);
+    D.o[k] = RO ? ld_ro(m + 6 + k) : ld_plain(m + 6 + k);
+  }
+  return D;
+}
+
+template <class R>
+BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
+                        R sig_j, R xu, R xj, int cu, int cj, R embq_u,
+                        R embq_j, R embx_j, R omega, const R *mu,
+                        const R *mj, Pass2Out<R> &o) {
+  const int pk = pair_kind(cu, cj);
+  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
+                      &tp = T.t[T_PHI + pk];
+  const SplineView<R> &trj = T.t[cj == 0 ? T_RHO_MG : T_RHO_H];
+  const SplineView<R> &tru = T.t[cu == 0 ? T_RHO_MG : T_RHO_H];
+  const R X = xu * xj;
+  const R w6 = (R)kW6, w9 = (R)kW9;
+
+  R self_q[3] = {0, 0, 0}, self_s = 0;
+  R cros_q[3] = {0, 0, 0}, cros_s = 0, cros_x = 0;
+
+  // ---- 12-point pair rule geometries: u-displaced (C) and j-displaced (D)
+  {
+    R rho_sum = 0, phi_sum = 0, bff_sum = 0;
+    for (int side = 0; side < 2; ++side) {
+      R amt = (side == 0 ? sig_u : -sig_j) * (R)kDelta6;
+      for (int k = 0; k < 3; ++k)
+        for (int sg = 0; sg < 2; ++sg) {
+          R a = sg ? -amt : amt;
+          Geo<R> g;
+          geo_eval(g, disp(r0, k, a), tu, tw);
+          R rj, drj, ru, dru, ph, dph;
+          spline_vd(trj, g.s, rj, drj);
+          spline_vd(tru, g.s, ru, dru);
+          spline_vd(tp, g.s, ph, dph);
+          R bc = bff_grad_coef(g);
+          // radial coefficient of d/dr for each piece
+          R c_self = w6 * (embq_u * xj * drj * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
+          R c_cros = w6 * (embq_j * xu * dru * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
+          self_q[0] += c_self * g.r.x; self_q[1] += c_self * g.r.y; self_q[2] += c_self * g.r.z;
+          cros_q[0] += c_cros * g.r.x; cros_q[1] += c_cros * g.r.y; cros_q[2] += c_cros * g.r.z;
+          if (side == 0) {  // only u-displaced points depend on sigma_u
+            R sd = (sg ? -(R)kDelta6 : (R)kDelta6) * comp(g.r, k);
+            self_s += c_self * sd;
+            cros_s += c_cros * sd;
+          }
+          rho_sum += ru;
+          phi_sum += ph;
+          bff_sum += bff(g);
+        }
+    }
+    cros_x += w6 * (embx_j * rho_sum + (R)0.5 * xj * phi_sum + (R)2 * X * xj * bff_sum);
+  }
+
+  // ---- triplet geometries
+  Geo<R> gc;
+  geo_eval(gc, r0, tu, tw);
+  const Dual<R> Xf0 = dual_feat(gc, X);  // dual of X f(r0)
+
+  // A: u displaced by +-3 sigma_u e_k.  Self i-displaced term (S4) and the
+  // neighbour-displaced term of j's energy (C5).
+  Feat<R> FA{};
+  {
+    const Dual<R> Dj_g0 = dual_at<R, true>(mj + kMomG0);
+    const Dual<R> Dc5 = dual_sub(dual_flip(Dj_g0), Xf0);
+    for (int k = 0; k < 3; ++k)
+      for (int sg = 0; sg < 2; ++sg) {
+        R amt = sig_u * (R)kDelta9;
+        Geo<R> g;
+        geo_eval(g, disp(r0, k, sg ? -amt : amt), tu, tw);
+        feat_add(FA, g);
+        R hb = (R)0.5 * X * bff_grad_coef(g);
+        V3<R> v4 = dual_J(dual_at<R, false>(mu + kMomGd + 9 * (2 * k + sg)), g);  // S4
+        V3<R> v5 = dual_J(Dc5, g);                 // C5 (first part)
+        R sfac = (R)2 * w9 * X;
+        V3<R> s4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
+        self_q[0] += sfac * s4.x; self_q[1] += sfac * s4.y; self_q[2] += sfac * s4.z;
+        cros_q[0] += sfac * v5.x; cros_q[1] += sfac * v5.y; cros_q[2] += sfac * v5.z;
+        R sd = sg ? -(R)kDelta9 : (R)kDelta9;
+        self_s += sfac * comp(s4, k) * sd;
+        cros_s += sfac * comp(v5, k) * sd;
+        // X5 first piece: (P Dj.g0) . f(r_A) - X B(f(r_A), f0)
+        cros_x += (R)2 * w9 * xj * dual_f(dual_sub(dual_flip(Dj_g0), dual_feat(gc, (R)2 * X)), g);
+      }
+  }
+  // B: j displaced by -+3 sigma_j e_k (centre j displaced by +-3 sigma_j e_k
+  // in j's frame).  Self neighbour-displaced term (S5) and j's centre-
+  // displaced term (C4).
+  Feat<R> FB{};
+  {
+    const Dual<R> Ds5 = dual_sub(dual_at<R, false>(mu + kMomG0), Xf0);
+    for (int k = 0; k < 3; ++k)
+      for (int sg = 0; sg < 2; ++sg) {
+        R amt = sig_j * (R)kDelta9;
+        Geo<R> g;
+        geo_eval(g, disp(r0, k, sg ? amt : -amt), tu, tw);
+        feat_add(FB, g);
+        R sfac = (R)2 * w9 * X;
+        V3<R> v5 = dual_J(Ds5, g);
+        self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
+        const Dual<R> Pj = dual_flip(dual_at<R, true>(mj + kMomGd + 9 * (2 * k + sg)));
+        V3<R> v4 = dual_J(Pj, g);
+        R hb = (R)0.5 * X * bff_grad_coef(g);
+        cros_q[0] += sfac * (v4.x - hb * g.r.x);
+        cros_q[1] += sfac * (v4.y - hb * g.r.y);
+        cros_q[2] += sfac * (v4.z - hb * g.r.z);
+        // X4: (P Dj.gd) . f - X B(f, f)
+        cros_x += (R)2 * w9 * xj * (dual_f(Pj, g) - X * bff(g));
+      }
+  }
+  // centre-geometry pieces of S5 and C5:  (D_H - X dual(F)) . J(r0)
+  {
+    R sfac = (R)2 * w9 * X;
+    Dual<R> dFB = dual_of<R, R>(FB.a, FB.l);
+    Dual<R> dFA = dual_of<R, R>(FA.a, FA.l);
+    for (int k = 0; k < 3; ++k) {
+      dFB.a[k] *= X; dFB.d[k] *= X; dFB.o[k] *= X;
+      dFA.a[k] *= X; dFA.d[k] *= X; dFA.o[k] *= X;
+    }
+    const Dual<R> Dj_h = dual_at<R, true>(mj + kMomH);
+    V3<R> vs = dual_J(dual_sub(dual_at<R, false>(mu + kMomH), dFB), gc);
+    V3<R> vc = dual_J(dual_sub(dual_flip(Dj_h), dFA), gc);
+    self_q[0] += sfac * vs.x; self_q[1] += sfac * vs.y; self_q[2] += sfac * vs.z;
+    cros_q[0] += sfac * vc.x; cros_q[1] += sfac * vc.y; cros_q[2] += sfac * vc.z;
+    // X5 second piece: (P Dj.h) . f0  (its -2X B(F_A, f0) part was summed in
+    // the A loop above)
+    cros_x += (R)2 * w9 * xj * dual_f(dual_flip(Dj_h), gc);
+  }
+
+  for (int k = 0; k < 3; ++k) o.gq[k] += self_q[k] + omega * cros_q[k];
+  o.gs += self_s + omega * cros_s;
+  o.gx += omega * cros_x;
+}
+
+// ---------------------------------------------------------------------------
+// Per-site epilogue of pass 1, in double.  Inputs are the raw sums over the
+// site's active neighbours (Pass1A fields and the six G(d) sums).
+struct SiteSums {
+  double rho, epair, ediag, cross, sself;
+  double g0a[3], g0l[6], ha[3], hl[6];
+  double gda[6][3], gdl[6][6];
+};
+
+struct SiteResult {
+  double rho, V0, S0, selfx;
+};
+
+// Physical constants of the reference (Macros.hpp:846-854).
+constexpr double kHbar = 6.5821192815E-4;   // eV ps
+constexpr double kUma = 103.4993333E-6;     // eV A^-2 ps^2 per amu
+
+// Energy of one site:  V0_i = x_i F(rho) + E_pair + E_angular
+// (evaluate_V0_i_adp_MgHx, MgHx-mf-V-bulk.cpp:791-953), its free entropy
+// S0_i (evaluate_S0_i_adp_MgHx, 957-1142), dV0_i/dx_i, and the moment
+// record for pass 2 (layout at kMomStride).
+template <class M>
+BTAM_HD void site_epilogue(const SiteSums &S, const SplineView<double> &emb,
+                           double xi, int code, double beta, double gamma,
+                           double sigma, double mass, SiteResult &res, M *mom) {
+  const double rho = kW6 * S.rho;
+  double F, dF;
+  spline_vd(emb, rho, F, dF);
+  const double e_pair = kW6 * S.epair;
+  const double e_diag = kW6 * S.ediag;
+  double bgd = 0.0;
+  for (int d = 0; d < 6; ++d) bgd += bself(S.gda[d], S.gdl[d]);
+  const double e_id = kW9 * (bgd - S.sself);
+  const double e_jd = 2.0 * kW9 * (bpair(S.ha, S.hl, S.g0a, S.g0l) - S.cross);
+  const double e_ang = e_id + e_jd + e_diag;
+  const double V0 = xi * F + e_pair + e_ang;
+  res.rho = rho;
+  res.V0 = V0;
+  // dV0_i/dx_i: H embedding F(rho) (2299-2302); Mg has none (2312-2315);
+  // pair and angular terms are linear / quadratic in x_i.
+  res.selfx = (code == 1 ? F : 0.0) + (e_pair + 2.0 * e_ang) / xi;
+  // S0_i = -log Z0 + beta (1/(2 beta) + V0) - gamma x~
+  double m = kUma * xi * mass;
+  double logZ = 3.0 * std::log((sigma * std::sqrt(m / beta)) / kHbar);
+  if (xi < 1.0) logZ += std::log(1.0 / (1.0 - xi));
+  double gx = (code == 1) ? gamma * (xi > 0.9999 ? 0.9999 : xi) : 0.0;
+  res.S0 = -logZ + beta * (1.0 / (2.0 * beta) + V0) - gx;
+  if (mom) {
+    mom[0] = (M)(xi * dF);
+    mom[1] = (M)((code == 1 ? xi : 1.0) * dF);
+    mom[2] = (M)beta;
+    mom[3] = (M)0;
+    store_dual(mom + kMomG0, dual_of<double, double>(S.g0a, S.g0l));
+    store_dual(mom + kMomH, dual_of<double, double>(S.ha, S.hl));
+    for (int d = 0; d < 6; ++d)
+      store_dual(mom + kMomGd + 9 * d, dual_of<double, double>(S.gda[d], S.gdl[d]));
+  }
+}
+
+// Residual epilogue of pass 2 for site u (H sites also get the occupancy
+// entropy terms; non-H sites carry no occupancy residual):
+//   R_sigma -= 3 / (beta sigma),   R_x = selfx + sum - (3/(2x) + [x<1]/(1-x))/beta
+//                                        - [x<0.9999] gamma/beta
+BTAM_HD void residual_epilogue(double sigma, double x, int code, double beta,
+                               double gamma, double selfx, double &rs,
+                               double &rx) {
+  rs -= 3.0 / (beta * sigma);
+  if (code == 1) {
+    double dlogz = 3.0 / (2.0 * x) + (x < 1.0 ? 1.0 / (1.0 - x) : 0.0);
+    rx += selfx - dlogz / beta;
+    if (x < 0.9999) rx -= gamma / beta;
+  } else {
+    rx = 0.0;
+  }
+}
+
+}  // namespace btam

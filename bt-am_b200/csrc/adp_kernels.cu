@@ -1,0 +1,314 @@
+// Two-pass mean-field ADP kernels for sm_100a.
+//
+// Work decomposition (one warp per site, no atomics, fixed summation order,
+// so every result is bitwise reproducible and independent of what else runs
+// on the device):
+//  pass 1, phase A: lanes stride over the site's neighbours; each lane
+//          evaluates a pair's 12 pair-rule points, its centre point and its
+//          6 neighbour-displaced triplet points (19 geometries, u/w/phi/rho
+//          splines) and accumulates 22 moment sums;
+//  pass 1, phase B: lane = (centre displacement d, neighbour group g),
+//          d in 0..5, g in 0..4 (30 lanes): each lane accumulates the 9
+//          components of G(d) plus B(g,g) over every 5th neighbour;
+//  pass 1 epilogue (lane 0, FP64): energy, free entropy, dV0/dx_i and the
+//          76-value moment record;
+//  pass 2: lanes stride over the neighbours of u; each lane evaluates the 25
+//          geometries of its pair with value+derivative splines and contracts
+//          them with u's moments (staged in shared memory) and the
+//          neighbour's moments (read-only cache), accumulating 5 residual
+//          components.
+// There is no tensor-core work: every term is a gather plus spline
+// evaluation plus a handful of FMAs.  FP32 form: per-pair arithmetic in
+// float, per-lane accumulation with two-sum compensation, lane/warp
+// reductions and the per-site epilogue in double.
+#include "adp_kernels.cuh"
+#include "topo_kernels.cuh"
+
+namespace btam {
+
+namespace {
+
+constexpr int kWarps = 4;  // warps per block
+
+// Per-lane accumulator: plain double for the FP64 form, a two-sum
+// compensated float pair for the FP32 form.
+template <class R> struct Acc;
+template <> struct Acc<double> {
+  double v = 0.0;
+  __device__ __forceinline__ void add(double t) { v += t; }
+  __device__ __forceinline__ double get() const { return v; }
+};
+template <> struct Acc<float> {
+  float hi = 0.0f, lo = 0.0f;
+  __device__ __forceinline__ void add(float t) {
+    float s = hi + t;
+    float bp = s - hi;
+    float e = (hi - (s - bp)) + (t - bp);
+    hi = s;
+    lo += e;
+  }
+  __device__ __forceinline__ double get() const { return (double)hi + (double)lo; }
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <class R>
+__device__ __forceinline__ V3<R> pair_vec(const double4 &a, const double4 &b) {
+  // the difference is taken in double so the FP32 form loses nothing to the
+  // absolute coordinate magnitude
+  return mk3<R>((R)(a.x - b.x), (R)(a.y - b.y), (R)(a.z - b.z));
+}
+
+__device__ __forceinline__ bool finite(double v) { return isfinite(v); }
+
+template <class R>
+__global__ void __launch_bounds__(kWarps * 32)
+pass1_kernel(const EvalArgs<R> a) {
+  __shared__ SiteSums ss[kWarps];
+  __shared__ double xbuf[kWarps][30][10];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kWarps + warp;
+  if (i >= a.n_real) return;
+  R *mom = a.mom + (size_t)i * kMomStride;
+  const double2 xbi = a.xb[i];
+  const double xi = xbi.x;
+  if (xi < kMinOcc) {  // empty site: no energy, no moments
+    for (int c = lane; c < kMomStride; c += 32) mom[c] = (R)0;
+    if (lane == 0) a.rho[i] = a.V0[i] = a.S0[i] = a.selfx[i] = 0.0;
+    return;
+  }
+  const double4 qi = a.pos[i];
+  const int ci = a.code[i];
+  const int nb0 = a.offs[i], nb1 = a.offs[i + 1];
+
+  // ---- phase A
+  Acc<R> acc[22];
+  for (int p = nb0 + lane; p < nb1; p += 32) {
+    const int j = a.idx[p];
+    const double2 xbj = a.xb[j];
+    if (xbj.x < kMinOcc) continue;
+    const double4 qj = a.pos[j];
+    Pass1A<R> o;
+    o.rho = o.epair = o.ediag = o.cross = (R)0;
+    for (int c = 0; c < 3; ++c) o.g0.a[c] = o.hsum.a[c] = (R)0;
+    for (int c = 0; c < 6; ++c) o.g0.l[c] = o.hsum.l[c] = (R)0;
+    pass1_pair_A<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)qj.w, (R)xi, (R)xbj.x, ci,
+                    a.code[j], o);
+    acc[0].add(o.rho);
+    acc[1].add(o.epair);
+    acc[2].add(o.ediag);
+    acc[3].add(o.cross);
+    for (int c = 0; c < 3; ++c) {
+      acc[4 + c].add(o.g0.a[c]);
+      acc[13 + c].add(o.hsum.a[c]);
+    }
+    for (int c = 0; c < 6; ++c) {
+      acc[7 + c].add(o.g0.l[c]);
+      acc[16 + c].add(o.hsum.l[c]);
+    }
+  }
+  double tot[22];
+#pragma unroll
+  for (int c = 0; c < 22; ++c) tot[c] = warp_sum(acc[c].get());
+
+  // ---- phase B
+  if (lane < 30) {
+    const int d = lane % 6, g = lane / 6, k = d >> 1, sg = d & 1;
+    Acc<R> b[10];
+    for (int p = nb0 + g; p < nb1; p += 5) {
+      const int j = a.idx[p];
+      const double2 xbj = a.xb[j];
+      if (xbj.x < kMinOcc) continue;
+      const double4 qj = a.pos[j];
+      Feat<R> gd;
+      for (int c = 0; c < 3; ++c) gd.a[c] = (R)0;
+      for (int c = 0; c < 6; ++c) gd.l[c] = (R)0;
+      R s = (R)0;
+      pass1_pair_B<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)(xi * xbj.x),
+                      pair_kind(ci, a.code[j]), k, sg, gd, s);
+      for (int c = 0; c < 3; ++c) b[c].add(gd.a[c]);
+      for (int c = 0; c < 6; ++c) b[3 + c].add(gd.l[c]);
+      b[9].add(s);
+    }
+    for (int c = 0; c < 10; ++c) xbuf[warp][lane][c] = b[c].get();
+  }
+  __syncwarp();
+  SiteSums &S = ss[warp];
+  if (lane < 6) {
+    double t[10];
+    for (int c = 0; c < 10; ++c) t[c] = 0.0;
+    for (int g = 0; g < 5; ++g)
+      for (int c = 0; c < 10; ++c) t[c] += xbuf[warp][lane + 6 * g][c];
+    for (int c = 0; c < 3; ++c) S.gda[lane][c] = t[c];
+    for (int c = 0; c < 6; ++c) S.gdl[lane][c] = t[3 + c];
+    xbuf[warp][lane][0] = t[9];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    S.rho = tot[0];
+    S.epair = tot[1];
+    S.ediag = tot[2];
+    S.cross = tot[3];
+    for (int c = 0; c < 3; ++c) {
+      S.g0a[c] = tot[4 + c];
+      S.ha[c] = tot[13 + c];
+    }
+    for (int c = 0; c < 6; ++c) {
+      S.g0l[c] = tot[7 + c];
+      S.hl[c] = tot[16 + c];
+    }
+    double sself = 0.0;
+    for (int d = 0; d < 6; ++d) sself += xbuf[warp][d][0];
+    S.sself = sself;
+    SiteResult res;
+    site_epilogue(S, a.emb[ci], xi, ci, xbi.y, a.gamma[i], qi.w, a.mass[ci], res, mom);
+    a.rho[i] = res.rho;
+    a.V0[i] = res.V0;
+    a.S0[i] = res.S0;
+    a.selfx[i] = res.selfx;
+    if (!(finite(res.V0) && finite(res.S0) && finite(res.selfx)))
+      atomicOr(a.err, 1 << kErrBitNonFinite);
+  }
+}
+
+template <class R>
+__global__ void __launch_bounds__(kWarps * 32)
+pass2_kernel(const EvalArgs<R> a) {
+  __shared__ R mu_s[kWarps][kMomStride];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int u = blockIdx.x * kWarps + warp;
+  if (u >= a.n_real) return;
+  const double2 xbu = a.xb[u];
+  const double xu = xbu.x;
+  if (xu < kMinOcc) {
+    if (lane == 0) {
+      a.Rq[3 * u] = a.Rq[3 * u + 1] = a.Rq[3 * u + 2] = 0.0;
+      a.Rs[u] = a.Rx[u] = 0.0;
+    }
+    return;
+  }
+  const R *mu_g = a.mom + (size_t)u * kMomStride;
+  for (int c = lane; c < kMomStride; c += 32) mu_s[warp][c] = mu_g[c];
+  __syncwarp();
+  const R *mu = mu_s[warp];
+  const double4 qu = a.pos[u];
+  const int cu = a.code[u];
+  const int nb0 = a.offs[u], nb1 = a.offs[u + 1];
+  Acc<R> acc[5];
+  for (int p = nb0 + lane; p < nb1; p += 32) {
+    const int j = a.idx[p];
+    const double2 xbj = a.xb[j];
+    if (xbj.x < kMinOcc) continue;
+    const int o = a.owner[j];
+    const double4 qj = a.pos[j];
+    const R *mj = a.mom + (size_t)o * kMomStride;
+    Pass2Out<R> out;
+    out.gq[0] = out.gq[1] = out.gq[2] = out.gs = out.gx = (R)0;
+    pass2_pair<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xu, (R)xbj.x, cu,
+                  a.code[j], mu[0], ld_ro(mj), ld_ro(mj + 1), (R)(xbj.y / xbu.y), mu, mj,
+                  out);
+    acc[0].add(out.gq[0]);
+    acc[1].add(out.gq[1]);
+    acc[2].add(out.gq[2]);
+    acc[3].add(out.gs);
+    acc[4].add(out.gx);
+  }
+  double t[5];
+#pragma unroll
+  for (int c = 0; c < 5; ++c) t[c] = warp_sum(acc[c].get());
+  if (lane == 0) {
+    double gs = t[3], gx = t[4];
+    residual_epilogue(qu.w, xu, cu, xbu.y, a.gamma[u], a.selfx[u], gs, gx);
+    a.Rq[3 * u] = t[0];
+    a.Rq[3 * u + 1] = t[1];
+    a.Rq[3 * u + 2] = t[2];
+    a.Rs[u] = gs;
+    a.Rx[u] = gx;
+    if (!(finite(t[0]) && finite(t[1]) && finite(t[2]) && finite(gs) && finite(gx)))
+      atomicOr(a.err, 1 << kErrBitNonFinite);
+  }
+}
+
+// Single-block deterministic reduction (fixed strides, fixed tree).
+__global__ void __launch_bounds__(1024)
+totals_kernel(int n, const double *V0, const double *S0, const double *Rq,
+              const double *Rs, const double *Rx, double *out) {
+  __shared__ double sh[4][1024];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    v[0] += V0[i];
+    v[1] += S0[i];
+    v[2] += Rq[3 * i] * Rq[3 * i] + Rq[3 * i + 1] * Rq[3 * i + 1] +
+            Rq[3 * i + 2] * Rq[3 * i + 2] + Rs[i] * Rs[i];
+    v[3] += Rx[i] * Rx[i];
+  }
+  for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[threadIdx.x] = sh[threadIdx.x][0];
+}
+
+__global__ void rho_nmf_kernel(int n, const double4 *pos, const double2 *xb, const int *code,
+                               const int *offs, const int *idx, SplineView<double> rmg,
+                               SplineView<double> rh, double *out) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  double acc = 0.0;
+  if (!(xb[i].x < kMinOcc)) {
+    const double4 qi = pos[i];
+    for (int p = offs[i] + lane; p < offs[i + 1]; p += 32) {
+      int j = idx[p];
+      double xj = xb[j].x;
+      if (xj < kMinOcc) continue;
+      double4 qj = pos[j];
+      double dx = qi.x - qj.x, dy = qi.y - qj.y, dz = qi.z - qj.z;
+      double r = sqrt(dx * dx + dy * dy + dz * dz);
+      acc += xj * spline_v(code[j] == 0 ? rmg : rh, r);
+    }
+  }
+  acc = warp_sum(acc);
+  if (lane == 0) out[i] = acc;
+}
+
+inline int nblocks(long long n, int per) { return (int)((n + per - 1) / per); }
+
+}  // namespace
+
+template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st) {
+  if (a.n_real > 0) pass1_kernel<R><<<nblocks(a.n_real, kWarps), kWarps * 32, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st) {
+  if (a.n_real > 0) pass2_kernel<R><<<nblocks(a.n_real, kWarps), kWarps * 32, 0, st>>>(a);
+  return cudaGetLastError();
+}
+template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t);
+template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t);
+template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t);
+template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t);
+
+cudaError_t launch_totals(int n_real, const double *V0, const double *S0, const double *Rq,
+                          const double *Rs, const double *Rx, double *out, cudaStream_t st) {
+  totals_kernel<<<1, 1024, 0, st>>>(n_real, V0, S0, Rq, Rs, Rx, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rho_nmf(int n_real, const double4 *pos, const double2 *xb, const int *code,
+                           const int *offs, const int *idx, SplineView<double> rho_mg,
+                           SplineView<double> rho_h, double *out, cudaStream_t st) {
+  if (n_real > 0)
+    rho_nmf_kernel<<<nblocks((long long)n_real * 32, 128), 128, 0, st>>>(
+        n_real, pos, xb, code, offs, idx, rho_mg, rho_h, out);
+  return cudaGetLastError();
+}
+
+}  // namespace btam

@@ -1,0 +1,48 @@
+// Launchers of the two-pass mean-field ADP kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "adp_core.cuh"
+
+namespace btam {
+
+// Device view of one system for an evaluation.  Site arrays cover real sites
+// then periodic images ("all sites"); per-site outputs cover real sites.
+template <class R> struct EvalArgs {
+  int n_real;
+  const double4 *pos;   // x, y, z, sigma            [all]
+  const double2 *xb;    // occupancy x, beta         [all]
+  const int *code;      // 0 = Mg, 1 = H             [all]
+  const int *owner;     // real site of each row     [all]
+  const double *gamma;  // chemical multiplier       [real]
+  const int *offs;      // CSR offsets               [real + 1]
+  const int *idx;       // neighbour indices (all-sites numbering)
+  TablesView<R> T;      // radial tables in R
+  SplineView<double> emb[2];  // embedding F (FP64) for Mg, H
+  double mass[2];             // Mg, H element masses
+  R *mom;                     // kMomStride per real site
+  double *rho, *V0, *S0, *selfx;  // [real]
+  double *Rq, *Rs, *Rx;           // [3*real], [real], [real]
+  int *err;
+};
+
+// Pass 1: rho-bar, V0, S0, dV0/dx (self) and the moment record of every
+// real site.  Pass 2: residuals of every real site.
+template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st);
+template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st);
+
+// Deterministic FP64 totals over real sites: out[0] = sum V0, out[1] = sum S0,
+// out[2] = sum |R_q|^2 + R_sigma^2 (active sites), out[3] = sum R_x^2.
+cudaError_t launch_totals(int n_real, const double *V0, const double *S0,
+                          const double *Rq, const double *Rs, const double *Rx,
+                          double *out, cudaStream_t st);
+
+// Non-mean-field density rho_i = sum_j x_j rho_{s_j}(|q_i - q_j|)
+// (density.cpp:44-104) for every real site.
+cudaError_t launch_rho_nmf(int n_real, const double4 *pos, const double2 *xb,
+                           const int *code, const int *offs, const int *idx,
+                           SplineView<double> rho_mg, SplineView<double> rho_h,
+                           double *out, cudaStream_t st);
+
+}  // namespace btam

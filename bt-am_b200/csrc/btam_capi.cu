@@ -1,0 +1,802 @@
+// Host side of libbtam.so: the C ABI declared in include/btam.h.
+//
+// Owns device memory per system (state, periodic images, neighbour lists,
+// moments, results) and one CUDA stream per system.  No torch, no host
+// fallback: every evaluation runs the kernels of adp_kernels.cu and
+// topo_kernels.cu on the current device.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/btam.h"
+#include "adp_core.cuh"
+#include "adp_kernels.cuh"
+#include "tables_io.hpp"
+#include "topo_kernels.cuh"
+
+using namespace btam;
+
+namespace {
+
+constexpr double kKB = 8.617332478E-5;  // k_B [eV/K] (Macros.hpp:849)
+
+int status_from_bits(int bits) {
+  if (bits & (1 << kErrBitOverflow)) return BTAM_ERR_NEIGHBOR_OVERFLOW;
+  if (bits & (1 << kErrBitEmpty)) return BTAM_ERR_NO_NEIGHBORS;
+  if (bits & (1 << kErrBitGhostOverflow)) return BTAM_ERR_GHOST_OVERFLOW;
+  if (bits & (1 << kErrBitCells)) return BTAM_ERR_OOM;
+  if (bits & (1 << kErrBitNonFinite)) return BTAM_ERR_NONFINITE;
+  if (bits & (1 << kErrBitTimeout)) return BTAM_ERR_TIMEOUT;
+  return BTAM_OK;
+}
+
+int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return BTAM_OK;
+  if (e == cudaErrorMemoryAllocation) return BTAM_ERR_OOM;
+  return BTAM_ERR_CUDA;
+}
+
+#define BTAM_TRY(expr)                         \
+  do {                                         \
+    cudaError_t _e = (expr);                   \
+    if (_e != cudaSuccess) return cuda_status(_e); \
+  } while (0)
+
+template <class T> cudaError_t dalloc(T *&p, size_t count) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)&p, count * sizeof(T));
+}
+
+template <class T> void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Packs row-major q, sigma and x of real sites into the device layout.
+__global__ void pack_state_kernel(int n, const double *q, const double *sigma,
+                                  const double *x, double4 *pos, double2 *xb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double4 p = pos[i];
+  double2 b = xb[i];
+  if (q) {
+    p.x = q[3 * i];
+    p.y = q[3 * i + 1];
+    p.z = q[3 * i + 2];
+  }
+  if (sigma) p.w = sigma[i];
+  if (x) b.x = x[i];
+  pos[i] = p;
+  xb[i] = b;
+}
+
+// FMA throughput probe: kProbeChains independent dependency chains per
+// thread keep the FMA pipe full; the result is stored so nothing is elided.
+constexpr int kProbeChains = 8;
+template <class T> __global__ void fma_probe_kernel(long long iters, T *sink) {
+  T v[kProbeChains];
+  const T a = (T)0.999999, b = (T)1e-7;
+  for (int c = 0; c < kProbeChains; ++c) v[c] = (T)(threadIdx.x + c);
+  for (long long it = 0; it < iters; ++it)
+#pragma unroll
+    for (int c = 0; c < kProbeChains; ++c) v[c] = fma(v[c], a, b);
+  T s = 0;
+  for (int c = 0; c < kProbeChains; ++c) s += v[c];
+  sink[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+__global__ void spline_eval_kernel(SplineView<double> s, int n, const double *r, double *v,
+                                   double *dv) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double a, b;
+  spline_vd(s, r[i], a, b);
+  v[i] = a;
+  dv[i] = b;
+}
+
+}  // namespace
+
+struct btam_tables {
+  HostTables host;
+  int device = 0;
+  Coef4<double> *d64 = nullptr;
+  Coef4<float> *d32 = nullptr;
+  TablesView<double> v64;
+  TablesView<float> v32;
+};
+
+struct btam_system {
+  const btam_tables *T = nullptr;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int n_real = 0, n_ghost = 0, cap_all = 0;
+  GhostBox box;
+  bool any_periodic = false;
+  // site arrays (real then images)
+  double4 *pos = nullptr;
+  double2 *xb = nullptr;
+  int *code = nullptr, *owner = nullptr;
+  char4 *image = nullptr;
+  double *gamma = nullptr;
+  // staging for host updates
+  double *stage = nullptr;  // 5 n_real doubles: q (3n), sigma, x
+  // neighbour lists
+  bool built = false;
+  int n_list = 0;
+  long long n_pairs = 0, idx_cap = 0;
+  int *offs = nullptr, *idx = nullptr, *cnt = nullptr, *tmp = nullptr;
+  long long tmp_cap = 0;
+  int q_cap = 0;
+  // cells
+  int cell_cap = 0, site_cap = 0;
+  unsigned long long *bbox = nullptr;
+  CellGrid *grid = nullptr;
+  int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cursor = nullptr,
+      *cell_sites = nullptr;
+  // results
+  double *rho = nullptr, *V0 = nullptr, *S0 = nullptr, *selfx = nullptr, *Rq = nullptr,
+         *Rs = nullptr, *Rx = nullptr, *totals = nullptr;
+  double *mom64 = nullptr;
+  float *mom32 = nullptr;
+  int *err = nullptr;
+  DeviceScratch scratch;
+};
+
+namespace {
+
+// Reciprocal rows and rc-shell widths of a cell (rows = lattice vectors).
+// Same arithmetic as the oracle's image rule (oracle/btam_oracle.cpp).
+int make_box(const double *origin, const double *cell, const int *periodic, double rc,
+             GhostBox &b) {
+  memset(&b, 0, sizeof(b));
+  double A[3][3];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) A[r][c] = cell[3 * r + c];
+  b.ortho = (cell[1] == 0 && cell[2] == 0 && cell[3] == 0 && cell[5] == 0 &&
+             cell[6] == 0 && cell[7] == 0) ? 1 : 0;
+  double det = A[0][0] * (A[1][1] * A[2][2] - A[1][2] * A[2][1]) -
+               A[0][1] * (A[1][0] * A[2][2] - A[1][2] * A[2][0]) +
+               A[0][2] * (A[1][0] * A[2][1] - A[1][1] * A[2][0]);
+  bool any = periodic[0] || periodic[1] || periodic[2];
+  if (det == 0.0 && any) return BTAM_ERR_BOX_TOO_SMALL;
+  for (int a = 0; a < 3; ++a) {
+    const double *p = A[(a + 1) % 3], *s = A[(a + 2) % 3];
+    if (det != 0.0) {
+      b.B[a][0] = (p[1] * s[2] - p[2] * s[1]) / det;
+      b.B[a][1] = (p[2] * s[0] - p[0] * s[2]) / det;
+      b.B[a][2] = (p[0] * s[1] - p[1] * s[0]) / det;
+    }
+  }
+  for (int a = 0; a < 3; ++a) {
+    for (int c = 0; c < 3; ++c) b.A[a][c] = A[a][c];
+    double bn = std::sqrt(b.B[a][0] * b.B[a][0] + b.B[a][1] * b.B[a][1] + b.B[a][2] * b.B[a][2]);
+    if (periodic[a]) {
+      if (!(bn > 0.0) || 1.0 / bn < 2.0 * rc) return BTAM_ERR_BOX_TOO_SMALL;
+    }
+    b.w[a] = rc * bn;
+    b.lo[a] = origin[a];
+    b.hi[a] = origin[a] + A[a][a];
+    b.origin[a] = origin[a];
+    b.periodic[a] = periodic[a] ? 1 : 0;
+  }
+  b.rc = rc;
+  return BTAM_OK;
+}
+
+int validate_state(const btam_system *s, int n, const double *q, const double *sigma,
+                   const double *x, const int *code) {
+  for (int i = 0; i < n; ++i) {
+    if (q)
+      for (int a = 0; a < 3; ++a)
+        if (!std::isfinite(q[3 * i + a])) return BTAM_ERR_NONFINITE;
+    if (sigma && !(std::isfinite(sigma[i]) && sigma[i] > 0.0)) return BTAM_ERR_NONFINITE;
+    if (x) {
+      if (!std::isfinite(x[i]) || x[i] < 0.0) return BTAM_ERR_NONFINITE;
+      if (code && code[i] == 0 && x[i] > 0.0 && x[i] < BTAM_MIN_OCCUPANCY)
+        return BTAM_ERR_OCCUPANCY;
+    }
+    if (q && s->any_periodic) {
+      const GhostBox &b = s->box;
+      for (int a = 0; a < 3; ++a) {
+        if (!b.periodic[a]) continue;
+        if (b.ortho) {
+          double v = q[3 * i + a];
+          if (!(v >= b.lo[a] && v < b.hi[a])) return BTAM_ERR_OUT_OF_BOX;
+        } else {
+          double d0 = q[3 * i] - b.origin[0], d1 = q[3 * i + 1] - b.origin[1],
+                 d2 = q[3 * i + 2] - b.origin[2];
+          double sa = d0 * b.B[a][0] + d1 * b.B[a][1] + d2 * b.B[a][2];
+          if (!(sa >= -1e-9 && sa < 1.0 + 1e-9)) return BTAM_ERR_OUT_OF_BOX;
+        }
+      }
+    }
+  }
+  return BTAM_OK;
+}
+
+int ensure_sites(btam_system *s, int n_all) {
+  if (n_all <= s->cap_all) return BTAM_OK;
+  int cap = n_all + n_all / 4 + 64;
+  double4 *pos = nullptr;
+  double2 *xb = nullptr;
+  int *code = nullptr, *owner = nullptr;
+  BTAM_TRY(dalloc(pos, cap));
+  BTAM_TRY(dalloc(xb, cap));
+  BTAM_TRY(dalloc(code, cap));
+  BTAM_TRY(dalloc(owner, cap));
+  if (s->pos) {
+    BTAM_TRY(cudaMemcpyAsync(pos, s->pos, (size_t)s->n_real * sizeof(double4),
+                             cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaMemcpyAsync(xb, s->xb, (size_t)s->n_real * sizeof(double2),
+                             cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaMemcpyAsync(code, s->code, (size_t)s->n_real * sizeof(int),
+                             cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaMemcpyAsync(owner, s->owner, (size_t)s->n_real * sizeof(int),
+                             cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaStreamSynchronize(s->st));
+  }
+  dfree(s->pos);
+  dfree(s->xb);
+  dfree(s->code);
+  dfree(s->owner);
+  s->pos = pos;
+  s->xb = xb;
+  s->code = code;
+  s->owner = owner;
+  s->cap_all = cap;
+  return BTAM_OK;
+}
+
+// Waits for the stream, returns the error bits raised since the last read
+// (as a status) and clears them.
+int read_err(btam_system *s) {
+  int bits = 0;
+  cudaError_t e = cudaMemcpyAsync(&bits, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  return status_from_bits(bits);
+}
+
+template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesView<R> &T) {
+  EvalArgs<R> a;
+  a.n_real = s->n_real;
+  a.pos = s->pos;
+  a.xb = s->xb;
+  a.code = s->code;
+  a.owner = s->owner;
+  a.gamma = s->gamma;
+  a.offs = s->offs;
+  a.idx = s->idx;
+  a.T = T;
+  a.emb[0] = s->T->v64.t[T_F_MG];
+  a.emb[1] = s->T->v64.t[T_F_H];
+  a.mass[0] = s->T->host.mass_mg;
+  a.mass[1] = s->T->host.mass_h;
+  a.mom = mom;
+  a.rho = s->rho;
+  a.V0 = s->V0;
+  a.S0 = s->S0;
+  a.selfx = s->selfx;
+  a.Rq = s->Rq;
+  a.Rs = s->Rs;
+  a.Rx = s->Rx;
+  a.err = s->err;
+  return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *btam_status_string(int st) {
+  switch (st) {
+  case BTAM_OK: return "ok";
+  case BTAM_ERR_ARG: return "bad argument";
+  case BTAM_ERR_IO: return "table file missing or malformed";
+  case BTAM_ERR_NEIGHBOR_OVERFLOW: return "more than maxneigh neighbours";
+  case BTAM_ERR_NO_NEIGHBORS: return "site without neighbours";
+  case BTAM_ERR_BOX_TOO_SMALL: return "periodic cell thinner than 2 rc";
+  case BTAM_ERR_NONFINITE: return "non-finite value";
+  case BTAM_ERR_OOM: return "device out of memory";
+  case BTAM_ERR_CUDA: return "CUDA error";
+  case BTAM_ERR_GHOST_OVERFLOW: return "periodic images exceed capacity";
+  case BTAM_ERR_OCCUPANCY: return "non-H site with 0 < x < min_occupancy";
+  case BTAM_ERR_SPECIES: return "species other than H or Mg";
+  case BTAM_ERR_TIMEOUT: return "bounded device wait gave up";
+  case BTAM_ERR_NOT_BUILT: return "neighbour lists not built";
+  case BTAM_ERR_OUT_OF_BOX: return "site outside the periodic cell";
+  }
+  return "unknown status";
+}
+
+int btam_version(void) { return 100; }
+
+int btam_tables_load(const char *dir, btam_tables **out) {
+  if (!dir || !out) return BTAM_ERR_ARG;
+  *out = nullptr;
+  btam_tables *t = new btam_tables();
+  if (load_host_tables(dir, t->host)) {
+    delete t;
+    return BTAM_ERR_IO;
+  }
+  cudaGetDevice(&t->device);
+  size_t total = 0;
+  for (int k = 0; k < T_COUNT; ++k) total += t->host.t[k].n;
+  std::vector<Coef4<double>> h64(total);
+  std::vector<Coef4<float>> h32(total);
+  size_t off[T_COUNT];
+  size_t o = 0;
+  for (int k = 0; k < T_COUNT; ++k) {
+    off[k] = o;
+    const HostSpline &hs = t->host.t[k];
+    for (int m = 0; m < hs.n; ++m) {
+      const double *c = &hs.abcd[4 * (size_t)m];
+      h64[o + m] = Coef4<double>{c[0], c[1], c[2], c[3]};
+      h32[o + m] = Coef4<float>{(float)c[0], (float)c[1], (float)c[2], (float)c[3]};
+    }
+    o += hs.n;
+  }
+  cudaError_t e = cudaMalloc(&t->d64, total * sizeof(Coef4<double>));
+  if (e == cudaSuccess) e = cudaMalloc(&t->d32, total * sizeof(Coef4<float>));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->d64, h64.data(), total * sizeof(Coef4<double>), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->d32, h32.data(), total * sizeof(Coef4<float>), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    btam_tables_destroy(t);
+    return cuda_status(e);
+  }
+  for (int k = 0; k < T_COUNT; ++k) {
+    const HostSpline &hs = t->host.t[k];
+    t->v64.t[k] = SplineView<double>{t->d64 + off[k], hs.dx, 1.0 / hs.dx, hs.n};
+    t->v32.t[k] = SplineView<float>{t->d32 + off[k], (float)hs.dx, (float)(1.0 / hs.dx), hs.n};
+  }
+  *out = t;
+  return BTAM_OK;
+}
+
+void btam_tables_destroy(btam_tables *t) {
+  if (!t) return;
+  if (t->d64) cudaFree(t->d64);
+  if (t->d32) cudaFree(t->d32);
+  delete t;
+}
+
+double btam_tables_mass(const btam_tables *t, int species) {
+  if (!t) return 0.0;
+  if (species == 12) return t->host.mass_mg;
+  if (species == 1) return t->host.mass_h;
+  return 0.0;
+}
+
+int btam_tables_spline(const btam_tables *t, int table, int n, const double *r,
+                       double *value, double *deriv) {
+  if (!t || table < 0 || table >= T_COUNT || n < 0 || (n > 0 && (!r || !value || !deriv)))
+    return BTAM_ERR_ARG;
+  if (n == 0) return BTAM_OK;
+  double *d = nullptr;
+  BTAM_TRY(cudaMalloc(&d, 3 * (size_t)n * sizeof(double)));
+  cudaError_t e = cudaMemcpy(d, r, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    spline_eval_kernel<<<(n + 127) / 128, 128>>>(t->v64.t[table], n, d, d + n, d + 2 * (size_t)n);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(value, d + n, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(deriv, d + 2 * (size_t)n, n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return cuda_status(e);
+}
+
+int btam_system_create(const btam_tables *t, int n, const double *q, const double *sigma,
+                       const double *x, const int *species, const double *beta,
+                       const double *gamma, const double origin[3], const double cell[9],
+                       const int periodic[3], btam_system **out) {
+  if (!t || !out || n <= 0 || !q || !sigma || !x || !species || !origin || !cell || !periodic)
+    return BTAM_ERR_ARG;
+  *out = nullptr;
+  std::vector<int> code(n);
+  for (int i = 0; i < n; ++i) {
+    if (species[i] == 12) code[i] = 0;
+    else if (species[i] == 1) code[i] = 1;
+    else return BTAM_ERR_SPECIES;
+  }
+  btam_system *s = new btam_system();
+  s->T = t;
+  cudaGetDevice(&s->device);
+  s->n_real = n;
+  int st = make_box(origin, cell, periodic, BTAM_R_CUTOFF, s->box);
+  if (st != BTAM_OK) {
+    delete s;
+    return st;
+  }
+  s->any_periodic = periodic[0] || periodic[1] || periodic[2];
+  st = validate_state(s, n, q, sigma, x, code.data());
+  if (st == BTAM_OK && beta)
+    for (int i = 0; i < n; ++i)
+      if (!(std::isfinite(beta[i]) && beta[i] > 0.0)) st = BTAM_ERR_NONFINITE;
+  if (st != BTAM_OK) {
+    delete s;
+    return st;
+  }
+  cudaError_t e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete s;
+    return cuda_status(e);
+  }
+  st = ensure_sites(s, n);
+  std::vector<double4> hp(n);
+  std::vector<double2> hx(n);
+  std::vector<int> ho(n);
+  for (int i = 0; i < n; ++i) {
+    hp[i] = make_double4(q[3 * i], q[3 * i + 1], q[3 * i + 2], sigma[i]);
+    hx[i] = make_double2(x[i], beta ? beta[i] : 1.0 / (kKB * 300.0));
+    ho[i] = i;
+  }
+  if (st == BTAM_OK) {
+    e = cudaMemcpy(s->pos, hp.data(), n * sizeof(double4), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->xb, hx.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->owner, ho.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = dalloc(s->gamma, n);
+    if (e == cudaSuccess) {
+      if (gamma) e = cudaMemcpy(s->gamma, gamma, n * sizeof(double), cudaMemcpyHostToDevice);
+      else e = cudaMemset(s->gamma, 0, n * sizeof(double));
+    }
+    if (e == cudaSuccess) e = dalloc(s->stage, 5 * (size_t)n);
+    if (e == cudaSuccess) e = dalloc(s->err, 1);
+    if (e == cudaSuccess) e = cudaMemset(s->err, 0, sizeof(int));
+    for (double **p : {&s->rho, &s->V0, &s->S0, &s->selfx, &s->Rs, &s->Rx})
+      if (e == cudaSuccess) e = dalloc(*p, n);
+    if (e == cudaSuccess) e = dalloc(s->Rq, 3 * (size_t)n);
+    if (e == cudaSuccess) e = dalloc(s->totals, 4);
+    if (e == cudaSuccess) e = dalloc(s->bbox, 6);
+    if (e == cudaSuccess) e = dalloc(s->grid, 1);
+    st = cuda_status(e);
+  }
+  if (st != BTAM_OK) {
+    btam_system_destroy(s);
+    return st;
+  }
+  *out = s;
+  return BTAM_OK;
+}
+
+void btam_system_destroy(btam_system *s) {
+  if (!s) return;
+  if (s->st) cudaStreamSynchronize(s->st);
+  dfree(s->pos); dfree(s->xb); dfree(s->code); dfree(s->owner); dfree(s->image);
+  dfree(s->gamma); dfree(s->stage); dfree(s->offs); dfree(s->idx); dfree(s->cnt);
+  dfree(s->tmp); dfree(s->bbox); dfree(s->grid); dfree(s->cell_of); dfree(s->cell_cnt);
+  dfree(s->cell_start); dfree(s->cursor); dfree(s->cell_sites); dfree(s->rho); dfree(s->V0);
+  dfree(s->S0); dfree(s->selfx); dfree(s->Rq); dfree(s->Rs); dfree(s->Rx); dfree(s->totals);
+  dfree(s->mom64); dfree(s->mom32); dfree(s->err);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+}
+
+int btam_system_set_state(btam_system *s, const double *q, const double *sigma,
+                          const double *x) {
+  if (!s) return BTAM_ERR_ARG;
+  std::vector<int> code;
+  if (x) {
+    code.resize(s->n_real);
+    BTAM_TRY(cudaMemcpyAsync(code.data(), s->code, s->n_real * sizeof(int),
+                             cudaMemcpyDeviceToHost, s->st));
+    BTAM_TRY(cudaStreamSynchronize(s->st));
+  }
+  int st = validate_state(s, s->n_real, q, sigma, x, x ? code.data() : nullptr);
+  if (st != BTAM_OK) return st;
+  const int n = s->n_real;
+  double *dq = s->stage, *ds = s->stage + 3 * (size_t)n, *dx = s->stage + 4 * (size_t)n;
+  if (q) BTAM_TRY(cudaMemcpyAsync(dq, q, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  if (sigma) BTAM_TRY(cudaMemcpyAsync(ds, sigma, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  if (x) BTAM_TRY(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  pack_state_kernel<<<(n + 127) / 128, 128, 0, s->st>>>(n, q ? dq : nullptr, sigma ? ds : nullptr,
+                                                        x ? dx : nullptr, s->pos, s->xb);
+  BTAM_TRY(cudaGetLastError());
+  if (s->n_ghost > 0)
+    BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                  s->box, s->st));
+  return BTAM_OK;
+}
+
+int btam_system_info(const btam_system *s, int *n_real, int *n_ghost, long long *n_pairs) {
+  if (!s) return BTAM_ERR_ARG;
+  if (n_real) *n_real = s->n_real;
+  if (n_ghost) *n_ghost = s->n_ghost;
+  if (n_pairs) *n_pairs = s->n_pairs;
+  return BTAM_OK;
+}
+
+void *btam_system_stream(const btam_system *s) { return s ? (void *)s->st : nullptr; }
+
+int btam_neighbors_build(btam_system *s, int all_sites) {
+  if (!s) return BTAM_ERR_ARG;
+  s->built = false;
+  const int n = s->n_real;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  // ---- periodic images
+  s->n_ghost = 0;
+  if (s->any_periodic) {
+    int *cnt = nullptr, *off = nullptr;
+    BTAM_TRY(dalloc(cnt, n + 1));
+    cudaError_t e = dalloc(off, n + 1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cnt + n, 0, sizeof(int), s->st);
+    if (e == cudaSuccess) e = launch_ghost_count(n, s->pos, s->box, cnt, s->st);
+    if (e == cudaSuccess) e = exclusive_scan(cnt, off, n + 1, s->scratch, s->st);
+    int ng = 0;
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&ng, off + n, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    int st = cuda_status(e);
+    if (st == BTAM_OK) st = ensure_sites(s, n + ng);
+    if (st == BTAM_OK && ng > 0) {
+      e = dalloc(s->image, ng);
+      if (e == cudaSuccess)
+        e = launch_ghost_emit(n, s->pos, s->xb, s->code, s->owner, s->image, s->box, off, ng,
+                              s->err, s->st);
+      st = cuda_status(e);
+    }
+    cudaFree(cnt);
+    cudaFree(off);
+    if (st != BTAM_OK) return st;
+    s->n_ghost = ng;
+  }
+  const int n_all = n + s->n_ghost;
+  const int n_query = all_sites ? n_all : n;
+  // ---- cells and neighbour buffers
+  int max_cells = 4 * n_all + 1024;
+  if (max_cells > s->cell_cap) {
+    BTAM_TRY(dalloc(s->cell_cnt, max_cells + 1));
+    BTAM_TRY(dalloc(s->cell_start, max_cells + 1));
+    BTAM_TRY(dalloc(s->cursor, max_cells));
+    s->cell_cap = max_cells;
+  }
+  if (n_all > s->site_cap) {
+    BTAM_TRY(dalloc(s->cell_of, n_all));
+    BTAM_TRY(dalloc(s->cell_sites, n_all));
+    s->site_cap = n_all;
+  }
+  if (n_query + 1 > s->q_cap) {
+    BTAM_TRY(dalloc(s->cnt, n_query + 1));
+    BTAM_TRY(dalloc(s->offs, n_query + 1));
+    s->q_cap = n_query + 1;
+  }
+  if ((long long)n_query * kNbrBuf > s->tmp_cap) {
+    BTAM_TRY(dalloc(s->tmp, (size_t)n_query * kNbrBuf));
+    s->tmp_cap = (long long)n_query * kNbrBuf;
+  }
+  NbrArgs a;
+  a.n_all = n_all;
+  a.n_query = n_query;
+  a.maxn = BTAM_MAXNEIGH;
+  a.max_cells = s->cell_cap;
+  a.rc = BTAM_R_CUTOFF;
+  a.cell_edge = BTAM_R_CUTOFF * (1.0 + 1e-9) + 1e-9;
+  a.pos = s->pos;
+  a.bbox = s->bbox;
+  a.grid = s->grid;
+  a.cell_of = s->cell_of;
+  a.cell_cnt = s->cell_cnt;
+  a.cell_start = s->cell_start;
+  a.cursor = s->cursor;
+  a.cell_sites = s->cell_sites;
+  a.cnt = s->cnt;
+  a.tmp = s->tmp;
+  a.offs = s->offs;
+  a.err = s->err;
+  a.scratch = &s->scratch;
+  BTAM_TRY(launch_neighbors(a, s->st));
+  int total = 0;
+  BTAM_TRY(cudaMemcpyAsync(&total, s->offs + n_query, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  int st = read_err(s);
+  if (st != BTAM_OK) return st;
+  if (total > s->idx_cap) {
+    BTAM_TRY(dalloc(s->idx, total));
+    s->idx_cap = total;
+  }
+  BTAM_TRY(launch_compact(n_query, s->tmp, s->offs, s->idx, s->st));
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  s->n_list = n_query;
+  s->n_pairs = total;
+  s->built = true;
+  return BTAM_OK;
+}
+
+int btam_neighbors_copy(const btam_system *s, int *offs, int *idx, long long idx_cap) {
+  if (!s || !offs) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  BTAM_TRY(cudaMemcpy(offs, s->offs, (s->n_list + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  if (idx) {
+    if (idx_cap < s->n_pairs) return BTAM_ERR_ARG;
+    BTAM_TRY(cudaMemcpy(idx, s->idx, s->n_pairs * sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  return BTAM_OK;
+}
+
+int btam_ghosts_copy(const btam_system *s, double *q, int *owner, int *image) {
+  if (!s) return BTAM_ERR_ARG;
+  const int n = s->n_real, ng = s->n_ghost;
+  if (ng == 0) return BTAM_OK;
+  std::vector<double4> hp(ng);
+  std::vector<char4> hi(ng);
+  BTAM_TRY(cudaMemcpy(hp.data(), s->pos + n, ng * sizeof(double4), cudaMemcpyDeviceToHost));
+  BTAM_TRY(cudaMemcpy(hi.data(), s->image, ng * sizeof(char4), cudaMemcpyDeviceToHost));
+  if (owner)
+    BTAM_TRY(cudaMemcpy(owner, s->owner + n, ng * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int k = 0; k < ng; ++k) {
+    if (q) {
+      q[3 * k] = hp[k].x;
+      q[3 * k + 1] = hp[k].y;
+      q[3 * k + 2] = hp[k].z;
+    }
+    if (image) {
+      image[3 * k] = hi[k].x;
+      image[3 * k + 1] = hi[k].y;
+      image[3 * k + 2] = hi[k].z;
+    }
+  }
+  return BTAM_OK;
+}
+
+int btam_mf_eval_async(btam_system *s, int precision) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  if (precision == BTAM_FP64) {
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
+    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
+    BTAM_TRY(launch_pass1(a, s->st));
+    BTAM_TRY(launch_pass2(a, s->st));
+  } else {
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
+    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
+    BTAM_TRY(launch_pass1(a, s->st));
+    BTAM_TRY(launch_pass2(a, s->st));
+  }
+  BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->st));
+  return BTAM_OK;
+}
+
+int btam_system_sync(btam_system *s) {
+  if (!s) return BTAM_ERR_ARG;
+  return read_err(s);
+}
+
+int btam_results_copy(btam_system *s, double *rho, double *V0, double *S0, double *Rq,
+                      double *Rs, double *Rx, double *totals) {
+  if (!s) return BTAM_ERR_ARG;
+  const size_t n = (size_t)s->n_real * sizeof(double);
+  struct {
+    double *dst;
+    const double *src;
+    size_t bytes;
+  } cp[7] = {{rho, s->rho, n}, {V0, s->V0, n}, {S0, s->S0, n}, {Rq, s->Rq, 3 * n},
+             {Rs, s->Rs, n},   {Rx, s->Rx, n}, {totals, s->totals, 4 * sizeof(double)}};
+  for (auto &c : cp)
+    if (c.dst) BTAM_TRY(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, s->st));
+  return read_err(s);
+}
+
+int btam_mf_eval(btam_system *s, int precision, double *rho, double *V0, double *S0,
+                 double *Rq, double *Rs, double *Rx, double *totals) {
+  if (!s) return BTAM_ERR_ARG;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  int st = btam_mf_eval_async(s, precision);
+  if (st != BTAM_OK) return st;
+  return btam_results_copy(s, rho, V0, S0, Rq, Rs, Rx, totals);
+}
+
+int btam_mf_rho(btam_system *s, int precision, double *rho) {
+  if (!s || !rho) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  if (precision == BTAM_FP64) {
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
+    BTAM_TRY(launch_pass1(eval_args<double>(s, s->mom64, s->T->v64), s->st));
+  } else if (precision == BTAM_FP32C) {
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
+    BTAM_TRY(launch_pass1(eval_args<float>(s, s->mom32, s->T->v32), s->st));
+  } else {
+    return BTAM_ERR_ARG;
+  }
+  BTAM_TRY(cudaMemcpyAsync(rho, s->rho, s->n_real * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  return read_err(s);
+}
+
+int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]) {
+  if (!s || !ms) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  cudaEvent_t ev[4];
+  for (auto &e : ev) BTAM_TRY(cudaEventCreate(&e));
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  cudaError_t e = cudaEventRecord(ev[0], s->st);
+  if (precision == BTAM_FP64) {
+    if (!s->mom64 && e == cudaSuccess) e = dalloc(s->mom64, nm);
+    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
+    if (e == cudaSuccess) e = launch_pass2(a, s->st);
+  } else {
+    if (!s->mom32 && e == cudaSuccess) e = dalloc(s->mom32, nm);
+    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
+    if (e == cudaSuccess) e = launch_pass2(a, s->st);
+  }
+  if (e == cudaSuccess) e = cudaEventRecord(ev[2], s->st);
+  if (e == cudaSuccess)
+    e = launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->st);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[3], s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+    float t = 0.f;
+    e = cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+    ms[k] = t;
+  }
+  for (auto &x : ev) cudaEventDestroy(x);
+  if (e != cudaSuccess) return cuda_status(e);
+  return read_err(s);
+}
+
+int btam_probe_fma_peak(int fp64, double seconds, double *tflops) {
+  if (!tflops || !(seconds > 0.0)) return BTAM_ERR_ARG;
+  int dev = 0, sms = 0;
+  BTAM_TRY(cudaGetDevice(&dev));
+  BTAM_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int threads = 256, blocks = sms * 8;
+  float *sink = nullptr;
+  BTAM_TRY(cudaMalloc(&sink, (size_t)blocks * threads * sizeof(double)));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  // calibrate the iteration count on a short run, then time one long launch
+  long long iters = 1 << 12;
+  double best = 0.0;
+  cudaError_t e = cudaSuccess;
+  for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+    cudaEventRecord(a);
+    if (fp64) fma_probe_kernel<double><<<blocks, threads>>>(iters, (double *)sink);
+    else fma_probe_kernel<float><<<blocks, threads>>>(iters, sink);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    double flops = 2.0 * kProbeChains * (double)iters * blocks * threads;
+    if (ms > 0) best = flops / (ms * 1e-3) / 1e12;
+    if (ms > 0 && rep < 3) {
+      double scale = seconds * 1e3 / ms;
+      if (scale > 1.0) iters = (long long)(iters * (scale > 1e4 ? 1e4 : scale));
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_status(e);
+  *tflops = best;
+  return BTAM_OK;
+}
+
+int btam_rho_nmf(btam_system *s, double *rho) {
+  if (!s || !rho) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  BTAM_TRY(launch_rho_nmf(s->n_real, s->pos, s->xb, s->code, s->offs, s->idx,
+                          s->T->v64.t[T_RHO_MG], s->T->v64.t[T_RHO_H], s->rho, s->st));
+  BTAM_TRY(cudaMemcpyAsync(rho, s->rho, s->n_real * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  return read_err(s);
+}
+
+}  // extern "C"

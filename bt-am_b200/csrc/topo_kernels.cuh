@@ -1,0 +1,83 @@
+// Device topology: periodic images, cell binning, neighbour lists.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+
+namespace btam {
+
+constexpr int kNbrBuf = 256;  // per-site candidate buffer (>= maxneigh = 250)
+
+// Error bits raised by kernels (mapped to btam_status codes by the host).
+enum ErrBit : int {
+  kErrBitOverflow = 0,       // more than maxneigh neighbours
+  kErrBitEmpty = 1,          // a site without neighbours
+  kErrBitGhostOverflow = 2,  // more images than allocated
+  kErrBitCells = 3,          // cell grid did not fit
+  kErrBitNonFinite = 4,      // NaN/Inf in an output
+  kErrBitTimeout = 5,        // a bounded wait gave up
+};
+
+// Box description shared by the image kernels.  A[b] = lattice vector b;
+// B[a] = reciprocal row a (fractional s_a = (q - origin) . B[a]);
+// w[a] = rc |B[a]| (fractional width of the rc shell across faces a).
+struct GhostBox {
+  double A[3][3], B[3][3], w[3], lo[3], hi[3], origin[3], rc;
+  int periodic[3];
+  int ortho;
+};
+
+struct CellGrid {
+  double lo[3];
+  double edge, inv_edge;
+  int n[3];
+};
+
+// Growable device scratch for library temporaries (CUB scans).
+struct DeviceScratch {
+  void *ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t ensure(size_t need) {
+    if (need <= bytes) return cudaSuccess;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    cudaError_t e = cudaMalloc(&ptr, need);
+    if (e == cudaSuccess) bytes = need;
+    return e;
+  }
+  ~DeviceScratch() {
+    if (ptr) cudaFree(ptr);
+  }
+};
+
+struct NbrArgs {
+  int n_all, n_query, maxn, max_cells;
+  double rc, cell_edge;
+  const double4 *pos;
+  unsigned long long *bbox;  // 6
+  CellGrid *grid;
+  int *cell_of, *cell_cnt, *cell_start, *cursor, *cell_sites;
+  int *cnt;   // n_query + 1
+  int *tmp;   // n_query * kNbrBuf
+  int *offs;  // n_query + 1
+  int *err;
+  DeviceScratch *scratch;
+};
+
+cudaError_t exclusive_scan(const int *in, int *out, int n, DeviceScratch &s,
+                           cudaStream_t st);
+cudaError_t launch_ghost_count(int n, const double4 *pos, const GhostBox &b, int *cnt,
+                               cudaStream_t st);
+cudaError_t launch_ghost_emit(int n, double4 *pos, double2 *xb, int *code, int *owner,
+                              char4 *image, const GhostBox &b, const int *off,
+                              int max_ghosts, int *err, cudaStream_t st);
+cudaError_t launch_ghost_refresh(int n_real, int n_ghost, double4 *pos, double2 *xb,
+                                 int *code, const int *owner, const char4 *image,
+                                 const GhostBox &b, cudaStream_t st);
+cudaError_t launch_neighbors(const NbrArgs &a, cudaStream_t st);
+cudaError_t launch_compact(int n_query, const int *tmp, const int *offs, int *idx,
+                           cudaStream_t st);
+
+}  // namespace btam

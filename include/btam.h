@@ -1,0 +1,170 @@
+/* btam.h -- C ABI of the B200 mean-field ADP library (libbtam.so).
+ *
+ * A drop-in for the hot path of BT-AM's mean-field diffusive molecular
+ * dynamics: the Gauss-Hermite-averaged angular-dependent potential (ADP) of
+ * Mg-H over mean positions q, Gaussian widths sigma and occupancies x.  Each
+ * entry point names the reference interface it replaces.  All functions take
+ * caller-owned plain pointers (host unless the name says _device), return an
+ * int status (BTAM_OK = 0), and never take ownership of caller memory.
+ *
+ * Units and encodings follow the reference: Angstrom, eV, ps; species are
+ * atomic numbers (H = 1, Mg = 12) as in AtomicSpecie (src/Macros.hpp:56-175);
+ * positions are row-major N x 3 doubles (the DMSwarm coordinate field).
+ *
+ * Threading: distinct systems may be used from distinct host threads; one
+ * system must not be used by two threads at once.  Every system owns one
+ * CUDA stream; work on different systems overlaps on the device.
+ */
+#ifndef BTAM_H
+#define BTAM_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------
+ * The reference's set-up functions return PetscErrorCode (0 or 99,
+ * src/Macros.hpp:29-38); its evaluators have no error channel. */
+#define BTAM_OK 0
+#define BTAM_ERR_ARG 1               /* bad argument / null pointer */
+#define BTAM_ERR_IO 2                /* table file missing or malformed (init_adp_MgHx returns EXIT_FAILURE, MgHx-ADP.cpp:389-392) */
+#define BTAM_ERR_NEIGHBOR_OVERFLOW 3 /* > maxneigh = 250 neighbours (Neighbors.cpp:96-104) */
+#define BTAM_ERR_NO_NEIGHBORS 4      /* a site without neighbours (Neighbors.cpp:106-113) */
+#define BTAM_ERR_BOX_TOO_SMALL 5     /* periodic cell thinner than 2 rc (Atom.cpp:230-255) */
+#define BTAM_ERR_NONFINITE 6         /* NaN/Inf in an input or output */
+#define BTAM_ERR_OOM 7               /* device allocation failed */
+#define BTAM_ERR_CUDA 8              /* other CUDA runtime error */
+#define BTAM_ERR_GHOST_OVERFLOW 9    /* periodic images exceed capacity */
+#define BTAM_ERR_OCCUPANCY 10        /* non-H site with 0 < x < min_occupancy (unsupported) */
+#define BTAM_ERR_SPECIES 11          /* species other than H (1) or Mg (12) */
+#define BTAM_ERR_TIMEOUT 12          /* a bounded device wait gave up */
+#define BTAM_ERR_NOT_BUILT 13        /* neighbour lists not built yet */
+#define BTAM_ERR_OUT_OF_BOX 14       /* site outside the cell along a periodic axis */
+
+/* arithmetic forms */
+#define BTAM_FP64 0   /* plain FP64 drop-in */
+#define BTAM_FP32C 1  /* FP32 quadrature/splines, compensated accumulation, FP64 reductions */
+
+/* table ids for btam_tables_spline */
+#define BTAM_T_RHO_MG 0
+#define BTAM_T_RHO_H 1
+#define BTAM_T_F_MG 2
+#define BTAM_T_F_H 3
+#define BTAM_T_PHI_MGMG 4
+#define BTAM_T_PHI_HH 5
+#define BTAM_T_PHI_MGH 6
+#define BTAM_T_U_MGMG 7
+#define BTAM_T_U_HH 8
+#define BTAM_T_U_MGH 9
+#define BTAM_T_W_MGMG 10
+#define BTAM_T_W_HH 11
+#define BTAM_T_W_MGH 12
+
+/* reference constants (src/Macros.hpp:857, 862, 869) */
+#define BTAM_R_CUTOFF 6.2934034034
+#define BTAM_MAXNEIGH 250
+#define BTAM_MIN_OCCUPANCY 5e-4
+
+typedef struct btam_tables btam_tables;
+typedef struct btam_system btam_system;
+
+const char *btam_status_string(int status);
+int btam_version(void);
+
+/* Replaces init_adp_MgHx(&adp_MgMg, MgMg, dir), (&adp_HH, HH, dir),
+ * (&adp_MgH, MgH, dir) (src/ADP/MgHx-ADP.cpp:366-501; called at
+ * main-BT-AM.cpp:108-110): reads adpmg.dat, adph.dat and adpmgh.dat from
+ * `dir` and uploads the splines to the current CUDA device. */
+int btam_tables_load(const char *dir, btam_tables **out);
+/* Replaces destroy_adp_MgHx (MgHx-ADP.cpp:505). */
+void btam_tables_destroy(btam_tables *t);
+/* Element mass of a species as read from the tables (element_mass[],
+ * MgHx-ADP.cpp:436).  Returns 0 for unknown species. */
+double btam_tables_mass(const btam_tables *t, int species);
+/* Replaces cubic_spline / d_cubic_spline (src/Numerical/cubic-spline.cpp:
+ * 84-112) on one table, evaluated on the device in FP64 for n host radii. */
+int btam_tables_spline(const btam_tables *t, int table, int n, const double *r,
+                       double *value, double *deriv);
+
+/* Replaces read_dump_information + init_DMD_simulation (dump-input.cpp:
+ * 51-214, Atom.cpp:80-431): one system of n sites with its DMSwarm fields
+ * (coordinates, "stdv-q", "molar-fraction", "specie", "beta", "gamma").
+ * The cell is given by its origin and three lattice vectors (rows of
+ * cell[9]); an orthogonal box [lo, hi) is origin = lo, cell = diag(hi - lo).
+ * periodic[a] != 0 makes axis a periodic (dump "pp"; 0 = "ff").
+ * beta/gamma may be NULL (beta = 1/(k_B 300 K), gamma = 0). */
+int btam_system_create(const btam_tables *t, int n, const double *q,
+                       const double *sigma, const double *x,
+                       const int *species, const double *beta,
+                       const double *gamma, const double origin[3],
+                       const double cell[9], const int periodic[3],
+                       btam_system **out);
+void btam_system_destroy(btam_system *s);
+/* Replaces the DMSwarmGetField/RestoreField round trip of q, sigma, x
+ * (main-BT-AM.cpp:174-228): new state from host arrays (any may be NULL).
+ * Periodic images follow their owners (DMSwarmMigrateGhostField,
+ * Ghosts.cpp:861-892). */
+int btam_system_set_state(btam_system *s, const double *q, const double *sigma,
+                          const double *x);
+/* Sizes: real sites, periodic images, neighbour-list entries. */
+int btam_system_info(const btam_system *s, int *n_real, int *n_ghost, long long *n_pairs);
+/* The system's CUDA stream (cudaStream_t), for callers that time or order
+ * work against it. */
+void *btam_system_stream(const btam_system *s);
+
+/* Replaces DMSwarmCreateGhostAtoms (Ghosts.cpp:42-802) +
+ * list_of_active_mechanical_sites_MgHx (Topology.cpp:53-132) + neighbors
+ * (Neighbors.cpp:39-134).  all_sites = 1 builds lists for images too, as the
+ * reference does; 0 builds them for real sites only (what evaluation needs). */
+int btam_neighbors_build(btam_system *s, int all_sites);
+/* Copies the CSR lists (ascending neighbour index, images numbered after the
+ * real sites).  offs holds n_list + 1 entries; idx_cap bounds idx. */
+int btam_neighbors_copy(const btam_system *s, int *offs, int *idx, long long idx_cap);
+/* Copies the periodic images: positions (n_ghost x 3), owning real site and
+ * integer image shift (image = q_ghost - q_owner in lattice vectors). */
+int btam_ghosts_copy(const btam_system *s, double *q, int *owner, int *image);
+
+/* Replaces the per-site loop of evaluate_mf_rho_i_adp_MgHx
+ * (MgHx-mf-V-bulk.cpp:708-787) over all real sites. */
+int btam_mf_rho(btam_system *s, int precision, double *rho);
+
+/* One residual evaluation of every real site.  Replaces the per-site loops
+ * over evaluate_mf_rho_i_adp_MgHx, evaluate_V0_i_adp_MgHx (791-953),
+ * evaluate_S0_i_adp_MgHx (957-1142), evaluate_DV0_i_Dq_u_MgHx (1823-2098) and
+ * evaluate_DV0_i_Dxi_u_adp_MgHx (2102-2325), assembled as
+ *   R_q(u) = sum_{i in {u} U N(u)} (beta_i/beta_u) dV0_i/dq_u
+ *   R_sigma(u) = sum_i (beta_i/beta_u) dV0_i/dsigma_u - 3/(beta_u sigma_u)
+ *   R_x(u) = sum_i (beta_i/beta_u) dV0_i/dx_u - (3/(2x_u) + [x_u<1]/(1-x_u))/beta_u
+ *            - [x_u<0.9999] gamma_u/beta_u        (H sites; 0 for Mg)
+ * i.e. (1/beta_u) times the gradient of sum_i S0_i.  Any output may be NULL.
+ * totals (4): sum V0, sum S0, sum |R_q|^2 + R_sigma^2, sum R_x^2. */
+int btam_mf_eval(btam_system *s, int precision, double *rho, double *V0,
+                 double *S0, double *Rq, double *Rs, double *Rx, double *totals);
+/* The same evaluation enqueued on the system's stream with inputs and
+ * outputs resident on the device; results stay in the system's buffers
+ * (btam_results_copy reads them).  Does not synchronise. */
+int btam_mf_eval_async(btam_system *s, int precision);
+int btam_results_copy(btam_system *s, double *rho, double *V0, double *S0,
+                      double *Rq, double *Rs, double *Rx, double *totals);
+/* Waits for the system's stream and returns the first error it raised. */
+int btam_system_sync(btam_system *s);
+
+/* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
+ * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
+int btam_rho_nmf(btam_system *s, double *rho);
+
+/* ---- measurement (no counterpart in the reference, which has only PETSc's
+ * SNES monitor for tracing) ------------------------------------------------ */
+/* One evaluation as btam_mf_eval_async, with CUDA events on the system's
+ * stream around each kernel: ms[0] pass 1, ms[1] pass 2, ms[2] totals.
+ * Synchronises. */
+int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]);
+/* Sustained FMA throughput of the current device in TFLOP/s (FMA = 2 flops)
+ * for fp64 = 0 (FP32) or 1 (FP64), from a register-resident FMA loop over
+ * every SM lasting about `seconds`. */
+int btam_probe_fma_peak(int fp64, double seconds, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BTAM_H */

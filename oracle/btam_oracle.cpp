@@ -691,8 +691,11 @@ double orc_mass(int species) { return (species >= 0 && species < 32) ? gMass[spe
 // on each axis, and the copy is shifted by -d times the box edge so that it
 // lies beyond the opposite face.  (The reference's own shift search,
 // Ghosts.cpp:768-794, tries the zero shift first and so leaves single-rank
-// copies unshifted; this is the shift it intends.)  Triclinic cells use the
-// same rule on fractional coordinates with slab width rc / (face spacing).
+// copies unshifted; this is the shift it intends.)  Triclinic cells (no
+// reference counterpart: the reference supports orthogonal boxes only) keep
+// every image q - sum_b d_b a_b whose fractional coordinates lie in
+// [-w_a, 1 + w_a), w_a = rc / (spacing of faces a); directions in the same
+// order.
 int orc_ghosts(int n, const double *q, const double *origin, const double *cell,
                const int *periodic, double rc, int max_ghosts, double *q_ghost,
                int *owner, int *image, int *n_ghost) {
@@ -724,35 +727,41 @@ int orc_ghosts(int n, const double *q, const double *origin, const double *cell,
   }
   int ng = 0;
   for (int i = 0; i < n; ++i) {
-    double c[3];
-    if (ortho) {
-      for (int a = 0; a < 3; ++a) c[a] = q[3 * i + a];
-    } else {
-      for (int a = 0; a < 3; ++a) {
-        double dq0 = q[3 * i] - origin[0], dq1 = q[3 * i + 1] - origin[1],
-               dq2 = q[3 * i + 2] - origin[2];
-        c[a] = dq0 * B[a][0] + dq1 * B[a][1] + dq2 * B[a][2];
-      }
-    }
+    const double *qi = q + 3 * i;
     for (int dir = 0; dir < 27; ++dir) {
       if (dir == 13) continue;
       int d[3] = {dir % 3 - 1, (dir / 3) % 3 - 1, dir / 9 - 1};
       bool in = true;
-      for (int a = 0; a < 3 && in; ++a) {
+      for (int a = 0; a < 3; ++a)
         if (d[a] != 0 && !periodic[a]) in = false;
-        double l = ortho ? lo[a] : 0.0, h = ortho ? hi[a] : 1.0;
-        double wa = ortho ? rc : w[a];
-        if (d[a] == -1) in = in && c[a] >= l && c[a] < l + wa;
-        else if (d[a] == 1) in = in && c[a] >= h - wa && c[a] < h;
-        else in = in && c[a] >= l && c[a] < h;
+      if (!in) continue;
+      double p[3];
+      for (int a = 0; a < 3; ++a) {
+        double s = qi[a];
+        for (int b = 0; b < 3; ++b)
+          if (d[b] != 0) s = s + (double)(-d[b]) * A[b][a];
+        p[a] = s;
+      }
+      if (ortho) {
+        // slab test on the original position (Ghosts.cpp:123-648)
+        for (int a = 0; a < 3 && in; ++a) {
+          if (d[a] == -1) in = qi[a] >= lo[a] && qi[a] < lo[a] + rc;
+          else if (d[a] == 1) in = qi[a] >= hi[a] - rc && qi[a] < hi[a];
+          else in = qi[a] >= lo[a] && qi[a] < hi[a];
+        }
+      } else {
+        // triclinic: keep the image if it lies in the cell widened by rc
+        // across every face, -w_a <= s_a < 1 + w_a
+        double dq0 = p[0] - origin[0], dq1 = p[1] - origin[1], dq2 = p[2] - origin[2];
+        for (int a = 0; a < 3 && in; ++a) {
+          double sa = dq0 * B[a][0] + dq1 * B[a][1] + dq2 * B[a][2];
+          in = sa >= -w[a] && sa < 1.0 + w[a];
+        }
       }
       if (!in) continue;
       if (ng >= max_ghosts) return kErrGhostOverflow;
       for (int a = 0; a < 3; ++a) {
-        double s = q[3 * i + a];
-        for (int b = 0; b < 3; ++b)
-          if (d[b] != 0) s = s + (double)(-d[b]) * A[b][a];
-        q_ghost[3 * ng + a] = s;
+        q_ghost[3 * ng + a] = p[a];
         image[3 * ng + a] = -d[a];
       }
       owner[ng] = i;

@@ -68,7 +68,7 @@ class Lib:
         x = np.ascontiguousarray(x, np.float64)
         spc = np.ascontiguousarray(spc, np.int32)
         out = np.zeros(3)
-        self._f("quadrature")(term, mode, slot, len(sigma), coincident, _d(q),
+        self._f("quadrature")(int(term), int(mode), int(slot), len(sigma), int(coincident), _d(q),
                               _d(sigma), _d(x), _i(spc), _d(out))
         return out if mode == 1 else out[0]
 
@@ -218,3 +218,32 @@ def evaluate(sys_, oracle, sites=None, residual_sites=None, rc=6.2934034034):
     Rq, Rs, Rx = oracle.residuals(full, rho, owner, image, offs, idx, us)
     return dict(rho=rho_real, V0=V0, S0=S0, Rq=Rq, Rs=Rs, Rx=Rx, offs=offs,
                 idx=idx, full=full, owner=owner, image=image, n_real=n)
+
+
+def sampled_residuals(sys_, oracle, sites, rc=6.2934034034):
+    """Literal residuals of a few real sites of a large system.  Neighbour
+    lists are built only for the sites the assembly reads (the sampled sites
+    and the owners of their neighbours); the other lists stay empty."""
+    full, n, owner, image = expand(sys_, oracle, rc)
+    sites = np.asarray(sites, np.int32)
+    offs_s, idx_s = oracle.neighbors(full["q"], query=sites, rc=rc)
+    need = set(int(s) for s in sites)
+    for k in range(len(sites)):
+        for j in idx_s[offs_s[k]:offs_s[k + 1]]:
+            need.add(int(owner[j]))
+    query = np.array(sorted(need), np.int32)
+    offs_q, idx_q = oracle.neighbors(full["q"], query=query, rc=rc)
+    counts = np.zeros(len(full["x"]), np.int64)
+    counts[query] = np.diff(offs_q)
+    offs = np.zeros(len(full["x"]) + 1, np.int32)
+    offs[1:] = np.cumsum(counts)
+    idx = np.zeros(offs[-1], np.int32)
+    for k, qi in enumerate(query):
+        idx[offs[qi]:offs[qi + 1]] = idx_q[offs_q[k]:offs_q[k + 1]]
+    rho_q = oracle.mf_rho(full, offs, idx, query)
+    rho_real = np.zeros(n)
+    rho_real[query] = rho_q
+    rho = rho_real[owner]
+    V0 = oracle.V0(full, rho, offs, idx, sites)
+    Rq, Rs, Rx = oracle.residuals(full, rho, owner, image, offs, idx, sites)
+    return dict(rho=rho_real[sites], V0=V0, Rq=Rq, Rs=Rs, Rx=Rx)

@@ -1,0 +1,166 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Values come from the reference's own arithmetic files compiled unmodified
+(oracle/_ref/libbtam_ref.so, built by oracle/Makefile from the reference
+tree): cubic_spline/d_cubic_spline, the Gaussian measure and degree-3 rule,
+the ADP terms, evaluate_mf_rho_i / V0_i / S0_i / DV0_i_Dq_u / DV0_i_Dxi_u.
+Periodic images and neighbour lists come from the restated rule
+(oracle/btam_oracle.cpp), because the reference builds them with PETSc
+DMSwarm, which is not available; the residual assembly is the project's
+definition (include/btam.h) applied to the reference's per-pair values.
+
+Run from the repository root, with the reference tree present:
+    python tests/golden/make_golden.py
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path[:0] = [os.path.join(ROOT, "oracle"), os.path.join(ROOT, "bt-am_b200")]
+import pyoracle  # noqa: E402
+from btam import dump, lattice  # noqa: E402
+
+OUT = os.path.dirname(os.path.abspath(__file__))
+REF_TREE = os.environ.get("BTAM_REFERENCE", "/root/reference")
+
+
+def residual_pairs(full, owner, image, offs, idx, us):
+    """(u', o) argument pairs of the assembly for each u in us, as the
+    restated orc_residuals forms them (images seen from the owner's frame)."""
+    plan = []
+    for k, u in enumerate(us):
+        cen = [u] + list(idx[offs[u]:offs[u + 1]])
+        for ic in cen:
+            o = owner[ic]
+            T = image[ic]
+            uu = u
+            if np.any(T != 0):
+                uu = -1
+                for cand in idx[offs[o]:offs[o + 1]]:
+                    if owner[cand] == u and np.all(image[cand] == -T):
+                        uu = cand
+                        break
+                if uu < 0:
+                    continue
+            plan.append((k, uu, o))
+    return plan
+
+
+def assemble(ref, full, rho, owner, image, offs, idx, us):
+    plan = residual_pairs(full, owner, image, offs, idx, us)
+    kk = np.array([p[0] for p in plan])
+    uu = np.array([p[1] for p in plan], np.int32)
+    oo = np.array([p[2] for p in plan], np.int32)
+    g4, gx = ref.DV0_pairs(full, rho, offs, idx, uu, oo)
+    beta, gamma, x, sig = full["beta"], full["gamma"], full["x"], full["sigma"]
+    Rq = np.zeros((len(us), 3))
+    Rs = np.zeros(len(us))
+    Rx = np.zeros(len(us))
+    for p in range(len(plan)):
+        k = kk[p]
+        u = us[k]
+        w = beta[oo[p]] / beta[u]
+        Rq[k] += w * g4[p, :3]
+        Rs[k] += w * g4[p, 3]
+        Rx[k] += w * gx[p]
+    for k, u in enumerate(us):
+        if x[u] < 5e-4:
+            Rq[k] = 0.0
+            Rs[k] = Rx[k] = 0.0
+            continue
+        Rs[k] -= 3.0 / (beta[u] * sig[u])
+        if full["species"][u] == 1:
+            dlogz = 3.0 / (2.0 * x[u]) + (1.0 / (1.0 - x[u]) if x[u] < 1.0 else 0.0)
+            Rx[k] -= dlogz / beta[u]
+            if x[u] < 0.9999:
+                Rx[k] -= gamma[u] / beta[u]
+        else:
+            Rx[k] = 0.0
+    return Rq, Rs, Rx
+
+
+def system_fixture(name, s, ref, orc, residual_sample=None, seed=0):
+    full, n, owner, image = pyoracle.expand(s, orc)
+    offs, idx = orc.neighbors(full["q"])
+    real = np.arange(n, dtype=np.int32)
+    rho_real = ref.mf_rho(full, offs, idx, real)
+    rho = rho_real[owner]
+    V0 = ref.V0(full, rho, offs, idx, real)
+    S0 = ref.S0(full, rho, offs, idx, real)
+    if residual_sample is None:
+        us = real
+    else:
+        rng = np.random.default_rng(seed)
+        us = np.sort(rng.choice(n, residual_sample, replace=False)).astype(np.int32)
+    Rq, Rs, Rx = assemble(ref, full, rho, owner, image, offs, idx, us)
+    rho_nmf = ref.rho_nmf(full, offs, idx, real)
+    path = os.path.join(OUT, f"{name}.npz")
+    np.savez_compressed(
+        path, q=s["q"], sigma=s["sigma"], x=s["x"], species=s["species"], beta=s["beta"],
+        gamma=s["gamma"], origin=s["origin"], cell=s["cell"], periodic=s["periodic"],
+        q_all=full["q"], owner=owner, image=image, offs=offs, idx=idx, rho=rho_real, V0=V0,
+        S0=S0, res_sites=us, Rq=Rq, Rs=Rs, Rx=Rx, rho_nmf=rho_nmf)
+    print(f"{name}: {n} real, {len(full['x'])} sites, {len(idx)} pairs, "
+          f"{len(us)} residual sites -> {os.path.getsize(path)} bytes")
+
+
+def main():
+    ref = pyoracle.reference()
+    if ref is None:
+        sys.exit("oracle/_ref/libbtam_ref.so missing: run `make -C oracle ref` first")
+    orc = pyoracle.Oracle()
+    # 1. splines of all 13 tables (cubic-spline.cpp:84-128)
+    r = np.concatenate([np.linspace(0.0, 7.0, 701), [6.2934034034, 6.29867867868, 6.3, 8.0]])
+    F = np.linspace(0.0, 0.2, 201)
+    vals = {}
+    for t in range(13):
+        rr = F if t in (2, 3) else r
+        vals[f"t{t}_r"] = rr
+        vals[f"t{t}_v"] = np.array([ref.spline(t, v, 0) for v in rr])
+        vals[f"t{t}_d"] = np.array([ref.spline(t, v, 1) for v in rr])
+    np.savez_compressed(os.path.join(OUT, "splines.npz"), **vals)
+    # 2. single-term quadratures: pairs, distinct and coincident triplets
+    rng = np.random.default_rng(2024)
+    rows = []
+    for trial in range(40):
+        q = rng.normal(0.0, 2.0, (3, 3))
+        q[0] = 0.0
+        sig = rng.uniform(0.05, 0.2, 3)
+        x = rng.uniform(0.01, 1.0, 3)
+        sp = rng.choice([1, 12], 3).astype(np.int32)
+        for term in range(4):
+            ns = 2 if term < 2 else 3
+            for coinc in ([0] if ns == 2 else [0, 1]):
+                qq, ss, xx, spc = q.copy(), sig.copy(), x.copy(), sp.copy()
+                if coinc:
+                    qq[2], ss[2], xx[2], spc[2] = qq[1], ss[1], xx[1], spc[1]
+                for mode in range(4):
+                    for slot in (range(ns) if mode else [0]):
+                        out = np.atleast_1d(ref.quadrature(term, mode, slot, qq[:ns], ss[:ns],
+                                                           xx[:ns], spc[:ns], coinc))
+                        o3 = np.zeros(3)
+                        o3[:len(out)] = out
+                        rows.append((term, mode, slot, ns, coinc, qq.ravel(), ss, xx, spc, o3))
+    np.savez_compressed(
+        os.path.join(OUT, "terms.npz"),
+        meta=np.array([r_[:5] for r_ in rows], np.int32),
+        q=np.array([r_[5] for r_ in rows]), sigma=np.array([r_[6] for r_ in rows]),
+        x=np.array([r_[7] for r_ in rows]), species=np.array([r_[8] for r_ in rows]),
+        out=np.array([r_[9] for r_ in rows]))
+    print(f"terms: {len(rows)} quadratures")
+    # 3. systems
+    sphere = lattice.cluster("sphere", 8.0, x_fn=lambda g, rr, n: g.uniform(0.0, 0.6, n),
+                             h_fraction=0.5, seed=3)
+    system_fixture("sphere", sphere, ref, orc)
+    cube = dump.read_dump(os.path.join(REF_TREE, "inputs", "Mg-hcp-cube-x5-x5-x5.dump"))
+    system_fixture("x5cube", cube, ref, orc, residual_sample=40, seed=5)
+    ortho = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.3, x_range=(0.0, 0.4),
+                              sigma_range=(0.08, 0.15), jitter=0.02, seed=5)
+    system_fixture("ortho_mgh", ortho, ref, orc)
+    system_fixture("config1", lattice.config1(), ref, orc, residual_sample=40, seed=1)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""The restated oracle against the reference's own arithmetic.
+
+Pins (a) against the committed golden fixtures, generated from the
+reference's source files compiled unmodified (tests/golden/make_golden.py),
+and (b) where the reference build is present, against it live."""
+import os
+
+import numpy as np
+import pytest
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, f"{name}.npz")))
+
+
+def system(g):
+    return {k: g[k] for k in ("q", "sigma", "x", "species", "beta", "gamma", "origin",
+                              "cell", "periodic")}
+
+
+def test_splines_bit_exact(oracle):
+    g = load("splines")
+    for t in range(13):
+        r = g[f"t{t}_r"]
+        v = np.array([oracle.spline(t, x, 0) for x in r])
+        d = np.array([oracle.spline(t, x, 1) for x in r])
+        assert np.array_equal(v, g[f"t{t}_v"]), t
+        assert np.array_equal(d, g[f"t{t}_d"]), t
+
+
+def test_survey_known_values(oracle):
+    # Values of the reference's own code (quoted to 16 digits) for Mg-Mg at
+    # q_j = (3.2, 0.1, 0.05), sigma = (0.10, 0.12), x = 1 and F_Mg(0.02).
+    q = np.array([0, 0, 0, 3.2, 0.1, 0.05])
+    s = np.array([0.10, 0.12])
+    x = np.ones(2)
+    sp = np.array([12, 12], np.int32)
+    close = lambda a, b: abs(a - b) <= 2e-16 * abs(b)
+    assert close(oracle.quadrature(1, 0, 0, q, s, x, sp), -5.130674333666740e-02)
+    assert close(oracle.quadrature(0, 0, 0, q, s, x, sp), 2.586903037283295e-02)
+    assert close(oracle.spline(2, 0.02, 0), -1.630017453898465e-01)
+
+
+def test_quadratures_bit_exact(oracle):
+    g = load("terms")
+    for k in range(len(g["meta"])):
+        term, mode, slot, ns, coinc = g["meta"][k]
+        out = np.atleast_1d(oracle.quadrature(term, mode, slot, g["q"][k].reshape(3, 3)[:ns],
+                                              g["sigma"][k][:ns], g["x"][k][:ns],
+                                              g["species"][k][:ns], coinc))
+        assert np.array_equal(out, g["out"][k][:len(out)]), (term, mode, slot, coinc)
+
+
+@pytest.mark.parametrize("name", ["sphere", "x5cube", "ortho_mgh", "config1"])
+def test_systems_against_golden(oracle, name):
+    import pyoracle
+    g = load(name)
+    s = system(g)
+    full, n, owner, image = pyoracle.expand(s, oracle)
+    # images and neighbour lists: the restated rule reproduces the fixture
+    assert np.array_equal(full["q"], g["q_all"])
+    assert np.array_equal(owner, g["owner"]) and np.array_equal(image, g["image"])
+    offs, idx = oracle.neighbors(full["q"])
+    assert np.array_equal(offs, g["offs"]) and np.array_equal(idx, g["idx"])
+    real = np.arange(n, dtype=np.int32)
+    rho = oracle.mf_rho(full, offs, idx, real)
+    assert np.array_equal(rho, g["rho"])
+    V0 = oracle.V0(full, rho[owner], offs, idx, real)
+    assert np.array_equal(V0, g["V0"])
+    S0 = oracle.S0(full, rho[owner], offs, idx, real)
+    assert np.array_equal(S0, g["S0"])
+    Rq, Rs, Rx = oracle.residuals(full, rho[owner], owner, image, offs, idx, g["res_sites"])
+    for a, b in ((Rq, g["Rq"]), (Rs, g["Rs"]), (Rx, g["Rx"])):
+        assert np.allclose(a, b, rtol=0, atol=1e-13 * max(1.0, np.abs(b).max()))
+    assert np.array_equal(oracle.rho_nmf(full, offs, idx, real), g["rho_nmf"])
+
+
+def test_oracle_matches_reference_live(oracle, ref):
+    from btam import lattice
+    import pyoracle
+    s = lattice.cluster("sphere", 7.0, x_fn=lambda g, r, n: g.uniform(0.0, 0.7, n),
+                        h_fraction=0.6, seed=11)
+    full, n, owner, image = pyoracle.expand(s, oracle)
+    offs, idx = oracle.neighbors(full["q"])
+    real = np.arange(n, dtype=np.int32)
+    r1, r2 = oracle.mf_rho(full, offs, idx, real), ref.mf_rho(full, offs, idx, real)
+    assert np.array_equal(r1, r2)
+    assert np.array_equal(oracle.V0(full, r1, offs, idx, real), ref.V0(full, r2, offs, idx, real))
+    us, is_ = [], []
+    for u in range(0, n, 9):
+        for i in [u, *idx[offs[u]:offs[u + 1]]]:
+            us.append(u)
+            is_.append(i)
+    a4, ax = oracle.DV0_pairs(full, r1, offs, idx, us, is_)
+    b4, bx = ref.DV0_pairs(full, r2, offs, idx, us, is_)
+    assert np.array_equal(a4, b4) and np.array_equal(ax, bx)
+
+
+def test_occupancy_threshold_quirks(oracle, ref):
+    """The reference's mixed thresholds (x < min_occupancy for H only in V0,
+    any species and <= in DV0_i_Dq_u): an H neighbour at exactly 5e-4 enters
+    V0 but not the j2 loop of the gradient.  The oracle reproduces both."""
+    q = np.array([[0.0, 0, 0], [3.1, 0.2, 0.1], [0.3, 2.9, 0.2], [-2.8, 0.4, 1.0]])
+    s = dict(q=q, sigma=np.full(4, 0.1), x=np.array([1.0, 5e-4, 0.3, 1.0]),
+             species=np.array([12, 1, 1, 12], np.int32), beta=np.full(4, 38.68),
+             gamma=np.zeros(4))
+    offs, idx = oracle.neighbors(q)
+    rho = oracle.mf_rho(s, offs, idx, np.arange(4, dtype=np.int32))
+    assert np.array_equal(rho, ref.mf_rho(s, offs, idx, np.arange(4, dtype=np.int32)))
+    a4, ax = oracle.DV0_pairs(s, rho, offs, idx, [0, 2, 1], [0, 0, 0])
+    b4, bx = ref.DV0_pairs(s, rho, offs, idx, [0, 2, 1], [0, 0, 0])
+    assert np.array_equal(a4, b4) and np.array_equal(ax, bx)
