@@ -173,9 +173,10 @@ def test_full_size_config2(gpu_tables, oracle):
         assert np.max(np.abs(a[k][sites] - lit[k])) < 1e-10 * max(1.0, np.abs(lit[k]).max()), k
     # dE/dq by central differences (beta uniform, so R_q is the energy gradient)
     h = 1e-4
-    for site, ax in ((5, 0), (9000 + 77, 2)):
-        if s["x"][site] < 5e-4:
-            continue
+    frac = s["q"] @ np.linalg.inv(s["cell"])
+    inside = np.all((frac > 0.05) & (frac < 0.95), axis=1) & (s["x"] >= 5e-4)
+    picks = [np.flatnonzero(inside & (s["species"] == sp))[3] for sp in (12, 1)]
+    for site, ax in ((picks[0], 0), (picks[1], 2)):
         E = []
         for sgn in (1, -1):
             q = s["q"].copy()
