@@ -68,6 +68,8 @@ _PROTOS = {
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
+    "btam_mf_eval_noalloc": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _V, _V, _V, _V,
+                                            _V, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
 
 _lib = None

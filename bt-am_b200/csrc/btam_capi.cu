@@ -295,6 +295,15 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesVie
 
 }  // namespace
 
+// Table views for the allocation-free entry point (noalloc.cu).
+namespace btam {
+const TablesView<double> &tables_view64(const btam_tables *t) { return t->v64; }
+const TablesView<float> &tables_view32(const btam_tables *t) { return t->v32; }
+double tables_mass(const btam_tables *t, int code) {
+  return code == 1 ? t->host.mass_h : t->host.mass_mg;
+}
+}  // namespace btam
+
 extern "C" {
 
 const char *btam_status_string(int st) {
@@ -314,6 +323,7 @@ const char *btam_status_string(int st) {
   case BTAM_ERR_TIMEOUT: return "bounded device wait gave up";
   case BTAM_ERR_NOT_BUILT: return "neighbour lists not built";
   case BTAM_ERR_OUT_OF_BOX: return "site outside the periodic cell";
+  case BTAM_ERR_TOO_LARGE: return "more sites than the static scratch of btam_mf_eval_noalloc holds";
   }
   return "unknown status";
 }

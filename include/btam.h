@@ -40,6 +40,7 @@ extern "C" {
 #define BTAM_ERR_TIMEOUT 12          /* a bounded device wait gave up */
 #define BTAM_ERR_NOT_BUILT 13        /* neighbour lists not built yet */
 #define BTAM_ERR_OUT_OF_BOX 14       /* site outside the cell along a periodic axis */
+#define BTAM_ERR_TOO_LARGE 15        /* more sites than btam_mf_eval_noalloc's static scratch holds */
 
 /* arithmetic forms */
 #define BTAM_FP64 0   /* plain FP64 drop-in */
@@ -152,6 +153,30 @@ int btam_system_sync(btam_system *s);
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);
+
+/* ---- evaluation without device allocation -------------------------------
+ * No counterpart in the reference.  For callers that must not call
+ * cudaMalloc/cudaFree (their device memory belongs to another allocator, or
+ * an allocation's implicit synchronisation is not acceptable): the same
+ * residual evaluation as btam_mf_eval_async on caller-owned DEVICE buffers,
+ * with the kernels' scratch in a fixed array inside the library instead of
+ * per-system allocations.
+ * Inputs (device): pos4 = (x, y, z, sigma) and xb = (x, beta) per site,
+ * code (0 = Mg, 1 = H) and owner (real site of each row) per site, real sites
+ * first then periodic images; gamma per real site; offs/idx = neighbour CSR
+ * of the real sites in that all-sites numbering.  Outputs (device): V0, Rs,
+ * Rx per real site, Rq 3 per real site, totals[4] as btam_mf_eval.
+ * Limit: n_real <= 16384 (BTAM_ERR_TOO_LARGE beyond).  The scratch (~10.4 MB
+ * per device) lives until the process exits and is shared by every call on
+ * that device: calls that overlap on the GPU race; serialise them.  The
+ * first call on each device looks the scratch up, so make it before any
+ * stream capture.  Runs on `stream` (a cudaStream_t, NULL = default) and
+ * synchronises it before returning. */
+int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_real,
+                         const double *pos4, const double *xb, const int *code,
+                         const int *owner, const double *gamma, const int *offs,
+                         const int *idx, double *V0, double *Rq, double *Rs,
+                         double *Rx, double *totals, void *stream);
 
 /* ---- measurement (no counterpart in the reference, which has only PETSc's
  * SNES monitor for tracing) ------------------------------------------------ */
