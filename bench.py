@@ -206,6 +206,8 @@ def run_btam(args, ws, rank, local):
     offs, idx = S.neighbors()
     owner = np.concatenate([np.arange(n), S.ghosts()[1]]).astype(np.int64)
     P = active_pairs(sys_, offs, idx, owner)
+    # kernel block shapes picked by the library's autotuner (setup, untimed)
+    shapes = {"fp32c": S.autotune(btam.FP32C), "fp64": S.autotune(btam.FP64)}
     stream = torch.cuda.ExternalStream(S.stream)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -306,7 +308,8 @@ def run_btam(args, ws, rank, local):
                 "config": {"workload": WORKLOAD, "sites": n, "images": ng,
                            "directed_active_pairs": P, "precision": "fp32c",
                            "l2": "flushed between steps (256 MiB write, outside step events)",
-                           "parallelism": f"{ws} independent replica(s), no collective"},
+                           "parallelism": f"{ws} independent replica(s), no collective",
+                           "kernel_shapes": shapes},
                 "fp64_drop_in": {"value": results["fp64"]["value"], "unit": "evals/s",
                                  "ms_per_step": results["fp64"]["ms"]},
                 "fp32c_over_fp64": results["fp32c"]["value"] / results["fp64"]["value"],

@@ -68,6 +68,7 @@ _PROTOS = {
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
+    "btam_autotune": (ctypes.c_int, [_V, ctypes.c_int, _I, _I]),
     "btam_mf_eval_noalloc": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _V, _V, _V, _V,
                                             _V, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
@@ -245,6 +246,14 @@ class System:
         args = [_d(out.get(k)) for k in ("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals")]
         _check(lib().btam_results_copy(self.handle, *args), "btam_results_copy")
         return out
+
+    def autotune(self, precision=FP32C):
+        """Pick the fastest kernel shapes for this system; returns their
+        indices (pass 1, pass 2)."""
+        v1, v2 = ctypes.c_int(), ctypes.c_int()
+        _check(lib().btam_autotune(self.handle, precision, ctypes.byref(v1), ctypes.byref(v2)),
+               "btam_autotune")
+        return v1.value, v2.value
 
     def profile(self, precision=FP64):
         """Per-kernel device times (ms) of one evaluation: pass 1, pass 2,

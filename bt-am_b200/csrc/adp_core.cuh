@@ -175,15 +175,72 @@ template <class R> struct Geo {
   R u, du, w, dw; // dipole and quadrupole splines and derivatives
 };
 
+// |r| and 1/|r| from |r|^2: IEEE sqrt and divide in double; in the FP32
+// form one approximate reciprocal square root (a few ulp, far inside the
+// form's 1e-6 relative energy budget).
+BTAM_HD void norm_inv(double s2, double &s, double &inv) {
+  s = std::sqrt(s2);
+  inv = 1.0 / s;
+}
+BTAM_HD void norm_inv(float s2, float &s, float &inv) {
+#if defined(__CUDA_ARCH__)
+  inv = rsqrtf(s2);
+#else
+  inv = 1.0f / std::sqrt(s2);
+#endif
+  s = s2 * inv;
+}
+
 template <class R>
 BTAM_HD void geo_eval(Geo<R> &g, const V3<R> &r, const SplineView<R> &tu,
                       const SplineView<R> &tw) {
   g.r = r;
-  R s2 = dot3(r, r);
-  g.s = my_sqrt(s2);
-  g.inv_s = (R)1 / g.s;
+  norm_inv(dot3(r, r), g.s, g.inv_s);
   spline_vd(tu, g.s, g.u, g.du);
   spline_vd(tw, g.s, g.w, g.dw);
+}
+
+// Values only (pass 1 needs no derivatives and no 1/|r|).
+template <class R>
+BTAM_HD void geo_val(Geo<R> &g, const V3<R> &r, const SplineView<R> &tu,
+                     const SplineView<R> &tw) {
+  g.r = r;
+  norm_inv(dot3(r, r), g.s, g.inv_s);
+  g.u = spline_v(tu, g.s);
+  g.w = spline_v(tw, g.s);
+}
+
+// A dual prepared for the six geometries r0 + a e_k that move along one
+// axis: Lambda r, r^T Lambda r and Da.r at r0, so each displaced geometry
+// costs a few FMAs instead of a full 3x3 contraction.
+template <class R> struct DualAx {
+  Dual<R> D;
+  V3<R> Lr0;
+  R rLr0, dar0;
+};
+template <class R> BTAM_HD DualAx<R> dual_ax(const Dual<R> &D, const V3<R> &r0) {
+  DualAx<R> P;
+  P.D = D;
+  P.Lr0 = lam_r(D, r0);
+  P.rLr0 = dot3(r0, P.Lr0);
+  P.dar0 = D.a[0] * r0.x + D.a[1] * r0.y + D.a[2] * r0.z;
+  return P;
+}
+// D . J(r) and D . f(r) at r = r0 + a e_k (g evaluated at that r).
+template <class R>
+BTAM_HD void dual_ax_at(const DualAx<R> &P, int k, R a, const Geo<R> &g, V3<R> &J, R &f) {
+  const Dual<R> &D = P.D;
+  V3<R> col = k == 0 ? mk3<R>(D.d[0], D.o[0], D.o[1])
+                     : (k == 1 ? mk3<R>(D.o[0], D.d[1], D.o[2]) : mk3<R>(D.o[1], D.o[2], D.d[2]));
+  R lkk = k == 0 ? D.d[0] : (k == 1 ? D.d[1] : D.d[2]);
+  V3<R> Lr = mk3<R>(P.Lr0.x + a * col.x, P.Lr0.y + a * col.y, P.Lr0.z + a * col.z);
+  R rLr = P.rLr0 + a * ((R)2 * comp(P.Lr0, k) + a * lkk);
+  R dar = P.dar0 + a * D.a[k];
+  R c = (g.du * dar + g.dw * rLr) * g.inv_s;
+  R tw = (R)2 * g.w;
+  J = mk3<R>(g.u * D.a[0] + c * g.r.x + tw * Lr.x, g.u * D.a[1] + c * g.r.y + tw * Lr.y,
+             g.u * D.a[2] + c * g.r.z + tw * Lr.z);
+  f = g.u * dar + g.w * rLr;
 }
 
 // D . f(r) with f(r) = (u r, w r r^T):  u (Da.r) + w (r^T Lambda r)
@@ -191,6 +248,18 @@ template <class R> BTAM_HD R dual_f(const Dual<R> &D, const Geo<R> &g) {
   V3<R> Da = mk3<R>(D.a[0], D.a[1], D.a[2]);
   V3<R> Lr = lam_r(D, g.r);
   return g.u * dot3(Da, g.r) + g.w * dot3(g.r, Lr);
+}
+
+// D . J(r) and D . f(r) together (one Lambda r).
+template <class R> BTAM_HD void dual_Jf(const Dual<R> &D, const Geo<R> &g, V3<R> &J, R &f) {
+  V3<R> Da = mk3<R>(D.a[0], D.a[1], D.a[2]);
+  V3<R> Lr = lam_r(D, g.r);
+  R dar = dot3(Da, g.r), rLr = dot3(g.r, Lr);
+  R c = (g.du * dar + g.dw * rLr) * g.inv_s;
+  R tw = (R)2 * g.w;
+  J = mk3<R>(g.u * Da.x + c * g.r.x + tw * Lr.x, g.u * Da.y + c * g.r.y + tw * Lr.y,
+             g.u * Da.z + c * g.r.z + tw * Lr.z);
+  f = g.u * dar + g.w * rLr;
 }
 
 // D . J(r) with J = df/dr:  u Da + [(u'/s) Da.r + (w'/s) r^T Lambda r] r + 2 w Lambda r
@@ -293,6 +362,15 @@ BTAM_HD int pair_kind(int ci, int cj) { return ci == cj ? ci : 2; }
 //   g0    += X f(r0)
 //   hsum  += X sum_{6 j-displaced triplet pts} f
 //   cross += X^2 B(sum_{6} f, f(r0))
+// B(X, Y) of two feature sums in the working type.
+template <class R> BTAM_HD R bpair_r(const Feat<R> &x, const Feat<R> &y) {
+  R ab = x.a[0] * y.a[0] + x.a[1] * y.a[1] + x.a[2] * y.a[2];
+  R lm = x.l[0] * y.l[0] + x.l[1] * y.l[1] + x.l[2] * y.l[2] +
+         (R)2 * (x.l[3] * y.l[3] + x.l[4] * y.l[4] + x.l[5] * y.l[5]);
+  R t1 = x.l[0] + x.l[1] + x.l[2], t2 = y.l[0] + y.l[1] + y.l[2];
+  return (R)0.5 * ab + (R)0.5 * lm - t1 * t2 / (R)6;
+}
+
 template <class R> struct Pass1A {
   R rho, epair, ediag, cross;
   Feat<R> g0, hsum;
@@ -312,7 +390,7 @@ BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
     for (int k = 0; k < 3; ++k)
       for (int sg = 0; sg < 2; ++sg) {
         Geo<R> g;
-        geo_eval(g, disp(r0, k, sg ? -amt : amt), tu, tw);
+        geo_val(g, disp(r0, k, sg ? -amt : amt), tu, tw);
         rho += spline_v(tr, g.s);
         phi += spline_v(tp, g.s);
         diag += bff(g);
@@ -323,7 +401,7 @@ BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
   o.ediag += X * X * diag;
   // centre geometry
   Geo<R> g0;
-  geo_eval(g0, r0, tu, tw);
+  geo_val(g0, r0, tu, tw);
   Feat<R> f0{};
   feat_add(f0, g0);
   // neighbour-displaced triplet geometries
@@ -332,7 +410,7 @@ BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
     for (int sg = 0; sg < 2; ++sg) {
       Geo<R> g;
       R amt = sig_j * (R)kDelta9;
-      geo_eval(g, disp(r0, k, sg ? amt : -amt), tu, tw);
+      geo_val(g, disp(r0, k, sg ? amt : -amt), tu, tw);
       feat_add(hs, g);
     }
   for (int c = 0; c < 3; ++c) {
@@ -343,7 +421,7 @@ BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
     o.g0.l[c] += X * f0.l[c];
     o.hsum.l[c] += X * hs.l[c];
   }
-  o.cross += X * X * (R)bpair(hs.a, hs.l, f0.a, f0.l);
+  o.cross += X * X * bpair_r(hs, f0);
 }
 
 // Pass 1, part B: one centre displacement d = (k, sg) of pair (i, j):
@@ -353,7 +431,7 @@ BTAM_HD void pass1_pair_B(const TablesView<R> &T, const V3<R> &r0, R sig_i,
                           R X, int pk, int k, int sg, Feat<R> &gd, R &sself) {
   Geo<R> g;
   R amt = sig_i * (R)kDelta9;
-  geo_eval(g, disp(r0, k, sg ? -amt : amt), T.t[T_U + pk], T.t[T_W + pk]);
+  geo_val(g, disp(r0, k, sg ? -amt : amt), T.t[T_U + pk], T.t[T_W + pk]);
   Feat<R> f{};
   feat_add(f, g);
   for (int c = 0; c < 3; ++c) gd.a[c] += X * f.a[c];
@@ -447,60 +525,68 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
   geo_eval(gc, r0, tu, tw);
   const Dual<R> Xf0 = dual_feat(gc, X);  // dual of X f(r0)
 
-  // A: u displaced by +-3 sigma_u e_k.  Self i-displaced term (S4) and the
-  // neighbour-displaced term of j's energy (C5).
+  const R sfac = (R)2 * w9 * X;
+  // A: u displaced by +-3 sigma_u e_k.  Self centre-displaced term (S4); the
+  // neighbour-displaced term of j's energy (C5) and its occupancy gradient
+  // (X5) use fixed duals, so they go through the axis-displacement form.
   Feat<R> FA{};
   {
     const Dual<R> Dj_g0 = dual_at<R, true>(mj + kMomG0);
     const Dual<R> Dc5 = dual_sub(dual_flip(Dj_g0), Xf0);
+    const DualAx<R> c5 = dual_ax(Dc5, r0);
+    const DualAx<R> x5 = dual_ax(dual_sub(Dc5, Xf0), r0);
+    const R amt = sig_u * (R)kDelta9;
     for (int k = 0; k < 3; ++k)
       for (int sg = 0; sg < 2; ++sg) {
-        R amt = sig_u * (R)kDelta9;
+        const R a = sg ? -amt : amt;
         Geo<R> g;
-        geo_eval(g, disp(r0, k, sg ? -amt : amt), tu, tw);
+        geo_eval(g, disp(r0, k, a), tu, tw);
         feat_add(FA, g);
         R hb = (R)0.5 * X * bff_grad_coef(g);
         V3<R> v4 = dual_J(dual_at<R, false>(mu + kMomGd + 9 * (2 * k + sg)), g);  // S4
-        V3<R> v5 = dual_J(Dc5, g);                 // C5 (first part)
-        R sfac = (R)2 * w9 * X;
+        V3<R> v5, vx;
+        R f5, fx;
+        dual_ax_at(c5, k, a, g, v5, f5);  // C5
+        dual_ax_at(x5, k, a, g, vx, fx);  // X5: (P Dj.g0 - 2X dual(f0)) . f(r_A)
         V3<R> s4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
         self_q[0] += sfac * s4.x; self_q[1] += sfac * s4.y; self_q[2] += sfac * s4.z;
         cros_q[0] += sfac * v5.x; cros_q[1] += sfac * v5.y; cros_q[2] += sfac * v5.z;
         R sd = sg ? -(R)kDelta9 : (R)kDelta9;
         self_s += sfac * comp(s4, k) * sd;
         cros_s += sfac * comp(v5, k) * sd;
-        // X5 first piece: (P Dj.g0) . f(r_A) - X B(f(r_A), f0)
-        cros_x += (R)2 * w9 * xj * dual_f(dual_sub(dual_flip(Dj_g0), dual_feat(gc, (R)2 * X)), g);
+        cros_x += (R)2 * w9 * xj * fx;
       }
   }
   // B: j displaced by -+3 sigma_j e_k (centre j displaced by +-3 sigma_j e_k
-  // in j's frame).  Self neighbour-displaced term (S5) and j's centre-
-  // displaced term (C4).
+  // in j's frame).  Self neighbour-displaced term (S5, fixed dual) and j's
+  // centre-displaced term (C4) with its occupancy gradient (X4).
   Feat<R> FB{};
   {
-    const Dual<R> Ds5 = dual_sub(dual_at<R, false>(mu + kMomG0), Xf0);
+    const DualAx<R> s5 = dual_ax(dual_sub(dual_at<R, false>(mu + kMomG0), Xf0), r0);
+    const R amt = sig_j * (R)kDelta9;
     for (int k = 0; k < 3; ++k)
       for (int sg = 0; sg < 2; ++sg) {
-        R amt = sig_j * (R)kDelta9;
+        const R a = sg ? amt : -amt;
         Geo<R> g;
-        geo_eval(g, disp(r0, k, sg ? amt : -amt), tu, tw);
+        geo_eval(g, disp(r0, k, a), tu, tw);
         feat_add(FB, g);
-        R sfac = (R)2 * w9 * X;
-        V3<R> v5 = dual_J(Ds5, g);
+        V3<R> v5;
+        R f5;
+        dual_ax_at(s5, k, a, g, v5, f5);
         self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
         const Dual<R> Pj = dual_flip(dual_at<R, true>(mj + kMomGd + 9 * (2 * k + sg)));
-        V3<R> v4 = dual_J(Pj, g);
+        V3<R> v4;
+        R f4;
+        dual_Jf(Pj, g, v4, f4);
         R hb = (R)0.5 * X * bff_grad_coef(g);
         cros_q[0] += sfac * (v4.x - hb * g.r.x);
         cros_q[1] += sfac * (v4.y - hb * g.r.y);
         cros_q[2] += sfac * (v4.z - hb * g.r.z);
-        // X4: (P Dj.gd) . f - X B(f, f)
-        cros_x += (R)2 * w9 * xj * (dual_f(Pj, g) - X * bff(g));
+        cros_x += (R)2 * w9 * xj * (f4 - X * bff(g));
       }
   }
   // centre-geometry pieces of S5 and C5:  (D_H - X dual(F)) . J(r0)
   {
-    R sfac = (R)2 * w9 * X;
     Dual<R> dFB = dual_of<R, R>(FB.a, FB.l);
     Dual<R> dFA = dual_of<R, R>(FA.a, FA.l);
     for (int k = 0; k < 3; ++k) {

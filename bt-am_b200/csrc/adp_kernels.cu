@@ -28,7 +28,6 @@ namespace btam {
 
 namespace {
 
-constexpr int kWarps = 4;  // warps per block
 
 // Per-lane accumulator: plain double for the FP64 form, a two-sum
 // compensated float pair for the FP32 form.
@@ -65,13 +64,17 @@ __device__ __forceinline__ V3<R> pair_vec(const double4 &a, const double4 &b) {
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
-template <class R>
-__global__ void __launch_bounds__(kWarps * 32)
+// Kernels are instantiated for several (warps per block, minimum resident
+// blocks) shapes; the second number caps the registers per thread and so
+// trades instruction-level parallelism for occupancy.  btam_autotune times
+// the shapes on the actual system and keeps the fastest.
+template <class R, int W, int MB>
+__global__ void __launch_bounds__(W * 32, MB)
 pass1_kernel(const EvalArgs<R> a) {
-  __shared__ SiteSums ss[kWarps];
-  __shared__ double xbuf[kWarps][30][10];
+  __shared__ SiteSums ss[W];
+  __shared__ double xbuf[W][30][10];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * kWarps + warp;
+  const int i = blockIdx.x * W + warp;
   if (i >= a.n_real) return;
   R *mom = a.mom + (size_t)i * kMomStride;
   const double2 xbi = a.xb[i];
@@ -175,12 +178,12 @@ pass1_kernel(const EvalArgs<R> a) {
   }
 }
 
-template <class R>
-__global__ void __launch_bounds__(kWarps * 32)
+template <class R, int W, int MB>
+__global__ void __launch_bounds__(W * 32, MB)
 pass2_kernel(const EvalArgs<R> a) {
-  __shared__ R mu_s[kWarps][kMomStride];
+  __shared__ R mu_s[W][kMomStride];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * kWarps + warp;
+  const int u = blockIdx.x * W + warp;
   if (u >= a.n_real) return;
   const double2 xbu = a.xb[u];
   const double xu = xbu.x;
@@ -283,18 +286,40 @@ inline int nblocks(long long n, int per) { return (int)((n + per - 1) / per); }
 
 }  // namespace
 
-template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st) {
-  if (a.n_real > 0) pass1_kernel<R><<<nblocks(a.n_real, kWarps), kWarps * 32, 0, st>>>(a);
+template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st) {
+  pass1_kernel<R, W, MB><<<nblocks(a.n_real, W), W * 32, 0, st>>>(a);
+}
+template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st) {
+  pass2_kernel<R, W, MB><<<nblocks(a.n_real, W), W * 32, 0, st>>>(a);
+}
+
+template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v) {
+  if (a.n_real <= 0) return cudaSuccess;
+  switch (v) {
+  case 1: go1<R, 4, 3>(a, st); break;
+  case 2: go1<R, 4, 4>(a, st); break;
+  case 3: go1<R, 8, 2>(a, st); break;
+  case 4: go1<R, 2, 8>(a, st); break;
+  default: go1<R, 4, 1>(a, st); break;
+  }
   return cudaGetLastError();
 }
-template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st) {
-  if (a.n_real > 0) pass2_kernel<R><<<nblocks(a.n_real, kWarps), kWarps * 32, 0, st>>>(a);
+template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v) {
+  if (a.n_real <= 0) return cudaSuccess;
+  switch (v) {
+  case 1: go2<R, 4, 3>(a, st); break;
+  case 2: go2<R, 4, 4>(a, st); break;
+  case 3: go2<R, 4, 5>(a, st); break;
+  case 4: go2<R, 8, 2>(a, st); break;
+  case 5: go2<R, 2, 8>(a, st); break;
+  default: go2<R, 4, 1>(a, st); break;
+  }
   return cudaGetLastError();
 }
-template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t);
-template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t);
-template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t);
-template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t);
+template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t, int);
+template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, int);
+template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t, int);
+template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t, int);
 
 cudaError_t launch_totals(int n_real, const double *V0, const double *S0, const double *Rq,
                           const double *Rs, const double *Rx, double *out, cudaStream_t st) {

@@ -28,9 +28,14 @@ template <class R> struct EvalArgs {
 };
 
 // Pass 1: rho-bar, V0, S0, dV0/dx (self) and the moment record of every
-// real site.  Pass 2: residuals of every real site.
-template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st);
-template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st);
+// real site.  Pass 2: residuals of every real site.  `variant` picks the
+// block shape / register cap (0 = default; see kPass1Variants below).
+template <class R>
+cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
+template <class R>
+cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
+constexpr int kPass1Variants = 5;  // (4 warps,-), (4,3), (4,4), (8,2), (2,8)
+constexpr int kPass2Variants = 6;  // (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
 
 // Deterministic FP64 totals over real sites: out[0] = sum V0, out[1] = sum S0,
 // out[2] = sum |R_q|^2 + R_sigma^2 (active sites), out[3] = sum R_x^2.

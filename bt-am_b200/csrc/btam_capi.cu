@@ -148,6 +148,9 @@ struct btam_system {
   float *mom32 = nullptr;
   int *err = nullptr;
   DeviceScratch scratch;
+  // kernel block shapes per arithmetic form (index 0 FP64, 1 FP32C), chosen
+  // by btam_autotune
+  int variant1[2] = {0, 0}, variant2[2] = {0, 0};
 };
 
 namespace {
@@ -667,15 +670,81 @@ int btam_mf_eval_async(btam_system *s, int precision) {
   if (precision == BTAM_FP64) {
     if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
     EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
-    BTAM_TRY(launch_pass1(a, s->st));
-    BTAM_TRY(launch_pass2(a, s->st));
+    BTAM_TRY(launch_pass1(a, s->st, s->variant1[0]));
+    BTAM_TRY(launch_pass2(a, s->st, s->variant2[0]));
   } else {
     if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
     EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
-    BTAM_TRY(launch_pass1(a, s->st));
-    BTAM_TRY(launch_pass2(a, s->st));
+    BTAM_TRY(launch_pass1(a, s->st, s->variant1[1]));
+    BTAM_TRY(launch_pass2(a, s->st, s->variant2[1]));
   }
   BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->st));
+  return BTAM_OK;
+}
+
+}  // extern "C"
+
+// Times every block shape of pass 1, then of pass 2 (after the best pass 1
+// has produced the moments pass 2 reads), reps times each, and keeps the
+// shape with the smallest time for this system and arithmetic form.
+template <class R>
+static int autotune_form(btam_system *s, EvalArgs<R> a, int form, int reps) {
+  cudaEvent_t e0, e1;
+  BTAM_TRY(cudaEventCreate(&e0));
+  BTAM_TRY(cudaEventCreate(&e1));
+  cudaError_t e = cudaSuccess;
+  auto time_one = [&](bool second, int v) -> float {
+    float best = 1e30f;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+      e = cudaEventRecord(e0, s->st);
+      if (e == cudaSuccess) e = second ? launch_pass2(a, s->st, v) : launch_pass1(a, s->st, v);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s->st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) best = ms;
+    }
+    return best;
+  };
+  int b1 = 0, b2 = 0;
+  float t1 = 1e30f, t2 = 1e30f;
+  for (int v = 0; v < kPass1Variants && e == cudaSuccess; ++v) {
+    float t = time_one(false, v);
+    if (t < t1) { t1 = t; b1 = v; }
+  }
+  if (e == cudaSuccess) e = launch_pass1(a, s->st, b1);
+  for (int v = 0; v < kPass2Variants && e == cudaSuccess; ++v) {
+    float t = time_one(true, v);
+    if (t < t2) { t2 = t; b2 = v; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e != cudaSuccess) return cuda_status(e);
+  s->variant1[form] = b1;
+  s->variant2[form] = b2;
+  return read_err(s);
+}
+
+extern "C" {
+
+int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_variant) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  int st;
+  if (precision == BTAM_FP64) {
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
+    st = autotune_form(s, eval_args<double>(s, s->mom64, s->T->v64), 0, 3);
+  } else if (precision == BTAM_FP32C) {
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
+    st = autotune_form(s, eval_args<float>(s, s->mom32, s->T->v32), 1, 3);
+  } else {
+    return BTAM_ERR_ARG;
+  }
+  if (st != BTAM_OK) return st;
+  const int f = precision == BTAM_FP64 ? 0 : 1;
+  if (pass1_variant) *pass1_variant = s->variant1[f];
+  if (pass2_variant) *pass2_variant = s->variant2[f];
   return BTAM_OK;
 }
 
@@ -737,15 +806,15 @@ int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]) {
   if (precision == BTAM_FP64) {
     if (!s->mom64 && e == cudaSuccess) e = dalloc(s->mom64, nm);
     EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
-    if (e == cudaSuccess) e = launch_pass1(a, s->st);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[0]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
-    if (e == cudaSuccess) e = launch_pass2(a, s->st);
+    if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[0]);
   } else {
     if (!s->mom32 && e == cudaSuccess) e = dalloc(s->mom32, nm);
     EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
-    if (e == cudaSuccess) e = launch_pass1(a, s->st);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[1]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
-    if (e == cudaSuccess) e = launch_pass2(a, s->st);
+    if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[1]);
   }
   if (e == cudaSuccess) e = cudaEventRecord(ev[2], s->st);
   if (e == cudaSuccess)

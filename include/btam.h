@@ -149,6 +149,11 @@ int btam_results_copy(btam_system *s, double *rho, double *V0, double *S0,
                       double *Rq, double *Rs, double *Rx, double *totals);
 /* Waits for the system's stream and returns the first error it raised. */
 int btam_system_sync(btam_system *s);
+/* Autotuner (no counterpart in the reference): times every compiled block
+ * shape / register cap of the two kernels on this system and keeps the
+ * fastest for later evaluations in `precision`; reports the chosen indices.
+ * Results are identical for every shape (same arithmetic, same order). */
+int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_variant);
 
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */

@@ -108,6 +108,21 @@ def test_deterministic_and_state_update(gpu_tables, hostmodel, oracle):
         assert rel(out[k], ref[k]) < 1e-11, k
 
 
+def test_autotuned_shapes_give_identical_results(gpu_tables):
+    """Every kernel block shape runs the same arithmetic in the same order, so
+    the autotuner's choice never changes a result bit."""
+    g = load("config1")
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    for prec in (btam.FP64, btam.FP32C):
+        before = S.evaluate(prec)
+        v1, v2 = S.autotune(prec)
+        assert 0 <= v1 < 5 and 0 <= v2 < 6
+        after = S.evaluate(prec)
+        for k in before:
+            assert np.array_equal(before[k], after[k]), (prec, k)
+
+
 def test_error_codes(gpu_tables):
     s = lattice.supercell(3, 2, 3, ortho=True, with_tetra=False)
     with pytest.raises(btam.BtamError) as e:
