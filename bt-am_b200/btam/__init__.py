@@ -69,6 +69,14 @@ _PROTOS = {
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
     "btam_autotune": (ctypes.c_int, [_V, ctypes.c_int, _I, _I]),
+    "btam_relax": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                  _D, _D]),
+    "btam_system_get_state": (ctypes.c_int, [_V, _D, _D, _D]),
+    "btam_dmd_setup": (ctypes.c_int, [_V]),
+    "btam_dmd_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D,
+                                     ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_dmd_occupancy": (ctypes.c_int, [_V, _D, ctypes.POINTER(ctypes.c_longlong), _D]),
+    "btam_dmd_graph_copy": (ctypes.c_int, [_V, _I, _I, ctypes.c_longlong]),
     "btam_mf_eval_noalloc": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _V, _V, _V, _V,
                                             _V, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
@@ -246,6 +254,58 @@ class System:
         args = [_d(out.get(k)) for k in ("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals")]
         _check(lib().btam_results_copy(self.handle, *args), "btam_results_copy")
         return out
+
+    def get_state(self):
+        q = np.zeros((self.n, 3))
+        sigma = np.zeros(self.n)
+        x = np.zeros(self.n)
+        _check(lib().btam_system_get_state(self.handle, _d(q), _d(sigma), _d(x)),
+               "btam_system_get_state")
+        return q, sigma, x
+
+    # -- consumers: relaxation and the hydrogen master equation
+    def relax(self, mode=0, tol=1e-8, max_iter=500, m=8, sigma_min=0.001, sigma_max=0.4,
+              x_min=0.01):
+        """L-BFGS relaxation of (q, sigma) on the device.  Returns a dict with
+        the final projected residual norm, iterations, evaluations, objective
+        and status (1 converged, 0 iteration limit, -1 stalled)."""
+        info = np.zeros(5)
+        bd = np.array([sigma_min, sigma_max, x_min], np.float64)
+        _check(lib().btam_relax(self.handle, mode, tol, max_iter, m, _d(bd), _d(info)),
+               "btam_relax")
+        return dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
+                    objective=info[3], status=int(info[4]))
+
+    def dmd_setup(self):
+        _check(lib().btam_dmd_setup(self.handle), "btam_dmd_setup")
+
+    def dmd_step(self, nsteps=1, precision=FP64, dt=4e-4, Df=0.045, dr=3.2, min_dx=1e-8,
+                 max_x=0.9):
+        """Master-equation steps; returns the exact total of the occupancy
+        quanta (Python int, units of 2^-50)."""
+        prm = np.array([dt, Df, dr, min_dx, max_x], np.float64)
+        tot = (ctypes.c_longlong * 2)()
+        _check(lib().btam_dmd_step(self.handle, precision, nsteps, _d(prm), tot),
+               "btam_dmd_step")
+        hi, lo = tot[0], tot[1] & 0xFFFFFFFFFFFFFFFF
+        return (hi << 64) + lo
+
+    def dmd_occupancy(self):
+        x = np.zeros(self.n)
+        qn = np.zeros(self.n, np.int64)
+        mu = np.zeros(self.n)
+        _check(lib().btam_dmd_occupancy(self.handle, _d(x),
+                                        qn.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+                                        _d(mu)), "btam_dmd_occupancy")
+        return x, qn, mu
+
+    def dmd_graph(self):
+        offs = np.zeros(self.n + 1, np.int32)
+        _check(lib().btam_dmd_graph_copy(self.handle, _i(offs), None, 0), "btam_dmd_graph_copy")
+        idx = np.zeros(max(int(offs[-1]), 1), np.int32)
+        _check(lib().btam_dmd_graph_copy(self.handle, _i(offs), _i(idx), len(idx)),
+               "btam_dmd_graph_copy")
+        return offs, idx[:offs[-1]]
 
     def autotune(self, precision=FP32C):
         """Pick the fastest kernel shapes for this system; returns their

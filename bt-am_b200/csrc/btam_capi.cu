@@ -16,6 +16,7 @@
 #include "../../include/btam.h"
 #include "adp_core.cuh"
 #include "adp_kernels.cuh"
+#include "solvers.cuh"
 #include "tables_io.hpp"
 #include "topo_kernels.cuh"
 
@@ -151,7 +152,22 @@ struct btam_system {
   // kernel block shapes per arithmetic form (index 0 FP64, 1 FP32C), chosen
   // by btam_autotune
   int variant1[2] = {0, 0}, variant2[2] = {0, 0};
+  int cnt_cap = 0;
+  // diffusive graph and master-equation state
+  bool dmd_ready = false;
+  int *doffs = nullptr, *didx = nullptr, dq_cap = 0;
+  long long didx_cap = 0, d_pairs = 0;
+  long long *X = nullptr, *X0 = nullptr, *dtot = nullptr;
+  double *mu = nullptr;
+  int *dact = nullptr, *ddeg = nullptr;
+  // relaxation work vectors
+  int relax_m = 0;
+  double *rv = nullptr;  // one block holding every relaxation vector
 };
+
+static int build_list(btam_system *s, int n_all, int n_query, double rc, int maxn, int filter,
+                      int allow_empty, int *&offs, int &q_cap, int *&idx, long long &idx_cap,
+                      int &total);
 
 namespace {
 
@@ -493,6 +509,8 @@ void btam_system_destroy(btam_system *s) {
   dfree(s->cell_start); dfree(s->cursor); dfree(s->cell_sites); dfree(s->rho); dfree(s->V0);
   dfree(s->S0); dfree(s->selfx); dfree(s->Rq); dfree(s->Rs); dfree(s->Rx); dfree(s->totals);
   dfree(s->mom64); dfree(s->mom32); dfree(s->err);
+  dfree(s->doffs); dfree(s->didx); dfree(s->X); dfree(s->X0); dfree(s->dtot); dfree(s->mu);
+  dfree(s->dact); dfree(s->ddeg); dfree(s->rv);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
 }
@@ -580,10 +598,30 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
     BTAM_TRY(dalloc(s->cell_sites, n_all));
     s->site_cap = n_all;
   }
-  if (n_query + 1 > s->q_cap) {
+  int total = 0;
+  int st = build_list(s, n_all, n_query, BTAM_R_CUTOFF, BTAM_MAXNEIGH, -1, 0, s->offs, s->q_cap,
+                      s->idx, s->idx_cap, total);
+  if (st != BTAM_OK) return st;
+  s->n_list = n_query;
+  s->n_pairs = total;
+  s->built = true;
+  return BTAM_OK;
+}
+
+}  // extern "C"
+
+// One CSR neighbour list over the current sites: cell binning, per-site
+// search (optionally restricted to one species code), scan and compaction.
+static int build_list(btam_system *s, int n_all, int n_query, double rc, int maxn, int filter,
+                      int allow_empty, int *&offs, int &q_cap, int *&idx, long long &idx_cap,
+                      int &total) {
+  if (n_query + 1 > s->cnt_cap) {
     BTAM_TRY(dalloc(s->cnt, n_query + 1));
-    BTAM_TRY(dalloc(s->offs, n_query + 1));
-    s->q_cap = n_query + 1;
+    s->cnt_cap = n_query + 1;
+  }
+  if (n_query + 1 > q_cap) {
+    BTAM_TRY(dalloc(offs, n_query + 1));
+    q_cap = n_query + 1;
   }
   if ((long long)n_query * kNbrBuf > s->tmp_cap) {
     BTAM_TRY(dalloc(s->tmp, (size_t)n_query * kNbrBuf));
@@ -592,10 +630,13 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
   NbrArgs a;
   a.n_all = n_all;
   a.n_query = n_query;
-  a.maxn = BTAM_MAXNEIGH;
+  a.maxn = maxn;
   a.max_cells = s->cell_cap;
-  a.rc = BTAM_R_CUTOFF;
-  a.cell_edge = BTAM_R_CUTOFF * (1.0 + 1e-9) + 1e-9;
+  a.rc = rc;
+  a.cell_edge = rc * (1.0 + 1e-9) + 1e-9;
+  a.code = s->code;
+  a.filter_code = filter;
+  a.allow_empty = allow_empty;
   a.pos = s->pos;
   a.bbox = s->bbox;
   a.grid = s->grid;
@@ -606,25 +647,24 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
   a.cell_sites = s->cell_sites;
   a.cnt = s->cnt;
   a.tmp = s->tmp;
-  a.offs = s->offs;
+  a.offs = offs;
   a.err = s->err;
   a.scratch = &s->scratch;
   BTAM_TRY(launch_neighbors(a, s->st));
-  int total = 0;
-  BTAM_TRY(cudaMemcpyAsync(&total, s->offs + n_query, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  total = 0;
+  BTAM_TRY(cudaMemcpyAsync(&total, offs + n_query, sizeof(int), cudaMemcpyDeviceToHost, s->st));
   int st = read_err(s);
   if (st != BTAM_OK) return st;
-  if (total > s->idx_cap) {
-    BTAM_TRY(dalloc(s->idx, total));
-    s->idx_cap = total;
+  if (total > idx_cap) {
+    BTAM_TRY(dalloc(idx, total));
+    idx_cap = total;
   }
-  BTAM_TRY(launch_compact(n_query, s->tmp, s->offs, s->idx, s->st));
+  BTAM_TRY(launch_compact(n_query, s->tmp, offs, idx, s->st));
   BTAM_TRY(cudaStreamSynchronize(s->st));
-  s->n_list = n_query;
-  s->n_pairs = total;
-  s->built = true;
   return BTAM_OK;
 }
+
+extern "C" {
 
 int btam_neighbors_copy(const btam_system *s, int *offs, int *idx, long long idx_cap) {
   if (!s || !offs) return BTAM_ERR_ARG;
@@ -876,6 +916,318 @@ int btam_rho_nmf(btam_system *s, double *rho) {
                           s->T->v64.t[T_RHO_MG], s->T->v64.t[T_RHO_H], s->rho, s->st));
   BTAM_TRY(cudaMemcpyAsync(rho, s->rho, s->n_real * sizeof(double), cudaMemcpyDeviceToHost, s->st));
   return read_err(s);
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Relaxation of (q, sigma) and the hydrogen master equation (solvers.cu).
+
+namespace {
+
+// Evaluation followed by the relaxation view of it: z, g, F and |R|^2.
+struct RelaxVecs {
+  double *z, *g, *p, *z0, *g0, *work, *tmp, *fterm, *rterm, *ones, *scal, *rho, *alpha;
+  double *S[16], *Y[16];
+  RelaxBounds bd;
+};
+
+int relax_eval(btam_system *s, int prec, RelaxVecs &v, double &f, double &r2) {
+  int st = btam_mf_eval_async(s, prec);
+  if (st != BTAM_OK) return st;
+  BTAM_TRY(relax_gather(s->n_real, s->pos, s->xb, s->V0, s->Rq, s->Rs, v.bd, v.z, v.g, v.fterm,
+                        v.rterm, v.scal, v.scal + 1, v.ones, s->st));
+  double h[2];
+  BTAM_TRY(cudaMemcpyAsync(h, v.scal, 2 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  st = read_err(s);
+  f = h[0];
+  r2 = h[1];
+  return st;
+}
+
+double dev_dot(btam_system *s, RelaxVecs &v, int n, const double *a, const double *b) {
+  vec_dot(n, a, b, v.tmp + 7, s->st);
+  double h = 0.0;
+  cudaMemcpyAsync(&h, v.tmp + 7, sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  cudaStreamSynchronize(s->st);
+  return h;
+}
+
+__global__ void fill_kernel(int n, double v, double *a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+
+// max over sites and components of |p| in unscaled units (p / sqrt(max(x, 1e-3)))
+__global__ void absmax_kernel(int n4, const double2 *xb, const double *a, double *out) {
+  __shared__ double sh[256];
+  double v = 0.0;
+  for (int i = threadIdx.x; i < n4; i += 256)
+    v = fmax(v, fabs(a[i]) / sqrt(fmax(xb[i >> 2].x, 1e-3)));
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int k = 128; k > 0; k >>= 1) {
+    if ((int)threadIdx.x < k) sh[threadIdx.x] = fmax(sh[threadIdx.x], sh[threadIdx.x + k]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = sh[0];
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m, const double *bounds,
+               double *info) {
+  if (!s || !(tol > 0.0) || max_iter < 0 || m < 1 || m > 16) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (mode < 0 || mode > 2) return BTAM_ERR_ARG;
+  const double sig_lo = bounds ? bounds[0] : 0.001, sig_hi = bounds ? bounds[1] : 0.4,
+               x_min = bounds ? bounds[2] : 0.01;
+  if (!(sig_lo > 0.0 && sig_hi > sig_lo && x_min >= 0.0)) return BTAM_ERR_ARG;
+  const int n = s->n_real, n4 = 4 * n;
+  // layout: z g p z0 g0 work (n4 each), S[m] Y[m] (n4 each), fterm rterm ones (n), small
+  const size_t need = (size_t)(6 + 2 * m) * n4 + 3 * (size_t)n + 64;
+  if (!s->rv || s->relax_m < m) {
+    BTAM_TRY(dalloc(s->rv, need));
+    s->relax_m = m;
+  }
+  RelaxVecs v;
+  double *b = s->rv;
+  v.z = b; v.g = b + n4; v.p = b + 2 * n4; v.z0 = b + 3 * n4; v.g0 = b + 4 * n4;
+  v.work = b + 5 * n4;
+  for (int k = 0; k < m; ++k) {
+    v.S[k] = b + (size_t)(6 + k) * n4;
+    v.Y[k] = b + (size_t)(6 + m + k) * n4;
+  }
+  v.fterm = b + (size_t)(6 + 2 * m) * n4;
+  v.rterm = v.fterm + n;
+  v.ones = v.rterm + n;
+  v.scal = v.ones + n;
+  v.tmp = v.scal + 2;       // 8 scratch scalars
+  v.rho = v.tmp + 8;        // m
+  v.alpha = v.rho + 16;     // m
+  v.bd.ls_lo = std::log(sig_lo);
+  v.bd.ls_hi = std::log(sig_hi);
+  v.bd.x_min = x_min;
+  fill_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(n, 1.0, v.ones);
+  BTAM_TRY(cudaGetLastError());
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+
+  int prec = (mode == 0) ? BTAM_FP64 : BTAM_FP32C;
+  const double switch_tol = 1e-5;  // FP32C noise floor is ~1e-6
+  double f, r2;
+  int evals = 0, it = 0, st;
+  if ((st = relax_eval(s, prec, v, f, r2)) != BTAM_OK) return st;
+  ++evals;
+  std::vector<int> order;
+  std::vector<double> rho_h(16, 0.0);
+  bool stalled = false;
+  for (; it < max_iter; ++it) {
+    if (mode == 1 && prec == BTAM_FP32C && std::sqrt(r2) < switch_tol) {
+      prec = BTAM_FP64;
+      order.clear();
+      if ((st = relax_eval(s, prec, v, f, r2)) != BTAM_OK) return st;
+      ++evals;
+    }
+    if (std::sqrt(r2) <= tol) break;
+    BTAM_TRY(lbfgs_direction(n4, v.g, v.S, v.Y, v.rho, order.data(), (int)order.size(), v.p,
+                             v.work, v.alpha, v.tmp, s->st));
+    double gp = dev_dot(s, v, n4, v.g, v.p);
+    if (!(gp < 0.0)) {  // not a descent direction: restart from steepest descent
+      order.clear();
+      BTAM_TRY(lbfgs_direction(n4, v.g, v.S, v.Y, v.rho, nullptr, 0, v.p, v.work, v.alpha, v.tmp,
+                               s->st));
+      gp = dev_dot(s, v, n4, v.g, v.p);
+    }
+    // first step of a history: move no q (A) or log sigma by more than 0.05;
+    // this step also seeds the curvature scale of the history
+    double alpha = 1.0;
+    if (order.empty()) {
+      absmax_kernel<<<1, 256, 0, s->st>>>(n4, s->xb, v.p, v.tmp + 6);
+      double pmax = 0.0;
+      BTAM_TRY(cudaMemcpyAsync(&pmax, v.tmp + 6, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+      BTAM_TRY(cudaStreamSynchronize(s->st));
+      if (pmax > 0.05) alpha = 0.05 / pmax;
+    }
+    BTAM_TRY(cudaMemcpyAsync(v.z0, v.z, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaMemcpyAsync(v.g0, v.g, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    const double f0 = f, r20 = r2;
+    bool ok = false;
+    for (int ls = 0; ls < 30; ++ls) {
+      BTAM_TRY(relax_apply(n, s->xb, v.z0, v.p, alpha, v.bd, s->pos, s->st));
+      if (s->n_ghost > 0)
+        BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                      s->box, s->st));
+      if ((st = relax_eval(s, prec, v, f, r2)) != BTAM_OK) return st;
+      ++evals;
+      // Armijo decrease of F; once F's changes are below its rounding (about
+      // 1e-7 relative in the FP32C form, 1e-13 in FP64), a step that lowers
+      // the residual is accepted instead
+      const double noise = (prec == BTAM_FP32C ? 1e-7 : 1e-13) * std::fabs(f0);
+      if (f <= f0 + 1e-4 * alpha * gp || (std::fabs(f - f0) <= noise && r2 < r20)) {
+        ok = true;
+        break;
+      }
+      alpha *= 0.5;
+    }
+    if (!ok) {  // no decrease resolvable at this precision: restore and stop
+      BTAM_TRY(relax_apply(n, s->xb, v.z0, v.p, 0.0, v.bd, s->pos, s->st));
+      if (s->n_ghost > 0)
+        BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                      s->box, s->st));
+      if (mode == 1 && prec == BTAM_FP32C) prec = BTAM_FP64;  // finish in FP64
+      if ((st = relax_eval(s, prec, v, f, r2)) != BTAM_OK) return st;
+      ++evals;
+      if (!order.empty()) {  // restart from steepest descent before giving up
+        order.clear();
+        continue;
+      }
+      stalled = true;
+      (void)r20;
+      break;
+    }
+    // history pair (newest last, oldest dropped)
+    int slot = (int)order.size() < m ? (int)order.size() : order.front();
+    if ((int)order.size() == m) order.erase(order.begin());
+    BTAM_TRY(lbfgs_push(n4, v.z, v.z0, v.g, v.g0, v.S[slot], v.Y[slot], v.tmp, s->st));
+    double sy = 0.0;
+    BTAM_TRY(cudaMemcpyAsync(&sy, v.tmp, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    BTAM_TRY(cudaStreamSynchronize(s->st));
+    if (sy > 1e-300) {
+      rho_h[slot] = 1.0 / sy;
+      BTAM_TRY(cudaMemcpyAsync(v.rho + slot, &rho_h[slot], sizeof(double), cudaMemcpyHostToDevice,
+                               s->st));
+      order.push_back(slot);
+    }
+  }
+  if (info) {
+    info[0] = std::sqrt(r2);
+    info[1] = it;
+    info[2] = evals;
+    info[3] = f;
+    info[4] = (std::sqrt(r2) <= tol) ? 1.0 : (stalled ? -1.0 : 0.0);
+  }
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  return BTAM_OK;
+}
+
+int btam_dmd_setup(btam_system *s) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  const int n = s->n_real;
+  int total = 0;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  int st = build_list(s, n + s->n_ghost, n, BTAM_R_CUTOFF_EB, BTAM_MAX_CHEMICAL_NEIGHS, 1, 1,
+                      s->doffs, s->dq_cap, s->didx, s->didx_cap, total);
+  if (st != BTAM_OK) return st;
+  s->d_pairs = total;
+  for (long long **p : {&s->X, &s->X0})
+    BTAM_TRY(dalloc(*p, n));
+  BTAM_TRY(dalloc(s->dtot, 2));
+  BTAM_TRY(dalloc(s->mu, n));
+  BTAM_TRY(dalloc(s->dact, n));
+  BTAM_TRY(dalloc(s->ddeg, n));
+  BTAM_TRY(dmd_init(n, s->xb, s->code, s->X, s->st));
+  BTAM_TRY(dmd_commit_all(n, s->code, s->X, s->xb, s->st));
+  if (s->n_ghost > 0)
+    BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                  s->box, s->st));
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  s->dmd_ready = true;
+  return BTAM_OK;
+}
+
+int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *params,
+                  long long *total_quanta) {
+  if (!s || nsteps < 0) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  DmdParams prm;
+  // defaults: the reference's diffusion parameters (Variables.hpp:68-92)
+  prm.dt = params ? params[0] : 4e-4;
+  prm.Df = params ? params[1] : 0.045;
+  prm.dr = params ? params[2] : 3.2;
+  prm.min_dx = params ? params[3] : 1e-8;
+  prm.max_x = params ? params[4] : 0.9;
+  if (!(prm.dt >= 0.0 && prm.Df >= 0.0 && prm.dr > 0.0 && prm.max_x > 0.0)) return BTAM_ERR_ARG;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  DmdArgs a;
+  a.n = s->n_real;
+  a.xb = s->xb;
+  a.code = s->code;
+  a.owner = s->owner;
+  a.Rx = s->Rx;
+  a.gamma = s->gamma;
+  a.moffs = s->offs;
+  a.midx = s->idx;
+  a.doffs = s->doffs;
+  a.didx = s->didx;
+  a.X = s->X;
+  a.X0 = s->X0;
+  a.mu = s->mu;
+  a.active = s->dact;
+  a.deg = s->ddeg;
+  for (int k = 0; k < nsteps; ++k) {
+    int st = btam_mf_eval_async(s, precision);  // chemical potentials at the current x
+    if (st != BTAM_OK) return st;
+    BTAM_TRY(dmd_step(a, prm, s->st));
+    if (s->n_ghost > 0)
+      BTAM_TRY(launch_ghost_refresh(s->n_real, s->n_ghost, s->pos, s->xb, s->code, s->owner,
+                                    s->image, s->box, s->st));
+  }
+  if (total_quanta) {
+    BTAM_TRY(dmd_total(s->n_real, s->code, s->X, s->dtot, s->st));
+    BTAM_TRY(cudaMemcpyAsync(total_quanta, s->dtot, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
+                             s->st));
+  }
+  return read_err(s);
+}
+
+int btam_dmd_occupancy(btam_system *s, double *x, long long *quanta, double *mu) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  const int n = s->n_real;
+  if (quanta)
+    BTAM_TRY(cudaMemcpyAsync(quanta, s->X, n * sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+  if (mu) BTAM_TRY(cudaMemcpyAsync(mu, s->mu, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  if (x) {
+    std::vector<double2> h(n);
+    BTAM_TRY(cudaMemcpyAsync(h.data(), s->xb, n * sizeof(double2), cudaMemcpyDeviceToHost, s->st));
+    BTAM_TRY(cudaStreamSynchronize(s->st));
+    for (int i = 0; i < n; ++i) x[i] = h[i].x;
+  }
+  return read_err(s);
+}
+
+int btam_dmd_graph_copy(const btam_system *s, int *offs, int *idx, long long idx_cap) {
+  if (!s || !offs) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  BTAM_TRY(cudaMemcpy(offs, s->doffs, (s->n_real + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  if (idx) {
+    if (idx_cap < s->d_pairs) return BTAM_ERR_ARG;
+    BTAM_TRY(cudaMemcpy(idx, s->didx, s->d_pairs * sizeof(int), cudaMemcpyDeviceToHost));
+  }
+  return BTAM_OK;
+}
+
+int btam_system_get_state(btam_system *s, double *q, double *sigma, double *x) {
+  if (!s) return BTAM_ERR_ARG;
+  const int n = s->n_real;
+  std::vector<double4> hp(n);
+  std::vector<double2> hx(n);
+  BTAM_TRY(cudaMemcpyAsync(hp.data(), s->pos, n * sizeof(double4), cudaMemcpyDeviceToHost, s->st));
+  BTAM_TRY(cudaMemcpyAsync(hx.data(), s->xb, n * sizeof(double2), cudaMemcpyDeviceToHost, s->st));
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  for (int i = 0; i < n; ++i) {
+    if (q) {
+      q[3 * i] = hp[i].x;
+      q[3 * i + 1] = hp[i].y;
+      q[3 * i + 2] = hp[i].z;
+    }
+    if (sigma) sigma[i] = hp[i].w;
+    if (x) x[i] = hx[i].x;
+  }
+  return BTAM_OK;
 }
 
 }  // extern "C"

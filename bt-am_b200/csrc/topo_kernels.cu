@@ -210,11 +210,16 @@ template <int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
 neighbor_kernel(int n_query, const double4 *pos, const CellGrid *gp,
                 const int *cell_start, const int *cell_sites, double rc,
-                int maxn, int *cnt, int *tmp, int *err) {
+                int maxn, int *cnt, int *tmp, int *err, const int *code, int filter,
+                int allow_empty) {
   __shared__ int buf[WARPS][kNbrBuf];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int i = blockIdx.x * WARPS + warp;
   if (i >= n_query) return;
+  if (filter >= 0 && code[i] != filter) {  // not a site of this graph
+    if (lane == 0) cnt[i] = 0;
+    return;
+  }
   CellGrid g = *gp;
   double4 qi = pos[i];
   int cx = cell_coord(g, qi.x, 0), cy = cell_coord(g, qi.y, 1), cz = cell_coord(g, qi.z, 2);
@@ -237,7 +242,7 @@ neighbor_kernel(int n_query, const double4 *pos, const CellGrid *gp,
           int j = -1;
           if (t < s1) {
             j = cell_sites[t];
-            if (j != i) {
+            if (j != i && (filter < 0 || code[j] == filter)) {
               double4 qj = pos[j];
               double ex = __dadd_rn(qi.x, -qj.x), ey = __dadd_rn(qi.y, -qj.y),
                      ez = __dadd_rn(qi.z, -qj.z);
@@ -278,7 +283,7 @@ neighbor_kernel(int n_query, const double4 *pos, const CellGrid *gp,
     if (lane == 0) atomicOr(err, 1 << kErrBitOverflow);
     count = maxn;
   }
-  if (count == 0 && lane == 0) atomicOr(err, 1 << kErrBitEmpty);
+  if (count == 0 && lane == 0 && !allow_empty) atomicOr(err, 1 << kErrBitEmpty);
   for (int t = lane; t < count; t += 32) tmp[(size_t)i * kNbrBuf + t] = b[t];
   if (lane == 0) cnt[i] = count;
 }
@@ -347,7 +352,7 @@ cudaError_t launch_neighbors(const NbrArgs &a, cudaStream_t st) {
   constexpr int W = 4;
   neighbor_kernel<W><<<blocks(a.n_query, W), W * 32, 0, st>>>(
       a.n_query, a.pos, a.grid, a.cell_start, a.cell_sites, a.rc, a.maxn, a.cnt, a.tmp,
-      a.err);
+      a.err, a.code, a.filter_code, a.allow_empty);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   // offsets: exclusive scan of counts with one extra zero slot at the end
   cudaMemsetAsync(a.cnt + a.n_query, 0, sizeof(int), st);

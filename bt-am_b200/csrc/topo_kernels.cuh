@@ -64,6 +64,11 @@ struct NbrArgs {
   int *offs;  // n_query + 1
   int *err;
   DeviceScratch *scratch;
+  // optional restriction to one species code (-1: all sites), e.g. the H-H
+  // diffusive graph; allow_empty = 1 accepts sites with no neighbour
+  const int *code = nullptr;
+  int filter_code = -1;
+  int allow_empty = 0;
 };
 
 cudaError_t exclusive_scan(const int *in, int *out, int n, DeviceScratch &s,

@@ -61,10 +61,17 @@ extern "C" {
 #define BTAM_T_W_HH 11
 #define BTAM_T_W_MGH 12
 
-/* reference constants (src/Macros.hpp:857, 862, 869) */
+/* reference constants (src/Macros.hpp:857-869) */
 #define BTAM_R_CUTOFF 6.2934034034
+#define BTAM_R_CUTOFF_EB 2.6          /* H-H diffusive pairs */
 #define BTAM_MAXNEIGH 250
+#define BTAM_MAX_CHEMICAL_NEIGHS 50
 #define BTAM_MIN_OCCUPANCY 5e-4
+
+/* relaxation schedules for btam_relax */
+#define BTAM_RELAX_FP64 0        /* every evaluation in FP64 */
+#define BTAM_RELAX_MIXED 1       /* FP32C until |R| < 1e-5, then FP64 */
+#define BTAM_RELAX_FP32C 2       /* FP32C only (stops at its ~1e-6 noise floor) */
 
 typedef struct btam_tables btam_tables;
 typedef struct btam_system btam_system;
@@ -107,6 +114,10 @@ void btam_system_destroy(btam_system *s);
  * Ghosts.cpp:861-892). */
 int btam_system_set_state(btam_system *s, const double *q, const double *sigma,
                           const double *x);
+/* Current state of the real sites (after relaxation or master-equation
+ * steps), into host arrays; any may be NULL.  Replaces reading the DMSwarm
+ * fields back with DMSwarmGetField. */
+int btam_system_get_state(btam_system *s, double *q, double *sigma, double *x);
 /* Sizes: real sites, periodic images, neighbour-list entries. */
 int btam_system_info(const btam_system *s, int *n_real, int *n_ghost, long long *n_pairs);
 /* The system's CUDA stream (cudaStream_t), for callers that time or order
@@ -158,6 +169,57 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);
+
+/* ---- consumers of the evaluation -----------------------------------------
+ * Relaxation of (q, sigma).  The reference configures a PETSc SNES
+ * (mechanical_relaxation_bulk, Mechanical-Relaxation-bulk.cpp:123-437; options
+ * at main-BT-AM.cpp:64-67) but solves only a 3-stretch bulk problem; this
+ * relaxes the q and sigma of every site with x >= x_min.  It minimises
+ *   F = sum_i beta_i V0_i - 3 sum_u log sigma_u   over (q, log sigma),
+ * whose gradient is beta_u (R_q(u), sigma_u R_sigma(u)), with sigma_min <=
+ * sigma <= sigma_max, by L-BFGS (m pairs, 1 <= m <= 16) on occupancy-scaled
+ * variables (sqrt(x) z) with an Armijo backtracking line search, on the
+ * device, until the projected residual norm sqrt(sum |R_q|^2 + R_sigma^2)
+ * over the relaxed sites (sigma components held at a bound excluded) is
+ * <= tol, or max_iter iterations.  mode: BTAM_RELAX_*.  Neighbour lists stay
+ * fixed, as in the reference.
+ * bounds (3, NULL = defaults): sigma_min (0.001 A, min_stdv_q of
+ * Macros.hpp:870), sigma_max (0.4 A: beyond ~0.43 A the 3-sigma quadrature
+ * points of the closest H-H pair, 1.30 A apart, pass through r = 0; the
+ * reference's max_stdv_q = 3.0 lets near-empty sites spread across their
+ * neighbours), x_min (0.01: sites below it are held fixed, since their
+ * energy scales with x and they barely resist moving).
+ * info (5, may be NULL): final residual norm, iterations, evaluations, final
+ * F, status (1 converged, 0 iteration limit, -1 no further decrease). */
+int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m,
+               const double *bounds, double *info);
+
+/* Hydrogen master equation (absent from the reference, which keeps only its
+ * parameters, Variables.hpp:68-92, and the diffusive graph builder
+ * list_of_diffusive_neighs, Neighbors.cpp:139-275).  Setup builds the H-H
+ * graph (pairs within 2.6 A, at most 50 per site) and carries every H
+ * occupancy as an integer number of 2^-50 quanta from then on.  A step:
+ * evaluates the residuals (precision), forms the chemical potential
+ *   mu_i = R_x(i) + [x_i<0.9999] gamma_i/beta_i     (x_i >= 5e-4)
+ *   mu_i = -(3/(2x) + 1/(1-x))/beta_i, x = max(x_i, 1e-12)   (emptier sites)
+ * of every H site that is diffusively active (x_i plus the x of its H
+ * neighbours within r_c >= 0.01, Topology.cpp:202-364) and moves, across
+ * every edge between active sites,
+ *   dt * Df/dr^2 * (beta_i+beta_j)/2 * xm(1-xm) * (mu_i - mu_j),  xm = (x_i+x_j)/2,
+ * rounded to quanta, skipped below min_dx, limited so that no site leaves
+ * [0, max(max_x, x)], from i to j.  Total hydrogen is conserved exactly.
+ * params (5, NULL = reference values): dt (4e-4), Df (0.045), dr (3.2),
+ * min_dx (1e-8), max_x (0.9).  total_quanta (2, may be NULL): 128-bit total
+ * of the quanta after the steps, as (high, low) 64-bit halves. */
+int btam_dmd_setup(btam_system *s);
+int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *params,
+                  long long *total_quanta);
+/* Current occupancies (n_real), their quanta and the last chemical
+ * potentials; any pointer may be NULL. */
+int btam_dmd_occupancy(btam_system *s, double *x, long long *quanta, double *mu);
+/* The diffusive graph as CSR over the real sites (images numbered after the
+ * real sites). */
+int btam_dmd_graph_copy(const btam_system *s, int *offs, int *idx, long long idx_cap);
 
 /* ---- evaluation without device allocation -------------------------------
  * No counterpart in the reference.  For callers that must not call

@@ -940,4 +940,54 @@ void orc_residuals(int n, const double *q, const double *sigma,
   });
 }
 
+// Hydrogen master-equation update (project definition; the reference keeps
+// only the parameters, Variables.hpp:68-92).  Sequential restatement of
+// btam_dmd_step's integer update.
+void orc_dmd_update(int n, const int *code_all, const int *owner, const double *x_all,
+                    const double *beta, const double *mu, const int *moffs,
+                    const int *midx, const int *doffs, const int *didx,
+                    const double *params, long long *X) {
+  const double q = 8.8817841970012523e-16, invq = 1125899906842624.0;
+  const double dt = params[0], Df = params[1], dr = params[2], min_dx = params[3],
+               max_x = params[4];
+  std::vector<int> active(n, 0);
+  std::vector<long long> deg(n, 0), X0(X, X + n);
+  // diffusive activity: x_i plus the occupancy of its H mechanical
+  // neighbours reaches 0.01 (list_of_active_diffusive_sites_MgHx,
+  // Topology.cpp:202-364)
+  for (int i = 0; i < n; ++i) {
+    if (code_all[i] != 1) continue;
+    double mass = (double)X0[i] * q;
+    for (int p = moffs[i]; p < moffs[i + 1]; ++p)
+      if (code_all[midx[p]] == 1) mass += x_all[midx[p]];
+    active[i] = mass >= 0.01;
+  }
+  for (int i = 0; i < n; ++i)
+    if (active[i])
+      for (int p = doffs[i]; p < doffs[i + 1]; ++p) deg[i] += active[owner[didx[p]]];
+  const long long xmax = llrint(max_x * invq);
+  for (int i = 0; i < n; ++i) {
+    if (!active[i]) continue;
+    for (int p = doffs[i]; p < doffs[i + 1]; ++p) {
+      int o = owner[didx[p]];
+      if (o <= i || !active[o]) continue;
+      double xi = (double)X0[i] * q, xo = (double)X0[o] * q;
+      double xm = 0.5 * (xi + xo), bm = 0.5 * (beta[i] + beta[o]);
+      double J = Df / (dr * dr) * bm * xm * (1.0 - xm) * (mu[i] - mu[o]);
+      double dlt = dt * J;
+      if (std::fabs(dlt) < min_dx) continue;
+      long long qn = llrint(dlt * invq);
+      long long di = deg[i] > 0 ? deg[i] : 1, dq = deg[o] > 0 ? deg[o] : 1;
+      long long out_i = X0[i] / di, out_o = X0[o] / dq;
+      long long in_i = xmax > X0[i] ? (xmax - X0[i]) / di : 0;
+      long long in_o = xmax > X0[o] ? (xmax - X0[o]) / dq : 0;
+      long long hi = out_i < in_o ? out_i : in_o;
+      long long lo = -(out_o < in_i ? out_o : in_i);
+      qn = qn > hi ? hi : (qn < lo ? lo : qn);
+      X[i] -= qn;
+      X[o] += qn;
+    }
+  }
+}
+
 }  // extern "C"

@@ -85,6 +85,18 @@ void orc_residuals(int n, const double *q, const double *sigma,
                    const int *u_list, int nu, double *Rq, double *Rs,
                    double *Rx);
 
+/* One hydrogen master-equation update (project definition, see
+ * include/btam.h btam_dmd_step) on real sites: X holds the occupancy quanta
+ * (2^-50) of the n real sites and is updated in place; mu the chemical
+ * potentials; x_all/code_all/owner the all-sites occupancy, species code
+ * (0 Mg, 1 H) and owner; moffs/midx the mechanical neighbours and
+ * doffs/didx the diffusive neighbours of the real sites; params as
+ * btam_dmd_step (dt, Df, dr, min_dx, max_x). */
+void orc_dmd_update(int n, const int *code_all, const int *owner, const double *x_all,
+                    const double *beta, const double *mu, const int *moffs,
+                    const int *midx, const int *doffs, const int *didx,
+                    const double *params, long long *X);
+
 #ifdef __cplusplus
 }
 #endif

@@ -247,3 +247,65 @@ def sampled_residuals(sys_, oracle, sites, rc=6.2934034034):
     V0 = oracle.V0(full, rho, offs, idx, sites)
     Rq, Rs, Rx = oracle.residuals(full, rho, owner, image, offs, idx, sites)
     return dict(rho=rho_real[sites], V0=V0, Rq=Rq, Rs=Rs, Rx=Rx)
+
+
+def diffusive_graph(q_all, species_all, n_real, rc=2.6, maxn=50):
+    """H-H pairs within rc for the real H sites, ascending index, with the
+    IEEE distance test sqrt((dx^2 + dy^2) + dz^2) <= rc of the neighbour rule
+    (list_of_diffusive_neighs, Neighbors.cpp:139-275); sites without H
+    neighbours get empty lists."""
+    q_all = np.asarray(q_all)
+    h = np.flatnonzero(np.asarray(species_all) == 1)
+    offs = np.zeros(n_real + 1, np.int32)
+    out = []
+    for i in range(n_real):
+        lst = []
+        if species_all[i] == 1:
+            d = q_all[i] - q_all[h]
+            r = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+            lst = [int(j) for j in h[(r <= rc) & (h != i)]]
+            if len(lst) > maxn:
+                raise RuntimeError("more than max_chemical_neighs diffusive neighbours")
+        out.extend(lst)
+        offs[i + 1] = len(out)
+    return offs, np.array(out, np.int32)
+
+
+def dmd_update(oracle, X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx, params):
+    """One master-equation update of the quanta X (copy returned)."""
+    X = np.ascontiguousarray(X, np.int64).copy()
+    n = len(X)
+    L = oracle.lib
+    f = L.orc_dmd_update
+    f.restype = None
+    code_all = np.ascontiguousarray(code_all, np.int32)
+    owner = np.ascontiguousarray(owner, np.int32)
+    x_all = np.ascontiguousarray(x_all, np.float64)
+    beta = np.ascontiguousarray(beta, np.float64)
+    mu = np.ascontiguousarray(mu, np.float64)
+    prm = np.ascontiguousarray(params, np.float64)
+    arrs = [np.ascontiguousarray(a, np.int32) for a in (moffs, midx, doffs, didx)]
+    f(n, _i(code_all), _i(owner), _d(x_all), _d(beta), _d(mu), *[_i(a) for a in arrs],
+      _d(prm), X.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
+    return X
+
+
+def residuals_on_topology(oracle, real, q_ghost, owner_ghost, image_ghost, offs_real, idx,
+                          sites):
+    """Literal residuals of `sites` on a given topology: the real-site state
+    `real`, the periodic images (positions, owners, shifts) and the
+    real-site neighbour lists of a device system, as they stand after a
+    relaxation that kept them fixed."""
+    n = len(real["x"])
+    owner = np.concatenate([np.arange(n), owner_ghost]).astype(np.int32)
+    image = np.concatenate([np.zeros((n, 3), np.int32), image_ghost]).astype(np.int32)
+    full = dict(real)
+    full["q"] = np.ascontiguousarray(np.concatenate([real["q"], q_ghost]))
+    for k in ("sigma", "x", "beta", "gamma"):
+        full[k] = np.ascontiguousarray(np.asarray(real[k])[owner])
+    full["species"] = np.ascontiguousarray(np.asarray(real["species"])[owner].astype(np.int32))
+    offs = np.concatenate([offs_real, np.full(len(owner) - n, offs_real[-1])]).astype(np.int32)
+    rho_real = oracle.mf_rho(full, offs, idx, np.arange(n, dtype=np.int32))
+    rho = rho_real[owner]
+    Rq, Rs, Rx = oracle.residuals(full, rho, owner, image, offs, idx, sites)
+    return dict(Rq=Rq, Rs=Rs, Rx=Rx)

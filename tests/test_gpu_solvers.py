@@ -1,0 +1,118 @@
+"""The consumers of the evaluation on the GPU: (q, sigma) relaxation and the
+hydrogen master equation, against their oracle definitions.
+
+Tolerances: relaxation to the requested residual norm, checked again with
+the literal oracle residuals of the relaxed state (<= 10 x tol); the
+master-equation update bit-exact in integer quanta given the same chemical
+potentials; total hydrogen conserved exactly (integer equality)."""
+import numpy as np
+import pytest
+
+import btam
+from btam import lattice
+
+pytestmark = pytest.mark.gpu
+
+
+def small_mgh(seed=5, h=0.3, xr=(0.0, 0.4)):
+    return lattice.supercell(4, 3, 3, ortho=True, h_fraction=h, x_range=xr,
+                             sigma_range=(0.08, 0.15), jitter=0.02, seed=seed)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_relaxation_reaches_tolerance(gpu_tables, oracle, mode):
+    """Well-occupied Mg-H cell: every site relaxes and the projected
+    residual reaches 1e-8; the literal oracle agrees the state is stationary."""
+    import pyoracle
+    s = small_mgh(xr=(0.3, 0.6))
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    info = S.relax(mode=mode, tol=1e-8, max_iter=600)
+    assert info["status"] == 1 and info["norm"] <= 1e-8, info
+    q, sigma, x = S.get_state()
+    assert np.all(sigma < 0.4)  # no bound active here, so the full residual vanishes
+    out = S.evaluate(btam.FP64)
+    assert np.sqrt(out["totals"][2]) <= 1e-8
+    # literal residuals on the same (fixed) images and neighbour lists
+    r = dict(s, q=q, sigma=sigma, x=x)
+    qg, og, ig = S.ghosts()
+    offs, idx = S.neighbors()
+    sites = np.array([0, 7, 40, 150, 200], np.int32)
+    lit = pyoracle.residuals_on_topology(oracle, r, qg, og, ig, offs, idx, sites)
+    assert np.abs(lit["Rq"]).max() <= 1e-7 and np.abs(lit["Rs"]).max() <= 1e-7
+
+
+def test_relaxation_dilute_hydrogen_config1(gpu_tables):
+    """Config 1 (x ~ U[0, 0.1]): sites below x_min stay fixed, sigma bounds
+    hold; the projected residual falls by orders of magnitude."""
+    s = lattice.config1()
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    r0 = np.sqrt(S.evaluate(btam.FP64)["totals"][2])
+    info = S.relax(mode=1, tol=1e-8, max_iter=800)
+    q, sigma, x = S.get_state()
+    assert np.all((sigma >= 0.001 - 1e-15) & (sigma <= 0.4 + 1e-12))
+    fixed = s["x"] < 0.01
+    assert np.array_equal(q[fixed], s["q"][fixed]) and np.array_equal(sigma[fixed],
+                                                                        s["sigma"][fixed])
+    assert info["norm"] < 1e-4 * r0, info
+
+
+def test_diffusive_graph_bit_exact(gpu_tables):
+    import pyoracle
+    s = small_mgh(h=0.6)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    S.dmd_setup()
+    offs, idx = S.dmd_graph()
+    qg, og, _ = S.ghosts()
+    n = len(s["x"])
+    q_all = np.concatenate([s["q"], qg])
+    sp_all = np.concatenate([s["species"], s["species"][og]])
+    o2, i2 = pyoracle.diffusive_graph(q_all, sp_all, n)
+    assert np.array_equal(offs, o2) and np.array_equal(idx, i2)
+
+
+def test_master_equation_matches_oracle_and_conserves(gpu_tables, oracle):
+    import pyoracle
+    s = small_mgh(h=0.6, xr=(0.0, 0.6))
+    n = len(s["x"])
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    S.dmd_setup()
+    x0, X0, _ = S.dmd_occupancy()
+    total0 = int(X0[s["species"] == 1].sum())
+    prm = dict(dt=1e-3, Df=0.045, dr=3.2, min_dx=1e-8, max_x=0.9)
+    for step in range(3):
+        xb, Xb, _ = S.dmd_occupancy()
+        total = S.dmd_step(1, btam.FP64, **prm)
+        assert total == total0  # exact conservation
+        x1, X1, mu = S.dmd_occupancy()
+        # the oracle's update from the same chemical potentials and state
+        qg, og, _ = S.ghosts()
+        owner = np.concatenate([np.arange(n), og]).astype(np.int32)
+        code_all = (s["species"][owner] == 1).astype(np.int32)
+        x_all = xb[owner]
+        moffs, midx = S.neighbors()
+        doffs, didx = S.dmd_graph()
+        Xo = pyoracle.dmd_update(oracle, Xb, code_all, owner, x_all, s["beta"], mu, moffs, midx,
+                                 doffs, didx, [prm[k] for k in ("dt", "Df", "dr", "min_dx",
+                                                                "max_x")])
+        assert np.array_equal(Xo, X1), step
+        assert np.any(X1 != Xb)
+
+
+def test_master_equation_long_run_conserves_and_bounds(gpu_tables):
+    s = small_mgh(h=0.8, xr=(0.0, 0.5), seed=9)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    S.dmd_setup()
+    _, X0, _ = S.dmd_occupancy()
+    total0 = int(X0[s["species"] == 1].sum())
+    total = S.dmd_step(200, btam.FP32C, dt=1e-3)
+    assert total == total0
+    x, X, mu = S.dmd_occupancy()
+    h = s["species"] == 1
+    assert np.all(X[h] >= 0) and np.all(x[h] <= 0.9 + 1e-12)
+    assert np.all(np.isfinite(mu))
+    assert np.array_equal(x[h], X[h] * 2.0 ** -50)
