@@ -186,6 +186,94 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def bench_batched(args, tables, flush, max_over_ranks, barrier):
+    """The batched workload: 128 hcp Mg-H spheres (radii log-uniform on
+    [8, 25] A, T ~ U[300, 600] K, H fraction ~ U[0, 0.5]).  One evaluation of
+    all 128 systems as one graph launch (persistent autotuned kernels,
+    FP32C), against the plain drop-in: 128 per-system evaluations, each on
+    its system's own stream so that they may overlap, in FP32C and FP64."""
+    import torch
+    import btam
+    from btam import lattice
+
+    dicts = lattice.config4()
+    systems = []
+    for d in dicts:
+        S = btam.System(tables, d)
+        S.build_neighbors()
+        systems.append(S)
+    B = btam.Batch(systems)
+    info = B.info()
+    shapes = B.autotune(btam.FP32C)
+    bstream = torch.cuda.ExternalStream(B.stream())
+
+    def graph_steps(k):
+        evs = []
+        for _ in range(k):
+            with torch.cuda.stream(bstream):
+                flush.add_(1.0)
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(bstream)
+                B.evaluate_async(btam.FP32C)
+                b.record(bstream)
+            evs.append((a, b))
+        B.sync()
+        return [a.elapsed_time(b) for a, b in evs]
+
+    def plain_steps(prec, k):
+        # device-bracketed host clock: the 128 evaluations run on 128 streams
+        ts = []
+        for _ in range(k):
+            flush.add_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for S in systems:
+                S.evaluate_async(prec)
+            for S in systems:
+                S.sync()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        return ts
+
+    graph_steps(args.warmup)
+    barrier()
+    g_ms = max_over_ranks(float(np.mean(graph_steps(args.steps))))
+    # wall clock of back-to-back graph launches (launch overhead included)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        B.evaluate_async(btam.FP32C)
+    B.sync()
+    g_wall = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    for S in systems:
+        S.autotune(btam.FP32C)
+        S.autotune(btam.FP64)
+    out = {}
+    for prec, name in ((btam.FP32C, "plain_fp32c"), (btam.FP64, "plain_fp64")):
+        plain_steps(prec, args.warmup)
+        barrier()
+        out[name] = max_over_ranks(float(np.mean(plain_steps(prec, args.steps))))
+    ns = info["n_sys"]
+    res = {"workload": "128 hcp Mg-H spheres, R log-uniform [8, 25] A, seed 4",
+           "systems": ns, "sites": info["n_real"], "directed_pairs": info["n_pairs"],
+           "unit": "system evals/s",
+           "graph_fp32c": {"ms_per_batch": g_ms, "value": ns * 1e3 / g_ms,
+                           "wall_ms_per_batch": g_wall, "kernel_variants": shapes,
+                           "launches_per_batch": 3},
+           "plain_fp32c_128_launches": {"ms_per_batch": out["plain_fp32c"],
+                                        "value": ns * 1e3 / out["plain_fp32c"],
+                                        "launches_per_batch": 3 * ns},
+           "plain_fp64_128_launches": {"ms_per_batch": out["plain_fp64"],
+                                       "value": ns * 1e3 / out["plain_fp64"],
+                                       "launches_per_batch": 3 * ns}}
+    res["graph_fp32c_over_plain_fp64"] = out["plain_fp64"] / g_ms
+    B.close()
+    for S in systems:
+        S.close()
+    return res
+
+
 def run_btam(args, ws, rank, local):
     import torch
     import btam
@@ -294,6 +382,8 @@ def run_btam(args, ws, rank, local):
     e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
     h2d = n * (24 + 8 + 8)
     d2h = n * (24 + 8 + 8) + 32
+    batched = None if args.no_batch else bench_batched(args, tables, flush, max_over_ranks,
+                                                        barrier)
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
@@ -318,7 +408,7 @@ def run_btam(args, ws, rank, local):
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
                 "gpu_launches": 3 * args.steps,
-                "clocks": clocks}
+                "clocks": clocks, "batched": batched}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -332,6 +422,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="btam", choices=["btam", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched workload")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":

@@ -30,7 +30,7 @@ STATUS = {
     5: "BTAM_ERR_BOX_TOO_SMALL", 6: "BTAM_ERR_NONFINITE", 7: "BTAM_ERR_OOM",
     8: "BTAM_ERR_CUDA", 9: "BTAM_ERR_GHOST_OVERFLOW", 10: "BTAM_ERR_OCCUPANCY",
     11: "BTAM_ERR_SPECIES", 12: "BTAM_ERR_TIMEOUT", 13: "BTAM_ERR_NOT_BUILT",
-    14: "BTAM_ERR_OUT_OF_BOX",
+    14: "BTAM_ERR_OUT_OF_BOX", 15: "BTAM_ERR_TOO_LARGE",
 }
 
 
@@ -77,6 +77,18 @@ _PROTOS = {
                                      ctypes.POINTER(ctypes.c_longlong)]),
     "btam_dmd_occupancy": (ctypes.c_int, [_V, _D, ctypes.POINTER(ctypes.c_longlong), _D]),
     "btam_dmd_graph_copy": (ctypes.c_int, [_V, _I, _I, ctypes.c_longlong]),
+    "btam_batch_create": (ctypes.c_int, [ctypes.POINTER(_V), ctypes.c_int, ctypes.POINTER(_V)]),
+    "btam_batch_destroy": (ctypes.c_int, [_V]),
+    "btam_batch_info": (ctypes.c_int, [_V, _I, _I, _I, ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_batch_stream": (_V, [_V]),
+    "btam_batch_set_state": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D]),
+    "btam_batch_autotune": (ctypes.c_int, [_V, ctypes.c_int, _I, _I]),
+    "btam_batch_set_variants": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "btam_set_variants": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    "btam_batch_eval_async": (ctypes.c_int, [_V, ctypes.c_int]),
+    "btam_batch_sync": (ctypes.c_int, [_V]),
+    "btam_batch_results_copy": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D]),
+    "btam_batch_totals_copy": (ctypes.c_int, [_V, _D]),
     "btam_mf_eval_noalloc": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _V, _V, _V, _V,
                                             _V, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
@@ -315,6 +327,11 @@ class System:
                "btam_autotune")
         return v1.value, v2.value
 
+    def set_variants(self, precision, v1, v2):
+        """Pins the launch variants (as returned by autotune)."""
+        _check(lib().btam_set_variants(self.handle, precision, int(v1), int(v2)),
+               "btam_set_variants")
+
     def profile(self, precision=FP64):
         """Per-kernel device times (ms) of one evaluation: pass 1, pass 2,
         totals."""
@@ -331,6 +348,83 @@ class System:
     def close(self):
         if getattr(self, "handle", None):
             lib().btam_system_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many built systems evaluated together: one CUDA graph launch (pass 1,
+    pass 2, per-system totals) per evaluation of all of them.  The systems
+    must stay alive while the batch is used."""
+
+    def __init__(self, systems):
+        self.systems = list(systems)
+        arr = (_V * len(self.systems))(*[s.handle for s in self.systems])
+        h = _V()
+        _check(lib().btam_batch_create(arr, len(self.systems), ctypes.byref(h)),
+               "btam_batch_create")
+        self.handle = h
+
+    def info(self):
+        ns, nr, na = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        npairs = ctypes.c_longlong()
+        _check(lib().btam_batch_info(self.handle, ctypes.byref(ns), ctypes.byref(nr),
+                                     ctypes.byref(na), ctypes.byref(npairs)), "btam_batch_info")
+        return dict(n_sys=ns.value, n_real=nr.value, n_all=na.value, n_pairs=npairs.value)
+
+    def stream(self):
+        return lib().btam_batch_stream(self.handle)
+
+    def set_state(self, k, q=None, sigma=None, x=None):
+        q = None if q is None else np.ascontiguousarray(q, np.float64)
+        sigma = None if sigma is None else np.ascontiguousarray(sigma, np.float64)
+        x = None if x is None else np.ascontiguousarray(x, np.float64)
+        _check(lib().btam_batch_set_state(self.handle, int(k), _d(q), _d(sigma), _d(x)),
+               "btam_batch_set_state")
+
+    def autotune(self, precision=FP32C):
+        v1, v2 = ctypes.c_int(), ctypes.c_int()
+        _check(lib().btam_batch_autotune(self.handle, precision, ctypes.byref(v1),
+                                         ctypes.byref(v2)), "btam_batch_autotune")
+        return v1.value, v2.value
+
+    def set_variants(self, precision, v1, v2):
+        _check(lib().btam_batch_set_variants(self.handle, precision, int(v1), int(v2)),
+               "btam_batch_set_variants")
+
+    def evaluate_async(self, precision=FP32C):
+        _check(lib().btam_batch_eval_async(self.handle, precision), "btam_batch_eval_async")
+
+    def sync(self):
+        _check(lib().btam_batch_sync(self.handle), "btam_batch_sync")
+
+    def evaluate(self, precision=FP32C):
+        """One evaluation of every system; returns the totals, shape (n_sys, 4)."""
+        self.evaluate_async(precision)
+        return self.totals()
+
+    def totals(self):
+        out = np.zeros((len(self.systems), 4))
+        _check(lib().btam_batch_totals_copy(self.handle, _d(out)), "btam_batch_totals_copy")
+        return out
+
+    def results(self, k, want=("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals")):
+        n = self.systems[k].n
+        shapes = dict(rho=(n,), V0=(n,), S0=(n,), Rq=(n, 3), Rs=(n,), Rx=(n,), totals=(4,))
+        out = {c: np.zeros(shapes[c]) for c in want}
+        args = [_d(out.get(c)) for c in ("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals")]
+        _check(lib().btam_batch_results_copy(self.handle, int(k), *args),
+               "btam_batch_results_copy")
+        return out
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().btam_batch_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -74,15 +74,16 @@ pass1_kernel(const EvalArgs<R> a) {
   __shared__ SiteSums ss[W];
   __shared__ double xbuf[W][30][10];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int i = blockIdx.x * W + warp;
-  if (i >= a.n_real) return;
+  // grid-stride over sites: one site per warp per trip (a full grid makes one
+  // trip; a persistent grid of a few blocks per SM makes several)
+  for (int i = blockIdx.x * W + warp; i < a.n_real; i += gridDim.x * W) {
   R *mom = a.mom + (size_t)i * kMomStride;
   const double2 xbi = a.xb[i];
   const double xi = xbi.x;
   if (xi < kMinOcc) {  // empty site: no energy, no moments
     for (int c = lane; c < kMomStride; c += 32) mom[c] = (R)0;
     if (lane == 0) a.rho[i] = a.V0[i] = a.S0[i] = a.selfx[i] = 0.0;
-    return;
+    continue;
   }
   const double4 qi = a.pos[i];
   const int ci = a.code[i];
@@ -176,6 +177,8 @@ pass1_kernel(const EvalArgs<R> a) {
     if (!(finite(res.V0) && finite(res.S0) && finite(res.selfx)))
       atomicOr(a.err, 1 << kErrBitNonFinite);
   }
+  __syncwarp();  // the warp's shared buffers are reused by its next site
+  }
 }
 
 template <class R, int W, int MB>
@@ -183,8 +186,7 @@ __global__ void __launch_bounds__(W * 32, MB)
 pass2_kernel(const EvalArgs<R> a) {
   __shared__ R mu_s[W][kMomStride];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int u = blockIdx.x * W + warp;
-  if (u >= a.n_real) return;
+  for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
   const double2 xbu = a.xb[u];
   const double xu = xbu.x;
   if (xu < kMinOcc) {
@@ -192,7 +194,7 @@ pass2_kernel(const EvalArgs<R> a) {
       a.Rq[3 * u] = a.Rq[3 * u + 1] = a.Rq[3 * u + 2] = 0.0;
       a.Rs[u] = a.Rx[u] = 0.0;
     }
-    return;
+    continue;
   }
   const R *mu_g = a.mom + (size_t)u * kMomStride;
   for (int c = lane; c < kMomStride; c += 32) mu_s[warp][c] = mu_g[c];
@@ -234,6 +236,34 @@ pass2_kernel(const EvalArgs<R> a) {
     if (!(finite(t[0]) && finite(t[1]) && finite(t[2]) && finite(gs) && finite(gx)))
       atomicOr(a.err, 1 << kErrBitNonFinite);
   }
+  __syncwarp();  // mu_s is reloaded for the warp's next site
+  }
+}
+
+// Per-system deterministic totals of a batch: one block per system whose
+// real sites are [seg[k], seg[k+1]); the same strides and tree as
+// totals_kernel, so out[4k..4k+3] equals that system's own totals bitwise.
+__global__ void __launch_bounds__(1024)
+seg_totals_kernel(const int *seg, const double *V0, const double *S0, const double *Rq,
+                  const double *Rs, const double *Rx, double *out) {
+  __shared__ double sh[4][1024];
+  const int k = blockIdx.x, lo = seg[k], hi = seg[k + 1];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+    v[0] += V0[i];
+    v[1] += S0[i];
+    v[2] += Rq[3 * i] * Rq[3 * i] + Rq[3 * i + 1] * Rq[3 * i + 1] +
+            Rq[3 * i + 2] * Rq[3 * i + 2] + Rs[i] * Rs[i];
+    v[3] += Rx[i] * Rx[i];
+  }
+  for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] = v[c];
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s)
+      for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x < 4) out[4 * k + threadIdx.x] = sh[threadIdx.x][0];
 }
 
 // Single-block deterministic reduction (fixed strides, fixed tree).
@@ -286,33 +316,49 @@ inline int nblocks(long long n, int per) { return (int)((n + per - 1) / per); }
 
 }  // namespace
 
-template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st) {
-  pass1_kernel<R, W, MB><<<nblocks(a.n_real, W), W * 32, 0, st>>>(a);
+// Grid of a launch: one warp per site, or (persistent, variant >= 8) as many
+// blocks as fit on the device at once, each warp looping over sites.
+template <class K> int grid_of(K kernel, int n, int W, bool persistent) {
+  int full = nblocks(n, W);
+  if (!persistent) return full;
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, W * 32, 0);
+  int g = sms * (per > 0 ? per : 1);
+  return g < full ? g : full;
 }
-template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st) {
-  pass2_kernel<R, W, MB><<<nblocks(a.n_real, W), W * 32, 0, st>>>(a);
+template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
+  auto k = pass1_kernel<R, W, MB>;
+  k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
+}
+template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
+  auto k = pass2_kernel<R, W, MB>;
+  k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
 }
 
 template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v) {
   if (a.n_real <= 0) return cudaSuccess;
-  switch (v) {
-  case 1: go1<R, 4, 3>(a, st); break;
-  case 2: go1<R, 4, 4>(a, st); break;
-  case 3: go1<R, 8, 2>(a, st); break;
-  case 4: go1<R, 2, 8>(a, st); break;
-  default: go1<R, 4, 1>(a, st); break;
+  const bool pers = (v & kPersistent) != 0;
+  switch (v & (kPersistent - 1)) {
+  case 1: go1<R, 4, 3>(a, st, pers); break;
+  case 2: go1<R, 4, 4>(a, st, pers); break;
+  case 3: go1<R, 8, 2>(a, st, pers); break;
+  case 4: go1<R, 2, 8>(a, st, pers); break;
+  default: go1<R, 4, 1>(a, st, pers); break;
   }
   return cudaGetLastError();
 }
 template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v) {
   if (a.n_real <= 0) return cudaSuccess;
-  switch (v) {
-  case 1: go2<R, 4, 3>(a, st); break;
-  case 2: go2<R, 4, 4>(a, st); break;
-  case 3: go2<R, 4, 5>(a, st); break;
-  case 4: go2<R, 8, 2>(a, st); break;
-  case 5: go2<R, 2, 8>(a, st); break;
-  default: go2<R, 4, 1>(a, st); break;
+  const bool pers = (v & kPersistent) != 0;
+  switch (v & (kPersistent - 1)) {
+  case 1: go2<R, 4, 3>(a, st, pers); break;
+  case 2: go2<R, 4, 4>(a, st, pers); break;
+  case 3: go2<R, 4, 5>(a, st, pers); break;
+  case 4: go2<R, 8, 2>(a, st, pers); break;
+  case 5: go2<R, 2, 8>(a, st, pers); break;
+  default: go2<R, 4, 1>(a, st, pers); break;
   }
   return cudaGetLastError();
 }
@@ -321,9 +367,69 @@ template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, 
 template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t, int);
 template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t, int);
 
+// Times every launch variant of pass 1 (block shapes, each with a full grid
+// and a persistent grid), then of pass 2 after the best pass 1 has written the
+// moments pass 2 reads; best of reps launches each.
+template <class R>
+cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int *best1,
+                            int *best2) {
+  cudaEvent_t e0, e1;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e != cudaSuccess) return e;
+  e = cudaEventCreate(&e1);
+  if (e != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return e;
+  }
+  auto time_one = [&](bool second, int v) -> float {
+    float best = 1e30f;
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+      e = cudaEventRecord(e0, st);
+      if (e == cudaSuccess) e = second ? launch_pass2(a, st, v) : launch_pass1(a, st, v);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, st);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) best = ms;
+    }
+    return best;
+  };
+  int b1 = 0, b2 = 0;
+  float t1 = 1e30f, t2 = 1e30f;
+  for (int p = 0; p < 2; ++p)
+    for (int v = 0; v < kPass1Variants && e == cudaSuccess; ++v) {
+      float t = time_one(false, v | (p ? kPersistent : 0));
+      if (t < t1) { t1 = t; b1 = v | (p ? kPersistent : 0); }
+    }
+  if (e == cudaSuccess) e = launch_pass1(a, st, b1);
+  for (int p = 0; p < 2; ++p)
+    for (int v = 0; v < kPass2Variants && e == cudaSuccess; ++v) {
+      float t = time_one(true, v | (p ? kPersistent : 0));
+      if (t < t2) { t2 = t; b2 = v | (p ? kPersistent : 0); }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (e == cudaSuccess) {
+    *best1 = b1;
+    *best2 = b2;
+  }
+  return e;
+}
+template cudaError_t autotune_passes<double>(const EvalArgs<double> &, cudaStream_t, int, int *,
+                                             int *);
+template cudaError_t autotune_passes<float>(const EvalArgs<float> &, cudaStream_t, int, int *,
+                                            int *);
+
 cudaError_t launch_totals(int n_real, const double *V0, const double *S0, const double *Rq,
                           const double *Rs, const double *Rx, double *out, cudaStream_t st) {
   totals_kernel<<<1, 1024, 0, st>>>(n_real, V0, S0, Rq, Rs, Rx, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_seg_totals(int n_sys, const int *seg, const double *V0, const double *S0,
+                              const double *Rq, const double *Rs, const double *Rx, double *out,
+                              cudaStream_t st) {
+  if (n_sys > 0) seg_totals_kernel<<<n_sys, 1024, 0, st>>>(seg, V0, S0, Rq, Rs, Rx, out);
   return cudaGetLastError();
 }
 

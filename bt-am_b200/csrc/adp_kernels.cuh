@@ -34,14 +34,34 @@ template <class R>
 cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
 template <class R>
 cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
-constexpr int kPass1Variants = 5;  // (4 warps,-), (4,3), (4,4), (8,2), (2,8)
-constexpr int kPass2Variants = 6;  // (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
+// variant = shape | kPersistent (persistent grid of resident blocks)
+constexpr int kPass1Variants = 5;  // shapes (4 warps,-), (4,3), (4,4), (8,2), (2,8)
+constexpr int kPass2Variants = 6;  // shapes (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
+constexpr int kPersistent = 8;
+inline bool valid_variants(int v1, int v2) {
+  return v1 >= 0 && v2 >= 0 && (v1 & ~(2 * kPersistent - 1)) == 0 &&
+         (v2 & ~(2 * kPersistent - 1)) == 0 && (v1 & (kPersistent - 1)) < kPass1Variants &&
+         (v2 & (kPersistent - 1)) < kPass2Variants;
+}
+
+// Times every pass-1 and pass-2 variant on this input (reps launches each,
+// synchronising st) and returns the fastest of each.  Every variant computes
+// bitwise identical results; only the launch shape differs.
+template <class R>
+cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int *best1,
+                            int *best2);
 
 // Deterministic FP64 totals over real sites: out[0] = sum V0, out[1] = sum S0,
 // out[2] = sum |R_q|^2 + R_sigma^2 (active sites), out[3] = sum R_x^2.
 cudaError_t launch_totals(int n_real, const double *V0, const double *S0,
                           const double *Rq, const double *Rs, const double *Rx,
                           double *out, cudaStream_t st);
+
+// Totals of each system of a batch: out[4k..4k+3] as launch_totals over the
+// real sites [seg[k], seg[k+1]), bitwise equal to that system's own totals.
+cudaError_t launch_seg_totals(int n_sys, const int *seg, const double *V0, const double *S0,
+                              const double *Rq, const double *Rs, const double *Rx,
+                              double *out, cudaStream_t st);
 
 // Non-mean-field density rho_i = sum_j x_j rho_{s_j}(|q_i - q_j|)
 // (density.cpp:44-104) for every real site.

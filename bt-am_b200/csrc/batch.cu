@@ -1,0 +1,421 @@
+// Batched evaluation: many independent systems (cells or clusters of uneven
+// size) evaluated by one persistent pass-1 launch, one persistent pass-2
+// launch and one per-system totals launch, replayed as a single CUDA graph.
+//
+// Layout in HBM: the real sites of every system first (system k owns rows
+// [R_k, R_k + n_k)), then the periodic images of every system (system k owns
+// rows [N + G_k, N + G_k + g_k), N = total real sites).  Neighbour indices,
+// owners and CSR offsets are renumbered into this layout once, on the device,
+// when the batch is made; the kernels of adp_kernels.cu then see one large
+// system whose sites happen to belong to different cells, which is exactly
+// what they already handle: a warp per site, each site reading only its own
+// neighbours, and per-site beta / gamma.  Because every per-site result is
+// computed by the same instructions in the same order as for the system on
+// its own, batch results equal the single-system results bitwise; the
+// per-system totals use the same reduction tree as a single system.
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "../../include/btam.h"
+#include "adp_kernels.cuh"
+#include "internal.cuh"
+
+namespace {
+
+// Renumbers system k's rows into the batch layout: rows below n_real go to
+// base_real + row, image rows to base_img + (row - n_real).
+__device__ __forceinline__ int batch_row(int j, int n_real, int base_real, int base_img) {
+  return j < n_real ? base_real + j : base_img + (j - n_real);
+}
+
+__global__ void remap_idx_kernel(long long n, const int *src, int *dst, int n_real,
+                                 int base_real, int base_img) {
+  long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) dst[p] = batch_row(src[p], n_real, base_real, base_img);
+}
+
+__global__ void remap_owner_kernel(int n_all, const int *src, int *dst_real, int *dst_img,
+                                   int n_real, int base_real) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_all) return;
+  int o = base_real + src[i];
+  if (i < n_real)
+    dst_real[i] = o;
+  else
+    dst_img[i - n_real] = o;
+}
+
+__global__ void shift_offs_kernel(int n, const int *src, int *dst, int base) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = base + src[i];
+}
+
+inline int blocks_of(long long n, int per) { return (int)((n + per - 1) / per); }
+
+}  // namespace
+
+struct btam_batch {
+  const btam_tables *T = nullptr;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev = nullptr;
+  std::vector<btam_system *> sys;
+  std::vector<int> base_real, base_img;  // per system
+  std::vector<long long> base_pair;
+  int n_sys = 0, n_real = 0, n_all = 0;
+  long long n_pairs = 0;
+  int *seg = nullptr;  // n_sys + 1 real-site offsets
+  double4 *pos = nullptr;
+  double2 *xb = nullptr;
+  int *code = nullptr, *owner = nullptr;
+  double *gamma = nullptr;
+  int *offs = nullptr, *idx = nullptr;
+  double *rho = nullptr, *V0 = nullptr, *S0 = nullptr, *selfx = nullptr, *Rq = nullptr,
+         *Rs = nullptr, *Rx = nullptr, *totals = nullptr;
+  double *mom64 = nullptr;
+  float *mom32 = nullptr;
+  int *err = nullptr;
+  // launch variants per arithmetic form (0 FP64, 1 FP32C); persistent grids
+  // unless btam_batch_autotune finds a full grid faster
+  int variant1[2] = {kPersistent, kPersistent}, variant2[2] = {kPersistent, kPersistent};
+  // instantiated graph per form and the variants it was captured with
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  int exec_v1[2] = {-1, -1}, exec_v2[2] = {-1, -1};
+};
+
+namespace {
+
+template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const TablesView<R> &T) {
+  EvalArgs<R> a;
+  a.n_real = b->n_real;
+  a.pos = b->pos;
+  a.xb = b->xb;
+  a.code = b->code;
+  a.owner = b->owner;
+  a.gamma = b->gamma;
+  a.offs = b->offs;
+  a.idx = b->idx;
+  a.T = T;
+  a.emb[0] = b->T->v64.t[T_F_MG];
+  a.emb[1] = b->T->v64.t[T_F_H];
+  a.mass[0] = b->T->host.mass_mg;
+  a.mass[1] = b->T->host.mass_h;
+  a.mom = mom;
+  a.rho = b->rho;
+  a.V0 = b->V0;
+  a.S0 = b->S0;
+  a.selfx = b->selfx;
+  a.Rq = b->Rq;
+  a.Rs = b->Rs;
+  a.Rx = b->Rx;
+  a.err = b->err;
+  return a;
+}
+
+int batch_read_err(btam_batch *b) {
+  int bits = 0;
+  cudaError_t e = cudaMemcpyAsync(&bits, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->err, 0, sizeof(int), b->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  return status_from_bits(bits);
+}
+
+// Copies system k's site rows (real and images) into the batch, ordered
+// after everything already enqueued on the system's stream.
+int copy_sites(btam_batch *b, int k) {
+  btam_system *s = b->sys[k];
+  BTAM_TRY(cudaEventRecord(b->ev, s->st));
+  BTAM_TRY(cudaStreamWaitEvent(b->st, b->ev, 0));
+  const int n = s->n_real, g = s->n_ghost;
+  BTAM_TRY(cudaMemcpyAsync(b->pos + b->base_real[k], s->pos, n * sizeof(double4),
+                           cudaMemcpyDeviceToDevice, b->st));
+  BTAM_TRY(cudaMemcpyAsync(b->xb + b->base_real[k], s->xb, n * sizeof(double2),
+                           cudaMemcpyDeviceToDevice, b->st));
+  if (g > 0) {
+    BTAM_TRY(cudaMemcpyAsync(b->pos + b->base_img[k], s->pos + n, g * sizeof(double4),
+                             cudaMemcpyDeviceToDevice, b->st));
+    BTAM_TRY(cudaMemcpyAsync(b->xb + b->base_img[k], s->xb + n, g * sizeof(double2),
+                             cudaMemcpyDeviceToDevice, b->st));
+  }
+  return BTAM_OK;
+}
+
+void free_batch(btam_batch *b) {
+  for (int f = 0; f < 2; ++f)
+    if (b->exec[f]) cudaGraphExecDestroy(b->exec[f]);
+  dfree(b->seg);
+  dfree(b->pos);
+  dfree(b->xb);
+  dfree(b->code);
+  dfree(b->owner);
+  dfree(b->gamma);
+  dfree(b->offs);
+  dfree(b->idx);
+  dfree(b->rho);
+  dfree(b->V0);
+  dfree(b->S0);
+  dfree(b->selfx);
+  dfree(b->Rq);
+  dfree(b->Rs);
+  dfree(b->Rx);
+  dfree(b->totals);
+  dfree(b->mom64);
+  dfree(b->mom32);
+  dfree(b->err);
+  if (b->ev) cudaEventDestroy(b->ev);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+}
+
+int batch_build(btam_batch *b) {
+  const int ns = b->n_sys;
+  // sizes and bases
+  std::vector<int> n_list_pairs(ns);
+  long long n_real = 0, n_img = 0, n_pairs = 0;
+  b->base_real.resize(ns);
+  b->base_img.resize(ns);
+  b->base_pair.resize(ns);
+  std::vector<int> seg(ns + 1);
+  for (int k = 0; k < ns; ++k) {
+    btam_system *s = b->sys[k];
+    int last = 0;  // real sites' pairs: offs[n_real] (the list may also cover images)
+    BTAM_TRY(cudaMemcpy(&last, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost));
+    n_list_pairs[k] = last;
+    if (n_real + n_img + s->n_real + s->n_ghost > 0x7fffffffLL || n_pairs + last > 0x7fffffffLL)
+      return BTAM_ERR_TOO_LARGE;
+    b->base_real[k] = (int)n_real;
+    b->base_pair[k] = n_pairs;
+    seg[k] = (int)n_real;
+    n_real += s->n_real;
+    n_img += s->n_ghost;
+    n_pairs += last;
+  }
+  seg[ns] = (int)n_real;
+  long long gacc = 0;
+  for (int k = 0; k < ns; ++k) {
+    b->base_img[k] = (int)(n_real + gacc);
+    gacc += b->sys[k]->n_ghost;
+  }
+  b->n_real = (int)n_real;
+  b->n_all = (int)(n_real + n_img);
+  b->n_pairs = n_pairs;
+  const size_t nr = n_real, na = b->n_all;
+  BTAM_TRY(dalloc(b->seg, ns + 1));
+  BTAM_TRY(dalloc(b->pos, na));
+  BTAM_TRY(dalloc(b->xb, na));
+  BTAM_TRY(dalloc(b->code, na));
+  BTAM_TRY(dalloc(b->owner, na));
+  BTAM_TRY(dalloc(b->gamma, nr));
+  BTAM_TRY(dalloc(b->offs, nr + 1));
+  BTAM_TRY(dalloc(b->idx, (size_t)n_pairs));
+  BTAM_TRY(dalloc(b->rho, nr));
+  BTAM_TRY(dalloc(b->V0, nr));
+  BTAM_TRY(dalloc(b->S0, nr));
+  BTAM_TRY(dalloc(b->selfx, nr));
+  BTAM_TRY(dalloc(b->Rq, 3 * nr));
+  BTAM_TRY(dalloc(b->Rs, nr));
+  BTAM_TRY(dalloc(b->Rx, nr));
+  BTAM_TRY(dalloc(b->totals, 4 * (size_t)ns));
+  BTAM_TRY(dalloc(b->err, 1));
+  BTAM_TRY(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
+  BTAM_TRY(cudaMemcpyAsync(b->seg, seg.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice,
+                           b->st));
+  for (int k = 0; k < ns; ++k) {
+    btam_system *s = b->sys[k];
+    const int n = s->n_real, g = s->n_ghost, R = b->base_real[k], G = b->base_img[k];
+    int st = copy_sites(b, k);
+    if (st != BTAM_OK) return st;
+    BTAM_TRY(cudaMemcpyAsync(b->code + R, s->code, n * sizeof(int), cudaMemcpyDeviceToDevice,
+                             b->st));
+    if (g > 0)
+      BTAM_TRY(cudaMemcpyAsync(b->code + G, s->code + n, g * sizeof(int),
+                               cudaMemcpyDeviceToDevice, b->st));
+    BTAM_TRY(cudaMemcpyAsync(b->gamma + R, s->gamma, n * sizeof(double),
+                             cudaMemcpyDeviceToDevice, b->st));
+    remap_owner_kernel<<<blocks_of(n + g, 256), 256, 0, b->st>>>(n + g, s->owner, b->owner + R,
+                                                                  b->owner + G, n, R);
+    shift_offs_kernel<<<blocks_of(n, 256), 256, 0, b->st>>>(n, s->offs, b->offs + R,
+                                                             (int)b->base_pair[k]);
+    if (n_list_pairs[k] > 0)
+      remap_idx_kernel<<<blocks_of(n_list_pairs[k], 256), 256, 0, b->st>>>(
+          n_list_pairs[k], s->idx, b->idx + b->base_pair[k], n, R, G);
+    BTAM_TRY(cudaGetLastError());
+  }
+  const int tail = (int)n_pairs;
+  BTAM_TRY(cudaMemcpyAsync(b->offs + b->n_real, &tail, sizeof(int), cudaMemcpyHostToDevice, b->st));
+  BTAM_TRY(cudaStreamSynchronize(b->st));
+  return BTAM_OK;
+}
+
+// Enqueues one evaluation of every system: pass 1, pass 2, per-system totals.
+template <class R> cudaError_t enqueue_eval(btam_batch *b, int form, R *mom, const TablesView<R> &T) {
+  EvalArgs<R> a = batch_args<R>(b, mom, T);
+  cudaError_t e = launch_pass1(a, b->st, b->variant1[form]);
+  if (e == cudaSuccess) e = launch_pass2(a, b->st, b->variant2[form]);
+  if (e == cudaSuccess)
+    e = launch_seg_totals(b->n_sys, b->seg, b->V0, b->S0, b->Rq, b->Rs, b->Rx, b->totals, b->st);
+  return e;
+}
+
+int ensure_moments(btam_batch *b, int precision) {
+  const size_t nm = (size_t)b->n_real * kMomStride;
+  if (precision == BTAM_FP64 && !b->mom64) BTAM_TRY(dalloc(b->mom64, nm));
+  if (precision == BTAM_FP32C && !b->mom32) BTAM_TRY(dalloc(b->mom32, nm));
+  return BTAM_OK;
+}
+
+// Captures the evaluation of one arithmetic form into a graph (again only
+// when the launch variants changed since the last capture).
+int ensure_graph(btam_batch *b, int precision) {
+  const int f = precision == BTAM_FP64 ? 0 : 1;
+  if (b->exec[f] && b->exec_v1[f] == b->variant1[f] && b->exec_v2[f] == b->variant2[f])
+    return BTAM_OK;
+  if (b->exec[f]) {
+    cudaGraphExecDestroy(b->exec[f]);
+    b->exec[f] = nullptr;
+  }
+  cudaGraph_t g = nullptr;
+  BTAM_TRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeRelaxed));
+  cudaError_t e = f == 0 ? enqueue_eval<double>(b, 0, b->mom64, b->T->v64)
+                         : enqueue_eval<float>(b, 1, b->mom32, b->T->v32);
+  cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec[f], g, 0);
+  if (g) cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    b->exec[f] = nullptr;
+    return cuda_status(e);
+  }
+  b->exec_v1[f] = b->variant1[f];
+  b->exec_v2[f] = b->variant2[f];
+  return BTAM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_batch_create(btam_system *const *systems, int n_sys, btam_batch **out) {
+  if (!out || !systems || n_sys <= 0) return BTAM_ERR_ARG;
+  *out = nullptr;
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess) return BTAM_ERR_CUDA;
+  const btam_tables *T = systems[0] ? systems[0]->T : nullptr;
+  for (int k = 0; k < n_sys; ++k) {
+    const btam_system *s = systems[k];
+    if (!s || s->T != T) return BTAM_ERR_ARG;
+    if (!s->built) return BTAM_ERR_NOT_BUILT;
+    if (s->device != cur) return BTAM_ERR_ARG;
+  }
+  btam_batch *b = new btam_batch;
+  b->T = T;
+  b->device = systems[0]->device;
+  b->n_sys = n_sys;
+  b->sys.assign(systems, systems + n_sys);
+  int st = cuda_status(cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking));
+  if (st == BTAM_OK) st = cuda_status(cudaEventCreateWithFlags(&b->ev, cudaEventDisableTiming));
+  if (st == BTAM_OK) st = batch_build(b);
+  if (st != BTAM_OK) {
+    free_batch(b);
+    return st;
+  }
+  *out = b;
+  return BTAM_OK;
+}
+
+int btam_batch_destroy(btam_batch *b) {
+  if (!b) return BTAM_ERR_ARG;
+  if (b->st) cudaStreamSynchronize(b->st);
+  free_batch(b);
+  return BTAM_OK;
+}
+
+int btam_batch_info(const btam_batch *b, int *n_sys, int *n_real, int *n_all,
+                    long long *n_pairs) {
+  if (!b) return BTAM_ERR_ARG;
+  if (n_sys) *n_sys = b->n_sys;
+  if (n_real) *n_real = b->n_real;
+  if (n_all) *n_all = b->n_all;
+  if (n_pairs) *n_pairs = b->n_pairs;
+  return BTAM_OK;
+}
+
+void *btam_batch_stream(const btam_batch *b) { return b ? (void *)b->st : nullptr; }
+
+int btam_batch_set_state(btam_batch *b, int k, const double *q, const double *sigma,
+                         const double *x) {
+  if (!b || k < 0 || k >= b->n_sys) return BTAM_ERR_ARG;
+  int st = btam_system_set_state(b->sys[k], q, sigma, x);
+  if (st != BTAM_OK) return st;
+  return copy_sites(b, k);
+}
+
+int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *pass2_variant) {
+  if (!b || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
+  int st = ensure_moments(b, precision);
+  if (st != BTAM_OK) return st;
+  const int f = precision == BTAM_FP64 ? 0 : 1;
+  int v1 = 0, v2 = 0;
+  cudaError_t e = f == 0 ? autotune_passes(batch_args<double>(b, b->mom64, b->T->v64), b->st, 3,
+                                           &v1, &v2)
+                         : autotune_passes(batch_args<float>(b, b->mom32, b->T->v32), b->st, 3,
+                                           &v1, &v2);
+  if (e != cudaSuccess) return cuda_status(e);
+  b->variant1[f] = v1;
+  b->variant2[f] = v2;
+  if (pass1_variant) *pass1_variant = v1;
+  if (pass2_variant) *pass2_variant = v2;
+  return batch_read_err(b);
+}
+
+int btam_batch_set_variants(btam_batch *b, int precision, int pass1_variant, int pass2_variant) {
+  if (!b || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
+  if (!valid_variants(pass1_variant, pass2_variant)) return BTAM_ERR_ARG;
+  const int f = precision == BTAM_FP64 ? 0 : 1;
+  b->variant1[f] = pass1_variant;
+  b->variant2[f] = pass2_variant;
+  return BTAM_OK;
+}
+
+int btam_batch_eval_async(btam_batch *b, int precision) {
+  if (!b || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
+  int st = ensure_moments(b, precision);
+  if (st == BTAM_OK) st = ensure_graph(b, precision);
+  if (st != BTAM_OK) return st;
+  return cuda_status(cudaGraphLaunch(b->exec[precision == BTAM_FP64 ? 0 : 1], b->st));
+}
+
+int btam_batch_sync(btam_batch *b) {
+  if (!b) return BTAM_ERR_ARG;
+  return batch_read_err(b);
+}
+
+int btam_batch_results_copy(btam_batch *b, int k, double *rho, double *V0, double *S0,
+                            double *Rq, double *Rs, double *Rx, double *totals) {
+  if (!b || k < 0 || k >= b->n_sys) return BTAM_ERR_ARG;
+  const int n = b->sys[k]->n_real;
+  const size_t o = b->base_real[k];
+  auto get = [&](double *dst, const double *src, size_t count) -> cudaError_t {
+    if (!dst || count == 0) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyDeviceToHost, b->st);
+  };
+  BTAM_TRY(get(rho, b->rho + o, n));
+  BTAM_TRY(get(V0, b->V0 + o, n));
+  BTAM_TRY(get(S0, b->S0 + o, n));
+  BTAM_TRY(get(Rq, b->Rq + 3 * o, 3 * (size_t)n));
+  BTAM_TRY(get(Rs, b->Rs + o, n));
+  BTAM_TRY(get(Rx, b->Rx + o, n));
+  BTAM_TRY(get(totals, b->totals + 4 * (size_t)k, 4));
+  return batch_read_err(b);
+}
+
+int btam_batch_totals_copy(btam_batch *b, double *totals) {
+  if (!b || !totals) return BTAM_ERR_ARG;
+  BTAM_TRY(cudaMemcpyAsync(totals, b->totals, 4 * (size_t)b->n_sys * sizeof(double),
+                           cudaMemcpyDeviceToHost, b->st));
+  return batch_read_err(b);
+}
+
+}  // extern "C"

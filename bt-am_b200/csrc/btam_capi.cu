@@ -19,46 +19,13 @@
 #include "solvers.cuh"
 #include "tables_io.hpp"
 #include "topo_kernels.cuh"
+#include "internal.cuh"
 
 using namespace btam;
 
 namespace {
 
 constexpr double kKB = 8.617332478E-5;  // k_B [eV/K] (Macros.hpp:849)
-
-int status_from_bits(int bits) {
-  if (bits & (1 << kErrBitOverflow)) return BTAM_ERR_NEIGHBOR_OVERFLOW;
-  if (bits & (1 << kErrBitEmpty)) return BTAM_ERR_NO_NEIGHBORS;
-  if (bits & (1 << kErrBitGhostOverflow)) return BTAM_ERR_GHOST_OVERFLOW;
-  if (bits & (1 << kErrBitCells)) return BTAM_ERR_OOM;
-  if (bits & (1 << kErrBitNonFinite)) return BTAM_ERR_NONFINITE;
-  if (bits & (1 << kErrBitTimeout)) return BTAM_ERR_TIMEOUT;
-  return BTAM_OK;
-}
-
-int cuda_status(cudaError_t e) {
-  if (e == cudaSuccess) return BTAM_OK;
-  if (e == cudaErrorMemoryAllocation) return BTAM_ERR_OOM;
-  return BTAM_ERR_CUDA;
-}
-
-#define BTAM_TRY(expr)                         \
-  do {                                         \
-    cudaError_t _e = (expr);                   \
-    if (_e != cudaSuccess) return cuda_status(_e); \
-  } while (0)
-
-template <class T> cudaError_t dalloc(T *&p, size_t count) {
-  if (p) cudaFree(p);
-  p = nullptr;
-  if (count == 0) count = 1;
-  return cudaMalloc((void **)&p, count * sizeof(T));
-}
-
-template <class T> void dfree(T *&p) {
-  if (p) cudaFree(p);
-  p = nullptr;
-}
 
 // Packs row-major q, sigma and x of real sites into the device layout.
 __global__ void pack_state_kernel(int n, const double *q, const double *sigma,
@@ -104,66 +71,6 @@ __global__ void spline_eval_kernel(SplineView<double> s, int n, const double *r,
 }
 
 }  // namespace
-
-struct btam_tables {
-  HostTables host;
-  int device = 0;
-  Coef4<double> *d64 = nullptr;
-  Coef4<float> *d32 = nullptr;
-  TablesView<double> v64;
-  TablesView<float> v32;
-};
-
-struct btam_system {
-  const btam_tables *T = nullptr;
-  int device = 0;
-  cudaStream_t st = nullptr;
-  int n_real = 0, n_ghost = 0, cap_all = 0;
-  GhostBox box;
-  bool any_periodic = false;
-  // site arrays (real then images)
-  double4 *pos = nullptr;
-  double2 *xb = nullptr;
-  int *code = nullptr, *owner = nullptr;
-  char4 *image = nullptr;
-  double *gamma = nullptr;
-  // staging for host updates
-  double *stage = nullptr;  // 5 n_real doubles: q (3n), sigma, x
-  // neighbour lists
-  bool built = false;
-  int n_list = 0;
-  long long n_pairs = 0, idx_cap = 0;
-  int *offs = nullptr, *idx = nullptr, *cnt = nullptr, *tmp = nullptr;
-  long long tmp_cap = 0;
-  int q_cap = 0;
-  // cells
-  int cell_cap = 0, site_cap = 0;
-  unsigned long long *bbox = nullptr;
-  CellGrid *grid = nullptr;
-  int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cursor = nullptr,
-      *cell_sites = nullptr;
-  // results
-  double *rho = nullptr, *V0 = nullptr, *S0 = nullptr, *selfx = nullptr, *Rq = nullptr,
-         *Rs = nullptr, *Rx = nullptr, *totals = nullptr;
-  double *mom64 = nullptr;
-  float *mom32 = nullptr;
-  int *err = nullptr;
-  DeviceScratch scratch;
-  // kernel block shapes per arithmetic form (index 0 FP64, 1 FP32C), chosen
-  // by btam_autotune
-  int variant1[2] = {0, 0}, variant2[2] = {0, 0};
-  int cnt_cap = 0;
-  // diffusive graph and master-equation state
-  bool dmd_ready = false;
-  int *doffs = nullptr, *didx = nullptr, dq_cap = 0;
-  long long didx_cap = 0, d_pairs = 0;
-  long long *X = nullptr, *X0 = nullptr, *dtot = nullptr;
-  double *mu = nullptr;
-  int *dact = nullptr, *ddeg = nullptr;
-  // relaxation work vectors
-  int relax_m = 0;
-  double *rv = nullptr;  // one block holding every relaxation vector
-};
 
 static int build_list(btam_system *s, int n_all, int n_query, double rc, int maxn, int filter,
                       int allow_empty, int *&offs, int &q_cap, int *&idx, long long &idx_cap,
@@ -274,17 +181,6 @@ int ensure_sites(btam_system *s, int n_all) {
   return BTAM_OK;
 }
 
-// Waits for the stream, returns the error bits raised since the last read
-// (as a status) and clears them.
-int read_err(btam_system *s) {
-  int bits = 0;
-  cudaError_t e = cudaMemcpyAsync(&bits, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->st);
-  if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-  if (e != cudaSuccess) return cuda_status(e);
-  return status_from_bits(bits);
-}
-
 template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesView<R> &T) {
   EvalArgs<R> a;
   a.n_real = s->n_real;
@@ -342,7 +238,7 @@ const char *btam_status_string(int st) {
   case BTAM_ERR_TIMEOUT: return "bounded device wait gave up";
   case BTAM_ERR_NOT_BUILT: return "neighbour lists not built";
   case BTAM_ERR_OUT_OF_BOX: return "site outside the periodic cell";
-  case BTAM_ERR_TOO_LARGE: return "more sites than the static scratch of btam_mf_eval_noalloc holds";
+  case BTAM_ERR_TOO_LARGE: return "more sites or pairs than the entry point holds";
   }
   return "unknown status";
 }
@@ -724,41 +620,12 @@ int btam_mf_eval_async(btam_system *s, int precision) {
 
 }  // extern "C"
 
-// Times every block shape of pass 1, then of pass 2 (after the best pass 1
-// has produced the moments pass 2 reads), reps times each, and keeps the
-// shape with the smallest time for this system and arithmetic form.
+// Keeps the fastest pass-1 and pass-2 launch variants for this system and
+// arithmetic form (timed by autotune_passes).
 template <class R>
 static int autotune_form(btam_system *s, EvalArgs<R> a, int form, int reps) {
-  cudaEvent_t e0, e1;
-  BTAM_TRY(cudaEventCreate(&e0));
-  BTAM_TRY(cudaEventCreate(&e1));
-  cudaError_t e = cudaSuccess;
-  auto time_one = [&](bool second, int v) -> float {
-    float best = 1e30f;
-    for (int r = 0; r < reps && e == cudaSuccess; ++r) {
-      e = cudaEventRecord(e0, s->st);
-      if (e == cudaSuccess) e = second ? launch_pass2(a, s->st, v) : launch_pass1(a, s->st, v);
-      if (e == cudaSuccess) e = cudaEventRecord(e1, s->st);
-      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
-      float ms = 0.f;
-      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best) best = ms;
-    }
-    return best;
-  };
   int b1 = 0, b2 = 0;
-  float t1 = 1e30f, t2 = 1e30f;
-  for (int v = 0; v < kPass1Variants && e == cudaSuccess; ++v) {
-    float t = time_one(false, v);
-    if (t < t1) { t1 = t; b1 = v; }
-  }
-  if (e == cudaSuccess) e = launch_pass1(a, s->st, b1);
-  for (int v = 0; v < kPass2Variants && e == cudaSuccess; ++v) {
-    float t = time_one(true, v);
-    if (t < t2) { t2 = t; b2 = v; }
-  }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaError_t e = autotune_passes(a, s->st, reps, &b1, &b2);
   if (e != cudaSuccess) return cuda_status(e);
   s->variant1[form] = b1;
   s->variant2[form] = b2;
@@ -785,6 +652,15 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
   const int f = precision == BTAM_FP64 ? 0 : 1;
   if (pass1_variant) *pass1_variant = s->variant1[f];
   if (pass2_variant) *pass2_variant = s->variant2[f];
+  return BTAM_OK;
+}
+
+int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass2_variant) {
+  if (!s || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
+  if (!valid_variants(pass1_variant, pass2_variant)) return BTAM_ERR_ARG;
+  const int f = precision == BTAM_FP64 ? 0 : 1;
+  s->variant1[f] = pass1_variant;
+  s->variant2[f] = pass2_variant;
   return BTAM_OK;
 }
 

@@ -1,0 +1,121 @@
+// Internal layout of the library's opaque handles (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "../../include/btam.h"
+
+#include "adp_core.cuh"
+#include "tables_io.hpp"
+#include "topo_kernels.cuh"
+
+using namespace btam;
+
+struct btam_tables {
+  HostTables host;
+  int device = 0;
+  Coef4<double> *d64 = nullptr;
+  Coef4<float> *d32 = nullptr;
+  TablesView<double> v64;
+  TablesView<float> v32;
+};
+
+struct btam_system {
+  const btam_tables *T = nullptr;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int n_real = 0, n_ghost = 0, cap_all = 0;
+  GhostBox box;
+  bool any_periodic = false;
+  // site arrays (real then images)
+  double4 *pos = nullptr;
+  double2 *xb = nullptr;
+  int *code = nullptr, *owner = nullptr;
+  char4 *image = nullptr;
+  double *gamma = nullptr;
+  // staging for host updates
+  double *stage = nullptr;  // 5 n_real doubles: q (3n), sigma, x
+  // neighbour lists
+  bool built = false;
+  int n_list = 0;
+  long long n_pairs = 0, idx_cap = 0;
+  int *offs = nullptr, *idx = nullptr, *cnt = nullptr, *tmp = nullptr;
+  long long tmp_cap = 0;
+  int q_cap = 0;
+  // cells
+  int cell_cap = 0, site_cap = 0;
+  unsigned long long *bbox = nullptr;
+  CellGrid *grid = nullptr;
+  int *cell_of = nullptr, *cell_cnt = nullptr, *cell_start = nullptr, *cursor = nullptr,
+      *cell_sites = nullptr;
+  // results
+  double *rho = nullptr, *V0 = nullptr, *S0 = nullptr, *selfx = nullptr, *Rq = nullptr,
+         *Rs = nullptr, *Rx = nullptr, *totals = nullptr;
+  double *mom64 = nullptr;
+  float *mom32 = nullptr;
+  int *err = nullptr;
+  DeviceScratch scratch;
+  // kernel block shapes per arithmetic form (index 0 FP64, 1 FP32C), chosen
+  // by btam_autotune
+  int variant1[2] = {0, 0}, variant2[2] = {0, 0};
+  int cnt_cap = 0;
+  // diffusive graph and master-equation state
+  bool dmd_ready = false;
+  int *doffs = nullptr, *didx = nullptr, dq_cap = 0;
+  long long didx_cap = 0, d_pairs = 0;
+  long long *X = nullptr, *X0 = nullptr, *dtot = nullptr;
+  double *mu = nullptr;
+  int *dact = nullptr, *ddeg = nullptr;
+  // relaxation work vectors
+  int relax_m = 0;
+  double *rv = nullptr;  // one block holding every relaxation vector
+};
+
+
+// ---- host helpers shared by the library sources
+
+inline int status_from_bits(int bits) {
+  if (bits & (1 << kErrBitOverflow)) return BTAM_ERR_NEIGHBOR_OVERFLOW;
+  if (bits & (1 << kErrBitEmpty)) return BTAM_ERR_NO_NEIGHBORS;
+  if (bits & (1 << kErrBitGhostOverflow)) return BTAM_ERR_GHOST_OVERFLOW;
+  if (bits & (1 << kErrBitCells)) return BTAM_ERR_OOM;
+  if (bits & (1 << kErrBitNonFinite)) return BTAM_ERR_NONFINITE;
+  if (bits & (1 << kErrBitTimeout)) return BTAM_ERR_TIMEOUT;
+  return BTAM_OK;
+}
+
+inline int cuda_status(cudaError_t e) {
+  if (e == cudaSuccess) return BTAM_OK;
+  if (e == cudaErrorMemoryAllocation) return BTAM_ERR_OOM;
+  return BTAM_ERR_CUDA;
+}
+
+#define BTAM_TRY(expr)                         \
+  do {                                         \
+    cudaError_t _e = (expr);                   \
+    if (_e != cudaSuccess) return cuda_status(_e); \
+  } while (0)
+
+template <class T> inline cudaError_t dalloc(T *&p, size_t count) {
+  if (p) cudaFree(p);
+  p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)&p, count * sizeof(T));
+}
+
+template <class T> inline void dfree(T *&p) {
+  if (p) cudaFree(p);
+  p = nullptr;
+}
+
+// Waits for the stream, returns the error bits raised since the last read
+// (as a status) and clears them.
+inline int read_err(btam_system *s) {
+  int bits = 0;
+  cudaError_t e = cudaMemcpyAsync(&bits, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  return status_from_bits(bits);
+}
+

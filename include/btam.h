@@ -40,7 +40,8 @@ extern "C" {
 #define BTAM_ERR_TIMEOUT 12          /* a bounded device wait gave up */
 #define BTAM_ERR_NOT_BUILT 13        /* neighbour lists not built yet */
 #define BTAM_ERR_OUT_OF_BOX 14       /* site outside the cell along a periodic axis */
-#define BTAM_ERR_TOO_LARGE 15        /* more sites than btam_mf_eval_noalloc's static scratch holds */
+#define BTAM_ERR_TOO_LARGE 15        /* more sites than btam_mf_eval_noalloc's static scratch holds,
+                                        or a batch beyond 32-bit site / pair indices */
 
 /* arithmetic forms */
 #define BTAM_FP64 0   /* plain FP64 drop-in */
@@ -75,6 +76,7 @@ extern "C" {
 
 typedef struct btam_tables btam_tables;
 typedef struct btam_system btam_system;
+typedef struct btam_batch btam_batch;
 
 const char *btam_status_string(int status);
 int btam_version(void);
@@ -161,10 +163,17 @@ int btam_results_copy(btam_system *s, double *rho, double *V0, double *S0,
 /* Waits for the system's stream and returns the first error it raised. */
 int btam_system_sync(btam_system *s);
 /* Autotuner (no counterpart in the reference): times every compiled block
- * shape / register cap of the two kernels on this system and keeps the
- * fastest for later evaluations in `precision`; reports the chosen indices.
- * Results are identical for every shape (same arithmetic, same order). */
+ * shape / register cap of the two kernels, each with a full grid and with a
+ * persistent grid of resident blocks, on this system and keeps the fastest
+ * for later evaluations in `precision`; reports the chosen variant ids
+ * (shape index, plus 8 for the persistent grid).  A given variant is bitwise
+ * reproducible; the grid (full or persistent) never changes a bit, while
+ * two block shapes are separate compilations and may round differently in
+ * the last bits (within the stated tolerance of the form). */
 int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_variant);
+/* Pins the launch variants of `precision` (as reported by btam_autotune),
+ * for runs that must reproduce one another bit for bit. */
+int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass2_variant);
 
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
@@ -244,6 +253,42 @@ int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_real,
                          const int *owner, const double *gamma, const int *offs,
                          const int *idx, double *V0, double *Rq, double *Rs,
                          double *Rx, double *totals, void *stream);
+
+/* ---- batched evaluation (no counterpart in the reference, which evaluates
+ * one DMSwarm per process) -----------------------------------------------
+ * A batch gathers many built systems (same tables, same device) into one
+ * device layout: every system's real sites, then every system's images,
+ * neighbour lists renumbered accordingly.  One evaluation of all systems is
+ * a single CUDA graph (pass 1, pass 2, per-system totals) on the batch's own
+ * stream, with persistent grids of resident blocks by default.  Each
+ * system's results equal those of btam_mf_eval on the system alone, bitwise,
+ * when both use the same block shapes (btam_set_variants /
+ * btam_batch_set_variants).
+ * The systems must outlive the batch; the batch keeps its own copy of their
+ * state, refreshed by btam_batch_set_state. */
+int btam_batch_create(btam_system *const *systems, int n_sys, btam_batch **out);
+int btam_batch_destroy(btam_batch *b);
+int btam_batch_info(const btam_batch *b, int *n_sys, int *n_real, int *n_all,
+                    long long *n_pairs);
+void *btam_batch_stream(const btam_batch *b);
+/* New (q, sigma, x) of system k (NULL keeps a field), as
+ * btam_system_set_state on that system, then copied into the batch. */
+int btam_batch_set_state(btam_batch *b, int k, const double *q, const double *sigma,
+                         const double *x);
+/* Times every pass-1 / pass-2 launch variant (block shape; full or
+ * persistent grid) on the whole batch and keeps the fastest. */
+int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *pass2_variant);
+int btam_batch_set_variants(btam_batch *b, int precision, int pass1_variant, int pass2_variant);
+/* Enqueues one evaluation of every system (one graph launch); does not
+ * synchronise.  btam_batch_sync waits and returns the first error raised. */
+int btam_batch_eval_async(btam_batch *b, int precision);
+int btam_batch_sync(btam_batch *b);
+/* Results of system k as btam_results_copy (NULL skips a field; totals[4]);
+ * synchronises the batch's stream. */
+int btam_batch_results_copy(btam_batch *b, int k, double *rho, double *V0, double *S0,
+                            double *Rq, double *Rs, double *Rx, double *totals);
+/* totals[4 k + c] of every system k; synchronises. */
+int btam_batch_totals_copy(btam_batch *b, double *totals);
 
 /* ---- measurement (no counterpart in the reference, which has only PETSc's
  * SNES monitor for tracing) ------------------------------------------------ */

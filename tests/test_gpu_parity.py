@@ -108,19 +108,37 @@ def test_deterministic_and_state_update(gpu_tables, hostmodel, oracle):
         assert rel(out[k], ref[k]) < 1e-11, k
 
 
-def test_autotuned_shapes_give_identical_results(gpu_tables):
-    """Every kernel block shape runs the same arithmetic in the same order, so
-    the autotuner's choice never changes a result bit."""
+def test_launch_variants(gpu_tables):
+    """Every launch variant (block shape x full or persistent grid) runs the
+    same per-site arithmetic in the same order: the grid never changes a bit;
+    block shapes are separate compilations whose multiply-add contraction may
+    differ, so they agree to rounding (FP64 1e-12 relative, FP32C within its
+    stated tolerance); a pinned variant reproduces itself bitwise."""
     g = load("config1")
     S = btam.System(gpu_tables, system_of(g))
     S.build_neighbors()
-    for prec in (btam.FP64, btam.FP32C):
-        before = S.evaluate(prec)
+    for prec, tol in ((btam.FP64, 1e-12), (btam.FP32C, 1e-6)):
+        base = S.evaluate(prec)
+        for shape1, shape2 in [(v, v) for v in range(5)] + [(0, 5)]:
+            for pers in (0, 8):
+                S.set_variants(prec, shape1 | pers, shape2 | pers)
+                out = S.evaluate(prec)
+                again = S.evaluate(prec)
+                for k in out:
+                    assert np.array_equal(out[k], again[k]), (prec, shape1, k)
+                if pers:
+                    for k in out:
+                        assert np.array_equal(out[k], full[k]), (prec, shape1, "grid", k)
+                else:
+                    full = out
+                for k in ("V0", "S0"):
+                    assert rel(out[k], base[k]) < tol, (prec, shape1, k)
+                for k in ("Rq", "Rs", "Rx"):
+                    assert np.abs(out[k] - base[k]).max() < 10 * tol, (prec, shape1, k)
         v1, v2 = S.autotune(prec)
-        assert 0 <= v1 < 5 and 0 <= v2 < 6
-        after = S.evaluate(prec)
-        for k in before:
-            assert np.array_equal(before[k], after[k]), (prec, k)
+        assert (v1 & 7) < 5 and (v2 & 7) < 6 and v1 < 16 and v2 < 16
+    with pytest.raises(btam.BtamError):
+        S.set_variants(btam.FP64, 5, 0)
 
 
 def test_error_codes(gpu_tables):
