@@ -89,9 +89,40 @@ _PROTOS = {
     "btam_batch_sync": (ctypes.c_int, [_V]),
     "btam_batch_results_copy": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D]),
     "btam_batch_totals_copy": (ctypes.c_int, [_V, _D]),
+    "btam_estimate_bytes": (ctypes.c_longlong, [ctypes.c_int, _D, _I]),
+    "btam_server_create": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_longlong,
+                                          ctypes.POINTER(_V)]),
+    "btam_server_submit": (ctypes.c_int, [_V, _V, ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_server_wait": (ctypes.c_int, [_V, ctypes.c_longlong, ctypes.c_double, _V, _D, _D, _D]),
+    "btam_server_stats": (ctypes.c_int, [_V, ctypes.POINTER(ctypes.c_longlong), _I,
+                                         ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_server_destroy": (ctypes.c_int, [_V]),
     "btam_mf_eval_noalloc": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _V, _V, _V, _V,
                                             _V, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
+
+
+
+class JobSpec(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("precision", ctypes.c_int), ("mode", ctypes.c_int),
+                ("n", ctypes.c_int), ("q", _D), ("sigma", _D), ("x", _D), ("species", _I),
+                ("beta", _D), ("gamma", _D), ("origin", _D), ("cell", _D), ("periodic", _I),
+                ("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("lbfgs_m", ctypes.c_int),
+                ("sigma_min", ctypes.c_double), ("sigma_max", ctypes.c_double),
+                ("x_min", ctypes.c_double), ("nsteps", ctypes.c_int),
+                ("dmd_params", ctypes.c_double * 5)]
+
+
+class JobResult(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("kind", ctypes.c_int), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_start", ctypes.c_double),
+                ("t_end", ctypes.c_double), ("norm", ctypes.c_double),
+                ("objective", ctypes.c_double), ("iterations", ctypes.c_int),
+                ("evaluations", ctypes.c_int), ("converged", ctypes.c_int),
+                ("h_quanta_hi", ctypes.c_longlong), ("h_quanta_lo", ctypes.c_longlong)]
+
 
 _lib = None
 
@@ -425,6 +456,93 @@ class Batch:
     def close(self):
         if getattr(self, "handle", None):
             lib().btam_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+JOB_RELAX, JOB_DMD, JOB_EVAL = 0, 1, 2
+RELAX_FP64, RELAX_MIXED, RELAX_FP32C = 0, 1, 2
+
+
+def estimate_bytes(sysdict):
+    n = len(sysdict["x"])
+    cell = np.ascontiguousarray(sysdict["cell"], np.float64).reshape(9)
+    per = np.ascontiguousarray(sysdict["periodic"], np.int32)
+    return int(lib().btam_estimate_bytes(n, _d(cell), _i(per)))
+
+
+class Server:
+    """Concurrent job server on the current device (btam_server_*)."""
+
+    def __init__(self, tables, workers=8, budget_bytes=0):
+        self.tables = tables
+        h = _V()
+        _check(lib().btam_server_create(tables.handle, int(workers), int(budget_bytes),
+                                        ctypes.byref(h)), "btam_server_create")
+        self.handle = h
+        self.sizes = {}
+
+    def submit(self, sysdict, kind, precision=FP32C, mode=RELAX_FP32C, tol=1e-5, max_iter=300,
+               nsteps=100, dmd=(1e-3, 0.045, 3.2, 1e-8, 0.9)):
+        s = sysdict
+        arrs = dict(q=np.ascontiguousarray(s["q"], np.float64),
+                    sigma=np.ascontiguousarray(s["sigma"], np.float64),
+                    x=np.ascontiguousarray(s["x"], np.float64),
+                    species=np.ascontiguousarray(s["species"], np.int32),
+                    origin=np.ascontiguousarray(s["origin"], np.float64),
+                    cell=np.ascontiguousarray(s["cell"], np.float64).reshape(9),
+                    periodic=np.ascontiguousarray(s["periodic"], np.int32))
+        for k in ("beta", "gamma"):
+            if s.get(k) is not None:
+                arrs[k] = np.ascontiguousarray(s[k], np.float64)
+        sp = JobSpec()
+        sp.kind, sp.precision, sp.mode, sp.n = int(kind), int(precision), int(mode), len(arrs["x"])
+        for k in ("q", "sigma", "x", "origin", "cell", "beta", "gamma"):
+            if k in arrs:
+                setattr(sp, k, _d(arrs[k]))
+        sp.species = _i(arrs["species"])
+        sp.periodic = _i(arrs["periodic"])
+        sp.tol, sp.max_iter, sp.nsteps = float(tol), int(max_iter), int(nsteps)
+        for c in range(5):
+            sp.dmd_params[c] = float(dmd[c])
+        jid = ctypes.c_longlong()
+        _check(lib().btam_server_submit(self.handle, ctypes.byref(sp), ctypes.byref(jid)),
+               "btam_server_submit")
+        self.sizes[jid.value] = sp.n
+        return jid.value
+
+    def wait(self, job_id, timeout=-1.0):
+        """Result dict of a job (its final state included); raises on a job
+        error."""
+        n = self.sizes.pop(job_id)
+        res = JobResult()
+        q = np.zeros((n, 3))
+        sigma = np.zeros(n)
+        x = np.zeros(n)
+        _check(lib().btam_server_wait(self.handle, job_id, float(timeout), ctypes.byref(res),
+                                      _d(q), _d(sigma), _d(x)), "btam_server_wait")
+        out = {f: getattr(res, f) for f, _ in JobResult._fields_}
+        out["h_quanta"] = (res.h_quanta_hi << 64) + (res.h_quanta_lo & 0xFFFFFFFFFFFFFFFF)
+        out.update(q=q, sigma=sigma, x=x)
+        return out
+
+    def stats(self):
+        w, c, f, b = (ctypes.c_longlong() for _ in range(4))
+        r = ctypes.c_int()
+        _check(lib().btam_server_stats(self.handle, ctypes.byref(w), ctypes.byref(r),
+                                       ctypes.byref(c), ctypes.byref(f), ctypes.byref(b)),
+               "btam_server_stats")
+        return dict(waiting=w.value, running=r.value, completed=c.value, failed=f.value,
+                    bytes_in_use=b.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib().btam_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

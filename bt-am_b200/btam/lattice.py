@@ -223,3 +223,53 @@ def config4(n=128, seed=4):
         hf = float(rng.uniform(0.0, 0.5))
         out.append(sphere(R, T=T, h_fraction=hf, seed=seed * 1000 + k))
     return out
+
+
+def periodic_cube(n_mg, *, h_fraction=0.3, T=300.0, seed=0):
+    """Periodic ortho-hexagonal block of about n_mg Mg (4 per cell), as close
+    to a cube as whole cells allow and at least 2 rc thick along every axis,
+    H on a seeded fraction of the tetrahedral sites with x ~ U[0, 0.3]."""
+    dims = np.array([A_MG, np.sqrt(3.0) * A_MG, C_OVER_A * A_MG])
+    edge = (n_mg / 4.0 * np.prod(dims)) ** (1.0 / 3.0)
+    n = np.maximum(np.round(edge / dims).astype(int), [4, 3, 3])
+    return supercell(int(n[0]), int(n[1]), int(n[2]), ortho=True, h_fraction=h_fraction,
+                     x_range=(0.0, 0.3), sigma_range=(0.08, 0.15), jitter=0.02, T=T,
+                     seed=seed)
+
+
+def wire(R, length, *, T=300.0, seed=0):
+    """hcp nanowire of radius R along c, ``length`` cells, periodic along the
+    axis; H x ~ U[0, 0.5] beyond 2/3 R and 0.02 inside (the precision
+    workload's profile, scaled)."""
+    def xf(rng, r, n):
+        x = np.full(n, 0.02)
+        m = r > (2.0 / 3.0) * R
+        x[m] = rng.uniform(0.0, 0.5, m.sum())
+        return x
+    return cluster("wire", R, length=length, x_fn=xf, T=T, seed=seed)
+
+
+def config5(n_jobs=64, rate=200.0, seed=5):
+    """The served job stream: Poisson arrivals (mean ``rate`` jobs/s) of
+    relaxation and 100-step master-equation jobs, half and half, on periodic
+    cubes of 250-60 000 Mg (log-uniform), nanowires (R ~ U[10, 30] A, 4-20
+    cells) and spheres (R log-uniform on [8, 25] A), T ~ U[300, 600] K.
+    Returns a list of (arrival time [s], system, job kind)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_jobs))
+    jobs = []
+    for k in range(n_jobs):
+        T = float(rng.uniform(300.0, 600.0))
+        shape = rng.choice(["cube", "cube", "wire", "sphere"])
+        s_seed = seed * 100000 + k
+        if shape == "cube":
+            n_mg = float(np.exp(rng.uniform(np.log(250.0), np.log(60000.0))))
+            s = periodic_cube(n_mg, h_fraction=float(rng.uniform(0.0, 0.5)), T=T, seed=s_seed)
+        elif shape == "wire":
+            s = wire(float(rng.uniform(10.0, 30.0)), int(rng.integers(4, 21)), T=T, seed=s_seed)
+        else:
+            R = float(np.exp(rng.uniform(np.log(8.0), np.log(25.0))))
+            s = sphere(R, T=T, h_fraction=float(rng.uniform(0.0, 0.5)), seed=s_seed)
+        kind = "relax" if rng.random() < 0.5 else "dmd"
+        jobs.append((float(t[k]), s, kind))
+    return jobs

@@ -145,25 +145,25 @@ int copy_sites(btam_batch *b, int k) {
 void free_batch(btam_batch *b) {
   for (int f = 0; f < 2; ++f)
     if (b->exec[f]) cudaGraphExecDestroy(b->exec[f]);
-  dfree(b->seg);
-  dfree(b->pos);
-  dfree(b->xb);
-  dfree(b->code);
-  dfree(b->owner);
-  dfree(b->gamma);
-  dfree(b->offs);
-  dfree(b->idx);
-  dfree(b->rho);
-  dfree(b->V0);
-  dfree(b->S0);
-  dfree(b->selfx);
-  dfree(b->Rq);
-  dfree(b->Rs);
-  dfree(b->Rx);
-  dfree(b->totals);
-  dfree(b->mom64);
-  dfree(b->mom32);
-  dfree(b->err);
+  dfree(b->seg, b->st);
+  dfree(b->pos, b->st);
+  dfree(b->xb, b->st);
+  dfree(b->code, b->st);
+  dfree(b->owner, b->st);
+  dfree(b->gamma, b->st);
+  dfree(b->offs, b->st);
+  dfree(b->idx, b->st);
+  dfree(b->rho, b->st);
+  dfree(b->V0, b->st);
+  dfree(b->S0, b->st);
+  dfree(b->selfx, b->st);
+  dfree(b->Rq, b->st);
+  dfree(b->Rs, b->st);
+  dfree(b->Rx, b->st);
+  dfree(b->totals, b->st);
+  dfree(b->mom64, b->st);
+  dfree(b->mom32, b->st);
+  dfree(b->err, b->st);
   if (b->ev) cudaEventDestroy(b->ev);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
@@ -181,7 +181,7 @@ int batch_build(btam_batch *b) {
   for (int k = 0; k < ns; ++k) {
     btam_system *s = b->sys[k];
     int last = 0;  // real sites' pairs: offs[n_real] (the list may also cover images)
-    BTAM_TRY(cudaMemcpy(&last, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost));
+    BTAM_TRY(copy_sync(&last, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     n_list_pairs[k] = last;
     if (n_real + n_img + s->n_real + s->n_ghost > 0x7fffffffLL || n_pairs + last > 0x7fffffffLL)
       return BTAM_ERR_TOO_LARGE;
@@ -202,23 +202,23 @@ int batch_build(btam_batch *b) {
   b->n_all = (int)(n_real + n_img);
   b->n_pairs = n_pairs;
   const size_t nr = n_real, na = b->n_all;
-  BTAM_TRY(dalloc(b->seg, ns + 1));
-  BTAM_TRY(dalloc(b->pos, na));
-  BTAM_TRY(dalloc(b->xb, na));
-  BTAM_TRY(dalloc(b->code, na));
-  BTAM_TRY(dalloc(b->owner, na));
-  BTAM_TRY(dalloc(b->gamma, nr));
-  BTAM_TRY(dalloc(b->offs, nr + 1));
-  BTAM_TRY(dalloc(b->idx, (size_t)n_pairs));
-  BTAM_TRY(dalloc(b->rho, nr));
-  BTAM_TRY(dalloc(b->V0, nr));
-  BTAM_TRY(dalloc(b->S0, nr));
-  BTAM_TRY(dalloc(b->selfx, nr));
-  BTAM_TRY(dalloc(b->Rq, 3 * nr));
-  BTAM_TRY(dalloc(b->Rs, nr));
-  BTAM_TRY(dalloc(b->Rx, nr));
-  BTAM_TRY(dalloc(b->totals, 4 * (size_t)ns));
-  BTAM_TRY(dalloc(b->err, 1));
+  BTAM_TRY(dalloc(b->seg, b->st, ns + 1));
+  BTAM_TRY(dalloc(b->pos, b->st, na));
+  BTAM_TRY(dalloc(b->xb, b->st, na));
+  BTAM_TRY(dalloc(b->code, b->st, na));
+  BTAM_TRY(dalloc(b->owner, b->st, na));
+  BTAM_TRY(dalloc(b->gamma, b->st, nr));
+  BTAM_TRY(dalloc(b->offs, b->st, nr + 1));
+  BTAM_TRY(dalloc(b->idx, b->st, (size_t)n_pairs));
+  BTAM_TRY(dalloc(b->rho, b->st, nr));
+  BTAM_TRY(dalloc(b->V0, b->st, nr));
+  BTAM_TRY(dalloc(b->S0, b->st, nr));
+  BTAM_TRY(dalloc(b->selfx, b->st, nr));
+  BTAM_TRY(dalloc(b->Rq, b->st, 3 * nr));
+  BTAM_TRY(dalloc(b->Rs, b->st, nr));
+  BTAM_TRY(dalloc(b->Rx, b->st, nr));
+  BTAM_TRY(dalloc(b->totals, b->st, 4 * (size_t)ns));
+  BTAM_TRY(dalloc(b->err, b->st, 1));
   BTAM_TRY(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
   BTAM_TRY(cudaMemcpyAsync(b->seg, seg.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice,
                            b->st));
@@ -261,8 +261,8 @@ template <class R> cudaError_t enqueue_eval(btam_batch *b, int form, R *mom, con
 
 int ensure_moments(btam_batch *b, int precision) {
   const size_t nm = (size_t)b->n_real * kMomStride;
-  if (precision == BTAM_FP64 && !b->mom64) BTAM_TRY(dalloc(b->mom64, nm));
-  if (precision == BTAM_FP32C && !b->mom32) BTAM_TRY(dalloc(b->mom32, nm));
+  if (precision == BTAM_FP64 && !b->mom64) BTAM_TRY(dalloc(b->mom64, b->st, nm));
+  if (precision == BTAM_FP32C && !b->mom32) BTAM_TRY(dalloc(b->mom32, b->st, nm));
   return BTAM_OK;
 }
 

@@ -154,10 +154,10 @@ int ensure_sites(btam_system *s, int n_all) {
   double4 *pos = nullptr;
   double2 *xb = nullptr;
   int *code = nullptr, *owner = nullptr;
-  BTAM_TRY(dalloc(pos, cap));
-  BTAM_TRY(dalloc(xb, cap));
-  BTAM_TRY(dalloc(code, cap));
-  BTAM_TRY(dalloc(owner, cap));
+  BTAM_TRY(dalloc(pos, s->st, cap));
+  BTAM_TRY(dalloc(xb, s->st, cap));
+  BTAM_TRY(dalloc(code, s->st, cap));
+  BTAM_TRY(dalloc(owner, s->st, cap));
   if (s->pos) {
     BTAM_TRY(cudaMemcpyAsync(pos, s->pos, (size_t)s->n_real * sizeof(double4),
                              cudaMemcpyDeviceToDevice, s->st));
@@ -169,10 +169,10 @@ int ensure_sites(btam_system *s, int n_all) {
                              cudaMemcpyDeviceToDevice, s->st));
     BTAM_TRY(cudaStreamSynchronize(s->st));
   }
-  dfree(s->pos);
-  dfree(s->xb);
-  dfree(s->code);
-  dfree(s->owner);
+  dfree(s->pos, s->st);
+  dfree(s->xb, s->st);
+  dfree(s->code, s->st);
+  dfree(s->owner, s->st);
   s->pos = pos;
   s->xb = xb;
   s->code = code;
@@ -212,6 +212,31 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesVie
 
 // Table views for the allocation-free entry point (noalloc.cu).
 namespace btam {
+// One pool per device, created on first use and kept for the life of the
+// process; its release threshold keeps freed blocks cached, so a stream of
+// systems of similar sizes reuses memory without returning it to the driver.
+cudaMemPool_t device_pool() {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((int)pools.size() <= dev) pools.resize(dev + 1, nullptr);
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 const TablesView<double> &tables_view64(const btam_tables *t) { return t->v64; }
 const TablesView<float> &tables_view32(const btam_tables *t) { return t->v32; }
 double tables_mass(const btam_tables *t, int code) {
@@ -368,24 +393,24 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
     ho[i] = i;
   }
   if (st == BTAM_OK) {
-    e = cudaMemcpy(s->pos, hp.data(), n * sizeof(double4), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(s->xb, hx.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(s->code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(s->owner, ho.data(), n * sizeof(int), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = dalloc(s->gamma, n);
+    e = copy_sync(s->pos, hp.data(), n * sizeof(double4), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = copy_sync(s->xb, hx.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = copy_sync(s->code, code.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = copy_sync(s->owner, ho.data(), n * sizeof(int), cudaMemcpyHostToDevice, s->st);
+    if (e == cudaSuccess) e = dalloc(s->gamma, s->st, n);
     if (e == cudaSuccess) {
-      if (gamma) e = cudaMemcpy(s->gamma, gamma, n * sizeof(double), cudaMemcpyHostToDevice);
-      else e = cudaMemset(s->gamma, 0, n * sizeof(double));
+      if (gamma) e = copy_sync(s->gamma, gamma, n * sizeof(double), cudaMemcpyHostToDevice, s->st);
+      else e = cudaMemsetAsync(s->gamma, 0, n * sizeof(double), s->st);
     }
-    if (e == cudaSuccess) e = dalloc(s->stage, 5 * (size_t)n);
-    if (e == cudaSuccess) e = dalloc(s->err, 1);
-    if (e == cudaSuccess) e = cudaMemset(s->err, 0, sizeof(int));
+    if (e == cudaSuccess) e = dalloc(s->stage, s->st, 5 * (size_t)n);
+    if (e == cudaSuccess) e = dalloc(s->err, s->st, 1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->st);
     for (double **p : {&s->rho, &s->V0, &s->S0, &s->selfx, &s->Rs, &s->Rx})
-      if (e == cudaSuccess) e = dalloc(*p, n);
-    if (e == cudaSuccess) e = dalloc(s->Rq, 3 * (size_t)n);
-    if (e == cudaSuccess) e = dalloc(s->totals, 4);
-    if (e == cudaSuccess) e = dalloc(s->bbox, 6);
-    if (e == cudaSuccess) e = dalloc(s->grid, 1);
+      if (e == cudaSuccess) e = dalloc(*p, s->st, n);
+    if (e == cudaSuccess) e = dalloc(s->Rq, s->st, 3 * (size_t)n);
+    if (e == cudaSuccess) e = dalloc(s->totals, s->st, 4);
+    if (e == cudaSuccess) e = dalloc(s->bbox, s->st, 6);
+    if (e == cudaSuccess) e = dalloc(s->grid, s->st, 1);
     st = cuda_status(e);
   }
   if (st != BTAM_OK) {
@@ -399,14 +424,16 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
 void btam_system_destroy(btam_system *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
-  dfree(s->pos); dfree(s->xb); dfree(s->code); dfree(s->owner); dfree(s->image);
-  dfree(s->gamma); dfree(s->stage); dfree(s->offs); dfree(s->idx); dfree(s->cnt);
-  dfree(s->tmp); dfree(s->bbox); dfree(s->grid); dfree(s->cell_of); dfree(s->cell_cnt);
-  dfree(s->cell_start); dfree(s->cursor); dfree(s->cell_sites); dfree(s->rho); dfree(s->V0);
-  dfree(s->S0); dfree(s->selfx); dfree(s->Rq); dfree(s->Rs); dfree(s->Rx); dfree(s->totals);
-  dfree(s->mom64); dfree(s->mom32); dfree(s->err);
-  dfree(s->doffs); dfree(s->didx); dfree(s->X); dfree(s->X0); dfree(s->dtot); dfree(s->mu);
-  dfree(s->dact); dfree(s->ddeg); dfree(s->rv);
+  dfree(s->pos, s->st); dfree(s->xb, s->st); dfree(s->code, s->st); dfree(s->owner, s->st); dfree(s->image, s->st);
+  dfree(s->gamma, s->st); dfree(s->stage, s->st); dfree(s->offs, s->st); dfree(s->idx, s->st); dfree(s->cnt, s->st);
+  dfree(s->tmp, s->st); dfree(s->bbox, s->st); dfree(s->grid, s->st); dfree(s->cell_of, s->st); dfree(s->cell_cnt, s->st);
+  dfree(s->cell_start, s->st); dfree(s->cursor, s->st); dfree(s->cell_sites, s->st); dfree(s->rho, s->st); dfree(s->V0, s->st);
+  dfree(s->S0, s->st); dfree(s->selfx, s->st); dfree(s->Rq, s->st); dfree(s->Rs, s->st); dfree(s->Rx, s->st); dfree(s->totals, s->st);
+  dfree(s->mom64, s->st); dfree(s->mom32, s->st); dfree(s->err, s->st);
+  dfree(s->doffs, s->st); dfree(s->didx, s->st); dfree(s->X, s->st); dfree(s->X0, s->st); dfree(s->dtot, s->st); dfree(s->mu, s->st);
+  dfree(s->dact, s->st); dfree(s->ddeg, s->st); dfree(s->rv, s->st);
+  s->scratch.release(s->st);
+  if (s->st) cudaStreamSynchronize(s->st);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
 }
@@ -456,8 +483,8 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
   s->n_ghost = 0;
   if (s->any_periodic) {
     int *cnt = nullptr, *off = nullptr;
-    BTAM_TRY(dalloc(cnt, n + 1));
-    cudaError_t e = dalloc(off, n + 1);
+    BTAM_TRY(dalloc(cnt, s->st, n + 1));
+    cudaError_t e = dalloc(off, s->st, n + 1);
     if (e == cudaSuccess) e = cudaMemsetAsync(cnt + n, 0, sizeof(int), s->st);
     if (e == cudaSuccess) e = launch_ghost_count(n, s->pos, s->box, cnt, s->st);
     if (e == cudaSuccess) e = exclusive_scan(cnt, off, n + 1, s->scratch, s->st);
@@ -468,14 +495,14 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
     int st = cuda_status(e);
     if (st == BTAM_OK) st = ensure_sites(s, n + ng);
     if (st == BTAM_OK && ng > 0) {
-      e = dalloc(s->image, ng);
+      e = dalloc(s->image, s->st, ng);
       if (e == cudaSuccess)
         e = launch_ghost_emit(n, s->pos, s->xb, s->code, s->owner, s->image, s->box, off, ng,
                               s->err, s->st);
       st = cuda_status(e);
     }
-    cudaFree(cnt);
-    cudaFree(off);
+    dfree(cnt, s->st);
+    dfree(off, s->st);
     if (st != BTAM_OK) return st;
     s->n_ghost = ng;
   }
@@ -484,14 +511,14 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
   // ---- cells and neighbour buffers
   int max_cells = 4 * n_all + 1024;
   if (max_cells > s->cell_cap) {
-    BTAM_TRY(dalloc(s->cell_cnt, max_cells + 1));
-    BTAM_TRY(dalloc(s->cell_start, max_cells + 1));
-    BTAM_TRY(dalloc(s->cursor, max_cells));
+    BTAM_TRY(dalloc(s->cell_cnt, s->st, max_cells + 1));
+    BTAM_TRY(dalloc(s->cell_start, s->st, max_cells + 1));
+    BTAM_TRY(dalloc(s->cursor, s->st, max_cells));
     s->cell_cap = max_cells;
   }
   if (n_all > s->site_cap) {
-    BTAM_TRY(dalloc(s->cell_of, n_all));
-    BTAM_TRY(dalloc(s->cell_sites, n_all));
+    BTAM_TRY(dalloc(s->cell_of, s->st, n_all));
+    BTAM_TRY(dalloc(s->cell_sites, s->st, n_all));
     s->site_cap = n_all;
   }
   int total = 0;
@@ -512,15 +539,15 @@ static int build_list(btam_system *s, int n_all, int n_query, double rc, int max
                       int allow_empty, int *&offs, int &q_cap, int *&idx, long long &idx_cap,
                       int &total) {
   if (n_query + 1 > s->cnt_cap) {
-    BTAM_TRY(dalloc(s->cnt, n_query + 1));
+    BTAM_TRY(dalloc(s->cnt, s->st, n_query + 1));
     s->cnt_cap = n_query + 1;
   }
   if (n_query + 1 > q_cap) {
-    BTAM_TRY(dalloc(offs, n_query + 1));
+    BTAM_TRY(dalloc(offs, s->st, n_query + 1));
     q_cap = n_query + 1;
   }
   if ((long long)n_query * kNbrBuf > s->tmp_cap) {
-    BTAM_TRY(dalloc(s->tmp, (size_t)n_query * kNbrBuf));
+    BTAM_TRY(dalloc(s->tmp, s->st, (size_t)n_query * kNbrBuf));
     s->tmp_cap = (long long)n_query * kNbrBuf;
   }
   NbrArgs a;
@@ -552,7 +579,7 @@ static int build_list(btam_system *s, int n_all, int n_query, double rc, int max
   int st = read_err(s);
   if (st != BTAM_OK) return st;
   if (total > idx_cap) {
-    BTAM_TRY(dalloc(idx, total));
+    BTAM_TRY(dalloc(idx, s->st, total));
     idx_cap = total;
   }
   BTAM_TRY(launch_compact(n_query, s->tmp, offs, idx, s->st));
@@ -565,10 +592,10 @@ extern "C" {
 int btam_neighbors_copy(const btam_system *s, int *offs, int *idx, long long idx_cap) {
   if (!s || !offs) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
-  BTAM_TRY(cudaMemcpy(offs, s->offs, (s->n_list + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  BTAM_TRY(copy_sync(offs, s->offs, (s->n_list + 1) * sizeof(int), cudaMemcpyDeviceToHost, s->st));
   if (idx) {
     if (idx_cap < s->n_pairs) return BTAM_ERR_ARG;
-    BTAM_TRY(cudaMemcpy(idx, s->idx, s->n_pairs * sizeof(int), cudaMemcpyDeviceToHost));
+    BTAM_TRY(copy_sync(idx, s->idx, s->n_pairs * sizeof(int), cudaMemcpyDeviceToHost, s->st));
   }
   return BTAM_OK;
 }
@@ -579,10 +606,10 @@ int btam_ghosts_copy(const btam_system *s, double *q, int *owner, int *image) {
   if (ng == 0) return BTAM_OK;
   std::vector<double4> hp(ng);
   std::vector<char4> hi(ng);
-  BTAM_TRY(cudaMemcpy(hp.data(), s->pos + n, ng * sizeof(double4), cudaMemcpyDeviceToHost));
-  BTAM_TRY(cudaMemcpy(hi.data(), s->image, ng * sizeof(char4), cudaMemcpyDeviceToHost));
+  BTAM_TRY(copy_sync(hp.data(), s->pos + n, ng * sizeof(double4), cudaMemcpyDeviceToHost, s->st));
+  BTAM_TRY(copy_sync(hi.data(), s->image, ng * sizeof(char4), cudaMemcpyDeviceToHost, s->st));
   if (owner)
-    BTAM_TRY(cudaMemcpy(owner, s->owner + n, ng * sizeof(int), cudaMemcpyDeviceToHost));
+    BTAM_TRY(copy_sync(owner, s->owner + n, ng * sizeof(int), cudaMemcpyDeviceToHost, s->st));
   for (int k = 0; k < ng; ++k) {
     if (q) {
       q[3 * k] = hp[k].x;
@@ -604,12 +631,12 @@ int btam_mf_eval_async(btam_system *s, int precision) {
   if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
   const size_t nm = (size_t)s->n_real * kMomStride;
   if (precision == BTAM_FP64) {
-    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
     EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
     BTAM_TRY(launch_pass1(a, s->st, s->variant1[0]));
     BTAM_TRY(launch_pass2(a, s->st, s->variant2[0]));
   } else {
-    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
     EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
     BTAM_TRY(launch_pass1(a, s->st, s->variant1[1]));
     BTAM_TRY(launch_pass2(a, s->st, s->variant2[1]));
@@ -640,10 +667,10 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
   const size_t nm = (size_t)s->n_real * kMomStride;
   int st;
   if (precision == BTAM_FP64) {
-    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
     st = autotune_form(s, eval_args<double>(s, s->mom64, s->T->v64), 0, 3);
   } else if (precision == BTAM_FP32C) {
-    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
     st = autotune_form(s, eval_args<float>(s, s->mom32, s->T->v32), 1, 3);
   } else {
     return BTAM_ERR_ARG;
@@ -699,10 +726,10 @@ int btam_mf_rho(btam_system *s, int precision, double *rho) {
   BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
   const size_t nm = (size_t)s->n_real * kMomStride;
   if (precision == BTAM_FP64) {
-    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, nm));
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
     BTAM_TRY(launch_pass1(eval_args<double>(s, s->mom64, s->T->v64), s->st));
   } else if (precision == BTAM_FP32C) {
-    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, nm));
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
     BTAM_TRY(launch_pass1(eval_args<float>(s, s->mom32, s->T->v32), s->st));
   } else {
     return BTAM_ERR_ARG;
@@ -720,13 +747,13 @@ int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]) {
   const size_t nm = (size_t)s->n_real * kMomStride;
   cudaError_t e = cudaEventRecord(ev[0], s->st);
   if (precision == BTAM_FP64) {
-    if (!s->mom64 && e == cudaSuccess) e = dalloc(s->mom64, nm);
+    if (!s->mom64 && e == cudaSuccess) e = dalloc(s->mom64, s->st, nm);
     EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
     if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[0]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
     if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[0]);
   } else {
-    if (!s->mom32 && e == cudaSuccess) e = dalloc(s->mom32, nm);
+    if (!s->mom32 && e == cudaSuccess) e = dalloc(s->mom32, s->st, nm);
     EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
     if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[1]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
@@ -865,7 +892,7 @@ int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m, const 
   // layout: z g p z0 g0 work (n4 each), S[m] Y[m] (n4 each), fterm rterm ones (n), small
   const size_t need = (size_t)(6 + 2 * m) * n4 + 3 * (size_t)n + 64;
   if (!s->rv || s->relax_m < m) {
-    BTAM_TRY(dalloc(s->rv, need));
+    BTAM_TRY(dalloc(s->rv, s->st, need));
     s->relax_m = m;
   }
   RelaxVecs v;
@@ -999,11 +1026,11 @@ int btam_dmd_setup(btam_system *s) {
   if (st != BTAM_OK) return st;
   s->d_pairs = total;
   for (long long **p : {&s->X, &s->X0})
-    BTAM_TRY(dalloc(*p, n));
-  BTAM_TRY(dalloc(s->dtot, 2));
-  BTAM_TRY(dalloc(s->mu, n));
-  BTAM_TRY(dalloc(s->dact, n));
-  BTAM_TRY(dalloc(s->ddeg, n));
+    BTAM_TRY(dalloc(*p, s->st, n));
+  BTAM_TRY(dalloc(s->dtot, s->st, 2));
+  BTAM_TRY(dalloc(s->mu, s->st, n));
+  BTAM_TRY(dalloc(s->dact, s->st, n));
+  BTAM_TRY(dalloc(s->ddeg, s->st, n));
   BTAM_TRY(dmd_init(n, s->xb, s->code, s->X, s->st));
   BTAM_TRY(dmd_commit_all(n, s->code, s->X, s->xb, s->st));
   if (s->n_ghost > 0)
@@ -1078,10 +1105,10 @@ int btam_dmd_occupancy(btam_system *s, double *x, long long *quanta, double *mu)
 int btam_dmd_graph_copy(const btam_system *s, int *offs, int *idx, long long idx_cap) {
   if (!s || !offs) return BTAM_ERR_ARG;
   if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
-  BTAM_TRY(cudaMemcpy(offs, s->doffs, (s->n_real + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+  BTAM_TRY(copy_sync(offs, s->doffs, (s->n_real + 1) * sizeof(int), cudaMemcpyDeviceToHost, s->st));
   if (idx) {
     if (idx_cap < s->d_pairs) return BTAM_ERR_ARG;
-    BTAM_TRY(cudaMemcpy(idx, s->didx, s->d_pairs * sizeof(int), cudaMemcpyDeviceToHost));
+    BTAM_TRY(copy_sync(idx, s->didx, s->d_pairs * sizeof(int), cudaMemcpyDeviceToHost, s->st));
   }
   return BTAM_OK;
 }

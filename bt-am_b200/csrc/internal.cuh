@@ -96,16 +96,32 @@ inline int cuda_status(cudaError_t e) {
     if (_e != cudaSuccess) return cuda_status(_e); \
   } while (0)
 
-template <class T> inline cudaError_t dalloc(T *&p, size_t count) {
-  if (p) cudaFree(p);
+// Device memory of systems and batches comes from the library's
+// stream-ordered pool of the current device (cudaMallocFromPoolAsync on the
+// owner's stream), so creating and destroying systems never synchronises the
+// device and never stalls other systems' work in flight; freed blocks stay
+// in the pool for the next system.
+template <class T> inline cudaError_t dalloc(T *&p, cudaStream_t st, size_t count) {
+  if (p) cudaFreeAsync(p, st);
   p = nullptr;
   if (count == 0) count = 1;
-  return cudaMalloc((void **)&p, count * sizeof(T));
+  cudaMemPool_t pool = btam::device_pool();
+  if (!pool) return cudaErrorMemoryAllocation;
+  return cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), pool, st);
 }
 
-template <class T> inline void dfree(T *&p) {
-  if (p) cudaFree(p);
+template <class T> inline void dfree(T *&p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
   p = nullptr;
+}
+
+// Synchronous copies ordered on a stream (the memory may come from the
+// stream-ordered pool, so the copy must follow the allocation on `st`).
+inline cudaError_t copy_sync(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind,
+                             cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, kind, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e;
 }
 
 // Waits for the stream, returns the error bits raised since the last read

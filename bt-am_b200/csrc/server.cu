@@ -1,0 +1,296 @@
+// Job server: relaxation and master-equation jobs of many sizes served
+// concurrently on one device (no counterpart in the reference, which runs
+// one simulation per MPI job).
+//
+// Each job is a whole system: submitted with its host arrays (copied at
+// submission), admitted by its estimated device-memory footprint
+// (sched.hpp), then run by one of the worker threads on its own
+// btam_system, i.e. its own CUDA stream, with q, sigma, x, the images and
+// the neighbour lists resident on the device from creation to the last step.
+// Workers never synchronise the device (stream-ordered allocation, one
+// stream per job), so the kernels of every running job overlap on the GPU;
+// a job that arrives while others run starts as soon as a worker and its
+// memory are free.  Results are the same as the job run alone: every kernel
+// is deterministic and a job's work touches only its own buffers.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "../../include/btam.h"
+#include "sched.hpp"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+  long long id = 0;
+  btam_job_spec spec{};
+  // owned copies of the inputs
+  std::vector<double> q, sigma, x, beta, gamma;
+  std::vector<int> species;
+  double origin[3], cell[9];
+  int periodic[3];
+  size_t bytes = 0;
+  // results
+  btam_job_result res{};
+  std::vector<double> q_out, sigma_out, x_out;
+  bool done = false;
+};
+
+double since(Clock::time_point t0) {
+  return std::chrono::duration<double>(Clock::now() - t0).count();
+}
+
+}  // namespace
+
+struct btam_server {
+  const btam_tables *T = nullptr;
+  int device = 0;
+  Clock::time_point t0;
+  std::mutex mu;
+  std::condition_variable work_cv, done_cv;
+  btam::AdmissionQueue queue{0};
+  std::map<long long, std::unique_ptr<Job>> jobs;
+  long long next_id = 1;
+  int running = 0;
+  bool stop = false;
+  std::vector<std::thread> workers;
+  long long completed = 0, failed = 0;
+};
+
+namespace {
+
+// Runs one job on the calling worker thread; fills job->res and the outputs.
+void run_job(btam_server *srv, Job *job) {
+  const btam_job_spec &sp = job->spec;
+  btam_job_result &r = job->res;
+  const int n = sp.n;
+  btam_system *s = nullptr;
+  int st = btam_system_create(srv->T, n, job->q.data(), job->sigma.data(), job->x.data(),
+                              job->species.data(), job->beta.empty() ? nullptr : job->beta.data(),
+                              job->gamma.empty() ? nullptr : job->gamma.data(), job->origin,
+                              job->cell, job->periodic, &s);
+  if (st == BTAM_OK) st = btam_neighbors_build(s, 0);
+  if (st == BTAM_OK) {
+    r.t_start = since(srv->t0);
+    if (sp.kind == BTAM_JOB_RELAX) {
+      double info[5] = {0, 0, 0, 0, 0};
+      const double bounds[3] = {sp.sigma_min > 0 ? sp.sigma_min : 0.001,
+                                sp.sigma_max > 0 ? sp.sigma_max : 0.4,
+                                sp.x_min > 0 ? sp.x_min : 0.01};
+      st = btam_relax(s, sp.mode, sp.tol, sp.max_iter, sp.lbfgs_m > 0 ? sp.lbfgs_m : 8, bounds,
+                      info);
+      r.norm = info[0];
+      r.iterations = (int)info[1];
+      r.evaluations = (int)info[2];
+      r.objective = info[3];
+      r.converged = (int)info[4];
+    } else if (sp.kind == BTAM_JOB_DMD) {
+      st = btam_dmd_setup(s);
+      long long tot[2] = {0, 0};
+      if (st == BTAM_OK) st = btam_dmd_step(s, sp.precision, sp.nsteps, sp.dmd_params, tot);
+      r.h_quanta_hi = tot[0];
+      r.h_quanta_lo = tot[1];
+      r.iterations = sp.nsteps;
+    } else if (sp.kind == BTAM_JOB_EVAL) {
+      double totals[4] = {0, 0, 0, 0};
+      st = btam_mf_eval(s, sp.precision, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                        totals);
+      r.objective = totals[0];
+      r.norm = totals[2];
+      r.evaluations = 1;
+    } else {
+      st = BTAM_ERR_ARG;
+    }
+  }
+  if (st == BTAM_OK) {
+    job->q_out.resize(3 * (size_t)n);
+    job->sigma_out.resize(n);
+    job->x_out.resize(n);
+    st = btam_system_get_state(s, job->q_out.data(), job->sigma_out.data(), job->x_out.data());
+  }
+  if (s) btam_system_destroy(s);
+  r.status = st;
+}
+
+void worker_main(btam_server *srv) {
+  cudaSetDevice(srv->device);
+  std::unique_lock<std::mutex> lock(srv->mu);
+  for (;;) {
+    long long id = -1;
+    srv->work_cv.wait(lock, [&] {
+      if (srv->stop) return true;
+      id = srv->queue.admit();
+      return id >= 0;
+    });
+    if (id < 0) return;  // stopping
+    Job *job = srv->jobs[id].get();
+    job->res.t_admit = since(srv->t0);
+    ++srv->running;
+    lock.unlock();
+    run_job(srv, job);
+    lock.lock();
+    job->res.t_end = since(srv->t0);
+    job->done = true;
+    --srv->running;
+    srv->queue.release(job->bytes);
+    if (job->res.status == BTAM_OK) ++srv->completed;
+    else ++srv->failed;
+    srv->done_cv.notify_all();
+    srv->work_cv.notify_all();  // freed memory may admit waiting jobs
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+long long btam_estimate_bytes(int n, const double cell[9], const int periodic[3]) {
+  if (n <= 0) return 0;
+  // images: each periodic direction adds a slab of width rc on both faces
+  double grow = 1.0;
+  for (int k = 0; k < 3; ++k) {
+    if (!periodic || !periodic[k] || !cell) continue;
+    const double *a = cell + 3 * ((k + 1) % 3), *b = cell + 3 * ((k + 2) % 3);
+    const double *c = cell + 3 * k;
+    double nx = a[1] * b[2] - a[2] * b[1], ny = a[2] * b[0] - a[0] * b[2],
+           nz = a[0] * b[1] - a[1] * b[0];
+    double area = std::sqrt(nx * nx + ny * ny + nz * nz);
+    double vol = std::fabs(c[0] * nx + c[1] * ny + c[2] * nz);
+    double h = area > 0 ? vol / area : 0.0;  // height of the cell along k
+    grow *= h > 0 ? 1.0 + 2.0 * BTAM_R_CUTOFF / h : 3.0;
+  }
+  const double n_all = n * grow;
+  // per all-sites row: position, occupancy/beta, species, owner, cell index,
+  // cell slot, image code; per real site: state, staging, results, both
+  // moment records, neighbour counts, the neighbour candidate buffer, the
+  // neighbour list at the cap, master-equation state and graph, relaxation
+  // vectors; plus a fixed allowance for cells and library scratch
+  const double per_all = 32 + 16 + 4 + 4 + 4 + 4 + 4;
+  const double per_real = 8 + 40 + 48 + 24 + 76 * 8 + 76 * 4 + 8 + 256 * 4 +
+                          BTAM_MAXNEIGH * 4 + 16 + 16 + 4 + BTAM_MAX_CHEMICAL_NEIGHS * 4 +
+                          (2 * 8 + 8) * 5 * 8;
+  return (long long)(n_all * per_all + n * per_real) + (8ll << 20);
+}
+
+int btam_server_create(const btam_tables *t, int n_workers, long long budget_bytes,
+                       btam_server **out) {
+  if (!t || !out || n_workers <= 0) return BTAM_ERR_ARG;
+  *out = nullptr;
+  btam_server *srv = new btam_server;
+  srv->T = t;
+  srv->t0 = Clock::now();
+  if (cudaGetDevice(&srv->device) != cudaSuccess) {
+    delete srv;
+    return BTAM_ERR_CUDA;
+  }
+  if (budget_bytes <= 0) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+      delete srv;
+      return BTAM_ERR_CUDA;
+    }
+    budget_bytes = (long long)(0.8 * (double)free_b);
+  }
+  srv->queue = btam::AdmissionQueue((size_t)budget_bytes);
+  for (int w = 0; w < n_workers; ++w) srv->workers.emplace_back(worker_main, srv);
+  *out = srv;
+  return BTAM_OK;
+}
+
+int btam_server_submit(btam_server *srv, const btam_job_spec *sp, long long *job_id) {
+  if (!srv || !sp || !job_id || sp->n <= 0 || !sp->q || !sp->sigma || !sp->x || !sp->species ||
+      !sp->origin || !sp->cell || !sp->periodic)
+    return BTAM_ERR_ARG;
+  if (sp->kind != BTAM_JOB_RELAX && sp->kind != BTAM_JOB_DMD && sp->kind != BTAM_JOB_EVAL)
+    return BTAM_ERR_ARG;
+  auto job = std::make_unique<Job>();
+  const size_t n = sp->n;
+  job->spec = *sp;
+  job->q.assign(sp->q, sp->q + 3 * n);
+  job->sigma.assign(sp->sigma, sp->sigma + n);
+  job->x.assign(sp->x, sp->x + n);
+  job->species.assign(sp->species, sp->species + n);
+  if (sp->beta) job->beta.assign(sp->beta, sp->beta + n);
+  if (sp->gamma) job->gamma.assign(sp->gamma, sp->gamma + n);
+  std::memcpy(job->origin, sp->origin, sizeof(job->origin));
+  std::memcpy(job->cell, sp->cell, sizeof(job->cell));
+  std::memcpy(job->periodic, sp->periodic, sizeof(job->periodic));
+  // the spec keeps no caller pointers
+  job->spec.q = job->spec.sigma = job->spec.x = job->spec.beta = job->spec.gamma = nullptr;
+  job->spec.species = nullptr;
+  job->spec.origin = job->spec.cell = nullptr;
+  job->spec.periodic = nullptr;
+  job->bytes = (size_t)btam_estimate_bytes(sp->n, job->cell, job->periodic);
+  std::lock_guard<std::mutex> lock(srv->mu);
+  if (srv->stop) return BTAM_ERR_ARG;
+  if (!srv->queue.fits_ever(job->bytes)) return BTAM_ERR_TOO_LARGE;
+  job->id = srv->next_id++;
+  job->res.t_submit = since(srv->t0);
+  job->res.kind = sp->kind;
+  *job_id = job->id;
+  srv->queue.push(job->id, job->bytes);
+  srv->jobs[job->id] = std::move(job);
+  srv->work_cv.notify_one();
+  return BTAM_OK;
+}
+
+int btam_server_wait(btam_server *srv, long long job_id, double timeout_s, btam_job_result *res,
+                     double *q, double *sigma, double *x) {
+  if (!srv) return BTAM_ERR_ARG;
+  std::unique_lock<std::mutex> lock(srv->mu);
+  auto it = srv->jobs.find(job_id);
+  if (it == srv->jobs.end()) return BTAM_ERR_ARG;
+  Job *job = it->second.get();
+  auto ready = [&] { return job->done; };
+  if (timeout_s < 0) {
+    srv->done_cv.wait(lock, ready);
+  } else if (!srv->done_cv.wait_for(lock, std::chrono::duration<double>(timeout_s), ready)) {
+    return BTAM_ERR_TIMEOUT;
+  }
+  if (res) *res = job->res;
+  const size_t n = job->spec.n;
+  if (job->res.status == BTAM_OK) {
+    if (q) std::memcpy(q, job->q_out.data(), 3 * n * sizeof(double));
+    if (sigma) std::memcpy(sigma, job->sigma_out.data(), n * sizeof(double));
+    if (x) std::memcpy(x, job->x_out.data(), n * sizeof(double));
+  }
+  int st = job->res.status;
+  srv->jobs.erase(it);  // a result is collected once
+  return st;
+}
+
+int btam_server_stats(btam_server *srv, long long *waiting, int *running, long long *completed,
+                      long long *failed, long long *bytes_in_use) {
+  if (!srv) return BTAM_ERR_ARG;
+  std::lock_guard<std::mutex> lock(srv->mu);
+  if (waiting) *waiting = (long long)srv->queue.waiting();
+  if (running) *running = srv->running;
+  if (completed) *completed = srv->completed;
+  if (failed) *failed = srv->failed;
+  if (bytes_in_use) *bytes_in_use = (long long)srv->queue.in_use();
+  return BTAM_OK;
+}
+
+int btam_server_destroy(btam_server *srv) {
+  if (!srv) return BTAM_ERR_ARG;
+  {
+    std::lock_guard<std::mutex> lock(srv->mu);
+    srv->stop = true;
+  }
+  srv->work_cv.notify_all();
+  for (auto &w : srv->workers) w.join();
+  delete srv;
+  return BTAM_OK;
+}
+
+}  // extern "C"

@@ -305,7 +305,7 @@ cudaError_t exclusive_scan(const int *in, int *out, int n, DeviceScratch &s,
   size_t need = 0;
   cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, need, in, out, n, st);
   if (e != cudaSuccess) return e;
-  if ((e = s.ensure(need)) != cudaSuccess) return e;
+  if ((e = s.ensure(need, st)) != cudaSuccess) return e;
   size_t have = s.bytes;
   return cub::DeviceScan::ExclusiveSum(s.ptr, have, in, out, n, st);
 }

@@ -34,18 +34,29 @@ struct CellGrid {
   int n[3];
 };
 
-// Growable device scratch for library temporaries (CUB scans).
+// The library's stream-ordered memory pool of the current device (defined
+// in btam_capi.cu).
+cudaMemPool_t device_pool();
+
+// Growable device scratch for library temporaries (CUB scans), allocated in
+// stream order from the library pool.
 struct DeviceScratch {
   void *ptr = nullptr;
   size_t bytes = 0;
-  cudaError_t ensure(size_t need) {
+  cudaError_t ensure(size_t need, cudaStream_t st) {
     if (need <= bytes) return cudaSuccess;
-    if (ptr) cudaFree(ptr);
+    release(st);
+    cudaMemPool_t pool = device_pool();
+    if (!pool) return cudaErrorMemoryAllocation;
+    cudaError_t e = cudaMallocFromPoolAsync(&ptr, need, pool, st);
+    if (e == cudaSuccess) bytes = need;
+    else ptr = nullptr;
+    return e;
+  }
+  void release(cudaStream_t st) {
+    if (ptr) cudaFreeAsync(ptr, st);
     ptr = nullptr;
     bytes = 0;
-    cudaError_t e = cudaMalloc(&ptr, need);
-    if (e == cudaSuccess) bytes = need;
-    return e;
   }
   ~DeviceScratch() {
     if (ptr) cudaFree(ptr);

@@ -290,6 +290,67 @@ int btam_batch_results_copy(btam_batch *b, int k, double *rho, double *V0, doubl
 /* totals[4 k + c] of every system k; synchronises. */
 int btam_batch_totals_copy(btam_batch *b, double *totals);
 
+/* ---- job server (no counterpart in the reference, which runs one
+ * simulation per MPI job) ---------------------------------------------------
+ * Serves relaxation / master-equation / single-evaluation jobs of any size
+ * concurrently on the current device.  Submission copies the job's inputs;
+ * a job is admitted when a worker is free and its estimated device footprint
+ * (btam_estimate_bytes) fits the memory budget next to the running jobs (a
+ * job may overtake the head of the queue only if it leaves room for the
+ * head).  Each running job owns a system and its stream: its state and
+ * neighbour lists stay resident on the device until it ends, and the work of
+ * all running jobs overlaps on the GPU.  A job's results equal those of the
+ * same job run alone (deterministic kernels, private buffers). */
+typedef struct btam_server btam_server;
+
+#define BTAM_JOB_RELAX 0  /* btam_relax(mode, tol, max_iter, lbfgs_m, bounds) */
+#define BTAM_JOB_DMD 1    /* btam_dmd_setup + btam_dmd_step(precision, nsteps, dmd_params) */
+#define BTAM_JOB_EVAL 2   /* one btam_mf_eval(precision) */
+
+typedef struct btam_job_spec {
+  int kind;        /* BTAM_JOB_* */
+  int precision;   /* BTAM_FP64 / BTAM_FP32C (DMD and EVAL jobs) */
+  int mode;        /* BTAM_RELAX_* (relaxation jobs) */
+  int n;           /* sites */
+  const double *q, *sigma, *x;  /* as btam_system_create */
+  const int *species;
+  const double *beta, *gamma;   /* may be NULL */
+  const double *origin, *cell;  /* [3], [9] */
+  const int *periodic;          /* [3] */
+  double tol;                   /* relaxation tolerance */
+  int max_iter, lbfgs_m;        /* relaxation iterations, history (0: 8) */
+  double sigma_min, sigma_max, x_min;  /* relaxation bounds (0: defaults) */
+  int nsteps;                   /* master-equation steps */
+  double dmd_params[5];         /* dt, Df, dr, min_dx, max_x */
+} btam_job_spec;
+
+typedef struct btam_job_result {
+  int status;      /* BTAM_OK or the first error of the job */
+  int kind;
+  double t_submit, t_admit, t_start, t_end;  /* seconds since server creation */
+  double norm;      /* relaxation: final projected residual norm; EVAL: sum R^2 */
+  double objective; /* relaxation objective; EVAL: sum V0 */
+  int iterations, evaluations, converged;
+  long long h_quanta_hi, h_quanta_lo;  /* DMD: total H quanta (signed 128-bit) */
+} btam_job_result;
+
+/* Device bytes a job of n sites in this cell is admitted against. */
+long long btam_estimate_bytes(int n, const double cell[9], const int periodic[3]);
+/* n_workers concurrent jobs; budget_bytes <= 0 takes 80% of the free memory. */
+int btam_server_create(const btam_tables *t, int n_workers, long long budget_bytes,
+                       btam_server **out);
+/* Queues a job; BTAM_ERR_TOO_LARGE if it can never fit the budget. */
+int btam_server_submit(btam_server *srv, const btam_job_spec *spec, long long *job_id);
+/* Waits (timeout_s < 0: forever; BTAM_ERR_TIMEOUT when it runs out) for a
+ * job, returns its status and copies its result and final state (any pointer
+ * may be NULL).  A result is collected once. */
+int btam_server_wait(btam_server *srv, long long job_id, double timeout_s,
+                     btam_job_result *result, double *q, double *sigma, double *x);
+int btam_server_stats(btam_server *srv, long long *waiting, int *running,
+                      long long *completed, long long *failed, long long *bytes_in_use);
+/* Lets running jobs finish, drops the jobs still queued, joins the workers. */
+int btam_server_destroy(btam_server *srv);
+
 /* ---- measurement (no counterpart in the reference, which has only PETSc's
  * SNES monitor for tracing) ------------------------------------------------ */
 /* One evaluation as btam_mf_eval_async, with CUDA events on the system's

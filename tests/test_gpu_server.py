@@ -1,0 +1,88 @@
+"""Job server: results of every job alone and in a concurrent mix.
+
+Tolerance: none.  A job's kernels are deterministic and touch only its own
+buffers, so its final state, residual norm, objective and hydrogen total must
+be bitwise the same whether it ran alone or overlapped with others."""
+import numpy as np
+import pytest
+
+import btam
+from btam import lattice
+
+pytestmark = pytest.mark.gpu
+
+
+def job_mix():
+    cell = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.4, x_range=(0.2, 0.5),
+                             sigma_range=(0.08, 0.15), jitter=0.02, seed=21)
+    hexa = lattice.supercell(5, 5, 4, ortho=False, h_fraction=0.5, x_range=(0.0, 0.4),
+                             sigma_range=(0.08, 0.15), jitter=0.02, seed=22)
+    sph = lattice.sphere(10.0, T=450.0, h_fraction=0.3, seed=23)
+    sph2 = lattice.sphere(13.0, T=350.0, h_fraction=0.45, seed=24)
+    return [
+        (cell, dict(kind=btam.JOB_RELAX, mode=btam.RELAX_FP32C, tol=1e-5, max_iter=120)),
+        (hexa, dict(kind=btam.JOB_DMD, precision=btam.FP32C, nsteps=20)),
+        (sph, dict(kind=btam.JOB_RELAX, mode=btam.RELAX_MIXED, tol=1e-7, max_iter=200)),
+        (sph2, dict(kind=btam.JOB_DMD, precision=btam.FP64, nsteps=10)),
+        (hexa, dict(kind=btam.JOB_EVAL, precision=btam.FP32C)),
+        (sph2, dict(kind=btam.JOB_EVAL, precision=btam.FP64)),
+    ]
+
+
+KEYS = ("status", "norm", "objective", "iterations", "evaluations", "converged", "h_quanta")
+
+
+def same(a, b):
+    for k in KEYS:
+        assert a[k] == b[k], k
+    for k in ("q", "sigma", "x"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_server_results_alone_equal_in_mix(gpu_tables):
+    jobs = job_mix()
+    alone = []
+    srv = btam.Server(gpu_tables, workers=1)
+    for s, kw in jobs:
+        alone.append(srv.wait(srv.submit(s, **kw)))
+    srv.close()
+    srv = btam.Server(gpu_tables, workers=6)
+    ids = [srv.submit(s, **kw) for s, kw in jobs for _ in range(2)]
+    mixed = [srv.wait(i) for i in ids]
+    st = srv.stats()
+    srv.close()
+    assert st["completed"] >= len(ids) and st["failed"] == 0
+    for k, r in enumerate(mixed):
+        same(alone[k // 2], r)
+    # the jobs did overlap: some job started before another had ended
+    spans = sorted((r["t_start"], r["t_end"]) for r in mixed)
+    assert any(spans[i + 1][0] < spans[i][1] for i in range(len(spans) - 1))
+    # an evaluation job equals the direct evaluation of the system
+    S = btam.System(gpu_tables, jobs[4][0])
+    S.build_neighbors()
+    tot = S.evaluate(btam.FP32C)["totals"]
+    assert alone[4]["objective"] == tot[0] and alone[4]["norm"] == tot[2]
+
+
+def test_server_admission_by_memory(gpu_tables):
+    """A budget that holds about two of these jobs at once: all still finish,
+    never more than the budget is admitted, and a job larger than the whole
+    budget is refused at submission."""
+    s = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.4, x_range=(0.0, 0.3), seed=31)
+    need = btam.estimate_bytes(s)
+    srv = btam.Server(gpu_tables, workers=8, budget_bytes=int(2.5 * need))
+    ids = [srv.submit(s, kind=btam.JOB_DMD, precision=btam.FP32C, nsteps=5) for _ in range(6)]
+    peak = 0
+    out = []
+    for i in ids:
+        peak = max(peak, srv.stats()["bytes_in_use"])
+        out.append(srv.wait(i))
+    assert peak <= int(2.5 * need)
+    for r in out[1:]:
+        assert r["h_quanta"] == out[0]["h_quanta"] and np.array_equal(r["x"], out[0]["x"])
+    big = lattice.supercell(12, 8, 8, ortho=True, h_fraction=0.4, seed=32)
+    assert btam.estimate_bytes(big) > 2.5 * need
+    with pytest.raises(btam.BtamError) as e:
+        srv.submit(big, kind=btam.JOB_EVAL)
+    assert e.value.code == 15
+    srv.close()
