@@ -609,6 +609,176 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
 }
 
 // ---------------------------------------------------------------------------
+// Pass 2, one undirected pair {u, j}: the contributions of j to u's residuals
+// (ou, exactly what pass2_pair returns for (u, j)) and of u to j's residuals
+// (oj, what pass2_pair returns for (j, u)), from the 25 geometries of (u, j)
+// only.  The two directions share every geometry: those of (j, u) are the
+// negated ones of (u, j) with the pair-rule sides and the triplet loops
+// swapped (j's centre-displaced points are u's neighbour-displaced points).
+// Position gradients follow from translation invariance of each pair term,
+//   dV0_j/dq_j|u = -dV0_j/dq_u|u,   dV0_u/dq_j|j = -dV0_u/dq_u|j,
+// so oj.gq = -cros_q - omega_ju self_q; the width and occupancy gradients of
+// j take the sigma_j and x_u derivatives of the same terms (rself_s, rcros_s,
+// rcros_x).  mu, mj: moment records of u and of j's owner; omega_uj =
+// beta_j / beta_u, omega_ju = beta_u / beta_j.
+template <class R>
+BTAM_HD void pass2_pair_sym(const TablesView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
+                            R xj, int cu, int cj, R embq_u, R embx_u, R embq_j, R embx_j,
+                            R omega_uj, R omega_ju, const R *mu, const R *mj,
+                            Pass2Out<R> &ou, Pass2Out<R> &oj) {
+  const int pk = pair_kind(cu, cj);
+  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
+                      &tp = T.t[T_PHI + pk];
+  const SplineView<R> &trj = T.t[cj == 0 ? T_RHO_MG : T_RHO_H];
+  const SplineView<R> &tru = T.t[cu == 0 ? T_RHO_MG : T_RHO_H];
+  const R X = xu * xj;
+  const R w6 = (R)kW6, w9 = (R)kW9;
+
+  // u's view: d/dq_u and d/dsigma_u of V0_u (self) and V0_j (cros), d/dx_u of V0_j
+  R self_q[3] = {0, 0, 0}, self_s = 0;
+  R cros_q[3] = {0, 0, 0}, cros_s = 0, cros_x = 0;
+  // j's view: d/dsigma_j of V0_j (rself_s) and of V0_u (rcros_s), d/dx_j of V0_u
+  R rself_s = 0, rcros_s = 0, rcros_x = 0;
+
+  // ---- 12-point pair rule: side 0 moves u (sigma_u), side 1 moves j (sigma_j)
+  {
+    R rho_u_sum = 0, rho_j_sum = 0, phi_sum = 0, bff_sum = 0;
+    for (int side = 0; side < 2; ++side) {
+      R amt = (side == 0 ? sig_u : -sig_j) * (R)kDelta6;
+      for (int k = 0; k < 3; ++k)
+        for (int sg = 0; sg < 2; ++sg) {
+          R a = sg ? -amt : amt;
+          Geo<R> g;
+          geo_eval(g, disp(r0, k, a), tu, tw);
+          R rj, drj, ru, dru, ph, dph;
+          spline_vd(trj, g.s, rj, drj);
+          spline_vd(tru, g.s, ru, dru);
+          spline_vd(tp, g.s, ph, dph);
+          R bc = bff_grad_coef(g);
+          R c_self = w6 * (embq_u * xj * drj * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
+          R c_cros = w6 * (embq_j * xu * dru * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
+          self_q[0] += c_self * g.r.x; self_q[1] += c_self * g.r.y; self_q[2] += c_self * g.r.z;
+          cros_q[0] += c_cros * g.r.x; cros_q[1] += c_cros * g.r.y; cros_q[2] += c_cros * g.r.z;
+          if (side == 0) {
+            R sd = (sg ? -(R)kDelta6 : (R)kDelta6) * comp(g.r, k);
+            self_s += c_self * sd;
+            cros_s += c_cros * sd;
+          } else {  // r = r0 + (sg ? +1 : -1) sqrt6 sigma_j e_k
+            R sd = (sg ? (R)kDelta6 : -(R)kDelta6) * comp(g.r, k);
+            rself_s += c_cros * sd;
+            rcros_s += c_self * sd;
+          }
+          rho_u_sum += ru;
+          rho_j_sum += rj;
+          phi_sum += ph;
+          bff_sum += bff(g);
+        }
+    }
+    cros_x += w6 * (embx_j * rho_u_sum + (R)0.5 * xj * phi_sum + (R)2 * X * xj * bff_sum);
+    rcros_x += w6 * (embx_u * rho_j_sum + (R)0.5 * xu * phi_sum + (R)2 * X * xu * bff_sum);
+  }
+
+  // ---- triplet geometries
+  Geo<R> gc;
+  geo_eval(gc, r0, tu, tw);
+  const Dual<R> Xf0 = dual_feat(gc, X);
+  const R sfac = (R)2 * w9 * X;
+  // A: u displaced by +-3 sigma_u e_k (j's neighbour-displaced points)
+  Feat<R> FA{};
+  {
+    const Dual<R> Dj_g0 = dual_at<R, true>(mj + kMomG0);
+    const Dual<R> Dc5 = dual_sub(dual_flip(Dj_g0), Xf0);
+    const DualAx<R> c5 = dual_ax(Dc5, r0);
+    const DualAx<R> x5 = dual_ax(dual_sub(Dc5, Xf0), r0);
+    const R amt = sig_u * (R)kDelta9;
+    for (int k = 0; k < 3; ++k)
+      for (int sg = 0; sg < 2; ++sg) {
+        const R a = sg ? -amt : amt;
+        Geo<R> g;
+        geo_eval(g, disp(r0, k, a), tu, tw);
+        feat_add(FA, g);
+        R hb = (R)0.5 * X * bff_grad_coef(g);
+        V3<R> v4;
+        R f4u;
+        dual_Jf(dual_at<R, true>(mu + kMomGd + 9 * (2 * k + sg)), g, v4, f4u);  // S4
+        V3<R> v5, vx;
+        R f5, fx;
+        dual_ax_at(c5, k, a, g, v5, f5);  // C5
+        dual_ax_at(x5, k, a, g, vx, fx);  // X5
+        V3<R> s4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
+        self_q[0] += sfac * s4.x; self_q[1] += sfac * s4.y; self_q[2] += sfac * s4.z;
+        cros_q[0] += sfac * v5.x; cros_q[1] += sfac * v5.y; cros_q[2] += sfac * v5.z;
+        R sd = sg ? -(R)kDelta9 : (R)kDelta9;
+        self_s += sfac * comp(s4, k) * sd;
+        cros_s += sfac * comp(v5, k) * sd;
+        cros_x += (R)2 * w9 * xj * fx;
+        // j's view: u's centre-displaced term as a function of x_j
+        rcros_x += (R)2 * w9 * xu * (f4u - X * bff(g));
+      }
+  }
+  // B: j displaced by -+3 sigma_j e_k (j's centre-displaced points)
+  Feat<R> FB{};
+  {
+    const Dual<R> Du_g0 = dual_at<R, true>(mu + kMomG0);
+    const DualAx<R> s5 = dual_ax(dual_sub(Du_g0, Xf0), r0);
+    const DualAx<R> xf = dual_ax(Xf0, r0);
+    const R amt = sig_j * (R)kDelta9;
+    for (int k = 0; k < 3; ++k)
+      for (int sg = 0; sg < 2; ++sg) {
+        const R a = sg ? amt : -amt;
+        Geo<R> g;
+        geo_eval(g, disp(r0, k, a), tu, tw);
+        feat_add(FB, g);
+        V3<R> v5, vxf;
+        R f5, fxf;
+        dual_ax_at(s5, k, a, g, v5, f5);  // S5
+        dual_ax_at(xf, k, a, g, vxf, fxf);
+        self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
+        const Dual<R> Pj = dual_flip(dual_at<R, true>(mj + kMomGd + 9 * (2 * k + sg)));
+        V3<R> v4;
+        R f4;
+        dual_Jf(Pj, g, v4, f4);  // C4
+        R hb = (R)0.5 * X * bff_grad_coef(g);
+        V3<R> c4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
+        cros_q[0] += sfac * c4.x; cros_q[1] += sfac * c4.y; cros_q[2] += sfac * c4.z;
+        R bffg = bff(g);
+        cros_x += (R)2 * w9 * xj * (f4 - X * bffg);
+        R sd = sg ? (R)kDelta9 : -(R)kDelta9;
+        rself_s += sfac * comp(c4, k) * sd;
+        rcros_s += sfac * comp(v5, k) * sd;
+        // j's view: u's neighbour-displaced term as a function of x_j
+        rcros_x += (R)2 * w9 * xu * (f5 - fxf);
+      }
+  }
+  // centre-geometry pieces
+  {
+    Dual<R> dFB = dual_of<R, R>(FB.a, FB.l);
+    Dual<R> dFA = dual_of<R, R>(FA.a, FA.l);
+    for (int k = 0; k < 3; ++k) {
+      dFB.a[k] *= X; dFB.d[k] *= X; dFB.o[k] *= X;
+      dFA.a[k] *= X; dFA.d[k] *= X; dFA.o[k] *= X;
+    }
+    const Dual<R> Dj_h = dual_at<R, true>(mj + kMomH);
+    const Dual<R> Du_h = dual_at<R, true>(mu + kMomH);
+    V3<R> vs = dual_J(dual_sub(Du_h, dFB), gc);
+    V3<R> vc = dual_J(dual_sub(dual_flip(Dj_h), dFA), gc);
+    self_q[0] += sfac * vs.x; self_q[1] += sfac * vs.y; self_q[2] += sfac * vs.z;
+    cros_q[0] += sfac * vc.x; cros_q[1] += sfac * vc.y; cros_q[2] += sfac * vc.z;
+    cros_x += (R)2 * w9 * xj * dual_f(dual_flip(Dj_h), gc);
+    rcros_x += (R)2 * w9 * xu * dual_f(Du_h, gc);
+  }
+
+  for (int k = 0; k < 3; ++k) {
+    ou.gq[k] += self_q[k] + omega_uj * cros_q[k];
+    oj.gq[k] += -cros_q[k] - omega_ju * self_q[k];
+  }
+  ou.gs += self_s + omega_uj * cros_s;
+  ou.gx += omega_uj * cros_x;
+  oj.gs += rself_s + omega_ju * rcros_s;
+  oj.gx += omega_ju * rcros_x;
+}
+
+// ---------------------------------------------------------------------------
 // Per-site epilogue of pass 1, in double.  Inputs are the raw sums over the
 // site's active neighbours (Pass1A fields and the six G(d) sums).
 struct SiteSums {

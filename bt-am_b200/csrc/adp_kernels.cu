@@ -76,6 +76,9 @@ pass1_kernel(const EvalArgs<R> a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // grid-stride over sites: one site per warp per trip (a full grid makes one
   // trip; a persistent grid of a few blocks per SM makes several)
+  // one copy of the body for every trip: a site or pair gives the same bits
+  // whichever trip of whichever grid computes it
+#pragma unroll 1
   for (int i = blockIdx.x * W + warp; i < a.n_real; i += gridDim.x * W) {
   R *mom = a.mom + (size_t)i * kMomStride;
   const double2 xbi = a.xb[i];
@@ -186,6 +189,9 @@ __global__ void __launch_bounds__(W * 32, MB)
 pass2_kernel(const EvalArgs<R> a) {
   __shared__ R mu_s[W][kMomStride];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // one copy of the body for every trip: a site or pair gives the same bits
+  // whichever trip of whichever grid computes it
+#pragma unroll 1
   for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
   const double2 xbu = a.xb[u];
   const double xu = xbu.x;
@@ -237,6 +243,115 @@ pass2_kernel(const EvalArgs<R> a) {
       atomicOr(a.err, 1 << kErrBitNonFinite);
   }
   __syncwarp();  // mu_s is reloaded for the warp's next site
+  }
+}
+
+// ---- undirected pass 2 ------------------------------------------------------
+// 256-bit record store/load of one slot (8 R).
+__device__ __forceinline__ void st_rec(float *p, const float (&v)[8]) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]),
+               "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void st_rec(double *p, const double (&v)[8]) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
+               "d"(v[2]), "d"(v[3])
+               : "memory");
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p + 4), "d"(v[4]), "d"(v[5]),
+               "d"(v[6]), "d"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void ld_rec(const float *p, float (&v)[8]) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+                 "=f"(v[6]), "=f"(v[7])
+               : "l"(p));
+}
+__device__ __forceinline__ void ld_rec(const double *p, double (&v)[8]) {
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+               : "l"(p));
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
+               : "l"(p + 4));
+}
+
+// One thread per owned slot p = (u, j): both directions of the pair from its
+// 25 geometries (pass2_pair_sym); u's part into slot p, j's part into the
+// reverse slot.  Pairs with an empty site give zero records, so every slot
+// of the real sites' lists is written exactly once per evaluation.
+template <class R, int TPB, int MB>
+__global__ void __launch_bounds__(TPB, MB)
+pass2u_pair_kernel(const EvalArgs<R> a) {
+  // one copy of the body for every trip: a site or pair gives the same bits
+  // whichever trip of whichever grid computes it
+#pragma unroll 1
+  for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
+    const int p = a.own_p[t], u = a.own_u[t];
+    const int j = a.idx[p], r = a.rev[p];
+    const double2 xbu = a.xb[u], xbj = a.xb[j];
+    R vu[8], vj[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) vu[c] = vj[c] = (R)0;
+    if (!(xbu.x < kMinOcc) && !(xbj.x < kMinOcc)) {
+      const int o = a.owner[j];
+      const double4 qu = a.pos[u], qj = a.pos[j];
+      const R *mu = a.mom + (size_t)u * kMomStride;
+      const R *mj = a.mom + (size_t)o * kMomStride;
+      Pass2Out<R> ou, oj;
+      ou.gq[0] = ou.gq[1] = ou.gq[2] = ou.gs = ou.gx = (R)0;
+      oj.gq[0] = oj.gq[1] = oj.gq[2] = oj.gs = oj.gx = (R)0;
+      pass2_pair_sym<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
+                        a.code[u], a.code[j], ld_ro(mu), ld_ro(mu + 1), ld_ro(mj),
+                        ld_ro(mj + 1), (R)(xbj.y / xbu.y), (R)(xbu.y / xbj.y), mu, mj, ou, oj);
+      vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
+      vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
+    }
+    st_rec(a.pbuf + 8 * (size_t)p, vu);
+    if (r >= 0) st_rec(a.pbuf + 8 * (size_t)r, vj);
+  }
+}
+
+// One warp per site: compensated sum of its slot records in slot order,
+// then the same epilogue as the directed kernel.
+template <class R, int W>
+__global__ void __launch_bounds__(W * 32)
+pass2u_site_kernel(const EvalArgs<R> a) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // one copy of the body for every trip: a site or pair gives the same bits
+  // whichever trip of whichever grid computes it
+#pragma unroll 1
+  for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
+    const double2 xbu = a.xb[u];
+    const double xu = xbu.x;
+    if (xu < kMinOcc) {
+      if (lane == 0) {
+        a.Rq[3 * u] = a.Rq[3 * u + 1] = a.Rq[3 * u + 2] = 0.0;
+        a.Rs[u] = a.Rx[u] = 0.0;
+      }
+      continue;
+    }
+    Acc<R> acc[5];
+    for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
+      R v[8];
+      ld_rec(a.pbuf + 8 * (size_t)p, v);
+#pragma unroll
+      for (int c = 0; c < 5; ++c) acc[c].add(v[c]);
+    }
+    double t[5];
+#pragma unroll
+    for (int c = 0; c < 5; ++c) t[c] = warp_sum(acc[c].get());
+    if (lane == 0) {
+      double gs = t[3], gx = t[4];
+      residual_epilogue(a.pos[u].w, xu, a.code[u], xbu.y, a.gamma[u], a.selfx[u], gs, gx);
+      a.Rq[3 * u] = t[0];
+      a.Rq[3 * u + 1] = t[1];
+      a.Rq[3 * u + 2] = t[2];
+      a.Rs[u] = gs;
+      a.Rx[u] = gx;
+      if (!(finite(t[0]) && finite(t[1]) && finite(t[2]) && finite(gs) && finite(gx)))
+        atomicOr(a.err, 1 << kErrBitNonFinite);
+    }
   }
 }
 
@@ -349,9 +464,38 @@ template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t s
   }
   return cudaGetLastError();
 }
+template <class R, int TPB, int MB> void go2u(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
+  auto k = pass2u_pair_kernel<R, TPB, MB>;
+  int g = nblocks(a.n_own, TPB);
+  if (pers) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TPB, 0);
+    int gp = sms * (per > 0 ? per : 1);
+    g = gp < g ? gp : g;
+  }
+  if (g > 0) k<<<g, TPB, 0, st>>>(a);
+  auto ks = pass2u_site_kernel<R, 4>;
+  ks<<<grid_of(ks, a.n_real, 4, pers), 128, 0, st>>>(a);
+}
+
 template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v) {
   if (a.n_real <= 0) return cudaSuccess;
   const bool pers = (v & kPersistent) != 0;
+  if (v & kUndirected) {
+    if (!has_undirected(a.rev, a.pbuf)) {
+      go2<R, 4, 1>(a, st, false);
+      return cudaGetLastError();
+    }
+    switch (v & (kPersistent - 1)) {
+    case 1: go2u<R, 128, 3>(a, st, pers); break;
+    case 2: go2u<R, 128, 4>(a, st, pers); break;
+    case 3: go2u<R, 256, 2>(a, st, pers); break;
+    default: go2u<R, 128, 1>(a, st, pers); break;
+    }
+    return cudaGetLastError();
+  }
   switch (v & (kPersistent - 1)) {
   case 1: go2<R, 4, 3>(a, st, pers); break;
   case 2: go2<R, 4, 4>(a, st, pers); break;
@@ -407,6 +551,13 @@ cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int
       float t = time_one(true, v | (p ? kPersistent : 0));
       if (t < t2) { t2 = t; b2 = v | (p ? kPersistent : 0); }
     }
+  if (has_undirected(a.rev, a.pbuf))
+    for (int p = 0; p < 2; ++p)
+      for (int v = 0; v < kPass2UVariants && e == cudaSuccess; ++v) {
+        const int var = v | kUndirected | (p ? kPersistent : 0);
+        float t = time_one(true, var);
+        if (t < t2) { t2 = t; b2 = var; }
+      }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e == cudaSuccess) {

@@ -25,6 +25,12 @@ template <class R> struct EvalArgs {
   double *rho, *V0, *S0, *selfx;  // [real]
   double *Rq, *Rs, *Rx;           // [3*real], [real], [real]
   int *err;
+  // undirected pass 2 (optional; nullptr / 0 when absent)
+  const int *rev = nullptr;    // reverse slot of each real-site slot, -1 if none
+  const int *own_p = nullptr;  // owned slots
+  const int *own_u = nullptr;  // their sites
+  int n_own = 0;
+  R *pbuf = nullptr;           // 8 R per slot: gq[3], gs, gx, 0, 0, 0
 };
 
 // Pass 1: rho-bar, V0, S0, dV0/dx (self) and the moment record of every
@@ -35,14 +41,27 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0)
 template <class R>
 cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
 // variant = shape | kPersistent (persistent grid of resident blocks)
+//           [| kUndirected for pass 2: each pair once, both directions]
 constexpr int kPass1Variants = 5;  // shapes (4 warps,-), (4,3), (4,4), (8,2), (2,8)
 constexpr int kPass2Variants = 6;  // shapes (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
+constexpr int kPass2UVariants = 4;  // undirected pair kernel (threads, min blocks): (128,-), (128,3), (128,4), (256,2)
 constexpr int kPersistent = 8;
+constexpr int kUndirected = 16;
 inline bool valid_variants(int v1, int v2) {
-  return v1 >= 0 && v2 >= 0 && (v1 & ~(2 * kPersistent - 1)) == 0 &&
-         (v2 & ~(2 * kPersistent - 1)) == 0 && (v1 & (kPersistent - 1)) < kPass1Variants &&
-         (v2 & (kPersistent - 1)) < kPass2Variants;
+  if (v1 < 0 || v2 < 0 || (v1 & ~(2 * kPersistent - 1)) != 0 ||
+      (v2 & ~(2 * kUndirected - 1)) != 0)
+    return false;
+  const int s2 = v2 & (kPersistent - 1);
+  return (v1 & (kPersistent - 1)) < kPass1Variants &&
+         s2 < ((v2 & kUndirected) ? kPass2UVariants : kPass2Variants);
 }
+
+// Undirected pass 2 in two launches: the pair kernel (one thread per owned
+// slot: both directions of the pair into the slot buffer) and the site
+// kernel (one warp per site: the sum over its slots and the epilogue).
+// Needs a.rev, a.own_p, a.own_u and a.pbuf; launch_pass2 falls back to the
+// directed default when they are absent.
+inline bool has_undirected(const void *rev, const void *pbuf) { return rev && pbuf; }
 
 // Times every pass-1 and pass-2 variant on this input (reps launches each,
 // synchronising st) and returns the fastest of each.  Every variant computes

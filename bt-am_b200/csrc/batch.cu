@@ -51,6 +51,12 @@ __global__ void shift_offs_kernel(int n, const int *src, int *dst, int base) {
   if (i < n) dst[i] = base + src[i];
 }
 
+// Reverse slots keep -1 (no reverse pair) and move by the pair base otherwise.
+__global__ void shift_rev_kernel(long long n, const int *src, int *dst, int base) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i] < 0 ? -1 : base + src[i];
+}
+
 inline int blocks_of(long long n, int per) { return (int)((n + per - 1) / per); }
 
 }  // namespace
@@ -71,6 +77,11 @@ struct btam_batch {
   int *code = nullptr, *owner = nullptr;
   double *gamma = nullptr;
   int *offs = nullptr, *idx = nullptr;
+  // undirected pass 2: reverse slots, owned slots and their sites, slot buffer
+  int *rev = nullptr, *own_p = nullptr, *own_u = nullptr;
+  int n_own = 0;
+  char *pbuf = nullptr;
+  size_t pbuf_bytes = 0, pbuf_elem = 0;
   double *rho = nullptr, *V0 = nullptr, *S0 = nullptr, *selfx = nullptr, *Rq = nullptr,
          *Rs = nullptr, *Rx = nullptr, *totals = nullptr;
   double *mom64 = nullptr;
@@ -82,6 +93,7 @@ struct btam_batch {
   // instantiated graph per form and the variants it was captured with
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   int exec_v1[2] = {-1, -1}, exec_v2[2] = {-1, -1};
+  const char *exec_pbuf[2] = {nullptr, nullptr};  // slot buffer the graph writes
 };
 
 namespace {
@@ -110,7 +122,22 @@ template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const TablesVie
   a.Rs = b->Rs;
   a.Rx = b->Rx;
   a.err = b->err;
+  a.rev = b->rev;
+  a.own_p = b->own_p;
+  a.own_u = b->own_u;
+  a.n_own = b->n_own;
+  a.pbuf = reinterpret_cast<R *>(b->pbuf);
   return a;
+}
+
+int batch_pbuf(btam_batch *b, size_t elem) {
+  if (elem < b->pbuf_elem) elem = b->pbuf_elem;
+  const size_t need = (size_t)(b->n_pairs > 0 ? b->n_pairs : 1) * 8 * elem;
+  b->pbuf_elem = elem;
+  if (need <= b->pbuf_bytes) return BTAM_OK;
+  BTAM_TRY(dalloc(b->pbuf, b->st, need));
+  b->pbuf_bytes = need;
+  return BTAM_OK;
 }
 
 int batch_read_err(btam_batch *b) {
@@ -164,6 +191,10 @@ void free_batch(btam_batch *b) {
   dfree(b->mom64, b->st);
   dfree(b->mom32, b->st);
   dfree(b->err, b->st);
+  dfree(b->rev, b->st);
+  dfree(b->own_p, b->st);
+  dfree(b->own_u, b->st);
+  dfree(b->pbuf, b->st);
   if (b->ev) cudaEventDestroy(b->ev);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
@@ -193,6 +224,8 @@ int batch_build(btam_batch *b) {
     n_pairs += last;
   }
   seg[ns] = (int)n_real;
+  long long own_total = 0;
+  for (int k = 0; k < ns; ++k) own_total += b->sys[k]->n_own;
   long long gacc = 0;
   for (int k = 0; k < ns; ++k) {
     b->base_img[k] = (int)(n_real + gacc);
@@ -219,9 +252,14 @@ int batch_build(btam_batch *b) {
   BTAM_TRY(dalloc(b->Rx, b->st, nr));
   BTAM_TRY(dalloc(b->totals, b->st, 4 * (size_t)ns));
   BTAM_TRY(dalloc(b->err, b->st, 1));
+  BTAM_TRY(dalloc(b->rev, b->st, (size_t)n_pairs));
+  BTAM_TRY(dalloc(b->own_p, b->st, (size_t)own_total));
+  BTAM_TRY(dalloc(b->own_u, b->st, (size_t)own_total));
+  b->n_own = (int)own_total;
   BTAM_TRY(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
   BTAM_TRY(cudaMemcpyAsync(b->seg, seg.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice,
                            b->st));
+  long long own_base = 0;
   for (int k = 0; k < ns; ++k) {
     btam_system *s = b->sys[k];
     const int n = s->n_real, g = s->n_ghost, R = b->base_real[k], G = b->base_img[k];
@@ -238,9 +276,19 @@ int batch_build(btam_batch *b) {
                                                                   b->owner + G, n, R);
     shift_offs_kernel<<<blocks_of(n, 256), 256, 0, b->st>>>(n, s->offs, b->offs + R,
                                                              (int)b->base_pair[k]);
-    if (n_list_pairs[k] > 0)
+    if (n_list_pairs[k] > 0) {
       remap_idx_kernel<<<blocks_of(n_list_pairs[k], 256), 256, 0, b->st>>>(
           n_list_pairs[k], s->idx, b->idx + b->base_pair[k], n, R, G);
+      shift_rev_kernel<<<blocks_of(n_list_pairs[k], 256), 256, 0, b->st>>>(
+          n_list_pairs[k], s->rev, b->rev + b->base_pair[k], (int)b->base_pair[k]);
+    }
+    if (s->n_own > 0) {
+      shift_offs_kernel<<<blocks_of(s->n_own, 256), 256, 0, b->st>>>(
+          s->n_own, s->own_p, b->own_p + own_base, (int)b->base_pair[k]);
+      shift_offs_kernel<<<blocks_of(s->n_own, 256), 256, 0, b->st>>>(
+          s->n_own, s->own_u, b->own_u + own_base, R);
+      own_base += s->n_own;
+    }
     BTAM_TRY(cudaGetLastError());
   }
   const int tail = (int)n_pairs;
@@ -270,7 +318,8 @@ int ensure_moments(btam_batch *b, int precision) {
 // when the launch variants changed since the last capture).
 int ensure_graph(btam_batch *b, int precision) {
   const int f = precision == BTAM_FP64 ? 0 : 1;
-  if (b->exec[f] && b->exec_v1[f] == b->variant1[f] && b->exec_v2[f] == b->variant2[f])
+  if (b->exec[f] && b->exec_v1[f] == b->variant1[f] && b->exec_v2[f] == b->variant2[f] &&
+      b->exec_pbuf[f] == b->pbuf)
     return BTAM_OK;
   if (b->exec[f]) {
     cudaGraphExecDestroy(b->exec[f]);
@@ -290,6 +339,7 @@ int ensure_graph(btam_batch *b, int precision) {
   }
   b->exec_v1[f] = b->variant1[f];
   b->exec_v2[f] = b->variant2[f];
+  b->exec_pbuf[f] = b->pbuf;
   return BTAM_OK;
 }
 
@@ -357,6 +407,8 @@ int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *p
   int st = ensure_moments(b, precision);
   if (st != BTAM_OK) return st;
   const int f = precision == BTAM_FP64 ? 0 : 1;
+  st = batch_pbuf(b, f == 0 ? sizeof(double) : sizeof(float));
+  if (st != BTAM_OK) return st;
   int v1 = 0, v2 = 0;
   cudaError_t e = f == 0 ? autotune_passes(batch_args<double>(b, b->mom64, b->T->v64), b->st, 3,
                                            &v1, &v2)
@@ -365,6 +417,10 @@ int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *p
   if (e != cudaSuccess) return cuda_status(e);
   b->variant1[f] = v1;
   b->variant2[f] = v2;
+  if (!((b->variant2[0] | b->variant2[1]) & kUndirected)) {
+    dfree(b->pbuf, b->st);
+    b->pbuf_bytes = b->pbuf_elem = 0;
+  }
   if (pass1_variant) *pass1_variant = v1;
   if (pass2_variant) *pass2_variant = v2;
   return batch_read_err(b);
@@ -373,6 +429,10 @@ int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *p
 int btam_batch_set_variants(btam_batch *b, int precision, int pass1_variant, int pass2_variant) {
   if (!b || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
   if (!valid_variants(pass1_variant, pass2_variant)) return BTAM_ERR_ARG;
+  if (pass2_variant & kUndirected) {
+    int st = batch_pbuf(b, precision == BTAM_FP64 ? sizeof(double) : sizeof(float));
+    if (st != BTAM_OK) return st;
+  }
   const int f = precision == BTAM_FP64 ? 0 : 1;
   b->variant1[f] = pass1_variant;
   b->variant2[f] = pass2_variant;

@@ -205,7 +205,24 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesVie
   a.Rs = s->Rs;
   a.Rx = s->Rx;
   a.err = s->err;
+  a.rev = s->rev;
+  a.own_p = s->own_p;
+  a.own_u = s->own_u;
+  a.n_own = s->n_own;
+  a.pbuf = reinterpret_cast<R *>(s->pbuf);
   return a;
+}
+
+// Slot buffer of the undirected pass 2: 8 values of R per slot of the real
+// sites' lists, allocated only when an undirected variant is in use.
+int ensure_pbuf(btam_system *s, size_t elem) {
+  if (elem < s->pbuf_elem) elem = s->pbuf_elem;
+  const size_t need = (size_t)(s->n_pairs > 0 ? s->n_pairs : 1) * 8 * elem;
+  s->pbuf_elem = elem;
+  if (need <= s->pbuf_bytes) return BTAM_OK;
+  BTAM_TRY(dalloc(s->pbuf, s->st, need));
+  s->pbuf_bytes = need;
+  return BTAM_OK;
 }
 
 }  // namespace
@@ -432,6 +449,8 @@ void btam_system_destroy(btam_system *s) {
   dfree(s->mom64, s->st); dfree(s->mom32, s->st); dfree(s->err, s->st);
   dfree(s->doffs, s->st); dfree(s->didx, s->st); dfree(s->X, s->st); dfree(s->X0, s->st); dfree(s->dtot, s->st); dfree(s->mu, s->st);
   dfree(s->dact, s->st); dfree(s->ddeg, s->st); dfree(s->rv, s->st);
+  dfree(s->rev, s->st); dfree(s->own_off, s->st); dfree(s->own_p, s->st); dfree(s->own_u, s->st);
+  dfree(s->pbuf, s->st);
   s->scratch.release(s->st);
   if (s->st) cudaStreamSynchronize(s->st);
   if (s->st) cudaStreamDestroy(s->st);
@@ -527,6 +546,21 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
   if (st != BTAM_OK) return st;
   s->n_list = n_query;
   s->n_pairs = total;
+  // reverse slots and owned pairs for the undirected pass 2
+  if (total > s->rev_cap) {
+    BTAM_TRY(dalloc(s->rev, s->st, total));
+    s->rev_cap = total;
+  }
+  if (n + 1 > s->own_off_cap) {
+    BTAM_TRY(dalloc(s->own_off, s->st, n + 1));
+    s->own_off_cap = n + 1;
+  }
+  BTAM_TRY(launch_pair_links(n, s->offs, s->idx, s->owner, s->rev, s->cnt, s->own_off, s->own_p,
+                             s->own_u, s->own_cap, &s->n_own, s->scratch, s->st));
+  if (s->pbuf_elem > 0) {  // a rebuilt list may be longer than the slot buffer
+    int st2 = ensure_pbuf(s, s->pbuf_elem);
+    if (st2 != BTAM_OK) return st2;
+  }
   s->built = true;
   return BTAM_OK;
 }
@@ -668,14 +702,21 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
   int st;
   if (precision == BTAM_FP64) {
     if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
+    if ((st = ensure_pbuf(s, sizeof(double))) != BTAM_OK) return st;
     st = autotune_form(s, eval_args<double>(s, s->mom64, s->T->v64), 0, 3);
   } else if (precision == BTAM_FP32C) {
     if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
+    if ((st = ensure_pbuf(s, sizeof(float))) != BTAM_OK) return st;
     st = autotune_form(s, eval_args<float>(s, s->mom32, s->T->v32), 1, 3);
   } else {
     return BTAM_ERR_ARG;
   }
   if (st != BTAM_OK) return st;
+  // the slot buffer stays only while an undirected variant is selected
+  if (!((s->variant2[0] | s->variant2[1]) & kUndirected)) {
+    dfree(s->pbuf, s->st);
+    s->pbuf_bytes = s->pbuf_elem = 0;
+  }
   const int f = precision == BTAM_FP64 ? 0 : 1;
   if (pass1_variant) *pass1_variant = s->variant1[f];
   if (pass2_variant) *pass2_variant = s->variant2[f];
@@ -685,6 +726,11 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
 int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass2_variant) {
   if (!s || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
   if (!valid_variants(pass1_variant, pass2_variant)) return BTAM_ERR_ARG;
+  if (pass2_variant & kUndirected) {
+    if (!s->built) return BTAM_ERR_NOT_BUILT;
+    int st = ensure_pbuf(s, precision == BTAM_FP64 ? sizeof(double) : sizeof(float));
+    if (st != BTAM_OK) return st;
+  }
   const int f = precision == BTAM_FP64 ? 0 : 1;
   s->variant1[f] = pass1_variant;
   s->variant2[f] = pass2_variant;

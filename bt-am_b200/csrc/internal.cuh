@@ -69,6 +69,12 @@ struct btam_system {
   // relaxation work vectors
   int relax_m = 0;
   double *rv = nullptr;  // one block holding every relaxation vector
+  // pair links and slot buffer of the undirected pass 2
+  int *rev = nullptr, *own_off = nullptr, *own_p = nullptr, *own_u = nullptr;
+  long long rev_cap = 0, own_cap = 0;
+  int own_off_cap = 0, n_own = 0;
+  char *pbuf = nullptr;
+  size_t pbuf_bytes = 0, pbuf_elem = 0;  // bytes; bytes per value (0: none yet)
 };
 
 

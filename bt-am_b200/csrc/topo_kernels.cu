@@ -361,6 +361,100 @@ cudaError_t launch_neighbors(const NbrArgs &a, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// ---- pair links --------------------------------------------------------
+// Slot of the entry of o's (ascending) list whose owner is u: a binary search
+// for u itself when the pair is between real sites, else a scan of o's image
+// entries (indices >= n_real, at the end of the list).
+__device__ int reverse_slot(int u, bool real_pair, int o, int n_real, const int *offs,
+                            const int *idx, const int *owner) {
+  int lo = offs[o], hi = offs[o + 1];
+  int a = lo, b = hi;  // first entry >= (real_pair ? u : n_real)
+  const int key = real_pair ? u : n_real;
+  while (a < b) {
+    int m = (a + b) >> 1;
+    if (idx[m] < key) a = m + 1;
+    else b = m;
+  }
+  if (real_pair) return (a < hi && idx[a] == u) ? a : -1;
+  for (int t = a; t < hi; ++t)
+    if (owner[idx[t]] == u) return t;
+  return -1;
+}
+
+__global__ void pair_rev_kernel(int n_real, const int *offs, const int *idx, const int *owner,
+                                int *rev, int *own_cnt) {
+  const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (u >= n_real) return;
+  int cnt = 0;
+  for (int base = offs[u]; base < offs[u + 1]; base += 32) {
+    int p = base + lane;
+    bool own = false;
+    if (p < offs[u + 1]) {
+      int j = idx[p], o = owner[j];
+      int r = reverse_slot(u, j < n_real, o, n_real, offs, idx, owner);
+      rev[p] = r;
+      own = (u < o) || r < 0;
+    }
+    cnt += __popc(__ballot_sync(0xffffffffu, own));
+  }
+  if (lane == 0) own_cnt[u] = cnt;
+}
+
+__global__ void pair_own_kernel(int n_real, const int *offs, const int *idx, const int *owner,
+                                const int *rev, const int *own_off, int *own_p, int *own_u) {
+  const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (u >= n_real) return;
+  int at = own_off[u];
+  for (int base = offs[u]; base < offs[u + 1]; base += 32) {
+    int p = base + lane;
+    bool own = false;
+    if (p < offs[u + 1]) own = (u < owner[idx[p]]) || rev[p] < 0;
+    unsigned m = __ballot_sync(0xffffffffu, own);
+    if (own) {
+      int k = at + __popc(m & ((1u << lane) - 1u));
+      own_p[k] = p;
+      own_u[k] = u;
+    }
+    at += __popc(m);
+  }
+}
+
+cudaError_t launch_pair_links(int n_real, const int *offs, const int *idx, const int *owner,
+                              int *rev, int *own_cnt, int *own_off, int *&own_p, int *&own_u,
+                              long long &own_cap, int *n_own, DeviceScratch &scratch,
+                              cudaStream_t st) {
+  cudaError_t e;
+  *n_own = 0;
+  if (n_real <= 0) return cudaSuccess;
+  const int blocks = (int)(((long long)n_real * 32 + 127) / 128);
+  pair_rev_kernel<<<blocks, 128, 0, st>>>(n_real, offs, idx, owner, rev, own_cnt);
+  if ((e = cudaMemsetAsync(own_cnt + n_real, 0, sizeof(int), st)) != cudaSuccess) return e;
+  if ((e = exclusive_scan(own_cnt, own_off, n_real + 1, scratch, st)) != cudaSuccess) return e;
+  int total = 0;
+  if ((e = cudaMemcpyAsync(&total, own_off + n_real, sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  if (total > own_cap) {
+    cudaMemPool_t pool = device_pool();
+    if (!pool) return cudaErrorMemoryAllocation;
+    if (own_p) cudaFreeAsync(own_p, st);
+    if (own_u) cudaFreeAsync(own_u, st);
+    own_p = own_u = nullptr;
+    own_cap = 0;
+    if ((e = cudaMallocFromPoolAsync((void **)&own_p, (size_t)total * sizeof(int), pool, st)) !=
+        cudaSuccess)
+      return e;
+    if ((e = cudaMallocFromPoolAsync((void **)&own_u, (size_t)total * sizeof(int), pool, st)) !=
+        cudaSuccess)
+      return e;
+    own_cap = total;
+  }
+  pair_own_kernel<<<blocks, 128, 0, st>>>(n_real, offs, idx, owner, rev, own_off, own_p, own_u);
+  *n_own = total;
+  return cudaGetLastError();
+}
+
 cudaError_t launch_compact(int n_query, const int *tmp, const int *offs, int *idx,
                            cudaStream_t st) {
   if (n_query > 0)

@@ -93,6 +93,18 @@ cudaError_t launch_ghost_refresh(int n_real, int n_ghost, double4 *pos, double2 
                                  int *code, const int *owner, const char4 *image,
                                  const GhostBox &b, cudaStream_t st);
 cudaError_t launch_neighbors(const NbrArgs &a, cudaStream_t st);
+// Pair links of the real sites' neighbour lists for the undirected pass 2:
+// rev[p] = the slot of the reverse pair (o, copy of u) in the list of o =
+// owner of idx[p], or -1 if o's list lacks it (rounding at exactly rc for an
+// image pair); slot p is owned by its site u when u < o or rev[p] < 0, and the
+// owned slots are listed as (own_p, own_u) in site-then-slot order.
+// own_cnt / own_off: n_real + 1 ints of scratch; *n_own returned after a
+// stream synchronisation.
+cudaError_t launch_pair_links(int n_real, const int *offs, const int *idx, const int *owner,
+                              int *rev, int *own_cnt, int *own_off, int *&own_p, int *&own_u,
+                              long long &own_cap, int *n_own, DeviceScratch &scratch,
+                              cudaStream_t st);
+
 cudaError_t launch_compact(int n_query, const int *tmp, const int *offs, int *idx,
                            cudaStream_t st);
 

@@ -32,7 +32,7 @@ template <> TablesView<float> view<float>() {
 }
 
 template <class R>
-void run(int n_all, int n_real, const double *q, const double *sigma,
+void run(bool sym, int n_all, int n_real, const double *q, const double *sigma,
          const double *x, const int *code, const double *beta,
          const double *gamma, const int *owner, const int *offs,
          const int *idx, double *rho, double *V0, double *S0, double *selfx,
@@ -79,6 +79,50 @@ void run(int n_all, int n_real, const double *q, const double *sigma,
     sx[i] = res.selfx;
   }
   for (size_t k = 0; k < mom.size(); ++k) momR[k] = (R)mom[k];
+  if (sym) {
+    // undirected pairs: each owned slot (u < owner of j) gives both
+    // directions; slot values are summed per site in slot order
+    std::vector<Pass2Out<R>> buf(offs[n_real]);
+    std::vector<int> rev(offs[n_real], -1);
+    for (int u = 0; u < n_real; ++u)
+      for (int p = offs[u]; p < offs[u + 1]; ++p) {
+        int o = owner[idx[p]];
+        for (int t = offs[o]; t < offs[o + 1]; ++t)
+          if (owner[idx[t]] == u) rev[p] = t;
+      }
+    for (auto &b : buf) b = Pass2Out<R>{};
+    for (int u = 0; u < n_real; ++u)
+      for (int p = offs[u]; p < offs[u + 1]; ++p) {
+        int j = idx[p], o = owner[j];
+        if (!(u < o) || x[u] < kMinOcc || x[j] < kMinOcc) continue;
+        const R *mu = momR.data() + (size_t)u * kMomStride;
+        const R *mj = momR.data() + (size_t)o * kMomStride;
+        V3<R> r0 = mk3<R>((R)(q[3 * u] - q[3 * j]), (R)(q[3 * u + 1] - q[3 * j + 1]),
+                          (R)(q[3 * u + 2] - q[3 * j + 2]));
+        Pass2Out<R> ou{}, oj{};
+        pass2_pair_sym<R>(T, r0, (R)sigma[u], (R)sigma[j], (R)x[u], (R)x[j], code[u], code[j],
+                          mu[0], mu[1], mj[0], mj[1], (R)(beta[o] / beta[u]),
+                          (R)(beta[u] / beta[o]), mu, mj, ou, oj);
+        buf[p] = ou;
+        buf[rev[p]] = oj;
+      }
+    for (int u = 0; u < n_real; ++u) {
+      Rq[3 * u] = Rq[3 * u + 1] = Rq[3 * u + 2] = 0.0;
+      Rs[u] = Rx[u] = 0.0;
+      if (x[u] < kMinOcc) continue;
+      double gq[3] = {0, 0, 0}, gs = 0, gx = 0;
+      for (int p = offs[u]; p < offs[u + 1]; ++p) {
+        for (int k = 0; k < 3; ++k) gq[k] += buf[p].gq[k];
+        gs += buf[p].gs;
+        gx += buf[p].gx;
+      }
+      residual_epilogue(sigma[u], x[u], code[u], beta[u], gamma[u], sx[u], gs, gx);
+      for (int k = 0; k < 3; ++k) Rq[3 * u + k] = gq[k];
+      Rs[u] = gs;
+      Rx[u] = gx;
+    }
+    return;
+  }
   for (int u = 0; u < n_real; ++u) {
     Rq[3 * u] = Rq[3 * u + 1] = Rq[3 * u + 2] = 0.0;
     Rs[u] = Rx[u] = 0.0;
@@ -122,16 +166,16 @@ int hm_load_tables(const char *dir) {
   return 0;
 }
 
-void hm_eval(int fp32, int n_all, int n_real, const double *q, const double *sigma,
+void hm_eval(int fp32, int sym, int n_all, int n_real, const double *q, const double *sigma,
              const double *x, const int *code, const double *beta,
              const double *gamma, const int *owner, const int *offs,
              const int *idx, double *rho, double *V0, double *S0,
              double *selfx, double *Rq, double *Rs, double *Rx) {
   if (fp32)
-    run<float>(n_all, n_real, q, sigma, x, code, beta, gamma, owner, offs, idx,
+    run<float>(sym != 0, n_all, n_real, q, sigma, x, code, beta, gamma, owner, offs, idx,
                rho, V0, S0, selfx, Rq, Rs, Rx);
   else
-    run<double>(n_all, n_real, q, sigma, x, code, beta, gamma, owner, offs, idx,
+    run<double>(sym != 0, n_all, n_real, q, sigma, x, code, beta, gamma, owner, offs, idx,
                 rho, V0, S0, selfx, Rq, Rs, Rx);
 }
 }

@@ -25,11 +25,11 @@ class HostModel:
         if self.lib.hm_load_tables(TABLES.encode()) != 0:
             raise RuntimeError("host model: cannot load tables")
 
-    def evaluate(self, full, n_real, owner, offs, idx, fp32=False):
+    def evaluate(self, full, n_real, owner, offs, idx, fp32=False, sym=False):
         code = np.ascontiguousarray((full["species"] == 1).astype(np.int32))
         out = {k: np.zeros(n_real) for k in ("rho", "V0", "S0", "selfx", "Rs", "Rx")}
         Rq = np.zeros((n_real, 3))
-        self.lib.hm_eval(int(fp32), len(full["x"]), n_real, _d(full["q"]), _d(full["sigma"]),
+        self.lib.hm_eval(int(fp32), int(sym), len(full["x"]), n_real, _d(full["q"]), _d(full["sigma"]),
                          _d(full["x"]), _i(code), _d(full["beta"]), _d(full["gamma"]),
                          _i(owner), _i(offs), _i(idx), _d(out["rho"]), _d(out["V0"]),
                          _d(out["S0"]), _d(out["selfx"]), _d(Rq), _d(out["Rs"]),

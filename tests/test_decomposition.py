@@ -34,11 +34,15 @@ def rel(a, b):
     return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
 
 
+@pytest.mark.parametrize("sym", [False, True], ids=["directed", "undirected"])
 @pytest.mark.parametrize("name", NAMES)
-def test_fp64_decomposition_matches_reference(hostmodel, name):
+def test_fp64_decomposition_matches_reference(hostmodel, name, sym):
+    """Directed pass 2 (each site over its neighbours) and undirected pass 2
+    (each pair once, both directions from its shared geometries) against the
+    reference's values."""
     g = load(name)
     n = len(g["x"])
-    out = hostmodel.evaluate(full_of(g), n, g["owner"], g["offs"], g["idx"])
+    out = hostmodel.evaluate(full_of(g), n, g["owner"], g["offs"], g["idx"], sym=sym)
     assert rel(out["rho"], g["rho"]) < 1e-12
     assert np.max(np.abs(out["V0"] - g["V0"]) / np.maximum(np.abs(g["V0"]), 1e-3)) < 1e-10
     assert rel(out["S0"], g["S0"]) < 1e-12
@@ -49,17 +53,29 @@ def test_fp64_decomposition_matches_reference(hostmodel, name):
     assert np.max(np.abs(out["Rx"][us] - g["Rx"])) < 1e-10 * max(1.0, np.abs(g["Rx"]).max())
 
 
+@pytest.mark.parametrize("sym", [False, True], ids=["directed", "undirected"])
 @pytest.mark.parametrize("name", NAMES)
-def test_fp32_form_within_tolerance(hostmodel, name):
+def test_fp32_form_within_tolerance(hostmodel, name, sym):
     g = load(name)
     n = len(g["x"])
-    out = hostmodel.evaluate(full_of(g), n, g["owner"], g["offs"], g["idx"], fp32=True)
+    out = hostmodel.evaluate(full_of(g), n, g["owner"], g["offs"], g["idx"], fp32=True, sym=sym)
     E, E0 = out["V0"].sum(), g["V0"].sum()
     assert abs(E - E0) <= 1e-6 * abs(E0)
     us = g["res_sites"]
     assert np.max(np.abs(out["Rq"][us] - g["Rq"])) <= 1e-5
     assert np.max(np.abs(out["Rs"][us] - g["Rs"])) <= 1e-5
     assert np.max(np.abs(out["Rx"][us] - g["Rx"])) <= 1e-5 * max(1.0, np.abs(g["Rx"]).max())
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_undirected_equals_directed(hostmodel, name):
+    """Both pass-2 forms in FP64 agree to rounding on every site."""
+    g = load(name)
+    n = len(g["x"])
+    a = hostmodel.evaluate(full_of(g), n, g["owner"], g["offs"], g["idx"])
+    b = hostmodel.evaluate(full_of(g), n, g["owner"], g["offs"], g["idx"], sym=True)
+    for k in ("Rq", "Rs", "Rx"):
+        assert np.max(np.abs(a[k] - b[k])) <= 1e-12 * max(1.0, np.abs(a[k]).max()), k
 
 
 def test_inactive_hydrogen_and_translation_invariance(hostmodel, oracle):

@@ -43,11 +43,18 @@ def test_images_and_neighbors_bit_exact(gpu_tables, name):
     assert np.array_equal(offs, g["offs"]) and np.array_equal(idx, g["idx"])
 
 
+# pass-2 launch variants: directed (each site over its neighbours) and
+# undirected (each pair once, both directions), full and persistent grids
+PASS2 = [0, 16, 16 | 8 | 2]
+
+
+@pytest.mark.parametrize("v2", PASS2)
 @pytest.mark.parametrize("name", NAMES)
-def test_fp64_against_golden(gpu_tables, name):
+def test_fp64_against_golden(gpu_tables, name, v2):
     g = load(name)
     S = btam.System(gpu_tables, system_of(g))
     S.build_neighbors()
+    S.set_variants(btam.FP64, 0, v2)
     out = S.evaluate(btam.FP64)
     assert rel(out["rho"], g["rho"]) < 1e-12
     assert np.max(np.abs(out["V0"] - g["V0"]) / np.maximum(np.abs(g["V0"]), 1e-3)) < 1e-10
@@ -58,11 +65,13 @@ def test_fp64_against_golden(gpu_tables, name):
     assert abs(out["totals"][0] - g["V0"].sum()) < 1e-10 * abs(g["V0"].sum())
 
 
+@pytest.mark.parametrize("v2", PASS2)
 @pytest.mark.parametrize("name", NAMES)
-def test_fp32c_against_golden(gpu_tables, name):
+def test_fp32c_against_golden(gpu_tables, name, v2):
     g = load(name)
     S = btam.System(gpu_tables, system_of(g))
     S.build_neighbors()
+    S.set_variants(btam.FP32C, 0, v2)
     out = S.evaluate(btam.FP32C)
     E0 = g["V0"].sum()
     assert abs(out["totals"][0] - E0) <= 1e-6 * abs(E0)
@@ -119,7 +128,8 @@ def test_launch_variants(gpu_tables):
     S.build_neighbors()
     for prec, tol in ((btam.FP64, 1e-12), (btam.FP32C, 1e-6)):
         base = S.evaluate(prec)
-        for shape1, shape2 in [(v, v) for v in range(5)] + [(0, 5)]:
+        for shape1, shape2 in ([(v, v) for v in range(5)] + [(0, 5)] +
+                               [(0, 16 | v) for v in range(4)]):
             for pers in (0, 8):
                 S.set_variants(prec, shape1 | pers, shape2 | pers)
                 out = S.evaluate(prec)
@@ -136,9 +146,28 @@ def test_launch_variants(gpu_tables):
                 for k in ("Rq", "Rs", "Rx"):
                     assert np.abs(out[k] - base[k]).max() < 10 * tol, (prec, shape1, k)
         v1, v2 = S.autotune(prec)
-        assert (v1 & 7) < 5 and (v2 & 7) < 6 and v1 < 16 and v2 < 16
+        assert (v1 & 7) < 5 and v1 < 16 and v2 < 32
+        assert (v2 & 7) < (4 if v2 & 16 else 6)
     with pytest.raises(btam.BtamError):
         S.set_variants(btam.FP64, 5, 0)
+
+
+def test_persistent_grid_bitwise_on_large_system(gpu_tables):
+    """A system with more sites and pairs than one wave of resident blocks:
+    the persistent grid computes most sites and pairs in later trips of its
+    loops, and every result must still equal the full grid's bitwise."""
+    s = lattice.supercell(12, 8, 8, ortho=True, h_fraction=0.5, x_range=(0.0, 0.4),
+                          sigma_range=(0.08, 0.15), jitter=0.02, seed=41)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    for prec in (btam.FP64, btam.FP32C):
+        for v1, v2 in [(0, 0), (1, 1), (3, 4), (2, 16), (4, 16 | 3), (0, 16 | 1)]:
+            S.set_variants(prec, v1, v2)
+            full = S.evaluate(prec)
+            S.set_variants(prec, v1 | 8, v2 | 8)
+            pers = S.evaluate(prec)
+            for k in full:
+                assert np.array_equal(full[k], pers[k]), (prec, v1, v2, k)
 
 
 def test_error_codes(gpu_tables):
