@@ -376,35 +376,50 @@ template <class R> struct Pass1A {
   Feat<R> g0, hsum;
 };
 
+// The 12-point pair rule of pair (i, j): the rho, phi and B(f, f) sums over
+// the points where the centre moves +-sqrt6 sigma_i e_k or the neighbour moves
+// -+sqrt6 sigma_j e_k.  Returns x_j sum rho_{s_j} in *rho_j and, for the
+// reverse pair (j, i) whose points are the same set negated, x_i sum rho_{s_i}
+// in *rho_i when rho_i is not null.
 template <class R>
-BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
-                          R sig_j, R xi, R xj, int ci, int cj, Pass1A<R> &o) {
+BTAM_HD void pass1_pair_rule(const TablesView<R> &T, const V3<R> &r0, R sig_i, R sig_j, R xi,
+                             R xj, int ci, int cj, R &rho_j, R *rho_i, R &epair, R &ediag) {
   const int pk = pair_kind(ci, cj);
   const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
-                      &tp = T.t[T_PHI + pk], &tr = T.t[cj == 0 ? T_RHO_MG : T_RHO_H];
+                      &tp = T.t[T_PHI + pk], &tr = T.t[cj == 0 ? T_RHO_MG : T_RHO_H],
+                      &tri = T.t[ci == 0 ? T_RHO_MG : T_RHO_H];
   const R X = xi * xj;
-  R rho = 0, phi = 0, diag = 0;
-  // 12-point pair rule: centre moves +-sqrt6 sigma_i e_k, neighbour -+sqrt6 sigma_j e_k
+  R rho = 0, rhoi = 0, phi = 0, diag = 0;
   for (int side = 0; side < 2; ++side) {
     R amt = (side == 0 ? sig_i : -sig_j) * (R)kDelta6;
     for (int k = 0; k < 3; ++k)
       for (int sg = 0; sg < 2; ++sg) {
         Geo<R> g;
         geo_val(g, disp(r0, k, sg ? -amt : amt), tu, tw);
-        rho += spline_v(tr, g.s);
+        const R rj = spline_v(tr, g.s);
+        rho += rj;
+        if (rho_i) rhoi += (ci == cj) ? rj : spline_v(tri, g.s);
         phi += spline_v(tp, g.s);
         diag += bff(g);
       }
   }
-  o.rho += xj * rho;
-  o.epair += (R)0.5 * X * phi;
-  o.ediag += X * X * diag;
-  // centre geometry
+  rho_j = xj * rho;
+  if (rho_i) *rho_i = xi * rhoi;
+  epair = (R)0.5 * X * phi;
+  ediag = X * X * diag;
+}
+
+// The triplet part of pair (i, j) except the six centre-displaced moments:
+//   g0 += X f(r0),  hsum += X sum_{6 j-displaced points} f,
+//   cross += X^2 B(sum_6 f, f(r0)).
+template <class R>
+BTAM_HD void pass1_pair_trip(const TablesView<R> &T, const V3<R> &r0, R sig_j, R X, int pk,
+                             Pass1A<R> &o) {
+  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk];
   Geo<R> g0;
   geo_val(g0, r0, tu, tw);
   Feat<R> f0{};
   feat_add(f0, g0);
-  // neighbour-displaced triplet geometries
   Feat<R> hs{};
   for (int k = 0; k < 3; ++k)
     for (int sg = 0; sg < 2; ++sg) {
@@ -422,6 +437,17 @@ BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
     o.hsum.l[c] += X * hs.l[c];
   }
   o.cross += X * X * bpair_r(hs, f0);
+}
+
+template <class R>
+BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
+                          R sig_j, R xi, R xj, int ci, int cj, Pass1A<R> &o) {
+  R rho, epair, ediag;
+  pass1_pair_rule<R>(T, r0, sig_i, sig_j, xi, xj, ci, cj, rho, nullptr, epair, ediag);
+  o.rho += rho;
+  o.epair += epair;
+  o.ediag += ediag;
+  pass1_pair_trip<R>(T, r0, sig_j, xi * xj, pair_kind(ci, cj), o);
 }
 
 // Pass 1, part B: one centre displacement d = (k, sg) of pair (i, j):

@@ -64,11 +64,88 @@ __device__ __forceinline__ V3<R> pair_vec(const double4 &a, const double4 &b) {
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
+// ---- slot records of the undirected kernels (8 R per slot) -----------------
+// 256-bit record store/load of one slot (8 R).
+__device__ __forceinline__ void st_rec(float *p, const float (&v)[8]) {
+  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]),
+               "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void st_rec(double *p, const double (&v)[8]) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
+               "d"(v[2]), "d"(v[3])
+               : "memory");
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p + 4), "d"(v[4]), "d"(v[5]),
+               "d"(v[6]), "d"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void ld_rec(const float *p, float (&v)[8]) {
+  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
+                 "=f"(v[6]), "=f"(v[7])
+               : "l"(p));
+}
+__device__ __forceinline__ void ld_rec(const double *p, double (&v)[8]) {
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+               : "l"(p));
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
+               : "l"(p + 4));
+}
+
+// First half of a record (pass 1: rho, epair, ediag, 0).
+__device__ __forceinline__ void st_rec4(float *p, const float (&v)[4]) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void st_rec4(double *p, const double (&v)[4]) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
+               "d"(v[2]), "d"(v[3])
+               : "memory");
+}
+__device__ __forceinline__ void ld_rec4(const float *p, float (&v)[4]) {
+  float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+}
+__device__ __forceinline__ void ld_rec4(const double *p, double (&v)[4]) {
+  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+               : "l"(p));
+}
+
+// One thread per owned slot p = (u, j): the 12-point pair-rule sums of the
+// pair, shared by both directions (the reverse pair's points are the same
+// set negated), into slot p and the reverse slot.
+template <class R, int TPB>
+__global__ void __launch_bounds__(TPB)
+pass1u_pair_kernel(const EvalArgs<R> a) {
+#pragma unroll 1
+  for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
+    const int p = a.own_p[t], u = a.own_u[t];
+    const int j = a.idx[p], r = a.rev[p];
+    const double2 xbu = a.xb[u], xbj = a.xb[j];
+    R vu[4] = {(R)0, (R)0, (R)0, (R)0}, vj[4] = {(R)0, (R)0, (R)0, (R)0};
+    if (!(xbu.x < kMinOcc) && !(xbj.x < kMinOcc)) {
+      const double4 qu = a.pos[u], qj = a.pos[j];
+      R rj, ri, ep, ed;
+      pass1_pair_rule<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
+                         a.code[u], a.code[j], rj, &ri, ep, ed);
+      vu[0] = rj; vu[1] = ep; vu[2] = ed;
+      vj[0] = ri; vj[1] = ep; vj[2] = ed;
+    }
+    st_rec4(a.pbuf + 8 * (size_t)p, vu);
+    if (r >= 0) st_rec4(a.pbuf + 8 * (size_t)r, vj);
+  }
+}
+
 // Kernels are instantiated for several (warps per block, minimum resident
 // blocks) shapes; the second number caps the registers per thread and so
 // trades instruction-level parallelism for occupancy.  btam_autotune times
 // the shapes on the actual system and keeps the fastest.
-template <class R, int W, int MB>
+// UND: the pair-rule sums (rho, phi, B(f, f) over the 12 pair points) come
+// from the slot records written by pass1u_pair_kernel instead of being
+// evaluated here.
+template <class R, int W, int MB, bool UND>
 __global__ void __launch_bounds__(W * 32, MB)
 pass1_kernel(const EvalArgs<R> a) {
   __shared__ SiteSums ss[W];
@@ -103,8 +180,18 @@ pass1_kernel(const EvalArgs<R> a) {
     o.rho = o.epair = o.ediag = o.cross = (R)0;
     for (int c = 0; c < 3; ++c) o.g0.a[c] = o.hsum.a[c] = (R)0;
     for (int c = 0; c < 6; ++c) o.g0.l[c] = o.hsum.l[c] = (R)0;
-    pass1_pair_A<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)qj.w, (R)xi, (R)xbj.x, ci,
-                    a.code[j], o);
+    if (UND) {
+      R rec[4];
+      ld_rec4(a.pbuf + 8 * (size_t)p, rec);
+      o.rho = rec[0];
+      o.epair = rec[1];
+      o.ediag = rec[2];
+      pass1_pair_trip<R>(a.T, pair_vec<R>(qi, qj), (R)qj.w, (R)xi * (R)xbj.x,
+                         pair_kind(ci, a.code[j]), o);
+    } else {
+      pass1_pair_A<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)qj.w, (R)xi, (R)xbj.x, ci,
+                      a.code[j], o);
+    }
     acc[0].add(o.rho);
     acc[1].add(o.epair);
     acc[2].add(o.ediag);
@@ -244,36 +331,6 @@ pass2_kernel(const EvalArgs<R> a) {
   }
   __syncwarp();  // mu_s is reloaded for the warp's next site
   }
-}
-
-// ---- undirected pass 2 ------------------------------------------------------
-// 256-bit record store/load of one slot (8 R).
-__device__ __forceinline__ void st_rec(float *p, const float (&v)[8]) {
-  asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]),
-               "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
-               : "memory");
-}
-__device__ __forceinline__ void st_rec(double *p, const double (&v)[8]) {
-  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
-               "d"(v[2]), "d"(v[3])
-               : "memory");
-  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p + 4), "d"(v[4]), "d"(v[5]),
-               "d"(v[6]), "d"(v[7])
-               : "memory");
-}
-__device__ __forceinline__ void ld_rec(const float *p, float (&v)[8]) {
-  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
-                 "=f"(v[6]), "=f"(v[7])
-               : "l"(p));
-}
-__device__ __forceinline__ void ld_rec(const double *p, double (&v)[8]) {
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
-               : "l"(p));
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
-               : "l"(p + 4));
 }
 
 // One thread per owned slot p = (u, j): both directions of the pair from its
@@ -443,9 +500,26 @@ template <class K> int grid_of(K kernel, int n, int W, bool persistent) {
   int g = sms * (per > 0 ? per : 1);
   return g < full ? g : full;
 }
-template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
-  auto k = pass1_kernel<R, W, MB>;
-  k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
+template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers,
+                                           bool und) {
+  if (und) {
+    auto kp = pass1u_pair_kernel<R, 128>;
+    int g = nblocks(a.n_own, 128);
+    if (pers) {
+      int dev = 0, sms = 0, per = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, 128, 0);
+      int gp = sms * (per > 0 ? per : 1);
+      g = gp < g ? gp : g;
+    }
+    if (g > 0) kp<<<g, 128, 0, st>>>(a);
+    auto k = pass1_kernel<R, W, MB, true>;
+    k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
+  } else {
+    auto k = pass1_kernel<R, W, MB, false>;
+    k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
+  }
 }
 template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
   auto k = pass2_kernel<R, W, MB>;
@@ -455,12 +529,13 @@ template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st
 template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v) {
   if (a.n_real <= 0) return cudaSuccess;
   const bool pers = (v & kPersistent) != 0;
+  const bool und = (v & kUndirected) != 0 && has_undirected(a.rev, a.pbuf);
   switch (v & (kPersistent - 1)) {
-  case 1: go1<R, 4, 3>(a, st, pers); break;
-  case 2: go1<R, 4, 4>(a, st, pers); break;
-  case 3: go1<R, 8, 2>(a, st, pers); break;
-  case 4: go1<R, 2, 8>(a, st, pers); break;
-  default: go1<R, 4, 1>(a, st, pers); break;
+  case 1: go1<R, 4, 3>(a, st, pers, und); break;
+  case 2: go1<R, 4, 4>(a, st, pers, und); break;
+  case 3: go1<R, 8, 2>(a, st, pers, und); break;
+  case 4: go1<R, 2, 8>(a, st, pers, und); break;
+  default: go1<R, 4, 1>(a, st, pers, und); break;
   }
   return cudaGetLastError();
 }
@@ -540,11 +615,14 @@ cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int
   };
   int b1 = 0, b2 = 0;
   float t1 = 1e30f, t2 = 1e30f;
-  for (int p = 0; p < 2; ++p)
-    for (int v = 0; v < kPass1Variants && e == cudaSuccess; ++v) {
-      float t = time_one(false, v | (p ? kPersistent : 0));
-      if (t < t1) { t1 = t; b1 = v | (p ? kPersistent : 0); }
-    }
+  const int n_forms1 = has_undirected(a.rev, a.pbuf) ? 2 : 1;
+  for (int u = 0; u < n_forms1; ++u)
+    for (int p = 0; p < 2; ++p)
+      for (int v = 0; v < kPass1Variants && e == cudaSuccess; ++v) {
+        const int var = v | (p ? kPersistent : 0) | (u ? kUndirected : 0);
+        float t = time_one(false, var);
+        if (t < t1) { t1 = t; b1 = var; }
+      }
   if (e == cudaSuccess) e = launch_pass1(a, st, b1);
   for (int p = 0; p < 2; ++p)
     for (int v = 0; v < kPass2Variants && e == cudaSuccess; ++v) {

@@ -41,14 +41,15 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0)
 template <class R>
 cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
 // variant = shape | kPersistent (persistent grid of resident blocks)
-//           [| kUndirected for pass 2: each pair once, both directions]
+//           [| kUndirected: pass 1 takes its pair-rule sums, pass 2 its
+//            whole per-pair work, from one evaluation per undirected pair]
 constexpr int kPass1Variants = 5;  // shapes (4 warps,-), (4,3), (4,4), (8,2), (2,8)
 constexpr int kPass2Variants = 6;  // shapes (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
 constexpr int kPass2UVariants = 4;  // undirected pair kernel (threads, min blocks): (128,-), (128,3), (128,4), (256,2)
 constexpr int kPersistent = 8;
 constexpr int kUndirected = 16;
 inline bool valid_variants(int v1, int v2) {
-  if (v1 < 0 || v2 < 0 || (v1 & ~(2 * kPersistent - 1)) != 0 ||
+  if (v1 < 0 || v2 < 0 || (v1 & ~(2 * kUndirected - 1)) != 0 ||
       (v2 & ~(2 * kUndirected - 1)) != 0)
     return false;
   const int s2 = v2 & (kPersistent - 1);

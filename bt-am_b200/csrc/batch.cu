@@ -417,7 +417,7 @@ int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *p
   if (e != cudaSuccess) return cuda_status(e);
   b->variant1[f] = v1;
   b->variant2[f] = v2;
-  if (!((b->variant2[0] | b->variant2[1]) & kUndirected)) {
+  if (!((b->variant1[0] | b->variant1[1] | b->variant2[0] | b->variant2[1]) & kUndirected)) {
     dfree(b->pbuf, b->st);
     b->pbuf_bytes = b->pbuf_elem = 0;
   }
@@ -429,7 +429,7 @@ int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *p
 int btam_batch_set_variants(btam_batch *b, int precision, int pass1_variant, int pass2_variant) {
   if (!b || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
   if (!valid_variants(pass1_variant, pass2_variant)) return BTAM_ERR_ARG;
-  if (pass2_variant & kUndirected) {
+  if ((pass1_variant | pass2_variant) & kUndirected) {
     int st = batch_pbuf(b, precision == BTAM_FP64 ? sizeof(double) : sizeof(float));
     if (st != BTAM_OK) return st;
   }

@@ -713,7 +713,7 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
   }
   if (st != BTAM_OK) return st;
   // the slot buffer stays only while an undirected variant is selected
-  if (!((s->variant2[0] | s->variant2[1]) & kUndirected)) {
+  if (!((s->variant1[0] | s->variant1[1] | s->variant2[0] | s->variant2[1]) & kUndirected)) {
     dfree(s->pbuf, s->st);
     s->pbuf_bytes = s->pbuf_elem = 0;
   }
@@ -726,7 +726,7 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
 int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass2_variant) {
   if (!s || (precision != BTAM_FP64 && precision != BTAM_FP32C)) return BTAM_ERR_ARG;
   if (!valid_variants(pass1_variant, pass2_variant)) return BTAM_ERR_ARG;
-  if (pass2_variant & kUndirected) {
+  if ((pass1_variant | pass2_variant) & kUndirected) {
     if (!s->built) return BTAM_ERR_NOT_BUILT;
     int st = ensure_pbuf(s, precision == BTAM_FP64 ? sizeof(double) : sizeof(float));
     if (st != BTAM_OK) return st;

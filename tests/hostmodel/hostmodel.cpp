@@ -42,6 +42,32 @@ void run(bool sym, int n_all, int n_real, const double *q, const double *sigma,
   std::vector<double> mom((size_t)n_real * kMomStride, 0.0);
   std::vector<R> momR((size_t)n_real * kMomStride, (R)0);
   std::vector<double> sx(n_real, 0.0);
+  // undirected form: reverse slots, and the pair-rule sums of every slot from
+  // its owned pair (both directions at once)
+  std::vector<int> rev(offs[n_real], -1);
+  std::vector<R> rec(3 * (size_t)offs[n_real], (R)0);
+  if (sym) {
+    for (int u = 0; u < n_real; ++u)
+      for (int p = offs[u]; p < offs[u + 1]; ++p) {
+        int o = owner[idx[p]];
+        for (int t = offs[o]; t < offs[o + 1]; ++t)
+          if (owner[idx[t]] == u) rev[p] = t;
+      }
+    for (int u = 0; u < n_real; ++u)
+      for (int p = offs[u]; p < offs[u + 1]; ++p) {
+        int j = idx[p], o = owner[j];
+        if (!(u < o || rev[p] < 0) || x[u] < kMinOcc || x[j] < kMinOcc) continue;
+        V3<R> r0 = mk3<R>((R)(q[3 * u] - q[3 * j]), (R)(q[3 * u + 1] - q[3 * j + 1]),
+                          (R)(q[3 * u + 2] - q[3 * j + 2]));
+        R rj, ri, ep, ed;
+        pass1_pair_rule<R>(T, r0, (R)sigma[u], (R)sigma[j], (R)x[u], (R)x[j], code[u], code[j],
+                           rj, &ri, ep, ed);
+        rec[3 * p] = rj; rec[3 * p + 1] = ep; rec[3 * p + 2] = ed;
+        if (rev[p] >= 0) {
+          rec[3 * rev[p]] = ri; rec[3 * rev[p] + 1] = ep; rec[3 * rev[p] + 2] = ed;
+        }
+      }
+  }
   for (int i = 0; i < n_real; ++i) {
     rho[i] = V0[i] = S0[i] = selfx[i] = 0.0;
     if (x[i] < kMinOcc) continue;
@@ -54,7 +80,12 @@ void run(bool sym, int n_all, int n_real, const double *q, const double *sigma,
                         (R)(q[3 * i + 2] - q[3 * j + 2]));
       Pass1A<R> a;
       memset(&a, 0, sizeof(a));
-      pass1_pair_A<R>(T, r0, (R)sigma[i], (R)sigma[j], (R)x[i], (R)x[j], code[i], code[j], a);
+      if (sym) {
+        a.rho = rec[3 * p]; a.epair = rec[3 * p + 1]; a.ediag = rec[3 * p + 2];
+        pass1_pair_trip<R>(T, r0, (R)sigma[j], (R)x[i] * (R)x[j], pair_kind(code[i], code[j]), a);
+      } else {
+        pass1_pair_A<R>(T, r0, (R)sigma[i], (R)sigma[j], (R)x[i], (R)x[j], code[i], code[j], a);
+      }
       S.rho += a.rho; S.epair += a.epair; S.ediag += a.ediag; S.cross += a.cross;
       for (int c = 0; c < 3; ++c) { S.g0a[c] += a.g0.a[c]; S.ha[c] += a.hsum.a[c]; }
       for (int c = 0; c < 6; ++c) { S.g0l[c] += a.g0.l[c]; S.hl[c] += a.hsum.l[c]; }
@@ -83,18 +114,11 @@ void run(bool sym, int n_all, int n_real, const double *q, const double *sigma,
     // undirected pairs: each owned slot (u < owner of j) gives both
     // directions; slot values are summed per site in slot order
     std::vector<Pass2Out<R>> buf(offs[n_real]);
-    std::vector<int> rev(offs[n_real], -1);
-    for (int u = 0; u < n_real; ++u)
-      for (int p = offs[u]; p < offs[u + 1]; ++p) {
-        int o = owner[idx[p]];
-        for (int t = offs[o]; t < offs[o + 1]; ++t)
-          if (owner[idx[t]] == u) rev[p] = t;
-      }
     for (auto &b : buf) b = Pass2Out<R>{};
     for (int u = 0; u < n_real; ++u)
       for (int p = offs[u]; p < offs[u + 1]; ++p) {
         int j = idx[p], o = owner[j];
-        if (!(u < o) || x[u] < kMinOcc || x[j] < kMinOcc) continue;
+        if (!(u < o || rev[p] < 0) || x[u] < kMinOcc || x[j] < kMinOcc) continue;
         const R *mu = momR.data() + (size_t)u * kMomStride;
         const R *mj = momR.data() + (size_t)o * kMomStride;
         V3<R> r0 = mk3<R>((R)(q[3 * u] - q[3 * j]), (R)(q[3 * u + 1] - q[3 * j + 1]),
@@ -104,7 +128,7 @@ void run(bool sym, int n_all, int n_real, const double *q, const double *sigma,
                           mu[0], mu[1], mj[0], mj[1], (R)(beta[o] / beta[u]),
                           (R)(beta[u] / beta[o]), mu, mj, ou, oj);
         buf[p] = ou;
-        buf[rev[p]] = oj;
+        if (rev[p] >= 0) buf[rev[p]] = oj;
       }
     for (int u = 0; u < n_real; ++u) {
       Rq[3 * u] = Rq[3 * u + 1] = Rq[3 * u + 2] = 0.0;

@@ -42,14 +42,14 @@ def assert_same(a, b, what):
         assert np.array_equal(a[f], b[f]), (what, f, np.abs(a[f] - b[f]).max())
 
 
-@pytest.mark.parametrize("v2", [0, 16], ids=["directed", "undirected"])
+@pytest.mark.parametrize("und", [0, 16], ids=["directed", "undirected"])
 @pytest.mark.parametrize("prec", [btam.FP64, btam.FP32C])
-def test_batch_equals_single_systems_bitwise(gpu_tables, prec, v2):
+def test_batch_equals_single_systems_bitwise(gpu_tables, prec, und):
     systems = built(gpu_tables, mixed_systems())
     for S in systems:
-        S.set_variants(prec, 0, v2)  # shape 0, full grid
+        S.set_variants(prec, und, und)  # shape 0, full grid
     B = btam.Batch(systems)
-    B.set_variants(prec, 8, v2 | 8)  # shape 0, persistent grid
+    B.set_variants(prec, und | 8, und | 8)  # shape 0, persistent grid
     info = B.info()
     assert info["n_sys"] == len(systems)
     assert info["n_real"] == sum(S.n for S in systems)
@@ -80,7 +80,7 @@ def test_batch_state_update_and_autotune(gpu_tables):
     assert v1 >= 0 and v2 >= 0
     B.evaluate(btam.FP32C)
     for k, S in enumerate(systems):
-        S.set_variants(btam.FP32C, v1 & 7, v2 & ~8)  # same kernels as the batch, full grid
+        S.set_variants(btam.FP32C, v1 & ~8, v2 & ~8)  # same kernels as the batch, full grid
         got = B.results(k)
         assert_same(got, S.evaluate(btam.FP32C), (k, v1, v2))
         if k > 1:  # unchanged systems: same energies (pass 1 is the same

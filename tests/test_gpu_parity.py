@@ -43,18 +43,19 @@ def test_images_and_neighbors_bit_exact(gpu_tables, name):
     assert np.array_equal(offs, g["offs"]) and np.array_equal(idx, g["idx"])
 
 
-# pass-2 launch variants: directed (each site over its neighbours) and
-# undirected (each pair once, both directions), full and persistent grids
-PASS2 = [0, 16, 16 | 8 | 2]
+# launch variants (pass 1, pass 2): directed (each site over its neighbours)
+# and undirected (each pair once for both directions), full and persistent
+# grids
+VARIANTS = [(0, 0), (0, 16), (16, 16), (16 | 8 | 3, 16 | 8 | 2)]
 
 
-@pytest.mark.parametrize("v2", PASS2)
+@pytest.mark.parametrize("v", VARIANTS, ids=lambda v: f"v{v[0]}-{v[1]}")
 @pytest.mark.parametrize("name", NAMES)
-def test_fp64_against_golden(gpu_tables, name, v2):
+def test_fp64_against_golden(gpu_tables, name, v):
     g = load(name)
     S = btam.System(gpu_tables, system_of(g))
     S.build_neighbors()
-    S.set_variants(btam.FP64, 0, v2)
+    S.set_variants(btam.FP64, *v)
     out = S.evaluate(btam.FP64)
     assert rel(out["rho"], g["rho"]) < 1e-12
     assert np.max(np.abs(out["V0"] - g["V0"]) / np.maximum(np.abs(g["V0"]), 1e-3)) < 1e-10
@@ -65,13 +66,13 @@ def test_fp64_against_golden(gpu_tables, name, v2):
     assert abs(out["totals"][0] - g["V0"].sum()) < 1e-10 * abs(g["V0"].sum())
 
 
-@pytest.mark.parametrize("v2", PASS2)
+@pytest.mark.parametrize("v", VARIANTS, ids=lambda v: f"v{v[0]}-{v[1]}")
 @pytest.mark.parametrize("name", NAMES)
-def test_fp32c_against_golden(gpu_tables, name, v2):
+def test_fp32c_against_golden(gpu_tables, name, v):
     g = load(name)
     S = btam.System(gpu_tables, system_of(g))
     S.build_neighbors()
-    S.set_variants(btam.FP32C, 0, v2)
+    S.set_variants(btam.FP32C, *v)
     out = S.evaluate(btam.FP32C)
     E0 = g["V0"].sum()
     assert abs(out["totals"][0] - E0) <= 1e-6 * abs(E0)
@@ -129,7 +130,8 @@ def test_launch_variants(gpu_tables):
     for prec, tol in ((btam.FP64, 1e-12), (btam.FP32C, 1e-6)):
         base = S.evaluate(prec)
         for shape1, shape2 in ([(v, v) for v in range(5)] + [(0, 5)] +
-                               [(0, 16 | v) for v in range(4)]):
+                               [(0, 16 | v) for v in range(4)] +
+                               [(16 | v, 16 | (v % 4)) for v in range(5)]):
             for pers in (0, 8):
                 S.set_variants(prec, shape1 | pers, shape2 | pers)
                 out = S.evaluate(prec)
@@ -146,7 +148,7 @@ def test_launch_variants(gpu_tables):
                 for k in ("Rq", "Rs", "Rx"):
                     assert np.abs(out[k] - base[k]).max() < 10 * tol, (prec, shape1, k)
         v1, v2 = S.autotune(prec)
-        assert (v1 & 7) < 5 and v1 < 16 and v2 < 32
+        assert (v1 & 7) < 5 and v1 < 32 and v2 < 32
         assert (v2 & 7) < (4 if v2 & 16 else 6)
     with pytest.raises(btam.BtamError):
         S.set_variants(btam.FP64, 5, 0)
@@ -161,7 +163,8 @@ def test_persistent_grid_bitwise_on_large_system(gpu_tables):
     S = btam.System(gpu_tables, s)
     S.build_neighbors()
     for prec in (btam.FP64, btam.FP32C):
-        for v1, v2 in [(0, 0), (1, 1), (3, 4), (2, 16), (4, 16 | 3), (0, 16 | 1)]:
+        for v1, v2 in [(0, 0), (1, 1), (3, 4), (2, 16), (4, 16 | 3), (0, 16 | 1), (16, 16),
+                       (16 | 3, 16 | 2)]:
             S.set_variants(prec, v1, v2)
             full = S.evaluate(prec)
             S.set_variants(prec, v1 | 8, v2 | 8)
