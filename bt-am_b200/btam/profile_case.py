@@ -1,0 +1,65 @@
+"""Fixed-shape evaluation runs for kernel profiling.
+
+Builds one synthetic system, pins the launch variants (no autotuner, so the
+launch sequence is known in advance) and runs a few residual evaluations in
+one arithmetic form.  Meant to run under a profiler with a kernel filter and
+a launch count, e.g.
+
+    ncu --set full --clock-control none -k regex:pass2u_pair -s 2 -c 1 \\
+        python -m btam.profile_case --workload dropin --precision fp32c
+
+(from bt-am_b200/, or with bt-am_b200 on PYTHONPATH).
+
+Workloads: "dropin" is the plain drop-in system (periodic hcp Mg 20x15x15
+hexagonal cells with H on all tetrahedral sites, 27 000 sites); "small" is a
+periodic ortho-hexagonal block of about 1 500 Mg with H on 30 % of the
+tetrahedral sites, for quick captures.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+import btam
+from btam import lattice
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="dropin", choices=["dropin", "small"])
+    ap.add_argument("--precision", default="fp32c", choices=["fp32c", "fp64"])
+    ap.add_argument("--v1", type=int, default=None, help="pass-1 variant (default: 19 fp32c, 25 fp64)")
+    ap.add_argument("--v2", type=int, default=None, help="pass-2 variant (default: 27 fp32c, 25 fp64)")
+    ap.add_argument("--evals", type=int, default=4)
+    args = ap.parse_args()
+    prec = btam.FP32C if args.precision == "fp32c" else btam.FP64
+    if args.workload == "dropin":
+        sysd = lattice.config2()
+    else:
+        sysd = lattice.periodic_cube(1500, seed=1)
+    tables = btam.Tables()
+    S = btam.System(tables, sysd)
+    S.build_neighbors()
+    v1 = args.v1 if args.v1 is not None else (19 if prec == btam.FP32C else 25)
+    v2 = args.v2 if args.v2 is not None else (27 if prec == btam.FP32C else 25)
+    S.set_variants(prec, v1, v2)
+    t0 = time.perf_counter()
+    for _ in range(args.evals):
+        S.evaluate_async(prec)
+    S.sync()
+    dt = time.perf_counter() - t0
+    tot = S.results(want=("totals",))["totals"]
+    nr, ng, npairs = S.info()
+    print(json.dumps({"workload": args.workload, "precision": args.precision, "v1": v1, "v2": v2,
+                      "sites": nr, "images": ng, "pairs": npairs, "evals": args.evals,
+                      "wall_ms_per_eval": dt * 1e3 / args.evals,
+                      "energy": float(tot[0]), "finite": bool(np.isfinite(tot).all())}))
+    S.close()
+    tables.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -35,14 +36,18 @@ def build(verbose=False, force=False):
     deps.append(os.path.join(os.path.dirname(HERE), "include", "btam.h"))
     if not force and not _stale(LIB, deps):
         return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(LIB_DIR, src.replace(".cu", ".o"))
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
+    objs = [os.path.join(LIB_DIR, src.replace(".cu", ".o")) for src in SOURCES]
+    cmds = [[NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+            for src, obj in zip(SOURCES, objs)]
+    if verbose:
+        for cmd in cmds:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds):
+            if r.returncode != 0:
+                sys.stderr.write(r.stdout + r.stderr)
+                raise subprocess.CalledProcessError(r.returncode, r.args)
     cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs]
     subprocess.run(cmd, check=True)
     for o in objs:

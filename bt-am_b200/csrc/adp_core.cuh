@@ -99,6 +99,103 @@ template <class R> BTAM_HD R spline_v(const SplineView<R> &s, R r) {
   return v;
 }
 
+// ---------------------------------------------------------------------------
+// Kernel form of the radial tables.  Every radial function of the potential
+// (rho_Mg, rho_H and phi, u, w of the three pair kinds) is tabulated on one
+// uniform knot grid (n = 1194, dx = 0.00527527527528; adpmg.dat:2,
+// adph.dat:2, adpmgh.dat:2 and the pair blocks after them), so one segment
+// index (m, p) serves every function at a geometry, and the coefficients of
+// the functions a geometry needs together sit in one aligned record (one
+// 32-byte sector per 8 floats):
+//   uw block of pair kind pk (at uw + 8 n pk): 8 R per segment: u (a, b, c,
+//           d), w (a, b, c, d);
+//   pr block of pair kind pk (at pr + 8 n pk): pr_stride(pk) R per segment:
+//           phi (a..d) and rho (a..d) of the species for the same-species
+//           kinds; phi, rho_Mg, rho_H and four zeros for Mg-H.
+// The blocks are found by arithmetic on the pair kind, not by indexing an
+// array of pointers, so lanes of different pair kinds never serialise on a
+// divergent parameter-space load.
+template <class R> struct RadialView {
+  const R *uw;
+  const R *pr;
+  R dx, inv_dx;
+  int n;
+};
+constexpr int kUWStride = 8;
+BTAM_HD int pr_stride(int pk) { return pk == 2 ? 16 : 8; }
+template <class R> BTAM_HD const R *uw_rec(const RadialView<R> &T, int pk, int m) {
+  return T.uw + (size_t)kUWStride * ((size_t)T.n * pk + m);
+}
+template <class R> BTAM_HD const R *pr_rec(const RadialView<R> &T, int pk, int m) {
+  return T.pr + (size_t)8 * T.n * pk + (size_t)pr_stride(pk) * m;
+}
+// Offset of rho of species c (0 Mg, 1 H) in a pr record of pair kind pk.
+BTAM_HD int rho_off(int pk, int c) { return (pk == 2 && c == 1) ? 8 : 4; }
+
+// Segment of |r| = s (cubic-spline.cpp:84-96): m = min(floor(s/dx), n-1),
+// p = min(s - m dx, dx).
+template <class R> BTAM_HD int seg_of(const RadialView<R> &T, R s, R &p) {
+  int m = (int)(s * T.inv_dx);
+  m = m < T.n - 1 ? m : T.n - 1;
+  p = rmin(s - (R)m * T.dx, T.dx);
+  return m;
+}
+
+// Cubic a + (b + (c + d p) p) p and its derivative b + (2c + 3d p) p.
+template <class R> BTAM_HD R cub_v(const R *k, R p) {
+  return k[0] + (k[1] + (k[2] + k[3] * p) * p) * p;
+}
+template <class R> BTAM_HD void cub_vd(const R *k, R p, R &v, R &dv) {
+  v = cub_v(k, p);
+  dv = k[1] + ((R)2 * k[2] + (R)3 * k[3] * p) * p;
+}
+
+// Read-only vector loads of 32-byte-aligned records (device: non-coherent
+// 256-bit loads; host: plain copies).
+BTAM_HD void ld8(const float *p, float (&v)[8]) {
+#if defined(__CUDA_ARCH__)
+  asm("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]),
+        "=f"(v[7])
+      : "l"(p));
+#else
+  for (int c = 0; c < 8; ++c) v[c] = p[c];
+#endif
+}
+BTAM_HD void ld8(const double *p, double (&v)[8]) {
+#if defined(__CUDA_ARCH__)
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+      : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+      : "l"(p));
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+      : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
+      : "l"(p + 4));
+#else
+  for (int c = 0; c < 8; ++c) v[c] = p[c];
+#endif
+}
+BTAM_HD void ld4(const float *p, float (&v)[4]) {
+#if defined(__CUDA_ARCH__)
+  float4 t = __ldg(reinterpret_cast<const float4 *>(p));
+  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+#else
+  for (int c = 0; c < 4; ++c) v[c] = p[c];
+#endif
+}
+BTAM_HD void ld4(const double *p, double (&v)[4]) {
+#if defined(__CUDA_ARCH__)
+  asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+      : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+      : "l"(p));
+#else
+  for (int c = 0; c < 4; ++c) v[c] = p[c];
+#endif
+}
+// Plain 8-value copy (records staged in shared memory).
+template <class R> BTAM_HD void cp8(const R *p, R (&v)[8]) {
+  for (int c = 0; c < 8; ++c) v[c] = p[c];
+}
+
 template <class R> struct V3 {
   R x, y, z;
 };
@@ -191,23 +288,55 @@ BTAM_HD void norm_inv(float s2, float &s, float &inv) {
   s = s2 * inv;
 }
 
-template <class R>
-BTAM_HD void geo_eval(Geo<R> &g, const V3<R> &r, const SplineView<R> &tu,
-                      const SplineView<R> &tw) {
+// u, w of pair kind pk at one geometry (values and, when D, derivatives);
+// returns the segment (m, p) for the pair-rule record of the same geometry.
+template <class R, bool D>
+BTAM_HD int geo_uw(Geo<R> &g, const V3<R> &r, const RadialView<R> &T, int pk, R &p) {
   g.r = r;
   norm_inv(dot3(r, r), g.s, g.inv_s);
-  spline_vd(tu, g.s, g.u, g.du);
-  spline_vd(tw, g.s, g.w, g.dw);
+  const int m = seg_of(T, g.s, p);
+  R k[8];
+  ld8(uw_rec(T, pk, m), k);
+  if (D) {
+    cub_vd(k, p, g.u, g.du);
+    cub_vd(k + 4, p, g.w, g.dw);
+  } else {
+    g.u = cub_v(k, p);
+    g.w = cub_v(k + 4, p);
+    g.du = g.dw = (R)0;
+  }
+  return m;
 }
 
-// Values only (pass 1 needs no derivatives and no 1/|r|).
-template <class R>
-BTAM_HD void geo_val(Geo<R> &g, const V3<R> &r, const SplineView<R> &tu,
-                     const SplineView<R> &tw) {
-  g.r = r;
-  norm_inv(dot3(r, r), g.s, g.inv_s);
-  g.u = spline_v(tu, g.s);
-  g.w = spline_v(tw, g.s);
+// Pair-rule functions of pair kind pk at segment (m, p): phi, rho of the
+// neighbour's species cj (rj) and, when WANT_I, of the centre's species ci
+// (ri); derivatives when D.
+template <class R, bool D, bool WANT_I>
+BTAM_HD void pr_at(const RadialView<R> &T, int pk, int ci, int cj, int m, R p, R &ph, R &dph,
+                   R &rj, R &drj, R &ri, R &dri) {
+  const R *base = pr_rec(T, pk, m);
+  R k[8];
+  ld8(base, k);
+  R r0 = (R)0, dr0 = (R)0, r1 = (R)0, dr1 = (R)0;
+  if (D) {
+    cub_vd(k, p, ph, dph);
+    cub_vd(k + 4, p, r0, dr0);
+  } else {
+    ph = cub_v(k, p);
+    r0 = cub_v(k + 4, p);
+    dph = (R)0;
+  }
+  if (pk == 2 && (cj == 1 || (WANT_I && ci == 1))) {
+    R h[4];
+    ld4(base + 8, h);
+    if (D) cub_vd(h, p, r1, dr1);
+    else r1 = cub_v(h, p);
+  }
+  const bool jh = pk == 2 && cj == 1, ih = pk == 2 && ci == 1;
+  rj = jh ? r1 : r0;
+  drj = jh ? dr1 : dr0;
+  ri = ih ? r1 : r0;
+  dri = ih ? dr1 : dr0;
 }
 
 // A dual prepared for the six geometries r0 + a e_k that move along one
@@ -323,29 +452,30 @@ template <class R> BTAM_HD Dual<R> dual_flip(const Dual<R> &A) {
   return D;
 }
 
-// Per-site moment record written by pass 1 and read by pass 2.
-// Layout (R units): [0] x_i F'(rho_i), [1] (H ? x_i : 1) F'(rho_i) (the
-// occupancy-gradient embedding factor of MgHx-mf-V-bulk.cpp:2299-2315),
-// [2] beta_i, [3] pad, then 8 duals of 9: G0, H, G(d) for d = (k, s) in the
-// order (x+, x-, y+, y-, z+, z-).
-constexpr int kMomStride = 4 + 8 * 9;  // 76
-constexpr int kMomG0 = 4, kMomH = 13, kMomGd = 22;
+// Per-site moment record written by pass 1 and read by pass 2 (kMomStride R,
+// 32-byte aligned for vector loads):
+//   [0] x_i F'(rho_i), [1] (H ? x_i : 1) F'(rho_i) (the occupancy-gradient
+//   embedding factor of MgHx-mf-V-bulk.cpp:2299-2315), [2] beta_i, [3..7] 0;
+//   then the bilinear-form duals of 8 feature sums, k = 0: G0, 1: H,
+//   2 + d: G(d) for d = (axis, sign) in the order (x+, x-, y+, y-, z+, z-):
+//   dual k's first eight components (a0 a1 a2 d0 d1 d2 o0 o1) at 8 + 8k and
+//   its last one (o2) at 72 + k.
+constexpr int kMomStride = 80;
+constexpr int kDualG0 = 0, kDualH = 1, kDualGd = 2;
 
-template <class R> BTAM_HD Dual<R> load_dual(const R *m) {
+template <class R> BTAM_HD Dual<R> dual_from(const R (&h)[8], R o2) {
   Dual<R> D;
-  for (int k = 0; k < 3; ++k) {
-    D.a[k] = m[k];
-    D.d[k] = m[3 + k];
-    D.o[k] = m[6 + k];
-  }
+  D.a[0] = h[0]; D.a[1] = h[1]; D.a[2] = h[2];
+  D.d[0] = h[3]; D.d[1] = h[4]; D.d[2] = h[5];
+  D.o[0] = h[6]; D.o[1] = h[7]; D.o[2] = o2;
   return D;
 }
-template <class R, class S> BTAM_HD void store_dual(R *m, const Dual<S> &D) {
-  for (int k = 0; k < 3; ++k) {
-    m[k] = (R)D.a[k];
-    m[3 + k] = (R)D.d[k];
-    m[6 + k] = (R)D.o[k];
-  }
+template <class R, class S> BTAM_HD void store_dual(R *m, int k, const Dual<S> &D) {
+  R *h = m + 8 + 8 * k;
+  h[0] = (R)D.a[0]; h[1] = (R)D.a[1]; h[2] = (R)D.a[2];
+  h[3] = (R)D.d[0]; h[4] = (R)D.d[1]; h[5] = (R)D.d[2];
+  h[6] = (R)D.o[0]; h[7] = (R)D.o[1];
+  m[72 + k] = (R)D.o[2];
 }
 
 // ---------------------------------------------------------------------------
@@ -354,14 +484,6 @@ template <class R, class S> BTAM_HD void store_dual(R *m, const Dual<S> &D) {
 BTAM_HD int pair_kind(int ci, int cj) { return ci == cj ? ci : 2; }
 
 // ---------------------------------------------------------------------------
-// Pass 1, part A: everything of pair (i, j) except the six centre-displaced
-// triplet moments.  Adds (unscaled by the caller's weights):
-//   rho   += x_j sum_{12 pair pts} rho_{s_j}(|r|)
-//   epair += 1/2 X sum_{12} phi                        (X = x_i x_j)
-//   ediag += X^2 sum_{12} B(f,f)
-//   g0    += X f(r0)
-//   hsum  += X sum_{6 j-displaced triplet pts} f
-//   cross += X^2 B(sum_{6} f, f(r0))
 // B(X, Y) of two feature sums in the working type.
 template <class R> BTAM_HD R bpair_r(const Feat<R> &x, const Feat<R> &y) {
   R ab = x.a[0] * y.a[0] + x.a[1] * y.a[1] + x.a[2] * y.a[2];
@@ -371,10 +493,58 @@ template <class R> BTAM_HD R bpair_r(const Feat<R> &x, const Feat<R> &y) {
   return (R)0.5 * ab + (R)0.5 * lm - t1 * t2 / (R)6;
 }
 
-template <class R> struct Pass1A {
-  R rho, epair, ediag, cross;
-  Feat<R> g0, hsum;
-};
+// The 12-point pair rule of an owned pair (u, j), once for both passes and
+// both directions.  Pass 1 needs its raw sums; pass 2 needs the gradient
+// pieces, which are linear in the embedding factors that pass 1 produces:
+// with A = rho'_{s_j}/s, B = rho'_{s_u}/s, C = X phi'/(2 s) + X^2 dB(f,f)/ds
+// / s at each point r (s = |r|), the radial coefficients of pass 2 are
+//   c_self = w6 (x_u F'(rho_u) x_j A + C),   c_cros = w6 (x_j F'(rho_j) x_u B + C),
+// so the record keeps sum A r, sum B r, sum C r and their sigma-direction
+// sums over each side.  Layout (kPrRec R, 32-byte aligned):
+//   [0] sum rho_{s_u}, [1] sum rho_{s_j}, [2] sum phi, [3] sum B(f, f),
+//   [4..6] sum A r, [7..9] sum B r, [10..12] sum C r,
+//   [13..15] sum (A, B, C) sd over the u-moved points (sd = -+sqrt6 r_k),
+//   [16..18] sum (A, B, C) sd over the j-moved points (sd = +-sqrt6 r_k),
+//   [19..23] 0.
+constexpr int kPrRec = 24;
+template <class R>
+BTAM_HD void pair_rule_record(const RadialView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
+                              R xj, int cu, int cj, R (&rec)[kPrRec]) {
+  const int pk = pair_kind(cu, cj);
+  const R X = xu * xj;
+#pragma unroll
+  for (int c = 0; c < kPrRec; ++c) rec[c] = (R)0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const R amt = (side == 0 ? sig_u : -sig_j) * (R)kDelta6;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int sg = 0; sg < 2; ++sg) {
+        const R a = sg ? -amt : amt;
+        Geo<R> g;
+        R p;
+        const int m = geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
+        R rj, drj, ru, dru, ph, dph;
+        pr_at<R, true, true>(T, pk, cu, cj, m, p, ph, dph, rj, drj, ru, dru);
+        const R A = drj * g.inv_s, B = dru * g.inv_s;
+        const R C = (R)0.5 * X * dph * g.inv_s + X * X * bff_grad_coef(g);
+        rec[0] += ru;
+        rec[1] += rj;
+        rec[2] += ph;
+        rec[3] += bff(g);
+        rec[4] += A * g.r.x; rec[5] += A * g.r.y; rec[6] += A * g.r.z;
+        rec[7] += B * g.r.x; rec[8] += B * g.r.y; rec[9] += B * g.r.z;
+        rec[10] += C * g.r.x; rec[11] += C * g.r.y; rec[12] += C * g.r.z;
+        // d r / d sigma along the moved site's axis: side 0 moves u, side 1 moves j
+        const R sd = ((side == 0) == (sg != 0) ? -(R)kDelta6 : (R)kDelta6) * comp(g.r, k);
+        const int o = side == 0 ? 13 : 16;
+        rec[o] += A * sd;
+        rec[o + 1] += B * sd;
+        rec[o + 2] += C * sd;
+      }
+  }
+}
 
 // The 12-point pair rule of pair (i, j): the rho, phi and B(f, f) sums over
 // the points where the centre moves +-sqrt6 sigma_i e_k or the neighbour moves
@@ -382,24 +552,27 @@ template <class R> struct Pass1A {
 // reverse pair (j, i) whose points are the same set negated, x_i sum rho_{s_i}
 // in *rho_i when rho_i is not null.
 template <class R>
-BTAM_HD void pass1_pair_rule(const TablesView<R> &T, const V3<R> &r0, R sig_i, R sig_j, R xi,
+BTAM_HD void pass1_pair_rule(const RadialView<R> &T, const V3<R> &r0, R sig_i, R sig_j, R xi,
                              R xj, int ci, int cj, R &rho_j, R *rho_i, R &epair, R &ediag) {
   const int pk = pair_kind(ci, cj);
-  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
-                      &tp = T.t[T_PHI + pk], &tr = T.t[cj == 0 ? T_RHO_MG : T_RHO_H],
-                      &tri = T.t[ci == 0 ? T_RHO_MG : T_RHO_H];
   const R X = xi * xj;
   R rho = 0, rhoi = 0, phi = 0, diag = 0;
+#pragma unroll
   for (int side = 0; side < 2; ++side) {
     R amt = (side == 0 ? sig_i : -sig_j) * (R)kDelta6;
+#pragma unroll
     for (int k = 0; k < 3; ++k)
+#pragma unroll
       for (int sg = 0; sg < 2; ++sg) {
         Geo<R> g;
-        geo_val(g, disp(r0, k, sg ? -amt : amt), tu, tw);
-        const R rj = spline_v(tr, g.s);
+        R p;
+        const int m = geo_uw<R, false>(g, disp(r0, k, sg ? -amt : amt), T, pk, p);
+        R ph, dph, rj, drj, ri, dri;
+        if (rho_i) pr_at<R, false, true>(T, pk, ci, cj, m, p, ph, dph, rj, drj, ri, dri);
+        else pr_at<R, false, false>(T, pk, ci, cj, m, p, ph, dph, rj, drj, ri, dri);
         rho += rj;
-        if (rho_i) rhoi += (ci == cj) ? rj : spline_v(tri, g.s);
-        phi += spline_v(tp, g.s);
+        if (rho_i) rhoi += ri;
+        phi += ph;
         diag += bff(g);
       }
   }
@@ -409,60 +582,93 @@ BTAM_HD void pass1_pair_rule(const TablesView<R> &T, const V3<R> &r0, R sig_i, R
   ediag = X * X * diag;
 }
 
-// The triplet part of pair (i, j) except the six centre-displaced moments:
-//   g0 += X f(r0),  hsum += X sum_{6 j-displaced points} f,
-//   cross += X^2 B(sum_6 f, f(r0)).
+// ---------------------------------------------------------------------------
+// Pass 1 per-pair moments in flat accumulator arrays (one lane per
+// neighbour), in two parts so that few accumulators are live at once.
+// Part I: the pair-rule sums, the centre point and the six
+// neighbour-displaced points (-+3 sigma_j e_k); part II: the six
+// centre-displaced points (+-3 sigma_i e_k).  Index layout of the flat
+// pass-1 values (the order of SiteSums' fields up to the G(d) block):
+constexpr int kP1Rho = 0, kP1Epair = 1, kP1Ediag = 2, kP1Cross = 3, kP1Sself = 4;
+constexpr int kP1G0 = 5, kP1H = 14, kP1Gd = 23;  // 9 each; G(d) at kP1Gd + 9 d
+constexpr int kP1Used = 77;
+// Part I accumulates values [0, 23) except sself; part II values sself and
+// [23, 77) at part-local index 0 (sself) and 1 + (v - 23).
+constexpr int kP1PartI = 32, kP1PartII = 64;  // padded array lengths
+
+// acc[base..base+8] += Xu r, Xw r r^T (feature scaled by X, as (a, L)).
+template <class R> BTAM_HD void feat_acc(R *acc, int base, const Geo<R> &g, R X) {
+  const R xu = X * g.u, xw = X * g.w;
+  const R x = g.r.x, y = g.r.y, z = g.r.z;
+  acc[base + 0] += xu * x;
+  acc[base + 1] += xu * y;
+  acc[base + 2] += xu * z;
+  acc[base + 3] += xw * (x * x);
+  acc[base + 4] += xw * (y * y);
+  acc[base + 5] += xw * (z * z);
+  acc[base + 6] += xw * (x * y);
+  acc[base + 7] += xw * (x * z);
+  acc[base + 8] += xw * (y * z);
+}
+
+// Part I without the pair rule: g0 += X f(r0), hsum += X sum_{6} f,
+// cross += X^2 B(sum_6 f, f(r0)) over the neighbour-displaced points.
 template <class R>
-BTAM_HD void pass1_pair_trip(const TablesView<R> &T, const V3<R> &r0, R sig_j, R X, int pk,
-                             Pass1A<R> &o) {
-  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk];
+BTAM_HD void pass1_pair_part1(const RadialView<R> &T, const V3<R> &r0, R sig_j, R X, int pk,
+                              R *acc) {
   Geo<R> g0;
-  geo_val(g0, r0, tu, tw);
+  R p;
+  geo_uw<R, false>(g0, r0, T, pk, p);
   Feat<R> f0{};
   feat_add(f0, g0);
   Feat<R> hs{};
+  const R amt_j = sig_j * (R)kDelta9;
+#pragma unroll
   for (int k = 0; k < 3; ++k)
+#pragma unroll
     for (int sg = 0; sg < 2; ++sg) {
       Geo<R> g;
-      R amt = sig_j * (R)kDelta9;
-      geo_val(g, disp(r0, k, sg ? amt : -amt), tu, tw);
+      geo_uw<R, false>(g, disp(r0, k, sg ? amt_j : -amt_j), T, pk, p);
       feat_add(hs, g);
     }
   for (int c = 0; c < 3; ++c) {
-    o.g0.a[c] += X * f0.a[c];
-    o.hsum.a[c] += X * hs.a[c];
+    acc[kP1G0 + c] += X * f0.a[c];
+    acc[kP1H + c] += X * hs.a[c];
   }
   for (int c = 0; c < 6; ++c) {
-    o.g0.l[c] += X * f0.l[c];
-    o.hsum.l[c] += X * hs.l[c];
+    acc[kP1G0 + 3 + c] += X * f0.l[c];
+    acc[kP1H + 3 + c] += X * hs.l[c];
   }
-  o.cross += X * X * bpair_r(hs, f0);
+  acc[kP1Cross] += X * X * bpair_r(hs, f0);
 }
 
+// Part II: G(d) += X f(r0 + d) for the six centre displacements d (part
+// index 1 + 9 d + c) and sself += X^2 sum_d B(f, f) (part index 0).
 template <class R>
-BTAM_HD void pass1_pair_A(const TablesView<R> &T, const V3<R> &r0, R sig_i,
-                          R sig_j, R xi, R xj, int ci, int cj, Pass1A<R> &o) {
-  R rho, epair, ediag;
-  pass1_pair_rule<R>(T, r0, sig_i, sig_j, xi, xj, ci, cj, rho, nullptr, epair, ediag);
-  o.rho += rho;
-  o.epair += epair;
-  o.ediag += ediag;
-  pass1_pair_trip<R>(T, r0, sig_j, xi * xj, pair_kind(ci, cj), o);
+BTAM_HD void pass1_pair_part2(const RadialView<R> &T, const V3<R> &r0, R sig_i, R X, int pk,
+                              R *acc) {
+  const R amt_i = sig_i * (R)kDelta9;
+  R ss = (R)0, p;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int sg = 0; sg < 2; ++sg) {
+      Geo<R> g;
+      geo_uw<R, false>(g, disp(r0, k, sg ? -amt_i : amt_i), T, pk, p);
+      feat_acc(acc, 1 + 9 * (2 * k + sg), g, X);
+      ss += bff(g);
+    }
+  acc[0] += X * X * ss;
 }
 
-// Pass 1, part B: one centre displacement d = (k, sg) of pair (i, j):
-//   gd    += X f(r0 + d),   sself += X^2 B(f, f)(r0 + d)
-template <class R>
-BTAM_HD void pass1_pair_B(const TablesView<R> &T, const V3<R> &r0, R sig_i,
-                          R X, int pk, int k, int sg, Feat<R> &gd, R &sself) {
-  Geo<R> g;
-  R amt = sig_i * (R)kDelta9;
-  geo_val(g, disp(r0, k, sg ? -amt : amt), T.t[T_U + pk], T.t[T_W + pk]);
-  Feat<R> f{};
-  feat_add(f, g);
-  for (int c = 0; c < 3; ++c) gd.a[c] += X * f.a[c];
-  for (int c = 0; c < 6; ++c) gd.l[c] += X * f.l[c];
-  sself += X * X * bff(g);
+// Flat pass-1 value of part II's local index t.
+BTAM_HD int p1_part2_value(int t) { return t == 0 ? kP1Sself : kP1Gd + (t - 1); }
+
+// Position of flat pass-1 value v in SiteSums viewed as an array of doubles.
+BTAM_HD int p1_site_slot(int v) {
+  if (v < kP1Gd) return v;
+  const int d = (v - kP1Gd) / 9, c = (v - kP1Gd) % 9;
+  return c < 3 ? kP1Gd + 3 * d + c : kP1Gd + 18 + 6 * d + (c - 3);
 }
 
 // ---------------------------------------------------------------------------
@@ -487,26 +693,31 @@ template <class R> BTAM_HD R ld_ro(const R *p) {
   return *p;
 #endif
 }
-template <class R, bool RO> BTAM_HD Dual<R> dual_at(const R *m) {
-  Dual<R> D;
-  for (int k = 0; k < 3; ++k) {
-    D.a[k] = RO ? ld_ro(m + k) : ld_plain(m + k);
-    D.d[k] = RO ? ld_ro(m + 3 + k) : ld_plain(m + 3 + k);
-    D.o[k] = RO ? ld_ro(m + 6 + k) : ld_plain(m + 6 + k);
+// A moment record in global memory (RO: read-only cached vector loads) or in
+// host / shared memory (plain loads).  The o2 components of its eight duals
+// are read once, with the record.
+template <class R, bool RO> struct MomRec {
+  const R *m;
+  R tail[8];
+  BTAM_HD explicit MomRec(const R *m_) : m(m_) {
+    if (RO) ld8(m + 72, tail);
+    else cp8(m + 72, tail);
   }
-  return D;
-}
+  BTAM_HD R scalar(int c) const { return RO ? ld_ro(m + c) : ld_plain(m + c); }
+  BTAM_HD Dual<R> dual(int k) const {
+    R h[8];
+    if (RO) ld8(m + 8 + 8 * k, h);
+    else cp8(m + 8 + 8 * k, h);
+    return dual_from(h, tail[k]);
+  }
+};
 
-template <class R>
-BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
+template <class R, class MU, class MJ>
+BTAM_HD void pass2_pair(const RadialView<R> &T, const V3<R> &r0, R sig_u,
                         R sig_j, R xu, R xj, int cu, int cj, R embq_u,
-                        R embq_j, R embx_j, R omega, const R *mu,
-                        const R *mj, Pass2Out<R> &o) {
+                        R embq_j, R embx_j, R omega, const MU &mu,
+                        const MJ &mj, Pass2Out<R> &o) {
   const int pk = pair_kind(cu, cj);
-  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
-                      &tp = T.t[T_PHI + pk];
-  const SplineView<R> &trj = T.t[cj == 0 ? T_RHO_MG : T_RHO_H];
-  const SplineView<R> &tru = T.t[cu == 0 ? T_RHO_MG : T_RHO_H];
   const R X = xu * xj;
   const R w6 = (R)kW6, w9 = (R)kW9;
 
@@ -516,17 +727,19 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
   // ---- 12-point pair rule geometries: u-displaced (C) and j-displaced (D)
   {
     R rho_sum = 0, phi_sum = 0, bff_sum = 0;
+#pragma unroll
     for (int side = 0; side < 2; ++side) {
       R amt = (side == 0 ? sig_u : -sig_j) * (R)kDelta6;
+#pragma unroll
       for (int k = 0; k < 3; ++k)
+#pragma unroll
         for (int sg = 0; sg < 2; ++sg) {
           R a = sg ? -amt : amt;
           Geo<R> g;
-          geo_eval(g, disp(r0, k, a), tu, tw);
+          R p;
+          const int m = geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
           R rj, drj, ru, dru, ph, dph;
-          spline_vd(trj, g.s, rj, drj);
-          spline_vd(tru, g.s, ru, dru);
-          spline_vd(tp, g.s, ph, dph);
+          pr_at<R, true, true>(T, pk, cu, cj, m, p, ph, dph, rj, drj, ru, dru);
           R bc = bff_grad_coef(g);
           // radial coefficient of d/dr for each piece
           R c_self = w6 * (embq_u * xj * drj * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
@@ -548,7 +761,10 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
 
   // ---- triplet geometries
   Geo<R> gc;
-  geo_eval(gc, r0, tu, tw);
+  {
+    R p;
+    geo_uw<R, true>(gc, r0, T, pk, p);
+  }
   const Dual<R> Xf0 = dual_feat(gc, X);  // dual of X f(r0)
 
   const R sfac = (R)2 * w9 * X;
@@ -557,19 +773,22 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
   // (X5) use fixed duals, so they go through the axis-displacement form.
   Feat<R> FA{};
   {
-    const Dual<R> Dj_g0 = dual_at<R, true>(mj + kMomG0);
+    const Dual<R> Dj_g0 = mj.dual(kDualG0);
     const Dual<R> Dc5 = dual_sub(dual_flip(Dj_g0), Xf0);
     const DualAx<R> c5 = dual_ax(Dc5, r0);
     const DualAx<R> x5 = dual_ax(dual_sub(Dc5, Xf0), r0);
     const R amt = sig_u * (R)kDelta9;
+#pragma unroll
     for (int k = 0; k < 3; ++k)
+#pragma unroll
       for (int sg = 0; sg < 2; ++sg) {
         const R a = sg ? -amt : amt;
         Geo<R> g;
-        geo_eval(g, disp(r0, k, a), tu, tw);
+        R p;
+        geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
         feat_add(FA, g);
         R hb = (R)0.5 * X * bff_grad_coef(g);
-        V3<R> v4 = dual_J(dual_at<R, false>(mu + kMomGd + 9 * (2 * k + sg)), g);  // S4
+        V3<R> v4 = dual_J(mu.dual(kDualGd + 2 * k + sg), g);  // S4
         V3<R> v5, vx;
         R f5, fx;
         dual_ax_at(c5, k, a, g, v5, f5);  // C5
@@ -588,19 +807,22 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
   // centre-displaced term (C4) with its occupancy gradient (X4).
   Feat<R> FB{};
   {
-    const DualAx<R> s5 = dual_ax(dual_sub(dual_at<R, false>(mu + kMomG0), Xf0), r0);
+    const DualAx<R> s5 = dual_ax(dual_sub(mu.dual(kDualG0), Xf0), r0);
     const R amt = sig_j * (R)kDelta9;
+#pragma unroll
     for (int k = 0; k < 3; ++k)
+#pragma unroll
       for (int sg = 0; sg < 2; ++sg) {
         const R a = sg ? amt : -amt;
         Geo<R> g;
-        geo_eval(g, disp(r0, k, a), tu, tw);
+        R p;
+        geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
         feat_add(FB, g);
         V3<R> v5;
         R f5;
         dual_ax_at(s5, k, a, g, v5, f5);
         self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
-        const Dual<R> Pj = dual_flip(dual_at<R, true>(mj + kMomGd + 9 * (2 * k + sg)));
+        const Dual<R> Pj = dual_flip(mj.dual(kDualGd + 2 * k + sg));
         V3<R> v4;
         R f4;
         dual_Jf(Pj, g, v4, f4);
@@ -619,8 +841,8 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
       dFB.a[k] *= X; dFB.d[k] *= X; dFB.o[k] *= X;
       dFA.a[k] *= X; dFA.d[k] *= X; dFA.o[k] *= X;
     }
-    const Dual<R> Dj_h = dual_at<R, true>(mj + kMomH);
-    V3<R> vs = dual_J(dual_sub(dual_at<R, false>(mu + kMomH), dFB), gc);
+    const Dual<R> Dj_h = mj.dual(kDualH);
+    V3<R> vs = dual_J(dual_sub(mu.dual(kDualH), dFB), gc);
     V3<R> vc = dual_J(dual_sub(dual_flip(Dj_h), dFA), gc);
     self_q[0] += sfac * vs.x; self_q[1] += sfac * vs.y; self_q[2] += sfac * vs.z;
     cros_q[0] += sfac * vc.x; cros_q[1] += sfac * vc.y; cros_q[2] += sfac * vc.z;
@@ -646,17 +868,15 @@ BTAM_HD void pass2_pair(const TablesView<R> &T, const V3<R> &r0, R sig_u,
 // so oj.gq = -cros_q - omega_ju self_q; the width and occupancy gradients of
 // j take the sigma_j and x_u derivatives of the same terms (rself_s, rcros_s,
 // rcros_x).  mu, mj: moment records of u and of j's owner; omega_uj =
-// beta_j / beta_u, omega_ju = beta_u / beta_j.
-template <class R>
-BTAM_HD void pass2_pair_sym(const TablesView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
+// beta_j / beta_u, omega_ju = beta_u / beta_j; pr: the pair's record from
+// pair_rule_record (its 12 pair-rule points were evaluated once, in pass 1;
+// only the 13 triplet geometries are evaluated here).
+template <class R, class MU, class MJ>
+BTAM_HD void pass2_pair_sym(const RadialView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
                             R xj, int cu, int cj, R embq_u, R embx_u, R embq_j, R embx_j,
-                            R omega_uj, R omega_ju, const R *mu, const R *mj,
-                            Pass2Out<R> &ou, Pass2Out<R> &oj) {
+                            R omega_uj, R omega_ju, const MU &mu, const MJ &mj,
+                            const R (&pr)[kPrRec], Pass2Out<R> &ou, Pass2Out<R> &oj) {
   const int pk = pair_kind(cu, cj);
-  const SplineView<R> &tu = T.t[T_U + pk], &tw = T.t[T_W + pk],
-                      &tp = T.t[T_PHI + pk];
-  const SplineView<R> &trj = T.t[cj == 0 ? T_RHO_MG : T_RHO_H];
-  const SplineView<R> &tru = T.t[cu == 0 ? T_RHO_MG : T_RHO_H];
   const R X = xu * xj;
   const R w6 = (R)kW6, w9 = (R)kW9;
 
@@ -666,67 +886,51 @@ BTAM_HD void pass2_pair_sym(const TablesView<R> &T, const V3<R> &r0, R sig_u, R 
   // j's view: d/dsigma_j of V0_j (rself_s) and of V0_u (rcros_s), d/dx_j of V0_u
   R rself_s = 0, rcros_s = 0, rcros_x = 0;
 
-  // ---- 12-point pair rule: side 0 moves u (sigma_u), side 1 moves j (sigma_j)
+  // ---- 12-point pair rule, from the pair's record (pair_rule_record)
   {
-    R rho_u_sum = 0, rho_j_sum = 0, phi_sum = 0, bff_sum = 0;
-    for (int side = 0; side < 2; ++side) {
-      R amt = (side == 0 ? sig_u : -sig_j) * (R)kDelta6;
-      for (int k = 0; k < 3; ++k)
-        for (int sg = 0; sg < 2; ++sg) {
-          R a = sg ? -amt : amt;
-          Geo<R> g;
-          geo_eval(g, disp(r0, k, a), tu, tw);
-          R rj, drj, ru, dru, ph, dph;
-          spline_vd(trj, g.s, rj, drj);
-          spline_vd(tru, g.s, ru, dru);
-          spline_vd(tp, g.s, ph, dph);
-          R bc = bff_grad_coef(g);
-          R c_self = w6 * (embq_u * xj * drj * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
-          R c_cros = w6 * (embq_j * xu * dru * g.inv_s + (R)0.5 * X * dph * g.inv_s + X * X * bc);
-          self_q[0] += c_self * g.r.x; self_q[1] += c_self * g.r.y; self_q[2] += c_self * g.r.z;
-          cros_q[0] += c_cros * g.r.x; cros_q[1] += c_cros * g.r.y; cros_q[2] += c_cros * g.r.z;
-          if (side == 0) {
-            R sd = (sg ? -(R)kDelta6 : (R)kDelta6) * comp(g.r, k);
-            self_s += c_self * sd;
-            cros_s += c_cros * sd;
-          } else {  // r = r0 + (sg ? +1 : -1) sqrt6 sigma_j e_k
-            R sd = (sg ? (R)kDelta6 : -(R)kDelta6) * comp(g.r, k);
-            rself_s += c_cros * sd;
-            rcros_s += c_self * sd;
-          }
-          rho_u_sum += ru;
-          rho_j_sum += rj;
-          phi_sum += ph;
-          bff_sum += bff(g);
-        }
+    const R ku = embq_u * xj, kj = embq_j * xu;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      self_q[c] = w6 * (ku * pr[4 + c] + pr[10 + c]);
+      cros_q[c] = w6 * (kj * pr[7 + c] + pr[10 + c]);
     }
-    cros_x += w6 * (embx_j * rho_u_sum + (R)0.5 * xj * phi_sum + (R)2 * X * xj * bff_sum);
-    rcros_x += w6 * (embx_u * rho_j_sum + (R)0.5 * xu * phi_sum + (R)2 * X * xu * bff_sum);
+    self_s = w6 * (ku * pr[13] + pr[15]);
+    cros_s = w6 * (kj * pr[14] + pr[15]);
+    rself_s = w6 * (kj * pr[17] + pr[18]);
+    rcros_s = w6 * (ku * pr[16] + pr[18]);
+    cros_x = w6 * (embx_j * pr[0] + (R)0.5 * xj * pr[2] + (R)2 * X * xj * pr[3]);
+    rcros_x = w6 * (embx_u * pr[1] + (R)0.5 * xu * pr[2] + (R)2 * X * xu * pr[3]);
   }
 
   // ---- triplet geometries
   Geo<R> gc;
-  geo_eval(gc, r0, tu, tw);
+  {
+    R p;
+    geo_uw<R, true>(gc, r0, T, pk, p);
+  }
   const Dual<R> Xf0 = dual_feat(gc, X);
   const R sfac = (R)2 * w9 * X;
   // A: u displaced by +-3 sigma_u e_k (j's neighbour-displaced points)
   Feat<R> FA{};
   {
-    const Dual<R> Dj_g0 = dual_at<R, true>(mj + kMomG0);
+    const Dual<R> Dj_g0 = mj.dual(kDualG0);
     const Dual<R> Dc5 = dual_sub(dual_flip(Dj_g0), Xf0);
     const DualAx<R> c5 = dual_ax(Dc5, r0);
     const DualAx<R> x5 = dual_ax(dual_sub(Dc5, Xf0), r0);
     const R amt = sig_u * (R)kDelta9;
+#pragma unroll
     for (int k = 0; k < 3; ++k)
+#pragma unroll
       for (int sg = 0; sg < 2; ++sg) {
         const R a = sg ? -amt : amt;
         Geo<R> g;
-        geo_eval(g, disp(r0, k, a), tu, tw);
+        R p;
+        geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
         feat_add(FA, g);
         R hb = (R)0.5 * X * bff_grad_coef(g);
         V3<R> v4;
         R f4u;
-        dual_Jf(dual_at<R, true>(mu + kMomGd + 9 * (2 * k + sg)), g, v4, f4u);  // S4
+        dual_Jf(mu.dual(kDualGd + 2 * k + sg), g, v4, f4u);  // S4
         V3<R> v5, vx;
         R f5, fx;
         dual_ax_at(c5, k, a, g, v5, f5);  // C5
@@ -745,22 +949,25 @@ BTAM_HD void pass2_pair_sym(const TablesView<R> &T, const V3<R> &r0, R sig_u, R 
   // B: j displaced by -+3 sigma_j e_k (j's centre-displaced points)
   Feat<R> FB{};
   {
-    const Dual<R> Du_g0 = dual_at<R, true>(mu + kMomG0);
+    const Dual<R> Du_g0 = mu.dual(kDualG0);
     const DualAx<R> s5 = dual_ax(dual_sub(Du_g0, Xf0), r0);
     const DualAx<R> xf = dual_ax(Xf0, r0);
     const R amt = sig_j * (R)kDelta9;
+#pragma unroll
     for (int k = 0; k < 3; ++k)
+#pragma unroll
       for (int sg = 0; sg < 2; ++sg) {
         const R a = sg ? amt : -amt;
         Geo<R> g;
-        geo_eval(g, disp(r0, k, a), tu, tw);
+        R p;
+        geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
         feat_add(FB, g);
         V3<R> v5, vxf;
         R f5, fxf;
         dual_ax_at(s5, k, a, g, v5, f5);  // S5
         dual_ax_at(xf, k, a, g, vxf, fxf);
         self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
-        const Dual<R> Pj = dual_flip(dual_at<R, true>(mj + kMomGd + 9 * (2 * k + sg)));
+        const Dual<R> Pj = dual_flip(mj.dual(kDualGd + 2 * k + sg));
         V3<R> v4;
         R f4;
         dual_Jf(Pj, g, v4, f4);  // C4
@@ -784,8 +991,8 @@ BTAM_HD void pass2_pair_sym(const TablesView<R> &T, const V3<R> &r0, R sig_u, R 
       dFB.a[k] *= X; dFB.d[k] *= X; dFB.o[k] *= X;
       dFA.a[k] *= X; dFA.d[k] *= X; dFA.o[k] *= X;
     }
-    const Dual<R> Dj_h = dual_at<R, true>(mj + kMomH);
-    const Dual<R> Du_h = dual_at<R, true>(mu + kMomH);
+    const Dual<R> Dj_h = mj.dual(kDualH);
+    const Dual<R> Du_h = mu.dual(kDualH);
     V3<R> vs = dual_J(dual_sub(Du_h, dFB), gc);
     V3<R> vc = dual_J(dual_sub(dual_flip(Dj_h), dFA), gc);
     self_q[0] += sfac * vs.x; self_q[1] += sfac * vs.y; self_q[2] += sfac * vs.z;
@@ -806,7 +1013,7 @@ BTAM_HD void pass2_pair_sym(const TablesView<R> &T, const V3<R> &r0, R sig_u, R 
 
 // ---------------------------------------------------------------------------
 // Per-site epilogue of pass 1, in double.  Inputs are the raw sums over the
-// site's active neighbours (Pass1A fields and the six G(d) sums).
+// site's active neighbours (the pass-1 values, kP1Rho ... kP1Gd).
 struct SiteSums {
   double rho, epair, ediag, cross, sself;
   double g0a[3], g0l[6], ha[3], hl[6];
@@ -824,18 +1031,27 @@ constexpr double kUma = 103.4993333E-6;     // eV A^-2 ps^2 per amu
 // Energy of one site:  V0_i = x_i F(rho) + E_pair + E_angular
 // (evaluate_V0_i_adp_MgHx, MgHx-mf-V-bulk.cpp:791-953), its free entropy
 // S0_i (evaluate_S0_i_adp_MgHx, 957-1142), dV0_i/dx_i, and the moment
-// record for pass 2 (layout at kMomStride).
+// record for pass 2 (layout at kMomStride).  In two parts so that a warp can
+// run them on several lanes: site_dual forms dual k of the record (k = 0:
+// G0, 1: H, 2 + d: G(d)) and returns B(G(d), G(d)) for the G(d) duals;
+// site_scalars takes bgd = sum_d B(G(d), G(d)) (summed in d order) and does
+// the rest.
+template <class M> BTAM_HD double site_dual(const SiteSums &S, int k, M *mom) {
+  const double *a = k == 0 ? S.g0a : (k == 1 ? S.ha : S.gda[k - 2]);
+  const double *l = k == 0 ? S.g0l : (k == 1 ? S.hl : S.gdl[k - 2]);
+  if (mom) store_dual(mom, k, dual_of<double, double>(a, l));
+  return k >= 2 ? bself(a, l) : 0.0;
+}
+
 template <class M>
-BTAM_HD void site_epilogue(const SiteSums &S, const SplineView<double> &emb,
-                           double xi, int code, double beta, double gamma,
-                           double sigma, double mass, SiteResult &res, M *mom) {
+BTAM_HD void site_scalars(const SiteSums &S, double bgd, const SplineView<double> &emb,
+                          double xi, int code, double beta, double gamma, double sigma,
+                          double mass, SiteResult &res, M *mom) {
   const double rho = kW6 * S.rho;
   double F, dF;
   spline_vd(emb, rho, F, dF);
   const double e_pair = kW6 * S.epair;
   const double e_diag = kW6 * S.ediag;
-  double bgd = 0.0;
-  for (int d = 0; d < 6; ++d) bgd += bself(S.gda[d], S.gdl[d]);
   const double e_id = kW9 * (bgd - S.sself);
   const double e_jd = 2.0 * kW9 * (bpair(S.ha, S.hl, S.g0a, S.g0l) - S.cross);
   const double e_ang = e_id + e_jd + e_diag;
@@ -855,12 +1071,20 @@ BTAM_HD void site_epilogue(const SiteSums &S, const SplineView<double> &emb,
     mom[0] = (M)(xi * dF);
     mom[1] = (M)((code == 1 ? xi : 1.0) * dF);
     mom[2] = (M)beta;
-    mom[3] = (M)0;
-    store_dual(mom + kMomG0, dual_of<double, double>(S.g0a, S.g0l));
-    store_dual(mom + kMomH, dual_of<double, double>(S.ha, S.hl));
-    for (int d = 0; d < 6; ++d)
-      store_dual(mom + kMomGd + 9 * d, dual_of<double, double>(S.gda[d], S.gdl[d]));
+    for (int c = 3; c < 8; ++c) mom[c] = (M)0;
   }
+}
+
+template <class M>
+BTAM_HD void site_epilogue(const SiteSums &S, const SplineView<double> &emb,
+                           double xi, int code, double beta, double gamma,
+                           double sigma, double mass, SiteResult &res, M *mom) {
+  double bgd = 0.0;
+  for (int k = 0; k < 8; ++k) {
+    const double b = site_dual(S, k, mom);
+    if (k >= 2) bgd += b;
+  }
+  site_scalars(S, bgd, emb, xi, code, beta, gamma, sigma, mass, res, mom);
 }
 
 // Residual epilogue of pass 2 for site u (H sites also get the occupancy

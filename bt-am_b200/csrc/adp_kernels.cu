@@ -94,54 +94,103 @@ __device__ __forceinline__ void ld_rec(const double *p, double (&v)[8]) {
                : "l"(p + 4));
 }
 
-// First half of a record (pass 1: rho, epair, ediag, 0).
-__device__ __forceinline__ void st_rec4(float *p, const float (&v)[4]) {
-  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
-}
-__device__ __forceinline__ void st_rec4(double *p, const double (&v)[4]) {
-  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
-               "d"(v[2]), "d"(v[3])
-               : "memory");
-}
-__device__ __forceinline__ void ld_rec4(const float *p, float (&v)[4]) {
-  float4 t = __ldg(reinterpret_cast<const float4 *>(p));
-  v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-}
-__device__ __forceinline__ void ld_rec4(const double *p, double (&v)[4]) {
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
-               : "l"(p));
-}
 
-// One thread per owned slot p = (u, j): the 12-point pair-rule sums of the
-// pair, shared by both directions (the reverse pair's points are the same
-// set negated), into slot p and the reverse slot.
+// One thread per owned pair t = (u, j): the pair's 12-point pair-rule record
+// (pair_rule_record), shared by pass 1 of both sites and by pass 2.  Pairs
+// with an empty site get a zero record.
 template <class R, int TPB>
 __global__ void __launch_bounds__(TPB)
 pass1u_pair_kernel(const EvalArgs<R> a) {
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
     const int p = a.own_p[t], u = a.own_u[t];
-    const int j = a.idx[p], r = a.rev[p];
+    const int j = a.idx[p];
     const double2 xbu = a.xb[u], xbj = a.xb[j];
-    R vu[4] = {(R)0, (R)0, (R)0, (R)0}, vj[4] = {(R)0, (R)0, (R)0, (R)0};
+    R rec[kPrRec];
     if (!(xbu.x < kMinOcc) && !(xbj.x < kMinOcc)) {
       const double4 qu = a.pos[u], qj = a.pos[j];
-      R rj, ri, ep, ed;
-      pass1_pair_rule<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
-                         a.code[u], a.code[j], rj, &ri, ep, ed);
-      vu[0] = rj; vu[1] = ep; vu[2] = ed;
-      vj[0] = ri; vj[1] = ep; vj[2] = ed;
+      pair_rule_record<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
+                          a.code[u], a.code[j], rec);
+    } else {
+#pragma unroll
+      for (int c = 0; c < kPrRec; ++c) rec[c] = (R)0;
     }
-    st_rec4(a.pbuf + 8 * (size_t)p, vu);
-    if (r >= 0) st_rec4(a.pbuf + 8 * (size_t)r, vj);
+    R *dst = a.prec + (size_t)kPrRec * t;
+#pragma unroll
+    for (int h = 0; h < kPrRec / 8; ++h) {
+      R v[8];
+#pragma unroll
+      for (int c = 0; c < 8; ++c) v[c] = rec[8 * h + c];
+      st_rec(dst + 8 * h, v);
+    }
   }
+}
+
+// Sum over the 32 lanes of a warp of each lane's N partials (N a multiple of
+// 32), by recursive halving: at each level a lane keeps half of its current
+// index range and adds its partner's values for that half (partner lane ^ 16,
+// 8, 4, 2, 1).  In the FP32 form every addition is a two-sum and the
+// rounding errors ride along as a second FP32 word (lo), so the per-site
+// totals are compensated sums of the lanes' partials.  Lane L ends with the
+// totals of values base(L) + [0, N/32), base = N/2 b4 + N/4 b3 + N/8 b2 +
+// N/16 b1 + N/32 b0 (b = bits of L), in v[0..N/32) (+ lo[0..N/32)).
+template <int N, int M, bool FIRST, class R, int CAP>
+__device__ __forceinline__ void halve_level(R (&v)[CAP], R (&lo)[CAP], int lane) {
+  const bool up = (lane & M) != 0;
+#pragma unroll
+  for (int k = 0; k < N / 2; ++k) {
+    const R keep = up ? v[N / 2 + k] : v[k];
+    const R give = up ? v[k] : v[N / 2 + k];
+    const R got = __shfl_xor_sync(0xffffffffu, give, M);
+    if (sizeof(R) == 4) {
+      R keep_lo = (R)0, got_lo = (R)0;
+      if (!FIRST) {
+        keep_lo = up ? lo[N / 2 + k] : lo[k];
+        const R give_lo = up ? lo[k] : lo[N / 2 + k];
+        got_lo = __shfl_xor_sync(0xffffffffu, give_lo, M);
+      }
+      const R s = keep + got;
+      const R bp = s - keep;
+      const R e = (keep - (s - bp)) + (got - bp);
+      v[k] = s;
+      lo[k] = (keep_lo + got_lo) + e;
+    } else {
+      v[k] = keep + got;
+    }
+  }
+}
+
+template <int N, class R> __device__ __forceinline__ void lane_tree(R (&v)[N], R (&lo)[N], int lane) {
+  if (sizeof(R) != 4) {  // FP64: no compensation word
+#pragma unroll
+    for (int k = 0; k < N; ++k) lo[k] = (R)0;
+  }
+  halve_level<N, 16, true>(v, lo, lane);
+  halve_level<N / 2, 8, false>(v, lo, lane);
+  halve_level<N / 4, 4, false>(v, lo, lane);
+  halve_level<N / 8, 2, false>(v, lo, lane);
+  halve_level<N / 16, 1, false>(v, lo, lane);
+}
+template <int N> __device__ __forceinline__ int lane_tree_base(int lane) {
+  return (N / 2) * ((lane >> 4) & 1) + (N / 4) * ((lane >> 3) & 1) + (N / 8) * ((lane >> 2) & 1) +
+         (N / 16) * ((lane >> 1) & 1) + (N / 32) * (lane & 1);
+}
+// The total of a lane_tree value: hi + lo in the FP32 form; the FP64 form
+// carries no lo word (its lo array is never written).
+template <class R> __device__ __forceinline__ double tree_total(R hi, R lo) {
+  return sizeof(R) == 4 ? (double)hi + (double)lo : (double)hi;
 }
 
 // Kernels are instantiated for several (warps per block, minimum resident
 // blocks) shapes; the second number caps the registers per thread and so
 // trades instruction-level parallelism for occupancy.  btam_autotune times
 // the shapes on the actual system and keeps the fastest.
+// Pass 1: one warp per site, one lane per neighbour, in two parts (pass1_pair_part1
+// and _part2, so that few accumulators are live at once): each lane
+// evaluates its pair's 13 triplet geometries (and, unless UND, its 12
+// pair-rule points) and adds them to its own FP32 partials (at most
+// ceil(250 / 32) = 8 pairs per lane); the warp then forms the per-site
+// compensated totals (lane_tree) and lane 0 runs the FP64 epilogue.
 // UND: the pair-rule sums (rho, phi, B(f, f) over the 12 pair points) come
 // from the slot records written by pass1u_pair_kernel instead of being
 // evaluated here.
@@ -149,7 +198,6 @@ template <class R, int W, int MB, bool UND>
 __global__ void __launch_bounds__(W * 32, MB)
 pass1_kernel(const EvalArgs<R> a) {
   __shared__ SiteSums ss[W];
-  __shared__ double xbuf[W][30][10];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   // grid-stride over sites: one site per warp per trip (a full grid makes one
   // trip; a persistent grid of a few blocks per SM makes several)
@@ -168,98 +216,71 @@ pass1_kernel(const EvalArgs<R> a) {
   const double4 qi = a.pos[i];
   const int ci = a.code[i];
   const int nb0 = a.offs[i], nb1 = a.offs[i + 1];
-
-  // ---- phase A
-  Acc<R> acc[22];
-  for (int p = nb0 + lane; p < nb1; p += 32) {
-    const int j = a.idx[p];
-    const double2 xbj = a.xb[j];
-    if (xbj.x < kMinOcc) continue;
-    const double4 qj = a.pos[j];
-    Pass1A<R> o;
-    o.rho = o.epair = o.ediag = o.cross = (R)0;
-    for (int c = 0; c < 3; ++c) o.g0.a[c] = o.hsum.a[c] = (R)0;
-    for (int c = 0; c < 6; ++c) o.g0.l[c] = o.hsum.l[c] = (R)0;
-    if (UND) {
-      R rec[4];
-      ld_rec4(a.pbuf + 8 * (size_t)p, rec);
-      o.rho = rec[0];
-      o.epair = rec[1];
-      o.ediag = rec[2];
-      pass1_pair_trip<R>(a.T, pair_vec<R>(qi, qj), (R)qj.w, (R)xi * (R)xbj.x,
-                         pair_kind(ci, a.code[j]), o);
-    } else {
-      pass1_pair_A<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)qj.w, (R)xi, (R)xbj.x, ci,
-                      a.code[j], o);
-    }
-    acc[0].add(o.rho);
-    acc[1].add(o.epair);
-    acc[2].add(o.ediag);
-    acc[3].add(o.cross);
-    for (int c = 0; c < 3; ++c) {
-      acc[4 + c].add(o.g0.a[c]);
-      acc[13 + c].add(o.hsum.a[c]);
-    }
-    for (int c = 0; c < 6; ++c) {
-      acc[7 + c].add(o.g0.l[c]);
-      acc[16 + c].add(o.hsum.l[c]);
-    }
-  }
-  double tot[22];
+  double *site = reinterpret_cast<double *>(&ss[warp]);
+  {  // part I: pair rule, centre and neighbour-displaced points
+    R acc[kP1PartI], lo[kP1PartI];
 #pragma unroll
-  for (int c = 0; c < 22; ++c) tot[c] = warp_sum(acc[c].get());
-
-  // ---- phase B
-  if (lane < 30) {
-    const int d = lane % 6, g = lane / 6, k = d >> 1, sg = d & 1;
-    Acc<R> b[10];
-    for (int p = nb0 + g; p < nb1; p += 5) {
+    for (int c = 0; c < kP1PartI; ++c) acc[c] = (R)0;
+#pragma unroll 1
+    for (int p = nb0 + lane; p < nb1; p += 32) {
       const int j = a.idx[p];
       const double2 xbj = a.xb[j];
       if (xbj.x < kMinOcc) continue;
       const double4 qj = a.pos[j];
-      Feat<R> gd;
-      for (int c = 0; c < 3; ++c) gd.a[c] = (R)0;
-      for (int c = 0; c < 6; ++c) gd.l[c] = (R)0;
-      R s = (R)0;
-      pass1_pair_B<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)(xi * xbj.x),
-                      pair_kind(ci, a.code[j]), k, sg, gd, s);
-      for (int c = 0; c < 3; ++c) b[c].add(gd.a[c]);
-      for (int c = 0; c < 6; ++c) b[3 + c].add(gd.l[c]);
-      b[9].add(s);
+      const int cj = a.code[j];
+      const V3<R> r0 = pair_vec<R>(qi, qj);
+      if (UND) {
+        const int so = a.slot_own[p];
+        R rec[4];
+        ld4(a.prec + (size_t)kPrRec * (so >> 1), rec);
+        const R xj = (R)xbj.x, X = (R)xi * xj;
+        acc[kP1Rho] += xj * rec[(so & 1) ? 0 : 1];
+        acc[kP1Epair] += (R)0.5 * X * rec[2];
+        acc[kP1Ediag] += X * X * rec[3];
+      } else {
+        R rj, ep, ed;
+        pass1_pair_rule<R>(a.T, r0, (R)qi.w, (R)qj.w, (R)xi, (R)xbj.x, ci, cj, rj, nullptr, ep,
+                           ed);
+        acc[kP1Rho] += rj;
+        acc[kP1Epair] += ep;
+        acc[kP1Ediag] += ed;
+      }
+      pass1_pair_part1<R>(a.T, r0, (R)qj.w, (R)xi * (R)xbj.x, pair_kind(ci, cj), acc);
     }
-    for (int c = 0; c < 10; ++c) xbuf[warp][lane][c] = b[c].get();
+    lane_tree<kP1PartI>(acc, lo, lane);
+    const int v = lane_tree_base<kP1PartI>(lane);
+    if (v < kP1Gd && v != kP1Sself) site[p1_site_slot(v)] = tree_total(acc[0], lo[0]);
+  }
+  {  // part II: centre-displaced points
+    R acc[kP1PartII], lo[kP1PartII];
+#pragma unroll
+    for (int c = 0; c < kP1PartII; ++c) acc[c] = (R)0;
+#pragma unroll 1
+    for (int p = nb0 + lane; p < nb1; p += 32) {
+      const int j = a.idx[p];
+      const double2 xbj = a.xb[j];
+      if (xbj.x < kMinOcc) continue;
+      const double4 qj = a.pos[j];
+      pass1_pair_part2<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)xi * (R)xbj.x,
+                          pair_kind(ci, a.code[j]), acc);
+    }
+    lane_tree<kP1PartII>(acc, lo, lane);
+    const int t0 = lane_tree_base<kP1PartII>(lane);
+#pragma unroll
+    for (int k = 0; k < kP1PartII / 32; ++k)
+      if (t0 + k < 1 + 54) site[p1_site_slot(p1_part2_value(t0 + k))] = tree_total(acc[k], lo[k]);
   }
   __syncwarp();
-  SiteSums &S = ss[warp];
-  if (lane < 6) {
-    double t[10];
-    for (int c = 0; c < 10; ++c) t[c] = 0.0;
-    for (int g = 0; g < 5; ++g)
-      for (int c = 0; c < 10; ++c) t[c] += xbuf[warp][lane + 6 * g][c];
-    for (int c = 0; c < 3; ++c) S.gda[lane][c] = t[c];
-    for (int c = 0; c < 6; ++c) S.gdl[lane][c] = t[3 + c];
-    xbuf[warp][lane][0] = t[9];
-  }
-  __syncwarp();
+  // epilogue: lanes 0..7 form the record's eight duals, lane 0 the rest
+  double b = 0.0;
+  if (lane < 8) b = site_dual(ss[warp], lane, mom);
+  double bgd = 0.0;
+#pragma unroll
+  for (int d = 0; d < 6; ++d) bgd += __shfl_sync(0xffffffffu, b, 2 + d);
   if (lane == 0) {
-    S.rho = tot[0];
-    S.epair = tot[1];
-    S.ediag = tot[2];
-    S.cross = tot[3];
-    for (int c = 0; c < 3; ++c) {
-      S.g0a[c] = tot[4 + c];
-      S.ha[c] = tot[13 + c];
-    }
-    for (int c = 0; c < 6; ++c) {
-      S.g0l[c] = tot[7 + c];
-      S.hl[c] = tot[16 + c];
-    }
-    double sself = 0.0;
-    for (int d = 0; d < 6; ++d) sself += xbuf[warp][d][0];
-    S.sself = sself;
     SiteResult res;
-    site_epilogue(S, a.emb[ci], xi, ci, xbi.y, a.gamma[i], qi.w, a.mass[ci], res, mom);
+    site_scalars(ss[warp], bgd, a.emb[ci], xi, ci, xbi.y, a.gamma[i], qi.w, a.mass[ci], res,
+                 mom);
     a.rho[i] = res.rho;
     a.V0[i] = res.V0;
     a.S0[i] = res.S0;
@@ -292,7 +313,7 @@ pass2_kernel(const EvalArgs<R> a) {
   const R *mu_g = a.mom + (size_t)u * kMomStride;
   for (int c = lane; c < kMomStride; c += 32) mu_s[warp][c] = mu_g[c];
   __syncwarp();
-  const R *mu = mu_s[warp];
+  const MomRec<R, false> mu(mu_s[warp]);
   const double4 qu = a.pos[u];
   const int cu = a.code[u];
   const int nb0 = a.offs[u], nb1 = a.offs[u + 1];
@@ -303,12 +324,12 @@ pass2_kernel(const EvalArgs<R> a) {
     if (xbj.x < kMinOcc) continue;
     const int o = a.owner[j];
     const double4 qj = a.pos[j];
-    const R *mj = a.mom + (size_t)o * kMomStride;
+    const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
     Pass2Out<R> out;
     out.gq[0] = out.gq[1] = out.gq[2] = out.gs = out.gx = (R)0;
     pass2_pair<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xu, (R)xbj.x, cu,
-                  a.code[j], mu[0], ld_ro(mj), ld_ro(mj + 1), (R)(xbj.y / xbu.y), mu, mj,
-                  out);
+                  a.code[j], mu.scalar(0), mj.scalar(0), mj.scalar(1), (R)(xbj.y / xbu.y), mu,
+                  mj, out);
     acc[0].add(out.gq[0]);
     acc[1].add(out.gq[1]);
     acc[2].add(out.gq[2]);
@@ -353,14 +374,24 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
     if (!(xbu.x < kMinOcc) && !(xbj.x < kMinOcc)) {
       const int o = a.owner[j];
       const double4 qu = a.pos[u], qj = a.pos[j];
-      const R *mu = a.mom + (size_t)u * kMomStride;
-      const R *mj = a.mom + (size_t)o * kMomStride;
+      const MomRec<R, true> mu(a.mom + (size_t)u * kMomStride);
+      const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
       Pass2Out<R> ou, oj;
       ou.gq[0] = ou.gq[1] = ou.gq[2] = ou.gs = ou.gx = (R)0;
       oj.gq[0] = oj.gq[1] = oj.gq[2] = oj.gs = oj.gx = (R)0;
+      R pr[kPrRec];
+      const R *src = a.prec + (size_t)kPrRec * t;
+#pragma unroll
+      for (int h = 0; h < kPrRec / 8; ++h) {
+        R v[8];
+        ld8(src + 8 * h, v);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) pr[8 * h + c] = v[c];
+      }
       pass2_pair_sym<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
-                        a.code[u], a.code[j], ld_ro(mu), ld_ro(mu + 1), ld_ro(mj),
-                        ld_ro(mj + 1), (R)(xbj.y / xbu.y), (R)(xbu.y / xbj.y), mu, mj, ou, oj);
+                        a.code[u], a.code[j], mu.scalar(0), mu.scalar(1), mj.scalar(0),
+                        mj.scalar(1), (R)(xbj.y / xbu.y), (R)(xbu.y / xbj.y), mu, mj, pr, ou,
+                        oj);
       vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
       vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
     }
@@ -526,15 +557,18 @@ template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st
   k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
 }
 
-template <class R> cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v) {
+template <class R>
+cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2) {
   if (a.n_real <= 0) return cudaSuccess;
   const bool pers = (v & kPersistent) != 0;
-  const bool und = (v & kUndirected) != 0 && has_undirected(a.rev, a.pbuf);
+  // the pair-rule records are made (and then also used by pass 1) whenever
+  // either pass runs undirected: the undirected pass 2 reads them
+  const bool und = ((v | v2) & kUndirected) != 0 && has_undirected(a);
   switch (v & (kPersistent - 1)) {
   case 1: go1<R, 4, 3>(a, st, pers, und); break;
   case 2: go1<R, 4, 4>(a, st, pers, und); break;
   case 3: go1<R, 8, 2>(a, st, pers, und); break;
-  case 4: go1<R, 2, 8>(a, st, pers, und); break;
+  case 4: go1<R, 4, 5>(a, st, pers, und); break;
   default: go1<R, 4, 1>(a, st, pers, und); break;
   }
   return cudaGetLastError();
@@ -559,7 +593,7 @@ template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t s
   if (a.n_real <= 0) return cudaSuccess;
   const bool pers = (v & kPersistent) != 0;
   if (v & kUndirected) {
-    if (!has_undirected(a.rev, a.pbuf)) {
+    if (!has_undirected(a)) {
       go2<R, 4, 1>(a, st, false);
       return cudaGetLastError();
     }
@@ -581,14 +615,16 @@ template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t s
   }
   return cudaGetLastError();
 }
-template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t, int);
-template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, int);
+template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t, int, int);
+template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, int, int);
 template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t, int);
 template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t, int);
 
-// Times every launch variant of pass 1 (block shapes, each with a full grid
-// and a persistent grid), then of pass 2 after the best pass 1 has written the
-// moments pass 2 reads; best of reps launches each.
+// Times every launch variant: for each form (directed; undirected when the
+// pair links exist) every pass-1 shape with a full and a persistent grid,
+// then every pass-2 shape of that form after the form's best pass 1 has
+// written the moments (and records) pass 2 reads; best of reps launches
+// each.  The form with the smaller pass-1 + pass-2 time wins.
 template <class R>
 cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int *best1,
                             int *best2) {
@@ -600,11 +636,11 @@ cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int
     cudaEventDestroy(e0);
     return e;
   }
-  auto time_one = [&](bool second, int v) -> float {
+  auto time_one = [&](bool second, int v, int v2) -> float {
     float best = 1e30f;
     for (int r = 0; r < reps && e == cudaSuccess; ++r) {
       e = cudaEventRecord(e0, st);
-      if (e == cudaSuccess) e = second ? launch_pass2(a, st, v) : launch_pass1(a, st, v);
+      if (e == cudaSuccess) e = second ? launch_pass2(a, st, v) : launch_pass1(a, st, v, v2);
       if (e == cudaSuccess) e = cudaEventRecord(e1, st);
       if (e == cudaSuccess) e = cudaEventSynchronize(e1);
       float ms = 0.f;
@@ -614,28 +650,32 @@ cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int
     return best;
   };
   int b1 = 0, b2 = 0;
-  float t1 = 1e30f, t2 = 1e30f;
-  const int n_forms1 = has_undirected(a.rev, a.pbuf) ? 2 : 1;
-  for (int u = 0; u < n_forms1; ++u)
+  float best_total = 1e30f;
+  const int n_forms = has_undirected(a) ? 2 : 1;
+  for (int u = 0; u < n_forms && e == cudaSuccess; ++u) {
+    const int form = u ? kUndirected : 0;
+    int f1 = form, f2 = form;
+    float t1 = 1e30f, t2 = 1e30f;
     for (int p = 0; p < 2; ++p)
       for (int v = 0; v < kPass1Variants && e == cudaSuccess; ++v) {
-        const int var = v | (p ? kPersistent : 0) | (u ? kUndirected : 0);
-        float t = time_one(false, var);
-        if (t < t1) { t1 = t; b1 = var; }
+        const int var = v | (p ? kPersistent : 0) | form;
+        float t = time_one(false, var, form);
+        if (t < t1) { t1 = t; f1 = var; }
       }
-  if (e == cudaSuccess) e = launch_pass1(a, st, b1);
-  for (int p = 0; p < 2; ++p)
-    for (int v = 0; v < kPass2Variants && e == cudaSuccess; ++v) {
-      float t = time_one(true, v | (p ? kPersistent : 0));
-      if (t < t2) { t2 = t; b2 = v | (p ? kPersistent : 0); }
-    }
-  if (has_undirected(a.rev, a.pbuf))
+    if (e == cudaSuccess) e = launch_pass1(a, st, f1, form);
+    const int n2 = u ? kPass2UVariants : kPass2Variants;
     for (int p = 0; p < 2; ++p)
-      for (int v = 0; v < kPass2UVariants && e == cudaSuccess; ++v) {
-        const int var = v | kUndirected | (p ? kPersistent : 0);
-        float t = time_one(true, var);
-        if (t < t2) { t2 = t; b2 = var; }
+      for (int v = 0; v < n2 && e == cudaSuccess; ++v) {
+        const int var = v | (p ? kPersistent : 0) | form;
+        float t = time_one(true, var, 0);
+        if (t < t2) { t2 = t; f2 = var; }
       }
+    if (t1 + t2 < best_total) {
+      best_total = t1 + t2;
+      b1 = f1;
+      b2 = f2;
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (e == cudaSuccess) {

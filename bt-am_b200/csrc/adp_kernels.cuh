@@ -18,7 +18,7 @@ template <class R> struct EvalArgs {
   const double *gamma;  // chemical multiplier       [real]
   const int *offs;      // CSR offsets               [real + 1]
   const int *idx;       // neighbour indices (all-sites numbering)
-  TablesView<R> T;      // radial tables in R
+  RadialView<R> T;      // radial tables in R (per-segment records)
   SplineView<double> emb[2];  // embedding F (FP64) for Mg, H
   double mass[2];             // Mg, H element masses
   R *mom;                     // kMomStride per real site
@@ -31,19 +31,27 @@ template <class R> struct EvalArgs {
   const int *own_u = nullptr;  // their sites
   int n_own = 0;
   R *pbuf = nullptr;           // 8 R per slot: gq[3], gs, gx, 0, 0, 0
+  // pair-rule records of the owned pairs (kPrRec R each, pair_rule_record)
+  // and each slot's owned pair and direction (2 t + 0 owned slot, + 1 its
+  // reverse)
+  R *prec = nullptr;
+  const int *slot_own = nullptr;
 };
 
 // Pass 1: rho-bar, V0, S0, dV0/dx (self) and the moment record of every
 // real site.  Pass 2: residuals of every real site.  `variant` picks the
-// block shape / register cap (0 = default; see kPass1Variants below).
+// block shape / register cap (0 = default; see kPass1Variants below); pass 1
+// also takes the pass-2 variant, because an undirected pass 2 needs the
+// pair-rule records that pass 1 then makes.
 template <class R>
-cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
+cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0,
+                         int pass2_variant = 0);
 template <class R>
 cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
 // variant = shape | kPersistent (persistent grid of resident blocks)
 //           [| kUndirected: pass 1 takes its pair-rule sums, pass 2 its
 //            whole per-pair work, from one evaluation per undirected pair]
-constexpr int kPass1Variants = 5;  // shapes (4 warps,-), (4,3), (4,4), (8,2), (2,8)
+constexpr int kPass1Variants = 5;  // shapes (4 warps,-), (4,3), (4,4), (8,2), (4,5)
 constexpr int kPass2Variants = 6;  // shapes (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
 constexpr int kPass2UVariants = 4;  // undirected pair kernel (threads, min blocks): (128,-), (128,3), (128,4), (256,2)
 constexpr int kPersistent = 8;
@@ -60,9 +68,11 @@ inline bool valid_variants(int v1, int v2) {
 // Undirected pass 2 in two launches: the pair kernel (one thread per owned
 // slot: both directions of the pair into the slot buffer) and the site
 // kernel (one warp per site: the sum over its slots and the epilogue).
-// Needs a.rev, a.own_p, a.own_u and a.pbuf; launch_pass2 falls back to the
-// directed default when they are absent.
-inline bool has_undirected(const void *rev, const void *pbuf) { return rev && pbuf; }
+// Needs a.rev, a.own_p, a.own_u, a.pbuf, a.prec and a.slot_own; the launchers
+// fall back to the directed default when they are absent.
+template <class R> inline bool has_undirected(const EvalArgs<R> &a) {
+  return a.rev && a.pbuf && a.prec && a.slot_own;
+}
 
 // Times every pass-1 and pass-2 variant on this input (reps launches each,
 // synchronising st) and returns the fastest of each.  Every variant computes

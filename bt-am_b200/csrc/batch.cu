@@ -57,6 +57,12 @@ __global__ void shift_rev_kernel(long long n, const int *src, int *dst, int base
   if (i < n) dst[i] = src[i] < 0 ? -1 : base + src[i];
 }
 
+// Slot-to-owned-pair links (2 t + direction) move by twice the owned-pair base.
+__global__ void shift_slot_own_kernel(long long n, const int *src, int *dst, int own_base) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = src[i] < 0 ? -1 : 2 * own_base + src[i];
+}
+
 inline int blocks_of(long long n, int per) { return (int)((n + per - 1) / per); }
 
 }  // namespace
@@ -78,7 +84,7 @@ struct btam_batch {
   double *gamma = nullptr;
   int *offs = nullptr, *idx = nullptr;
   // undirected pass 2: reverse slots, owned slots and their sites, slot buffer
-  int *rev = nullptr, *own_p = nullptr, *own_u = nullptr;
+  int *rev = nullptr, *slot_own = nullptr, *own_p = nullptr, *own_u = nullptr;
   int n_own = 0;
   char *pbuf = nullptr;
   size_t pbuf_bytes = 0, pbuf_elem = 0;
@@ -98,7 +104,7 @@ struct btam_batch {
 
 namespace {
 
-template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const TablesView<R> &T) {
+template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const RadialView<R> &T) {
   EvalArgs<R> a;
   a.n_real = b->n_real;
   a.pos = b->pos;
@@ -127,12 +133,16 @@ template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const TablesVie
   a.own_u = b->own_u;
   a.n_own = b->n_own;
   a.pbuf = reinterpret_cast<R *>(b->pbuf);
+  a.slot_own = b->slot_own;
+  a.prec = b->pbuf ? a.pbuf + 8 * (size_t)b->n_pairs : nullptr;
   return a;
 }
 
+// Slot records (8 R per slot) then pair-rule records (kPrRec R per owned pair).
 int batch_pbuf(btam_batch *b, size_t elem) {
   if (elem < b->pbuf_elem) elem = b->pbuf_elem;
-  const size_t need = (size_t)(b->n_pairs > 0 ? b->n_pairs : 1) * 8 * elem;
+  const size_t need =
+      ((size_t)(b->n_pairs > 0 ? b->n_pairs : 1) * 8 + (size_t)b->n_own * kPrRec) * elem;
   b->pbuf_elem = elem;
   if (need <= b->pbuf_bytes) return BTAM_OK;
   BTAM_TRY(dalloc(b->pbuf, b->st, need));
@@ -192,6 +202,7 @@ void free_batch(btam_batch *b) {
   dfree(b->mom32, b->st);
   dfree(b->err, b->st);
   dfree(b->rev, b->st);
+  dfree(b->slot_own, b->st);
   dfree(b->own_p, b->st);
   dfree(b->own_u, b->st);
   dfree(b->pbuf, b->st);
@@ -253,6 +264,7 @@ int batch_build(btam_batch *b) {
   BTAM_TRY(dalloc(b->totals, b->st, 4 * (size_t)ns));
   BTAM_TRY(dalloc(b->err, b->st, 1));
   BTAM_TRY(dalloc(b->rev, b->st, (size_t)n_pairs));
+  BTAM_TRY(dalloc(b->slot_own, b->st, (size_t)n_pairs));
   BTAM_TRY(dalloc(b->own_p, b->st, (size_t)own_total));
   BTAM_TRY(dalloc(b->own_u, b->st, (size_t)own_total));
   b->n_own = (int)own_total;
@@ -281,6 +293,8 @@ int batch_build(btam_batch *b) {
           n_list_pairs[k], s->idx, b->idx + b->base_pair[k], n, R, G);
       shift_rev_kernel<<<blocks_of(n_list_pairs[k], 256), 256, 0, b->st>>>(
           n_list_pairs[k], s->rev, b->rev + b->base_pair[k], (int)b->base_pair[k]);
+      shift_slot_own_kernel<<<blocks_of(n_list_pairs[k], 256), 256, 0, b->st>>>(
+          n_list_pairs[k], s->slot_own, b->slot_own + b->base_pair[k], (int)own_base);
     }
     if (s->n_own > 0) {
       shift_offs_kernel<<<blocks_of(s->n_own, 256), 256, 0, b->st>>>(
@@ -298,9 +312,9 @@ int batch_build(btam_batch *b) {
 }
 
 // Enqueues one evaluation of every system: pass 1, pass 2, per-system totals.
-template <class R> cudaError_t enqueue_eval(btam_batch *b, int form, R *mom, const TablesView<R> &T) {
+template <class R> cudaError_t enqueue_eval(btam_batch *b, int form, R *mom, const RadialView<R> &T) {
   EvalArgs<R> a = batch_args<R>(b, mom, T);
-  cudaError_t e = launch_pass1(a, b->st, b->variant1[form]);
+  cudaError_t e = launch_pass1(a, b->st, b->variant1[form], b->variant2[form]);
   if (e == cudaSuccess) e = launch_pass2(a, b->st, b->variant2[form]);
   if (e == cudaSuccess)
     e = launch_seg_totals(b->n_sys, b->seg, b->V0, b->S0, b->Rq, b->Rs, b->Rx, b->totals, b->st);
@@ -327,8 +341,8 @@ int ensure_graph(btam_batch *b, int precision) {
   }
   cudaGraph_t g = nullptr;
   BTAM_TRY(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeRelaxed));
-  cudaError_t e = f == 0 ? enqueue_eval<double>(b, 0, b->mom64, b->T->v64)
-                         : enqueue_eval<float>(b, 1, b->mom32, b->T->v32);
+  cudaError_t e = f == 0 ? enqueue_eval<double>(b, 0, b->mom64, b->T->r64)
+                         : enqueue_eval<float>(b, 1, b->mom32, b->T->r32);
   cudaError_t e2 = cudaStreamEndCapture(b->st, &g);
   if (e == cudaSuccess) e = e2;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec[f], g, 0);
@@ -410,9 +424,9 @@ int btam_batch_autotune(btam_batch *b, int precision, int *pass1_variant, int *p
   st = batch_pbuf(b, f == 0 ? sizeof(double) : sizeof(float));
   if (st != BTAM_OK) return st;
   int v1 = 0, v2 = 0;
-  cudaError_t e = f == 0 ? autotune_passes(batch_args<double>(b, b->mom64, b->T->v64), b->st, 3,
+  cudaError_t e = f == 0 ? autotune_passes(batch_args<double>(b, b->mom64, b->T->r64), b->st, 3,
                                            &v1, &v2)
-                         : autotune_passes(batch_args<float>(b, b->mom32, b->T->v32), b->st, 3,
+                         : autotune_passes(batch_args<float>(b, b->mom32, b->T->r32), b->st, 3,
                                            &v1, &v2);
   if (e != cudaSuccess) return cuda_status(e);
   b->variant1[f] = v1;

@@ -181,7 +181,7 @@ int ensure_sites(btam_system *s, int n_all) {
   return BTAM_OK;
 }
 
-template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesView<R> &T) {
+template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const RadialView<R> &T) {
   EvalArgs<R> a;
   a.n_real = s->n_real;
   a.pos = s->pos;
@@ -210,14 +210,18 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const TablesVie
   a.own_u = s->own_u;
   a.n_own = s->n_own;
   a.pbuf = reinterpret_cast<R *>(s->pbuf);
+  a.slot_own = s->slot_own;
+  a.prec = s->pbuf ? a.pbuf + 8 * (size_t)s->n_pairs : nullptr;
   return a;
 }
 
-// Slot buffer of the undirected pass 2: 8 values of R per slot of the real
-// sites' lists, allocated only when an undirected variant is in use.
+// Buffer of the undirected kernels, allocated only when an undirected variant
+// is in use: 8 values of R per slot of the real sites' lists (pass-2 slot
+// records), then kPrRec per owned pair (pair-rule records).
 int ensure_pbuf(btam_system *s, size_t elem) {
   if (elem < s->pbuf_elem) elem = s->pbuf_elem;
-  const size_t need = (size_t)(s->n_pairs > 0 ? s->n_pairs : 1) * 8 * elem;
+  const size_t need =
+      ((size_t)(s->n_pairs > 0 ? s->n_pairs : 1) * 8 + (size_t)s->n_own * kPrRec) * elem;
   s->pbuf_elem = elem;
   if (need <= s->pbuf_bytes) return BTAM_OK;
   BTAM_TRY(dalloc(s->pbuf, s->st, need));
@@ -256,6 +260,8 @@ cudaMemPool_t device_pool() {
 
 const TablesView<double> &tables_view64(const btam_tables *t) { return t->v64; }
 const TablesView<float> &tables_view32(const btam_tables *t) { return t->v32; }
+const RadialView<double> &radial_view64(const btam_tables *t) { return t->r64; }
+const RadialView<float> &radial_view32(const btam_tables *t) { return t->r32; }
 double tables_mass(const btam_tables *t, int code) {
   return code == 1 ? t->host.mass_h : t->host.mass_mg;
 }
@@ -327,6 +333,37 @@ int btam_tables_load(const char *dir, btam_tables **out) {
     t->v64.t[k] = SplineView<double>{t->d64 + off[k], hs.dx, 1.0 / hs.dx, hs.n};
     t->v32.t[k] = SplineView<float>{t->d32 + off[k], (float)hs.dx, (float)(1.0 / hs.dx), hs.n};
   }
+  // the kernels' per-segment records (every radial table on one knot grid)
+  std::vector<double> r64;
+  std::vector<float> r32;
+  size_t uw64[3], pr64[3], uw32[3], pr32[3];
+  double rdx = 0.0;
+  int rn = 0;
+  if (!pack_radial(t->host, r64, uw64, pr64, rdx, rn) ||
+      !pack_radial(t->host, r32, uw32, pr32, rdx, rn)) {
+    btam_tables_destroy(t);
+    return BTAM_ERR_IO;
+  }
+  e = cudaMalloc(&t->rad64, r64.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&t->rad32, r32.size() * sizeof(float));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->rad64, r64.data(), r64.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t->rad32, r32.data(), r32.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    btam_tables_destroy(t);
+    return cuda_status(e);
+  }
+  t->r64.uw = t->rad64 + uw64[0];
+  t->r64.pr = t->rad64 + pr64[0];
+  t->r32.uw = t->rad32 + uw32[0];
+  t->r32.pr = t->rad32 + pr32[0];
+  t->r64.dx = rdx;
+  t->r64.inv_dx = 1.0 / rdx;
+  t->r64.n = rn;
+  t->r32.dx = (float)rdx;
+  t->r32.inv_dx = (float)(1.0 / rdx);
+  t->r32.n = rn;
   *out = t;
   return BTAM_OK;
 }
@@ -335,6 +372,8 @@ void btam_tables_destroy(btam_tables *t) {
   if (!t) return;
   if (t->d64) cudaFree(t->d64);
   if (t->d32) cudaFree(t->d32);
+  if (t->rad64) cudaFree(t->rad64);
+  if (t->rad32) cudaFree(t->rad32);
   delete t;
 }
 
@@ -449,7 +488,7 @@ void btam_system_destroy(btam_system *s) {
   dfree(s->mom64, s->st); dfree(s->mom32, s->st); dfree(s->err, s->st);
   dfree(s->doffs, s->st); dfree(s->didx, s->st); dfree(s->X, s->st); dfree(s->X0, s->st); dfree(s->dtot, s->st); dfree(s->mu, s->st);
   dfree(s->dact, s->st); dfree(s->ddeg, s->st); dfree(s->rv, s->st);
-  dfree(s->rev, s->st); dfree(s->own_off, s->st); dfree(s->own_p, s->st); dfree(s->own_u, s->st);
+  dfree(s->rev, s->st); dfree(s->slot_own, s->st); dfree(s->own_off, s->st); dfree(s->own_p, s->st); dfree(s->own_u, s->st);
   dfree(s->pbuf, s->st);
   s->scratch.release(s->st);
   if (s->st) cudaStreamSynchronize(s->st);
@@ -549,14 +588,16 @@ int btam_neighbors_build(btam_system *s, int all_sites) {
   // reverse slots and owned pairs for the undirected pass 2
   if (total > s->rev_cap) {
     BTAM_TRY(dalloc(s->rev, s->st, total));
+    BTAM_TRY(dalloc(s->slot_own, s->st, total));
     s->rev_cap = total;
   }
   if (n + 1 > s->own_off_cap) {
     BTAM_TRY(dalloc(s->own_off, s->st, n + 1));
     s->own_off_cap = n + 1;
   }
-  BTAM_TRY(launch_pair_links(n, s->offs, s->idx, s->owner, s->rev, s->cnt, s->own_off, s->own_p,
-                             s->own_u, s->own_cap, &s->n_own, s->scratch, s->st));
+  BTAM_TRY(launch_pair_links(n, s->offs, s->idx, s->owner, s->rev, s->slot_own, s->cnt,
+                             s->own_off, s->own_p, s->own_u, s->own_cap, &s->n_own, s->scratch,
+                             s->st));
   if (s->pbuf_elem > 0) {  // a rebuilt list may be longer than the slot buffer
     int st2 = ensure_pbuf(s, s->pbuf_elem);
     if (st2 != BTAM_OK) return st2;
@@ -666,13 +707,13 @@ int btam_mf_eval_async(btam_system *s, int precision) {
   const size_t nm = (size_t)s->n_real * kMomStride;
   if (precision == BTAM_FP64) {
     if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
-    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
-    BTAM_TRY(launch_pass1(a, s->st, s->variant1[0]));
+    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
+    BTAM_TRY(launch_pass1(a, s->st, s->variant1[0], s->variant2[0]));
     BTAM_TRY(launch_pass2(a, s->st, s->variant2[0]));
   } else {
     if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
-    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
-    BTAM_TRY(launch_pass1(a, s->st, s->variant1[1]));
+    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
+    BTAM_TRY(launch_pass1(a, s->st, s->variant1[1], s->variant2[1]));
     BTAM_TRY(launch_pass2(a, s->st, s->variant2[1]));
   }
   BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->st));
@@ -703,11 +744,11 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
   if (precision == BTAM_FP64) {
     if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
     if ((st = ensure_pbuf(s, sizeof(double))) != BTAM_OK) return st;
-    st = autotune_form(s, eval_args<double>(s, s->mom64, s->T->v64), 0, 3);
+    st = autotune_form(s, eval_args<double>(s, s->mom64, s->T->r64), 0, 3);
   } else if (precision == BTAM_FP32C) {
     if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
     if ((st = ensure_pbuf(s, sizeof(float))) != BTAM_OK) return st;
-    st = autotune_form(s, eval_args<float>(s, s->mom32, s->T->v32), 1, 3);
+    st = autotune_form(s, eval_args<float>(s, s->mom32, s->T->r32), 1, 3);
   } else {
     return BTAM_ERR_ARG;
   }
@@ -773,10 +814,10 @@ int btam_mf_rho(btam_system *s, int precision, double *rho) {
   const size_t nm = (size_t)s->n_real * kMomStride;
   if (precision == BTAM_FP64) {
     if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
-    BTAM_TRY(launch_pass1(eval_args<double>(s, s->mom64, s->T->v64), s->st));
+    BTAM_TRY(launch_pass1(eval_args<double>(s, s->mom64, s->T->r64), s->st));
   } else if (precision == BTAM_FP32C) {
     if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
-    BTAM_TRY(launch_pass1(eval_args<float>(s, s->mom32, s->T->v32), s->st));
+    BTAM_TRY(launch_pass1(eval_args<float>(s, s->mom32, s->T->r32), s->st));
   } else {
     return BTAM_ERR_ARG;
   }
@@ -794,14 +835,14 @@ int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]) {
   cudaError_t e = cudaEventRecord(ev[0], s->st);
   if (precision == BTAM_FP64) {
     if (!s->mom64 && e == cudaSuccess) e = dalloc(s->mom64, s->st, nm);
-    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->v64);
-    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[0]);
+    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[0], s->variant2[0]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
     if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[0]);
   } else {
     if (!s->mom32 && e == cudaSuccess) e = dalloc(s->mom32, s->st, nm);
-    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->v32);
-    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[1]);
+    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[1], s->variant2[1]);
     if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
     if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[1]);
   }

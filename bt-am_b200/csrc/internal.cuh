@@ -18,6 +18,11 @@ struct btam_tables {
   Coef4<float> *d32 = nullptr;
   TablesView<double> v64;
   TablesView<float> v32;
+  // the radial tables as the kernels' per-segment records
+  double *rad64 = nullptr;
+  float *rad32 = nullptr;
+  RadialView<double> r64;
+  RadialView<float> r32;
 };
 
 struct btam_system {
@@ -70,7 +75,8 @@ struct btam_system {
   int relax_m = 0;
   double *rv = nullptr;  // one block holding every relaxation vector
   // pair links and slot buffer of the undirected pass 2
-  int *rev = nullptr, *own_off = nullptr, *own_p = nullptr, *own_u = nullptr;
+  int *rev = nullptr, *slot_own = nullptr, *own_off = nullptr, *own_p = nullptr,
+      *own_u = nullptr;
   long long rev_cap = 0, own_cap = 0;
   int own_off_cap = 0, n_own = 0;
   char *pbuf = nullptr;

@@ -14,7 +14,7 @@
 //  * at most kNoAllocMaxSites real sites per call (larger requests return
 //    BTAM_ERR_TOO_LARGE before touching the device);
 //  * the array is created when the library is loaded on a device and stays
-//    allocated until the process exits (about 10.4 MB per device);
+//    allocated until the process exits (about 10.9 MB per device);
 //  * every call on a device uses the same array and leaves its contents
 //    behind: calls whose work overlaps on the GPU (different streams or
 //    host threads at the same time) race on it and give wrong results;
@@ -76,7 +76,8 @@ int noalloc_status(cudaError_t e) {
 // Defined in btam_capi.cu: the device table views of a loaded btam_tables.
 namespace btam {
 const TablesView<double> &tables_view64(const btam_tables *t);
-const TablesView<float> &tables_view32(const btam_tables *t);
+const RadialView<double> &radial_view64(const btam_tables *t);
+const RadialView<float> &radial_view32(const btam_tables *t);
 double tables_mass(const btam_tables *t, int code);
 }  // namespace btam
 
@@ -130,14 +131,14 @@ extern "C" int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_r
   if (precision == BTAM_FP64) {
     EvalArgs<double> a;
     fill(a);
-    a.T = tables_view64(t);
+    a.T = radial_view64(t);
     a.mom = mom;
     e = launch_pass1(a, st);
     if (e == cudaSuccess) e = launch_pass2(a, st);
   } else {
     EvalArgs<float> a;
     fill(a);
-    a.T = tables_view32(t);
+    a.T = radial_view32(t);
     a.mom = (float *)mom;
     e = launch_pass1(a, st);
     if (e == cudaSuccess) e = launch_pass2(a, st);

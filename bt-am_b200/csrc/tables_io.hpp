@@ -71,4 +71,48 @@ inline int load_host_tables(const std::string &dir, HostTables &T) {
   return 0;
 }
 
+// Packs the radial tables into the kernels' per-segment records (layout at
+// RadialView in adp_core.cuh): the uw block of pair kind pk at off_uw[pk] =
+// off_uw[0] + 8 n pk, the pr block at off_pr[pk] = off_pr[0] + 8 n pk, all
+// offsets multiples of 8 values.  Table ids: 0 rho_Mg, 1 rho_H,
+// 4 + pk phi, 7 + pk u, 10 + pk w.  Returns false when the radial tables do
+// not share one knot grid (then the records cannot serve them).
+template <class R>
+bool pack_radial(const HostTables &T, std::vector<R> &buf, size_t off_uw[3], size_t off_pr[3],
+                 double &dx, int &n) {
+  const int ids[11] = {0, 1, 4, 5, 6, 7, 8, 9, 10, 11, 12};
+  n = T.t[0].n;
+  dx = T.t[0].dx;
+  for (int id : ids)
+    if (T.t[id].n != n || T.t[id].dx != dx) return false;
+  const size_t N = (size_t)n;
+  size_t at = 0;
+  for (int pk = 0; pk < 3; ++pk) {
+    off_uw[pk] = at;
+    at += 8 * N;
+  }
+  for (int pk = 0; pk < 3; ++pk) {
+    off_pr[pk] = at;
+    at += (pk == 2 ? 16 : 8) * N;
+  }
+  buf.assign(at, (R)0);
+  auto put = [&](size_t dst, int id, size_t m) {
+    for (int c = 0; c < 4; ++c) buf[dst + c] = (R)T.t[id].abcd[4 * m + c];
+  };
+  for (size_t m = 0; m < N; ++m)
+    for (int pk = 0; pk < 3; ++pk) {
+      put(off_uw[pk] + 8 * m, 7 + pk, m);
+      put(off_uw[pk] + 8 * m + 4, 10 + pk, m);
+      const size_t st = pk == 2 ? 16 : 8;
+      put(off_pr[pk] + st * m, 4 + pk, m);
+      if (pk == 2) {
+        put(off_pr[pk] + st * m + 4, 0, m);
+        put(off_pr[pk] + st * m + 8, 1, m);
+      } else {
+        put(off_pr[pk] + st * m + 4, pk, m);  // rho of the kind's species
+      }
+    }
+  return true;
+}
+
 }  // namespace btam

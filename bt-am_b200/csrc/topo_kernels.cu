@@ -400,8 +400,11 @@ __global__ void pair_rev_kernel(int n_real, const int *offs, const int *idx, con
   if (lane == 0) own_cnt[u] = cnt;
 }
 
+// Owned pairs in site order, and every slot's owned pair and direction:
+// slot_own = 2 t for the owned slot of pair t, 2 t + 1 for its reverse slot.
 __global__ void pair_own_kernel(int n_real, const int *offs, const int *idx, const int *owner,
-                                const int *rev, const int *own_off, int *own_p, int *own_u) {
+                                const int *rev, const int *own_off, int *own_p, int *own_u,
+                                int *slot_own) {
   const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (u >= n_real) return;
   int at = own_off[u];
@@ -414,15 +417,17 @@ __global__ void pair_own_kernel(int n_real, const int *offs, const int *idx, con
       int k = at + __popc(m & ((1u << lane) - 1u));
       own_p[k] = p;
       own_u[k] = u;
+      slot_own[p] = 2 * k;
+      if (rev[p] >= 0) slot_own[rev[p]] = 2 * k + 1;
     }
     at += __popc(m);
   }
 }
 
 cudaError_t launch_pair_links(int n_real, const int *offs, const int *idx, const int *owner,
-                              int *rev, int *own_cnt, int *own_off, int *&own_p, int *&own_u,
-                              long long &own_cap, int *n_own, DeviceScratch &scratch,
-                              cudaStream_t st) {
+                              int *rev, int *slot_own, int *own_cnt, int *own_off, int *&own_p,
+                              int *&own_u, long long &own_cap, int *n_own,
+                              DeviceScratch &scratch, cudaStream_t st) {
   cudaError_t e;
   *n_own = 0;
   if (n_real <= 0) return cudaSuccess;
@@ -450,7 +455,16 @@ cudaError_t launch_pair_links(int n_real, const int *offs, const int *idx, const
       return e;
     own_cap = total;
   }
-  pair_own_kernel<<<blocks, 128, 0, st>>>(n_real, offs, idx, owner, rev, own_off, own_p, own_u);
+  int n_slots = 0;
+  if ((e = cudaMemcpyAsync(&n_slots, offs + n_real, sizeof(int), cudaMemcpyDeviceToHost, st)) !=
+      cudaSuccess)
+    return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  if (n_slots > 0 &&
+      (e = cudaMemsetAsync(slot_own, 0xff, (size_t)n_slots * sizeof(int), st)) != cudaSuccess)
+    return e;
+  pair_own_kernel<<<blocks, 128, 0, st>>>(n_real, offs, idx, owner, rev, own_off, own_p, own_u,
+                                          slot_own);
   *n_own = total;
   return cudaGetLastError();
 }

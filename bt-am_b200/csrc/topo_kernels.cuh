@@ -101,9 +101,9 @@ cudaError_t launch_neighbors(const NbrArgs &a, cudaStream_t st);
 // own_cnt / own_off: n_real + 1 ints of scratch; *n_own returned after a
 // stream synchronisation.
 cudaError_t launch_pair_links(int n_real, const int *offs, const int *idx, const int *owner,
-                              int *rev, int *own_cnt, int *own_off, int *&own_p, int *&own_u,
-                              long long &own_cap, int *n_own, DeviceScratch &scratch,
-                              cudaStream_t st);
+                              int *rev, int *slot_own, int *own_cnt, int *own_off, int *&own_p,
+                              int *&own_u, long long &own_cap, int *n_own,
+                              DeviceScratch &scratch, cudaStream_t st);
 
 cudaError_t launch_compact(int n_query, const int *tmp, const int *offs, int *idx,
                            cudaStream_t st);
