@@ -40,6 +40,25 @@ WORKLOAD = ("plain drop-in: periodic hcp Mg 20x15x15 hexagonal cells, 9000 Mg + 
             "T=400 K, seed 2")
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 FLOP_PASS1, FLOP_PASS2 = 1000.0, 2000.0  # algorithmic flops per directed active pair
+# spline lookups per directed pair: 48 at the 12 pair-rule points (rho, phi,
+# u, w), 26 at the 13 triplet points (u, w); the algorithmic flops of each
+# pass are attributed to kernels by these lookups
+LOOK_PR, LOOK_TRIP = 48.0, 26.0
+
+
+def kernel_flops(undirected):
+    """Algorithmic flops per directed active pair of the five kernels of one
+    evaluation (pass-1 pair-rule, pass-1 site, pass-2 pair, pass-2 site,
+    totals).  Undirected variants: the pair-rule kernel evaluates the pair
+    rule of both passes (value and derivative) once per pair for both
+    directions, the pass-1 site kernel the triplet points of pass 1, the
+    pass-2 pair kernel the triplet points of pass 2; directed variants have
+    no pair kernels."""
+    tot = LOOK_PR + LOOK_TRIP
+    if undirected:
+        return [(FLOP_PASS1 + FLOP_PASS2) * LOOK_PR / tot, FLOP_PASS1 * LOOK_TRIP / tot,
+                FLOP_PASS2 * LOOK_TRIP / tot, 0.0, 0.0]
+    return [0.0, FLOP_PASS1, 0.0, FLOP_PASS2, 0.0]
 
 
 def dist_env():
@@ -95,6 +114,15 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
                 "samples": len(self.samples)}
+
+
+def launches_per_eval(shape):
+    """Kernel launches of one evaluation with launch variants (v1, v2): pass 1
+    (plus the pair-rule kernel when either pass is undirected), pass 2 (pair
+    and site kernels when undirected), two totals launches."""
+    v1, v2 = shape
+    und = bool((v1 | v2) & 16)
+    return (2 if und else 1) + (2 if v2 & 16 else 1) + 2
 
 
 def active_pairs(sys_, offs, idx, owner):
@@ -394,24 +422,30 @@ def run_btam(args, ws, rank, local):
         step_ms = max_over_ranks(float(np.mean(ms)))
         results[name] = dict(ms=step_ms, value=ws * 1e3 / step_ms)
     # per-kernel times for the roofline (FP32C form)
-    prof = np.array([S.profile(btam.FP32C) for _ in range(5)])
-    prof64 = np.array([S.profile(btam.FP64) for _ in range(5)])
-    p1, p2, _ = np.median(prof, axis=0)
-    p1d, p2d, _ = np.median(prof64, axis=0)
+    prof = np.median(np.array([S.profile(btam.FP32C) for _ in range(7)]), axis=0)
+    prof64 = np.median(np.array([S.profile(btam.FP64) for _ in range(7)]), axis=0)
     fp32_peak = btam.probe_fma_peak(False, 0.5)
     fp64_peak = btam.probe_fma_peak(True, 0.5)
-    dom = "pass2" if p2 >= p1 else "pass1"
-    dom_ms = max(p1, p2)
-    dom_flops = (FLOP_PASS2 if dom == "pass2" else FLOP_PASS1) * P
-    achieved = dom_flops / (dom_ms * 1e-3) / 1e12
-    roofline = {"bound": "fp32", "kernel": f"{dom} (FP32C)", "achieved": achieved,
+    und = bool(shapes["fp32c"][1] & 16)
+    flops = kernel_flops(und)
+    names = ["pass1 pair-rule kernel", "pass1 site kernel", "pass2 pair kernel",
+             "pass2 site kernel", "totals"]
+    dom = int(np.argmax(prof))
+    achieved = flops[dom] * P / (prof[dom] * 1e-3) / 1e12
+    eval_rate = (FLOP_PASS1 + FLOP_PASS2) * P / (results["fp32c"]["ms"] * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": names[dom] + " (FP32C)", "achieved": achieved,
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                 "traffic": None,
                 "peak_source": "measured live: btam_probe_fma_peak FP32 FMA loop on all SMs",
-                "flops_per_launch": dom_flops,
-                "pass1_ms": p1, "pass2_ms": p2,
-                "fp64_form": {"pass1_ms": p1d, "pass2_ms": p2d, "fp64_peak": fp64_peak,
-                              "frac_pass2": FLOP_PASS2 * P / (p2d * 1e-3) / 1e12 / fp64_peak}}
+                "flops_per_launch": flops[dom] * P,
+                "kernel_ms": dict(zip(names, map(float, prof))),
+                "kernel_flops_per_directed_pair": dict(zip(names, flops)),
+                "evaluation": {"flops": (FLOP_PASS1 + FLOP_PASS2) * P, "achieved": eval_rate,
+                               "frac": eval_rate / fp32_peak},
+                "fp64_form": {"kernel_ms": dict(zip(names, map(float, prof64))),
+                              "fp64_peak": fp64_peak,
+                              "evaluation_frac": (FLOP_PASS1 + FLOP_PASS2) * P /
+                              (results["fp64"]["ms"] * 1e-3) / 1e12 / fp64_peak}}
     # e2e through the C ABI with pinned host buffers
     qh = torch.from_numpy(sys_["q"]).pin_memory().numpy()
     sh = torch.from_numpy(sys_["sigma"]).pin_memory().numpy()
@@ -464,7 +498,7 @@ def run_btam(args, ws, rank, local):
                 "e2e": {"value": ws * 1e3 / e2e_ms, "unit": "evals/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
-                "gpu_launches": 3 * args.steps,
+                "gpu_launches": launches_per_eval(shapes["fp32c"]) * args.steps,
                 "clocks": clocks, "batched": batched, "serving": serving}
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -475,7 +509,7 @@ def run_btam(args, ws, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="btam", choices=["btam", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")

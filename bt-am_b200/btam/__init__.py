@@ -364,9 +364,10 @@ class System:
                "btam_set_variants")
 
     def profile(self, precision=FP64):
-        """Per-kernel device times (ms) of one evaluation: pass 1, pass 2,
-        totals."""
-        ms = np.zeros(3)
+        """Per-kernel device times (ms) of one evaluation: pass-1 pair-rule
+        kernel, pass-1 site kernel, pass-2 pair kernel, pass-2 site kernel,
+        totals (the pair kernels read ~0 for the directed variants)."""
+        ms = np.zeros(5)
         _check(lib().btam_mf_eval_profile(self.handle, precision, _d(ms)),
                "btam_mf_eval_profile")
         return ms

@@ -500,13 +500,15 @@ template <class R> BTAM_HD R bpair_r(const Feat<R> &x, const Feat<R> &y) {
 // / s at each point r (s = |r|), the radial coefficients of pass 2 are
 //   c_self = w6 (x_u F'(rho_u) x_j A + C),   c_cros = w6 (x_j F'(rho_j) x_u B + C),
 // so the record keeps sum A r, sum B r, sum C r and their sigma-direction
-// sums over each side.  Layout (kPrRec R, 32-byte aligned):
+// sums over each side.  Layout (kPrRec R), stored as two arrays: the four
+// pass-1 sums (kPr1 R per pair, compact so that pass 1's scattered reads
+// stay in L2) and the pass-2 pieces (kPr2 R per pair, 32-byte aligned):
 //   [0] sum rho_{s_u}, [1] sum rho_{s_j}, [2] sum phi, [3] sum B(f, f),
 //   [4..6] sum A r, [7..9] sum B r, [10..12] sum C r,
 //   [13..15] sum (A, B, C) sd over the u-moved points (sd = -+sqrt6 r_k),
 //   [16..18] sum (A, B, C) sd over the j-moved points (sd = +-sqrt6 r_k),
-//   [19..23] 0.
-constexpr int kPrRec = 24;
+//   [19] 0.
+constexpr int kPr1 = 4, kPr2 = 16, kPrRec = kPr1 + kPr2;
 template <class R>
 BTAM_HD void pair_rule_record(const RadialView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
                               R xj, int cu, int cj, R (&rec)[kPrRec]) {

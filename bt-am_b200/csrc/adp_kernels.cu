@@ -79,6 +79,16 @@ __device__ __forceinline__ void st_rec(double *p, const double (&v)[8]) {
                "d"(v[6]), "d"(v[7])
                : "memory");
 }
+// 16-byte (FP32) / 32-byte (FP64) store of the first four values of a record.
+template <class R> __device__ __forceinline__ void st_rec4(R *p, const R *v);
+template <> __device__ __forceinline__ void st_rec4<float>(float *p, const float *v) {
+  *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+}
+template <> __device__ __forceinline__ void st_rec4<double>(double *p, const double *v) {
+  asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
+               "d"(v[2]), "d"(v[3])
+               : "memory");
+}
 __device__ __forceinline__ void ld_rec(const float *p, float (&v)[8]) {
   asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
@@ -115,12 +125,13 @@ pass1u_pair_kernel(const EvalArgs<R> a) {
 #pragma unroll
       for (int c = 0; c < kPrRec; ++c) rec[c] = (R)0;
     }
-    R *dst = a.prec + (size_t)kPrRec * t;
+    st_rec4(a.prec1 + (size_t)kPr1 * t, rec);
+    R *dst = a.prec2 + (size_t)kPr2 * t;
 #pragma unroll
-    for (int h = 0; h < kPrRec / 8; ++h) {
+    for (int h = 0; h < kPr2 / 8; ++h) {
       R v[8];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) v[c] = rec[8 * h + c];
+      for (int c = 0; c < 8; ++c) v[c] = rec[kPr1 + 8 * h + c];
       st_rec(dst + 8 * h, v);
     }
   }
@@ -232,7 +243,7 @@ pass1_kernel(const EvalArgs<R> a) {
       if (UND) {
         const int so = a.slot_own[p];
         R rec[4];
-        ld4(a.prec + (size_t)kPrRec * (so >> 1), rec);
+        ld4(a.prec1 + (size_t)kPr1 * (so >> 1), rec);
         const R xj = (R)xbj.x, X = (R)xi * xj;
         acc[kP1Rho] += xj * rec[(so & 1) ? 0 : 1];
         acc[kP1Epair] += (R)0.5 * X * rec[2];
@@ -380,13 +391,19 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
       ou.gq[0] = ou.gq[1] = ou.gq[2] = ou.gs = ou.gx = (R)0;
       oj.gq[0] = oj.gq[1] = oj.gq[2] = oj.gs = oj.gx = (R)0;
       R pr[kPrRec];
-      const R *src = a.prec + (size_t)kPrRec * t;
+      {
+        R v4[4];
+        ld4(a.prec1 + (size_t)kPr1 * t, v4);
 #pragma unroll
-      for (int h = 0; h < kPrRec / 8; ++h) {
+        for (int c = 0; c < kPr1; ++c) pr[c] = v4[c];
+      }
+      const R *src = a.prec2 + (size_t)kPr2 * t;
+#pragma unroll
+      for (int h = 0; h < kPr2 / 8; ++h) {
         R v[8];
         ld8(src + 8 * h, v);
 #pragma unroll
-        for (int c = 0; c < 8; ++c) pr[8 * h + c] = v[c];
+        for (int c = 0; c < 8; ++c) pr[kPr1 + 8 * h + c] = v[c];
       }
       pass2_pair_sym<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
                         a.code[u], a.code[j], mu.scalar(0), mu.scalar(1), mj.scalar(0),
@@ -443,53 +460,46 @@ pass2u_site_kernel(const EvalArgs<R> a) {
   }
 }
 
-// Per-system deterministic totals of a batch: one block per system whose
-// real sites are [seg[k], seg[k+1]); the same strides and tree as
-// totals_kernel, so out[4k..4k+3] equals that system's own totals bitwise.
-__global__ void __launch_bounds__(1024)
-seg_totals_kernel(const int *seg, const double *V0, const double *S0, const double *Rq,
-                  const double *Rs, const double *Rx, double *out) {
-  __shared__ double sh[4][1024];
-  const int k = blockIdx.x, lo = seg[k], hi = seg[k + 1];
+// Deterministic FP64 totals in two stages.  Stage 1: block (b, k) sums the
+// sites [lo + len b / P, lo + len (b + 1) / P) of system k (lo = seg[k],
+// len = seg[k + 1] - lo; one system [0, n) when seg is null) with fixed
+// per-thread strides and a fixed tree into part[k][b]; stage 2: one warp per
+// system sums its P partials in a fixed shuffle tree.  The order depends only
+// on the system's own sites, so a system's totals in a batch equal its own
+// totals bitwise.
+__global__ void __launch_bounds__(kTotThreads)
+totals_part_kernel(const int *seg, int n, const double *V0, const double *S0, const double *Rq,
+                   const double *Rs, const double *Rx, double *part) {
+  __shared__ double sh[4][kTotThreads];
+  const int k = blockIdx.y, b = blockIdx.x, t = threadIdx.x;
+  const long long lo = seg ? seg[k] : 0, len = (seg ? seg[k + 1] : n) - lo;
+  const long long i0 = lo + len * b / kTotParts, i1 = lo + len * (b + 1) / kTotParts;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+  for (long long i = i0 + t; i < i1; i += kTotThreads) {
     v[0] += V0[i];
     v[1] += S0[i];
     v[2] += Rq[3 * i] * Rq[3 * i] + Rq[3 * i + 1] * Rq[3 * i + 1] +
             Rq[3 * i + 2] * Rq[3 * i + 2] + Rs[i] * Rs[i];
     v[3] += Rx[i] * Rx[i];
   }
-  for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] = v[c];
+  for (int c = 0; c < 4; ++c) sh[c][t] = v[c];
   __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if ((int)threadIdx.x < s)
-      for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
+  for (int h = kTotThreads / 2; h > 0; h >>= 1) {
+    if (t < h)
+      for (int c = 0; c < 4; ++c) sh[c][t] += sh[c][t + h];
     __syncthreads();
   }
-  if (threadIdx.x < 4) out[4 * k + threadIdx.x] = sh[threadIdx.x][0];
+  if (t < 4) part[((size_t)k * kTotParts + b) * 4 + t] = sh[t][0];
 }
 
-// Single-block deterministic reduction (fixed strides, fixed tree).
-__global__ void __launch_bounds__(1024)
-totals_kernel(int n, const double *V0, const double *S0, const double *Rq,
-              const double *Rs, const double *Rx, double *out) {
-  __shared__ double sh[4][1024];
-  double v[4] = {0.0, 0.0, 0.0, 0.0};
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    v[0] += V0[i];
-    v[1] += S0[i];
-    v[2] += Rq[3 * i] * Rq[3 * i] + Rq[3 * i + 1] * Rq[3 * i + 1] +
-            Rq[3 * i + 2] * Rq[3 * i + 2] + Rs[i] * Rs[i];
-    v[3] += Rx[i] * Rx[i];
+__global__ void __launch_bounds__(32) totals_final_kernel(const double *part, double *out) {
+  const int k = blockIdx.x, lane = threadIdx.x;
+  for (int c = 0; c < 4; ++c) {
+    double v = part[((size_t)k * kTotParts + lane) * 4 + c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) out[4 * k + c] = v;
   }
-  for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] = v[c];
-  __syncthreads();
-  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-    if ((int)threadIdx.x < s)
-      for (int c = 0; c < 4; ++c) sh[c][threadIdx.x] += sh[c][threadIdx.x + s];
-    __syncthreads();
-  }
-  if (threadIdx.x < 4) out[threadIdx.x] = sh[threadIdx.x][0];
 }
 
 __global__ void rho_nmf_kernel(int n, const double4 *pos, const double2 *xb, const int *code,
@@ -532,7 +542,7 @@ template <class K> int grid_of(K kernel, int n, int W, bool persistent) {
   return g < full ? g : full;
 }
 template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers,
-                                           bool und) {
+                                           bool und, cudaEvent_t mid) {
   if (und) {
     auto kp = pass1u_pair_kernel<R, 128>;
     int g = nblocks(a.n_own, 128);
@@ -545,9 +555,11 @@ template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st
       g = gp < g ? gp : g;
     }
     if (g > 0) kp<<<g, 128, 0, st>>>(a);
+    if (mid) cudaEventRecord(mid, st);
     auto k = pass1_kernel<R, W, MB, true>;
     k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
   } else {
+    if (mid) cudaEventRecord(mid, st);
     auto k = pass1_kernel<R, W, MB, false>;
     k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
   }
@@ -558,22 +570,23 @@ template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st
 }
 
 template <class R>
-cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2) {
+cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2, cudaEvent_t mid) {
   if (a.n_real <= 0) return cudaSuccess;
   const bool pers = (v & kPersistent) != 0;
   // the pair-rule records are made (and then also used by pass 1) whenever
   // either pass runs undirected: the undirected pass 2 reads them
   const bool und = ((v | v2) & kUndirected) != 0 && has_undirected(a);
   switch (v & (kPersistent - 1)) {
-  case 1: go1<R, 4, 3>(a, st, pers, und); break;
-  case 2: go1<R, 4, 4>(a, st, pers, und); break;
-  case 3: go1<R, 8, 2>(a, st, pers, und); break;
-  case 4: go1<R, 4, 5>(a, st, pers, und); break;
-  default: go1<R, 4, 1>(a, st, pers, und); break;
+  case 1: go1<R, 4, 3>(a, st, pers, und, mid); break;
+  case 2: go1<R, 4, 4>(a, st, pers, und, mid); break;
+  case 3: go1<R, 8, 2>(a, st, pers, und, mid); break;
+  case 4: go1<R, 4, 5>(a, st, pers, und, mid); break;
+  default: go1<R, 4, 1>(a, st, pers, und, mid); break;
   }
   return cudaGetLastError();
 }
-template <class R, int TPB, int MB> void go2u(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
+template <class R, int TPB, int MB>
+void go2u(const EvalArgs<R> &a, cudaStream_t st, bool pers, cudaEvent_t mid) {
   auto k = pass2u_pair_kernel<R, TPB, MB>;
   int g = nblocks(a.n_own, TPB);
   if (pers) {
@@ -585,24 +598,27 @@ template <class R, int TPB, int MB> void go2u(const EvalArgs<R> &a, cudaStream_t
     g = gp < g ? gp : g;
   }
   if (g > 0) k<<<g, TPB, 0, st>>>(a);
+  if (mid) cudaEventRecord(mid, st);
   auto ks = pass2u_site_kernel<R, 4>;
   ks<<<grid_of(ks, a.n_real, 4, pers), 128, 0, st>>>(a);
 }
 
-template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v) {
+template <class R>
+cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent_t mid) {
   if (a.n_real <= 0) return cudaSuccess;
   const bool pers = (v & kPersistent) != 0;
-  if (v & kUndirected) {
-    if (!has_undirected(a)) {
-      go2<R, 4, 1>(a, st, false);
-      return cudaGetLastError();
-    }
+  if ((v & kUndirected) && has_undirected(a)) {
     switch (v & (kPersistent - 1)) {
-    case 1: go2u<R, 128, 3>(a, st, pers); break;
-    case 2: go2u<R, 128, 4>(a, st, pers); break;
-    case 3: go2u<R, 256, 2>(a, st, pers); break;
-    default: go2u<R, 128, 1>(a, st, pers); break;
+    case 1: go2u<R, 128, 3>(a, st, pers, mid); break;
+    case 2: go2u<R, 128, 4>(a, st, pers, mid); break;
+    case 3: go2u<R, 256, 2>(a, st, pers, mid); break;
+    default: go2u<R, 128, 1>(a, st, pers, mid); break;
     }
+    return cudaGetLastError();
+  }
+  if (mid) cudaEventRecord(mid, st);
+  if (v & kUndirected) {  // links absent: the directed default
+    go2<R, 4, 1>(a, st, false);
     return cudaGetLastError();
   }
   switch (v & (kPersistent - 1)) {
@@ -615,10 +631,13 @@ template <class R> cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t s
   }
   return cudaGetLastError();
 }
-template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t, int, int);
-template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, int, int);
-template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t, int);
-template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t, int);
+template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t, int, int,
+                                          cudaEvent_t);
+template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, int, int,
+                                         cudaEvent_t);
+template cudaError_t launch_pass2<double>(const EvalArgs<double> &, cudaStream_t, int,
+                                          cudaEvent_t);
+template cudaError_t launch_pass2<float>(const EvalArgs<float> &, cudaStream_t, int, cudaEvent_t);
 
 // Times every launch variant: for each form (directed; undirected when the
 // pair links exist) every pass-1 shape with a full and a persistent grid,
@@ -690,15 +709,22 @@ template cudaError_t autotune_passes<float>(const EvalArgs<float> &, cudaStream_
                                             int *);
 
 cudaError_t launch_totals(int n_real, const double *V0, const double *S0, const double *Rq,
-                          const double *Rs, const double *Rx, double *out, cudaStream_t st) {
-  totals_kernel<<<1, 1024, 0, st>>>(n_real, V0, S0, Rq, Rs, Rx, out);
+                          const double *Rs, const double *Rx, double *out, double *part,
+                          cudaStream_t st) {
+  totals_part_kernel<<<dim3(kTotParts, 1), kTotThreads, 0, st>>>(nullptr, n_real, V0, S0, Rq,
+                                                                 Rs, Rx, part);
+  totals_final_kernel<<<1, 32, 0, st>>>(part, out);
   return cudaGetLastError();
 }
 
 cudaError_t launch_seg_totals(int n_sys, const int *seg, const double *V0, const double *S0,
                               const double *Rq, const double *Rs, const double *Rx, double *out,
-                              cudaStream_t st) {
-  if (n_sys > 0) seg_totals_kernel<<<n_sys, 1024, 0, st>>>(seg, V0, S0, Rq, Rs, Rx, out);
+                              double *part, cudaStream_t st) {
+  if (n_sys > 0) {
+    totals_part_kernel<<<dim3(kTotParts, n_sys), kTotThreads, 0, st>>>(seg, 0, V0, S0, Rq, Rs,
+                                                                      Rx, part);
+    totals_final_kernel<<<n_sys, 32, 0, st>>>(part, out);
+  }
   return cudaGetLastError();
 }
 

@@ -31,10 +31,10 @@ template <class R> struct EvalArgs {
   const int *own_u = nullptr;  // their sites
   int n_own = 0;
   R *pbuf = nullptr;           // 8 R per slot: gq[3], gs, gx, 0, 0, 0
-  // pair-rule records of the owned pairs (kPrRec R each, pair_rule_record)
-  // and each slot's owned pair and direction (2 t + 0 owned slot, + 1 its
-  // reverse)
-  R *prec = nullptr;
+  // pair-rule records of the owned pairs (pair_rule_record: kPr1 R each in
+  // prec1, the other kPr2 in prec2) and each slot's owned pair and direction
+  // (2 t + 0 owned slot, + 1 its reverse)
+  R *prec1 = nullptr, *prec2 = nullptr;
   const int *slot_own = nullptr;
 };
 
@@ -43,11 +43,15 @@ template <class R> struct EvalArgs {
 // block shape / register cap (0 = default; see kPass1Variants below); pass 1
 // also takes the pass-2 variant, because an undirected pass 2 needs the
 // pair-rule records that pass 1 then makes.
+// `mid`, when given, is recorded between a pass's pair kernel and its site
+// kernel (at the start when the pass has no pair kernel), for per-kernel
+// timing.
 template <class R>
 cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int variant = 0,
-                         int pass2_variant = 0);
+                         int pass2_variant = 0, cudaEvent_t mid = nullptr);
 template <class R>
-cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0);
+cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0,
+                         cudaEvent_t mid = nullptr);
 // variant = shape | kPersistent (persistent grid of resident blocks)
 //           [| kUndirected: pass 1 takes its pair-rule sums, pass 2 its
 //            whole per-pair work, from one evaluation per undirected pair]
@@ -68,10 +72,15 @@ inline bool valid_variants(int v1, int v2) {
 // Undirected pass 2 in two launches: the pair kernel (one thread per owned
 // slot: both directions of the pair into the slot buffer) and the site
 // kernel (one warp per site: the sum over its slots and the epilogue).
-// Needs a.rev, a.own_p, a.own_u, a.pbuf, a.prec and a.slot_own; the launchers
+// Needs a.rev, a.own_p, a.own_u, a.pbuf, a.prec1/2 and a.slot_own; the launchers
 // fall back to the directed default when they are absent.
+// Offset (in R) of prec2 after prec1 in one buffer: kPr1 per owned pair,
+// rounded up to 8 values so that prec2's records stay 32-byte aligned.
+inline size_t prec2_offset(long long n_own) {
+  return ((size_t)kPr1 * (size_t)n_own + 7) / 8 * 8;
+}
 template <class R> inline bool has_undirected(const EvalArgs<R> &a) {
-  return a.rev && a.pbuf && a.prec && a.slot_own;
+  return a.rev && a.pbuf && a.prec1 && a.prec2 && a.slot_own;
 }
 
 // Times every pass-1 and pass-2 variant on this input (reps launches each,
@@ -82,16 +91,18 @@ cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int
                             int *best2);
 
 // Deterministic FP64 totals over real sites: out[0] = sum V0, out[1] = sum S0,
-// out[2] = sum |R_q|^2 + R_sigma^2 (active sites), out[3] = sum R_x^2.
+// out[2] = sum |R_q|^2 + R_sigma^2 (active sites), out[3] = sum R_x^2.  Two
+// launches; part is device scratch of kTotParts * 4 doubles per system.
+constexpr int kTotParts = 32, kTotThreads = 256;
 cudaError_t launch_totals(int n_real, const double *V0, const double *S0,
                           const double *Rq, const double *Rs, const double *Rx,
-                          double *out, cudaStream_t st);
+                          double *out, double *part, cudaStream_t st);
 
 // Totals of each system of a batch: out[4k..4k+3] as launch_totals over the
 // real sites [seg[k], seg[k+1]), bitwise equal to that system's own totals.
 cudaError_t launch_seg_totals(int n_sys, const int *seg, const double *V0, const double *S0,
                               const double *Rq, const double *Rs, const double *Rx,
-                              double *out, cudaStream_t st);
+                              double *out, double *part, cudaStream_t st);
 
 // Non-mean-field density rho_i = sum_j x_j rho_{s_j}(|q_i - q_j|)
 // (density.cpp:44-104) for every real site.

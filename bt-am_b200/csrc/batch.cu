@@ -134,15 +134,19 @@ template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const RadialVie
   a.n_own = b->n_own;
   a.pbuf = reinterpret_cast<R *>(b->pbuf);
   a.slot_own = b->slot_own;
-  a.prec = b->pbuf ? a.pbuf + 8 * (size_t)b->n_pairs : nullptr;
+  if (b->pbuf) {
+    a.prec1 = a.pbuf + 8 * (size_t)b->n_pairs;
+    a.prec2 = a.prec1 + prec2_offset(b->n_own);
+  }
   return a;
 }
 
-// Slot records (8 R per slot) then pair-rule records (kPrRec R per owned pair).
+// Slot records (8 R per slot) then the pair-rule records (prec1, prec2).
 int batch_pbuf(btam_batch *b, size_t elem) {
   if (elem < b->pbuf_elem) elem = b->pbuf_elem;
   const size_t need =
-      ((size_t)(b->n_pairs > 0 ? b->n_pairs : 1) * 8 + (size_t)b->n_own * kPrRec) * elem;
+      ((size_t)(b->n_pairs > 0 ? b->n_pairs : 1) * 8 + prec2_offset(b->n_own) +
+       (size_t)b->n_own * kPr2) * elem;
   b->pbuf_elem = elem;
   if (need <= b->pbuf_bytes) return BTAM_OK;
   BTAM_TRY(dalloc(b->pbuf, b->st, need));
@@ -261,7 +265,8 @@ int batch_build(btam_batch *b) {
   BTAM_TRY(dalloc(b->Rq, b->st, 3 * nr));
   BTAM_TRY(dalloc(b->Rs, b->st, nr));
   BTAM_TRY(dalloc(b->Rx, b->st, nr));
-  BTAM_TRY(dalloc(b->totals, b->st, 4 * (size_t)ns));
+  // totals (4 per system), then the partial sums of the totals reduction
+  BTAM_TRY(dalloc(b->totals, b->st, 4 * (size_t)ns * (1 + kTotParts)));
   BTAM_TRY(dalloc(b->err, b->st, 1));
   BTAM_TRY(dalloc(b->rev, b->st, (size_t)n_pairs));
   BTAM_TRY(dalloc(b->slot_own, b->st, (size_t)n_pairs));
@@ -317,7 +322,8 @@ template <class R> cudaError_t enqueue_eval(btam_batch *b, int form, R *mom, con
   cudaError_t e = launch_pass1(a, b->st, b->variant1[form], b->variant2[form]);
   if (e == cudaSuccess) e = launch_pass2(a, b->st, b->variant2[form]);
   if (e == cudaSuccess)
-    e = launch_seg_totals(b->n_sys, b->seg, b->V0, b->S0, b->Rq, b->Rs, b->Rx, b->totals, b->st);
+    e = launch_seg_totals(b->n_sys, b->seg, b->V0, b->S0, b->Rq, b->Rs, b->Rx, b->totals,
+                          b->totals + 4 * (size_t)b->n_sys, b->st);
   return e;
 }
 

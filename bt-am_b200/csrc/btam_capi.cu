@@ -211,17 +211,21 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const RadialVie
   a.n_own = s->n_own;
   a.pbuf = reinterpret_cast<R *>(s->pbuf);
   a.slot_own = s->slot_own;
-  a.prec = s->pbuf ? a.pbuf + 8 * (size_t)s->n_pairs : nullptr;
+  if (s->pbuf) {
+    a.prec1 = a.pbuf + 8 * (size_t)s->n_pairs;
+    a.prec2 = a.prec1 + prec2_offset(s->n_own);
+  }
   return a;
 }
 
 // Buffer of the undirected kernels, allocated only when an undirected variant
 // is in use: 8 values of R per slot of the real sites' lists (pass-2 slot
-// records), then kPrRec per owned pair (pair-rule records).
+// records), then the pair-rule records of the owned pairs (prec1, prec2).
 int ensure_pbuf(btam_system *s, size_t elem) {
   if (elem < s->pbuf_elem) elem = s->pbuf_elem;
   const size_t need =
-      ((size_t)(s->n_pairs > 0 ? s->n_pairs : 1) * 8 + (size_t)s->n_own * kPrRec) * elem;
+      ((size_t)(s->n_pairs > 0 ? s->n_pairs : 1) * 8 + prec2_offset(s->n_own) +
+       (size_t)s->n_own * kPr2) * elem;
   s->pbuf_elem = elem;
   if (need <= s->pbuf_bytes) return BTAM_OK;
   BTAM_TRY(dalloc(s->pbuf, s->st, need));
@@ -464,7 +468,8 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
     for (double **p : {&s->rho, &s->V0, &s->S0, &s->selfx, &s->Rs, &s->Rx})
       if (e == cudaSuccess) e = dalloc(*p, s->st, n);
     if (e == cudaSuccess) e = dalloc(s->Rq, s->st, 3 * (size_t)n);
-    if (e == cudaSuccess) e = dalloc(s->totals, s->st, 4);
+    // totals, then the partial sums of the two-stage totals reduction
+    if (e == cudaSuccess) e = dalloc(s->totals, s->st, 4 + 4 * kTotParts);
     if (e == cudaSuccess) e = dalloc(s->bbox, s->st, 6);
     if (e == cudaSuccess) e = dalloc(s->grid, s->st, 1);
     st = cuda_status(e);
@@ -716,7 +721,8 @@ int btam_mf_eval_async(btam_system *s, int precision) {
     BTAM_TRY(launch_pass1(a, s->st, s->variant1[1], s->variant2[1]));
     BTAM_TRY(launch_pass2(a, s->st, s->variant2[1]));
   }
-  BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->st));
+  BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->totals + 4,
+                          s->st));
   return BTAM_OK;
 }
 
@@ -825,33 +831,35 @@ int btam_mf_rho(btam_system *s, int precision, double *rho) {
   return read_err(s);
 }
 
-int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]) {
+int btam_mf_eval_profile(btam_system *s, int precision, double ms[5]) {
   if (!s || !ms) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
-  cudaEvent_t ev[4];
+  cudaEvent_t ev[6];
   for (auto &e : ev) BTAM_TRY(cudaEventCreate(&e));
   const size_t nm = (size_t)s->n_real * kMomStride;
   cudaError_t e = cudaEventRecord(ev[0], s->st);
+  const int f = precision == BTAM_FP64 ? 0 : 1;
   if (precision == BTAM_FP64) {
     if (!s->mom64 && e == cudaSuccess) e = dalloc(s->mom64, s->st, nm);
     EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
-    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[0], s->variant2[0]);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
-    if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[0]);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[f], s->variant2[f], ev[1]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], s->st);
+    if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[f], ev[3]);
   } else {
     if (!s->mom32 && e == cudaSuccess) e = dalloc(s->mom32, s->st, nm);
     EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
-    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[1], s->variant2[1]);
-    if (e == cudaSuccess) e = cudaEventRecord(ev[1], s->st);
-    if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[1]);
+    if (e == cudaSuccess) e = launch_pass1(a, s->st, s->variant1[f], s->variant2[f], ev[1]);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], s->st);
+    if (e == cudaSuccess) e = launch_pass2(a, s->st, s->variant2[f], ev[3]);
   }
-  if (e == cudaSuccess) e = cudaEventRecord(ev[2], s->st);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[4], s->st);
   if (e == cudaSuccess)
-    e = launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->st);
-  if (e == cudaSuccess) e = cudaEventRecord(ev[3], s->st);
+    e = launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->totals + 4,
+                      s->st);
+  if (e == cudaSuccess) e = cudaEventRecord(ev[5], s->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
-  for (int k = 0; k < 3 && e == cudaSuccess; ++k) {
+  for (int k = 0; k < 5 && e == cudaSuccess; ++k) {
     float t = 0.f;
     e = cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
     ms[k] = t;

@@ -38,9 +38,10 @@ namespace {
 constexpr int kNoAllocMaxSites = 16384;
 constexpr int kNoAllocMaxDevices = 64;
 // moment records (kMomStride doubles per site; the FP32 form uses the same
-// bytes as floats), then rho, S0, dV0/dx per site, then the error flag
+// bytes as floats), then rho, S0, dV0/dx per site, then the error flag (32
+// doubles' room), then the partial sums of the totals reduction
 constexpr size_t kNoAllocDoubles =
-    (size_t)kNoAllocMaxSites * kMomStride + 3 * (size_t)kNoAllocMaxSites + 32;
+    (size_t)kNoAllocMaxSites * kMomStride + 3 * (size_t)kNoAllocMaxSites + 32 + 4 * kTotParts;
 
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
@@ -102,6 +103,7 @@ extern "C" int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_r
   double *S0 = rho + kNoAllocMaxSites;
   double *selfx = S0 + kNoAllocMaxSites;
   int *err = (int *)(selfx + kNoAllocMaxSites);
+  double *part = selfx + kNoAllocMaxSites + 32;
   // the only state that must start at zero: the error flag (the kernels
   // overwrite every moment record and per-site value they later read)
   e = cudaMemsetAsync(err, 0, sizeof(int), st);
@@ -143,7 +145,7 @@ extern "C" int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_r
     e = launch_pass1(a, st);
     if (e == cudaSuccess) e = launch_pass2(a, st);
   }
-  if (e == cudaSuccess) e = launch_totals(n_real, V0, S0, Rq, Rs, Rx, totals, st);
+  if (e == cudaSuccess) e = launch_totals(n_real, V0, S0, Rq, Rs, Rx, totals, part, st);
   int bits = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&bits, err, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -242,7 +242,7 @@ int btam_dmd_graph_copy(const btam_system *s, int *offs, int *idx, long long idx
  * first then periodic images; gamma per real site; offs/idx = neighbour CSR
  * of the real sites in that all-sites numbering.  Outputs (device): V0, Rs,
  * Rx per real site, Rq 3 per real site, totals[4] as btam_mf_eval.
- * Limit: n_real <= 16384 (BTAM_ERR_TOO_LARGE beyond).  The scratch (~10.4 MB
+ * Limit: n_real <= 16384 (BTAM_ERR_TOO_LARGE beyond).  The scratch (~10.9 MB
  * per device) lives until the process exits and is shared by every call on
  * that device: calls that overlap on the GPU race; serialise them.  The
  * first call on each device looks the scratch up, so make it before any
@@ -354,9 +354,11 @@ int btam_server_destroy(btam_server *srv);
 /* ---- measurement (no counterpart in the reference, which has only PETSc's
  * SNES monitor for tracing) ------------------------------------------------ */
 /* One evaluation as btam_mf_eval_async, with CUDA events on the system's
- * stream around each kernel: ms[0] pass 1, ms[1] pass 2, ms[2] totals.
- * Synchronises. */
-int btam_mf_eval_profile(btam_system *s, int precision, double ms[3]);
+ * stream around each kernel: ms[0] the pass-1 pair-rule kernel, ms[1] the
+ * pass-1 site kernel, ms[2] the pass-2 pair kernel, ms[3] the pass-2 site
+ * kernel, ms[4] the totals (ms[0] and ms[2] are ~0 for the directed
+ * variants, which have no pair kernels).  Synchronises. */
+int btam_mf_eval_profile(btam_system *s, int precision, double ms[5]);
 /* Sustained FMA throughput of the current device in TFLOP/s (FMA = 2 flops)
  * for fp64 = 0 (FP32) or 1 (FP64), from a register-resident FMA loop over
  * every SM lasting about `seconds`. */
