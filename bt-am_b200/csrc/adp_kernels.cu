@@ -171,20 +171,29 @@ __device__ __forceinline__ void halve_level(R (&v)[CAP], R (&lo)[CAP], int lane)
   }
 }
 
-template <int N, class R> __device__ __forceinline__ void lane_tree(R (&v)[N], R (&lo)[N], int lane) {
+// The levels of a tree over groups of G lanes (G = 32 or 16; masks G/2 ... 1):
+// afterwards lane L of a group holds the totals of its group's values
+// tree_base<N, G>(L) + [0, N/G).
+template <int N, int M, class R, int CAP>
+__device__ __forceinline__ void tree_levels(R (&v)[CAP], R (&lo)[CAP], int lane) {
+  halve_level<N, M, N == CAP>(v, lo, lane);
+  if constexpr (M > 1) tree_levels<N / 2, M / 2>(v, lo, lane);
+}
+template <int G, int N, class R> __device__ __forceinline__ void lane_tree(R (&v)[N], R (&lo)[N], int lane) {
   if (sizeof(R) != 4) {  // FP64: no compensation word
 #pragma unroll
     for (int k = 0; k < N; ++k) lo[k] = (R)0;
   }
-  halve_level<N, 16, true>(v, lo, lane);
-  halve_level<N / 2, 8, false>(v, lo, lane);
-  halve_level<N / 4, 4, false>(v, lo, lane);
-  halve_level<N / 8, 2, false>(v, lo, lane);
-  halve_level<N / 16, 1, false>(v, lo, lane);
+  tree_levels<N, G / 2>(v, lo, lane);
 }
-template <int N> __device__ __forceinline__ int lane_tree_base(int lane) {
-  return (N / 2) * ((lane >> 4) & 1) + (N / 4) * ((lane >> 3) & 1) + (N / 8) * ((lane >> 2) & 1) +
-         (N / 16) * ((lane >> 1) & 1) + (N / 32) * (lane & 1);
+template <int N, int G> __device__ __forceinline__ int tree_base(int lane) {
+  int b = 0, n = N;
+#pragma unroll
+  for (int m = G / 2; m >= 1; m >>= 1) {
+    n >>= 1;
+    if (lane & m) b += n;
+  }
+  return b;
 }
 // The total of a lane_tree value: hi + lo in the FP32 form; the FP64 form
 // carries no lo word (its lo array is never written).
@@ -196,44 +205,46 @@ template <class R> __device__ __forceinline__ double tree_total(R hi, R lo) {
 // blocks) shapes; the second number caps the registers per thread and so
 // trades instruction-level parallelism for occupancy.  btam_autotune times
 // the shapes on the actual system and keeps the fastest.
-// Pass 1: one warp per site, one lane per neighbour, in two parts (pass1_pair_part1
+// Pass 1: one group of G lanes per site (G = 32: one site per warp; G = 16:
+// two sites per warp), one lane per neighbour, in two parts (pass1_pair_part1
 // and _part2, so that few accumulators are live at once): each lane
-// evaluates its pair's 13 triplet geometries (and, unless UND, its 12
+// evaluates its pairs' 13 triplet geometries (and, unless UND, their 12
 // pair-rule points) and adds them to its own FP32 partials (at most
-// ceil(250 / 32) = 8 pairs per lane); the warp then forms the per-site
-// compensated totals (lane_tree) and lane 0 runs the FP64 epilogue.
+// ceil(250 / G) pairs per lane); the group then forms the per-site
+// compensated totals (lane_tree) and runs the FP64 epilogue (eight lanes form
+// the record's duals, one the rest).
 // UND: the pair-rule sums (rho, phi, B(f, f) over the 12 pair points) come
-// from the slot records written by pass1u_pair_kernel instead of being
+// from the pair-rule records written by pass1u_pair_kernel instead of being
 // evaluated here.
-template <class R, int W, int MB, bool UND>
+template <class R, int W, int MB, int G, bool UND>
 __global__ void __launch_bounds__(W * 32, MB)
 pass1_kernel(const EvalArgs<R> a) {
-  __shared__ SiteSums ss[W];
+  constexpr int SPW = 32 / G;  // sites per warp
+  __shared__ SiteSums ss[W * SPW];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  // grid-stride over sites: one site per warp per trip (a full grid makes one
-  // trip; a persistent grid of a few blocks per SM makes several)
-  // one copy of the body for every trip: a site or pair gives the same bits
-  // whichever trip of whichever grid computes it
+  const int half = lane / G, sl = lane % G, gbase = half * G;
+  // grid-stride over groups of SPW sites: one group per warp per trip (a full
+  // grid makes one trip; a persistent grid of a few blocks per SM makes
+  // several); one copy of the body for every trip: a site gives the same
+  // bits whichever trip of whichever grid computes it
 #pragma unroll 1
-  for (int i = blockIdx.x * W + warp; i < a.n_real; i += gridDim.x * W) {
-  R *mom = a.mom + (size_t)i * kMomStride;
-  const double2 xbi = a.xb[i];
+  for (int wi = blockIdx.x * W + warp; wi * SPW < a.n_real; wi += gridDim.x * W) {
+  const int i = wi * SPW + half;
+  const bool live = i < a.n_real;
+  const double2 xbi = live ? a.xb[i] : make_double2(0.0, 1.0);
   const double xi = xbi.x;
-  if (xi < kMinOcc) {  // empty site: no energy, no moments
-    for (int c = lane; c < kMomStride; c += 32) mom[c] = (R)0;
-    if (lane == 0) a.rho[i] = a.V0[i] = a.S0[i] = a.selfx[i] = 0.0;
-    continue;
-  }
-  const double4 qi = a.pos[i];
-  const int ci = a.code[i];
-  const int nb0 = a.offs[i], nb1 = a.offs[i + 1];
-  double *site = reinterpret_cast<double *>(&ss[warp]);
+  const bool act = live && !(xi < kMinOcc);
+  R *mom = a.mom + (size_t)(live ? i : 0) * kMomStride;
+  const double4 qi = act ? a.pos[i] : make_double4(0.0, 0.0, 0.0, 0.0);
+  const int ci = act ? a.code[i] : 0;
+  const int nb0 = act ? a.offs[i] : 0, nb1 = act ? a.offs[i + 1] : 0;
+  double *site = reinterpret_cast<double *>(&ss[warp * SPW + half]);
   {  // part I: pair rule, centre and neighbour-displaced points
     R acc[kP1PartI], lo[kP1PartI];
 #pragma unroll
     for (int c = 0; c < kP1PartI; ++c) acc[c] = (R)0;
 #pragma unroll 1
-    for (int p = nb0 + lane; p < nb1; p += 32) {
+    for (int p = nb0 + sl; p < nb1; p += G) {
       const int j = a.idx[p];
       const double2 xbj = a.xb[j];
       if (xbj.x < kMinOcc) continue;
@@ -258,16 +269,19 @@ pass1_kernel(const EvalArgs<R> a) {
       }
       pass1_pair_part1<R>(a.T, r0, (R)qj.w, (R)xi * (R)xbj.x, pair_kind(ci, cj), acc);
     }
-    lane_tree<kP1PartI>(acc, lo, lane);
-    const int v = lane_tree_base<kP1PartI>(lane);
-    if (v < kP1Gd && v != kP1Sself) site[p1_site_slot(v)] = tree_total(acc[0], lo[0]);
+    lane_tree<G>(acc, lo, lane);
+    const int v0 = tree_base<kP1PartI, G>(sl);
+#pragma unroll
+    for (int k = 0; k < kP1PartI / G; ++k)
+      if (act && v0 + k < kP1Gd && v0 + k != kP1Sself)
+        site[p1_site_slot(v0 + k)] = tree_total(acc[k], lo[k]);
   }
   {  // part II: centre-displaced points
     R acc[kP1PartII], lo[kP1PartII];
 #pragma unroll
     for (int c = 0; c < kP1PartII; ++c) acc[c] = (R)0;
 #pragma unroll 1
-    for (int p = nb0 + lane; p < nb1; p += 32) {
+    for (int p = nb0 + sl; p < nb1; p += G) {
       const int j = a.idx[p];
       const double2 xbj = a.xb[j];
       if (xbj.x < kMinOcc) continue;
@@ -275,23 +289,25 @@ pass1_kernel(const EvalArgs<R> a) {
       pass1_pair_part2<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)xi * (R)xbj.x,
                           pair_kind(ci, a.code[j]), acc);
     }
-    lane_tree<kP1PartII>(acc, lo, lane);
-    const int t0 = lane_tree_base<kP1PartII>(lane);
+    lane_tree<G>(acc, lo, lane);
+    const int t0 = tree_base<kP1PartII, G>(sl);
 #pragma unroll
-    for (int k = 0; k < kP1PartII / 32; ++k)
-      if (t0 + k < 1 + 54) site[p1_site_slot(p1_part2_value(t0 + k))] = tree_total(acc[k], lo[k]);
+    for (int k = 0; k < kP1PartII / G; ++k)
+      if (act && t0 + k < 1 + 54)
+        site[p1_site_slot(p1_part2_value(t0 + k))] = tree_total(acc[k], lo[k]);
   }
   __syncwarp();
-  // epilogue: lanes 0..7 form the record's eight duals, lane 0 the rest
+  // epilogue: lanes 0..7 of the group form the record's eight duals, lane 0
+  // the rest
   double b = 0.0;
-  if (lane < 8) b = site_dual(ss[warp], lane, mom);
+  if (act && sl < 8) b = site_dual(ss[warp * SPW + half], sl, mom);
   double bgd = 0.0;
 #pragma unroll
-  for (int d = 0; d < 6; ++d) bgd += __shfl_sync(0xffffffffu, b, 2 + d);
-  if (lane == 0) {
+  for (int d = 0; d < 6; ++d) bgd += __shfl_sync(0xffffffffu, b, gbase + 2 + d);
+  if (act && sl == 0) {
     SiteResult res;
-    site_scalars(ss[warp], bgd, a.emb[ci], xi, ci, xbi.y, a.gamma[i], qi.w, a.mass[ci], res,
-                 mom);
+    site_scalars(ss[warp * SPW + half], bgd, a.emb[ci], xi, ci, xbi.y, a.gamma[i], qi.w,
+                 a.mass[ci], res, mom);
     a.rho[i] = res.rho;
     a.V0[i] = res.V0;
     a.S0[i] = res.S0;
@@ -299,7 +315,11 @@ pass1_kernel(const EvalArgs<R> a) {
     if (!(finite(res.V0) && finite(res.S0) && finite(res.selfx)))
       atomicOr(a.err, 1 << kErrBitNonFinite);
   }
-  __syncwarp();  // the warp's shared buffers are reused by its next site
+  if (live && !act) {  // empty site: no energy, no moments
+    for (int c = sl; c < kMomStride; c += G) mom[c] = (R)0;
+    if (sl == 0) a.rho[i] = a.V0[i] = a.S0[i] = a.selfx[i] = 0.0;
+  }
+  __syncwarp();  // the warp's shared buffers are reused by its next sites
   }
 }
 
@@ -541,8 +561,9 @@ template <class K> int grid_of(K kernel, int n, int W, bool persistent) {
   int g = sms * (per > 0 ? per : 1);
   return g < full ? g : full;
 }
-template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers,
-                                           bool und, cudaEvent_t mid) {
+template <class R, int W, int MB, int G>
+void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers, bool und, cudaEvent_t mid) {
+  const int n_groups = (a.n_real + 32 / G - 1) / (32 / G);
   if (und) {
     auto kp = pass1u_pair_kernel<R, 128>;
     int g = nblocks(a.n_own, 128);
@@ -556,12 +577,12 @@ template <class R, int W, int MB> void go1(const EvalArgs<R> &a, cudaStream_t st
     }
     if (g > 0) kp<<<g, 128, 0, st>>>(a);
     if (mid) cudaEventRecord(mid, st);
-    auto k = pass1_kernel<R, W, MB, true>;
-    k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
+    auto k = pass1_kernel<R, W, MB, G, true>;
+    k<<<grid_of(k, n_groups, W, pers), W * 32, 0, st>>>(a);
   } else {
     if (mid) cudaEventRecord(mid, st);
-    auto k = pass1_kernel<R, W, MB, false>;
-    k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
+    auto k = pass1_kernel<R, W, MB, G, false>;
+    k<<<grid_of(k, n_groups, W, pers), W * 32, 0, st>>>(a);
   }
 }
 template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
@@ -577,11 +598,11 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2, c
   // either pass runs undirected: the undirected pass 2 reads them
   const bool und = ((v | v2) & kUndirected) != 0 && has_undirected(a);
   switch (v & (kPersistent - 1)) {
-  case 1: go1<R, 4, 3>(a, st, pers, und, mid); break;
-  case 2: go1<R, 4, 4>(a, st, pers, und, mid); break;
-  case 3: go1<R, 8, 2>(a, st, pers, und, mid); break;
-  case 4: go1<R, 4, 5>(a, st, pers, und, mid); break;
-  default: go1<R, 4, 1>(a, st, pers, und, mid); break;
+  case 1: go1<R, 4, 4, 32>(a, st, pers, und, mid); break;
+  case 2: go1<R, 4, 4, 16>(a, st, pers, und, mid); break;
+  case 3: go1<R, 8, 2, 16>(a, st, pers, und, mid); break;
+  case 4: go1<R, 4, 5, 16>(a, st, pers, und, mid); break;
+  default: go1<R, 4, 1, 32>(a, st, pers, und, mid); break;
   }
   return cudaGetLastError();
 }

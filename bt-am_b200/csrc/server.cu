@@ -25,6 +25,7 @@
 #include <vector>
 
 #include "../../include/btam.h"
+#include "adp_kernels.cuh"
 #include "sched.hpp"
 
 namespace {
@@ -69,6 +70,14 @@ struct btam_server {
 
 namespace {
 
+// Launch variants of served jobs (index 0 FP64, 1 FP32C): undirected,
+// persistent grid, and the block shapes the autotuner picks for the plain
+// drop-in workload on a B200.
+constexpr int kServeVariant1[2] = {btam::kUndirected | btam::kPersistent | 1,
+                                   btam::kUndirected | btam::kPersistent | 3};
+constexpr int kServeVariant2[2] = {btam::kUndirected | btam::kPersistent | 0,
+                                   btam::kUndirected | btam::kPersistent | 2};
+
 // Runs one job on the calling worker thread; fills job->res and the outputs.
 void run_job(btam_server *srv, Job *job) {
   const btam_job_spec &sp = job->spec;
@@ -80,6 +89,11 @@ void run_job(btam_server *srv, Job *job) {
                               job->gamma.empty() ? nullptr : job->gamma.data(), job->origin,
                               job->cell, job->periodic, &s);
   if (st == BTAM_OK) st = btam_neighbors_build(s, 0);
+  // every job runs the undirected kernels (each neighbour pair evaluated once
+  // for both directions) on persistent grids, in both arithmetic forms; their
+  // pair buffers are part of btam_estimate_bytes
+  if (st == BTAM_OK) st = btam_set_variants(s, BTAM_FP32C, kServeVariant1[1], kServeVariant2[1]);
+  if (st == BTAM_OK) st = btam_set_variants(s, BTAM_FP64, kServeVariant1[0], kServeVariant2[0]);
   if (st == BTAM_OK) {
     r.t_start = since(srv->t0);
     if (sp.kind == BTAM_JOB_RELAX) {
@@ -174,11 +188,15 @@ long long btam_estimate_bytes(int n, const double cell[9], const int periodic[3]
   // cell slot, image code; per real site: state, staging, results, both
   // moment records, neighbour counts, the neighbour candidate buffer, the
   // neighbour list at the cap, master-equation state and graph, relaxation
-  // vectors; plus a fixed allowance for cells and library scratch
+  // vectors, and the undirected kernels' buffers at the cap (per slot:
+  // reverse slot, owned-pair link and an FP64 slot record; per owned pair,
+  // at most one per two slots: the pair and site indices and an FP64
+  // pair-rule record); plus a fixed allowance for cells and library scratch
   const double per_all = 32 + 16 + 4 + 4 + 4 + 4 + 4;
-  const double per_real = 8 + 40 + 48 + 24 + 76 * 8 + 76 * 4 + 8 + 256 * 4 +
+  const double per_slot = 4 + 4 + 8 * 8 + 0.5 * (4 + 4 + (btam::kPrRec + 8) * 8);
+  const double per_real = 8 + 40 + 48 + 24 + btam::kMomStride * 8 + btam::kMomStride * 4 + 8 + 256 * 4 +
                           BTAM_MAXNEIGH * 4 + 16 + 16 + 4 + BTAM_MAX_CHEMICAL_NEIGHS * 4 +
-                          (2 * 8 + 8) * 5 * 8;
+                          (2 * 8 + 8) * 5 * 8 + BTAM_MAXNEIGH * per_slot;
   return (long long)(n_all * per_all + n * per_real) + (8ll << 20);
 }
 

@@ -60,6 +60,7 @@ def test_server_results_alone_equal_in_mix(gpu_tables):
     # an evaluation job equals the direct evaluation of the system
     S = btam.System(gpu_tables, jobs[4][0])
     S.build_neighbors()
+    S.set_variants(btam.FP32C, 16 | 8 | 3, 16 | 8 | 2)  # the server's FP32C launch variants
     tot = S.evaluate(btam.FP32C)["totals"]
     assert alone[4]["objective"] == tot[0] and alone[4]["norm"] == tot[2]
 
