@@ -44,6 +44,10 @@ FLOP_PASS1, FLOP_PASS2 = 1000.0, 2000.0  # algorithmic flops per directed active
 # u, w), 26 at the 13 triplet points (u, w); the algorithmic flops of each
 # pass are attributed to kernels by these lookups
 LOOK_PR, LOOK_TRIP = 48.0, 26.0
+# DRAM bytes (read + write) per launch of the FP32C kernels on this workload,
+# from one ncu capture (--set full) of the undirected variants (28, 26)
+NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 118.4e6, "pass1 site kernel": 65.3e6,
+                  "pass2 pair kernel": 286.9e6, "pass2 site kernel": 120.7e6, "totals": 1.5e6}
 
 
 def kernel_flops(undirected):
@@ -452,7 +456,8 @@ def run_btam(args, ws, rank, local):
     eval_rate = (FLOP_PASS1 + FLOP_PASS2) * P / (results["fp32c"]["ms"] * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": names[dom] + " (FP32C)", "achieved": achieved,
                 "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": None,
+                "traffic": NCU_DRAM_BYTES.get(names[dom]) if und else None,
+                "traffic_unit": "bytes per launch (ncu dram read + write)",
                 "peak_source": "measured live: btam_probe_fma_peak FP32 FMA loop on all SMs",
                 "flops_per_launch": flops[dom] * P,
                 "kernel_ms": dict(zip(names, map(float, prof))),

@@ -630,7 +630,7 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent
   const bool pers = (v & kPersistent) != 0;
   if ((v & kUndirected) && has_undirected(a)) {
     switch (v & (kPersistent - 1)) {
-    case 1: go2u<R, 128, 3>(a, st, pers, mid); break;
+    case 1: go2u<R, 128, 5>(a, st, pers, mid); break;
     case 2: go2u<R, 128, 4>(a, st, pers, mid); break;
     case 3: go2u<R, 256, 2>(a, st, pers, mid); break;
     default: go2u<R, 128, 1>(a, st, pers, mid); break;

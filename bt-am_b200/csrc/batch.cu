@@ -1,6 +1,7 @@
 // Batched evaluation: many independent systems (cells or clusters of uneven
-// size) evaluated by one persistent pass-1 launch, one persistent pass-2
-// launch and one per-system totals launch, replayed as a single CUDA graph.
+// size) evaluated by the same kernels as one system (pass 1 with its
+// pair-rule kernel, pass 2 with its pair and site kernels, per-system
+// totals), on persistent grids, replayed as a single CUDA graph.
 //
 // Layout in HBM: the real sites of every system first (system k owns rows
 // [R_k, R_k + n_k)), then the periodic images of every system (system k owns

@@ -431,6 +431,7 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
   }
   s->any_periodic = periodic[0] || periodic[1] || periodic[2];
   st = validate_state(s, n, q, sigma, x, code.data());
+  s->host_code = code;
   if (st == BTAM_OK && beta)
     for (int i = 0; i < n; ++i)
       if (!(std::isfinite(beta[i]) && beta[i] > 0.0)) st = BTAM_ERR_NONFINITE;
@@ -504,14 +505,7 @@ void btam_system_destroy(btam_system *s) {
 int btam_system_set_state(btam_system *s, const double *q, const double *sigma,
                           const double *x) {
   if (!s) return BTAM_ERR_ARG;
-  std::vector<int> code;
-  if (x) {
-    code.resize(s->n_real);
-    BTAM_TRY(cudaMemcpyAsync(code.data(), s->code, s->n_real * sizeof(int),
-                             cudaMemcpyDeviceToHost, s->st));
-    BTAM_TRY(cudaStreamSynchronize(s->st));
-  }
-  int st = validate_state(s, s->n_real, q, sigma, x, x ? code.data() : nullptr);
+  int st = validate_state(s, s->n_real, q, sigma, x, x ? s->host_code.data() : nullptr);
   if (st != BTAM_OK) return st;
   const int n = s->n_real;
   double *dq = s->stage, *ds = s->stage + 3 * (size_t)n, *dx = s->stage + 4 * (size_t)n;

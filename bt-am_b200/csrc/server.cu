@@ -73,8 +73,8 @@ namespace {
 // Launch variants of served jobs (index 0 FP64, 1 FP32C): undirected,
 // persistent grid, and the block shapes the autotuner picks for the plain
 // drop-in workload on a B200.
-constexpr int kServeVariant1[2] = {btam::kUndirected | btam::kPersistent | 1,
-                                   btam::kUndirected | btam::kPersistent | 3};
+constexpr int kServeVariant1[2] = {btam::kUndirected | btam::kPersistent | 3,
+                                   btam::kUndirected | btam::kPersistent | 4};
 constexpr int kServeVariant2[2] = {btam::kUndirected | btam::kPersistent | 0,
                                    btam::kUndirected | btam::kPersistent | 2};
 
