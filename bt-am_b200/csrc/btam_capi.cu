@@ -45,6 +45,40 @@ __global__ void pack_state_kernel(int n, const double *q, const double *sigma,
   xb[i] = b;
 }
 
+// Validation of a staged state update (the checks of validate_state, on the
+// device): bit 0 a non-finite or non-positive value, bit 1 a non-H site with
+// 0 < x < min_occupancy, bit 2 a site outside the cell along a periodic axis.
+__global__ void validate_stage_kernel(int n, const double *q, const double *sigma,
+                                      const double *x, const int *code, GhostBox b,
+                                      int *flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int f = 0;
+  if (q) {
+    const double q0 = q[3 * i], q1 = q[3 * i + 1], q2 = q[3 * i + 2];
+    if (!(isfinite(q0) && isfinite(q1) && isfinite(q2))) f |= 1;
+    else
+      for (int a = 0; a < 3; ++a) {
+        if (!b.periodic[a]) continue;
+        if (b.ortho) {
+          const double v = a == 0 ? q0 : (a == 1 ? q1 : q2);
+          if (!(v >= b.lo[a] && v < b.hi[a])) f |= 4;
+        } else {
+          const double d0 = q0 - b.origin[0], d1 = q1 - b.origin[1], d2 = q2 - b.origin[2];
+          const double sa = d0 * b.B[a][0] + d1 * b.B[a][1] + d2 * b.B[a][2];
+          if (!(sa >= -1e-9 && sa < 1.0 + 1e-9)) f |= 4;
+        }
+      }
+  }
+  if (sigma && !(isfinite(sigma[i]) && sigma[i] > 0.0)) f |= 1;
+  if (x) {
+    const double v = x[i];
+    if (!isfinite(v) || v < 0.0) f |= 1;
+    else if (code[i] == 0 && v > 0.0 && v < BTAM_MIN_OCCUPANCY) f |= 2;
+  }
+  if (f) atomicOr(flags, f);
+}
+
 // FMA throughput probe: kProbeChains independent dependency chains per
 // thread keep the FMA pipe full; the result is stored so nothing is elided.
 constexpr int kProbeChains = 8;
@@ -431,7 +465,6 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
   }
   s->any_periodic = periodic[0] || periodic[1] || periodic[2];
   st = validate_state(s, n, q, sigma, x, code.data());
-  s->host_code = code;
   if (st == BTAM_OK && beta)
     for (int i = 0; i < n; ++i)
       if (!(std::isfinite(beta[i]) && beta[i] > 0.0)) st = BTAM_ERR_NONFINITE;
@@ -464,7 +497,8 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
       else e = cudaMemsetAsync(s->gamma, 0, n * sizeof(double), s->st);
     }
     if (e == cudaSuccess) e = dalloc(s->stage, s->st, 5 * (size_t)n);
-    if (e == cudaSuccess) e = dalloc(s->err, s->st, 1);
+    // err[0]: error bits of the kernels; err[1]: state-validation flags
+    if (e == cudaSuccess) e = dalloc(s->err, s->st, 2);
     if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->st);
     for (double **p : {&s->rho, &s->V0, &s->S0, &s->selfx, &s->Rs, &s->Rx})
       if (e == cudaSuccess) e = dalloc(*p, s->st, n);
@@ -505,13 +539,24 @@ void btam_system_destroy(btam_system *s) {
 int btam_system_set_state(btam_system *s, const double *q, const double *sigma,
                           const double *x) {
   if (!s) return BTAM_ERR_ARG;
-  int st = validate_state(s, s->n_real, q, sigma, x, x ? s->host_code.data() : nullptr);
-  if (st != BTAM_OK) return st;
+  // the update is staged on the device and validated there (the checks of
+  // validate_state); the device keeps the old state if it is rejected
   const int n = s->n_real;
   double *dq = s->stage, *ds = s->stage + 3 * (size_t)n, *dx = s->stage + 4 * (size_t)n;
   if (q) BTAM_TRY(cudaMemcpyAsync(dq, q, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s->st));
   if (sigma) BTAM_TRY(cudaMemcpyAsync(ds, sigma, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
   if (x) BTAM_TRY(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  if (!q && !sigma && !x) return BTAM_OK;
+  BTAM_TRY(cudaMemsetAsync(s->err + 1, 0, sizeof(int), s->st));
+  validate_stage_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(
+      n, q ? dq : nullptr, sigma ? ds : nullptr, x ? dx : nullptr, s->code, s->box, s->err + 1);
+  BTAM_TRY(cudaGetLastError());
+  int flags = 0;
+  BTAM_TRY(cudaMemcpyAsync(&flags, s->err + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  if (flags & 1) return BTAM_ERR_NONFINITE;
+  if (flags & 2) return BTAM_ERR_OCCUPANCY;
+  if (flags & 4) return BTAM_ERR_OUT_OF_BOX;
   pack_state_kernel<<<(n + 127) / 128, 128, 0, s->st>>>(n, q ? dq : nullptr, sigma ? ds : nullptr,
                                                         x ? dx : nullptr, s->pos, s->xb);
   BTAM_TRY(cudaGetLastError());

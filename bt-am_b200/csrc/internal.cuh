@@ -40,9 +40,6 @@ struct btam_system {
   int *code = nullptr, *owner = nullptr;
   char4 *image = nullptr;
   double *gamma = nullptr;
-  // species codes of the real sites on the host (fixed at creation; read by
-  // the state validation of every update without a device round trip)
-  std::vector<int> host_code;
   // staging for host updates
   double *stage = nullptr;  // 5 n_real doubles: q (3n), sigma, x
   // neighbour lists

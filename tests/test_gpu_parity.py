@@ -154,6 +154,34 @@ def test_launch_variants(gpu_tables):
         S.set_variants(btam.FP64, 5, 0)
 
 
+def test_state_update_rejections(gpu_tables):
+    """btam_system_set_state validates an update before it replaces the
+    state: non-finite or non-positive values, a non-H site with
+    0 < x < min_occupancy and a site outside a periodic cell are rejected
+    with their codes, and the device keeps the previous state."""
+    s = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.5, x_range=(0.0, 0.3), seed=17)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    base = S.evaluate(btam.FP64)
+    mg = np.flatnonzero(s["species"] == 12)[0]
+    bad_q = s["q"].copy()
+    bad_q[5, 1] = np.nan
+    out_q = s["q"].copy()
+    out_q[7, 0] = s["origin"][0] - 1.0
+    bad_s = s["sigma"].copy()
+    bad_s[3] = 0.0
+    bad_x = s["x"].copy()
+    bad_x[mg] = 1e-4
+    for kw, code in ((dict(q=bad_q), 6), (dict(q=out_q), 14), (dict(sigma=bad_s), 6),
+                     (dict(x=bad_x), 10)):
+        with pytest.raises(btam.BtamError) as e:
+            S.set_state(**kw)
+        assert e.value.code == code, (kw.keys(), e.value.code)
+        again = S.evaluate(btam.FP64)
+        for k in ("V0", "Rq", "Rs", "Rx"):
+            assert np.array_equal(again[k], base[k]), k
+
+
 def test_persistent_grid_bitwise_on_large_system(gpu_tables):
     """A system with more sites and pairs than one wave of resident blocks:
     the persistent grid computes most sites and pairs in later trips of its
