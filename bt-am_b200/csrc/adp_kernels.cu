@@ -64,6 +64,79 @@ __device__ __forceinline__ V3<R> pair_vec(const double4 &a, const double4 &b) {
 
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
+// What the pair kernels read about a neighbour: one 32-byte load from the
+// packed Site32 rows in the FP32C form, the separate arrays otherwise.
+template <class R> struct NbSite {
+  double x, y, z;
+  R sigma, occ;
+  int code;
+  bool active;
+};
+template <class R> __device__ __forceinline__ NbSite<R> nb_site(const EvalArgs<R> &a, int j) {
+  NbSite<R> n;
+  if (sizeof(R) == 4 && a.s32) {
+    double4 h;
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"(h.x), "=d"(h.y), "=d"(h.z), "=d"(h.w)
+        : "l"(a.s32 + j));
+    const long long w = __double_as_longlong(h.w);  // (sig_code, occ), low word first
+    const float sig_code = __int_as_float((int)(w & 0xffffffffll));
+    const float occ = __int_as_float((int)(w >> 32));
+    n.x = h.x;
+    n.y = h.y;
+    n.z = h.z;
+    n.sigma = (R)fabsf(sig_code);
+    n.code = sig_code < 0.0f ? 1 : 0;
+    n.occ = (R)occ;
+    n.active = occ >= 0.0f;
+  } else {
+    const double4 q = a.pos[j];
+    const double2 xb = a.xb[j];
+    n.x = q.x;
+    n.y = q.y;
+    n.z = q.z;
+    n.sigma = (R)q.w;
+    n.occ = (R)xb.x;
+    n.code = a.code[j];
+    n.active = !(xb.x < kMinOcc);
+  }
+  return n;
+}
+template <class R> __device__ __forceinline__ double nb_beta(const EvalArgs<R> &a, int j) {
+  return (sizeof(R) == 4 && a.sb) ? a.sb[j].beta : a.xb[j].y;
+}
+template <class R> __device__ __forceinline__ int nb_owner(const EvalArgs<R> &a, int j) {
+  return (sizeof(R) == 4 && a.sb) ? a.sb[j].owner : a.owner[j];
+}
+template <class R> __device__ __forceinline__ V3<R> pair_vec(const double4 &a, const NbSite<R> &b) {
+  return mk3<R>((R)(a.x - b.x), (R)(a.y - b.y), (R)(a.z - b.z));
+}
+template <class R>
+__device__ __forceinline__ V3<R> pair_vec(const NbSite<R> &a, const NbSite<R> &b) {
+  return mk3<R>((R)(a.x - b.x), (R)(a.y - b.y), (R)(a.z - b.z));
+}
+
+// Packs the FP32C neighbour rows (Site32, SiteB) of all sites.
+__global__ void pack_sites_kernel(int n, const double4 *pos, const double2 *xb, const int *code,
+                                  const int *owner, Site32 *s32, SiteB *sb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 q = pos[i];
+  const double2 b = xb[i];
+  Site32 r;
+  r.x = q.x;
+  r.y = q.y;
+  r.z = q.z;
+  r.sig_code = code[i] == 1 ? -(float)q.w : (float)q.w;
+  r.occ = b.x < kMinOcc ? -1.0f : (float)b.x;
+  s32[i] = r;
+  SiteB e;
+  e.beta = b.y;
+  e.owner = owner[i];
+  e.pad = 0;
+  sb[i] = e;
+}
+
 // ---- slot records of the undirected kernels (8 R per slot) -----------------
 // 256-bit record store/load of one slot (8 R).
 __device__ __forceinline__ void st_rec(float *p, const float (&v)[8]) {
@@ -115,12 +188,11 @@ pass1u_pair_kernel(const EvalArgs<R> a) {
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
     const int p = a.own_p[t], u = a.own_u[t];
     const int j = a.idx[p];
-    const double2 xbu = a.xb[u], xbj = a.xb[j];
+    const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
     R rec[kPrRec];
-    if (!(xbu.x < kMinOcc) && !(xbj.x < kMinOcc)) {
-      const double4 qu = a.pos[u], qj = a.pos[j];
-      pair_rule_record<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
-                          a.code[u], a.code[j], rec);
+    if (su.active && sj.active) {
+      pair_rule_record<R>(a.T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
+                          sj.code, rec);
     } else {
 #pragma unroll
       for (int c = 0; c < kPrRec; ++c) rec[c] = (R)0;
@@ -245,29 +317,27 @@ pass1_kernel(const EvalArgs<R> a) {
     for (int c = 0; c < kP1PartI; ++c) acc[c] = (R)0;
 #pragma unroll 1
     for (int p = nb0 + sl; p < nb1; p += G) {
-      const int j = a.idx[p];
-      const double2 xbj = a.xb[j];
-      if (xbj.x < kMinOcc) continue;
-      const double4 qj = a.pos[j];
-      const int cj = a.code[j];
-      const V3<R> r0 = pair_vec<R>(qi, qj);
+      const NbSite<R> sj = nb_site(a, a.idx[p]);
+      if (!sj.active) continue;
+      const int cj = sj.code;
+      const V3<R> r0 = pair_vec<R>(qi, sj);
       if (UND) {
         const int so = a.slot_own[p];
         R rec[4];
         ld4(a.prec1 + (size_t)kPr1 * (so >> 1), rec);
-        const R xj = (R)xbj.x, X = (R)xi * xj;
+        const R xj = sj.occ, X = (R)xi * xj;
         acc[kP1Rho] += xj * rec[(so & 1) ? 0 : 1];
         acc[kP1Epair] += (R)0.5 * X * rec[2];
         acc[kP1Ediag] += X * X * rec[3];
       } else {
         R rj, ep, ed;
-        pass1_pair_rule<R>(a.T, r0, (R)qi.w, (R)qj.w, (R)xi, (R)xbj.x, ci, cj, rj, nullptr, ep,
+        pass1_pair_rule<R>(a.T, r0, (R)qi.w, sj.sigma, (R)xi, sj.occ, ci, cj, rj, nullptr, ep,
                            ed);
         acc[kP1Rho] += rj;
         acc[kP1Epair] += ep;
         acc[kP1Ediag] += ed;
       }
-      pass1_pair_part1<R>(a.T, r0, (R)qj.w, (R)xi * (R)xbj.x, pair_kind(ci, cj), acc);
+      pass1_pair_part1<R>(a.T, r0, sj.sigma, (R)xi * sj.occ, pair_kind(ci, cj), acc);
     }
     lane_tree<G>(acc, lo, lane);
     const int v0 = tree_base<kP1PartI, G>(sl);
@@ -282,12 +352,10 @@ pass1_kernel(const EvalArgs<R> a) {
     for (int c = 0; c < kP1PartII; ++c) acc[c] = (R)0;
 #pragma unroll 1
     for (int p = nb0 + sl; p < nb1; p += G) {
-      const int j = a.idx[p];
-      const double2 xbj = a.xb[j];
-      if (xbj.x < kMinOcc) continue;
-      const double4 qj = a.pos[j];
-      pass1_pair_part2<R>(a.T, pair_vec<R>(qi, qj), (R)qi.w, (R)xi * (R)xbj.x,
-                          pair_kind(ci, a.code[j]), acc);
+      const NbSite<R> sj = nb_site(a, a.idx[p]);
+      if (!sj.active) continue;
+      pass1_pair_part2<R>(a.T, pair_vec<R>(qi, sj), (R)qi.w, (R)xi * sj.occ,
+                          pair_kind(ci, sj.code), acc);
     }
     lane_tree<G>(acc, lo, lane);
     const int t0 = tree_base<kP1PartII, G>(sl);
@@ -398,13 +466,13 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
     const int p = a.own_p[t], u = a.own_u[t];
     const int j = a.idx[p], r = a.rev[p];
-    const double2 xbu = a.xb[u], xbj = a.xb[j];
+    const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
     R vu[8], vj[8];
 #pragma unroll
     for (int c = 0; c < 8; ++c) vu[c] = vj[c] = (R)0;
-    if (!(xbu.x < kMinOcc) && !(xbj.x < kMinOcc)) {
-      const int o = a.owner[j];
-      const double4 qu = a.pos[u], qj = a.pos[j];
+    if (su.active && sj.active) {
+      const int o = nb_owner(a, j);
+      const double bu = nb_beta(a, u), bj = nb_beta(a, j);
       const MomRec<R, true> mu(a.mom + (size_t)u * kMomStride);
       const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
       Pass2Out<R> ou, oj;
@@ -425,10 +493,9 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
 #pragma unroll
         for (int c = 0; c < 8; ++c) pr[kPr1 + 8 * h + c] = v[c];
       }
-      pass2_pair_sym<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xbu.x, (R)xbj.x,
-                        a.code[u], a.code[j], mu.scalar(0), mu.scalar(1), mj.scalar(0),
-                        mj.scalar(1), (R)(xbj.y / xbu.y), (R)(xbu.y / xbj.y), mu, mj, pr, ou,
-                        oj);
+      pass2_pair_sym<R>(a.T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
+                        sj.code, mu.scalar(0), mu.scalar(1), mj.scalar(0), mj.scalar(1),
+                        (R)(bj / bu), (R)(bu / bj), mu, mj, pr, ou, oj);
       vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
       vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
     }
@@ -597,6 +664,9 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2, c
   // the pair-rule records are made (and then also used by pass 1) whenever
   // either pass runs undirected: the undirected pass 2 reads them
   const bool und = ((v | v2) & kUndirected) != 0 && has_undirected(a);
+  if (a.s32 && a.n_all > 0)
+    pack_sites_kernel<<<nblocks(a.n_all, 256), 256, 0, st>>>(a.n_all, a.pos, a.xb, a.code,
+                                                             a.owner, a.s32, a.sb);
   switch (v & (kPersistent - 1)) {
   case 1: go1<R, 4, 4, 32>(a, st, pers, und, mid); break;
   case 2: go1<R, 4, 4, 16>(a, st, pers, und, mid); break;

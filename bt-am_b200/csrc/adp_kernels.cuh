@@ -7,10 +7,28 @@
 
 namespace btam {
 
+// Packed copy of what the FP32C kernels read about a neighbour, one 32-byte
+// sector per site (made by launch_pass1 from pos / xb / code): the position
+// in double, sigma with the species in its sign (negative: H), and the
+// occupancy as the kernels use it, or -1 when the site is empty (occupancy
+// below min_occupancy, decided in double).
+struct __align__(32) Site32 {
+  double x, y, z;
+  float sig_code, occ;
+};
+// beta and owner of a site, for the pass-2 pair kernel.
+struct __align__(16) SiteB {
+  double beta;
+  int owner, pad;
+};
+
 // Device view of one system for an evaluation.  Site arrays cover real sites
 // then periodic images ("all sites"); per-site outputs cover real sites.
 template <class R> struct EvalArgs {
   int n_real;
+  int n_all = 0;        // real sites + images (rows of the site arrays)
+  Site32 *s32 = nullptr;  // FP32C: packed neighbour data [all] (nullptr: unpacked)
+  SiteB *sb = nullptr;    // FP32C: beta and owner [all]
   const double4 *pos;   // x, y, z, sigma            [all]
   const double2 *xb;    // occupancy x, beta         [all]
   const int *code;      // 0 = Mg, 1 = H             [all]

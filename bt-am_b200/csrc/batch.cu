@@ -85,6 +85,8 @@ struct btam_batch {
   double *gamma = nullptr;
   int *offs = nullptr, *idx = nullptr;
   // undirected pass 2: reverse slots, owned slots and their sites, slot buffer
+  Site32 *s32 = nullptr;  // packed neighbour rows of the FP32C kernels [all]
+  SiteB *sb = nullptr;
   int *rev = nullptr, *slot_own = nullptr, *own_p = nullptr, *own_u = nullptr;
   int n_own = 0;
   char *pbuf = nullptr;
@@ -108,6 +110,11 @@ namespace {
 template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const RadialView<R> &T) {
   EvalArgs<R> a;
   a.n_real = b->n_real;
+  a.n_all = b->n_all;
+  if (sizeof(R) == 4) {
+    a.s32 = b->s32;
+    a.sb = b->sb;
+  }
   a.pos = b->pos;
   a.xb = b->xb;
   a.code = b->code;
@@ -207,6 +214,8 @@ void free_batch(btam_batch *b) {
   dfree(b->mom32, b->st);
   dfree(b->err, b->st);
   dfree(b->rev, b->st);
+  dfree(b->s32, b->st);
+  dfree(b->sb, b->st);
   dfree(b->slot_own, b->st);
   dfree(b->own_p, b->st);
   dfree(b->own_u, b->st);
@@ -256,6 +265,8 @@ int batch_build(btam_batch *b) {
   BTAM_TRY(dalloc(b->xb, b->st, na));
   BTAM_TRY(dalloc(b->code, b->st, na));
   BTAM_TRY(dalloc(b->owner, b->st, na));
+  BTAM_TRY(dalloc(b->s32, b->st, na));
+  BTAM_TRY(dalloc(b->sb, b->st, na));
   BTAM_TRY(dalloc(b->gamma, b->st, nr));
   BTAM_TRY(dalloc(b->offs, b->st, nr + 1));
   BTAM_TRY(dalloc(b->idx, b->st, (size_t)n_pairs));

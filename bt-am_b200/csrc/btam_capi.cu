@@ -211,6 +211,9 @@ int ensure_sites(btam_system *s, int n_all) {
   s->xb = xb;
   s->code = code;
   s->owner = owner;
+  // packed neighbour rows of the FP32C kernels (rewritten by every pass 1)
+  BTAM_TRY(dalloc(s->s32, s->st, cap));
+  BTAM_TRY(dalloc(s->sb, s->st, cap));
   s->cap_all = cap;
   return BTAM_OK;
 }
@@ -218,6 +221,11 @@ int ensure_sites(btam_system *s, int n_all) {
 template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const RadialView<R> &T) {
   EvalArgs<R> a;
   a.n_real = s->n_real;
+  a.n_all = s->n_real + s->n_ghost;
+  if (sizeof(R) == 4) {
+    a.s32 = s->s32;
+    a.sb = s->sb;
+  }
   a.pos = s->pos;
   a.xb = s->xb;
   a.code = s->code;
@@ -521,6 +529,7 @@ void btam_system_destroy(btam_system *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
   dfree(s->pos, s->st); dfree(s->xb, s->st); dfree(s->code, s->st); dfree(s->owner, s->st); dfree(s->image, s->st);
+  dfree(s->s32, s->st); dfree(s->sb, s->st);
   dfree(s->gamma, s->st); dfree(s->stage, s->st); dfree(s->offs, s->st); dfree(s->idx, s->st); dfree(s->cnt, s->st);
   dfree(s->tmp, s->st); dfree(s->bbox, s->st); dfree(s->grid, s->st); dfree(s->cell_of, s->st); dfree(s->cell_cnt, s->st);
   dfree(s->cell_start, s->st); dfree(s->cursor, s->st); dfree(s->cell_sites, s->st); dfree(s->rho, s->st); dfree(s->V0, s->st);

@@ -9,6 +9,7 @@
 
 #include "adp_core.cuh"
 #include "tables_io.hpp"
+#include "adp_kernels.cuh"
 #include "topo_kernels.cuh"
 
 using namespace btam;
@@ -40,6 +41,8 @@ struct btam_system {
   int *code = nullptr, *owner = nullptr;
   char4 *image = nullptr;
   double *gamma = nullptr;
+  Site32 *s32 = nullptr;  // packed neighbour rows of the FP32C kernels [all]
+  SiteB *sb = nullptr;
   // staging for host updates
   double *stage = nullptr;  // 5 n_real doubles: q (3n), sigma, x
   // neighbour lists
