@@ -318,6 +318,47 @@ def bench_batched(args, tables, flush, max_over_ranks, barrier):
     return res
 
 
+def bench_nanowire(args, tables):
+    """The precision workload: hcp Mg nanowire of radius 30 A along c, 20
+    cells long, periodic along the axis, H occupancy x ~ U[0, 0.5] beyond
+    20 A and 0.02 inside (seed 3).  1000 master-equation steps (dt = 1e-3)
+    with FP32C residuals and FP64 occupancy updates in integer quanta: total
+    hydrogen is checked to the quantum and the trajectory against the same
+    run with FP64 residuals."""
+    import torch
+    import btam
+    from btam import lattice
+
+    sys_ = lattice.config3()
+    h = sys_["species"] == 1
+    steps = args.dmd_steps
+    out, xs = {}, {}
+    for prec, name in ((btam.FP32C, "fp32c"), (btam.FP64, "fp64")):
+        S = btam.System(tables, sys_)
+        S.build_neighbors()
+        S.autotune(prec)
+        S.dmd_setup()
+        total0 = S.dmd_step(0, prec, dt=1e-3)
+        S.dmd_step(3, prec, dt=0.0)  # warm-up steps that move nothing (dt = 0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        total = S.dmd_step(steps, prec, dt=1e-3)
+        t = time.perf_counter() - t0
+        x, X, mu = S.dmd_occupancy()
+        xs[name] = x
+        out[name] = {"steps_per_s": steps / t, "ms_per_step": t * 1e3 / steps,
+                     "total_h_conserved": bool(total == total0),
+                     "x_min": float(x[h].min()), "x_max": float(x[h].max())}
+        S.close()
+    nr = len(sys_["x"])
+    return {"workload": "hcp Mg nanowire R = 30 A along c, 20 cells, periodic along the axis, "
+                        "x ~ U[0, 0.5] beyond 20 A, 0.02 inside, seed 3",
+            "sites": nr, "h_sites": int(h.sum()), "steps": steps, "dt": 1e-3,
+            "timing": "host clock around one call of all steps (device-resident loop)",
+            **out,
+            "fp32c_vs_fp64_max_abs_dx": float(np.abs(xs["fp32c"] - xs["fp64"]).max())}
+
+
 def bench_serving(args, tables):
     """The served workload: a seeded Poisson stream (mean 200 jobs/s) of 64
     jobs, half relaxations (L-BFGS to |R| <= 1e-5 or 100 iterations) and half
@@ -508,6 +549,7 @@ def run_btam(args, ws, rank, local):
     batched = None if args.no_batch else bench_batched(args, tables, flush, max_over_ranks,
                                                         barrier)
     serving = None if args.no_serve else bench_serving(args, tables)
+    nanowire = None if args.no_wire else bench_nanowire(args, tables)
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
@@ -539,7 +581,8 @@ def run_btam(args, ws, rank, local):
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "ms_per_step": e2e_ms},
                 "gpu_launches": launches_per_eval(shapes["fp32c"]) * args.steps,
-                "clocks": clocks, "batched": batched, "serving": serving}
+                "clocks": clocks, "batched": batched, "serving": serving,
+                "precision_nanowire": nanowire}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -556,6 +599,9 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched workload")
     ap.add_argument("--no-serve", action="store_true", help="skip the served workload")
     ap.add_argument("--serve-jobs", type=int, default=64, help="jobs in the served stream")
+    ap.add_argument("--no-wire", action="store_true", help="skip the nanowire DMD workload")
+    ap.add_argument("--dmd-steps", type=int, default=1000,
+                    help="master-equation steps of the nanowire workload")
     args = ap.parse_args()
     ws, rank, local = dist_env()
     if args.impl == "reference":

@@ -116,3 +116,21 @@ def test_master_equation_long_run_conserves_and_bounds(gpu_tables):
     assert np.all(X[h] >= 0) and np.all(x[h] <= 0.9 + 1e-12)
     assert np.all(np.isfinite(mu))
     assert np.array_equal(x[h], X[h] * 2.0 ** -50)
+
+
+def test_master_equation_nanowire_conserves(gpu_tables):
+    """The precision workload's system (hcp Mg nanowire, radius 30 A, 20
+    cells, periodic along the axis, H x ~ U[0, 0.5] beyond 20 A): FP32C
+    residuals, FP64 occupancy updates; total hydrogen exact to the quantum
+    and occupancies inside [0, 0.9] after 50 steps."""
+    s = lattice.config3()
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    S.dmd_setup()
+    total0 = S.dmd_step(0, btam.FP32C, dt=1e-3)
+    total = S.dmd_step(50, btam.FP32C, dt=1e-3)
+    assert total == total0
+    x, X, mu = S.dmd_occupancy()
+    h = s["species"] == 1
+    assert np.all(X[h] >= 0) and np.all(x[h] <= 0.9 + 1e-12) and np.all(np.isfinite(mu))
+    assert np.abs(x[h] - s["x"][h]).max() > 0.0  # hydrogen moved
