@@ -120,6 +120,23 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def reduce_max(v, dist, device):
+    """v on this rank -> the maximum over ranks (v itself without a process
+    group); device: where the reduction tensor lives ("cuda" for NCCL)."""
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(ws, step_ms):
+    """Whole-job evaluations per second: every rank evaluates its own replica
+    once per step, and a step lasts as long as the slowest rank's."""
+    return ws * 1e3 / step_ms
+
+
 def launches_per_eval(shape):
     """Kernel launches of one evaluation with launch variants (v1, v2): pass 1
     (plus the pair-rule kernel when either pass is undirected), pass 2 (pair
@@ -460,11 +477,7 @@ def run_btam(args, ws, rank, local):
             dist.barrier()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(v, dist, "cuda")
 
     results = {}
     clocks = None
@@ -481,7 +494,7 @@ def run_btam(args, ws, rank, local):
         if name == "fp32c":
             clocks = cs.summary()
         step_ms = max_over_ranks(float(np.mean(ms)))
-        results[name] = dict(ms=step_ms, value=ws * 1e3 / step_ms)
+        results[name] = dict(ms=step_ms, value=replica_value(ws, step_ms))
     S.set_variants(btam.FP64, *shapes["fp64"])
     # per-kernel times for the roofline (FP32C form)
     prof = np.median(np.array([S.profile(btam.FP32C) for _ in range(7)]), axis=0)

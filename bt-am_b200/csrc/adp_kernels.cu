@@ -137,8 +137,8 @@ __global__ void pack_sites_kernel(int n, const double4 *pos, const double2 *xb, 
   sb[i] = e;
 }
 
-// ---- slot records of the undirected kernels (8 R per slot) -----------------
-// 256-bit record store/load of one slot (8 R).
+// ---- record stores of the undirected kernels -------------------------------
+// 256-bit store of 8 R.
 __device__ __forceinline__ void st_rec(float *p, const float (&v)[8]) {
   asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(v[0]),
                "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
@@ -161,20 +161,6 @@ template <> __device__ __forceinline__ void st_rec4<double>(double *p, const dou
   asm volatile("st.global.v4.f64 [%0], {%1,%2,%3,%4};" ::"l"(p), "d"(v[0]), "d"(v[1]),
                "d"(v[2]), "d"(v[3])
                : "memory");
-}
-__device__ __forceinline__ void ld_rec(const float *p, float (&v)[8]) {
-  asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]),
-                 "=f"(v[6]), "=f"(v[7])
-               : "l"(p));
-}
-__device__ __forceinline__ void ld_rec(const double *p, double (&v)[8]) {
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
-               : "l"(p));
-  asm volatile("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
-               : "=d"(v[4]), "=d"(v[5]), "=d"(v[6]), "=d"(v[7])
-               : "l"(p + 4));
 }
 
 
@@ -499,8 +485,13 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
       vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
       vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
     }
-    st_rec(a.pbuf + 8 * (size_t)p, vu);
-    if (r >= 0) st_rec(a.pbuf + 8 * (size_t)r, vj);
+    // slot records: (gq, gs) as one 4-vector, gx in its own array
+    st_rec4(a.pbuf + 4 * (size_t)p, vu);
+    a.pgx[p] = vu[4];
+    if (r >= 0) {
+      st_rec4(a.pbuf + 4 * (size_t)r, vj);
+      a.pgx[r] = vj[4];
+    }
   }
 }
 
@@ -525,10 +516,11 @@ pass2u_site_kernel(const EvalArgs<R> a) {
     }
     Acc<R> acc[5];
     for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
-      R v[8];
-      ld_rec(a.pbuf + 8 * (size_t)p, v);
+      R v[4];
+      ld4(a.pbuf + 4 * (size_t)p, v);
 #pragma unroll
-      for (int c = 0; c < 5; ++c) acc[c].add(v[c]);
+      for (int c = 0; c < 4; ++c) acc[c].add(v[c]);
+      acc[4].add(ld_ro(a.pgx + p));
     }
     double t[5];
 #pragma unroll
@@ -551,7 +543,7 @@ pass2u_site_kernel(const EvalArgs<R> a) {
 // sites [lo + len b / P, lo + len (b + 1) / P) of system k (lo = seg[k],
 // len = seg[k + 1] - lo; one system [0, n) when seg is null) with fixed
 // per-thread strides and a fixed tree into part[k][b]; stage 2: one warp per
-// system sums its P partials in a fixed shuffle tree.  The order depends only
+// system sums its P partials (lane-strided, then a fixed shuffle tree).  The order depends only
 // on the system's own sites, so a system's totals in a batch equal its own
 // totals bitwise.
 __global__ void __launch_bounds__(kTotThreads)
@@ -582,7 +574,8 @@ totals_part_kernel(const int *seg, int n, const double *V0, const double *S0, co
 __global__ void __launch_bounds__(32) totals_final_kernel(const double *part, double *out) {
   const int k = blockIdx.x, lane = threadIdx.x;
   for (int c = 0; c < 4; ++c) {
-    double v = part[((size_t)k * kTotParts + lane) * 4 + c];
+    double v = 0.0;
+    for (int b = lane; b < kTotParts; b += 32) v += part[((size_t)k * kTotParts + b) * 4 + c];
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if (lane == 0) out[4 * k + c] = v;

@@ -48,7 +48,8 @@ template <class R> struct EvalArgs {
   const int *own_p = nullptr;  // owned slots
   const int *own_u = nullptr;  // their sites
   int n_own = 0;
-  R *pbuf = nullptr;           // 8 R per slot: gq[3], gs, gx, 0, 0, 0
+  R *pbuf = nullptr;           // 4 R per slot: gq[3], gs (pass-2 contributions)
+  R *pgx = nullptr;            // 1 R per slot: gx
   // pair-rule records of the owned pairs (pair_rule_record: kPr1 R each in
   // prec1, the other kPr2 in prec2) and each slot's owned pair and direction
   // (2 t + 0 owned slot, + 1 its reverse)
@@ -94,13 +95,21 @@ inline bool valid_variants(int v1, int v2) {
 // kernel (one warp per site: the sum over its slots and the epilogue).
 // Needs a.rev, a.own_p, a.own_u, a.pbuf, a.prec1/2 and a.slot_own; the launchers
 // fall back to the directed default when they are absent.
-// Offset (in R) of prec2 after prec1 in one buffer: kPr1 per owned pair,
-// rounded up to 8 values so that prec2's records stay 32-byte aligned.
-inline size_t prec2_offset(long long n_own) {
-  return ((size_t)kPr1 * (size_t)n_own + 7) / 8 * 8;
+// Layout (in R) of the undirected kernels' buffer: the slot 4-vectors (4 per
+// slot), the slot gx values (1 per slot), the pair-rule records prec1 (kPr1
+// per owned pair) and prec2 (kPr2 per owned pair), each part starting on a
+// 32-byte boundary.
+inline size_t round8(size_t v) { return (v + 7) / 8 * 8; }
+inline size_t pbuf_gx_offset(long long n_slots) { return round8(4 * (size_t)n_slots); }
+inline size_t pbuf_prec1_offset(long long n_slots) {
+  return pbuf_gx_offset(n_slots) + round8((size_t)n_slots);
+}
+inline size_t prec2_offset(long long n_own) { return round8((size_t)kPr1 * (size_t)n_own); }
+inline size_t pbuf_values(long long n_slots, long long n_own) {
+  return pbuf_prec1_offset(n_slots) + prec2_offset(n_own) + (size_t)kPr2 * (size_t)n_own;
 }
 template <class R> inline bool has_undirected(const EvalArgs<R> &a) {
-  return a.rev && a.pbuf && a.prec1 && a.prec2 && a.slot_own;
+  return a.rev && a.pbuf && a.pgx && a.prec1 && a.prec2 && a.slot_own;
 }
 
 // Times every pass-1 and pass-2 variant on this input (reps launches each,
@@ -113,7 +122,7 @@ cudaError_t autotune_passes(const EvalArgs<R> &a, cudaStream_t st, int reps, int
 // Deterministic FP64 totals over real sites: out[0] = sum V0, out[1] = sum S0,
 // out[2] = sum |R_q|^2 + R_sigma^2 (active sites), out[3] = sum R_x^2.  Two
 // launches; part is device scratch of kTotParts * 4 doubles per system.
-constexpr int kTotParts = 32, kTotThreads = 256;
+constexpr int kTotParts = 64, kTotThreads = 256;
 cudaError_t launch_totals(int n_real, const double *V0, const double *S0,
                           const double *Rq, const double *Rs, const double *Rx,
                           double *out, double *part, cudaStream_t st);

@@ -143,18 +143,19 @@ template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const RadialVie
   a.pbuf = reinterpret_cast<R *>(b->pbuf);
   a.slot_own = b->slot_own;
   if (b->pbuf) {
-    a.prec1 = a.pbuf + 8 * (size_t)b->n_pairs;
+    a.pgx = a.pbuf + pbuf_gx_offset(b->n_pairs);
+    a.prec1 = a.pbuf + pbuf_prec1_offset(b->n_pairs);
     a.prec2 = a.prec1 + prec2_offset(b->n_own);
   }
   return a;
 }
 
-// Slot records (8 R per slot) then the pair-rule records (prec1, prec2).
+// Slot records (5 R per slot) then the pair-rule records (prec1, prec2);
+// layout in pbuf_values and its helpers.
 int batch_pbuf(btam_batch *b, size_t elem) {
   if (elem < b->pbuf_elem) elem = b->pbuf_elem;
   const size_t need =
-      ((size_t)(b->n_pairs > 0 ? b->n_pairs : 1) * 8 + prec2_offset(b->n_own) +
-       (size_t)b->n_own * kPr2) * elem;
+      pbuf_values(b->n_pairs > 0 ? b->n_pairs : 1, b->n_own) * elem;
   b->pbuf_elem = elem;
   if (need <= b->pbuf_bytes) return BTAM_OK;
   BTAM_TRY(dalloc(b->pbuf, b->st, need));

@@ -254,20 +254,21 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const RadialVie
   a.pbuf = reinterpret_cast<R *>(s->pbuf);
   a.slot_own = s->slot_own;
   if (s->pbuf) {
-    a.prec1 = a.pbuf + 8 * (size_t)s->n_pairs;
+    a.pgx = a.pbuf + pbuf_gx_offset(s->n_pairs);
+    a.prec1 = a.pbuf + pbuf_prec1_offset(s->n_pairs);
     a.prec2 = a.prec1 + prec2_offset(s->n_own);
   }
   return a;
 }
 
 // Buffer of the undirected kernels, allocated only when an undirected variant
-// is in use: 8 values of R per slot of the real sites' lists (pass-2 slot
-// records), then the pair-rule records of the owned pairs (prec1, prec2).
+// is in use: the pass-2 slot records of the real sites' lists (5 values of R
+// per slot), then the pair-rule records of the owned pairs (prec1, prec2);
+// layout in pbuf_values and its helpers.
 int ensure_pbuf(btam_system *s, size_t elem) {
   if (elem < s->pbuf_elem) elem = s->pbuf_elem;
   const size_t need =
-      ((size_t)(s->n_pairs > 0 ? s->n_pairs : 1) * 8 + prec2_offset(s->n_own) +
-       (size_t)s->n_own * kPr2) * elem;
+      pbuf_values(s->n_pairs > 0 ? s->n_pairs : 1, s->n_own) * elem;
   s->pbuf_elem = elem;
   if (need <= s->pbuf_bytes) return BTAM_OK;
   BTAM_TRY(dalloc(s->pbuf, s->st, need));
