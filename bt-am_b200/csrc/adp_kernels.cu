@@ -195,14 +195,13 @@ pass1u_pair_kernel(const EvalArgs<R> a) {
   }
 }
 
-// Sum over the 32 lanes of a warp of each lane's N partials (N a multiple of
-// 32), by recursive halving: at each level a lane keeps half of its current
-// index range and adds its partner's values for that half (partner lane ^ 16,
-// 8, 4, 2, 1).  In the FP32 form every addition is a two-sum and the
-// rounding errors ride along as a second FP32 word (lo), so the per-site
-// totals are compensated sums of the lanes' partials.  Lane L ends with the
-// totals of values base(L) + [0, N/32), base = N/2 b4 + N/4 b3 + N/8 b2 +
-// N/16 b1 + N/32 b0 (b = bits of L), in v[0..N/32) (+ lo[0..N/32)).
+// Sum over a group of G lanes of each lane's N partials (N a multiple of G),
+// by recursive halving: at each level a lane keeps half of its current index
+// range and adds its partner's values for that half (partner lane ^ G/2, ...,
+// ^ 1).  In the FP32 form every addition is a two-sum and the rounding
+// errors ride along as a second FP32 word (lo), so the per-site totals are
+// compensated sums of the lanes' partials.  Lane L of a group ends with the
+// totals of values tree_base<N, G>(L) + [0, N/G), in v[0..N/G) (+ lo).
 template <int N, int M, bool FIRST, class R, int CAP>
 __device__ __forceinline__ void halve_level(R (&v)[CAP], R (&lo)[CAP], int lane) {
   const bool up = (lane & M) != 0;
@@ -229,7 +228,7 @@ __device__ __forceinline__ void halve_level(R (&v)[CAP], R (&lo)[CAP], int lane)
   }
 }
 
-// The levels of a tree over groups of G lanes (G = 32 or 16; masks G/2 ... 1):
+// The levels of a tree over groups of G lanes (G = 32, 16 or 8; masks G/2 ... 1):
 // afterwards lane L of a group holds the totals of its group's values
 // tree_base<N, G>(L) + [0, N/G).
 template <int N, int M, class R, int CAP>
@@ -263,8 +262,8 @@ template <class R> __device__ __forceinline__ double tree_total(R hi, R lo) {
 // blocks) shapes; the second number caps the registers per thread and so
 // trades instruction-level parallelism for occupancy.  btam_autotune times
 // the shapes on the actual system and keeps the fastest.
-// Pass 1: one group of G lanes per site (G = 32: one site per warp; G = 16:
-// two sites per warp), one lane per neighbour, in two parts (pass1_pair_part1
+// Pass 1: one group of G lanes per site (G = 32, 16 or 8: one, two or four
+// sites per warp), one lane per neighbour, in two parts (pass1_pair_part1
 // and _part2, so that few accumulators are live at once): each lane
 // evaluates its pairs' 13 triplet geometries (and, unless UND, their 12
 // pair-rule points) and adds them to its own FP32 partials (at most
@@ -661,7 +660,7 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2, c
     pack_sites_kernel<<<nblocks(a.n_all, 256), 256, 0, st>>>(a.n_all, a.pos, a.xb, a.code,
                                                              a.owner, a.s32, a.sb);
   switch (v & (kPersistent - 1)) {
-  case 1: go1<R, 4, 4, 32>(a, st, pers, und, mid); break;
+  case 1: go1<R, 4, 5, 8>(a, st, pers, und, mid); break;
   case 2: go1<R, 4, 4, 16>(a, st, pers, und, mid); break;
   case 3: go1<R, 8, 2, 16>(a, st, pers, und, mid); break;
   case 4: go1<R, 4, 5, 16>(a, st, pers, und, mid); break;
