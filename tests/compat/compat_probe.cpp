@@ -1,0 +1,103 @@
+// Test infrastructure only: a reference-style caller of the mean-field
+// plugin table, built against the reference's type declarations (the
+// oracle's shim of Macros.hpp) and include/btam_dmd_equations.hpp, linked
+// with libbtam.so.  Reads a system from a binary file, evaluates it site by
+// site through the table the way a residual assembly would (summing the
+// pair derivatives over i in {u} U N(u)), and writes the per-site values.
+//
+// Input (doubles unless noted): n (int), species (n ints), q (3n), sigma,
+// x, beta, gamma (n each), origin (3), cell (9), periodic (3 ints).
+// Output: per site rho, V0, S0, Rq (3), dV0/dsigma, dV0/dx; then the
+// status of the last evaluation.
+#include "Macros.hpp"
+#include "btam_dmd_equations.hpp"
+
+#include <cstdio>
+#include <vector>
+
+int main(int argc, char **argv) {
+  if (argc != 4) return 2;
+  FILE *f = fopen(argv[2], "rb");
+  if (!f) return 2;
+  int n = 0;
+  if (fread(&n, sizeof(int), 1, f) != 1) return 2;
+  std::vector<int> spc(n), per(3);
+  std::vector<double> q(3 * n), sigma(n), x(n), beta(n), gamma(n), origin(3), cell(9);
+  bool ok = fread(spc.data(), sizeof(int), n, f) == (size_t)n &&
+            fread(q.data(), sizeof(double), 3 * n, f) == (size_t)(3 * n) &&
+            fread(sigma.data(), sizeof(double), n, f) == (size_t)n &&
+            fread(x.data(), sizeof(double), n, f) == (size_t)n &&
+            fread(beta.data(), sizeof(double), n, f) == (size_t)n &&
+            fread(gamma.data(), sizeof(double), n, f) == (size_t)n &&
+            fread(origin.data(), sizeof(double), 3, f) == 3 &&
+            fread(cell.data(), sizeof(double), 9, f) == 9 &&
+            fread(per.data(), sizeof(int), 3, f) == 3;
+  fclose(f);
+  if (!ok) return 2;
+  btam_tables *T = nullptr;
+  btam_system *S = nullptr;
+  int st = btam_tables_load(argv[1], &T);
+  if (st == BTAM_OK)
+    st = btam_system_create(T, n, q.data(), sigma.data(), x.data(), spc.data(), beta.data(),
+                            gamma.data(), origin.data(), cell.data(), per.data(), &S);
+  if (st == BTAM_OK) st = btam_neighbors_build(S, 0);
+  if (st == BTAM_OK) st = btam_compat::bind(S, BTAM_FP64, beta.data(), gamma.data());
+  if (st != BTAM_OK) {
+    fprintf(stderr, "set-up failed: %s\n", btam_status_string(st));
+    return 1;
+  }
+  long long np = 0;
+  int nr = 0, ng = 0;
+  btam_system_info(S, &nr, &ng, &np);
+  std::vector<int> offs(n + 1), idx(np > 0 ? np : 1);
+  btam_neighbors_copy(S, offs.data(), idx.data(), (long long)idx.size());
+  // the caller's fields, as the reference holds them (images are not rows
+  // of these arrays: neighbours of a site that are images are skipped)
+  Eigen::MatrixXd mean_q(n, 3);
+  Eigen::VectorXd stdv_q(n), xi(n), rho_v(n), beta_v(n), gamma_v(n);
+  std::vector<AtomicSpecie> specie(n);
+  for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < 3; ++k) mean_q(i, k) = q[3 * i + k];
+    stdv_q(i) = sigma[i];
+    xi(i) = x[i];
+    beta_v(i) = beta[i];
+    gamma_v(i) = gamma[i];
+    specie[i] = (AtomicSpecie)spc[i];
+  }
+  dmd_equations eq = btam_DMD_MgHx_constructor();
+  FILE *o = fopen(argv[3], "wb");
+  if (!o) return 2;
+  for (int u = 0; u < n; ++u) {
+    std::vector<PetscInt> nb;
+    for (int p = offs[u]; p < offs[u + 1]; ++p)
+      if (idx[p] < n) nb.push_back(idx[p]);
+    AtomTopology topo{(int)nb.size(), nb.data()};
+    double v[8];
+    v[0] = eq.evaluate_mf_rho_i(u, mean_q, stdv_q, xi, specie.data(), topo);
+    rho_v(u) = v[0];
+    v[1] = eq.evaluate_V0_i(u, mean_q, stdv_q, xi, rho_v, specie.data(), topo);
+    v[2] = eq.evaluate_S0_i(u, mean_q, stdv_q, xi, rho_v, beta_v, gamma_v, specie.data(), topo);
+    // residual assembly over i in {u} U N(u), as a caller of the reference's
+    // pair derivatives would write it
+    double g[4] = {0, 0, 0, 0}, gx = 0;
+    for (int k = -1; k < (int)nb.size(); ++k) {
+      const unsigned i = k < 0 ? u : nb[k];
+      Eigen::Vector4d d = eq.evaluate_DV0_i_Dq_j(u, i, mean_q, stdv_q, xi, rho_v,
+                                                 specie.data(), topo);
+      for (int c = 0; c < 4; ++c) g[c] += d(c);
+      gx += eq.evaluate_DV0_i_Dxi_j(u, i, mean_q, stdv_q, xi, rho_v, specie.data(), topo);
+    }
+    v[3] = g[0];
+    v[4] = g[1];
+    v[5] = g[2];
+    v[6] = g[3];
+    v[7] = gx;
+    fwrite(v, sizeof(double), 8, o);
+  }
+  const int last = btam_compat::last_status();
+  fwrite(&last, sizeof(int), 1, o);
+  fclose(o);
+  btam_system_destroy(S);
+  btam_tables_destroy(T);
+  return last == BTAM_OK ? 0 : 1;
+}

@@ -40,3 +40,11 @@ def test_workload_sizes():
     assert 80 <= (c1["species"] == 1).sum() <= 120
     c2 = lattice.supercell(20, 15, 15, with_tetra=True)
     assert (c2["species"] == 12).sum() == 9000 and (c2["species"] == 1).sum() == 18000
+
+
+def test_plugin_table_adapter_builds():
+    """include/btam_dmd_equations.hpp compiles against the reference's type
+    declarations (the oracle's shim of Macros.hpp and of Eigen) into a
+    reference-style caller, and that caller links against libbtam.so."""
+    import compat_build
+    assert os.path.exists(compat_build.build_probe())

@@ -1,0 +1,58 @@
+"""The reference's per-site plugin table (dmd_equations) served by
+libbtam through include/btam_dmd_equations.hpp: a reference-style caller
+(tests/compat/compat_probe.cpp) evaluates a system site by site and sums the
+pair derivatives over i in {u} U N(u), as a residual assembly would; the
+per-site values and the assembled derivatives must equal the direct
+evaluation through the C ABI, to the bit for the values and within 1e-12
+for the derivatives the adapter rebuilds from the residuals."""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import btam
+from btam import lattice
+
+pytestmark = pytest.mark.gpu
+TABLES = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                      "bt-am_b200", "data")
+
+
+def write_system(path, s):
+    n = len(s["x"])
+    with open(path, "wb") as f:
+        f.write(np.int32(n).tobytes())
+        f.write(np.ascontiguousarray(s["species"], np.int32).tobytes())
+        for k in ("q", "sigma", "x", "beta", "gamma", "origin", "cell"):
+            f.write(np.ascontiguousarray(s[k], np.float64).tobytes())
+        f.write(np.ascontiguousarray(s["periodic"], np.int32).tobytes())
+
+
+def test_plugin_table_matches_direct_evaluation(gpu_tables, tmp_path):
+    import compat_build
+    probe = compat_build.build_probe()
+    s = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.5, x_range=(0.0, 0.4),
+                          sigma_range=(0.08, 0.15), jitter=0.02, seed=23)
+    n = len(s["x"])
+    inp, out = str(tmp_path / "sys.bin"), str(tmp_path / "out.bin")
+    write_system(inp, s)
+    r = subprocess.run([probe, TABLES, inp, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    raw = open(out, "rb").read()
+    v = np.frombuffer(raw[:8 * 8 * n], np.float64).reshape(n, 8)
+    assert np.frombuffer(raw[8 * 8 * n:], np.int32)[0] == 0
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    d = S.evaluate(btam.FP64)
+    assert np.array_equal(v[:, 0], d["rho"]) and np.array_equal(v[:, 1], d["V0"])
+    assert np.array_equal(v[:, 2], d["S0"]) and np.array_equal(v[:, 3:6], d["Rq"])
+    beta, sigma, x, gamma = s["beta"], s["sigma"], s["x"], s["gamma"]
+    dsig = d["Rs"] + 3.0 / (beta * sigma)
+    h = (s["species"] == 1) & (x >= 5e-4)
+    dlogz = 3.0 / (2.0 * x[h]) + np.where(x[h] < 1.0, 1.0 / (1.0 - x[h]), 0.0)
+    dx = np.zeros(n)
+    dx[h] = d["Rx"][h] + dlogz / beta[h] + np.where(x[h] < 0.9999, gamma[h] / beta[h], 0.0)
+    scale = max(1.0, np.abs(dsig).max(), np.abs(dx).max())
+    assert np.abs(v[:, 6] - dsig).max() <= 1e-12 * scale
+    assert np.abs(v[:, 7] - dx).max() <= 1e-12 * scale
