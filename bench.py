@@ -44,10 +44,16 @@ FLOP_PASS1, FLOP_PASS2 = 1000.0, 2000.0  # algorithmic flops per directed active
 # u, w), 26 at the 13 triplet points (u, w); the algorithmic flops of each
 # pass are attributed to kernels by these lookups
 LOOK_PR, LOOK_TRIP = 48.0, 26.0
-# DRAM bytes (read + write) per launch of the FP32C kernels on this workload,
-# from one ncu capture (--set full) of the undirected variants (28, 26)
-NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 118.4e6, "pass1 site kernel": 65.3e6,
-                  "pass2 pair kernel": 286.9e6, "pass2 site kernel": 120.7e6, "totals": 1.5e6}
+# Per launch of the FP32C kernels on this workload, from one ncu capture
+# (--set full) of the undirected variants (28, 26): DRAM bytes (read +
+# write), and L1 global-load sectors (32 bytes each) with the L1 LSU
+# data-pipe utilisation
+NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 112.6e6, "pass1 site kernel": 67.7e6,
+                  "pass2 pair kernel": 254.2e6, "pass2 site kernel": 75.1e6, "totals": 1.5e6}
+NCU_L1_SECTORS = {"pass1 pair-rule kernel": 51.73e6, "pass1 site kernel": 54.59e6,
+                  "pass2 pair kernel": 50.42e6, "pass2 site kernel": 2.56e6}
+NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.71,
+               "pass2 pair kernel": 0.66, "pass2 site kernel": 0.30}
 
 
 def kernel_flops(undirected):
@@ -382,14 +388,16 @@ def bench_serving(args, tables):
     100-step master-equation runs, on periodic cubes of 250-60 000 Mg,
     nanowires and spheres.  FP32C jobs served by 8 workers with memory-budget
     admission, against the plain drop-in: the same stream run one job at a
-    time in FP64.  Latency = completion - arrival, queueing included."""
+    time in FP64 on the plain two-pass kernel pair (and, beside it, the same
+    one-at-a-time stream on the server's FP64 kernels).  Latency = completion
+    - arrival, queueing included."""
     import threading
     import btam
     from btam import lattice
 
     jobs = lattice.config5(n_jobs=args.serve_jobs)
 
-    def serve(workers, fp64):
+    def serve(workers, fp64, plain=False):
         srv = btam.Server(tables, workers=workers)
         srv.wait(srv.submit(lattice.periodic_cube(300, seed=1), kind=btam.JOB_EVAL))  # warm-up
         ids = [None] * len(jobs)
@@ -402,10 +410,12 @@ def bench_serving(args, tables):
                     time.sleep(d)
                 if kind == "relax":
                     ids[k] = srv.submit(sysd, kind=btam.JOB_RELAX, tol=1e-5, max_iter=100,
-                                        mode=btam.RELAX_FP64 if fp64 else btam.RELAX_FP32C)
+                                        mode=btam.RELAX_FP64 if fp64 else btam.RELAX_FP32C,
+                                        plain=plain)
                 else:
                     ids[k] = srv.submit(sysd, kind=btam.JOB_DMD, nsteps=100,
-                                        precision=btam.FP64 if fp64 else btam.FP32C)
+                                        precision=btam.FP64 if fp64 else btam.FP32C,
+                                        plain=plain)
 
         th = threading.Thread(target=feeder)
         th.start()
@@ -421,15 +431,19 @@ def bench_serving(args, tables):
                 "residual_evaluations": evals}
 
     served = serve(8, False)
-    plain = serve(1, True)
+    plain = serve(1, True, plain=True)
+    fp64_one = serve(1, True)
     sizes = np.array([len(s["x"]) for _, s, _ in jobs])
     return {"workload": f"{len(jobs)} jobs, Poisson mean 200 jobs/s (seed 5): relaxation "
                         "(|R| <= 1e-5 or 100 L-BFGS iterations) and 100-step master "
                         "equation, half each, on periodic cubes 250-60000 Mg, nanowires, "
                         "spheres",
             "sites_total": int(sizes.sum()), "sites_max": int(sizes.max()),
-            "served_fp32c_8_workers": served, "plain_fp64_one_at_a_time": plain,
-            "served_over_plain_jobs_per_s": served["jobs_per_s"] / plain["jobs_per_s"]}
+            "served_fp32c_8_workers": served,
+            "plain_fp64_one_at_a_time": dict(plain, kernels="plain two-pass pair, variants (0, 0)"),
+            "fp64_one_at_a_time": dict(fp64_one, kernels="the server's undirected kernels"),
+            "served_over_plain_jobs_per_s": served["jobs_per_s"] / plain["jobs_per_s"],
+            "served_over_fp64_one_at_a_time": served["jobs_per_s"] / fp64_one["jobs_per_s"]}
 
 
 def run_btam(args, ws, rank, local):
@@ -501,6 +515,7 @@ def run_btam(args, ws, rank, local):
     prof64 = np.median(np.array([S.profile(btam.FP64) for _ in range(7)]), axis=0)
     fp32_peak = btam.probe_fma_peak(False, 0.5)
     fp64_peak = btam.probe_fma_peak(True, 0.5)
+    gather_peak = btam.probe_gather_peak(tables, 0.5)
     und = bool(shapes["fp32c"][1] & 16)
     flops = kernel_flops(und)
     names = ["pass1 pair-rule kernel", "pass1 site kernel", "pass2 pair kernel",
@@ -518,6 +533,18 @@ def run_btam(args, ws, rank, local):
                 "kernel_flops_per_directed_pair": dict(zip(names, flops)),
                 "evaluation": {"flops": (FLOP_PASS1 + FLOP_PASS2) * P, "achieved": eval_rate,
                                "frac": eval_rate / fp32_peak},
+                "l1_gather": {
+                    "bound": "L1 data pipe (random 32-byte record gathers)",
+                    "peak_gbs": gather_peak,
+                    "peak_source": "measured live: btam_probe_gather_peak, random 32-byte "
+                                   "spline-record gathers on all SMs",
+                    "kernels": {k: {"sector_gbs": NCU_L1_SECTORS[k] * 32 / (prof[i] * 1e-3) / 1e9,
+                                    "frac": NCU_L1_SECTORS[k] * 32 / (prof[i] * 1e-3) / 1e9 /
+                                    gather_peak,
+                                    "ncu_data_pipe_frac": NCU_L1_PIPE[k]}
+                                for i, k in enumerate(names) if k in NCU_L1_SECTORS} if und
+                    else None,
+                    "sectors_source": "L1 global-load sectors per launch from one ncu capture"},
                 "fp64_form": {"kernel_ms": dict(zip(names, map(float, prof64))),
                               "fp64_peak": fp64_peak,
                               "evaluation_frac": (FLOP_PASS1 + FLOP_PASS2) * P /

@@ -68,6 +68,7 @@ _PROTOS = {
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
+    "btam_probe_gather_peak": (ctypes.c_int, [_V, ctypes.c_double, _D]),
     "btam_autotune": (ctypes.c_int, [_V, ctypes.c_int, _I, _I]),
     "btam_relax": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                   _D, _D]),
@@ -112,7 +113,7 @@ class JobSpec(ctypes.Structure):
                 ("tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("lbfgs_m", ctypes.c_int),
                 ("sigma_min", ctypes.c_double), ("sigma_max", ctypes.c_double),
                 ("x_min", ctypes.c_double), ("nsteps", ctypes.c_int),
-                ("dmd_params", ctypes.c_double * 5)]
+                ("dmd_params", ctypes.c_double * 5), ("plain", ctypes.c_int)]
 
 
 class JobResult(ctypes.Structure):
@@ -162,6 +163,15 @@ def _i(a):
 def _check(code, what):
     if code != 0:
         raise BtamError(code, what)
+
+
+def probe_gather_peak(tables, seconds=0.5):
+    """Random 32-byte record gathers from the L1-resident spline tables,
+    GB/s over the device."""
+    out = np.zeros(1)
+    _check(lib().btam_probe_gather_peak(tables.handle, float(seconds), _d(out)),
+           "btam_probe_gather_peak")
+    return float(out[0])
 
 
 def probe_fma_peak(fp64=False, seconds=0.5):
@@ -489,7 +499,9 @@ class Server:
         self.sizes = {}
 
     def submit(self, sysdict, kind, precision=FP32C, mode=RELAX_FP32C, tol=1e-5, max_iter=300,
-               nsteps=100, dmd=(1e-3, 0.045, 3.2, 1e-8, 0.9)):
+               nsteps=100, dmd=(1e-3, 0.045, 3.2, 1e-8, 0.9), plain=False):
+        """Queues a job; plain=True runs it on the plain two-pass kernel pair
+        instead of the server's undirected kernels."""
         s = sysdict
         arrs = dict(q=np.ascontiguousarray(s["q"], np.float64),
                     sigma=np.ascontiguousarray(s["sigma"], np.float64),
@@ -509,6 +521,7 @@ class Server:
         sp.species = _i(arrs["species"])
         sp.periodic = _i(arrs["periodic"])
         sp.tol, sp.max_iter, sp.nsteps = float(tol), int(max_iter), int(nsteps)
+        sp.plain = int(bool(plain))
         for c in range(5):
             sp.dmd_params[c] = float(dmd[c])
         jid = ctypes.c_longlong()

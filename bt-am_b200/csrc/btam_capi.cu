@@ -94,6 +94,29 @@ template <class T> __global__ void fma_probe_kernel(long long iters, T *sink) {
   sink[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Random-gather throughput probe: every thread draws segment indices with a
+// xorshift generator and loads whole 32-byte spline records (u and w of a
+// pair kind at a segment) from the FP32 radial tables, the access pattern of
+// the evaluation kernels' quadrature points.
+__global__ void gather_probe_kernel(const float *rec, int n_rec, long long iters, float *sink) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned st = 0x9E3779B9u * (unsigned)(tid + 1);
+  float acc = 0.f;
+  for (long long it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      st ^= st << 13;
+      st ^= st >> 17;
+      st ^= st << 5;
+      const int m = (int)(((unsigned long long)st * (unsigned)n_rec) >> 32);
+      float v[8];
+      ld8(rec + 8 * (size_t)m, v);
+      acc += v[0] + v[7];
+    }
+  }
+  sink[tid] = acc;
+}
+
 __global__ void spline_eval_kernel(SplineView<double> s, int n, const double *r, double *v,
                                    double *dv) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -953,6 +976,43 @@ int btam_probe_fma_peak(int fp64, double seconds, double *tflops) {
   cudaFree(sink);
   if (e != cudaSuccess) return cuda_status(e);
   *tflops = best;
+  return BTAM_OK;
+}
+
+int btam_probe_gather_peak(const btam_tables *t, double seconds, double *gbs) {
+  if (!t || !gbs || !(seconds > 0.0)) return BTAM_ERR_ARG;
+  int dev = 0, sms = 0;
+  BTAM_TRY(cudaGetDevice(&dev));
+  BTAM_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int threads = 256, blocks = sms * 8;
+  const int n_rec = 3 * t->r32.n;  // the u, w records of the three pair kinds
+  float *sink = nullptr;
+  BTAM_TRY(cudaMalloc(&sink, (size_t)blocks * threads * sizeof(float)));
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  long long iters = 1 << 8;
+  double best = 0.0;
+  cudaError_t e = cudaSuccess;
+  for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+    cudaEventRecord(a);
+    gather_probe_kernel<<<blocks, threads>>>(t->r32.uw, n_rec, iters, sink);
+    cudaEventRecord(b);
+    e = cudaEventSynchronize(b);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    const double bytes = 32.0 * 4.0 * (double)iters * blocks * threads;
+    if (ms > 0) best = bytes / (ms * 1e-3) / 1e9;
+    if (ms > 0 && rep < 3) {
+      double scale = seconds * 1e3 / ms;
+      if (scale > 1.0) iters = (long long)(iters * (scale > 1e4 ? 1e4 : scale));
+    }
+  }
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_status(e);
+  *gbs = best;
   return BTAM_OK;
 }
 

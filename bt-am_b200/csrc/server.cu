@@ -89,11 +89,14 @@ void run_job(btam_server *srv, Job *job) {
                               job->gamma.empty() ? nullptr : job->gamma.data(), job->origin,
                               job->cell, job->periodic, &s);
   if (st == BTAM_OK) st = btam_neighbors_build(s, 0);
-  // every job runs the undirected kernels (each neighbour pair evaluated once
-  // for both directions) on persistent grids, in both arithmetic forms; their
-  // pair buffers are part of btam_estimate_bytes
-  if (st == BTAM_OK) st = btam_set_variants(s, BTAM_FP32C, kServeVariant1[1], kServeVariant2[1]);
-  if (st == BTAM_OK) st = btam_set_variants(s, BTAM_FP64, kServeVariant1[0], kServeVariant2[0]);
+  // jobs run the undirected kernels (each neighbour pair evaluated once for
+  // both directions) on persistent grids, in both arithmetic forms, unless
+  // they ask for the plain two-pass pair; the pair buffers are part of
+  // btam_estimate_bytes
+  if (st == BTAM_OK && !sp.plain)
+    st = btam_set_variants(s, BTAM_FP32C, kServeVariant1[1], kServeVariant2[1]);
+  if (st == BTAM_OK && !sp.plain)
+    st = btam_set_variants(s, BTAM_FP64, kServeVariant1[0], kServeVariant2[0]);
   if (st == BTAM_OK) {
     r.t_start = since(srv->t0);
     if (sp.kind == BTAM_JOB_RELAX) {

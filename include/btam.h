@@ -322,6 +322,8 @@ typedef struct btam_job_spec {
   double sigma_min, sigma_max, x_min;  /* relaxation bounds (0: defaults) */
   int nsteps;                   /* master-equation steps */
   double dmd_params[5];         /* dt, Df, dr, min_dx, max_x */
+  int plain;  /* 0: the server's kernels (undirected, persistent); nonzero:
+                 the plain two-pass kernel pair (launch variants (0, 0)) */
 } btam_job_spec;
 
 typedef struct btam_job_result {
@@ -363,6 +365,11 @@ int btam_mf_eval_profile(btam_system *s, int precision, double ms[5]);
  * for fp64 = 0 (FP32) or 1 (FP64), from a register-resident FMA loop over
  * every SM lasting about `seconds`. */
 int btam_probe_fma_peak(int fp64, double seconds, double *tflops);
+/* Device-wide throughput (GB/s) of random 32-byte record gathers from the
+ * FP32 radial tables (L1-resident), the access pattern of the evaluation
+ * kernels' quadrature points; one launch timed after calibration to about
+ * `seconds`. */
+int btam_probe_gather_peak(const btam_tables *t, double seconds, double *gbs);
 
 #ifdef __cplusplus
 }
