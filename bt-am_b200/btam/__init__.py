@@ -66,6 +66,10 @@ _PROTOS = {
     "btam_results_copy": (ctypes.c_int, [_V, _D, _D, _D, _D, _D, _D, _D]),
     "btam_system_sync": (ctypes.c_int, [_V]),
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
+    "btam_pt_eval": (ctypes.c_int, [_V, _D, _D, _D, _D, _D]),
+    "btam_stretch_apply": (ctypes.c_int, [_V, _D]),
+    "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                          _D, _D]),
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
     "btam_probe_gather_peak": (ctypes.c_int, [_V, ctypes.c_double, _D]),
@@ -386,6 +390,34 @@ class System:
         out = np.zeros(self.n)
         _check(lib().btam_rho_nmf(self.handle, _d(out)), "btam_rho_nmf")
         return out
+
+    # -- non-mean-field forms and the bulk stretch relaxation
+    def pt_eval(self):
+        """Non-mean-field forms at the current q and x: dict of rho (n), V (n),
+        Fq (n, 3) = sum_{i in {u} U N(u)} dV_i/dq_u, W (n, 3, 3) = dV_u/dF at
+        q0 = q, totals (12): sum V, sum |Fq|^2, sum W (9), 0."""
+        n = self.n
+        out = dict(rho=np.zeros(n), V=np.zeros(n), Fq=np.zeros((n, 3)), W=np.zeros((n, 3, 3)),
+                   totals=np.zeros(12))
+        _check(lib().btam_pt_eval(self.handle, _d(out["rho"]), _d(out["V"]), _d(out["Fq"]),
+                                  _d(out["W"]), _d(out["totals"])), "btam_pt_eval")
+        return out
+
+    def stretch(self, F):
+        """q <- diag(F) q, cell and origin likewise; neighbour lists kept."""
+        F = np.ascontiguousarray(F, np.float64)
+        _check(lib().btam_stretch_apply(self.handle, _d(F)), "btam_stretch_apply")
+
+    def relax_stretch(self, atol=1e-12, rtol=1e-10, max_iter=20, F0=(1.0, 1.0, 1.0)):
+        """Bulk stretch relaxation (diagonal F zeroing the mean stress of the
+        non-mean-field forms); leaves the system stretched.  Returns (F, info
+        dict: norm, iterations, evaluations, status, volume)."""
+        F = np.ascontiguousarray(F0, np.float64).copy()
+        info = np.zeros(5)
+        _check(lib().btam_relax_stretch(self.handle, atol, rtol, max_iter, _d(F), _d(info)),
+               "btam_relax_stretch")
+        return F, dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
+                       status=int(info[3]), volume=info[4])
 
     def close(self):
         if getattr(self, "handle", None):

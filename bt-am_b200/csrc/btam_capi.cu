@@ -337,6 +337,10 @@ double tables_mass(const btam_tables *t, int code) {
 }
 }  // namespace btam
 
+int make_box_for(const double *origin, const double *cell, const int *periodic, GhostBox &b) {
+  return make_box(origin, cell, periodic, BTAM_R_CUTOFF, b);
+}
+
 extern "C" {
 
 const char *btam_status_string(int st) {
@@ -553,6 +557,7 @@ void btam_system_destroy(btam_system *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
   dfree(s->pos, s->st); dfree(s->xb, s->st); dfree(s->code, s->st); dfree(s->owner, s->st); dfree(s->image, s->st);
+  dfree(s->pt, s->st);
   dfree(s->s32, s->st); dfree(s->sb, s->st);
   dfree(s->gamma, s->st); dfree(s->stage, s->st); dfree(s->offs, s->st); dfree(s->idx, s->st); dfree(s->cnt, s->st);
   dfree(s->tmp, s->st); dfree(s->bbox, s->st); dfree(s->grid, s->st); dfree(s->cell_of, s->st); dfree(s->cell_cnt, s->st);

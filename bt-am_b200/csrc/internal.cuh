@@ -86,7 +86,14 @@ struct btam_system {
   int own_off_cap = 0, n_own = 0;
   char *pbuf = nullptr;
   size_t pbuf_bytes = 0, pbuf_elem = 0;  // bytes; bytes per value (0: none yet)
+  // non-mean-field forms: site records, outputs and totals (point.cu)
+  double *pt = nullptr;
+  size_t pt_cap = 0;
 };
+
+// Box of a cell (rows = lattice vectors) and origin at the potential's
+// cutoff, with the checks of btam_system_create (btam_capi.cu).
+int make_box_for(const double *origin, const double *cell, const int *periodic, GhostBox &b);
 
 
 // ---- host helpers shared by the library sources

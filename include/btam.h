@@ -179,6 +179,48 @@ int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);
 
+/* ---- non-mean-field forms (sigma -> 0: every term at the mean positions) --
+ * One device evaluation over the system's neighbour lists (kept as built):
+ *   rho (n): rho_i = sum_j x_j rho_{s_j}(|q_j - q_i|), as btam_rho_nmf
+ *            (evaluate_rho_i_adp_MgHx, MgHx-mf-V-bulk.cpp:83-143);
+ *   V (n):   the point energy x_i F(rho_i) + sum_j 1/2 x_i x_j phi + the
+ *            dipole and quadrupole sums over j1 <= j2 (no reference function
+ *            returns it; 0 for x_i < min_occupancy);
+ *   Fq (3n): sum_{i in {u} U N(u)} dV_i/dq_u per real site u, the assembled
+ *            evaluate_DV_i_Dq_u_adp_MgHx (147-330);
+ *   W (9n):  dV_u/dF per real site, row-major (row: gradient component,
+ *            column: position component), at reference positions q0 = q
+ *            (evaluate_DV_i_dF_MgHx, 530-704).  At reference positions
+ *            q0 = diag(F)^-1 q it is W(a, b) / F_b;
+ *   totals (12): sum V, sum |Fq|^2, sum of W over the sites (9), 0.
+ * Any output may be NULL.  sigma is not read. */
+int btam_pt_eval(btam_system *s, double *rho, double *V, double *Fq, double *W,
+                 double *totals);
+/* Stretches the system by diag(F) (F[a] > 0): q <- F q for every site, the
+ * cell rows and the origin likewise; images follow; neighbour lists are
+ * kept.  BTAM_ERR_BOX_TOO_SMALL (nothing changed) if a periodic cell would
+ * become narrower than 2 rc. */
+int btam_stretch_apply(btam_system *s, const double F[3]);
+/* Bulk stretch relaxation: replaces mechanical_relaxation_bulk
+ * (Mechanical-Relaxation-bulk.cpp:123-437), the reference's one compiled
+ * solver.  Finds the diagonal stretch F with
+ *   Y_a(F) = (1/V0) sum_u dV_u/dF(a, a) = 0,  q = diag(F) q_ref,
+ * V0 = |det cell| at entry, dV_u/dF of the non-mean-field forms at fixed x
+ * and fixed neighbour lists (evaluate_RHS, 441-600).  Newton's method with
+ * the Jacobian by forward differences (three extra residuals per
+ * iteration, as the reference's MatFDColoring of the dense 3x3 pattern) and
+ * a backtracking line search on |Y|^2; converged when |Y| <= atol or
+ * |Y| <= rtol |Y(F_start)| (the reference: 1e-12, 1e-10, at most 20
+ * iterations).  F (3): the start on entry (the reference starts at 1), the
+ * solution on return, and the system is left stretched by it (cell and
+ * origin too, 366-384).  info (5, may be NULL): final |Y|, iterations,
+ * residual evaluations, status (1 converged, 0 iteration limit, -1 no
+ * descent), V0.  The reference's options select PETSc's NGMRES with a
+ * critical-point line search (main-BT-AM.cpp:64-67); PETSc is not used
+ * here, and any solver that converges finds the same F. */
+int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, double F[3],
+                       double *info);
+
 /* ---- consumers of the evaluation -----------------------------------------
  * Relaxation of (q, sigma).  The reference configures a PETSc SNES
  * (mechanical_relaxation_bulk, Mechanical-Relaxation-bulk.cpp:123-437; options

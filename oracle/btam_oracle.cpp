@@ -619,6 +619,111 @@ double DV0_dx(const View &v, int u, int i) {
   return emb + pair + dip + quad;
 }
 
+// ---------------------------------------------------------------------------
+// Non-mean-field forms: the ADP terms at the mean positions (sigma -> 0).
+
+// evaluate_DV_i_Dq_u_adp_MgHx (MgHx-mf-V-bulk.cpp:147-330): dV_i/dq_u.  The
+// reference tests u's membership per term after building it; the test is
+// made first here (the value is the same).
+void DV_dq(const View &v, int u, int i, double *out3) {
+  for (int a = 0; a < 3; ++a) out3[a] = 0.0;
+  if (v.spc[u] == kH && v.x[u] < kMinOcc) return;  // 161-165
+  if (v.spc[i] == kH && v.x[i] < kMinOcc) return;  // 185-188
+  double drho[3] = {0, 0, 0}, pair[3] = {0, 0, 0}, dip[3] = {0, 0, 0}, quad[3] = {0, 0, 0};
+  const int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    const int j1 = v.idx[k1];
+    if (v.spc[j1] == kH && v.x[j1] < kMinOcc) continue;  // 200-202
+    double qq[6], nn[2] = {v.x[i], v.x[j1]};
+    int sp[2] = {v.spc[i], v.spc[j1]}, sites2[2] = {i, j1};
+    for (int a = 0; a < 3; ++a) {
+      qq[a] = v.q[3 * i + a];
+      qq[3 + a] = v.q[3 * j1 + a];
+    }
+    for (int dir = 0; dir < 2; ++dir) {
+      if (sites2[dir] != u) continue;
+      double g[3];
+      rho_dq(dir, g, nn, qq, sp);
+      for (int a = 0; a < 3; ++a) drho[a] += g[a];
+      pair_dq(dir, g, nn, qq, sp);
+      for (int a = 0; a < 3; ++a) pair[a] += g[a];
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      const int j2 = v.idx[k2];
+      if (v.spc[j2] == kH && v.x[j2] < kMinOcc) continue;  // 252-254
+      int sites3[3] = {i, j1, j2};
+      if (sites3[0] != u && sites3[1] != u && sites3[2] != u) continue;
+      double q3[9], n3[3] = {v.x[i], v.x[j1], v.x[j2]};
+      int sp3[3] = {v.spc[i], v.spc[j1], v.spc[j2]};
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) q3[3 * k + a] = v.q[3 * sites3[k] + a];
+      const double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        if (sites3[dir] != u) continue;
+        double g[3];
+        dip_dq(dir, g, n3, q3, sp3);
+        for (int a = 0; a < 3; ++a) dip[a] += f * g[a];
+        quad_dq(dir, g, n3, q3, sp3);
+        for (int a = 0; a < 3; ++a) quad[a] += f * g[a];
+      }
+    }
+  }
+  const double dF = spline_d1(embed_of(v.spc[i]), v.rho[i]);  // 308-315
+  for (int a = 0; a < 3; ++a) out3[a] = v.x[i] * dF * drho[a] + pair[a] + dip[a] + quad[a];
+}
+
+// evaluate_DV_i_dF_MgHx (MgHx-mf-V-bulk.cpp:530-704): sum over the sites a
+// of every term of V_i of dV_i/dq_a (x) q0_a, 3x3 row-major (row: gradient
+// component, column: reference-position component).
+void DV_dF(const View &v, const double *q0, int i, double *out9) {
+  for (int c = 0; c < 9; ++c) out9[c] = 0.0;
+  if (v.x[i] < kMinOcc) return;  // 546-549
+  double drho[9] = {0}, pair[9] = {0}, dip[9] = {0}, quad[9] = {0};
+  const int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    const int j1 = v.idx[k1];
+    if (v.spc[j1] == kH && v.x[j1] < kMinOcc) continue;  // 574-576
+    double qq[6], nn[2] = {v.x[i], v.x[j1]};
+    int sp[2] = {v.spc[i], v.spc[j1]}, sites2[2] = {i, j1};
+    for (int a = 0; a < 3; ++a) {
+      qq[a] = v.q[3 * i + a];
+      qq[3 + a] = v.q[3 * j1 + a];
+    }
+    for (int dir = 0; dir < 2; ++dir) {
+      const double *r0 = q0 + 3 * sites2[dir];
+      double g[3];
+      rho_dq(dir, g, nn, qq, sp);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) drho[3 * a + b] += g[a] * r0[b];
+      pair_dq(dir, g, nn, qq, sp);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) pair[3 * a + b] += g[a] * r0[b];
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      const int j2 = v.idx[k2];
+      if (v.spc[j2] == kH && v.x[j2] < kMinOcc) continue;  // 633-635
+      int sites3[3] = {i, j1, j2};
+      double q3[9], n3[3] = {v.x[i], v.x[j1], v.x[j2]};
+      int sp3[3] = {v.spc[i], v.spc[j1], v.spc[j2]};
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) q3[3 * k + a] = v.q[3 * sites3[k] + a];
+      const double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        const double *r0 = q0 + 3 * sites3[dir];
+        double g[3];
+        dip_dq(dir, g, n3, q3, sp3);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) dip[3 * a + b] += f * g[a] * r0[b];
+        quad_dq(dir, g, n3, q3, sp3);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) quad[3 * a + b] += f * g[a] * r0[b];
+      }
+    }
+  }
+  const double dF = spline_d1(embed_of(v.spc[i]), v.rho[i]);  // 688-695
+  for (int c = 0; c < 9; ++c) out9[c] = v.x[i] * dF * drho[c] + pair[c] + dip[c] + quad[c];
+}
+
 // evaluate_S0_i_adp_MgHx (957-1142)
 double S0_i(const View &v, int i, double beta, double gamma) {
   double xi = v.x[i];
@@ -882,6 +987,22 @@ void orc_rho_nmf(int n, const double *q, const double *x, const int *spc,
     }
     out[k] = acc;
   });
+}
+
+void orc_pt_DV_pairs(int n, const double *q, const double *x, const int *spc,
+                     const double *rho, const int *offs, const int *idx, const int *u_list,
+                     const int *i_list, int npairs, double *out3) {
+  (void)n;
+  View v{q, nullptr, x, rho, spc, offs, idx};
+  par_for(npairs, [&](int k) { DV_dq(v, u_list[k], i_list[k], out3 + 3 * k); });
+}
+
+void orc_pt_DV_dF(int n, const double *q, const double *q0, const double *x, const int *spc,
+                  const double *rho, const int *offs, const int *idx, const int *sites,
+                  int nsites, double *out9) {
+  (void)n;
+  View v{q, nullptr, x, rho, spc, offs, idx};
+  par_for(nsites, [&](int k) { DV_dF(v, q0, sites[k], out9 + 9 * k); });
 }
 
 void orc_residuals(int n, const double *q, const double *sigma,

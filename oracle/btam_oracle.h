@@ -67,6 +67,19 @@ void orc_rho_nmf(int n, const double *q, const double *x, const int *spc,
                  const int *offs, const int *idx, const int *sites, int nsites,
                  double *out);
 
+/* Non-mean-field forms (sigma -> 0), restated from MgHx-mf-V-bulk.cpp:
+ * orc_pt_DV_pairs: dV_i/dq_u per (u, i) pair, 3 values
+ *   (evaluate_DV_i_Dq_u_adp_MgHx, 147-330);
+ * orc_pt_DV_dF: dV_i/dF per site, 9 values row-major, with reference
+ *   positions q0 of every site (evaluate_DV_i_dF_MgHx, 530-704).
+ * rho: the non-mean-field density of every site (orc_rho_nmf). */
+void orc_pt_DV_pairs(int n, const double *q, const double *x, const int *spc,
+                     const double *rho, const int *offs, const int *idx, const int *u_list,
+                     const int *i_list, int npairs, double *out3);
+void orc_pt_DV_dF(int n, const double *q, const double *q0, const double *x, const int *spc,
+                  const double *rho, const int *offs, const int *idx, const int *sites,
+                  int nsites, double *out9);
+
 /* Residual assembly for real sites u (project definition):
  *   R_q(u)     = sum_{i in {u} U N(u)} (beta_i/beta_u) dV0_i/dq_u
  *   R_sigma(u) = sum_i (beta_i/beta_u) dV0_i/dsigma_u - 3/(beta_u sigma_u)

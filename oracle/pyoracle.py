@@ -117,6 +117,26 @@ class Lib:
         return out
 
 
+    # --- non-mean-field forms (sigma -> 0) ---------------------------------
+    def pt_DV_pairs(self, s, rho, offs, idx, u_list, i_list):
+        """dV_i/dq_u per (u, i) pair (evaluate_DV_i_Dq_u_adp_MgHx)."""
+        u_list = np.ascontiguousarray(u_list, np.int32)
+        i_list = np.ascontiguousarray(i_list, np.int32)
+        out = np.zeros((len(u_list), 3))
+        self._f("pt_DV_pairs")(len(s["x"]), _d(s["q"]), _d(s["x"]), _i(s["species"]), _d(rho),
+                               _i(offs), _i(idx), _i(u_list), _i(i_list), len(u_list), _d(out))
+        return out
+
+    def pt_DV_dF(self, s, q0, rho, offs, idx, sites):
+        """dV_i/dF per site, 3x3 (evaluate_DV_i_dF_MgHx), reference positions q0."""
+        sites = np.ascontiguousarray(sites, np.int32)
+        q0 = np.ascontiguousarray(q0, np.float64)
+        out = np.zeros((len(sites), 3, 3))
+        self._f("pt_DV_dF")(len(s["x"]), _d(s["q"]), _d(q0), _d(s["x"]), _i(s["species"]),
+                            _d(rho), _i(offs), _i(idx), _i(sites), len(sites), _d(out))
+        return out
+
+
 class Oracle(Lib):
     """The restated oracle plus its project-defined pieces."""
 

@@ -285,4 +285,41 @@ void ref_rho_nmf(int n, const double *q, const double *x, const int *spc,
   free(s.spc);
 }
 
+// evaluate_DV_i_Dq_u_adp_MgHx (MgHx-mf-V-bulk.cpp:147-330): the
+// non-mean-field gradient dV_i/dq_u, 3 values per (u, i) pair; rho is the
+// non-mean-field density of every site.
+void ref_pt_DV_pairs(int n, const double *q, const double *x, const int *spc,
+                     const double *rho, const int *offs, const int *idx, const int *u_list,
+                     const int *i_list, int npairs, double *out3) {
+  Sys s;
+  make_sys(s, n, q, nullptr, x, spc, offs, idx);
+  for (int i = 0; i < n; ++i) s.rho(i) = rho[i];
+  parallel_for(npairs, [&](int k) {
+    int u = u_list[k], i = i_list[k];
+    Eigen::Vector3d g = evaluate_DV_i_Dq_u_adp_MgHx(u, i, s.q, s.x, s.rho, s.spc, topo(s, i));
+    for (int c = 0; c < 3; ++c) out3[3 * k + c] = g(c);
+  });
+  free(s.spc);
+}
+
+// evaluate_DV_i_dF_MgHx (MgHx-mf-V-bulk.cpp:530-704): 9 values per site,
+// row-major, with reference positions q0 of every site.
+void ref_pt_DV_dF(int n, const double *q, const double *q0, const double *x, const int *spc,
+                  const double *rho, const int *offs, const int *idx, const int *sites,
+                  int nsites, double *out9) {
+  Sys s;
+  make_sys(s, n, q, nullptr, x, spc, offs, idx);
+  for (int i = 0; i < n; ++i) s.rho(i) = rho[i];
+  Eigen::MatrixXd Q0(n, 3);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) Q0(i, k) = q0[3 * i + k];
+  parallel_for(nsites, [&](int k) {
+    int i = sites[k];
+    Eigen::Matrix3d g = evaluate_DV_i_dF_MgHx(i, s.q, Q0, s.x, s.rho, s.spc, topo(s, i));
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) out9[9 * k + 3 * a + b] = g(a, b);
+  });
+  free(s.spc);
+}
+
 } // extern "C"

@@ -10,7 +10,9 @@ DMSwarm, which is not available; the residual assembly is the project's
 definition (include/btam.h) applied to the reference's per-pair values.
 
 Run from the repository root, with the reference tree present:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py            # every fixture
+    python tests/golden/make_golden.py --point    # point.npz only (it reads
+                                                  # the system fixtures)
 """
 import os
 import sys
@@ -106,8 +108,50 @@ def system_fixture(name, s, ref, orc, residual_sample=None, seed=0):
           f"{len(us)} residual sites -> {os.path.getsize(path)} bytes")
 
 
+# Stretch of the non-mean-field fixtures: q <- diag(F) q on every site.
+PT_STRETCH = np.array([1.01, 0.99, 1.02])
+
+
+def point_fixture(ref):
+    """Non-mean-field forms (sigma -> 0) on the committed systems, from the
+    reference's own evaluate_rho_i / evaluate_DV_i_Dq_u_adp_MgHx /
+    evaluate_DV_i_dF_MgHx, on the neighbour lists stored in each fixture:
+    the assembled gradient sum_{i in {u} U N(u)} dV_i/dq_u of every real
+    site, dV_i/dF with q0 = q, and dV_i/dF after the stretch PT_STRETCH
+    (q0 = the unstretched positions, neighbour lists kept)."""
+    out = {"stretch": PT_STRETCH}
+    for name in ("sphere", "ortho_mgh", "x5cube", "config1"):
+        g = np.load(os.path.join(OUT, f"{name}.npz"))
+        n = len(g["x"])
+        owner, image, offs, idx = g["owner"], g["image"], g["offs"], g["idx"]
+        full = {"q": np.ascontiguousarray(g["q_all"]),
+                "x": np.ascontiguousarray(g["x"][owner]),
+                "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+        real = np.arange(n, dtype=np.int32)
+        rho = ref.rho_nmf(full, offs, idx, real)
+        plan = residual_pairs(full, owner, image, offs, idx, real)
+        kk = np.array([p[0] for p in plan])
+        g3 = ref.pt_DV_pairs(full, rho[owner], offs, idx,
+                             np.array([p[1] for p in plan], np.int32),
+                             np.array([p[2] for p in plan], np.int32))
+        Fq = np.zeros((n, 3))
+        np.add.at(Fq, kk, g3)
+        W = ref.pt_DV_dF(full, full["q"], rho[owner], offs, idx, real)
+        st = dict(full)
+        st["q"] = np.ascontiguousarray(full["q"] * PT_STRETCH)
+        rho_s = ref.rho_nmf(st, offs, idx, real)
+        W_s = ref.pt_DV_dF(st, full["q"], rho_s[owner], offs, idx, real)
+        out.update({f"{name}_rho": rho, f"{name}_Fq": Fq, f"{name}_W": W,
+                    f"{name}_rho_s": rho_s, f"{name}_W_s": W_s})
+        print(f"point forms {name}: {n} sites, {len(plan)} gradient pairs")
+    np.savez_compressed(os.path.join(OUT, "point.npz"), **out)
+
+
 def main():
     ref = pyoracle.reference()
+    if ref is not None and sys.argv[1:] == ["--point"]:
+        point_fixture(ref)
+        return
     if ref is None:
         sys.exit("oracle/_ref/libbtam_ref.so missing: run `make -C oracle ref` first")
     orc = pyoracle.Oracle()
@@ -160,6 +204,7 @@ def main():
                               sigma_range=(0.08, 0.15), jitter=0.02, seed=5)
     system_fixture("ortho_mgh", ortho, ref, orc)
     system_fixture("config1", lattice.config1(), ref, orc, residual_sample=40, seed=1)
+    point_fixture(ref)
 
 
 if __name__ == "__main__":

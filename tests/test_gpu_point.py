@@ -1,0 +1,150 @@
+"""Non-mean-field forms and the bulk stretch relaxation on the device, against
+the reference's values (tests/golden/point.npz, from evaluate_rho_i_adp_MgHx,
+evaluate_DV_i_Dq_u_adp_MgHx and evaluate_DV_i_dF_MgHx compiled unmodified)
+and against finite differences of the device's own point energy.
+
+Tolerances: rho 1e-12 relative; Fq and W 1e-10 of max(1, the largest
+component) (the forces of a near-perfect lattice are sums of O(1) terms
+that cancel to 1e-5; the reference sums dV/dq_a q0_a over absolute
+positions, the device over q_j - q_u); finite differences 1e-6 relative."""
+import os
+
+import numpy as np
+import pytest
+
+import btam
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+NAMES = ["sphere", "x5cube", "ortho_mgh", "config1"]
+KEYS = ("q", "sigma", "x", "species", "beta", "gamma", "origin", "cell", "periodic")
+
+
+def load(name):
+    return dict(np.load(os.path.join(GOLD, f"{name}.npz")))
+
+
+def system_of(g):
+    return {k: g[k] for k in KEYS}
+
+
+def rel(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+
+
+def err1(a, b):
+    return np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1.0)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_point_forms_against_reference(gpu_tables, name):
+    g, p = load(name), load("point")
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    out = S.pt_eval()
+    assert rel(out["rho"], p[f"{name}_rho"]) < 1e-12
+    assert np.array_equal(out["rho"], S.rho_nmf())
+    assert err1(out["Fq"], p[f"{name}_Fq"]) < 1e-10
+    assert err1(out["W"], p[f"{name}_W"]) < 1e-10
+    t = out["totals"]
+    assert abs(t[0] - out["V"].sum()) <= 1e-12 * np.abs(out["V"]).sum()
+    assert np.allclose(t[2:11], out["W"].sum(0).ravel(), rtol=1e-12, atol=1e-12)
+    # stretched: the reference's dV/dF at the unstretched q0 is W(a, b) / F_b
+    F = p["stretch"]
+    S.stretch(F)
+    out = S.pt_eval()
+    assert rel(out["rho"], p[f"{name}_rho_s"]) < 1e-12
+    assert err1(out["W"] / F[None, None, :], p[f"{name}_W_s"]) < 1e-10
+
+
+def test_point_gradient_is_energy_derivative(gpu_tables):
+    """Fq_u = d(sum_i V_i)/dq_u with the images following (central
+    differences of the device's point energy, periodic MgH system)."""
+    g = load("ortho_mgh")
+    s = system_of(g)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    Fq = S.pt_eval()["Fq"]
+    rng = np.random.default_rng(3)
+    active = np.flatnonzero(s["x"] >= 5e-4)
+    h = 1e-5
+    for u in rng.choice(active, 6, replace=False):
+        for a in range(3):
+            E = []
+            for sgn in (1.0, -1.0):
+                q = s["q"].copy()
+                q[u, a] += sgn * h
+                S.set_state(q=q)
+                E.append(S.pt_eval()["totals"][0])
+            fd = (E[0] - E[1]) / (2 * h)
+            assert abs(fd - Fq[u, a]) <= 1e-6 * max(1.0, abs(Fq[u, a])), (u, a, fd, Fq[u, a])
+    S.set_state(q=s["q"])
+
+
+def test_stress_is_energy_derivative(gpu_tables):
+    """sum_u W_u(a, a) = d(sum_i V_i)/dF_aa at F = 1 (central differences of
+    the point energy under the stretch)."""
+    g = load("x5cube")
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    W = S.pt_eval()["totals"][2:11].reshape(3, 3)
+    h = 1e-6
+    for a in range(3):
+        up = np.ones(3)
+        up[a] = 1.0 + h
+        S.stretch(up)
+        Ep = S.pt_eval()["totals"][0]
+        dn = np.ones(3)
+        dn[a] = (1.0 - h) / (1.0 + h)
+        S.stretch(dn)
+        Em = S.pt_eval()["totals"][0]
+        back = np.ones(3)
+        back[a] = 1.0 / (1.0 - h)
+        S.stretch(back)
+        fd = (Ep - Em) / (2 * h)
+        assert abs(fd - W[a, a]) <= 1e-6 * max(1.0, abs(W[a, a])), (a, fd, W[a, a])
+
+
+@pytest.mark.parametrize("name", ["x5cube", "ortho_mgh"])
+def test_relax_stretch_zeroes_reference_stress(gpu_tables, oracle, name):
+    """The bulk stretch relaxation converges (|Y| <= 1e-12) and the F it
+    finds zeroes the stress of the restated reference functions: the
+    oracle's evaluate_rho_i / evaluate_DV_i_dF_MgHx at q = diag(F) q0 on the
+    fixture's images and neighbour lists."""
+    g = load(name)
+    s = system_of(g)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    F, info = S.relax_stretch(atol=1e-12, rtol=1e-10, max_iter=20)
+    assert info["status"] == 1 and info["norm"] <= 1e-12, info
+    assert np.all(np.abs(F - 1.0) < 0.1)
+    vol = abs(np.linalg.det(s["cell"].reshape(3, 3)))
+    assert abs(info["volume"] - vol) <= 1e-12 * vol
+    q, _, _ = S.get_state()
+    assert np.array_equal(q, s["q"] * F)
+    # the oracle's residual at the solution
+    n = len(g["x"])
+    owner = g["owner"]
+    full = {"q": np.ascontiguousarray(g["q_all"] * F), "x": np.ascontiguousarray(g["x"][owner]),
+            "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+    real = np.arange(n, dtype=np.int32)
+    rho = oracle.rho_nmf(full, g["offs"], g["idx"], real)
+    W = oracle.pt_DV_dF(full, g["q_all"], rho[owner], g["offs"], g["idx"], real)
+    Y = np.array([W[:, a, a].sum() for a in range(3)]) / vol
+    assert np.max(np.abs(Y)) <= 1e-9, Y
+    # the device agrees at the relaxed state
+    out = S.pt_eval()
+    Yd = np.array([out["W"][:, a, a].sum() / F[a] for a in range(3)]) / vol
+    assert np.max(np.abs(Yd)) <= 1e-11
+
+
+def test_relax_stretch_rejections(gpu_tables):
+    g = load("sphere")
+    S = btam.System(gpu_tables, system_of(g))
+    with pytest.raises(btam.BtamError):
+        S.relax_stretch()  # neighbour lists not built
+    S.build_neighbors()
+    with pytest.raises(btam.BtamError):
+        S.relax_stretch(F0=(1.0, -1.0, 1.0))
+    with pytest.raises(btam.BtamError):
+        S.stretch((1.0, 0.0, 1.0))

@@ -112,3 +112,54 @@ def test_occupancy_threshold_quirks(oracle, ref):
     a4, ax = oracle.DV0_pairs(s, rho, offs, idx, [0, 2, 1], [0, 0, 0])
     b4, bx = ref.DV0_pairs(s, rho, offs, idx, [0, 2, 1], [0, 0, 0])
     assert np.array_equal(a4, b4) and np.array_equal(ax, bx)
+
+
+@pytest.mark.parametrize("name", ["sphere", "x5cube", "ortho_mgh", "config1"])
+def test_point_forms_against_golden(oracle, name):
+    """Non-mean-field forms (evaluate_DV_i_Dq_u_adp_MgHx, evaluate_DV_i_dF_MgHx)
+    of the restated oracle against the reference's values in point.npz."""
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import residual_pairs
+    g, p = load(name), load("point")
+    n = len(g["x"])
+    owner, image, offs, idx = g["owner"], g["image"], g["offs"], g["idx"]
+    full = {"q": g["q_all"], "x": np.ascontiguousarray(g["x"][owner]),
+            "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+    real = np.arange(n, dtype=np.int32)
+    rho = oracle.rho_nmf(full, offs, idx, real)
+    assert np.array_equal(rho, p[f"{name}_rho"])
+    plan = residual_pairs(full, owner, image, offs, idx, real)
+    g3 = oracle.pt_DV_pairs(full, rho[owner], offs, idx, [q[1] for q in plan],
+                            [q[2] for q in plan])
+    Fq = np.zeros((n, 3))
+    np.add.at(Fq, np.array([q[0] for q in plan]), g3)
+    assert np.array_equal(Fq, p[f"{name}_Fq"])
+    W = oracle.pt_DV_dF(full, full["q"], rho[owner], offs, idx, real)
+    assert np.array_equal(W, p[f"{name}_W"])
+    st = dict(full, q=np.ascontiguousarray(full["q"] * p["stretch"]))
+    rho_s = oracle.rho_nmf(st, offs, idx, real)
+    assert np.array_equal(rho_s, p[f"{name}_rho_s"])
+    assert np.array_equal(oracle.pt_DV_dF(st, full["q"], rho_s[owner], offs, idx, real),
+                          p[f"{name}_W_s"])
+
+
+def test_point_forms_match_reference_live(oracle, ref):
+    from btam import lattice
+    import pyoracle
+    s = lattice.cluster("sphere", 7.0, x_fn=lambda g, r, n: g.uniform(0.0, 0.7, n),
+                        h_fraction=0.6, seed=12)
+    full, n, owner, image = pyoracle.expand(s, oracle)
+    offs, idx = oracle.neighbors(full["q"])
+    real = np.arange(n, dtype=np.int32)
+    rho = ref.rho_nmf(full, offs, idx, real)
+    us, is_ = [], []
+    for u in range(0, n, 5):
+        for i in [u, *idx[offs[u]:offs[u + 1]]]:
+            us.append(u)
+            is_.append(i)
+    assert np.array_equal(oracle.pt_DV_pairs(full, rho, offs, idx, us, is_),
+                          ref.pt_DV_pairs(full, rho, offs, idx, us, is_))
+    q0 = full["q"] + 0.01
+    assert np.array_equal(oracle.pt_DV_dF(full, q0, rho, offs, idx, real),
+                          ref.pt_DV_dF(full, q0, rho, offs, idx, real))
