@@ -37,10 +37,23 @@
  *    caller that sums over i, as every residual assembly does, gets the
  *    assembled value.  The occupancy derivative is defined for H sites
  *    (zero for Mg, as the device's R_x).
- *  - The non-mean-field gradient, the Hessians and the stretch derivatives
- *    (evaluate_DV_i_Dq_j, evaluate_D2V_i_Dq2_j, evaluate_DV_i_DF,
- *    evaluate_D2V0_i_Dmeanq2_j, evaluate_DV0_i_DF) are not provided: their
- *    slots are null. */
+ *  - The non-mean-field forms (evaluate_rho_i, evaluate_DV_i_Dq_j,
+ *    evaluate_DV_i_DF) come from one btam_pt_eval of the state; the
+ *    gradient is lumped like the mean-field derivatives (the whole
+ *    sum_{i in {u} U N(u)} dV_i/dq_u at site_i == site_i_star).  The
+ *    caller's `rho` argument is not read.
+ *  - Stretches: when the caller's mean_q is a diagonal stretch diag(F) of the
+ *    positions bound with bind() (to 1e-13 relative, every row), the system's
+ *    cell is stretched with it, so periodic images follow as the caller's
+ *    stretched ghost rows do (Mechanical-Relaxation-bulk.cpp:505-520);
+ *    any other mean_q is a new state in the current cell.
+ *    evaluate_DV_i_DF is defined for mean_q0 equal to the bound positions
+ *    (the reference's bulk residual passes its unstretched positions,
+ *    Mechanical-Relaxation-bulk.cpp:577-579); other mean_q0 give NaN and
+ *    last_status() BTAM_ERR_ARG.
+ *  - The Hessians and the mean-field stretch derivative
+ *    (evaluate_D2V_i_Dq2_j, evaluate_D2V0_i_Dmeanq2_j, evaluate_DV0_i_DF)
+ *    are not provided: their slots are null. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -57,11 +70,16 @@ struct Cache {
   btam_system *sys = nullptr;
   int precision = BTAM_FP64;
   int n = 0;
-  bool valid = false, nmf_valid = false;
-  int status = BTAM_OK;  // status of the last evaluation
+  bool have_state = false;  // q, sigma, x below are the system's state
+  bool valid = false;       // mean-field results of that state
+  bool pt_valid = false;    // non-mean-field results of that state
+  int status = BTAM_OK;     // status of the last evaluation
   std::vector<double> beta, gamma;
   std::vector<double> q, sigma, x;  // the evaluated state (q row-major)
-  std::vector<double> rho, V0, S0, Rq, Rs, Rx, rho_nmf;
+  std::vector<double> q_bind;       // positions at bind(): the stretch reference
+  double F[3] = {1.0, 1.0, 1.0};    // stretch of the system's cell against them
+  std::vector<double> rho, V0, S0, Rq, Rs, Rx;
+  std::vector<double> pt_rho, pt_Fq, pt_W;
 };
 
 inline Cache &cache() {
@@ -83,7 +101,8 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.sys = s;
   c.precision = precision;
   c.n = n_real;
-  c.valid = c.nmf_valid = false;
+  c.have_state = c.valid = c.pt_valid = false;
+  c.F[0] = c.F[1] = c.F[2] = 1.0;
   c.beta.assign(beta ? beta : nullptr, beta ? beta + n_real : nullptr);
   c.gamma.assign(gamma ? gamma : nullptr, gamma ? gamma + n_real : nullptr);
   if (!beta) c.beta.assign(n_real, 1.0 / (8.617332478e-5 * 300.0));  // k_B 300 K
@@ -97,8 +116,13 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.Rq.assign(3 * (size_t)n_real, 0.0);
   c.Rs.assign(n_real, 0.0);
   c.Rx.assign(n_real, 0.0);
-  c.rho_nmf.assign(n_real, 0.0);
-  return btam_system_get_state(s, c.q.data(), c.sigma.data(), c.x.data());
+  c.pt_rho.assign(n_real, 0.0);
+  c.pt_Fq.assign(3 * (size_t)n_real, 0.0);
+  c.pt_W.assign(9 * (size_t)n_real, 0.0);
+  st = btam_system_get_state(s, c.q.data(), c.sigma.data(), c.x.data());
+  c.have_state = st == BTAM_OK;
+  c.q_bind = c.q;
+  return st;
 }
 
 /* Status of the last evaluation the adapter ran (the table's functions have
@@ -116,32 +140,67 @@ inline bool same_site(const Cache &c, int j, const M &mean_q, const V *stdv_q, c
   return xi(j) == c.x[j];
 }
 
-// Re-evaluates when the sites a value depends on differ from the cache.
+// Diagonal stretch F with c.q = diag(F) q_bind on every row (to 1e-13
+// relative), fitted by least squares per component; false if none.
+inline bool stretch_of(const Cache &c, double F[3]) {
+  for (int k = 0; k < 3; ++k) {
+    double num = 0.0, den = 0.0;
+    for (int j = 0; j < c.n; ++j) {
+      num += c.q[3 * (size_t)j + k] * c.q_bind[3 * (size_t)j + k];
+      den += c.q_bind[3 * (size_t)j + k] * c.q_bind[3 * (size_t)j + k];
+    }
+    F[k] = den > 0.0 ? num / den : 1.0;
+    if (!(F[k] > 0.0) || !std::isfinite(F[k])) return false;
+    for (int j = 0; j < c.n; ++j) {
+      const double v = c.q[3 * (size_t)j + k], b = F[k] * c.q_bind[3 * (size_t)j + k];
+      if (std::fabs(v - b) > 1e-13 * (std::fabs(v) + 1.0)) return false;
+    }
+  }
+  return true;
+}
+
+enum { kMeanField = 1, kPoint = 2 };
+
+// Loads the caller's state when the sites a value depends on differ from the
+// cache, then evaluates what `what` asks for and is not yet evaluated.
 template <class M, class V>
 inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *stdv_q,
-                    const V &xi, const AtomTopology &topo, bool nmf) {
-  bool same = c.valid && same_site(c, (int)a, mean_q, stdv_q, xi) &&
+                    const V &xi, const AtomTopology &topo, int what) {
+  bool same = c.have_state && same_site(c, (int)a, mean_q, stdv_q, xi) &&
               same_site(c, (int)b, mean_q, stdv_q, xi);
   for (int k = 0; same && k < topo.numneigh; ++k)
     same = same_site(c, (int)topo.mech_neighs_ptr[k], mean_q, stdv_q, xi);
-  if (same && (!nmf || c.nmf_valid)) return;
   if (!same) {
     for (int j = 0; j < c.n; ++j) {
       for (int k = 0; k < 3; ++k) c.q[3 * (size_t)j + k] = mean_q(j, k);
       if (stdv_q) c.sigma[j] = (*stdv_q)(j);
       c.x[j] = xi(j);
     }
-    c.status = btam_system_set_state(c.sys, c.q.data(), c.sigma.data(), c.x.data());
-    c.valid = c.nmf_valid = false;
+    c.valid = c.pt_valid = false;
+    // a stretch of the bound positions takes the cell with it; any other
+    // state keeps the current cell
+    double F[3];
+    c.status = BTAM_OK;
+    if (stretch_of(c, F) && (F[0] != c.F[0] || F[1] != c.F[1] || F[2] != c.F[2])) {
+      const double rel[3] = {F[0] / c.F[0], F[1] / c.F[1], F[2] / c.F[2]};
+      c.status = btam_stretch_apply(c.sys, rel);
+      if (c.status == BTAM_OK)
+        for (int k = 0; k < 3; ++k) c.F[k] = F[k];
+    }
+    if (c.status == BTAM_OK)
+      c.status = btam_system_set_state(c.sys, c.q.data(), c.sigma.data(), c.x.data());
+    c.have_state = c.status == BTAM_OK;
   }
-  if (c.status == BTAM_OK && !c.valid) {
+  if (!c.have_state) return;
+  if ((what & kMeanField) && !c.valid) {
     c.status = btam_mf_eval(c.sys, c.precision, c.rho.data(), c.V0.data(), c.S0.data(),
                             c.Rq.data(), c.Rs.data(), c.Rx.data(), nullptr);
     c.valid = c.status == BTAM_OK;
   }
-  if (nmf && c.status == BTAM_OK && !c.nmf_valid) {
-    c.status = btam_rho_nmf(c.sys, c.rho_nmf.data());
-    c.nmf_valid = c.status == BTAM_OK;
+  if ((what & kPoint) && !c.pt_valid) {
+    c.status = btam_pt_eval(c.sys, c.pt_rho.data(), nullptr, c.pt_Fq.data(), c.pt_W.data(),
+                            nullptr);
+    c.pt_valid = c.status == BTAM_OK;
   }
 }
 
@@ -164,15 +223,53 @@ inline double rho_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::Vect
                     const AtomicSpecie *, const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, topo, true);
-  return c.nmf_valid && (int)i < c.n ? c.rho_nmf[i] : NAN;
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, topo, kPoint);
+  return c.pt_valid && (int)i < c.n ? c.pt_rho[i] : NAN;
+}
+
+inline Eigen::Vector3d DV_Dq(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
+                             const Eigen::VectorXd &xi, const Eigen::VectorXd &,
+                             const AtomicSpecie *, const AtomTopology topo) {
+  Cache &c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, u, i, mean_q, nullptr, xi, topo, kPoint);
+  Eigen::Vector3d g;
+  for (int k = 0; k < 3; ++k)
+    g(k) = !c.pt_valid || (int)u >= c.n ? NAN : (u == i ? c.pt_Fq[3 * (size_t)u + k] : 0.0);
+  return g;
+}
+
+inline Eigen::Matrix3d DV_DF(unsigned i, const Eigen::MatrixXd &mean_q,
+                             const Eigen::MatrixXd &mean_q0, const Eigen::VectorXd &xi,
+                             const Eigen::VectorXd &, const AtomicSpecie *,
+                             const AtomTopology topo) {
+  Cache &c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, topo, kPoint);
+  Eigen::Matrix3d W;
+  bool ok = c.pt_valid && (int)i < c.n;
+  // the device's W is taken at q0 = q; at q0 = the bound positions, which
+  // the cell's stretch F maps to q, it is W(a, b) / F_b
+  auto bound = [&](int j) {
+    if (j < 0 || j >= c.n) return true;
+    for (int k = 0; k < 3; ++k)
+      if (mean_q0(j, k) != c.q_bind[3 * (size_t)j + k]) return false;
+    return true;
+  };
+  ok = ok && bound((int)i);
+  for (int k = 0; ok && k < topo.numneigh; ++k) ok = bound((int)topo.mech_neighs_ptr[k]);
+  if (c.pt_valid && !ok) c.status = BTAM_ERR_ARG;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      W(a, b) = ok ? c.pt_W[9 * (size_t)i + 3 * a + b] / c.F[b] : NAN;
+  return W;
 }
 
 inline double mf_rho_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::VectorXd &stdv_q,
                        const Eigen::VectorXd &xi, const AtomicSpecie *, const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kMeanField);
   return c.valid && (int)i < c.n ? c.rho[i] : NAN;
 }
 
@@ -181,7 +278,7 @@ inline double V0_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::Vecto
                    const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kMeanField);
   return c.valid && (int)i < c.n ? c.V0[i] : NAN;
 }
 
@@ -190,7 +287,7 @@ inline double S0_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::Vecto
                    const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kMeanField);
   return c.valid && (int)i < c.n ? c.S0[i] : NAN;
 }
 
@@ -200,7 +297,7 @@ inline Eigen::Vector3d DV0_Dmeanq(unsigned u, unsigned i, const Eigen::MatrixXd 
                                   const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
   Eigen::Vector3d g;
   for (int k = 0; k < 3; ++k)
     g(k) = !c.valid || (int)u >= c.n ? NAN : (u == i ? c.Rq[3 * (size_t)u + k] : 0.0);
@@ -212,7 +309,7 @@ inline double DV0_Dstdvq(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                          const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
   if (!c.valid || (int)u >= c.n) return NAN;
   return u == i ? dV0_dsigma(c, (int)u) : 0.0;
 }
@@ -223,7 +320,7 @@ inline Eigen::Vector4d DV0_Dq(unsigned u, unsigned i, const Eigen::MatrixXd &mea
                               const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
   Eigen::Vector4d g;
   const bool ok = c.valid && (int)u < c.n;
   for (int k = 0; k < 3; ++k) g(k) = !ok ? NAN : (u == i ? c.Rq[3 * (size_t)u + k] : 0.0);
@@ -237,7 +334,7 @@ inline double DV0_Dxi(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                       const AtomTopology topo) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, false);
+  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
   if (!c.valid || (int)u >= c.n) return NAN;
   return u == i ? dV0_dx(c, (int)u, specie && (int)specie[u] == 1) : 0.0;  // 1: H
 }
@@ -251,9 +348,9 @@ inline dmd_equations btam_DMD_MgHx_constructor() {
   namespace d = btam_compat::detail;
   dmd_equations eq;
   eq.evaluate_rho_i = d::rho_i;
-  eq.evaluate_DV_i_Dq_j = nullptr;
+  eq.evaluate_DV_i_Dq_j = d::DV_Dq;
   eq.evaluate_D2V_i_Dq2_j = nullptr;
-  eq.evaluate_DV_i_DF = nullptr;
+  eq.evaluate_DV_i_DF = d::DV_DF;
   eq.evaluate_mf_rho_i = d::mf_rho_i;
   eq.evaluate_V0_i = d::V0_i;
   eq.evaluate_S0_i = d::S0_i;

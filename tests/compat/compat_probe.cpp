@@ -9,14 +9,25 @@
 // x, beta, gamma (n each), origin (3), cell (9), periodic (3 ints).
 // Output: per site rho, V0, S0, Rq (3), dV0/dsigma, dV0/dx; then the
 // status of the last evaluation.
+//
+// With the arguments `pt F0 F1 F2` after the output path, the probe runs
+// the reference's bulk residual instead (evaluate_RHS,
+// Mechanical-Relaxation-bulk.cpp:441-600) at mean_q = diag(F) q with
+// mean_q0 = q: evaluate_rho_i over the sites, then per site the assembled
+// evaluate_DV_i_Dq_j and evaluate_DV_i_DF.  Output: per site rho, the
+// gradient (3), dV/dF (9, row-major); then Y (3) = sum_u diag(dV_u/dF) / V0
+// and the status.
 #include "Macros.hpp"
 #include "btam_dmd_equations.hpp"
 
+#include <cmath>
 #include <cstdio>
+#include <string>
 #include <vector>
 
 int main(int argc, char **argv) {
-  if (argc != 4) return 2;
+  const bool pt = argc == 8 && std::string(argv[4]) == "pt";
+  if (argc != 4 && !pt) return 2;
   FILE *f = fopen(argv[2], "rb");
   if (!f) return 2;
   int n = 0;
@@ -67,6 +78,49 @@ int main(int argc, char **argv) {
   dmd_equations eq = btam_DMD_MgHx_constructor();
   FILE *o = fopen(argv[3], "wb");
   if (!o) return 2;
+  if (pt) {
+    const double F[3] = {atof(argv[5]), atof(argv[6]), atof(argv[7])};
+    Eigen::MatrixXd q_ref = mean_q;
+    for (int i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) mean_q(i, k) = F[k] * q_ref(i, k);
+    const double vol = std::fabs(cell[0] * (cell[4] * cell[8] - cell[5] * cell[7]) -
+                                 cell[1] * (cell[3] * cell[8] - cell[5] * cell[6]) +
+                                 cell[2] * (cell[3] * cell[7] - cell[4] * cell[6]));
+    std::vector<std::vector<PetscInt>> nbs(n);
+    for (int u = 0; u < n; ++u)
+      for (int p = offs[u]; p < offs[u + 1]; ++p)
+        if (idx[p] < n) nbs[u].push_back(idx[p]);
+    for (int u = 0; u < n; ++u) {
+      AtomTopology topo{(int)nbs[u].size(), nbs[u].data()};
+      rho_v(u) = eq.evaluate_rho_i(u, mean_q, xi, specie.data(), topo);
+    }
+    double Y[3] = {0, 0, 0};
+    for (int u = 0; u < n; ++u) {
+      AtomTopology topo{(int)nbs[u].size(), nbs[u].data()};
+      double v[13];
+      v[0] = rho_v(u);
+      double g[3] = {0, 0, 0};
+      for (int k = -1; k < (int)nbs[u].size(); ++k) {
+        const unsigned i = k < 0 ? u : nbs[u][k];
+        Eigen::Vector3d d = eq.evaluate_DV_i_Dq_j(u, i, mean_q, xi, rho_v, specie.data(), topo);
+        for (int c = 0; c < 3; ++c) g[c] += d(c);
+      }
+      for (int c = 0; c < 3; ++c) v[1 + c] = g[c];
+      Eigen::Matrix3d W = eq.evaluate_DV_i_DF(u, mean_q, q_ref, xi, rho_v, specie.data(), topo);
+      for (int a = 0; a < 3; ++a) {
+        for (int b = 0; b < 3; ++b) v[4 + 3 * a + b] = W(a, b);
+        Y[a] += W(a, a) / vol;
+      }
+      fwrite(v, sizeof(double), 13, o);
+    }
+    fwrite(Y, sizeof(double), 3, o);
+    const int last = btam_compat::last_status();
+    fwrite(&last, sizeof(int), 1, o);
+    fclose(o);
+    btam_system_destroy(S);
+    btam_tables_destroy(T);
+    return last == BTAM_OK ? 0 : 1;
+  }
   for (int u = 0; u < n; ++u) {
     std::vector<PetscInt> nb;
     for (int p = offs[u]; p < offs[u + 1]; ++p)

@@ -56,3 +56,39 @@ def test_plugin_table_matches_direct_evaluation(gpu_tables, tmp_path):
     scale = max(1.0, np.abs(dsig).max(), np.abs(dx).max())
     assert np.abs(v[:, 6] - dsig).max() <= 1e-12 * scale
     assert np.abs(v[:, 7] - dx).max() <= 1e-12 * scale
+
+
+def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
+    """The non-mean-field slots (evaluate_rho_i, evaluate_DV_i_Dq_j,
+    evaluate_DV_i_DF) driven the way the reference's bulk residual drives
+    them, unstretched and at a stretch of the bound positions, against the
+    reference's own values (tests/golden/point.npz)."""
+    import compat_build
+    probe = compat_build.build_probe()
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    g = dict(np.load(os.path.join(gold, "ortho_mgh.npz")))
+    p = dict(np.load(os.path.join(gold, "point.npz")))
+    s = {k: g[k] for k in ("q", "sigma", "x", "species", "beta", "gamma", "origin", "cell",
+                           "periodic")}
+    n = len(s["x"])
+    inp = str(tmp_path / "sys.bin")
+    write_system(inp, s)
+    vol = abs(np.linalg.det(s["cell"].reshape(3, 3)))
+    for F, kr, kw in ((np.ones(3), "ortho_mgh_rho", "ortho_mgh_W"),
+                      (p["stretch"], "ortho_mgh_rho_s", "ortho_mgh_W_s")):
+        out = str(tmp_path / "out.bin")
+        r = subprocess.run([probe, TABLES, inp, out, "pt"] + [repr(float(f)) for f in F],
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        raw = open(out, "rb").read()
+        v = np.frombuffer(raw[:8 * 13 * n], np.float64).reshape(n, 13)
+        Y = np.frombuffer(raw[8 * 13 * n:8 * 13 * n + 24], np.float64)
+        assert np.frombuffer(raw[8 * 13 * n + 24:], np.int32)[0] == 0
+        assert np.max(np.abs(v[:, 0] - p[kr])) <= 1e-12 * np.abs(p[kr]).max()
+        W = v[:, 4:].reshape(n, 3, 3)
+        assert np.max(np.abs(W - p[kw])) <= 1e-10 * max(1.0, np.abs(p[kw]).max())
+        Yref = np.array([p[kw][:, a, a].sum() for a in range(3)]) / vol
+        assert np.max(np.abs(Y - Yref)) <= 1e-10 * max(1.0, np.abs(Yref).max())
+        if F[0] == 1.0:
+            Fq = p["ortho_mgh_Fq"]
+            assert np.max(np.abs(v[:, 1:4] - Fq)) <= 1e-10 * max(1.0, np.abs(Fq).max())
