@@ -382,6 +382,82 @@ def bench_nanowire(args, tables):
             "fp32c_vs_fp64_max_abs_dx": float(np.abs(xs["fp32c"] - xs["fp64"]).max())}
 
 
+def bench_bulk_stretch(args, tables, cpu_budget_s=6.0):
+    """The reference's one compiled solver, the bulk stretch relaxation
+    (mechanical_relaxation_bulk), on the plain drop-in workload: Newton on
+    the diagonal stretch F with the non-mean-field stress residual
+    Y = sum_u diag(dV_u/dF) / V0 at fixed x and neighbour lists, from F = 1
+    to |Y| <= 1e-12.  Each residual is one device evaluation of rho and
+    dV_u/dF over all sites.  The reference's arithmetic for one residual
+    (evaluate_rho_i and evaluate_DV_i_dF_MgHx, oracle/_ref, all host
+    threads) is timed on a sample of sites and scaled to all sites."""
+    import torch
+    import btam
+    import pyoracle
+    from btam import lattice
+
+    sys_ = lattice.config2()
+    runs = []
+    for k in range(2):  # the first run warms up (allocations, module load)
+        S = btam.System(tables, sys_)
+        S.build_neighbors()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        F, info = S.relax_stretch(atol=1e-12, rtol=1e-10, max_iter=20)
+        runs.append((time.perf_counter() - t0, F, info))
+        S.close()
+    t, F, info = runs[-1]
+    out = {"workload": WORKLOAD, "sites": len(sys_["x"]),
+           "solver": "Newton, forward-difference Jacobian (3 residuals), backtracking",
+           "F": [float(f) for f in F], "iterations": info["iterations"],
+           "residual_evaluations": info["evaluations"], "final_norm": info["norm"],
+           "status": info["status"], "ms_total": t * 1e3,
+           "ms_per_residual": t * 1e3 / max(info["evaluations"], 1),
+           "timing": "host clock around the call (each residual ends in a 96-byte read)"}
+    if not args.no_cpu:
+        ref = pyoracle.reference(fast=True)
+        kind = "reference"
+        orc = pyoracle.Oracle()
+        if ref is None:
+            ref, kind = orc, "port"
+        threads = os.cpu_count() or 1
+        os.environ["BTAM_REF_THREADS"] = str(threads)
+        os.environ["BTAM_ORACLE_THREADS"] = str(threads)
+        full, nr, owner, image = pyoracle.expand(sys_, orc)
+        rng = np.random.default_rng(7)
+        sample = np.sort(rng.choice(nr, 400, replace=False)).astype(np.int32)
+        need = np.unique(np.concatenate([sample, owner[orc.neighbors(full["q"],
+                                                                     query=sample)[1]]]))
+        need = need.astype(np.int32)
+        oq, iq = orc.neighbors(full["q"], query=need)
+        counts = np.zeros(len(full["x"]), np.int64)
+        counts[need] = np.diff(oq)
+        offs = np.zeros(len(full["x"]) + 1, np.int32)
+        offs[1:] = np.cumsum(counts)
+        idx = np.zeros(offs[-1], np.int32)
+        for k, qi in enumerate(need):
+            idx[offs[qi]:offs[qi + 1]] = iq[oq[k]:oq[k + 1]]
+        t0 = time.perf_counter()
+        rho_n = ref.rho_nmf(full, offs, idx, need)
+        t_rho = (time.perf_counter() - t0) / len(need)
+        rho = np.zeros(nr)
+        rho[need] = rho_n
+        per = []
+        for chunk in np.array_split(sample, 8):
+            t0 = time.perf_counter()
+            ref.pt_DV_dF(full, full["q"], rho[owner], offs, idx, chunk)
+            per.append((time.perf_counter() - t0) / len(chunk))
+            if sum(per) * len(chunk) > cpu_budget_s:
+                break
+        t_res = nr * (t_rho + float(np.mean(per)))
+        out["cpu_reference"] = {
+            "s_per_residual": t_res, "threads": threads, "kind": kind,
+            "sample": f"evaluate_rho_i of {len(need)} sites and evaluate_DV_i_dF_MgHx of "
+                      f"{len(per) * (len(sample) // 8)} sites, scaled to all {nr} sites"}
+        out["gpu_over_cpu_per_residual"] = t_res / (out["ms_per_residual"] * 1e-3)
+    return out
+
+
 def bench_serving(args, tables):
     """The served workload: a seeded Poisson stream (mean 200 jobs/s) of 64
     jobs, half relaxations (L-BFGS to |R| <= 1e-5 or 100 iterations) and half
@@ -590,6 +666,7 @@ def run_btam(args, ws, rank, local):
                                                         barrier)
     serving = None if args.no_serve else bench_serving(args, tables)
     nanowire = None if args.no_wire else bench_nanowire(args, tables)
+    stretch = None if args.no_stretch else bench_bulk_stretch(args, tables)
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
@@ -622,7 +699,7 @@ def run_btam(args, ws, rank, local):
                         "ms_per_step": e2e_ms},
                 "gpu_launches": launches_per_eval(shapes["fp32c"]) * args.steps,
                 "clocks": clocks, "batched": batched, "serving": serving,
-                "precision_nanowire": nanowire}
+                "precision_nanowire": nanowire, "bulk_stretch": stretch}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -640,6 +717,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true", help="skip the served workload")
     ap.add_argument("--serve-jobs", type=int, default=64, help="jobs in the served stream")
     ap.add_argument("--no-wire", action="store_true", help="skip the nanowire DMD workload")
+    ap.add_argument("--no-stretch", action="store_true",
+                    help="skip the bulk stretch relaxation workload")
     ap.add_argument("--dmd-steps", type=int, default=1000,
                     help="master-equation steps of the nanowire workload")
     args = ap.parse_args()
