@@ -70,6 +70,9 @@ _PROTOS = {
     "btam_stretch_apply": (ctypes.c_int, [_V, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
+    "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int, _D, _D]),
+    "btam_mf_stress": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
     "btam_probe_gather_peak": (ctypes.c_int, [_V, ctypes.c_double, _D]),
@@ -416,6 +419,24 @@ class System:
         info = np.zeros(5)
         _check(lib().btam_relax_stretch(self.handle, atol, rtol, max_iter, _d(F), _d(info)),
                "btam_relax_stretch")
+        return F, dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
+                       status=int(info[3]), volume=info[4])
+
+    def mf_stress(self, precision=FP64):
+        """Mean-field stress dV0_u/dF at q0 = q, sigma and x held: (per-site
+        (n, 3, 3), sum (3, 3))."""
+        W = np.zeros((self.n, 3, 3))
+        tot = np.zeros(9)
+        _check(lib().btam_mf_stress(self.handle, precision, _d(W), _d(tot)), "btam_mf_stress")
+        return W, tot.reshape(3, 3)
+
+    def relax_stretch_mf(self, precision=FP64, atol=1e-12, rtol=1e-10, max_iter=20,
+                         F0=(1.0, 1.0, 1.0)):
+        """Bulk stretch relaxation on the mean-field stress (sigma, x held)."""
+        F = np.ascontiguousarray(F0, np.float64).copy()
+        info = np.zeros(5)
+        _check(lib().btam_relax_stretch_mf(self.handle, precision, atol, rtol, max_iter, _d(F),
+                                           _d(info)), "btam_relax_stretch_mf")
         return F, dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
                        status=int(info[3]), volume=info[4])
 

@@ -438,6 +438,66 @@ pass2_kernel(const EvalArgs<R> a) {
   }
 }
 
+// Mean-field stress of every real site, W0_u = sum_j dV0_u/dq_j (x) (q_j - q_u)
+// at fixed sigma and x: evaluate_DV0_i_dF_bulk_MgHx (MgHx-mf-V-bulk.cpp:
+// 2329-2552) at reference positions q0 = q (by translation invariance of
+// V0_u, the reference's sum over the term sites a of d<term>/dq_a (x) q0_a).
+// pass2_pair with omega = 0 returns the self part of pair j, the terms of
+// dV0_u/dq_u that pair j carries, which is -dV0_u/dq_j; with r0 = q_u - q_j
+// the pair adds self (x) r0.  Directed form, a warp per site.
+template <class R, int W>
+__global__ void __launch_bounds__(W * 32)
+mf_stress_kernel(const EvalArgs<R> a, double *W0) {
+  __shared__ R mu_s[W][kMomStride];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
+  const double2 xbu = a.xb[u];
+  const double xu = xbu.x;
+  if (xu < kMinOcc) {
+    if (lane < 9) W0[9 * (size_t)u + lane] = 0.0;
+    continue;
+  }
+  const R *mu_g = a.mom + (size_t)u * kMomStride;
+  for (int c = lane; c < kMomStride; c += 32) mu_s[warp][c] = mu_g[c];
+  __syncwarp();
+  const MomRec<R, false> mu(mu_s[warp]);
+  const double4 qu = a.pos[u];
+  const int cu = a.code[u];
+  Acc<R> acc[9];
+  for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
+    const int j = a.idx[p];
+    const double2 xbj = a.xb[j];
+    if (xbj.x < kMinOcc) continue;
+    const int o = a.owner[j];
+    const double4 qj = a.pos[j];
+    const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
+    Pass2Out<R> out;
+    out.gq[0] = out.gq[1] = out.gq[2] = out.gs = out.gx = (R)0;
+    const V3<R> r0 = pair_vec<R>(qu, qj);
+    pass2_pair<R>(a.T, r0, (R)qu.w, (R)qj.w, (R)xu, (R)xbj.x, cu, a.code[j], mu.scalar(0),
+                  mj.scalar(0), mj.scalar(1), (R)0, mu, mj, out);
+    const R rv[3] = {r0.x, r0.y, r0.z};
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int d = 0; d < 3; ++d) acc[3 * c + d].add(out.gq[c] * rv[d]);
+  }
+  double t[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) t[c] = warp_sum(acc[c].get());
+  if (lane == 0) {
+    bool ok = true;
+    for (int c = 0; c < 9; ++c) {
+      W0[9 * (size_t)u + c] = t[c];
+      ok = ok && finite(t[c]);
+    }
+    if (!ok) atomicOr(a.err, 1 << kErrBitNonFinite);
+  }
+  __syncwarp();  // mu_s is reloaded for the warp's next site
+  }
+}
+
 // One thread per owned slot p = (u, j): both directions of the pair from its
 // 25 geometries (pass2_pair_sym); u's part into slot p, j's part into the
 // reverse slot.  Pairs with an empty site give zero records, so every slot
@@ -714,6 +774,15 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent
   }
   return cudaGetLastError();
 }
+template <class R>
+cudaError_t launch_mf_stress(const EvalArgs<R> &a, double *W0, cudaStream_t st) {
+  if (a.n_real > 0)
+    mf_stress_kernel<R, 4><<<nblocks(a.n_real, 4), 128, 0, st>>>(a, W0);
+  return cudaGetLastError();
+}
+template cudaError_t launch_mf_stress<double>(const EvalArgs<double> &, double *, cudaStream_t);
+template cudaError_t launch_mf_stress<float>(const EvalArgs<float> &, double *, cudaStream_t);
+
 template cudaError_t launch_pass1<double>(const EvalArgs<double> &, cudaStream_t, int, int,
                                           cudaEvent_t);
 template cudaError_t launch_pass1<float>(const EvalArgs<float> &, cudaStream_t, int, int,

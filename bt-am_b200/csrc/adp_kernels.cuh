@@ -135,6 +135,10 @@ cudaError_t launch_seg_totals(int n_sys, const int *seg, const double *V0, const
 
 // Non-mean-field density rho_i = sum_j x_j rho_{s_j}(|q_i - q_j|)
 // (density.cpp:44-104) for every real site.
+// Mean-field stress W0 (9 per real site, row-major) from the moment
+// records of a directed pass 1 (launch_pass1 with variants 0, 0).
+template <class R>
+cudaError_t launch_mf_stress(const EvalArgs<R> &a, double *W0, cudaStream_t st);
 cudaError_t launch_rho_nmf(int n_real, const double4 *pos, const double2 *xb,
                            const int *code, const int *offs, const int *idx,
                            SplineView<double> rho_mg, SplineView<double> rho_h,

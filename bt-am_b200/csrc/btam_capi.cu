@@ -1021,6 +1021,48 @@ int btam_probe_gather_peak(const btam_tables *t, double seconds, double *gbs) {
   return BTAM_OK;
 }
 
+}  // extern "C"
+
+int mf_stress_enqueue(btam_system *s, int precision, double **W_out, double **tot_out) {
+  double *W = nullptr, *part = nullptr, *tot = nullptr;
+  int st = pt_stress_buffers(s, &W, &part, &tot);
+  if (st != BTAM_OK) return st;
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  // the directed pass 1 writes the moment records the stress kernel reads
+  if (precision == BTAM_FP64) {
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
+    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
+    BTAM_TRY(launch_pass1(a, s->st, 0, 0));
+    BTAM_TRY(launch_mf_stress(a, W, s->st));
+  } else {
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
+    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
+    BTAM_TRY(launch_pass1(a, s->st, 0, 0));
+    BTAM_TRY(launch_mf_stress(a, W, s->st));
+  }
+  BTAM_TRY(launch_pt_totals(s->n_real, nullptr, nullptr, W, part, tot, s->st));
+  *W_out = W;
+  *tot_out = tot;
+  return BTAM_OK;
+}
+
+extern "C" {
+
+int btam_mf_stress(btam_system *s, int precision, double *W0, double *total) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  double *W = nullptr, *tot = nullptr;
+  int st = mf_stress_enqueue(s, precision, &W, &tot);
+  if (st != BTAM_OK) return st;
+  if (W0)
+    BTAM_TRY(cudaMemcpyAsync(W0, W, 9 * (size_t)s->n_real * sizeof(double),
+                             cudaMemcpyDeviceToHost, s->st));
+  if (total)
+    BTAM_TRY(cudaMemcpyAsync(total, tot + 2, 9 * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+  return read_err(s);
+}
+
 int btam_rho_nmf(btam_system *s, double *rho) {
   if (!s || !rho) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;

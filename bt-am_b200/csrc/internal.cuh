@@ -91,6 +91,18 @@ struct btam_system {
   size_t pt_cap = 0;
 };
 
+// Point-form buffers reused by the mean-field stress, and the fixed-order
+// totals over per-site V, Fq, W (V, Fq may be NULL) into tot[12]
+// (point.cu).
+int pt_stress_buffers(btam_system *s, double **W, double **part, double **tot);
+cudaError_t launch_pt_totals(int n, const double *V, const double *Fq, const double *W,
+                             double *part, double *tot, cudaStream_t st);
+
+// Enqueues the directed pass 1 and the mean-field stress of the current
+// state; *W: per-site stress (9 n), *tot: totals whose [2..10] hold the sum
+// (btam_capi.cu).
+int mf_stress_enqueue(btam_system *s, int precision, double **W, double **tot);
+
 // Box of a cell (rows = lattice vectors) and origin at the potential's
 // cutoff, with the checks of btam_system_create (btam_capi.cu).
 int make_box_for(const double *origin, const double *cell, const int *periodic, GhostBox &b);

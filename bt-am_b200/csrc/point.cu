@@ -208,9 +208,11 @@ __global__ void __launch_bounds__(256) pt_totals_part_kernel(int n, const double
 #pragma unroll
   for (int c = 0; c < kPtTot; ++c) v[c] = 0.0;
   for (int i = lo + t; i < hi; i += 256) {
-    v[0] += V[i];
-    v[1] += Fq[3 * (size_t)i] * Fq[3 * (size_t)i] + Fq[3 * (size_t)i + 1] * Fq[3 * (size_t)i + 1] +
-            Fq[3 * (size_t)i + 2] * Fq[3 * (size_t)i + 2];
+    if (V) v[0] += V[i];
+    if (Fq)
+      v[1] += Fq[3 * (size_t)i] * Fq[3 * (size_t)i] +
+              Fq[3 * (size_t)i + 1] * Fq[3 * (size_t)i + 1] +
+              Fq[3 * (size_t)i + 2] * Fq[3 * (size_t)i + 2];
     for (int c = 0; c < 9; ++c) v[2 + c] += W[9 * (size_t)i + c];
   }
   for (int c = 0; c < kPtTot; ++c) sh[c][t] = v[c];
@@ -298,6 +300,28 @@ int pt_run(btam_system *s, const PtLayout &L) {
   pt_totals_final_kernel<<<1, 32, 0, s->st>>>(L.part, L.tot);
   return cuda_status(cudaGetLastError());
 }
+
+}  // namespace
+
+// The point-form buffer's W, partials and totals, for the mean-field
+// stress (btam_mf_stress), and the fixed-order totals over its sites.
+int pt_stress_buffers(btam_system *s, double **W, double **part, double **tot) {
+  PtLayout L;
+  int st = pt_buffers(s, L);
+  if (st != BTAM_OK) return st;
+  *W = L.W;
+  *part = L.part;
+  *tot = L.tot;
+  return BTAM_OK;
+}
+cudaError_t launch_pt_totals(int n, const double *V, const double *Fq, const double *W,
+                             double *part, double *tot, cudaStream_t st) {
+  pt_totals_part_kernel<<<kPtParts, 256, 0, st>>>(n, V, Fq, W, part);
+  pt_totals_final_kernel<<<1, 32, 0, st>>>(part, tot);
+  return cudaGetLastError();
+}
+
+namespace {
 
 double cell_volume(const GhostBox &b) {
   const double(*A)[3] = b.A;
@@ -402,8 +426,14 @@ int btam_stretch_apply(btam_system *s, const double F[3]) {
   return read_err(s);
 }
 
-int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, double F[3],
-                       double *info) {
+}  // extern "C"
+
+namespace {
+
+// form 0: the non-mean-field stress (the reference's bulk residual);
+// 1, 2: the mean-field stress at fixed sigma and x, FP64 or FP32C.
+int relax_stretch(btam_system *s, int form, double atol, double rtol, int max_iter,
+                  double F[3], double *info) {
   if (!s || !F || !(atol >= 0.0) || !(rtol >= 0.0) || max_iter < 0) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   for (int a = 0; a < 3; ++a)
@@ -426,10 +456,18 @@ int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, d
     for (int a = 0; a < 3; ++a) Fx[a] = X[a] > 0.0 ? X[a] : 1.0;
     GhostBox bF;
     int r = apply_stretch(s, q0, box0, Fx, bF);
-    if (r == BTAM_OK) r = pt_run(s, L);
+    double *dtot = L.tot;
+    if (r == BTAM_OK) {
+      if (form == 0) {
+        r = pt_run(s, L);
+      } else {
+        double *W = nullptr;
+        r = mf_stress_enqueue(s, form == 1 ? BTAM_FP64 : BTAM_FP32C, &W, &dtot);
+      }
+    }
     double tot[kPtTot];
     if (r == BTAM_OK)
-      r = cuda_status(cudaMemcpyAsync(tot, L.tot, sizeof(tot), cudaMemcpyDeviceToHost, s->st));
+      r = cuda_status(cudaMemcpyAsync(tot, dtot, sizeof(tot), cudaMemcpyDeviceToHost, s->st));
     if (r == BTAM_OK) r = read_err(s);
     if (r != BTAM_OK) return r;
     ++evals;
@@ -453,12 +491,14 @@ int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, d
     if (it >= max_iter) break;
     // Jacobian by forward differences, one column per evaluation (the
     // reference's MatFDColoring of a dense 3x3 pattern: three colours,
-    // step sqrt(eps) |X_a|, at least 1e-6 sqrt(eps))
+    // step sqrt(eps) |X_a|, at least 1e-6 sqrt(eps)); the FP32C stress
+    // carries ~1e-7 relative noise, so its step is 1e-4 |X_a|
+    const double hrel = form == 2 ? 1e-4 : 1.4901161193847656e-08;
     double J[3][3];
     for (int c = 0; c < 3 && st == BTAM_OK; ++c) {
       double Xp[3] = {X[0], X[1], X[2]}, Yp[3];
-      double h = 1.4901161193847656e-08 * std::fabs(X[c]);
-      if (h < 1.4901161193847656e-14) h = 1.4901161193847656e-14;
+      double h = hrel * std::fabs(X[c]);
+      if (h < 1e-6 * hrel) h = 1e-6 * hrel;
       Xp[c] += h;
       h = Xp[c] - X[c];
       st = residual(Xp, Yp);
@@ -526,6 +566,21 @@ int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, d
     info[4] = vol;
   }
   return st;
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, double F[3],
+                       double *info) {
+  return relax_stretch(s, 0, atol, rtol, max_iter, F, info);
+}
+
+int btam_relax_stretch_mf(btam_system *s, int precision, double atol, double rtol,
+                          int max_iter, double F[3], double *info) {
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  return relax_stretch(s, precision == BTAM_FP64 ? 1 : 2, atol, rtol, max_iter, F, info);
 }
 
 }  // extern "C"

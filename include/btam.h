@@ -175,6 +175,16 @@ int btam_autotune(btam_system *s, int precision, int *pass1_variant, int *pass2_
  * for runs that must reproduce one another bit for bit. */
 int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass2_variant);
 
+/* Mean-field stress: W0 (9 per real site, row-major; row: gradient
+ * component, column: position component) = dV0_u/dF at fixed sigma and x,
+ * at reference positions q0 = q: evaluate_DV0_i_dF_bulk_MgHx
+ * (MgHx-mf-V-bulk.cpp:2329-2552).  At reference positions q0 =
+ * diag(F)^-1 q it is W0(a, b) / F_b.  total (9): the sum over the real
+ * sites.  Runs the directed pass 1 first, so the system's rho, V0 and S0
+ * buffers hold the current state's values afterwards.  Either output may
+ * be NULL. */
+int btam_mf_stress(btam_system *s, int precision, double *W0, double *total);
+
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);
@@ -220,6 +230,13 @@ int btam_stretch_apply(btam_system *s, const double F[3]);
  * here, and any solver that converges finds the same F. */
 int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, double F[3],
                        double *info);
+/* The same relaxation on the mean-field stress (btam_mf_stress: the
+ * reference's evaluate_DV0_i_dF_bulk_MgHx, whose table slot
+ * evaluate_DV0_i_DF no reference solver calls) at fixed sigma and x, in
+ * `precision` (BTAM_FP64 or BTAM_FP32C; the FP32C stress resolves |Y| to
+ * about 1e-9 eV/A^3, so give it atol >= 1e-8). */
+int btam_relax_stretch_mf(btam_system *s, int precision, double atol, double rtol,
+                          int max_iter, double F[3], double *info);
 
 /* ---- consumers of the evaluation -----------------------------------------
  * Relaxation of (q, sigma).  The reference configures a PETSc SNES

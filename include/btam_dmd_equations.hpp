@@ -47,13 +47,14 @@
  *    cell is stretched with it, so periodic images follow as the caller's
  *    stretched ghost rows do (Mechanical-Relaxation-bulk.cpp:505-520);
  *    any other mean_q is a new state in the current cell.
- *    evaluate_DV_i_DF is defined for mean_q0 equal to the bound positions
- *    (the reference's bulk residual passes its unstretched positions,
- *    Mechanical-Relaxation-bulk.cpp:577-579); other mean_q0 give NaN and
- *    last_status() BTAM_ERR_ARG.
- *  - The Hessians and the mean-field stretch derivative
- *    (evaluate_D2V_i_Dq2_j, evaluate_D2V0_i_Dmeanq2_j, evaluate_DV0_i_DF)
- *    are not provided: their slots are null. */
+ *    evaluate_DV_i_DF and evaluate_DV0_i_DF are defined for mean_q0 equal
+ *    to the bound positions (the reference's bulk residual passes its
+ *    unstretched positions, Mechanical-Relaxation-bulk.cpp:577-579); other
+ *    mean_q0 give NaN and last_status() BTAM_ERR_ARG.
+ *  - evaluate_DV0_i_DF (the mean-field stretch derivative) comes from
+ *    btam_mf_stress in the bound precision.
+ *  - The Hessians (evaluate_D2V_i_Dq2_j, evaluate_D2V0_i_Dmeanq2_j) are not
+ *    provided: their slots are null. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -73,13 +74,14 @@ struct Cache {
   bool have_state = false;  // q, sigma, x below are the system's state
   bool valid = false;       // mean-field results of that state
   bool pt_valid = false;    // non-mean-field results of that state
+  bool mfs_valid = false;   // mean-field stress of that state
   int status = BTAM_OK;     // status of the last evaluation
   std::vector<double> beta, gamma;
   std::vector<double> q, sigma, x;  // the evaluated state (q row-major)
   std::vector<double> q_bind;       // positions at bind(): the stretch reference
   double F[3] = {1.0, 1.0, 1.0};    // stretch of the system's cell against them
   std::vector<double> rho, V0, S0, Rq, Rs, Rx;
-  std::vector<double> pt_rho, pt_Fq, pt_W;
+  std::vector<double> pt_rho, pt_Fq, pt_W, mf_W;
 };
 
 inline Cache &cache() {
@@ -101,7 +103,7 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.sys = s;
   c.precision = precision;
   c.n = n_real;
-  c.have_state = c.valid = c.pt_valid = false;
+  c.have_state = c.valid = c.pt_valid = c.mfs_valid = false;
   c.F[0] = c.F[1] = c.F[2] = 1.0;
   c.beta.assign(beta ? beta : nullptr, beta ? beta + n_real : nullptr);
   c.gamma.assign(gamma ? gamma : nullptr, gamma ? gamma + n_real : nullptr);
@@ -119,6 +121,7 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.pt_rho.assign(n_real, 0.0);
   c.pt_Fq.assign(3 * (size_t)n_real, 0.0);
   c.pt_W.assign(9 * (size_t)n_real, 0.0);
+  c.mf_W.assign(9 * (size_t)n_real, 0.0);
   st = btam_system_get_state(s, c.q.data(), c.sigma.data(), c.x.data());
   c.have_state = st == BTAM_OK;
   c.q_bind = c.q;
@@ -159,7 +162,7 @@ inline bool stretch_of(const Cache &c, double F[3]) {
   return true;
 }
 
-enum { kMeanField = 1, kPoint = 2 };
+enum { kMeanField = 1, kPoint = 2, kStress = 4 };
 
 // Loads the caller's state when the sites a value depends on differ from the
 // cache, then evaluates what `what` asks for and is not yet evaluated.
@@ -176,7 +179,7 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
       if (stdv_q) c.sigma[j] = (*stdv_q)(j);
       c.x[j] = xi(j);
     }
-    c.valid = c.pt_valid = false;
+    c.valid = c.pt_valid = c.mfs_valid = false;
     // a stretch of the bound positions takes the cell with it; any other
     // state keeps the current cell
     double F[3];
@@ -202,6 +205,31 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
                             nullptr);
     c.pt_valid = c.status == BTAM_OK;
   }
+  if ((what & kStress) && !c.mfs_valid) {
+    c.status = btam_mf_stress(c.sys, c.precision, c.mf_W.data(), nullptr);
+    c.mfs_valid = c.status == BTAM_OK;
+  }
+}
+
+// A stress W taken at q0 = q, at reference positions mean_q0, which must be
+// the bound positions (the cell's stretch F maps them to q): W(a, b) / F_b.
+template <class M>
+inline Eigen::Matrix3d stress_at_q0(Cache &c, const std::vector<double> &Wq, bool valid,
+                                    unsigned i, const M &mean_q0, const AtomTopology &topo) {
+  bool ok = valid && (int)i < c.n;
+  auto bound = [&](int j) {
+    if (j < 0 || j >= c.n) return true;
+    for (int k = 0; k < 3; ++k)
+      if (mean_q0(j, k) != c.q_bind[3 * (size_t)j + k]) return false;
+    return true;
+  };
+  ok = ok && bound((int)i);
+  for (int k = 0; ok && k < topo.numneigh; ++k) ok = bound((int)topo.mech_neighs_ptr[k]);
+  if (valid && !ok) c.status = BTAM_ERR_ARG;
+  Eigen::Matrix3d W;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) W(a, b) = ok ? Wq[9 * (size_t)i + 3 * a + b] / c.F[b] : NAN;
+  return W;
 }
 
 // Assembled sigma derivative of V0 (the residual without its entropy term
@@ -246,23 +274,17 @@ inline Eigen::Matrix3d DV_DF(unsigned i, const Eigen::MatrixXd &mean_q,
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
   refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, topo, kPoint);
-  Eigen::Matrix3d W;
-  bool ok = c.pt_valid && (int)i < c.n;
-  // the device's W is taken at q0 = q; at q0 = the bound positions, which
-  // the cell's stretch F maps to q, it is W(a, b) / F_b
-  auto bound = [&](int j) {
-    if (j < 0 || j >= c.n) return true;
-    for (int k = 0; k < 3; ++k)
-      if (mean_q0(j, k) != c.q_bind[3 * (size_t)j + k]) return false;
-    return true;
-  };
-  ok = ok && bound((int)i);
-  for (int k = 0; ok && k < topo.numneigh; ++k) ok = bound((int)topo.mech_neighs_ptr[k]);
-  if (c.pt_valid && !ok) c.status = BTAM_ERR_ARG;
-  for (int a = 0; a < 3; ++a)
-    for (int b = 0; b < 3; ++b)
-      W(a, b) = ok ? c.pt_W[9 * (size_t)i + 3 * a + b] / c.F[b] : NAN;
-  return W;
+  return stress_at_q0(c, c.pt_W, c.pt_valid, i, mean_q0, topo);
+}
+
+inline Eigen::Matrix3d DV0_DF(unsigned i, const Eigen::MatrixXd &mean_q,
+                              const Eigen::MatrixXd &mean_q0, const Eigen::VectorXd &stdv_q,
+                              const Eigen::VectorXd &xi, const Eigen::VectorXd &,
+                              const AtomicSpecie *, const AtomTopology topo) {
+  Cache &c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kStress);
+  return stress_at_q0(c, c.mf_W, c.mfs_valid, i, mean_q0, topo);
 }
 
 inline double mf_rho_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::VectorXd &stdv_q,
@@ -359,7 +381,7 @@ inline dmd_equations btam_DMD_MgHx_constructor() {
   eq.evaluate_DV0_i_Dstdvq_j = d::DV0_Dstdvq;
   eq.evaluate_DV0_i_Dq_j = d::DV0_Dq;
   eq.evaluate_DV0_i_Dxi_j = d::DV0_Dxi;
-  eq.evaluate_DV0_i_DF = nullptr;
+  eq.evaluate_DV0_i_DF = d::DV0_DF;
   return eq;
 }
 

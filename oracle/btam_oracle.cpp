@@ -619,6 +619,53 @@ double DV0_dx(const View &v, int u, int i) {
   return emb + pair + dip + quad;
 }
 
+// evaluate_DV0_i_dF_bulk_MgHx (MgHx-mf-V-bulk.cpp:2329-2552): sum over the
+// sites a of every term of V0_i of d<term>/dmean_q_a (x) q0_a (sigma held),
+// 3x3 row-major.
+void DV0_dF(const View &v, const double *q0, int i, double *out9) {
+  for (int c = 0; c < 9; ++c) out9[c] = 0.0;
+  if (v.x[i] < kMinOcc) return;  // 2371-2373
+  double drho[9] = {0}, pair[9] = {0}, dip[9] = {0}, quad[9] = {0};
+  const int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    const int j1 = v.idx[k1];
+    if (v.spc[j1] == kH && v.x[j1] < kMinOcc) continue;  // 2408-2410
+    PairCtx c;
+    pair_ctx(v, i, j1, c);
+    int sites2[2] = {i, j1};
+    for (int dir = 0; dir < 2; ++dir) {
+      const double *r0 = q0 + 3 * sites2[dir];
+      double g[3];
+      integ_dmq(dir, kRho, c.m, g);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) drho[3 * a + b] += g[a] * r0[b];
+      integ_dmq(dir, kPair, c.m, g);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) pair[3 * a + b] += g[a] * r0[b];
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      const int j2 = v.idx[k2];
+      if (v.spc[j2] == kH && v.x[j2] < kMinOcc) continue;  // 2465-2467
+      TriCtx t;
+      tri_ctx(v, i, j1, j2, t);
+      int sites3[3] = {i, j1, j2};
+      const double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        const double *r0 = q0 + 3 * sites3[dir];
+        double g[3];
+        integ_dmq(dir, kDip, t.m, g);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) dip[3 * a + b] += f * g[a] * r0[b];
+        integ_dmq(dir, kQuad, t.m, g);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) quad[3 * a + b] += f * g[a] * r0[b];
+      }
+    }
+  }
+  const double dF = spline_d1(embed_of(v.spc[i]), v.rho[i]);  // 2536-2543
+  for (int c = 0; c < 9; ++c) out9[c] = v.x[i] * dF * drho[c] + pair[c] + dip[c] + quad[c];
+}
+
 // ---------------------------------------------------------------------------
 // Non-mean-field forms: the ADP terms at the mean positions (sigma -> 0).
 
@@ -1003,6 +1050,14 @@ void orc_pt_DV_dF(int n, const double *q, const double *q0, const double *x, con
   (void)n;
   View v{q, nullptr, x, rho, spc, offs, idx};
   par_for(nsites, [&](int k) { DV_dF(v, q0, sites[k], out9 + 9 * k); });
+}
+
+void orc_mf_DV0_dF(int n, const double *q, const double *q0, const double *sigma,
+                   const double *x, const int *spc, const double *rho, const int *offs,
+                   const int *idx, const int *sites, int nsites, double *out9) {
+  (void)n;
+  View v{q, sigma, x, rho, spc, offs, idx};
+  par_for(nsites, [&](int k) { DV0_dF(v, q0, sites[k], out9 + 9 * k); });
 }
 
 void orc_residuals(int n, const double *q, const double *sigma,

@@ -80,6 +80,13 @@ void orc_pt_DV_dF(int n, const double *q, const double *q0, const double *x, con
                   const double *rho, const int *offs, const int *idx, const int *sites,
                   int nsites, double *out9);
 
+/* Mean-field stretch derivative dV0_i/dF per site, 9 values row-major,
+ * with reference positions q0 of every site (evaluate_DV0_i_dF_bulk_MgHx,
+ * MgHx-mf-V-bulk.cpp:2329-2552); rho: the mean-field density of every site. */
+void orc_mf_DV0_dF(int n, const double *q, const double *q0, const double *sigma,
+                   const double *x, const int *spc, const double *rho, const int *offs,
+                   const int *idx, const int *sites, int nsites, double *out9);
+
 /* Residual assembly for real sites u (project definition):
  *   R_q(u)     = sum_{i in {u} U N(u)} (beta_i/beta_u) dV0_i/dq_u
  *   R_sigma(u) = sum_i (beta_i/beta_u) dV0_i/dsigma_u - 3/(beta_u sigma_u)

@@ -137,6 +137,18 @@ class Lib:
         return out
 
 
+    def mf_DV0_dF(self, s, q0, rho, offs, idx, sites):
+        """dV0_i/dF per site, 3x3 (evaluate_DV0_i_dF_bulk_MgHx), reference
+        positions q0, mean-field density rho of every site."""
+        sites = np.ascontiguousarray(sites, np.int32)
+        q0 = np.ascontiguousarray(q0, np.float64)
+        out = np.zeros((len(sites), 3, 3))
+        self._f("mf_DV0_dF")(len(s["x"]), _d(s["q"]), _d(q0), _d(s["sigma"]), _d(s["x"]),
+                             _i(s["species"]), _d(rho), _i(offs), _i(idx), _i(sites),
+                             len(sites), _d(out))
+        return out
+
+
 class Oracle(Lib):
     """The restated oracle plus its project-defined pieces."""
 

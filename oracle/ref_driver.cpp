@@ -322,4 +322,26 @@ void ref_pt_DV_dF(int n, const double *q, const double *q0, const double *x, con
   free(s.spc);
 }
 
+// evaluate_DV0_i_dF_bulk_MgHx (MgHx-mf-V-bulk.cpp:2329-2552): 9 values per
+// site, row-major, with reference positions q0 of every site; rho is the
+// mean-field density of every site.
+void ref_mf_DV0_dF(int n, const double *q, const double *q0, const double *sigma,
+                   const double *x, const int *spc, const double *rho, const int *offs,
+                   const int *idx, const int *sites, int nsites, double *out9) {
+  Sys s;
+  make_sys(s, n, q, sigma, x, spc, offs, idx);
+  for (int i = 0; i < n; ++i) s.rho(i) = rho[i];
+  Eigen::MatrixXd Q0(n, 3);
+  for (int i = 0; i < n; ++i)
+    for (int k = 0; k < 3; ++k) Q0(i, k) = q0[3 * i + k];
+  parallel_for(nsites, [&](int k) {
+    int i = sites[k];
+    Eigen::Matrix3d g =
+        evaluate_DV0_i_dF_bulk_MgHx(i, s.q, Q0, s.sigma, s.x, s.rho, s.spc, topo(s, i));
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) out9[9 * k + 3 * a + b] = g(a, b);
+  });
+  free(s.spc);
+}
+
 } // extern "C"

@@ -14,9 +14,10 @@
 // the reference's bulk residual instead (evaluate_RHS,
 // Mechanical-Relaxation-bulk.cpp:441-600) at mean_q = diag(F) q with
 // mean_q0 = q: evaluate_rho_i over the sites, then per site the assembled
-// evaluate_DV_i_Dq_j and evaluate_DV_i_DF.  Output: per site rho, the
-// gradient (3), dV/dF (9, row-major); then Y (3) = sum_u diag(dV_u/dF) / V0
-// and the status.
+// evaluate_DV_i_Dq_j, evaluate_DV_i_DF and the mean-field
+// evaluate_DV0_i_DF.  Output: per site rho, the gradient (3), dV/dF (9,
+// row-major), dV0/dF (9); then Y (3) = sum_u diag(dV_u/dF) / V0 and the
+// status.
 #include "Macros.hpp"
 #include "btam_dmd_equations.hpp"
 
@@ -97,7 +98,7 @@ int main(int argc, char **argv) {
     double Y[3] = {0, 0, 0};
     for (int u = 0; u < n; ++u) {
       AtomTopology topo{(int)nbs[u].size(), nbs[u].data()};
-      double v[13];
+      double v[22];
       v[0] = rho_v(u);
       double g[3] = {0, 0, 0};
       for (int k = -1; k < (int)nbs[u].size(); ++k) {
@@ -111,7 +112,11 @@ int main(int argc, char **argv) {
         for (int b = 0; b < 3; ++b) v[4 + 3 * a + b] = W(a, b);
         Y[a] += W(a, a) / vol;
       }
-      fwrite(v, sizeof(double), 13, o);
+      Eigen::Matrix3d W0 =
+          eq.evaluate_DV0_i_DF(u, mean_q, q_ref, stdv_q, xi, rho_v, specie.data(), topo);
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) v[13 + 3 * a + b] = W0(a, b);
+      fwrite(v, sizeof(double), 22, o);
     }
     fwrite(Y, sizeof(double), 3, o);
     const int last = btam_compat::last_status();

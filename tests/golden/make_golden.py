@@ -118,7 +118,9 @@ def point_fixture(ref):
     evaluate_DV_i_dF_MgHx, on the neighbour lists stored in each fixture:
     the assembled gradient sum_{i in {u} U N(u)} dV_i/dq_u of every real
     site, dV_i/dF with q0 = q, and dV_i/dF after the stretch PT_STRETCH
-    (q0 = the unstretched positions, neighbour lists kept)."""
+    (q0 = the unstretched positions, neighbour lists kept); and the
+    mean-field stretch derivative evaluate_DV0_i_dF_bulk_MgHx at q0 = q and
+    after the same stretch (with the mean-field rho-bar there)."""
     out = {"stretch": PT_STRETCH}
     for name in ("sphere", "ortho_mgh", "x5cube", "config1"):
         g = np.load(os.path.join(OUT, f"{name}.npz"))
@@ -143,6 +145,14 @@ def point_fixture(ref):
         W_s = ref.pt_DV_dF(st, full["q"], rho_s[owner], offs, idx, real)
         out.update({f"{name}_rho": rho, f"{name}_Fq": Fq, f"{name}_W": W,
                     f"{name}_rho_s": rho_s, f"{name}_W_s": W_s})
+        # the mean-field stretch derivative (evaluate_DV0_i_dF_bulk_MgHx),
+        # sigma and x held, at q0 = q and after the stretch
+        mf = dict(full, sigma=np.ascontiguousarray(g["sigma"][owner]))
+        W0 = ref.mf_DV0_dF(mf, full["q"], g["rho"][owner], offs, idx, real)
+        mfs = dict(mf, q=st["q"])
+        rho0_s = ref.mf_rho(mfs, offs, idx, real)
+        W0_s = ref.mf_DV0_dF(mfs, full["q"], rho0_s[owner], offs, idx, real)
+        out.update({f"{name}_W0": W0, f"{name}_rho0_s": rho0_s, f"{name}_W0_s": W0_s})
         print(f"point forms {name}: {n} sites, {len(plan)} gradient pairs")
     np.savez_compressed(os.path.join(OUT, "point.npz"), **out)
 

@@ -61,8 +61,9 @@ def test_plugin_table_matches_direct_evaluation(gpu_tables, tmp_path):
 def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
     """The non-mean-field slots (evaluate_rho_i, evaluate_DV_i_Dq_j,
     evaluate_DV_i_DF) driven the way the reference's bulk residual drives
-    them, unstretched and at a stretch of the bound positions, against the
-    reference's own values (tests/golden/point.npz)."""
+    them, and the mean-field stretch slot evaluate_DV0_i_DF, unstretched and
+    at a stretch of the bound positions, against the reference's own values
+    (tests/golden/point.npz)."""
     import compat_build
     probe = compat_build.build_probe()
     gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -81,11 +82,13 @@ def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
                            capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr
         raw = open(out, "rb").read()
-        v = np.frombuffer(raw[:8 * 13 * n], np.float64).reshape(n, 13)
-        Y = np.frombuffer(raw[8 * 13 * n:8 * 13 * n + 24], np.float64)
-        assert np.frombuffer(raw[8 * 13 * n + 24:], np.int32)[0] == 0
+        v = np.frombuffer(raw[:8 * 22 * n], np.float64).reshape(n, 22)
+        Y = np.frombuffer(raw[8 * 22 * n:8 * 22 * n + 24], np.float64)
+        assert np.frombuffer(raw[8 * 22 * n + 24:], np.int32)[0] == 0
         assert np.max(np.abs(v[:, 0] - p[kr])) <= 1e-12 * np.abs(p[kr]).max()
-        W = v[:, 4:].reshape(n, 3, 3)
+        W = v[:, 4:13].reshape(n, 3, 3)
+        W0, kw0 = v[:, 13:].reshape(n, 3, 3), kw.replace("_W", "_W0")
+        assert np.max(np.abs(W0 - p[kw0])) <= 1e-10 * max(1.0, np.abs(p[kw0]).max())
         assert np.max(np.abs(W - p[kw])) <= 1e-10 * max(1.0, np.abs(p[kw]).max())
         Yref = np.array([p[kw][:, a, a].sum() for a in range(3)]) / vol
         assert np.max(np.abs(Y - Yref)) <= 1e-10 * max(1.0, np.abs(Yref).max())

@@ -148,3 +148,82 @@ def test_relax_stretch_rejections(gpu_tables):
         S.relax_stretch(F0=(1.0, -1.0, 1.0))
     with pytest.raises(btam.BtamError):
         S.stretch((1.0, 0.0, 1.0))
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_mf_stress_against_reference(gpu_tables, name):
+    """Mean-field stretch derivative (evaluate_DV0_i_dF_bulk_MgHx) at q0 = q
+    and after a stretch, FP64 within 1e-10 and FP32C within 1e-4 of
+    max(1, the largest component)."""
+    g, p = load(name), load("point")
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    W, tot = S.mf_stress(btam.FP64)
+    assert err1(W, p[f"{name}_W0"]) < 1e-10
+    assert np.allclose(tot, W.sum(0), rtol=1e-12, atol=1e-12)
+    W32, _ = S.mf_stress(btam.FP32C)
+    assert err1(W32, p[f"{name}_W0"]) < 1e-4
+    F = p["stretch"]
+    S.stretch(F)
+    W, _ = S.mf_stress(btam.FP64)
+    assert err1(W / F[None, None, :], p[f"{name}_W0_s"]) < 1e-10
+
+
+def test_mf_stress_is_energy_derivative(gpu_tables):
+    """sum_u W0_u(a, a) = d(sum_i V0_i)/dF_aa at F = 1, sigma and x held.
+    Past the table end (6.2987 A) a spline keeps its end value but the
+    reference's derivative keeps the end slope (1e-5 to 3e-4,
+    cubic-spline.cpp:90-93, 114-128), so quadrature points beyond it make
+    the analytic stress differ from the energy's slope (6e-5 relative at
+    sigma ~ 0.1 A).  With the widths scaled by 0.1 few points reach past
+    the end and the two agree to 5e-6."""
+    g = load("ortho_mgh")
+    s = system_of(g)
+    s["sigma"] = s["sigma"] * 0.1
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    _, W = S.mf_stress(btam.FP64)
+    h = 1e-6
+    for a in range(3):
+        up = np.ones(3)
+        up[a] = 1.0 + h
+        S.stretch(up)
+        Ep = S.evaluate(btam.FP64)["totals"][0]
+        dn = np.ones(3)
+        dn[a] = (1.0 - h) / (1.0 + h)
+        S.stretch(dn)
+        Em = S.evaluate(btam.FP64)["totals"][0]
+        back = np.ones(3)
+        back[a] = 1.0 / (1.0 - h)
+        S.stretch(back)
+        fd = (Ep - Em) / (2 * h)
+        assert abs(fd - W[a, a]) <= 5e-6 * max(1.0, abs(W[a, a])), (a, fd, W[a, a])
+
+
+def test_relax_stretch_mf_zeroes_reference_stress(gpu_tables, oracle):
+    """The mean-field bulk stretch relaxation: FP64 to |Y| <= 1e-12, where
+    the oracle's evaluate_DV0_i_dF_bulk_MgHx stress is <= 1e-9; FP32C to
+    |Y| <= 1e-8, within 1e-5 of the FP64 stretch."""
+    g = load("ortho_mgh")
+    s = system_of(g)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    F, info = S.relax_stretch_mf(btam.FP64, atol=1e-12, rtol=1e-10, max_iter=20)
+    assert info["status"] == 1 and info["norm"] <= 1e-12, info
+    vol = info["volume"]
+    n = len(g["x"])
+    owner = g["owner"]
+    full = {"q": np.ascontiguousarray(g["q_all"] * F),
+            "sigma": np.ascontiguousarray(g["sigma"][owner]),
+            "x": np.ascontiguousarray(g["x"][owner]),
+            "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+    real = np.arange(n, dtype=np.int32)
+    rho = oracle.mf_rho(full, g["offs"], g["idx"], real)
+    W = oracle.mf_DV0_dF(full, g["q_all"], rho[owner], g["offs"], g["idx"], real)
+    Y = np.array([W[:, a, a].sum() for a in range(3)]) / vol
+    assert np.max(np.abs(Y)) <= 1e-9, Y
+    S2 = btam.System(gpu_tables, s)
+    S2.build_neighbors()
+    F32, info32 = S2.relax_stretch_mf(btam.FP32C, atol=1e-8, rtol=1e-10, max_iter=20)
+    assert info32["status"] == 1, info32
+    assert np.max(np.abs(F32 - F)) <= 1e-5

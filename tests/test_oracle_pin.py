@@ -142,6 +142,15 @@ def test_point_forms_against_golden(oracle, name):
     assert np.array_equal(rho_s, p[f"{name}_rho_s"])
     assert np.array_equal(oracle.pt_DV_dF(st, full["q"], rho_s[owner], offs, idx, real),
                           p[f"{name}_W_s"])
+    # mean-field stretch derivative (evaluate_DV0_i_dF_bulk_MgHx)
+    mf = dict(full, sigma=np.ascontiguousarray(g["sigma"][owner]))
+    assert np.array_equal(oracle.mf_DV0_dF(mf, full["q"], g["rho"][owner], offs, idx, real),
+                          p[f"{name}_W0"])
+    mfs = dict(mf, q=st["q"])
+    rho0_s = oracle.mf_rho(mfs, offs, idx, real)
+    assert np.array_equal(rho0_s, p[f"{name}_rho0_s"])
+    assert np.array_equal(oracle.mf_DV0_dF(mfs, full["q"], rho0_s[owner], offs, idx, real),
+                          p[f"{name}_W0_s"])
 
 
 def test_point_forms_match_reference_live(oracle, ref):
