@@ -80,6 +80,8 @@ _PROTOS = {
     "btam_relax": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                   _D, _D]),
     "btam_system_get_state": (ctypes.c_int, [_V, _D, _D, _D]),
+    "btam_relax_newton": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
+                                         _D]),
     "btam_dmd_setup": (ctypes.c_int, [_V]),
     "btam_dmd_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D,
                                      ctypes.POINTER(ctypes.c_longlong)]),
@@ -335,6 +337,18 @@ class System:
                "btam_relax")
         return dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
                     objective=info[3], status=int(info[4]))
+
+    def relax_newton(self, tol=1e-8, max_newton=50, max_cg=200, sigma_min=0.001,
+                     sigma_max=0.4, x_min=0.01):
+        """Damped truncated-Newton relaxation of (q, sigma) (FP64,
+        Hessian-vector products by differences of the residual).  Returns a
+        dict like relax() plus the CG iteration count."""
+        info = np.zeros(6)
+        bd = np.array([sigma_min, sigma_max, x_min], np.float64)
+        _check(lib().btam_relax_newton(self.handle, tol, max_newton, max_cg, _d(bd), _d(info)),
+               "btam_relax_newton")
+        return dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
+                    objective=info[3], status=int(info[4]), cg_iterations=int(info[5]))
 
     def dmd_setup(self):
         _check(lib().btam_dmd_setup(self.handle), "btam_dmd_setup")

@@ -1266,6 +1266,146 @@ int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m, const 
   return BTAM_OK;
 }
 
+int btam_relax_newton(btam_system *s, double tol, int max_newton, int max_cg,
+                      const double *bounds, double *info) {
+  if (!s || !(tol > 0.0) || max_newton < 0 || max_cg < 1) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  const double sig_lo = bounds ? bounds[0] : 0.001, sig_hi = bounds ? bounds[1] : 0.4,
+               x_min = bounds ? bounds[2] : 0.01;
+  if (!(sig_lo > 0.0 && sig_hi > sig_lo && x_min >= 0.0)) return BTAM_ERR_ARG;
+  const int n = s->n_real, n4 = 4 * n;
+  // layout: z g p z0 g0 r d hd (n4 each), fterm rterm ones (n), small; the
+  // block of btam_relax with m = 1 has exactly this size
+  const size_t need = (size_t)8 * n4 + 3 * (size_t)n + 64;
+  if (!s->rv) {
+    BTAM_TRY(dalloc(s->rv, s->st, need));
+    s->relax_m = 1;
+  }
+  RelaxVecs v;
+  double *b = s->rv;
+  v.z = b; v.g = b + n4; v.p = b + 2 * n4; v.z0 = b + 3 * n4; v.g0 = b + 4 * n4;
+  double *r = b + 5 * n4, *d = b + 6 * n4, *hd = b + 7 * n4;
+  v.work = nullptr;
+  v.fterm = b + (size_t)8 * n4;
+  v.rterm = v.fterm + n;
+  v.ones = v.rterm + n;
+  v.scal = v.ones + n;
+  v.tmp = v.scal + 2;
+  v.bd.ls_lo = std::log(sig_lo);
+  v.bd.ls_hi = std::log(sig_hi);
+  v.bd.x_min = x_min;
+  fill_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(n, 1.0, v.ones);
+  BTAM_TRY(cudaGetLastError());
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  auto move = [&](const double *z0, const double *p, double alpha) -> int {
+    BTAM_TRY(relax_apply(n, s->xb, z0, p, alpha, v.bd, s->pos, s->st));
+    if (s->n_ghost > 0)
+      BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                    s->box, s->st));
+    return BTAM_OK;
+  };
+  double f, r2;
+  int evals = 0, it = 0, cg_total = 0, st;
+  if ((st = relax_eval(s, BTAM_FP64, v, f, r2)) != BTAM_OK) return st;
+  ++evals;
+  bool stalled = false;
+  double lam = 0.0;  // damping of the Newton system
+  for (; it < max_newton; ++it) {
+    if (std::sqrt(r2) <= tol) break;
+    BTAM_TRY(cudaMemcpyAsync(v.z0, v.z, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaMemcpyAsync(v.g0, v.g, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    const double f0 = f, r20 = r2;
+    const double gg = dev_dot(s, v, n4, v.g0, v.g0), gnorm = std::sqrt(gg);
+    const double zz = dev_dot(s, v, n4, v.z0, v.z0);
+    // conjugate gradients on (H + lam I) p = -g, H d by a forward
+    // difference of the gradient (one evaluation per iteration), forcing
+    // term min(0.5, sqrt|g|).  Negative curvature raises lam past it and
+    // restarts (at most 4 times); lam shrinks after full steps.
+    const double eta = std::min(0.5, std::sqrt(gnorm));
+    for (int restart = 0; restart < 5; ++restart) {
+      BTAM_TRY(cudaMemsetAsync(v.p, 0, n4 * sizeof(double), s->st));
+      BTAM_TRY(vec_axpby(n4, -1.0, v.g0, 0.0, v.g0, r, s->st));
+      BTAM_TRY(cudaMemcpyAsync(d, r, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+      double rr = gg;
+      bool negative = false;
+      for (int k = 0; k < max_cg; ++k) {
+        const double dd = dev_dot(s, v, n4, d, d);
+        if (!(dd > 0.0)) break;
+        const double eps = 1.4901161193847656e-08 * (1.0 + std::sqrt(zz)) / std::sqrt(dd);
+        if ((st = move(v.z0, d, eps)) != BTAM_OK) return st;
+        if ((st = relax_eval(s, BTAM_FP64, v, f, r2)) != BTAM_OK) return st;
+        ++evals;
+        ++cg_total;
+        BTAM_TRY(vec_axpby(n4, 1.0 / eps, v.g, -1.0 / eps, v.g0, hd, s->st));
+        if (lam > 0.0) BTAM_TRY(vec_axpby(n4, 1.0, hd, lam, d, hd, s->st));
+        const double dhd = dev_dot(s, v, n4, d, hd);
+        if (!(dhd > 0.0)) {
+          if (restart < 4) {
+            lam = std::max(4.0 * lam, 2.0 * (lam - dhd / dd));
+            negative = true;
+          } else if (k == 0) {
+            BTAM_TRY(cudaMemcpyAsync(v.p, d, n4 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                     s->st));
+          }
+          break;
+        }
+        const double a = rr / dhd;
+        BTAM_TRY(vec_axpby(n4, 1.0, v.p, a, d, v.p, s->st));
+        BTAM_TRY(vec_axpby(n4, 1.0, r, -a, hd, r, s->st));
+        const double rr1 = dev_dot(s, v, n4, r, r);
+        if (std::sqrt(rr1) <= eta * gnorm) break;
+        BTAM_TRY(vec_axpby(n4, 1.0, r, rr1 / rr, d, d, s->st));
+        rr = rr1;
+      }
+      if (!negative) break;
+    }
+    double gp = dev_dot(s, v, n4, v.g0, v.p);
+    if (!(gp < 0.0)) {  // no descent: steepest descent
+      BTAM_TRY(vec_axpby(n4, -1.0, v.g0, 0.0, v.g0, v.p, s->st));
+      gp = -gg;
+    }
+    // no q (A) or log sigma moves by more than 0.2 in one step
+    double alpha = 1.0;
+    absmax_kernel<<<1, 256, 0, s->st>>>(n4, s->xb, v.p, v.tmp + 6);
+    double pmax = 0.0;
+    BTAM_TRY(cudaMemcpyAsync(&pmax, v.tmp + 6, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    BTAM_TRY(cudaStreamSynchronize(s->st));
+    if (pmax > 0.2) alpha = 0.2 / pmax;
+    const double alpha0 = alpha;
+    bool ok = false;
+    for (int ls = 0; ls < 30; ++ls) {
+      if ((st = move(v.z0, v.p, alpha)) != BTAM_OK) return st;
+      if ((st = relax_eval(s, BTAM_FP64, v, f, r2)) != BTAM_OK) return st;
+      ++evals;
+      const double noise = 1e-13 * std::fabs(f0);
+      if (f <= f0 + 1e-4 * alpha * gp || (std::fabs(f - f0) <= noise && r2 < r20)) {
+        ok = true;
+        break;
+      }
+      alpha *= 0.5;
+    }
+    if (ok && alpha == alpha0) lam *= 0.25;
+    else if (ok) lam = std::max(2.0 * lam, 1e-3);
+    if (!ok) {  // restore the last point and stop
+      if ((st = move(v.z0, v.p, 0.0)) != BTAM_OK) return st;
+      if ((st = relax_eval(s, BTAM_FP64, v, f, r2)) != BTAM_OK) return st;
+      ++evals;
+      stalled = true;
+      break;
+    }
+  }
+  if (info) {
+    info[0] = std::sqrt(r2);
+    info[1] = it;
+    info[2] = evals;
+    info[3] = f;
+    info[4] = (std::sqrt(r2) <= tol) ? 1.0 : (stalled ? -1.0 : 0.0);
+    info[5] = cg_total;
+  }
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  return BTAM_OK;
+}
+
 int btam_dmd_setup(btam_system *s) {
   if (!s) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;

@@ -143,6 +143,20 @@ cudaError_t relax_apply(int n, const double2 *xb, const double *z0, const double
   return cudaGetLastError();
 }
 
+namespace {
+__global__ void axpby_kernel(int n, double a, const double *x, double b, const double *y,
+                             double *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = a * x[i] + b * y[i];
+}
+}  // namespace
+
+cudaError_t vec_axpby(int n, double a, const double *x, double b, const double *y, double *out,
+                      cudaStream_t st) {
+  if (n > 0) axpby_kernel<<<nb(n), 256, 0, st>>>(n, a, x, b, y, out);
+  return cudaGetLastError();
+}
+
 cudaError_t vec_dot(int n, const double *a, const double *b, double *out, cudaStream_t st) {
   dot_kernel<<<1, kRB, 0, st>>>(n, a, b, out);
   return cudaGetLastError();

@@ -17,6 +17,9 @@ cudaError_t relax_gather(int n, const double4 *pos, const double2 *xb, const dou
 cudaError_t relax_apply(int n, const double2 *xb, const double *z0, const double *p,
                         double alpha, const RelaxBounds &bd, double4 *pos, cudaStream_t st);
 cudaError_t vec_dot(int n, const double *a, const double *b, double *out, cudaStream_t st);
+// out = a x + b y (out may alias x or y)
+cudaError_t vec_axpby(int n, double a, const double *x, double b, const double *y, double *out,
+                      cudaStream_t st);
 cudaError_t lbfgs_direction(int n4, const double *g, double *const *S, double *const *Y,
                             const double *rho, const int *order, int m_used, double *p,
                             double *work_q, double *alpha, double *tmp, cudaStream_t st);

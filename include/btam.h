@@ -262,6 +262,22 @@ int btam_relax_stretch_mf(btam_system *s, int precision, double atol, double rto
 int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m,
                const double *bounds, double *info);
 
+/* Newton option of the same relaxation (the reference's SNES is a Newton
+ * method, NEWTONLS, Mechanical-Relaxation-bulk.cpp:293): damped truncated
+ * Newton on the same F and variables, FP64.  Each step solves
+ * (H + lam I) p = -g by conjugate gradients (at most max_cg iterations,
+ * forcing term min(0.5, sqrt|g|)), with H d from a forward difference of
+ * the gradient (one residual evaluation per CG iteration; no Hessian is
+ * formed); negative curvature raises the damping lam and restarts the
+ * solve, full steps lower it.  Then an Armijo backtracking line search (no
+ * q or log sigma moves more than 0.2 per step).  Converged at the projected
+ * residual norm <= tol, or max_newton steps.  bounds as btam_relax.
+ * info (6, may be NULL): final norm, Newton steps, evaluations, final F,
+ * status (1 converged, 0 step limit, -1 no further decrease), CG
+ * iterations. */
+int btam_relax_newton(btam_system *s, double tol, int max_newton, int max_cg,
+                      const double *bounds, double *info);
+
 /* Hydrogen master equation (absent from the reference, which keeps only its
  * parameters, Variables.hpp:68-92, and the diffusive graph builder
  * list_of_diffusive_neighs, Neighbors.cpp:139-275).  Setup builds the H-H

@@ -58,6 +58,45 @@ def test_relaxation_dilute_hydrogen_config1(gpu_tables):
     assert info["norm"] < 1e-4 * r0, info
 
 
+def test_newton_relaxation_stationary_by_oracle(gpu_tables, oracle):
+    """The Newton option on the well-occupied cell: converged, and the
+    literal oracle residuals of the relaxed state vanish."""
+    import pyoracle
+    s = small_mgh(xr=(0.3, 0.6))
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    info = S.relax_newton(tol=1e-8, max_newton=100, max_cg=300)
+    assert info["status"] == 1 and info["norm"] <= 1e-8, info
+    q, sigma, x = S.get_state()
+    r = dict(s, q=q, sigma=sigma, x=x)
+    qg, og, ig = S.ghosts()
+    offs, idx = S.neighbors()
+    sites = np.array([0, 7, 40, 150, 200], np.int32)
+    lit = pyoracle.residuals_on_topology(oracle, r, qg, og, ig, offs, idx, sites)
+    assert np.abs(lit["Rq"]).max() <= 1e-7 and np.abs(lit["Rs"]).max() <= 1e-7
+
+
+def test_newton_relaxation_config1_same_minimum(gpu_tables):
+    """Config 1 (dilute H, sigma bounds active): the Newton option reaches
+    1e-8 and the same minimum as L-BFGS (objective within 1e-10 relative,
+    positions within 1e-5 A); held sites stay fixed."""
+    s = lattice.config1()
+    A = btam.System(gpu_tables, s)
+    A.build_neighbors()
+    ia = A.relax(mode=0, tol=1e-8, max_iter=2000)
+    B = btam.System(gpu_tables, s)
+    B.build_neighbors()
+    ib = B.relax_newton(tol=1e-8, max_newton=100, max_cg=300)
+    assert ia["status"] == 1 and ib["status"] == 1, (ia, ib)
+    assert abs(ia["objective"] - ib["objective"]) <= 1e-10 * abs(ia["objective"])
+    qa, sa, _ = A.get_state()
+    qb, sb, _ = B.get_state()
+    assert np.abs(qa - qb).max() <= 1e-5 and np.abs(sa - sb).max() <= 1e-5
+    fixed = s["x"] < 0.01
+    assert np.array_equal(qb[fixed], s["q"][fixed])
+    assert np.all((sb >= 0.001 - 1e-15) & (sb <= 0.4 + 1e-12))
+
+
 def test_diffusive_graph_bit_exact(gpu_tables):
     import pyoracle
     s = small_mgh(h=0.6)
