@@ -634,12 +634,14 @@ def run_btam(args, ws, rank, local):
     lib = btam.lib()
 
     def e2e_step():
-        S.set_state(q=qh, sigma=sh, x=xh)
-        code = lib.btam_mf_eval(S.handle, btam.FP32C, None, None, None,
-                                btam._d(outs["Rq"]), btam._d(outs["Rs"]), btam._d(outs["Rx"]),
-                                btam._d(outs["totals"]))
+        # new (q, sigma, x) from host buffers, evaluation, residuals back to
+        # host buffers: one C-ABI call
+        code = lib.btam_mf_eval_state(S.handle, btam.FP32C, btam._d(qh), btam._d(sh),
+                                      btam._d(xh), None, None, None, btam._d(outs["Rq"]),
+                                      btam._d(outs["Rs"]), btam._d(outs["Rx"]),
+                                      btam._d(outs["totals"]))
         if code:
-            raise btam.BtamError(code, "btam_mf_eval")
+            raise btam.BtamError(code, "btam_mf_eval_state")
 
     for _ in range(args.warmup):
         e2e_step()

@@ -63,6 +63,8 @@ _PROTOS = {
     "btam_mf_rho": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_mf_eval": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D]),
     "btam_mf_eval_async": (ctypes.c_int, [_V, ctypes.c_int]),
+    "btam_mf_eval_state": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D,
+                                          _D, _D]),
     "btam_results_copy": (ctypes.c_int, [_V, _D, _D, _D, _D, _D, _D, _D]),
     "btam_system_sync": (ctypes.c_int, [_V]),
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
@@ -301,6 +303,19 @@ class System:
         _check(lib().btam_mf_eval(self.handle, precision, _d(out["rho"]), _d(out["V0"]),
                                   _d(out["S0"]), _d(out["Rq"]), _d(out["Rs"]), _d(out["Rx"]),
                                   _d(out["totals"])), "btam_mf_eval")
+        return out
+
+    def evaluate_state(self, precision=FP64, q=None, sigma=None, x=None):
+        """New state and its evaluation in one call (btam_mf_eval_state)."""
+        n = self.n
+        out = dict(rho=np.zeros(n), V0=np.zeros(n), S0=np.zeros(n), Rq=np.zeros((n, 3)),
+                   Rs=np.zeros(n), Rx=np.zeros(n), totals=np.zeros(4))
+        cv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        q, sigma, x = cv(q), cv(sigma), cv(x)
+        _check(lib().btam_mf_eval_state(self.handle, precision, _d(q), _d(sigma), _d(x),
+                                        _d(out["rho"]), _d(out["V0"]), _d(out["S0"]),
+                                        _d(out["Rq"]), _d(out["Rs"]), _d(out["Rx"]),
+                                        _d(out["totals"])), "btam_mf_eval_state")
         return out
 
     def evaluate_async(self, precision=FP64):

@@ -29,9 +29,10 @@ constexpr double kKB = 8.617332478E-5;  // k_B [eV/K] (Macros.hpp:849)
 
 // Packs row-major q, sigma and x of real sites into the device layout.
 __global__ void pack_state_kernel(int n, const double *q, const double *sigma,
-                                  const double *x, double4 *pos, double2 *xb) {
+                                  const double *x, double4 *pos, double2 *xb,
+                                  const int *reject = nullptr) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || (reject && *reject)) return;  // a rejected update leaves the state
   double4 p = pos[i];
   double2 b = xb[i];
   if (q) {
@@ -888,6 +889,43 @@ int btam_mf_eval(btam_system *s, int precision, double *rho, double *V0, double 
   int st = btam_mf_eval_async(s, precision);
   if (st != BTAM_OK) return st;
   return btam_results_copy(s, rho, V0, S0, Rq, Rs, Rx, totals);
+}
+
+int btam_mf_eval_state(btam_system *s, int precision, const double *q, const double *sigma,
+                       const double *x, double *rho, double *V0, double *S0, double *Rq,
+                       double *Rs, double *Rx, double *totals) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  // as btam_system_set_state, but the validation flags are read with the
+  // results: the update is applied on the device only if it passes, and
+  // the host waits once
+  const int n = s->n_real;
+  double *dq = s->stage, *ds = s->stage + 3 * (size_t)n, *dx = s->stage + 4 * (size_t)n;
+  if (q) BTAM_TRY(cudaMemcpyAsync(dq, q, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  if (sigma) BTAM_TRY(cudaMemcpyAsync(ds, sigma, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  if (x) BTAM_TRY(cudaMemcpyAsync(dx, x, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, 2 * sizeof(int), s->st));
+  if (q || sigma || x) {
+    validate_stage_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(
+        n, q ? dq : nullptr, sigma ? ds : nullptr, x ? dx : nullptr, s->code, s->box, s->err + 1);
+    BTAM_TRY(cudaGetLastError());
+    pack_state_kernel<<<(n + 127) / 128, 128, 0, s->st>>>(
+        n, q ? dq : nullptr, sigma ? ds : nullptr, x ? dx : nullptr, s->pos, s->xb, s->err + 1);
+    BTAM_TRY(cudaGetLastError());
+    if (s->n_ghost > 0)
+      BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                    s->box, s->st));
+  }
+  int st = btam_mf_eval_async(s, precision);
+  if (st != BTAM_OK) return st;
+  int flags = 0;
+  BTAM_TRY(cudaMemcpyAsync(&flags, s->err + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  st = btam_results_copy(s, rho, V0, S0, Rq, Rs, Rx, totals);
+  if (flags & 1) return BTAM_ERR_NONFINITE;
+  if (flags & 2) return BTAM_ERR_OCCUPANCY;
+  if (flags & 4) return BTAM_ERR_OUT_OF_BOX;
+  return st;
 }
 
 int btam_mf_rho(btam_system *s, int precision, double *rho) {

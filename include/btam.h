@@ -154,6 +154,15 @@ int btam_mf_rho(btam_system *s, int precision, double *rho);
  * totals (4): sum V0, sum S0, sum |R_q|^2 + R_sigma^2, sum R_x^2. */
 int btam_mf_eval(btam_system *s, int precision, double *rho, double *V0,
                  double *S0, double *Rq, double *Rs, double *Rx, double *totals);
+/* btam_system_set_state followed by btam_mf_eval in one call that waits
+ * for the device once (no counterpart in the reference): the new state (any
+ * of q, sigma, x may be NULL) is copied, checked and applied on the device,
+ * then evaluated.  A rejected state returns the set_state error and leaves
+ * the system's state unchanged; the outputs then hold the evaluation of
+ * that unchanged state. */
+int btam_mf_eval_state(btam_system *s, int precision, const double *q, const double *sigma,
+                       const double *x, double *rho, double *V0, double *S0, double *Rq,
+                       double *Rs, double *Rx, double *totals);
 /* The same evaluation enqueued on the system's stream with inputs and
  * outputs resident on the device; results stay in the system's buffers
  * (btam_results_copy reads them).  Does not synchronise. */

@@ -182,6 +182,39 @@ def test_state_update_rejections(gpu_tables):
             assert np.array_equal(again[k], base[k]), k
 
 
+def test_eval_state_matches_set_state_then_eval(gpu_tables):
+    """btam_mf_eval_state (one wait for the device) gives the bits of
+    btam_system_set_state followed by btam_mf_eval, in both forms, and a
+    rejected update returns the set_state code with the state kept."""
+    s = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.5, x_range=(0.0, 0.3), seed=17)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    rng = np.random.default_rng(4)
+    cell = s["cell"].reshape(3, 3)
+    lo, hi = s["origin"], s["origin"] + np.diag(cell)
+    inside = np.all((s["q"] > lo + 0.05) & (s["q"] < hi - 0.05), axis=1)
+    q2 = s["q"].copy()
+    q2[inside] += rng.normal(0.0, 0.01, (int(inside.sum()), 3))
+    sig2 = s["sigma"] * 1.05
+    for prec in (btam.FP64, btam.FP32C):
+        S.set_state(q=s["q"], sigma=s["sigma"], x=s["x"])
+        S.set_state(q=q2, sigma=sig2)
+        a = S.evaluate(prec)
+        S.set_state(q=s["q"], sigma=s["sigma"], x=s["x"])
+        b = S.evaluate_state(prec, q=q2, sigma=sig2)
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (prec, k)
+    base = S.evaluate(btam.FP64)
+    bad_q = q2.copy()
+    bad_q[5, 1] = np.nan
+    with pytest.raises(btam.BtamError) as e:
+        S.evaluate_state(btam.FP64, q=bad_q)
+    assert e.value.code == 6
+    again = S.evaluate(btam.FP64)
+    for k in ("V0", "Rq", "Rs", "Rx"):
+        assert np.array_equal(again[k], base[k]), k
+
+
 def test_persistent_grid_bitwise_on_large_system(gpu_tables):
     """A system with more sites and pairs than one wave of resident blocks:
     the persistent grid computes most sites and pairs in later trips of its
