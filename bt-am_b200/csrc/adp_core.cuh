@@ -126,6 +126,10 @@ BTAM_HD int pr_stride(int pk) { return pk == 2 ? 16 : 8; }
 template <class R> BTAM_HD const R *uw_rec(const RadialView<R> &T, int pk, int m) {
   return T.uw + (size_t)kUWStride * ((size_t)T.n * pk + m);
 }
+// The same tables with the uw block staged in shared memory by the kernel
+// (FP32 only: 3 pair kinds x n segments x 32 bytes = 115 KB at n = 1194);
+// the pr block stays in global memory.
+template <class R> struct RadialViewS : RadialView<R> {};
 template <class R> BTAM_HD const R *pr_rec(const RadialView<R> &T, int pk, int m) {
   return T.pr + (size_t)8 * T.n * pk + (size_t)pr_stride(pk) * m;
 }
@@ -194,6 +198,21 @@ BTAM_HD void ld4(const double *p, double (&v)[4]) {
 // Plain 8-value copy (records staged in shared memory).
 template <class R> BTAM_HD void cp8(const R *p, R (&v)[8]) {
   for (int c = 0; c < 8; ++c) v[c] = p[c];
+}
+// 8 floats from a 32-byte-aligned record in shared memory (two 128-bit
+// shared loads; host: plain copy).
+BTAM_HD void lds8(const float *p, float (&v)[8]) {
+#if defined(__CUDA_ARCH__)
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
+               : "r"(a));
+  asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+               : "r"(a + 16));
+#else
+  for (int c = 0; c < 8; ++c) v[c] = p[c];
+#endif
 }
 
 template <class R> struct V3 {
@@ -288,15 +307,24 @@ BTAM_HD void norm_inv(float s2, float &s, float &inv) {
   s = s2 * inv;
 }
 
+// The uw record of pair kind pk, segment m: a read-only global load, or a
+// shared load when the view's uw block is staged in shared memory.
+template <class R> BTAM_HD void ld_uw(const RadialView<R> &T, int pk, int m, R (&k)[8]) {
+  ld8(uw_rec(T, pk, m), k);
+}
+BTAM_HD void ld_uw(const RadialViewS<float> &T, int pk, int m, float (&k)[8]) {
+  lds8(uw_rec<float>(T, pk, m), k);
+}
+
 // u, w of pair kind pk at one geometry (values and, when D, derivatives);
 // returns the segment (m, p) for the pair-rule record of the same geometry.
-template <class R, bool D>
-BTAM_HD int geo_uw(Geo<R> &g, const V3<R> &r, const RadialView<R> &T, int pk, R &p) {
+template <class R, bool D, class TV = RadialView<R>>
+BTAM_HD int geo_uw(Geo<R> &g, const V3<R> &r, const TV &T, int pk, R &p) {
   g.r = r;
   norm_inv(dot3(r, r), g.s, g.inv_s);
-  const int m = seg_of(T, g.s, p);
+  const int m = seg_of<R>(T, g.s, p);
   R k[8];
-  ld8(uw_rec(T, pk, m), k);
+  ld_uw(T, pk, m, k);
   if (D) {
     cub_vd(k, p, g.u, g.du);
     cub_vd(k + 4, p, g.w, g.dw);
@@ -873,8 +901,8 @@ BTAM_HD void pass2_pair(const RadialView<R> &T, const V3<R> &r0, R sig_u,
 // beta_j / beta_u, omega_ju = beta_u / beta_j; pr: the pair's record from
 // pair_rule_record (its 12 pair-rule points were evaluated once, in pass 1;
 // only the 13 triplet geometries are evaluated here).
-template <class R, class MU, class MJ>
-BTAM_HD void pass2_pair_sym(const RadialView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
+template <class R, class MU, class MJ, class TV>
+BTAM_HD void pass2_pair_sym(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
                             R xj, int cu, int cj, R embq_u, R embx_u, R embq_j, R embx_j,
                             R omega_uj, R omega_ju, const MU &mu, const MJ &mj,
                             const R (&pr)[kPrRec], Pass2Out<R> &ou, Pass2Out<R> &oj) {

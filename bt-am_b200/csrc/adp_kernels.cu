@@ -498,60 +498,88 @@ mf_stress_kernel(const EvalArgs<R> a, double *W0) {
   }
 }
 
-// One thread per owned slot p = (u, j): both directions of the pair from its
-// 25 geometries (pass2_pair_sym); u's part into slot p, j's part into the
+// One owned slot p = (u, j): both directions of the pair from its 25
+// geometries (pass2_pair_sym); u's part into slot p, j's part into the
 // reverse slot.  Pairs with an empty site give zero records, so every slot
 // of the real sites' lists is written exactly once per evaluation.
+template <class R, class TV>
+__device__ __forceinline__ void pass2u_one(const EvalArgs<R> &a, const TV &T, int t) {
+  const int p = a.own_p[t], u = a.own_u[t];
+  const int j = a.idx[p], r = a.rev[p];
+  const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
+  R vu[8], vj[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) vu[c] = vj[c] = (R)0;
+  if (su.active && sj.active) {
+    const int o = nb_owner(a, j);
+    const double bu = nb_beta(a, u), bj = nb_beta(a, j);
+    const MomRec<R, true> mu(a.mom + (size_t)u * kMomStride);
+    const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
+    Pass2Out<R> ou, oj;
+    ou.gq[0] = ou.gq[1] = ou.gq[2] = ou.gs = ou.gx = (R)0;
+    oj.gq[0] = oj.gq[1] = oj.gq[2] = oj.gs = oj.gx = (R)0;
+    R pr[kPrRec];
+    {
+      R v4[4];
+      ld4(a.prec1 + (size_t)kPr1 * t, v4);
+#pragma unroll
+      for (int c = 0; c < kPr1; ++c) pr[c] = v4[c];
+    }
+    const R *src = a.prec2 + (size_t)kPr2 * t;
+#pragma unroll
+    for (int h = 0; h < kPr2 / 8; ++h) {
+      R v[8];
+      ld8(src + 8 * h, v);
+#pragma unroll
+      for (int c = 0; c < 8; ++c) pr[kPr1 + 8 * h + c] = v[c];
+    }
+    pass2_pair_sym<R>(T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
+                      sj.code, mu.scalar(0), mu.scalar(1), mj.scalar(0), mj.scalar(1),
+                      (R)(bj / bu), (R)(bu / bj), mu, mj, pr, ou, oj);
+    vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
+    vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
+  }
+  // slot records: (gq, gs) as one 4-vector, gx in its own array
+  st_rec4(a.pbuf + 4 * (size_t)p, vu);
+  a.pgx[p] = vu[4];
+  if (r >= 0) {
+    st_rec4(a.pbuf + 4 * (size_t)r, vj);
+    a.pgx[r] = vj[4];
+  }
+}
+
+// One thread per owned slot (pass2u_one).
 template <class R, int TPB, int MB>
 __global__ void __launch_bounds__(TPB, MB)
 pass2u_pair_kernel(const EvalArgs<R> a) {
   // one copy of the body for every trip: a site or pair gives the same bits
   // whichever trip of whichever grid computes it
 #pragma unroll 1
-  for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
-    const int p = a.own_p[t], u = a.own_u[t];
-    const int j = a.idx[p], r = a.rev[p];
-    const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
-    R vu[8], vj[8];
-#pragma unroll
-    for (int c = 0; c < 8; ++c) vu[c] = vj[c] = (R)0;
-    if (su.active && sj.active) {
-      const int o = nb_owner(a, j);
-      const double bu = nb_beta(a, u), bj = nb_beta(a, j);
-      const MomRec<R, true> mu(a.mom + (size_t)u * kMomStride);
-      const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
-      Pass2Out<R> ou, oj;
-      ou.gq[0] = ou.gq[1] = ou.gq[2] = ou.gs = ou.gx = (R)0;
-      oj.gq[0] = oj.gq[1] = oj.gq[2] = oj.gs = oj.gx = (R)0;
-      R pr[kPrRec];
-      {
-        R v4[4];
-        ld4(a.prec1 + (size_t)kPr1 * t, v4);
-#pragma unroll
-        for (int c = 0; c < kPr1; ++c) pr[c] = v4[c];
-      }
-      const R *src = a.prec2 + (size_t)kPr2 * t;
-#pragma unroll
-      for (int h = 0; h < kPr2 / 8; ++h) {
-        R v[8];
-        ld8(src + 8 * h, v);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) pr[kPr1 + 8 * h + c] = v[c];
-      }
-      pass2_pair_sym<R>(a.T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
-                        sj.code, mu.scalar(0), mu.scalar(1), mj.scalar(0), mj.scalar(1),
-                        (R)(bj / bu), (R)(bu / bj), mu, mj, pr, ou, oj);
-      vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
-      vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
-    }
-    // slot records: (gq, gs) as one 4-vector, gx in its own array
-    st_rec4(a.pbuf + 4 * (size_t)p, vu);
-    a.pgx[p] = vu[4];
-    if (r >= 0) {
-      st_rec4(a.pbuf + 4 * (size_t)r, vj);
-      a.pgx[r] = vj[4];
-    }
-  }
+  for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
+    pass2u_one(a, a.T, t);
+}
+
+// The same with the uw block of the tables staged in shared memory (FP32,
+// 115 KB, one block of TPB threads per SM): the 13 triplet geometries of a
+// pair then gather their spline records from shared memory instead of L1.
+constexpr int kUWSharedMax = 3 * kUWStride * 1200;  // floats: up to 1200 segments
+template <int TPB>
+__global__ void __launch_bounds__(TPB, 1)
+pass2u_pair_smem_kernel(const EvalArgs<float> a) {
+  extern __shared__ __align__(32) float uw_s[];
+  const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 floats
+  for (int c = threadIdx.x; c < nuw / 4; c += TPB)
+    reinterpret_cast<float4 *>(uw_s)[c] = __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
+  __syncthreads();
+  RadialViewS<float> T;
+  T.uw = uw_s;
+  T.pr = a.T.pr;
+  T.dx = a.T.dx;
+  T.inv_dx = a.T.inv_dx;
+  T.n = a.T.n;
+#pragma unroll 1
+  for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
+    pass2u_one(a, T, t);
 }
 
 // One warp per site: compensated sum of its slot records in slot order,
@@ -746,6 +774,35 @@ void go2u(const EvalArgs<R> &a, cudaStream_t st, bool pers, cudaEvent_t mid) {
   ks<<<grid_of(ks, a.n_real, 4, pers), 128, 0, st>>>(a);
 }
 
+// Shared-memory variant of the undirected pass-2 pair kernel: FP32 tables
+// of up to 1200 segments, one block of 512 threads per SM (always a
+// persistent grid); otherwise (FP64, larger tables) the default shape.
+inline void go2u_smem(const EvalArgs<float> &a, cudaStream_t st, cudaEvent_t mid) {
+  constexpr int TPB = 512;
+  const size_t bytes = (size_t)3 * kUWStride * a.T.n * sizeof(float);
+  if (a.T.n > kUWSharedMax / (3 * kUWStride)) {
+    go2u<float, 128, 1>(a, st, false, mid);
+    return;
+  }
+  auto k = pass2u_pair_smem_kernel<TPB>;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(float) * kUWSharedMax));
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TPB, bytes);
+  int g = sms * (per > 0 ? per : 1);
+  const int full = nblocks(a.n_own, TPB);
+  g = g < full ? g : full;
+  if (g > 0) k<<<g, TPB, bytes, st>>>(a);
+  if (mid) cudaEventRecord(mid, st);
+  auto ks = pass2u_site_kernel<float, 4>;
+  ks<<<grid_of(ks, a.n_real, 4, true), 128, 0, st>>>(a);
+}
+inline void go2u_smem(const EvalArgs<double> &a, cudaStream_t st, cudaEvent_t mid) {
+  go2u<double, 128, 1>(a, st, false, mid);
+}
+
 template <class R>
 cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent_t mid) {
   if (a.n_real <= 0) return cudaSuccess;
@@ -755,6 +812,7 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent
     case 1: go2u<R, 128, 5>(a, st, pers, mid); break;
     case 2: go2u<R, 128, 4>(a, st, pers, mid); break;
     case 3: go2u<R, 256, 2>(a, st, pers, mid); break;
+    case 4: go2u_smem(a, st, mid); break;
     default: go2u<R, 128, 1>(a, st, pers, mid); break;
     }
     return cudaGetLastError();

@@ -46,7 +46,7 @@ def test_images_and_neighbors_bit_exact(gpu_tables, name):
 # launch variants (pass 1, pass 2): directed (each site over its neighbours)
 # and undirected (each pair once for both directions), full and persistent
 # grids
-VARIANTS = [(0, 0), (0, 16), (16, 16), (16 | 8 | 3, 16 | 8 | 2)]
+VARIANTS = [(0, 0), (0, 16), (16, 16), (16 | 8 | 3, 16 | 8 | 2), (16 | 8 | 3, 16 | 4)]
 
 
 @pytest.mark.parametrize("v", VARIANTS, ids=lambda v: f"v{v[0]}-{v[1]}")
@@ -130,8 +130,8 @@ def test_launch_variants(gpu_tables):
     for prec, tol in ((btam.FP64, 1e-12), (btam.FP32C, 1e-6)):
         base = S.evaluate(prec)
         for shape1, shape2 in ([(v, v) for v in range(5)] + [(0, 5)] +
-                               [(0, 16 | v) for v in range(4)] +
-                               [(16 | v, 16 | (v % 4)) for v in range(5)]):
+                               [(0, 16 | v) for v in range(5)] +
+                               [(16 | v, 16 | v) for v in range(5)]):
             for pers in (0, 8):
                 S.set_variants(prec, shape1 | pers, shape2 | pers)
                 out = S.evaluate(prec)
@@ -149,7 +149,7 @@ def test_launch_variants(gpu_tables):
                     assert np.abs(out[k] - base[k]).max() < 10 * tol, (prec, shape1, k)
         v1, v2 = S.autotune(prec)
         assert (v1 & 7) < 5 and v1 < 32 and v2 < 32
-        assert (v2 & 7) < (4 if v2 & 16 else 6)
+        assert (v2 & 7) < (5 if v2 & 16 else 6)
     with pytest.raises(btam.BtamError):
         S.set_variants(btam.FP64, 5, 0)
 
