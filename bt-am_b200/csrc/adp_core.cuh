@@ -537,8 +537,8 @@ template <class R> BTAM_HD R bpair_r(const Feat<R> &x, const Feat<R> &y) {
 //   [16..18] sum (A, B, C) sd over the j-moved points (sd = +-sqrt6 r_k),
 //   [19] 0.
 constexpr int kPr1 = 4, kPr2 = 16, kPrRec = kPr1 + kPr2;
-template <class R>
-BTAM_HD void pair_rule_record(const RadialView<R> &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
+template <class R, class TV>
+BTAM_HD void pair_rule_record(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
                               R xj, int cu, int cj, R (&rec)[kPrRec]) {
   const int pk = pair_kind(cu, cj);
   const R X = xu * xj;
@@ -581,8 +581,8 @@ BTAM_HD void pair_rule_record(const RadialView<R> &T, const V3<R> &r0, R sig_u, 
 // -+sqrt6 sigma_j e_k.  Returns x_j sum rho_{s_j} in *rho_j and, for the
 // reverse pair (j, i) whose points are the same set negated, x_i sum rho_{s_i}
 // in *rho_i when rho_i is not null.
-template <class R>
-BTAM_HD void pass1_pair_rule(const RadialView<R> &T, const V3<R> &r0, R sig_i, R sig_j, R xi,
+template <class R, class TV>
+BTAM_HD void pass1_pair_rule(const TV &T, const V3<R> &r0, R sig_i, R sig_j, R xi,
                              R xj, int ci, int cj, R &rho_j, R *rho_i, R &epair, R &ediag) {
   const int pk = pair_kind(ci, cj);
   const R X = xi * xj;
@@ -643,8 +643,8 @@ template <class R> BTAM_HD void feat_acc(R *acc, int base, const Geo<R> &g, R X)
 
 // Part I without the pair rule: g0 += X f(r0), hsum += X sum_{6} f,
 // cross += X^2 B(sum_6 f, f(r0)) over the neighbour-displaced points.
-template <class R>
-BTAM_HD void pass1_pair_part1(const RadialView<R> &T, const V3<R> &r0, R sig_j, R X, int pk,
+template <class R, class TV>
+BTAM_HD void pass1_pair_part1(const TV &T, const V3<R> &r0, R sig_j, R X, int pk,
                               R *acc) {
   Geo<R> g0;
   R p;
@@ -674,8 +674,8 @@ BTAM_HD void pass1_pair_part1(const RadialView<R> &T, const V3<R> &r0, R sig_j, 
 
 // Part II: G(d) += X f(r0 + d) for the six centre displacements d (part
 // index 1 + 9 d + c) and sself += X^2 sum_d B(f, f) (part index 0).
-template <class R>
-BTAM_HD void pass1_pair_part2(const RadialView<R> &T, const V3<R> &r0, R sig_i, R X, int pk,
+template <class R, class TV>
+BTAM_HD void pass1_pair_part2(const TV &T, const V3<R> &r0, R sig_i, R X, int pk,
                               R *acc) {
   const R amt_i = sig_i * (R)kDelta9;
   R ss = (R)0, p;

@@ -167,9 +167,38 @@ template <> __device__ __forceinline__ void st_rec4<double>(double *p, const dou
 // One thread per owned pair t = (u, j): the pair's 12-point pair-rule record
 // (pair_rule_record), shared by pass 1 of both sites and by pass 2.  Pairs
 // with an empty site get a zero record.
+// The tables as a kernel reads them.  SM (FP32 only): the uw block is first
+// copied into the block's dynamic shared memory by all its threads, so the
+// call must come before any thread leaves; the pr block stays in global
+// memory.
+template <class R, bool SM> struct KView { using type = RadialView<R>; };
+template <> struct KView<float, true> { using type = RadialViewS<float>; };
+constexpr int kUWSharedMax = 3 * kUWStride * 1200;  // floats: up to 1200 segments
+template <class R, bool SM>
+__device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArgs<R> &a) {
+  if constexpr (SM && sizeof(R) == 4) {
+    extern __shared__ __align__(32) float uw_dyn[];
+    const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 floats
+    for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x)
+      reinterpret_cast<float4 *>(uw_dyn)[c] =
+          __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
+    __syncthreads();
+    RadialViewS<float> T;
+    T.uw = uw_dyn;
+    T.pr = a.T.pr;
+    T.dx = a.T.dx;
+    T.inv_dx = a.T.inv_dx;
+    T.n = a.T.n;
+    return T;
+  } else {
+    return a.T;
+  }
+}
+
 template <class R, int TPB>
 __global__ void __launch_bounds__(TPB)
 pass1u_pair_kernel(const EvalArgs<R> a) {
+  const RadialView<R> &T = a.T;
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
     const int p = a.own_p[t], u = a.own_u[t];
@@ -177,7 +206,7 @@ pass1u_pair_kernel(const EvalArgs<R> a) {
     const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
     R rec[kPrRec];
     if (su.active && sj.active) {
-      pair_rule_record<R>(a.T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
+      pair_rule_record<R>(T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
                           sj.code, rec);
     } else {
 #pragma unroll
@@ -278,6 +307,7 @@ __global__ void __launch_bounds__(W * 32, MB)
 pass1_kernel(const EvalArgs<R> a) {
   constexpr int SPW = 32 / G;  // sites per warp
   __shared__ SiteSums ss[W * SPW];
+  const RadialView<R> &T = a.T;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int half = lane / G, sl = lane % G, gbase = half * G;
   // grid-stride over groups of SPW sites: one group per warp per trip (a full
@@ -316,13 +346,13 @@ pass1_kernel(const EvalArgs<R> a) {
         acc[kP1Ediag] += X * X * rec[3];
       } else {
         R rj, ep, ed;
-        pass1_pair_rule<R>(a.T, r0, (R)qi.w, sj.sigma, (R)xi, sj.occ, ci, cj, rj, nullptr, ep,
+        pass1_pair_rule<R>(T, r0, (R)qi.w, sj.sigma, (R)xi, sj.occ, ci, cj, rj, nullptr, ep,
                            ed);
         acc[kP1Rho] += rj;
         acc[kP1Epair] += ep;
         acc[kP1Ediag] += ed;
       }
-      pass1_pair_part1<R>(a.T, r0, sj.sigma, (R)xi * sj.occ, pair_kind(ci, cj), acc);
+      pass1_pair_part1<R>(T, r0, sj.sigma, (R)xi * sj.occ, pair_kind(ci, cj), acc);
     }
     lane_tree<G>(acc, lo, lane);
     const int v0 = tree_base<kP1PartI, G>(sl);
@@ -339,7 +369,7 @@ pass1_kernel(const EvalArgs<R> a) {
     for (int p = nb0 + sl; p < nb1; p += G) {
       const NbSite<R> sj = nb_site(a, a.idx[p]);
       if (!sj.active) continue;
-      pass1_pair_part2<R>(a.T, pair_vec<R>(qi, sj), (R)qi.w, (R)xi * sj.occ,
+      pass1_pair_part2<R>(T, pair_vec<R>(qi, sj), (R)qi.w, (R)xi * sj.occ,
                           pair_kind(ci, sj.code), acc);
     }
     lane_tree<G>(acc, lo, lane);
@@ -562,21 +592,10 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
 // The same with the uw block of the tables staged in shared memory (FP32,
 // 115 KB, one block of TPB threads per SM): the 13 triplet geometries of a
 // pair then gather their spline records from shared memory instead of L1.
-constexpr int kUWSharedMax = 3 * kUWStride * 1200;  // floats: up to 1200 segments
 template <int TPB>
 __global__ void __launch_bounds__(TPB, 1)
 pass2u_pair_smem_kernel(const EvalArgs<float> a) {
-  extern __shared__ __align__(32) float uw_s[];
-  const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 floats
-  for (int c = threadIdx.x; c < nuw / 4; c += TPB)
-    reinterpret_cast<float4 *>(uw_s)[c] = __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
-  __syncthreads();
-  RadialViewS<float> T;
-  T.uw = uw_s;
-  T.pr = a.T.pr;
-  T.dx = a.T.dx;
-  T.inv_dx = a.T.inv_dx;
-  T.n = a.T.n;
+  const auto T = kernel_view<float, true>(a);
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
     pass2u_one(a, T, t);
@@ -732,6 +751,20 @@ void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers, bool und, cudaEvent_t
     k<<<grid_of(k, n_groups, W, pers), W * 32, 0, st>>>(a);
   }
 }
+// Persistent grid of a kernel that holds `smem` bytes of dynamic shared
+// memory (the uw tables): as many blocks as fit on the device at once, at
+// most `full`.
+template <class K> int smem_grid(K kernel, int threads, size_t smem, int full) {
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(float) * kUWSharedMax));
+  int dev = 0, sms = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, smem);
+  const int g = sms * (per > 0 ? per : 1);
+  return g < full ? g : full;
+}
+
 template <class R, int W, int MB> void go2(const EvalArgs<R> &a, cudaStream_t st, bool pers) {
   auto k = pass2_kernel<R, W, MB>;
   k<<<grid_of(k, a.n_real, W, pers), W * 32, 0, st>>>(a);
@@ -779,21 +812,13 @@ void go2u(const EvalArgs<R> &a, cudaStream_t st, bool pers, cudaEvent_t mid) {
 // persistent grid); otherwise (FP64, larger tables) the default shape.
 inline void go2u_smem(const EvalArgs<float> &a, cudaStream_t st, cudaEvent_t mid) {
   constexpr int TPB = 512;
-  const size_t bytes = (size_t)3 * kUWStride * a.T.n * sizeof(float);
   if (a.T.n > kUWSharedMax / (3 * kUWStride)) {
     go2u<float, 128, 1>(a, st, false, mid);
     return;
   }
+  const size_t bytes = (size_t)3 * kUWStride * a.T.n * sizeof(float);
   auto k = pass2u_pair_smem_kernel<TPB>;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(sizeof(float) * kUWSharedMax));
-  int dev = 0, sms = 0, per = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, TPB, bytes);
-  int g = sms * (per > 0 ? per : 1);
-  const int full = nblocks(a.n_own, TPB);
-  g = g < full ? g : full;
+  const int g = smem_grid(k, TPB, bytes, nblocks(a.n_own, TPB));
   if (g > 0) k<<<g, TPB, bytes, st>>>(a);
   if (mid) cudaEventRecord(mid, st);
   auto ks = pass2u_site_kernel<float, 4>;
