@@ -48,12 +48,17 @@ LOOK_PR, LOOK_TRIP = 48.0, 26.0
 # (--set full) of the undirected variants (28, 26): DRAM bytes (read +
 # write), and L1 global-load sectors (32 bytes each) with the L1 LSU
 # data-pipe utilisation
-NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 112.6e6, "pass1 site kernel": 67.7e6,
-                  "pass2 pair kernel": 254.2e6, "pass2 site kernel": 75.1e6, "totals": 1.5e6}
+NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 112.4e6, "pass1 site kernel": 66.0e6,
+                  "pass2 pair kernel": 254.9e6, "pass2 site kernel": 75.0e6, "totals": 1.5e6}
 NCU_L1_SECTORS = {"pass1 pair-rule kernel": 51.73e6, "pass1 site kernel": 54.59e6,
-                  "pass2 pair kernel": 50.42e6, "pass2 site kernel": 2.56e6}
-NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.71,
-               "pass2 pair kernel": 0.66, "pass2 site kernel": 0.30}
+                  "pass2 pair kernel": 29.08e6, "pass2 site kernel": 2.56e6}
+NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.70,
+               "pass2 pair kernel": 0.745, "pass2 site kernel": 0.29}
+# shared-memory wavefronts per launch: the pass-2 pair kernel reads its u/w
+# spline records from shared memory (its global sectors are the moment and
+# pair records only)
+NCU_SHARED_WAVEFRONTS = {"pass1 pair-rule kernel": 0.45e6, "pass1 site kernel": 3.35e6,
+                         "pass2 pair kernel": 20.76e6, "pass2 site kernel": 1.37e6}
 
 
 def kernel_flops(undirected):
@@ -617,7 +622,8 @@ def run_btam(args, ws, rank, local):
                     "kernels": {k: {"sector_gbs": NCU_L1_SECTORS[k] * 32 / (prof[i] * 1e-3) / 1e9,
                                     "frac": NCU_L1_SECTORS[k] * 32 / (prof[i] * 1e-3) / 1e9 /
                                     gather_peak,
-                                    "ncu_data_pipe_frac": NCU_L1_PIPE[k]}
+                                    "ncu_data_pipe_frac": NCU_L1_PIPE[k],
+                                    "ncu_shared_wavefronts": NCU_SHARED_WAVEFRONTS[k]}
                                 for i, k in enumerate(names) if k in NCU_L1_SECTORS} if und
                     else None,
                     "sectors_source": "L1 global-load sectors per launch from one ncu capture"},
