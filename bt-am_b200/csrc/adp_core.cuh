@@ -199,21 +199,31 @@ BTAM_HD void ld4(const double *p, double (&v)[4]) {
 template <class R> BTAM_HD void cp8(const R *p, R (&v)[8]) {
   for (int c = 0; c < 8; ++c) v[c] = p[c];
 }
-// 8 floats from a 32-byte-aligned record in shared memory (two 128-bit
-// shared loads; host: plain copy).
-BTAM_HD void lds8(const float *p, float (&v)[8]) {
+// 8 floats of a 32-byte record in shared memory whose two 16-byte halves
+// are stored swapped when `swap` (two 128-bit shared loads; host: plain
+// copy).  Records stored with their halves swapped on every other group of
+// four spread the first loaded halves of random records over all eight
+// 16-byte bank groups instead of four.
+BTAM_HD void lds8(const float *p, bool swap, float (&v)[8]) {
 #if defined(__CUDA_ARCH__)
   const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  const unsigned a0 = swap ? a + 16 : a, a1 = swap ? a : a + 16;
   asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
                : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3])
-               : "r"(a));
+               : "r"(a0));
   asm volatile("ld.shared.v4.f32 {%0,%1,%2,%3}, [%4];"
                : "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
-               : "r"(a + 16));
+               : "r"(a1));
 #else
-  for (int c = 0; c < 8; ++c) v[c] = p[c];
+  const int o0 = swap ? 4 : 0, o1 = swap ? 0 : 4;
+  for (int c = 0; c < 4; ++c) {
+    v[c] = p[o0 + c];
+    v[4 + c] = p[o1 + c];
+  }
 #endif
 }
+// Whether record r (= n pk + m) of a staged uw block has its halves swapped.
+BTAM_HD bool uw_swapped(int r) { return ((r >> 2) & 1) != 0; }
 
 template <class R> struct V3 {
   R x, y, z;
@@ -313,7 +323,7 @@ template <class R> BTAM_HD void ld_uw(const RadialView<R> &T, int pk, int m, R (
   ld8(uw_rec(T, pk, m), k);
 }
 BTAM_HD void ld_uw(const RadialViewS<float> &T, int pk, int m, float (&k)[8]) {
-  lds8(uw_rec<float>(T, pk, m), k);
+  lds8(uw_rec<float>(T, pk, m), uw_swapped(T.n * pk + m), k);
 }
 
 // u, w of pair kind pk at one geometry (values and, when D, derivatives);

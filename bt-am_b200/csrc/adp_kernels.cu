@@ -179,9 +179,12 @@ __device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArg
   if constexpr (SM && sizeof(R) == 4) {
     extern __shared__ __align__(32) float uw_dyn[];
     const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 floats
-    for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x)
-      reinterpret_cast<float4 *>(uw_dyn)[c] =
+    // 16-byte halves c of record c / 2, stored swapped where uw_swapped says
+    for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x) {
+      const int dst = uw_swapped(c >> 1) ? (c ^ 1) : c;
+      reinterpret_cast<float4 *>(uw_dyn)[dst] =
           __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
+    }
     __syncthreads();
     RadialViewS<float> T;
     T.uw = uw_dyn;
