@@ -719,6 +719,192 @@ void DV_dq(const View &v, int u, int i, double *out3) {
   for (int a = 0; a < 3; ++a) out3[a] = v.x[i] * dF * drho[a] + pair[a] + dip[a] + quad[a];
 }
 
+// ---- second derivatives of the point terms, restated from the terms'
+// definitions (the reference's d2F_dq2 slots, MgHx-ADP.cpp:664-735,
+// 1030-1090, 1380-1600, 2040-2300).  Only the diagonal blocks d2/dq_a^2 of
+// one slot a are needed; with r = q_0 - q_k every block is a second
+// derivative in r_k (the sign of dr/dq cancels).
+
+// H += c (f'' rr^T/s^2 + f' (I - rr^T/s^2)/s): the Hessian of c f(|r|).
+void radial_hess(const double *r, double s, double d1, double d2, double c, double *H) {
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const double rr = r[a] * r[b] / (s * s);
+      H[3 * a + b] += c * (d2 * rr + d1 * ((a == b ? 1.0 : 0.0) - rr) / s);
+    }
+}
+
+// sum_al m_al d2 A_al / dr dr with A = c u(|r|) r:
+//   c [u' (m r^T + r m^T)/s + (m.r)(u'' rr^T/s^2 + u' (I - rr^T/s^2)/s)]
+void vec_hess(const double *m, const double *r, double s, double u1, double u2, double c,
+              double *H) {
+  const double mr = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const double rr = r[a] * r[b] / (s * s);
+      H[3 * a + b] += c * (u1 * (m[a] * r[b] + r[a] * m[b]) / s +
+                           mr * (u2 * rr + u1 * ((a == b ? 1.0 : 0.0) - rr) / s));
+    }
+}
+
+// sum_ab M_ab d2 B_ab / dr dr with B = c w(|r|) r r^T (M symmetric):
+//   c [(r^T M r)(w'' rr^T/s^2 + w' (I - rr^T/s^2)/s)
+//      + 2 w' (r (Mr)^T + (Mr) r^T)/s + 2 w M]
+void ten_hess(const double *M, const double *r, double s, double w0, double w1, double w2,
+              double c, double *H) {
+  double Mr[3];
+  for (int a = 0; a < 3; ++a) Mr[a] = M[3 * a] * r[0] + M[3 * a + 1] * r[1] + M[3 * a + 2] * r[2];
+  const double rMr = r[0] * Mr[0] + r[1] * Mr[1] + r[2] * Mr[2];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const double rr = r[a] * r[b] / (s * s);
+      H[3 * a + b] += c * (rMr * (w2 * rr + w1 * ((a == b ? 1.0 : 0.0) - rr) / s) +
+                           2.0 * w1 * (r[a] * Mr[b] + Mr[a] * r[b]) / s + 2.0 * w0 * M[3 * a + b]);
+    }
+}
+
+// d2/dq_a^2 of V_dip(0, 1, 2) = 1/2 A1.A2, A_k = n0 n_k u(|r_k|) r_k: block
+// a = 0 moves both r_k, blocks 1 and 2 move r_1 or r_2 alone.
+void dip_d2(int a, const double *n, const double *q, const int *spc, double *H) {
+  for (int c = 0; c < 9; ++c) H[c] = 0.0;
+  Tri t = tri_geom(q);
+  const Spline &S1 = pot_of(spc[0], spc[1]).u, &S2 = pot_of(spc[0], spc[2]).u;
+  const double c1 = n[0] * n[1], c2 = n[0] * n[2];
+  const double u1 = spline_val(S1, t.n1), du1 = spline_d1(S1, t.n1), dd1 = spline_d2(S1, t.n1);
+  const double u2 = spline_val(S2, t.n2), du2 = spline_d1(S2, t.n2), dd2 = spline_d2(S2, t.n2);
+  double A1[3], A2[3];
+  for (int k = 0; k < 3; ++k) {
+    A1[k] = c1 * u1 * t.r1[k];
+    A2[k] = c2 * u2 * t.r2[k];
+  }
+  double h[9] = {0};
+  if (a == 0 || a == 1) vec_hess(A2, t.r1, t.n1, du1, dd1, c1, h);
+  if (a == 0 || a == 2) vec_hess(A1, t.r2, t.n2, du2, dd2, c2, h);
+  if (a == 0) {  // J1^T J2 + J2^T J1, J_k = c_k (u I + u' r r^T / s)
+    double J1[9], J2[9];
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) {
+        J1[3 * x + y] = c1 * ((x == y ? u1 : 0.0) + du1 * t.r1[x] * t.r1[y] / t.n1);
+        J2[3 * x + y] = c2 * ((x == y ? u2 : 0.0) + du2 * t.r2[x] * t.r2[y] / t.n2);
+      }
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y)
+        for (int z = 0; z < 3; ++z)
+          h[3 * x + y] += J1[3 * z + x] * J2[3 * z + y] + J2[3 * z + x] * J1[3 * z + y];
+  }
+  for (int c = 0; c < 9; ++c) H[c] = 0.5 * h[c];
+}
+
+// d2/dq_a^2 of V_quad(0, 1, 2) = 1/2 B1:B2 - 1/6 t1 t2, B_k = n0 n_k w r_k r_k^T,
+// t_k = tr B_k = n0 n_k w s_k^2.
+void quad_d2(int a, const double *n, const double *q, const int *spc, double *H) {
+  for (int c = 0; c < 9; ++c) H[c] = 0.0;
+  Tri t = tri_geom(q);
+  const Spline &S1 = pot_of(spc[0], spc[1]).w, &S2 = pot_of(spc[0], spc[2]).w;
+  const double c1 = n[0] * n[1], c2 = n[0] * n[2];
+  const double w1 = spline_val(S1, t.n1), dw1 = spline_d1(S1, t.n1), ddw1 = spline_d2(S1, t.n1);
+  const double w2 = spline_val(S2, t.n2), dw2 = spline_d1(S2, t.n2), ddw2 = spline_d2(S2, t.n2);
+  double B1[9], B2[9];
+  for (int x = 0; x < 3; ++x)
+    for (int y = 0; y < 3; ++y) {
+      B1[3 * x + y] = c1 * w1 * t.r1[x] * t.r1[y];
+      B2[3 * x + y] = c2 * w2 * t.r2[x] * t.r2[y];
+    }
+  const double t1 = c1 * w1 * t.r1sq, t2 = c2 * w2 * t.r2sq;
+  // trace terms: h(s) = w s^2, h' = w' s^2 + 2 w s, h'' = w'' s^2 + 4 w' s + 2 w
+  const double hp1 = dw1 * t.r1sq + 2.0 * w1 * t.n1, hpp1 = ddw1 * t.r1sq + 4.0 * dw1 * t.n1 + 2.0 * w1;
+  const double hp2 = dw2 * t.r2sq + 2.0 * w2 * t.n2, hpp2 = ddw2 * t.r2sq + 4.0 * dw2 * t.n2 + 2.0 * w2;
+  double h[9] = {0};
+  if (a == 0 || a == 1) {
+    ten_hess(B2, t.r1, t.n1, w1, dw1, ddw1, 0.5 * c1, h);
+    radial_hess(t.r1, t.n1, hp1, hpp1, -t2 * c1 / 6.0, h);
+  }
+  if (a == 0 || a == 2) {
+    ten_hess(B1, t.r2, t.n2, w2, dw2, ddw2, 0.5 * c2, h);
+    radial_hess(t.r2, t.n2, hp2, hpp2, -t1 * c2 / 6.0, h);
+  }
+  if (a == 0) {
+    // 1/2 (dB1:dB2 + dB2:dB1) - 1/6 (grad t1 grad t2^T + grad t2 grad t1^T)
+    double G[9] = {0};  // sum_ab dB1_ab/dr_x dB2_ab/dr_y
+    const double d12 = t.dot;
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y)
+        G[3 * x + y] = c1 * c2 *
+                       (dw1 * dw2 * (t.r1[x] / t.n1) * (t.r2[y] / t.n2) * d12 * d12 +
+                        2.0 * dw1 * w2 * (t.r1[x] / t.n1) * t.r1[y] * d12 +
+                        2.0 * w1 * dw2 * t.r2[x] * (t.r2[y] / t.n2) * d12 +
+                        2.0 * w1 * w2 * ((x == y ? d12 : 0.0) + t.r2[x] * t.r1[y]));
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) {
+        const double g1x = c1 * hp1 * t.r1[x] / t.n1, g1y = c1 * hp1 * t.r1[y] / t.n1;
+        const double g2x = c2 * hp2 * t.r2[x] / t.n2, g2y = c2 * hp2 * t.r2[y] / t.n2;
+        h[3 * x + y] += 0.5 * (G[3 * x + y] + G[3 * y + x]) - (g1x * g2y + g2x * g1y) / 6.0;
+      }
+  }
+  for (int c = 0; c < 9; ++c) H[c] = h[c];
+}
+
+// evaluate_D2V_i_Dq2_u_MgHx (MgHx-mf-V-bulk.cpp:333-528): d2V_i/dq_u^2 as
+// the reference forms it, from the diagonal blocks of the slots holding u
+// (for j1 = j2 = u the two slot blocks, without their cross blocks).
+void D2V_dq2(const View &v, int u, int i, double *out9) {
+  for (int c = 0; c < 9; ++c) out9[c] = 0.0;
+  if (v.x[u] < kMinOcc) return;  // 354-357
+  if (v.x[i] < kMinOcc) return;  // 380-383
+  double drho[3] = {0, 0, 0}, d2rho[9] = {0}, pair[9] = {0}, dip[9] = {0}, quad[9] = {0};
+  const int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    const int j1 = v.idx[k1];
+    if (v.x[j1] <= kMinOcc) continue;  // 398-400
+    double qq[6], nn[2] = {v.x[i], v.x[j1]};
+    int sp[2] = {v.spc[i], v.spc[j1]}, sites2[2] = {i, j1};
+    for (int a = 0; a < 3; ++a) {
+      qq[a] = v.q[3 * i + a];
+      qq[3 + a] = v.q[3 * j1 + a];
+    }
+    double r[3], s2 = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      r[a] = qq[a] - qq[3 + a];
+      s2 += sq(r[a]);
+    }
+    const double s = std::sqrt(s2);
+    for (int dir = 0; dir < 2; ++dir) {
+      if (sites2[dir] != u) continue;
+      double g[3];
+      rho_dq(dir, g, nn, qq, sp);
+      for (int a = 0; a < 3; ++a) drho[a] += g[a];
+      const Spline &R = rho_of(sp[1]), &P = pot_of(sp[0], sp[1]).pair;
+      radial_hess(r, s, spline_d1(R, s), spline_d2(R, s), nn[1], d2rho);
+      radial_hess(r, s, spline_d1(P, s), spline_d2(P, s), 0.5 * nn[0] * nn[1], pair);
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      const int j2 = v.idx[k2];
+      if (v.x[j2] <= kMinOcc) continue;  // 452-454
+      int sites3[3] = {i, j1, j2};
+      if (sites3[0] != u && sites3[1] != u && sites3[2] != u) continue;
+      double q3[9], n3[3] = {v.x[i], v.x[j1], v.x[j2]};
+      int sp3[3] = {v.spc[i], v.spc[j1], v.spc[j2]};
+      for (int k = 0; k < 3; ++k)
+        for (int a = 0; a < 3; ++a) q3[3 * k + a] = v.q[3 * sites3[k] + a];
+      const double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        if (sites3[dir] != u) continue;
+        double h[9];
+        dip_d2(dir, n3, q3, sp3, h);
+        for (int c = 0; c < 9; ++c) dip[c] += f * h[c];
+        quad_d2(dir, n3, q3, sp3, h);
+        for (int c = 0; c < 9; ++c) quad[c] += f * h[c];
+      }
+    }
+  }
+  const Spline &E = embed_of(v.spc[i]);
+  const double dF = spline_d1(E, v.rho[i]), ddF = spline_d2(E, v.rho[i]);  // 512-519
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      out9[3 * a + b] = v.x[i] * ddF * drho[a] * drho[b] + v.x[i] * dF * d2rho[3 * a + b] +
+                        pair[3 * a + b] + dip[3 * a + b] + quad[3 * a + b];
+}
+
 // evaluate_DV_i_dF_MgHx (MgHx-mf-V-bulk.cpp:530-704): sum over the sites a
 // of every term of V_i of dV_i/dq_a (x) q0_a, 3x3 row-major (row: gradient
 // component, column: reference-position component).
@@ -1058,6 +1244,14 @@ void orc_mf_DV0_dF(int n, const double *q, const double *q0, const double *sigma
   (void)n;
   View v{q, sigma, x, rho, spc, offs, idx};
   par_for(nsites, [&](int k) { DV0_dF(v, q0, sites[k], out9 + 9 * k); });
+}
+
+void orc_pt_D2V_pairs(int n, const double *q, const double *x, const int *spc,
+                      const double *rho, const int *offs, const int *idx, const int *u_list,
+                      const int *i_list, int npairs, double *out9) {
+  (void)n;
+  View v{q, nullptr, x, rho, spc, offs, idx};
+  par_for(npairs, [&](int k) { D2V_dq2(v, u_list[k], i_list[k], out9 + 9 * k); });
 }
 
 void orc_residuals(int n, const double *q, const double *sigma,

@@ -80,6 +80,12 @@ void orc_pt_DV_dF(int n, const double *q, const double *q0, const double *x, con
                   const double *rho, const int *offs, const int *idx, const int *sites,
                   int nsites, double *out9);
 
+/* Non-mean-field d2V_i/dq_u^2 per (u, i) pair, 9 values row-major, as
+ * evaluate_D2V_i_Dq2_u_MgHx (MgHx-mf-V-bulk.cpp:333-528) forms it. */
+void orc_pt_D2V_pairs(int n, const double *q, const double *x, const int *spc,
+                      const double *rho, const int *offs, const int *idx, const int *u_list,
+                      const int *i_list, int npairs, double *out9);
+
 /* Mean-field stretch derivative dV0_i/dF per site, 9 values row-major,
  * with reference positions q0 of every site (evaluate_DV0_i_dF_bulk_MgHx,
  * MgHx-mf-V-bulk.cpp:2329-2552); rho: the mean-field density of every site. */

@@ -149,6 +149,17 @@ class Lib:
         return out
 
 
+    def pt_D2V_pairs(self, s, rho, offs, idx, u_list, i_list):
+        """d2V_i/dq_u^2 per (u, i) pair, 3x3 (evaluate_D2V_i_Dq2_u_MgHx)."""
+        u_list = np.ascontiguousarray(u_list, np.int32)
+        i_list = np.ascontiguousarray(i_list, np.int32)
+        out = np.zeros((len(u_list), 3, 3))
+        self._f("pt_D2V_pairs")(len(s["x"]), _d(s["q"]), _d(s["x"]), _i(s["species"]),
+                                _d(rho), _i(offs), _i(idx), _i(u_list), _i(i_list),
+                                len(u_list), _d(out))
+        return out
+
+
 class Oracle(Lib):
     """The restated oracle plus its project-defined pieces."""
 

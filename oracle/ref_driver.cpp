@@ -344,4 +344,21 @@ void ref_mf_DV0_dF(int n, const double *q, const double *q0, const double *sigma
   free(s.spc);
 }
 
+// evaluate_D2V_i_Dq2_u_MgHx (MgHx-mf-V-bulk.cpp:333-528): 9 values per
+// (u, i) pair, row-major; rho is the non-mean-field density of every site.
+void ref_pt_D2V_pairs(int n, const double *q, const double *x, const int *spc,
+                      const double *rho, const int *offs, const int *idx, const int *u_list,
+                      const int *i_list, int npairs, double *out9) {
+  Sys s;
+  make_sys(s, n, q, nullptr, x, spc, offs, idx);
+  for (int i = 0; i < n; ++i) s.rho(i) = rho[i];
+  parallel_for(npairs, [&](int k) {
+    int u = u_list[k], i = i_list[k];
+    Eigen::Matrix3d g = evaluate_D2V_i_Dq2_u_MgHx(u, i, s.q, s.x, s.rho, s.spc, topo(s, i));
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) out9[9 * k + 3 * a + b] = g(a, b);
+  });
+  free(s.spc);
+}
+
 } // extern "C"

@@ -117,7 +117,7 @@ def point_fixture(ref):
     reference's own evaluate_rho_i / evaluate_DV_i_Dq_u_adp_MgHx /
     evaluate_DV_i_dF_MgHx, on the neighbour lists stored in each fixture:
     the assembled gradient sum_{i in {u} U N(u)} dV_i/dq_u of every real
-    site, dV_i/dF with q0 = q, and dV_i/dF after the stretch PT_STRETCH
+    site, the same sum of evaluate_D2V_i_Dq2_u_MgHx, dV_i/dF with q0 = q, and dV_i/dF after the stretch PT_STRETCH
     (q0 = the unstretched positions, neighbour lists kept); and the
     mean-field stretch derivative evaluate_DV0_i_dF_bulk_MgHx at q0 = q and
     after the same stretch (with the mean-field rho-bar there)."""
@@ -138,12 +138,18 @@ def point_fixture(ref):
                              np.array([p[2] for p in plan], np.int32))
         Fq = np.zeros((n, 3))
         np.add.at(Fq, kk, g3)
+        # the Hessian blocks of evaluate_D2V_i_Dq2_u_MgHx, summed the same way
+        h9 = ref.pt_D2V_pairs(full, rho[owner], offs, idx,
+                              np.array([p[1] for p in plan], np.int32),
+                              np.array([p[2] for p in plan], np.int32))
+        H = np.zeros((n, 3, 3))
+        np.add.at(H, kk, h9)
         W = ref.pt_DV_dF(full, full["q"], rho[owner], offs, idx, real)
         st = dict(full)
         st["q"] = np.ascontiguousarray(full["q"] * PT_STRETCH)
         rho_s = ref.rho_nmf(st, offs, idx, real)
         W_s = ref.pt_DV_dF(st, full["q"], rho_s[owner], offs, idx, real)
-        out.update({f"{name}_rho": rho, f"{name}_Fq": Fq, f"{name}_W": W,
+        out.update({f"{name}_rho": rho, f"{name}_Fq": Fq, f"{name}_W": W, f"{name}_H": H,
                     f"{name}_rho_s": rho_s, f"{name}_W_s": W_s})
         # the mean-field stretch derivative (evaluate_DV0_i_dF_bulk_MgHx),
         # sigma and x held, at q0 = q and after the stretch

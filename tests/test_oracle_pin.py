@@ -135,6 +135,13 @@ def test_point_forms_against_golden(oracle, name):
     Fq = np.zeros((n, 3))
     np.add.at(Fq, np.array([q[0] for q in plan]), g3)
     assert np.array_equal(Fq, p[f"{name}_Fq"])
+    # Hessian blocks: restated from the terms' definitions, not line by line,
+    # so they agree with the reference to rounding
+    h9 = oracle.pt_D2V_pairs(full, rho[owner], offs, idx, [q[1] for q in plan],
+                             [q[2] for q in plan])
+    H = np.zeros((n, 3, 3))
+    np.add.at(H, np.array([q[0] for q in plan]), h9)
+    assert np.abs(H - p[f"{name}_H"]).max() <= 1e-12 * max(1.0, np.abs(p[f"{name}_H"]).max())
     W = oracle.pt_DV_dF(full, full["q"], rho[owner], offs, idx, real)
     assert np.array_equal(W, p[f"{name}_W"])
     st = dict(full, q=np.ascontiguousarray(full["q"] * p["stretch"]))
