@@ -70,6 +70,7 @@ _PROTOS = {
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
     "btam_pt_eval": (ctypes.c_int, [_V, _D, _D, _D, _D, _D]),
     "btam_stretch_apply": (ctypes.c_int, [_V, _D]),
+    "btam_pt_hessian": (ctypes.c_int, [_V, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
@@ -434,6 +435,13 @@ class System:
         _check(lib().btam_pt_eval(self.handle, _d(out["rho"]), _d(out["V"]), _d(out["Fq"]),
                                   _d(out["W"]), _d(out["totals"])), "btam_pt_eval")
         return out
+
+    def pt_hessian(self):
+        """Hessian blocks of the non-mean-field forms, (n, 3, 3): the sum over
+        i in {u} U N(u) of evaluate_D2V_i_Dq2_u_MgHx."""
+        H = np.zeros((self.n, 3, 3))
+        _check(lib().btam_pt_hessian(self.handle, _d(H)), "btam_pt_hessian")
+        return H
 
     def stretch(self, F):
         """q <- diag(F) q, cell and origin likewise; neighbour lists kept."""

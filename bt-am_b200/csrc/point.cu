@@ -195,6 +195,208 @@ __global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a) {
   }
 }
 
+// ---- Hessian blocks of the point forms (evaluate_D2V_i_Dq2_u_MgHx,
+// MgHx-mf-V-bulk.cpp:333-528), summed over i in {u} U N(u).  Through the
+// moments (r = q_nb - q_c, P = r r^T / s^2, Q = (I - P) / s):
+//   i = u: the full Hessian of V_u in q_u,
+//     x F'' g g^T + K^T K + sum_ab dLambda_ab dLambda_ab^T - 1/3 T T^T   (pass 1b)
+//     + per neighbour, linear in u's record (pass 2b):
+//       e x_j rho_j-Hessian + 1/2 t phi-Hessian + mu . d2(a_j) + Lambda : d2(b_j)
+//       - 1/3 tr Lambda d2(tr b_j),
+//     g = sum drho/dq, K = dmu/dq, dLambda/dq, T = d tr Lambda/dq;
+//   i = neighbour j: the reference sums the diagonal slot blocks of u in
+//     V_j's terms, whose triplet parts are linear in j's moments (for
+//     j1 = j2 = u it adds the two slot blocks without their cross blocks):
+//       x_j F''(rho_j) (x_u rho_u')^2 P + e_j x_u rho_u-Hessian + 1/2 t phi-Hessian
+//       + mu_j . d2(a_u) + Lambda_j : d2(b_u) - 1/3 tr Lambda_j d2(tr b_u).
+// a = t u(s) r, b = t w(s) r r^T with t = x_c x_nb.
+
+// Spline value and first and second derivatives of a segment record.
+__device__ __forceinline__ void cub_vdd(const double *k, double p, double &v, double &d1,
+                                        double &d2) {
+  v = k[0] + (k[1] + (k[2] + k[3] * p) * p) * p;
+  d1 = k[1] + (2.0 * k[2] + 3.0 * k[3] * p) * p;
+  d2 = 2.0 * k[2] + 6.0 * k[3] * p;
+}
+
+struct PtSpl {
+  double s, u, du, ddu, w, dw, ddw, ph, dph, ddph;
+  double rn, drn, ddrn;  // rho of the neighbour's species
+  double rc, drc, ddrc;  // rho of the centre's species
+};
+
+// Every spline of pair kind pk at |r| = s, with second derivatives.
+__device__ __forceinline__ PtSpl pt_splines(const RadialView<double> &T, int pk, int cc, int cn,
+                                            double s) {
+  PtSpl o;
+  o.s = s;
+  double p;
+  const int m = seg_of(T, s, p);
+  double k[8];
+  ld8(uw_rec(T, pk, m), k);
+  cub_vdd(k, p, o.u, o.du, o.ddu);
+  cub_vdd(k + 4, p, o.w, o.dw, o.ddw);
+  const double *pr = pr_rec(T, pk, m);
+  double h[8];
+  ld8(pr, h);
+  cub_vdd(h, p, o.ph, o.dph, o.ddph);
+  double hr[4];
+  const int on = rho_off(pk, cn), oc = rho_off(pk, cc);
+  for (int c = 0; c < 4; ++c) hr[c] = pr[on + c];
+  cub_vdd(hr, p, o.rn, o.drn, o.ddrn);
+  for (int c = 0; c < 4; ++c) hr[c] = pr[oc + c];
+  cub_vdd(hr, p, o.rc, o.drc, o.ddrc);
+  return o;
+}
+
+// Symmetric 3x3 as xx yy zz yz xz xy.
+__device__ __forceinline__ int sym6(int a, int b) {
+  return a == b ? a : (a + b == 3 ? 3 : (a + b == 2 ? 4 : 5));
+}
+
+// Adds the terms linear in a centre's record m (e = x_c F'(rho_c), mu,
+// Lambda, tr Lambda) for the neighbour at r, plus f P with the given radial
+// coefficients: c_rad = the coefficient pair (c'', c') of P and Q.
+__device__ __forceinline__ void pt_hess_linear(const double (&m)[kPtRec], const double *r,
+                                               const PtSpl &S, double t, double cpp,
+                                               double cp, double (&H)[6]) {
+  const double s = S.s, is = 1.0 / s;
+  const double mu[3] = {m[2], m[3], m[4]};
+  const double L[9] = {m[5], m[10], m[9], m[10], m[6], m[8], m[9], m[8], m[7]};
+  double Lr[3];
+  for (int a = 0; a < 3; ++a) Lr[a] = L[3 * a] * r[0] + L[3 * a + 1] * r[1] + L[3 * a + 2] * r[2];
+  const double mr = mu[0] * r[0] + mu[1] * r[1] + mu[2] * r[2];
+  const double rLr = r[0] * Lr[0] + r[1] * Lr[1] + r[2] * Lr[2];
+  const double hp = S.dw * s * s + 2.0 * S.w * s, hpp = S.ddw * s * s + 4.0 * S.dw * s + 2.0 * S.w;
+  // coefficients of P and Q
+  const double cP = cpp + t * mr * S.ddu + t * rLr * S.ddw - m[11] * t * hpp / 3.0;
+  const double cQ = cp + t * mr * S.du + t * rLr * S.dw - m[11] * t * hp / 3.0;
+  for (int a = 0; a < 3; ++a)
+    for (int b = a; b < 3; ++b) {
+      const double P = r[a] * r[b] * is * is;
+      const double Q = ((a == b ? 1.0 : 0.0) - P) * is;
+      H[sym6(a, b)] += cP * P + cQ * Q + t * S.du * (mu[a] * r[b] + r[a] * mu[b]) * is +
+                       2.0 * t * S.dw * (r[a] * Lr[b] + Lr[a] * r[b]) * is +
+                       2.0 * t * S.w * L[3 * a + b];
+    }
+}
+
+// Pass 1b: the self products of site i and x_i F''(rho_i) into hrec (8 per
+// site: x F'', then the six entries of x F'' g g^T + K^T K + sum dL dL^T -
+// T T^T / 3).
+__global__ void __launch_bounds__(128) pt_hself_kernel(PtArgs a, double *hrec) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= a.n_real) return;
+  const double xi = a.xb[i].x;
+  const int ci = a.code[i];
+  // g (3), K (6 sym), dLambda (6 entries x 3), T (3)
+  double acc[30];
+#pragma unroll
+  for (int c = 0; c < 30; ++c) acc[c] = 0.0;
+  if (!(xi < kMinOcc)) {
+    const double4 qi = a.pos[i];
+    for (int p = a.offs[i] + lane; p < a.offs[i + 1]; p += 32) {
+      const int j = a.idx[p];
+      const double xj = a.xb[j].x;
+      if (xj < kMinOcc) continue;
+      const double4 qj = a.pos[j];
+      const int cj = a.code[j], pk = pair_kind(ci, cj);
+      const double r[3] = {qj.x - qi.x, qj.y - qi.y, qj.z - qi.z};
+      const double s = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]), is = 1.0 / s;
+      const PtSpl S = pt_splines(a.T, pk, ci, cj, s);
+      const double t = xi * xj;
+      for (int c = 0; c < 3; ++c) acc[c] += xj * S.drn * r[c] * is;
+      for (int x = 0; x < 3; ++x)
+        for (int y = x; y < 3; ++y)
+          acc[3 + sym6(x, y)] += t * ((x == y ? S.u : 0.0) + S.du * r[x] * r[y] * is);
+      for (int x = 0; x < 3; ++x)
+        for (int y = x; y < 3; ++y)
+          for (int g = 0; g < 3; ++g)
+            acc[9 + 3 * sym6(x, y) + g] +=
+                t * (S.dw * r[g] * is * r[x] * r[y] +
+                     S.w * ((x == g ? r[y] : 0.0) + (y == g ? r[x] : 0.0)));
+      const double hp = S.dw * s * s + 2.0 * S.w * s;
+      for (int c = 0; c < 3; ++c) acc[27 + c] += t * hp * r[c] * is;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 30; ++c) acc[c] = wsum(acc[c]);
+  if (lane == 0) {
+    double o[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (!(xi < kMinOcc)) {
+      const double rho = a.rec[(size_t)kPtRec * i];
+      double F, dF, ddF;
+      const SplineView<double> &E = ci == 0 ? a.emb_mg : a.emb_h;
+      int m = (int)(rho * E.inv_dx);
+      m = m < E.n - 1 ? m : E.n - 1;
+      const double pp = fmin(rho - (double)m * E.dx, E.dx);
+      const double k[4] = {E.c[m].a, E.c[m].b, E.c[m].c, E.c[m].d};
+      cub_vdd(k, pp, F, dF, ddF);
+      const double f = xi * ddF;
+      o[0] = f;
+      double K[9];
+      for (int x = 0; x < 3; ++x)
+        for (int y = 0; y < 3; ++y) K[3 * x + y] = acc[3 + sym6(x, y)];
+      for (int x = 0; x < 3; ++x)
+        for (int y = x; y < 3; ++y) {
+          double v = f * acc[x] * acc[y] - acc[27 + x] * acc[27 + y] / 3.0;
+          for (int z = 0; z < 3; ++z) v += K[3 * z + x] * K[3 * z + y];
+          for (int e = 0; e < 6; ++e)
+            v += (e < 3 ? 1.0 : 2.0) * acc[9 + 3 * e + x] * acc[9 + 3 * e + y];
+          o[1 + sym6(x, y)] = v;
+        }
+    }
+    double4 *d = reinterpret_cast<double4 *>(hrec + 8 * (size_t)i);
+    d[0] = make_double4(o[0], o[1], o[2], o[3]);
+    d[1] = make_double4(o[4], o[5], o[6], o[7]);
+  }
+}
+
+// Pass 2b: H_u (9 per real site) = the self products + the neighbours'
+// linear terms of both kinds.
+__global__ void __launch_bounds__(128) pt_hess_kernel(PtArgs a, const double *hrec, double *H) {
+  const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (u >= a.n_real) return;
+  const double xu = a.xb[u].x;
+  const int cu = a.code[u];
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (!(xu < kMinOcc)) {
+    double mu_[kPtRec];
+    ld_rec(a.rec + (size_t)kPtRec * u, mu_);
+    const double4 qu = a.pos[u];
+    for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
+      const int j = a.idx[p];
+      const double xj = a.xb[j].x;
+      if (xj < kMinOcc) continue;
+      const double4 qj = a.pos[j];
+      const int cj = a.code[j], pk = pair_kind(cu, cj), o = a.owner[j];
+      const double r[3] = {qj.x - qu.x, qj.y - qu.y, qj.z - qu.z};
+      const double rn[3] = {-r[0], -r[1], -r[2]};
+      const double s = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      const PtSpl S = pt_splines(a.T, pk, cu, cj, s);
+      const double t = xu * xj;
+      // V_u's terms: embedding and pair radial parts, then the moment parts
+      pt_hess_linear(mu_, r, S, t, mu_[1] * xj * S.ddrn + 0.5 * t * S.ddph,
+                     mu_[1] * xj * S.drn + 0.5 * t * S.dph, acc);
+      // V_j's terms (j's owner record)
+      double mo[kPtRec];
+      ld_rec(a.rec + (size_t)kPtRec * o, mo);
+      const double fj = hrec[8 * (size_t)o];
+      pt_hess_linear(mo, rn, S, t,
+                     fj * (xu * S.drc) * (xu * S.drc) + mo[1] * xu * S.ddrc + 0.5 * t * S.ddph,
+                     mo[1] * xu * S.drc + 0.5 * t * S.dph, acc);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) acc[c] = wsum(acc[c]);
+  if (lane == 0) {
+    double h[6];
+    for (int c = 0; c < 6; ++c) h[c] = (xu < kMinOcc) ? 0.0 : acc[c] + hrec[8 * (size_t)u + 1 + c];
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) H[9 * (size_t)u + 3 * x + y] = h[sym6(x, y)];
+  }
+}
+
 // Totals in a fixed order: block b sums a contiguous chunk of sites, the
 // final warp sums the blocks' partials.
 __global__ void __launch_bounds__(256) pt_totals_part_kernel(int n, const double *V,
@@ -252,14 +454,18 @@ inline int nblk(long long n, int per) { return (int)((n + per - 1) / per); }
 namespace {
 
 // Layout of the system's point-form buffer (doubles): rec (16 n), rho (n),
-// V (n), Fq (3 n), W (9 n), partials (64 x 12), totals (12).
+// V (n), Fq (3 n), W (9 n), partials (64 x 12), totals (12), Hessian
+// records (8 n), Hessian blocks (9 n).
 struct PtLayout {
-  double *rec, *rho, *V, *Fq, *W, *part, *tot;
+  double *rec, *rho, *V, *Fq, *W, *part, *tot, *hrec, *H;
 };
 
 int pt_buffers(btam_system *s, PtLayout &L) {
   const int n = s->n_real;
-  const size_t need = (size_t)(kPtRec + 14) * n + (size_t)kPtParts * kPtTot + kPtTot;
+  // the Hessian records start on a 32-byte boundary (double4 stores)
+  const size_t hoff = ((size_t)(kPtRec + 14) * n + (size_t)kPtParts * kPtTot + kPtTot + 3) &
+                      ~(size_t)3;
+  const size_t need = hoff + 17 * (size_t)n;
   if (!s->pt || s->pt_cap < need) {
     BTAM_TRY(dalloc(s->pt, s->st, need));
     s->pt_cap = need;
@@ -272,11 +478,25 @@ int pt_buffers(btam_system *s, PtLayout &L) {
   L.W = L.Fq + 3 * (size_t)n;
   L.part = L.W + 9 * (size_t)n;
   L.tot = L.part + (size_t)kPtParts * kPtTot;
+  L.hrec = b + hoff;
+  L.H = L.hrec + 8 * (size_t)n;
   return BTAM_OK;
 }
 
+PtArgs pt_args(btam_system *s, const PtLayout &L);
+
 // Enqueues both passes and the totals on the system's stream.
 int pt_run(btam_system *s, const PtLayout &L) {
+  const PtArgs a = pt_args(s, L);
+  const int g = nblk((long long)s->n_real * 32, 128);
+  pt_moments_kernel<<<g, 128, 0, s->st>>>(a);
+  pt_grad_kernel<<<g, 128, 0, s->st>>>(a);
+  pt_totals_part_kernel<<<kPtParts, 256, 0, s->st>>>(s->n_real, L.V, L.Fq, L.W, L.part);
+  pt_totals_final_kernel<<<1, 32, 0, s->st>>>(L.part, L.tot);
+  return cuda_status(cudaGetLastError());
+}
+
+PtArgs pt_args(btam_system *s, const PtLayout &L) {
   PtArgs a;
   a.n_real = s->n_real;
   a.pos = s->pos;
@@ -293,12 +513,7 @@ int pt_run(btam_system *s, const PtLayout &L) {
   a.V = L.V;
   a.Fq = L.Fq;
   a.W = L.W;
-  const int g = nblk((long long)s->n_real * 32, 128);
-  pt_moments_kernel<<<g, 128, 0, s->st>>>(a);
-  pt_grad_kernel<<<g, 128, 0, s->st>>>(a);
-  pt_totals_part_kernel<<<kPtParts, 256, 0, s->st>>>(s->n_real, L.V, L.Fq, L.W, L.part);
-  pt_totals_final_kernel<<<1, 32, 0, s->st>>>(L.part, L.tot);
-  return cuda_status(cudaGetLastError());
+  return a;
 }
 
 }  // namespace
@@ -401,6 +616,23 @@ int btam_pt_eval(btam_system *s, double *rho, double *V, double *Fq, double *W,
   if (totals)
     BTAM_TRY(cudaMemcpyAsync(totals, L.tot, kPtTot * sizeof(double), cudaMemcpyDeviceToHost,
                              s->st));
+  return read_err(s);
+}
+
+int btam_pt_hessian(btam_system *s, double *H) {
+  if (!s || !H) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  PtLayout L;
+  int st = pt_buffers(s, L);
+  if (st != BTAM_OK) return st;
+  const PtArgs a = pt_args(s, L);
+  const int g = nblk((long long)s->n_real * 32, 128);
+  pt_moments_kernel<<<g, 128, 0, s->st>>>(a);
+  pt_hself_kernel<<<g, 128, 0, s->st>>>(a, L.hrec);
+  pt_hess_kernel<<<g, 128, 0, s->st>>>(a, L.hrec, L.H);
+  BTAM_TRY(cudaGetLastError());
+  BTAM_TRY(cudaMemcpyAsync(H, L.H, 9 * (size_t)s->n_real * sizeof(double),
+                           cudaMemcpyDeviceToHost, s->st));
   return read_err(s);
 }
 

@@ -215,6 +215,13 @@ int btam_rho_nmf(btam_system *s, double *rho);
  * Any output may be NULL.  sigma is not read. */
 int btam_pt_eval(btam_system *s, double *rho, double *V, double *Fq, double *W,
                  double *totals);
+/* Hessian blocks of the non-mean-field forms: H (9 per real site,
+ * row-major) = sum_{i in {u} U N(u)} evaluate_D2V_i_Dq2_u_MgHx(u, i)
+ * (MgHx-mf-V-bulk.cpp:333-528), as the reference forms each term: for
+ * i = u the Hessian of V_u in q_u; for a neighbour i the diagonal blocks of
+ * the slots u holds in V_i's terms (for j1 = j2 = u the two slot blocks
+ * without their cross blocks, so this is not d2(sum V)/dq_u^2 there). */
+int btam_pt_hessian(btam_system *s, double *H);
 /* Stretches the system by diag(F) (F[a] > 0): q <- F q for every site, the
  * cell rows and the origin likewise; images follow; neighbour lists are
  * kept.  BTAM_ERR_BOX_TOO_SMALL (nothing changed) if a periodic cell would

@@ -53,8 +53,10 @@
  *    mean_q0 give NaN and last_status() BTAM_ERR_ARG.
  *  - evaluate_DV0_i_DF (the mean-field stretch derivative) comes from
  *    btam_mf_stress in the bound precision.
- *  - The Hessians (evaluate_D2V_i_Dq2_j, evaluate_D2V0_i_Dmeanq2_j) are not
- *    provided: their slots are null. */
+ *  - evaluate_D2V_i_Dq2_j (btam_pt_hessian) is lumped like the gradients:
+ *    the whole sum over i in {u} U N(u) at site_i == site_i_star.
+ *  - The mean-field Hessian (evaluate_D2V0_i_Dmeanq2_j) is not provided: its
+ *    slot is null. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -75,13 +77,14 @@ struct Cache {
   bool valid = false;       // mean-field results of that state
   bool pt_valid = false;    // non-mean-field results of that state
   bool mfs_valid = false;   // mean-field stress of that state
+  bool pth_valid = false;   // non-mean-field Hessian blocks of that state
   int status = BTAM_OK;     // status of the last evaluation
   std::vector<double> beta, gamma;
   std::vector<double> q, sigma, x;  // the evaluated state (q row-major)
   std::vector<double> q_bind;       // positions at bind(): the stretch reference
   double F[3] = {1.0, 1.0, 1.0};    // stretch of the system's cell against them
   std::vector<double> rho, V0, S0, Rq, Rs, Rx;
-  std::vector<double> pt_rho, pt_Fq, pt_W, mf_W;
+  std::vector<double> pt_rho, pt_Fq, pt_W, mf_W, pt_H;
 };
 
 inline Cache &cache() {
@@ -103,7 +106,7 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.sys = s;
   c.precision = precision;
   c.n = n_real;
-  c.have_state = c.valid = c.pt_valid = c.mfs_valid = false;
+  c.have_state = c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = false;
   c.F[0] = c.F[1] = c.F[2] = 1.0;
   c.beta.assign(beta ? beta : nullptr, beta ? beta + n_real : nullptr);
   c.gamma.assign(gamma ? gamma : nullptr, gamma ? gamma + n_real : nullptr);
@@ -122,6 +125,7 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.pt_Fq.assign(3 * (size_t)n_real, 0.0);
   c.pt_W.assign(9 * (size_t)n_real, 0.0);
   c.mf_W.assign(9 * (size_t)n_real, 0.0);
+  c.pt_H.assign(9 * (size_t)n_real, 0.0);
   st = btam_system_get_state(s, c.q.data(), c.sigma.data(), c.x.data());
   c.have_state = st == BTAM_OK;
   c.q_bind = c.q;
@@ -162,7 +166,7 @@ inline bool stretch_of(const Cache &c, double F[3]) {
   return true;
 }
 
-enum { kMeanField = 1, kPoint = 2, kStress = 4 };
+enum { kMeanField = 1, kPoint = 2, kStress = 4, kHessian = 8 };
 
 // Loads the caller's state when the sites a value depends on differ from the
 // cache, then evaluates what `what` asks for and is not yet evaluated.
@@ -179,7 +183,7 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
       if (stdv_q) c.sigma[j] = (*stdv_q)(j);
       c.x[j] = xi(j);
     }
-    c.valid = c.pt_valid = c.mfs_valid = false;
+    c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = false;
     // a stretch of the bound positions takes the cell with it; any other
     // state keeps the current cell
     double F[3];
@@ -208,6 +212,10 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
   if ((what & kStress) && !c.mfs_valid) {
     c.status = btam_mf_stress(c.sys, c.precision, c.mf_W.data(), nullptr);
     c.mfs_valid = c.status == BTAM_OK;
+  }
+  if ((what & kHessian) && !c.pth_valid) {
+    c.status = btam_pt_hessian(c.sys, c.pt_H.data());
+    c.pth_valid = c.status == BTAM_OK;
   }
 }
 
@@ -265,6 +273,20 @@ inline Eigen::Vector3d DV_Dq(unsigned u, unsigned i, const Eigen::MatrixXd &mean
   for (int k = 0; k < 3; ++k)
     g(k) = !c.pt_valid || (int)u >= c.n ? NAN : (u == i ? c.pt_Fq[3 * (size_t)u + k] : 0.0);
   return g;
+}
+
+inline Eigen::Matrix3d D2V_Dq2(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
+                               const Eigen::VectorXd &xi, const Eigen::VectorXd &,
+                               const AtomicSpecie *, const AtomTopology topo) {
+  Cache &c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, u, i, mean_q, nullptr, xi, topo, kHessian);
+  Eigen::Matrix3d H;
+  const bool ok = c.pth_valid && (int)u < c.n;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      H(a, b) = !ok ? NAN : (u == i ? c.pt_H[9 * (size_t)u + 3 * a + b] : 0.0);
+  return H;
 }
 
 inline Eigen::Matrix3d DV_DF(unsigned i, const Eigen::MatrixXd &mean_q,
@@ -371,7 +393,7 @@ inline dmd_equations btam_DMD_MgHx_constructor() {
   dmd_equations eq;
   eq.evaluate_rho_i = d::rho_i;
   eq.evaluate_DV_i_Dq_j = d::DV_Dq;
-  eq.evaluate_D2V_i_Dq2_j = nullptr;
+  eq.evaluate_D2V_i_Dq2_j = d::D2V_Dq2;
   eq.evaluate_DV_i_DF = d::DV_DF;
   eq.evaluate_mf_rho_i = d::mf_rho_i;
   eq.evaluate_V0_i = d::V0_i;

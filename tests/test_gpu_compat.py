@@ -82,12 +82,12 @@ def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
                            capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr
         raw = open(out, "rb").read()
-        v = np.frombuffer(raw[:8 * 22 * n], np.float64).reshape(n, 22)
-        Y = np.frombuffer(raw[8 * 22 * n:8 * 22 * n + 24], np.float64)
-        assert np.frombuffer(raw[8 * 22 * n + 24:], np.int32)[0] == 0
+        v = np.frombuffer(raw[:8 * 31 * n], np.float64).reshape(n, 31)
+        Y = np.frombuffer(raw[8 * 31 * n:8 * 31 * n + 24], np.float64)
+        assert np.frombuffer(raw[8 * 31 * n + 24:], np.int32)[0] == 0
         assert np.max(np.abs(v[:, 0] - p[kr])) <= 1e-12 * np.abs(p[kr]).max()
         W = v[:, 4:13].reshape(n, 3, 3)
-        W0, kw0 = v[:, 13:].reshape(n, 3, 3), kw.replace("_W", "_W0")
+        W0, kw0 = v[:, 13:22].reshape(n, 3, 3), kw.replace("_W", "_W0")
         assert np.max(np.abs(W0 - p[kw0])) <= 1e-10 * max(1.0, np.abs(p[kw0]).max())
         assert np.max(np.abs(W - p[kw])) <= 1e-10 * max(1.0, np.abs(p[kw]).max())
         Yref = np.array([p[kw][:, a, a].sum() for a in range(3)]) / vol
@@ -95,3 +95,6 @@ def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
         if F[0] == 1.0:
             Fq = p["ortho_mgh_Fq"]
             assert np.max(np.abs(v[:, 1:4] - Fq)) <= 1e-10 * max(1.0, np.abs(Fq).max())
+            H = p["ortho_mgh_H"]
+            assert np.max(np.abs(v[:, 22:].reshape(n, 3, 3) - H)) <= 1e-9 * max(1.0,
+                                                                               np.abs(H).max())

@@ -227,3 +227,18 @@ def test_relax_stretch_mf_zeroes_reference_stress(gpu_tables, oracle):
     F32, info32 = S2.relax_stretch_mf(btam.FP32C, atol=1e-8, rtol=1e-10, max_iter=20)
     assert info32["status"] == 1, info32
     assert np.max(np.abs(F32 - F)) <= 1e-5
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_point_hessian_against_reference(gpu_tables, name):
+    """Assembled Hessian blocks of the point forms (sum over i in {u} U N(u)
+    of evaluate_D2V_i_Dq2_u_MgHx) within 1e-9 of max(1, the largest entry);
+    symmetric; zero on empty sites."""
+    g, p = load(name), load("point")
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    H = S.pt_hessian()
+    assert err1(H, p[f"{name}_H"]) < 1e-9
+    assert np.array_equal(H, np.transpose(H, (0, 2, 1)))
+    assert np.all(H[g["x"] < 5e-4] == 0.0)
+    assert np.array_equal(S.pt_hessian(), H)
