@@ -905,6 +905,90 @@ void D2V_dq2(const View &v, int u, int i, double *out9) {
                         pair[3 * a + b] + dip[3 * a + b] + quad[3 * a + b];
 }
 
+// Block a of the Hessian of term `term` (0 rho, 1 pair, 2 dipole, 3
+// quadrupole) at one geometry.
+void term_d2(int term, int a, const double *n, const double *q, const int *spc, double *H) {
+  if (term >= 2) {
+    if (term == 2) dip_d2(a, n, q, spc, H);
+    else quad_d2(a, n, q, spc, H);
+    return;
+  }
+  for (int c = 0; c < 9; ++c) H[c] = 0.0;
+  double r[3], s2 = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    r[k] = q[k] - q[3 + k];
+    s2 += sq(r[k]);
+  }
+  const double s = std::sqrt(s2);
+  const Spline &S = term == 0 ? rho_of(spc[1]) : pot_of(spc[0], spc[1]).pair;
+  radial_hess(r, s, spline_d1(S, s), spline_d2(S, s), term == 0 ? n[1] : 0.5 * n[0] * n[1], H);
+}
+
+// meanfield_integral_gh_3th_d2mq (Quadrature-Hermitian-3th.cpp:382-463):
+// the block averaged over the rule's points.
+void integ_d2(int term, int a, const Measure &m, double *out9) {
+  const double W = 1.0 / (2.0 * m.D);
+  double ql[9], h[9];
+  for (int c = 0; c < 9; ++c) out9[c] = 0.0;
+  for (double sgn : {1.0, -1.0})
+    for (int l = 0; l < m.D; ++l) {
+      point(m, l, sgn, ql);
+      term_d2(term, a, m.x, ql, m.spc, h);
+      for (int c = 0; c < 9; ++c) out9[c] += h[c] * W;
+    }
+}
+
+// evaluate_D2V0_i_Dmeanq2_u_MgHx (MgHx-mf-V-bulk.cpp:1366-1600).
+void D2V0_dq2(const View &v, int u, int i, double *out9) {
+  for (int c = 0; c < 9; ++c) out9[c] = 0.0;
+  if (v.spc[u] == kH && v.x[u] < kMinOcc) return;  // 1398-1402
+  if (v.spc[i] == kH && v.x[i] < kMinOcc) return;  // 1424-1427
+  double drho[3] = {0, 0, 0}, d2rho[9] = {0}, pair[9] = {0}, dip[9] = {0}, quad[9] = {0};
+  const int nb0 = v.offs[i], nb1 = v.offs[i + 1];
+  for (int k1 = nb0; k1 < nb1; ++k1) {
+    const int j1 = v.idx[k1];
+    if (v.spc[j1] == kH && v.x[j1] <= kMinOcc) continue;  // 1441-1443
+    int sites2[2] = {i, j1};
+    if (sites2[0] == u || sites2[1] == u) {
+      PairCtx c;
+      pair_ctx(v, i, j1, c);
+      for (int dir = 0; dir < 2; ++dir) {
+        if (sites2[dir] != u) continue;
+        double g[3], h[9];
+        integ_dmq(dir, kRho, c.m, g);
+        for (int a = 0; a < 3; ++a) drho[a] += g[a];
+        integ_d2(0, dir, c.m, h);
+        for (int k = 0; k < 9; ++k) d2rho[k] += h[k];
+        integ_d2(1, dir, c.m, h);
+        for (int k = 0; k < 9; ++k) pair[k] += h[k];
+      }
+    }
+    for (int k2 = k1; k2 < nb1; ++k2) {
+      const int j2 = v.idx[k2];
+      if (v.spc[j2] == kH && v.x[j2] <= kMinOcc) continue;  // 1500-1502
+      int sites3[3] = {i, j1, j2};
+      if (sites3[0] != u && sites3[1] != u && sites3[2] != u) continue;
+      TriCtx t;
+      tri_ctx(v, i, j1, j2, t);
+      const double f = (k1 == k2) ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        if (sites3[dir] != u) continue;
+        double h[9];
+        integ_d2(2, dir, t.m, h);
+        for (int k = 0; k < 9; ++k) dip[k] += f * h[k];
+        integ_d2(3, dir, t.m, h);
+        for (int k = 0; k < 9; ++k) quad[k] += f * h[k];
+      }
+    }
+  }
+  const Spline &E = embed_of(v.spc[i]);
+  const double dF = spline_d1(E, v.rho[i]), ddF = spline_d2(E, v.rho[i]);  // 1584-1591
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      out9[3 * a + b] = v.x[i] * ddF * drho[a] * drho[b] + v.x[i] * dF * d2rho[3 * a + b] +
+                        pair[3 * a + b] + dip[3 * a + b] + quad[3 * a + b];
+}
+
 // evaluate_DV_i_dF_MgHx (MgHx-mf-V-bulk.cpp:530-704): sum over the sites a
 // of every term of V_i of dV_i/dq_a (x) q0_a, 3x3 row-major (row: gradient
 // component, column: reference-position component).
@@ -1252,6 +1336,14 @@ void orc_pt_D2V_pairs(int n, const double *q, const double *x, const int *spc,
   (void)n;
   View v{q, nullptr, x, rho, spc, offs, idx};
   par_for(npairs, [&](int k) { D2V_dq2(v, u_list[k], i_list[k], out9 + 9 * k); });
+}
+
+void orc_mf_D2V0_pairs(int n, const double *q, const double *sigma, const double *x,
+                       const int *spc, const double *rho, const int *offs, const int *idx,
+                       const int *u_list, const int *i_list, int npairs, double *out9) {
+  (void)n;
+  View v{q, sigma, x, rho, spc, offs, idx};
+  par_for(npairs, [&](int k) { D2V0_dq2(v, u_list[k], i_list[k], out9 + 9 * k); });
 }
 
 void orc_residuals(int n, const double *q, const double *sigma,

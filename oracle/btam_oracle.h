@@ -86,6 +86,13 @@ void orc_pt_D2V_pairs(int n, const double *q, const double *x, const int *spc,
                       const double *rho, const int *offs, const int *idx, const int *u_list,
                       const int *i_list, int npairs, double *out9);
 
+/* Mean-field d2V0_i/dmean_q_u^2 per (u, i) pair, 9 values row-major
+ * (evaluate_D2V0_i_Dmeanq2_u_MgHx, MgHx-mf-V-bulk.cpp:1366-1600); rho: the
+ * mean-field density of every site. */
+void orc_mf_D2V0_pairs(int n, const double *q, const double *sigma, const double *x,
+                       const int *spc, const double *rho, const int *offs, const int *idx,
+                       const int *u_list, const int *i_list, int npairs, double *out9);
+
 /* Mean-field stretch derivative dV0_i/dF per site, 9 values row-major,
  * with reference positions q0 of every site (evaluate_DV0_i_dF_bulk_MgHx,
  * MgHx-mf-V-bulk.cpp:2329-2552); rho: the mean-field density of every site. */

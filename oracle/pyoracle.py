@@ -160,6 +160,18 @@ class Lib:
         return out
 
 
+    def mf_D2V0_pairs(self, s, rho, offs, idx, u_list, i_list):
+        """d2V0_i/dmean_q_u^2 per (u, i) pair, 3x3
+        (evaluate_D2V0_i_Dmeanq2_u_MgHx); rho: mean-field density."""
+        u_list = np.ascontiguousarray(u_list, np.int32)
+        i_list = np.ascontiguousarray(i_list, np.int32)
+        out = np.zeros((len(u_list), 3, 3))
+        self._f("mf_D2V0_pairs")(len(s["x"]), _d(s["q"]), _d(s["sigma"]), _d(s["x"]),
+                                 _i(s["species"]), _d(rho), _i(offs), _i(idx), _i(u_list),
+                                 _i(i_list), len(u_list), _d(out))
+        return out
+
+
 class Oracle(Lib):
     """The restated oracle plus its project-defined pieces."""
 

@@ -361,4 +361,22 @@ void ref_pt_D2V_pairs(int n, const double *q, const double *x, const int *spc,
   free(s.spc);
 }
 
+// evaluate_D2V0_i_Dmeanq2_u_MgHx (MgHx-mf-V-bulk.cpp:1366-1600): 9 values per
+// (u, i) pair, row-major; rho is the mean-field density of every site.
+void ref_mf_D2V0_pairs(int n, const double *q, const double *sigma, const double *x,
+                       const int *spc, const double *rho, const int *offs, const int *idx,
+                       const int *u_list, const int *i_list, int npairs, double *out9) {
+  Sys s;
+  make_sys(s, n, q, sigma, x, spc, offs, idx);
+  for (int i = 0; i < n; ++i) s.rho(i) = rho[i];
+  parallel_for(npairs, [&](int k) {
+    int u = u_list[k], i = i_list[k];
+    Eigen::Matrix3d g =
+        evaluate_D2V0_i_Dmeanq2_u_MgHx(u, i, s.q, s.sigma, s.x, s.rho, s.spc, topo(s, i));
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) out9[9 * k + 3 * a + b] = g(a, b);
+  });
+  free(s.spc);
+}
+
 } // extern "C"

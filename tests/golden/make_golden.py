@@ -120,7 +120,8 @@ def point_fixture(ref):
     site, the same sum of evaluate_D2V_i_Dq2_u_MgHx, dV_i/dF with q0 = q, and dV_i/dF after the stretch PT_STRETCH
     (q0 = the unstretched positions, neighbour lists kept); and the
     mean-field stretch derivative evaluate_DV0_i_dF_bulk_MgHx at q0 = q and
-    after the same stretch (with the mean-field rho-bar there)."""
+    after the same stretch (with the mean-field rho-bar there), and the
+    assembled mean-field Hessian blocks evaluate_D2V0_i_Dmeanq2_u_MgHx."""
     out = {"stretch": PT_STRETCH}
     for name in ("sphere", "ortho_mgh", "x5cube", "config1"):
         g = np.load(os.path.join(OUT, f"{name}.npz"))
@@ -159,6 +160,14 @@ def point_fixture(ref):
         rho0_s = ref.mf_rho(mfs, offs, idx, real)
         W0_s = ref.mf_DV0_dF(mfs, full["q"], rho0_s[owner], offs, idx, real)
         out.update({f"{name}_W0": W0, f"{name}_rho0_s": rho0_s, f"{name}_W0_s": W0_s})
+        # the mean-field Hessian blocks (evaluate_D2V0_i_Dmeanq2_u_MgHx),
+        # summed over i in {u} U N(u) like the gradients
+        h9 = ref.mf_D2V0_pairs(mf, g["rho"][owner], offs, idx,
+                               np.array([p[1] for p in plan], np.int32),
+                               np.array([p[2] for p in plan], np.int32))
+        H0 = np.zeros((n, 3, 3))
+        np.add.at(H0, kk, h9)
+        out[f"{name}_H0"] = H0
         print(f"point forms {name}: {n} sites, {len(plan)} gradient pairs")
     np.savez_compressed(os.path.join(OUT, "point.npz"), **out)
 

@@ -153,6 +153,11 @@ def test_point_forms_against_golden(oracle, name):
     mf = dict(full, sigma=np.ascontiguousarray(g["sigma"][owner]))
     assert np.array_equal(oracle.mf_DV0_dF(mf, full["q"], g["rho"][owner], offs, idx, real),
                           p[f"{name}_W0"])
+    h9 = oracle.mf_D2V0_pairs(mf, g["rho"][owner], offs, idx, [q[1] for q in plan],
+                              [q[2] for q in plan])
+    H0 = np.zeros((n, 3, 3))
+    np.add.at(H0, np.array([q[0] for q in plan]), h9)
+    assert np.abs(H0 - p[f"{name}_H0"]).max() <= 1e-12 * max(1.0, np.abs(p[f"{name}_H0"]).max())
     mfs = dict(mf, q=st["q"])
     rho0_s = oracle.mf_rho(mfs, offs, idx, real)
     assert np.array_equal(rho0_s, p[f"{name}_rho0_s"])
