@@ -71,6 +71,7 @@ _PROTOS = {
     "btam_pt_eval": (ctypes.c_int, [_V, _D, _D, _D, _D, _D]),
     "btam_stretch_apply": (ctypes.c_int, [_V, _D]),
     "btam_pt_hessian": (ctypes.c_int, [_V, _D]),
+    "btam_mf_hessian": (ctypes.c_int, [_V, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
@@ -441,6 +442,13 @@ class System:
         i in {u} U N(u) of evaluate_D2V_i_Dq2_u_MgHx."""
         H = np.zeros((self.n, 3, 3))
         _check(lib().btam_pt_hessian(self.handle, _d(H)), "btam_pt_hessian")
+        return H
+
+    def mf_hessian(self):
+        """Mean-field Hessian blocks, (n, 3, 3): the sum over i in {u} U N(u)
+        of evaluate_D2V0_i_Dmeanq2_u_MgHx (FP64)."""
+        H = np.zeros((self.n, 3, 3))
+        _check(lib().btam_mf_hessian(self.handle, _d(H)), "btam_mf_hessian")
         return H
 
     def stretch(self, F):

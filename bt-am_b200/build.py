@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libbtam.so")
 SOURCES = ["btam_capi.cu", "adp_kernels.cu", "topo_kernels.cu", "solvers.cu", "batch.cu",
-           "server.cu", "noalloc.cu", "point.cu"]
+           "server.cu", "noalloc.cu", "point.cu", "mf_hessian.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",

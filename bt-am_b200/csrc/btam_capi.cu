@@ -1061,6 +1061,12 @@ int btam_probe_gather_peak(const btam_tables *t, double seconds, double *gbs) {
 
 }  // extern "C"
 
+int mf_rho64_enqueue(btam_system *s) {
+  if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, (size_t)s->n_real * kMomStride));
+  BTAM_TRY(launch_pass1(eval_args<double>(s, s->mom64, s->T->r64), s->st, 0, 0));
+  return BTAM_OK;
+}
+
 int mf_stress_enqueue(btam_system *s, int precision, double **W_out, double **tot_out) {
   double *W = nullptr, *part = nullptr, *tot = nullptr;
   int st = pt_stress_buffers(s, &W, &part, &tot);

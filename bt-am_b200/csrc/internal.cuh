@@ -98,6 +98,10 @@ int pt_stress_buffers(btam_system *s, double **W, double **part, double **tot);
 cudaError_t launch_pt_totals(int n, const double *V, const double *Fq, const double *W,
                              double *part, double *tot, cudaStream_t st);
 
+// Enqueues the FP64 directed pass 1: the mean-field rho-bar, V0 and S0 of
+// the current state into the system's buffers (btam_capi.cu).
+int mf_rho64_enqueue(btam_system *s);
+
 // Enqueues the directed pass 1 and the mean-field stress of the current
 // state; *W: per-site stress (9 n), *tot: totals whose [2..10] hold the sum
 // (btam_capi.cu).

@@ -194,6 +194,17 @@ int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass
  * be NULL. */
 int btam_mf_stress(btam_system *s, int precision, double *W0, double *total);
 
+/* Mean-field Hessian blocks: H (9 per real site, row-major) = sum over
+ * i in {u} U N(u) of evaluate_D2V0_i_Dmeanq2_u_MgHx(u, i)
+ * (MgHx-mf-V-bulk.cpp:1366-1600), FP64, as the reference forms each term
+ * (for a neighbour i the diagonal blocks of u's slots; for j1 = j2 = u
+ * without their cross blocks).  A direct evaluation of the reference's
+ * sums (about N_nb^2 x 18 term Hessians per site), not the moment form of
+ * the evaluation kernels: no solver needs it on a hot path.  Runs the FP64
+ * pass 1 first (the system's rho, V0, S0 buffers then hold the current
+ * state's values). */
+int btam_mf_hessian(btam_system *s, double *H);
+
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);

@@ -53,10 +53,10 @@
  *    mean_q0 give NaN and last_status() BTAM_ERR_ARG.
  *  - evaluate_DV0_i_DF (the mean-field stretch derivative) comes from
  *    btam_mf_stress in the bound precision.
- *  - evaluate_D2V_i_Dq2_j (btam_pt_hessian) is lumped like the gradients:
- *    the whole sum over i in {u} U N(u) at site_i == site_i_star.
- *  - The mean-field Hessian (evaluate_D2V0_i_Dmeanq2_j) is not provided: its
- *    slot is null. */
+ *  - evaluate_D2V_i_Dq2_j (btam_pt_hessian) and evaluate_D2V0_i_Dmeanq2_j
+ *    (btam_mf_hessian, FP64 whatever the bound precision) are lumped like
+ *    the gradients: the whole sum over i in {u} U N(u) at site_i ==
+ *    site_i_star.  Every slot of the table is served. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -78,13 +78,14 @@ struct Cache {
   bool pt_valid = false;    // non-mean-field results of that state
   bool mfs_valid = false;   // mean-field stress of that state
   bool pth_valid = false;   // non-mean-field Hessian blocks of that state
+  bool mfh_valid = false;   // mean-field Hessian blocks of that state
   int status = BTAM_OK;     // status of the last evaluation
   std::vector<double> beta, gamma;
   std::vector<double> q, sigma, x;  // the evaluated state (q row-major)
   std::vector<double> q_bind;       // positions at bind(): the stretch reference
   double F[3] = {1.0, 1.0, 1.0};    // stretch of the system's cell against them
   std::vector<double> rho, V0, S0, Rq, Rs, Rx;
-  std::vector<double> pt_rho, pt_Fq, pt_W, mf_W, pt_H;
+  std::vector<double> pt_rho, pt_Fq, pt_W, mf_W, pt_H, mf_H;
 };
 
 inline Cache &cache() {
@@ -106,7 +107,7 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.sys = s;
   c.precision = precision;
   c.n = n_real;
-  c.have_state = c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = false;
+  c.have_state = c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = c.mfh_valid = false;
   c.F[0] = c.F[1] = c.F[2] = 1.0;
   c.beta.assign(beta ? beta : nullptr, beta ? beta + n_real : nullptr);
   c.gamma.assign(gamma ? gamma : nullptr, gamma ? gamma + n_real : nullptr);
@@ -126,6 +127,7 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.pt_W.assign(9 * (size_t)n_real, 0.0);
   c.mf_W.assign(9 * (size_t)n_real, 0.0);
   c.pt_H.assign(9 * (size_t)n_real, 0.0);
+  c.mf_H.assign(9 * (size_t)n_real, 0.0);
   st = btam_system_get_state(s, c.q.data(), c.sigma.data(), c.x.data());
   c.have_state = st == BTAM_OK;
   c.q_bind = c.q;
@@ -166,7 +168,7 @@ inline bool stretch_of(const Cache &c, double F[3]) {
   return true;
 }
 
-enum { kMeanField = 1, kPoint = 2, kStress = 4, kHessian = 8 };
+enum { kMeanField = 1, kPoint = 2, kStress = 4, kHessian = 8, kMfHessian = 16 };
 
 // Loads the caller's state when the sites a value depends on differ from the
 // cache, then evaluates what `what` asks for and is not yet evaluated.
@@ -183,7 +185,7 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
       if (stdv_q) c.sigma[j] = (*stdv_q)(j);
       c.x[j] = xi(j);
     }
-    c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = false;
+    c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = c.mfh_valid = false;
     // a stretch of the bound positions takes the cell with it; any other
     // state keeps the current cell
     double F[3];
@@ -216,6 +218,10 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
   if ((what & kHessian) && !c.pth_valid) {
     c.status = btam_pt_hessian(c.sys, c.pt_H.data());
     c.pth_valid = c.status == BTAM_OK;
+  }
+  if ((what & kMfHessian) && !c.mfh_valid) {
+    c.status = btam_mf_hessian(c.sys, c.mf_H.data());
+    c.mfh_valid = c.status == BTAM_OK;
   }
 }
 
@@ -286,6 +292,21 @@ inline Eigen::Matrix3d D2V_Dq2(unsigned u, unsigned i, const Eigen::MatrixXd &me
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b)
       H(a, b) = !ok ? NAN : (u == i ? c.pt_H[9 * (size_t)u + 3 * a + b] : 0.0);
+  return H;
+}
+
+inline Eigen::Matrix3d D2V0_Dmeanq2(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
+                                    const Eigen::VectorXd &stdv_q, const Eigen::VectorXd &xi,
+                                    const Eigen::VectorXd &, const AtomicSpecie *,
+                                    const AtomTopology topo) {
+  Cache &c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMfHessian);
+  Eigen::Matrix3d H;
+  const bool ok = c.mfh_valid && (int)u < c.n;
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      H(a, b) = !ok ? NAN : (u == i ? c.mf_H[9 * (size_t)u + 3 * a + b] : 0.0);
   return H;
 }
 
@@ -399,7 +420,7 @@ inline dmd_equations btam_DMD_MgHx_constructor() {
   eq.evaluate_V0_i = d::V0_i;
   eq.evaluate_S0_i = d::S0_i;
   eq.evaluate_DV0_i_Dmeanq_j = d::DV0_Dmeanq;
-  eq.evaluate_D2V0_i_Dmeanq2_j = nullptr;
+  eq.evaluate_D2V0_i_Dmeanq2_j = d::D2V0_Dmeanq2;
   eq.evaluate_DV0_i_Dstdvq_j = d::DV0_Dstdvq;
   eq.evaluate_DV0_i_Dq_j = d::DV0_Dq;
   eq.evaluate_DV0_i_Dxi_j = d::DV0_Dxi;

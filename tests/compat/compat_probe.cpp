@@ -15,9 +15,10 @@
 // Mechanical-Relaxation-bulk.cpp:441-600) at mean_q = diag(F) q with
 // mean_q0 = q: evaluate_rho_i over the sites, then per site the assembled
 // evaluate_DV_i_Dq_j, evaluate_DV_i_DF, the mean-field evaluate_DV0_i_DF and
-// the assembled evaluate_D2V_i_Dq2_j.  Output: per site rho, the gradient
-// (3), dV/dF (9, row-major), dV0/dF (9), the Hessian block (9); then Y (3) =
-// sum_u diag(dV_u/dF) / V0 and the status.
+// the assembled evaluate_D2V_i_Dq2_j and evaluate_D2V0_i_Dmeanq2_j.  Output:
+// per site rho, the gradient (3), dV/dF (9, row-major), dV0/dF (9), the
+// Hessian block (9), the mean-field Hessian block (9); then Y (3) = sum_u
+// diag(dV_u/dF) / V0 and the status.
 #include "Macros.hpp"
 #include "btam_dmd_equations.hpp"
 
@@ -98,9 +99,10 @@ int main(int argc, char **argv) {
     double Y[3] = {0, 0, 0};
     for (int u = 0; u < n; ++u) {
       AtomTopology topo{(int)nbs[u].size(), nbs[u].data()};
-      double v[31];
+      double v[40];
       v[0] = rho_v(u);
       double g[3] = {0, 0, 0}, h[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      double h0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
       for (int k = -1; k < (int)nbs[u].size(); ++k) {
         const unsigned i = k < 0 ? u : nbs[u][k];
         Eigen::Vector3d d = eq.evaluate_DV_i_Dq_j(u, i, mean_q, xi, rho_v, specie.data(), topo);
@@ -109,8 +111,13 @@ int main(int argc, char **argv) {
             eq.evaluate_D2V_i_Dq2_j(u, i, mean_q, xi, rho_v, specie.data(), topo);
         for (int a = 0; a < 3; ++a)
           for (int b = 0; b < 3; ++b) h[3 * a + b] += dd(a, b);
+        Eigen::Matrix3d d0 = eq.evaluate_D2V0_i_Dmeanq2_j(u, i, mean_q, stdv_q, xi, rho_v,
+                                                          specie.data(), topo);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) h0[3 * a + b] += d0(a, b);
       }
       for (int c = 0; c < 9; ++c) v[22 + c] = h[c];
+      for (int c = 0; c < 9; ++c) v[31 + c] = h0[c];
       for (int c = 0; c < 3; ++c) v[1 + c] = g[c];
       Eigen::Matrix3d W = eq.evaluate_DV_i_DF(u, mean_q, q_ref, xi, rho_v, specie.data(), topo);
       for (int a = 0; a < 3; ++a) {
@@ -121,7 +128,7 @@ int main(int argc, char **argv) {
           eq.evaluate_DV0_i_DF(u, mean_q, q_ref, stdv_q, xi, rho_v, specie.data(), topo);
       for (int a = 0; a < 3; ++a)
         for (int b = 0; b < 3; ++b) v[13 + 3 * a + b] = W0(a, b);
-      fwrite(v, sizeof(double), 31, o);
+      fwrite(v, sizeof(double), 40, o);
     }
     fwrite(Y, sizeof(double), 3, o);
     const int last = btam_compat::last_status();

@@ -82,9 +82,9 @@ def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
                            capture_output=True, text=True, timeout=300)
         assert r.returncode == 0, r.stderr
         raw = open(out, "rb").read()
-        v = np.frombuffer(raw[:8 * 31 * n], np.float64).reshape(n, 31)
-        Y = np.frombuffer(raw[8 * 31 * n:8 * 31 * n + 24], np.float64)
-        assert np.frombuffer(raw[8 * 31 * n + 24:], np.int32)[0] == 0
+        v = np.frombuffer(raw[:8 * 40 * n], np.float64).reshape(n, 40)
+        Y = np.frombuffer(raw[8 * 40 * n:8 * 40 * n + 24], np.float64)
+        assert np.frombuffer(raw[8 * 40 * n + 24:], np.int32)[0] == 0
         assert np.max(np.abs(v[:, 0] - p[kr])) <= 1e-12 * np.abs(p[kr]).max()
         W = v[:, 4:13].reshape(n, 3, 3)
         W0, kw0 = v[:, 13:22].reshape(n, 3, 3), kw.replace("_W", "_W0")
@@ -96,5 +96,8 @@ def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
             Fq = p["ortho_mgh_Fq"]
             assert np.max(np.abs(v[:, 1:4] - Fq)) <= 1e-10 * max(1.0, np.abs(Fq).max())
             H = p["ortho_mgh_H"]
-            assert np.max(np.abs(v[:, 22:].reshape(n, 3, 3) - H)) <= 1e-9 * max(1.0,
-                                                                               np.abs(H).max())
+            assert np.max(np.abs(v[:, 22:31].reshape(n, 3, 3) - H)) <= 1e-9 * max(
+                1.0, np.abs(H).max())
+            H0 = p["ortho_mgh_H0"]
+            assert np.max(np.abs(v[:, 31:].reshape(n, 3, 3) - H0)) <= 1e-9 * max(
+                1.0, np.abs(H0).max())

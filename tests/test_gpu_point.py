@@ -242,3 +242,17 @@ def test_point_hessian_against_reference(gpu_tables, name):
     assert np.array_equal(H, np.transpose(H, (0, 2, 1)))
     assert np.all(H[g["x"] < 5e-4] == 0.0)
     assert np.array_equal(S.pt_hessian(), H)
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_mf_hessian_against_reference(gpu_tables, name):
+    """Assembled mean-field Hessian blocks (sum over i in {u} U N(u) of
+    evaluate_D2V0_i_Dmeanq2_u_MgHx) within 1e-9 of max(1, the largest
+    entry); symmetric; reproducible."""
+    g, p = load(name), load("point")
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    H = S.mf_hessian()
+    assert err1(H, p[f"{name}_H0"]) < 1e-9
+    assert np.array_equal(H, np.transpose(H, (0, 2, 1)))
+    assert np.array_equal(S.mf_hessian(), H)
