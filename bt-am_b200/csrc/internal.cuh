@@ -102,6 +102,10 @@ cudaError_t launch_pt_totals(int n, const double *V, const double *Fq, const dou
 // the current state into the system's buffers (btam_capi.cu).
 int mf_rho64_enqueue(btam_system *s);
 
+// Enqueues the mean-field Hessian blocks of the current state into Hd (9
+// per real site) (mf_hessian.cu).
+int mf_hessian_enqueue(btam_system *s, double *Hd);
+
 // Enqueues the directed pass 1 and the mean-field stress of the current
 // state; *W: per-site stress (9 n), *tot: totals whose [2..10] hold the sum
 // (btam_capi.cu).

@@ -342,15 +342,9 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
 }  // namespace
 }  // namespace btam
 
-extern "C" {
-
-int btam_mf_hessian(btam_system *s, double *H) {
-  if (!s || !H) return BTAM_ERR_ARG;
-  if (!s->built) return BTAM_ERR_NOT_BUILT;
-  double *Hd = nullptr;
+int mf_hessian_enqueue(btam_system *s, double *Hd) {
   int st = mf_rho64_enqueue(s);  // rho-bar of the real sites into the system's rho
   if (st != BTAM_OK) return st;
-  BTAM_TRY(dalloc(Hd, s->st, 9 * (size_t)s->n_real));
   MfhArgs a;
   a.n_real = s->n_real;
   a.pos = s->pos;
@@ -366,7 +360,22 @@ int btam_mf_hessian(btam_system *s, double *H) {
   a.H = Hd;
   const int g = (int)(((long long)s->n_real * 32 + 127) / 128);
   if (g > 0) mf_hess_kernel<<<g, 128, 0, s->st>>>(a);
-  cudaError_t e = cudaGetLastError();
+  return cuda_status(cudaGetLastError());
+}
+
+extern "C" {
+
+int btam_mf_hessian(btam_system *s, double *H) {
+  if (!s || !H) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  double *Hd = nullptr;
+  BTAM_TRY(dalloc(Hd, s->st, 9 * (size_t)s->n_real));
+  int st = mf_hessian_enqueue(s, Hd);
+  if (st != BTAM_OK) {
+    dfree(Hd, s->st);
+    return st;
+  }
+  cudaError_t e = cudaSuccess;
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(H, Hd, 9 * (size_t)s->n_real * sizeof(double), cudaMemcpyDeviceToHost,
                         s->st);
