@@ -375,10 +375,8 @@ int btam_mf_hessian(btam_system *s, double *H) {
     dfree(Hd, s->st);
     return st;
   }
-  cudaError_t e = cudaSuccess;
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(H, Hd, 9 * (size_t)s->n_real * sizeof(double), cudaMemcpyDeviceToHost,
-                        s->st);
+  const cudaError_t e = cudaMemcpyAsync(H, Hd, 9 * (size_t)s->n_real * sizeof(double),
+                                        cudaMemcpyDeviceToHost, s->st);
   dfree(Hd, s->st);
   if (e != cudaSuccess) return cuda_status(e);
   return read_err(s);
