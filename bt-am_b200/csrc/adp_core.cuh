@@ -120,6 +120,9 @@ template <class R> struct RadialView {
   const R *pr;
   R dx, inv_dx;
   int n;
+  // the uw block again, laid out as the shared-memory kernels stage it
+  // (halves swapped where uw_swapped says), for one bulk copy; may be null
+  const R *uws = nullptr;
 };
 constexpr int kUWStride = 8;
 BTAM_HD int pr_stride(int pk) { return pk == 2 ? 16 : 8; }

@@ -174,18 +174,71 @@ template <> __device__ __forceinline__ void st_rec4<double>(double *p, const dou
 template <class R, bool SM> struct KView { using type = RadialView<R>; };
 template <> struct KView<float, true> { using type = RadialViewS<float>; };
 constexpr int kUWSharedMax = 3 * kUWStride * 1200;  // floats: up to 1200 segments
+// Bounded wait on phase 0 of a shared-memory mbarrier (true: completed).
+__device__ __forceinline__ bool mbar_wait0(unsigned bar) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
 template <class R, bool SM>
 __device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArgs<R> &a) {
   if constexpr (SM && sizeof(R) == 4) {
-    extern __shared__ __align__(32) float uw_dyn[];
+    // dynamic shared memory: the table (a multiple of 32 bytes), then an
+    // 8-byte mbarrier; the kernels that stage it hold no static shared memory
+    extern __shared__ __align__(128) float uw_dyn[];
     const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 floats
-    // 16-byte halves c of record c / 2, stored swapped where uw_swapped says
-    for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x) {
-      const int dst = uw_swapped(c >> 1) ? (c ^ 1) : c;
-      reinterpret_cast<float4 *>(uw_dyn)[dst] =
-          __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
+    bool staged = false;
+    if (a.T.uws) {
+      // one bulk copy of the pre-laid-out table (the tile is regular: one
+      // contiguous, 16-byte aligned block), completion on the mbarrier
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(uw_dyn);
+      const unsigned bar = dst + 4u * (unsigned)nuw;
+      const unsigned bytes = 4u * (unsigned)nuw;
+      if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned long long state;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+                     : "=l"(state)
+                     : "r"(bar), "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+            "[%3];" ::"r"(dst),
+            "l"(a.T.uws), "r"(bytes), "r"(bar)
+            : "memory");
+        (void)state;
+      }
+      staged = __syncthreads_and(mbar_wait0(bar)) != 0;
+      if (!staged) {  // the copy did not complete in time: flag it, wait
+                      // once more, then copy with the threads
+        if (threadIdx.x == 0) atomicOr(a.err, 1 << kErrBitTimeout);
+        mbar_wait0(bar);
+        __syncthreads();
+      }
     }
-    __syncthreads();
+    if (!staged) {
+      // 16-byte halves c of record c / 2, stored swapped where uw_swapped says
+      for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x) {
+        const int dst = uw_swapped(c >> 1) ? (c ^ 1) : c;
+        reinterpret_cast<float4 *>(uw_dyn)[dst] =
+            __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
+      }
+      __syncthreads();
+    }
     RadialViewS<float> T;
     T.uw = uw_dyn;
     T.pr = a.T.pr;
@@ -759,7 +812,7 @@ void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers, bool und, cudaEvent_t
 // most `full`.
 template <class K> int smem_grid(K kernel, int threads, size_t smem, int full) {
   cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(sizeof(float) * kUWSharedMax));
+                       (int)(sizeof(float) * kUWSharedMax + 16));
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -819,7 +872,8 @@ inline void go2u_smem(const EvalArgs<float> &a, cudaStream_t st, cudaEvent_t mid
     go2u<float, 128, 1>(a, st, false, mid);
     return;
   }
-  const size_t bytes = (size_t)3 * kUWStride * a.T.n * sizeof(float);
+  // the table and its 8-byte mbarrier (kernel_view)
+  const size_t bytes = (size_t)3 * kUWStride * a.T.n * sizeof(float) + 16;
   auto k = pass2u_pair_smem_kernel<TPB>;
   const int g = smem_grid(k, TPB, bytes, nblocks(a.n_own, TPB));
   if (g > 0) k<<<g, TPB, bytes, st>>>(a);

@@ -439,6 +439,24 @@ int btam_tables_load(const char *dir, btam_tables **out) {
   t->r32.dx = (float)rdx;
   t->r32.inv_dx = (float)(1.0 / rdx);
   t->r32.n = rn;
+  {  // the FP32 uw block with its 16-byte halves placed as the shared-memory
+     // kernels read them, so a block stages it with one bulk copy
+    const size_t nuw = (size_t)3 * kUWStride * rn;  // floats, a multiple of 8
+    std::vector<float> sw(nuw);
+    const float *src = r32.data() + uw32[0];
+    for (size_t c = 0; c < nuw / 4; ++c) {
+      const size_t dst = uw_swapped((int)(c >> 1)) ? (c ^ 1) : c;
+      for (int k = 0; k < 4; ++k) sw[4 * dst + k] = src[4 * c + k];
+    }
+    e = cudaMalloc(&t->uws32, nuw * sizeof(float));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(t->uws32, sw.data(), nuw * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      btam_tables_destroy(t);
+      return cuda_status(e);
+    }
+    t->r32.uws = t->uws32;
+  }
   *out = t;
   return BTAM_OK;
 }
@@ -449,6 +467,7 @@ void btam_tables_destroy(btam_tables *t) {
   if (t->d32) cudaFree(t->d32);
   if (t->rad64) cudaFree(t->rad64);
   if (t->rad32) cudaFree(t->rad32);
+  if (t->uws32) cudaFree(t->uws32);
   delete t;
 }
 

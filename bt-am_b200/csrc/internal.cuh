@@ -24,6 +24,7 @@ struct btam_tables {
   // the radial tables as the kernels' per-segment records
   double *rad64 = nullptr;
   float *rad32 = nullptr;
+  float *uws32 = nullptr;  // the FP32 uw block in its shared-memory layout
   RadialView<double> r64;
   RadialView<float> r32;
 };
