@@ -48,17 +48,17 @@ LOOK_PR, LOOK_TRIP = 48.0, 26.0
 # (--set full) of the undirected variants (28, 26): DRAM bytes (read +
 # write), and L1 global-load sectors (32 bytes each) with the L1 LSU
 # data-pipe utilisation
-NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 112.4e6, "pass1 site kernel": 66.0e6,
-                  "pass2 pair kernel": 254.9e6, "pass2 site kernel": 75.0e6, "totals": 1.5e6}
+NCU_DRAM_BYTES = {"pass1 pair-rule kernel": 113.1e6, "pass1 site kernel": 65.4e6,
+                  "pass2 pair kernel": 253.2e6, "pass2 site kernel": 75.4e6, "totals": 1.5e6}
 NCU_L1_SECTORS = {"pass1 pair-rule kernel": 51.73e6, "pass1 site kernel": 54.59e6,
-                  "pass2 pair kernel": 29.08e6, "pass2 site kernel": 2.56e6}
-NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.70,
-               "pass2 pair kernel": 0.745, "pass2 site kernel": 0.29}
+                  "pass2 pair kernel": 28.55e6, "pass2 site kernel": 2.56e6}
+NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.71,
+               "pass2 pair kernel": 0.69, "pass2 site kernel": 0.31}
 # shared-memory wavefronts per launch: the pass-2 pair kernel reads its u/w
 # spline records from shared memory (its global sectors are the moment and
 # pair records only)
 NCU_SHARED_WAVEFRONTS = {"pass1 pair-rule kernel": 0.45e6, "pass1 site kernel": 3.35e6,
-                         "pass2 pair kernel": 20.76e6, "pass2 site kernel": 1.37e6}
+                         "pass2 pair kernel": 15.30e6, "pass2 site kernel": 1.37e6}
 
 
 def kernel_flops(undirected):
