@@ -574,8 +574,8 @@ class Batch:
             pass
 
 
-JOB_RELAX, JOB_DMD, JOB_EVAL = 0, 1, 2
-RELAX_FP64, RELAX_MIXED, RELAX_FP32C = 0, 1, 2
+JOB_RELAX, JOB_DMD, JOB_EVAL, JOB_STRETCH = 0, 1, 2, 3
+RELAX_FP64, RELAX_MIXED, RELAX_FP32C, RELAX_NEWTON = 0, 1, 2, 3
 
 
 def estimate_bytes(sysdict):

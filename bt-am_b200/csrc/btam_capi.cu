@@ -1198,7 +1198,14 @@ int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m, const 
                double *info) {
   if (!s || !(tol > 0.0) || max_iter < 0 || m < 1 || m > 16) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
-  if (mode < 0 || mode > 2) return BTAM_ERR_ARG;
+  if (mode < 0 || mode > 3) return BTAM_ERR_ARG;
+  if (mode == BTAM_RELAX_NEWTON) {  // max_iter Newton steps, m unused
+    double inf6[6];
+    const int st = btam_relax_newton(s, tol, max_iter, 300, bounds, inf6);
+    if (info)
+      for (int c = 0; c < 5; ++c) info[c] = inf6[c];
+    return st;
+  }
   const double sig_lo = bounds ? bounds[0] : 0.001, sig_hi = bounds ? bounds[1] : 0.4,
                x_min = bounds ? bounds[2] : 0.01;
   if (!(sig_lo > 0.0 && sig_hi > sig_lo && x_min >= 0.0)) return BTAM_ERR_ARG;

@@ -118,6 +118,15 @@ void run_job(btam_server *srv, Job *job) {
       r.h_quanta_hi = tot[0];
       r.h_quanta_lo = tot[1];
       r.iterations = sp.nsteps;
+    } else if (sp.kind == BTAM_JOB_STRETCH) {
+      double F[3] = {1.0, 1.0, 1.0}, info[5] = {0, 0, 0, 0, 0};
+      st = btam_relax_stretch(s, sp.tol > 0 ? sp.tol : 1e-12, 1e-10,
+                              sp.max_iter > 0 ? sp.max_iter : 20, F, info);
+      r.norm = info[0];
+      r.iterations = (int)info[1];
+      r.evaluations = (int)info[2];
+      r.converged = info[3] > 0 ? 1 : 0;
+      r.objective = F[0] * F[1] * F[2];
     } else if (sp.kind == BTAM_JOB_EVAL) {
       double totals[4] = {0, 0, 0, 0};
       st = btam_mf_eval(s, sp.precision, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -232,7 +241,8 @@ int btam_server_submit(btam_server *srv, const btam_job_spec *sp, long long *job
   if (!srv || !sp || !job_id || sp->n <= 0 || !sp->q || !sp->sigma || !sp->x || !sp->species ||
       !sp->origin || !sp->cell || !sp->periodic)
     return BTAM_ERR_ARG;
-  if (sp->kind != BTAM_JOB_RELAX && sp->kind != BTAM_JOB_DMD && sp->kind != BTAM_JOB_EVAL)
+  if (sp->kind != BTAM_JOB_RELAX && sp->kind != BTAM_JOB_DMD && sp->kind != BTAM_JOB_EVAL &&
+      sp->kind != BTAM_JOB_STRETCH)
     return BTAM_ERR_ARG;
   auto job = std::make_unique<Job>();
   const size_t n = sp->n;

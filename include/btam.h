@@ -73,6 +73,7 @@ extern "C" {
 #define BTAM_RELAX_FP64 0        /* every evaluation in FP64 */
 #define BTAM_RELAX_MIXED 1       /* FP32C until |R| < 1e-5, then FP64 */
 #define BTAM_RELAX_FP32C 2       /* FP32C only (stops at its ~1e-6 noise floor) */
+#define BTAM_RELAX_NEWTON 3      /* btam_relax_newton (FP64): max_iter Newton steps, m unused */
 
 typedef struct btam_tables btam_tables;
 typedef struct btam_system btam_system;
@@ -408,6 +409,10 @@ typedef struct btam_server btam_server;
 #define BTAM_JOB_RELAX 0  /* btam_relax(mode, tol, max_iter, lbfgs_m, bounds) */
 #define BTAM_JOB_DMD 1    /* btam_dmd_setup + btam_dmd_step(precision, nsteps, dmd_params) */
 #define BTAM_JOB_EVAL 2   /* one btam_mf_eval(precision) */
+#define BTAM_JOB_STRETCH 3  /* btam_relax_stretch(atol = tol (0: 1e-12), rtol 1e-10,
+                              max_iter (0: 20)) from F = 1; result: norm |Y|,
+                              objective det F, iterations, evaluations,
+                              converged; the final state is the stretched q */
 
 typedef struct btam_job_spec {
   int kind;        /* BTAM_JOB_* */

@@ -26,6 +26,8 @@ def job_mix():
         (sph2, dict(kind=btam.JOB_DMD, precision=btam.FP64, nsteps=10)),
         (hexa, dict(kind=btam.JOB_EVAL, precision=btam.FP32C)),
         (sph2, dict(kind=btam.JOB_EVAL, precision=btam.FP64)),
+        (cell, dict(kind=btam.JOB_STRETCH, tol=1e-12, max_iter=20)),
+        (sph, dict(kind=btam.JOB_RELAX, mode=btam.RELAX_NEWTON, tol=1e-7, max_iter=40)),
     ]
 
 
@@ -87,3 +89,29 @@ def test_server_admission_by_memory(gpu_tables):
         srv.submit(big, kind=btam.JOB_EVAL)
     assert e.value.code == 15
     srv.close()
+
+
+def test_stretch_and_newton_jobs_equal_direct_calls(gpu_tables):
+    """A bulk stretch job and a Newton relaxation job give the final state,
+    residual and counts of the same calls made directly on a system."""
+    jobs = job_mix()
+    cell, kw_s = jobs[6]
+    sph, kw_n = jobs[7]
+    srv = btam.Server(gpu_tables, workers=2)
+    rs = srv.wait(srv.submit(cell, **kw_s))
+    rn = srv.wait(srv.submit(sph, **kw_n))
+    srv.close()
+    S = btam.System(gpu_tables, cell)
+    S.build_neighbors()
+    F, info = S.relax_stretch(atol=1e-12, rtol=1e-10, max_iter=20)
+    q, _, _ = S.get_state()
+    assert rs["status"] == 0 and rs["converged"] == 1 and info["status"] == 1
+    assert np.array_equal(rs["q"], q) and rs["objective"] == F[0] * F[1] * F[2]
+    N = btam.System(gpu_tables, sph)
+    N.build_neighbors()
+    N.set_variants(btam.FP64, 16 | 8 | 3, 16 | 8 | 0)
+    info = N.relax_newton(tol=1e-7, max_newton=40, max_cg=300)
+    qn, sn, _ = N.get_state()
+    assert rn["status"] == 0 and rn["converged"] == info["status"]
+    assert rn["norm"] == info["norm"] and rn["evaluations"] == info["evaluations"]
+    assert np.array_equal(rn["q"], qn) and np.array_equal(rn["sigma"], sn)
