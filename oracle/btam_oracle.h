@@ -1,6 +1,6 @@
 /* Test infrastructure only: the CPU oracle.  Nothing in the product library
  * links or calls this; only tests/, __graft_entry__.smoke() and bench.py's
- * CPU-baseline leg load it, as the checker.
+ * CPU-baseline leg load it, to check results or to time the CPU path.
  *
  * A plain restatement of the reference's algorithm for the mean-field ADP
  * path (each function cites the reference file:line it follows), plus the

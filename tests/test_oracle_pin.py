@@ -30,7 +30,7 @@ def test_splines_bit_exact(oracle):
         assert np.array_equal(d, g[f"t{t}_d"]), t
 
 
-def test_survey_known_values(oracle):
+def test_quoted_known_values(oracle):
     # Values of the reference's own code (quoted to 16 digits) for Mg-Mg at
     # q_j = (3.2, 0.1, 0.05), sigma = (0.10, 0.12), x = 1 and F_Mg(0.02).
     q = np.array([0, 0, 0, 3.2, 0.1, 0.05])
