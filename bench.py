@@ -165,10 +165,10 @@ def active_pairs(sys_, offs, idx, owner):
     return int(np.sum(act_i & (xa[idx] >= 5e-4)))
 
 
-def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0):
-    """Times the reference's own arithmetic (oracle/_ref, -Ofast build, all
-    host threads) on a bounded sample of one evaluation and extrapolates.
-    Returns (evals_per_s, description)."""
+def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1):
+    """Times the reference's own arithmetic (oracle/_ref, -Ofast build, on
+    `threads` host threads) on a bounded sample of one evaluation (divided
+    by `scale`) and extrapolates.  Returns (evals_per_s, description)."""
     import pyoracle
     ref = pyoracle.reference(fast=True)
     kind = "reference"
@@ -181,7 +181,7 @@ def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0):
     n = len(sys_["x"])
     full, nr, owner, image = pyoracle.expand(sys_, orc)
     # neighbour lists of the sampled sites and of their neighbours' owners
-    sample_rho = np.sort(rng.choice(n, 1200, replace=False)).astype(np.int32)
+    sample_rho = np.sort(rng.choice(n, 1200 // scale, replace=False)).astype(np.int32)
     sample_v0 = sample_rho[::12]
     sample_res = sample_rho[::100]
     need = set(map(int, sample_rho))
@@ -680,6 +680,9 @@ def run_btam(args, ws, rank, local):
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
         cpu = {"value": v, "unit": "evals/s", "cores": os.cpu_count() or 1, "kind": kind,
                "sample": desc}
+        # the same arithmetic on one thread, on a quarter of the sample
+        v1, desc1, _, _ = cpu_reference_sample(sys_, 1, seed=1, scale=4)
+        cpu["single_thread"] = {"value": v1, "unit": "evals/s", "cores": 1, "sample": desc1}
     if rank == 0:
         line = {"metric": METRIC, "value": results["fp32c"]["value"], "unit": "evals/s",
                 "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
