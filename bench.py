@@ -463,6 +463,41 @@ def bench_bulk_stretch(args, tables, cpu_budget_s=6.0):
     return out
 
 
+def bench_config1(args, tables):
+    """The CPU-runnable workload end to end: periodic 5x5x5 hexagonal cells
+    (250 Mg, 100 H at x ~ U[0, 0.1]), one relaxation of (q, sigma) to
+    |R| <= 1e-8 (the Newton option; L-BFGS beside it), then 10
+    master-equation steps with dt = 1e-3, all in FP64."""
+    import torch
+    import btam
+    from btam import lattice
+
+    sys_ = lattice.config1()
+    out = {"workload": "periodic 5x5x5 hexagonal cells, 250 Mg + 100 H (x ~ U[0, 0.1]), "
+                       "relaxation to |R| <= 1e-8 then 10 master-equation steps (dt 1e-3), FP64",
+           "sites": len(sys_["x"])}
+    for name in ("newton", "lbfgs"):
+        S = btam.System(tables, sys_)
+        S.build_neighbors()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        if name == "newton":
+            info = S.relax_newton(tol=1e-8, max_newton=100, max_cg=300)
+        else:
+            info = S.relax(mode=btam.RELAX_FP64, tol=1e-8, max_iter=2000)
+        t1 = time.perf_counter()
+        S.dmd_setup()
+        S.dmd_step(10, btam.FP64, dt=1e-3)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        out[name] = {"relax_ms": (t1 - t0) * 1e3, "relax_evaluations": info["evaluations"],
+                     "relax_norm": info["norm"], "converged": info["status"] == 1,
+                     "dmd_10_steps_ms": (t2 - t1) * 1e3, "total_ms": (t2 - t0) * 1e3}
+        S.close()
+    out["timing"] = "host clock around each call (device-resident loops)"
+    return out
+
+
 def bench_serving(args, tables):
     """The served workload: a seeded Poisson stream (mean 200 jobs/s) of 64
     jobs, half relaxations (L-BFGS to |R| <= 1e-5 or 100 iterations) and half
@@ -675,6 +710,7 @@ def run_btam(args, ws, rank, local):
     serving = None if args.no_serve else bench_serving(args, tables)
     nanowire = None if args.no_wire else bench_nanowire(args, tables)
     stretch = None if args.no_stretch else bench_bulk_stretch(args, tables)
+    config1 = None if args.no_stretch else bench_config1(args, tables)
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
@@ -710,7 +746,8 @@ def run_btam(args, ws, rank, local):
                         "ms_per_step": e2e_ms},
                 "gpu_launches": launches_per_eval(shapes["fp32c"]) * args.steps,
                 "clocks": clocks, "batched": batched, "serving": serving,
-                "precision_nanowire": nanowire, "bulk_stretch": stretch}
+                "precision_nanowire": nanowire, "bulk_stretch": stretch,
+                "config1_workflow": config1}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -729,7 +766,7 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=64, help="jobs in the served stream")
     ap.add_argument("--no-wire", action="store_true", help="skip the nanowire DMD workload")
     ap.add_argument("--no-stretch", action="store_true",
-                    help="skip the bulk stretch relaxation workload")
+                    help="skip the bulk stretch relaxation and config-1 workflow workloads")
     ap.add_argument("--dmd-steps", type=int, default=1000,
                     help="master-equation steps of the nanowire workload")
     args = ap.parse_args()
