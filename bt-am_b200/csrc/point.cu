@@ -63,6 +63,19 @@ __device__ __forceinline__ void ld_rec(const double *r, double (&a)[kPtRec]) {
     a[8 + k] = hi[k];
   }
 }
+// Its first 12 values (rho .. tr Lambda), all a gradient needs: three
+// 256-bit loads.
+__device__ __forceinline__ void ld_rec12(const double *r, double (&a)[kPtRec]) {
+  double lo[8], hi[4];
+  ld8(r, lo);
+  ld4(r + 8, hi);
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = lo[k];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) a[8 + k] = hi[k];
+#pragma unroll
+  for (int k = 12; k < kPtRec; ++k) a[k] = 0.0;
+}
 
 // Pass 1: rho_i = sum_j x_j rho_{s_j}(r) (evaluate_rho_i_adp_MgHx,
 // MgHx-mf-V-bulk.cpp:83-143), the moments and the point energy.  Neighbours
@@ -170,7 +183,7 @@ __global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a) {
       const double t = xu * xj;
       const V3<double> gu = pt_grad(mu_, r, g, t, xj, drj, dph);
       double mo[kPtRec];
-      ld_rec(a.rec + (size_t)kPtRec * a.owner[j], mo);
+      ld_rec12(a.rec + (size_t)kPtRec * a.owner[j], mo);
       const V3<double> rn = mk3<double>(-r.x, -r.y, -r.z);
       const V3<double> hj = pt_grad(mo, rn, g, t, xu, dru, dph);
       acc[0] += hj.x - gu.x;
