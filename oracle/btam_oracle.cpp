@@ -332,11 +332,23 @@ struct Term {
   double (*F)(const double *, const double *, const int *);
   void (*dq)(int, double *, const double *, const double *, const int *);
   double (*dn)(int, const double *, const double *, const int *);
+  int id;  // 0 rho, 1 pair, 2 dipole, 3 quadrupole
 };
-const Term kRho = {rho_F, rho_dq, rho_dn};
-const Term kPair = {pair_F, pair_dq, pair_dn};
-const Term kDip = {dip_F, dip_dq, dip_dn};
-const Term kQuad = {quad_F, quad_dq, quad_dn};
+const Term kRho = {rho_F, rho_dq, rho_dn, 0};
+const Term kPair = {pair_F, pair_dq, pair_dn, 1};
+const Term kDip = {dip_F, dip_dq, dip_dn, 2};
+const Term kQuad = {quad_F, quad_dq, quad_dn, 3};
+
+// The integration rule behind the reference's compile switch
+// (MgHx-mf-V-bulk.cpp:715-724): 0 the degree-3 Gauss-Hermite rule
+// (GH3TH_INTEGRAL, the shipped build); 1 the multipole rule
+// (MULTIPOLE_INTEGRAL) as the reference's build flags compile it, whose
+// `#ifdef NUMERICAL_DERIVATIVES` (Quadrature-Multipole.cpp:134, 185) holds
+// under CMakeLists.txt:185's -DNUMERICAL_DERIVATIVES=0 and selects the
+// finite-difference Hessians; 2 the multipole rule with the analytic
+// Hessians (NUMERICAL_DERIVATIVES undefined).  The occupancy derivative
+// always uses the degree-3 rule (meanfield_integral_gh_3th_dxi, 2160-2257).
+int gRule = 0;
 
 // ---------------------------------------------------------------------------
 // Gaussian measure (Quadrature-Measure.cpp:30-109): reduce the dof table so
@@ -345,6 +357,7 @@ const Term kQuad = {quad_F, quad_dq, quad_dn};
 struct Measure {
   int ns = 0, D = 0;
   int board[9][9];
+  int dof[9];
   const double *mean, *sigma, *x;
   const int *spc;
 };
@@ -358,6 +371,7 @@ Measure make_measure(const double *mean, const double *sigma, const double *x,
   m.x = x;
   m.spc = spc;
   int aux[3][3];
+  for (int k = 0; k < ns * ns; ++k) m.dof[k] = dof[k];
   for (int i = 0; i < ns; ++i)
     for (int j = 0; j < ns; ++j) aux[i][j] = dof[i * ns + j];
   for (int i = 0; i < ns; ++i)
@@ -391,7 +405,12 @@ void point(const Measure &m, int l, double sgn, double *ql) {
     }
 }
 
+double integ_mp(const Term &f, const Measure &m);
+void integ_mp_dmq(int dir, const Term &f, const Measure &m, double *out);
+double integ_mp_dsq(int dir, const Term &f, const Measure &m);
+
 double integ(const Term &f, const Measure &m) {
+  if (gRule != 0) return integ_mp(f, m);
   double W = 1.0 / (2.0 * m.D), acc = 0.0, ql[9];
   for (double sgn : {1.0, -1.0})
     for (int l = 0; l < m.D; ++l) {
@@ -403,6 +422,7 @@ double integ(const Term &f, const Measure &m) {
 
 // meanfield_integral_gh_3th_dmq (212-296)
 void integ_dmq(int dir, const Term &f, const Measure &m, double *out) {
+  if (gRule != 0) return integ_mp_dmq(dir, f, m, out);
   double W = 1.0 / (2.0 * m.D), ql[9], g[3];
   for (int a = 0; a < 3; ++a) out[a] = 0.0;
   for (double sgn : {1.0, -1.0})
@@ -415,6 +435,7 @@ void integ_dmq(int dir, const Term &f, const Measure &m, double *out) {
 
 // meanfield_integral_gh3th_dsq (114-208)
 double integ_dsq(int dir, const Term &f, const Measure &m) {
+  if (gRule != 0) return integ_mp_dsq(dir, f, m);
   double W = 1.0 / (2.0 * m.D), ql[9], g[3], acc = 0.0;
   double zeta = std::sqrt((double)m.D) / kSqrt2;
   for (double sgn : {1.0, -1.0})
@@ -938,6 +959,137 @@ void integ_d2(int term, int a, const Measure &m, double *out9) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Multipole rule (Quadrature-Multipole.cpp:97-288).
+
+// Trace of the j1-j2 cross block of a triplet term (directions 5 and 7 of
+// dV2_dipole_ij1j2_dq2, MgHx-ADP.cpp:1435-1603, and of
+// dV2_quadrupole_ij1j2_dq2, 2000-2268; both blocks have the same trace).
+// With r_k = q_0 - q_k, s_k = |r_k|, d = r_1.r_2 and c_k = n_0 n_k:
+//   dipole      1/2 c1 c2 (u1' u2' d^2/(s1 s2) + u1' u2 s1 + u1 u2' s2 + 3 u1 u2)
+//   quadrupole  1/2 c1 c2 d (w1' w2' d^2/(s1 s2) + 2 w1' w2 s1 + 2 w1 w2' s2 + 8 w1 w2)
+//               - 1/6 c1 c2 d (w1' s1 + 2 w1)(w2' s2 + 2 w2)
+double tri_cross_trace(int term, const double *n, const double *q, const int *spc) {
+  Tri t = tri_geom(q);
+  const double c1 = n[0] * n[1], c2 = n[0] * n[2];
+  const Spline &S1 = term == 2 ? pot_of(spc[0], spc[1]).u : pot_of(spc[0], spc[1]).w;
+  const Spline &S2 = term == 2 ? pot_of(spc[0], spc[2]).u : pot_of(spc[0], spc[2]).w;
+  const double f1 = spline_val(S1, t.n1), d1 = spline_d1(S1, t.n1);
+  const double f2 = spline_val(S2, t.n2), d2 = spline_d1(S2, t.n2);
+  const double d = t.dot;
+  if (term == 2)
+    return 0.5 * c1 * c2 * (d1 * d2 * d * d / (t.n1 * t.n2) + d1 * f2 * t.n1 + f1 * d2 * t.n2 +
+                            3.0 * f1 * f2);
+  return 0.5 * c1 * c2 * d *
+             (d1 * d2 * d * d / (t.n1 * t.n2) + 2.0 * d1 * f2 * t.n1 + 2.0 * f1 * d2 * t.n2 +
+              8.0 * f1 * f2) -
+         c1 * c2 * d * (d1 * t.n1 + 2.0 * f1) * (d2 * t.n2 + 2.0 * f2) / 6.0;
+}
+
+// Diagonal entry (al, al) of the finite-difference Hessian of block
+// `direction` (d2_rho_ij_dq2_FD, MgHx-ADP.cpp:736-812; d2V_pair_ij_dq2_FD,
+// 1091-1167; dV2_dipole_ij1j2_dq2_FD, 1605-1680;
+// dV2_quadrupole_ij1j2_dq2_FD, 2270-2349): the five-point second difference
+// (step 1e-4) of f in coordinate al of slot direction / (ns + 1).  Only the
+// diagonal entries are formed.  The j1-j2 cross directions 5 and 7 map to
+// slot 1 for the dipole and give zero for the quadrupole (whose FD Hessian
+// forms directions 0, 4 and 8 only, 2291).
+double fd_hess_diag(const Term &f, int ns, int direction, int al, const Measure &m,
+                    const double *q) {
+  if (f.id == 3 && direction != 0 && direction != 4 && direction != 8) return 0.0;
+  const double dr = 0.0001;
+  const int k = direction / (1 + ns) * 3 + al;
+  double qpp[9], qp[9], qm[9], qmm[9];
+  for (int c = 0; c < 3 * ns; ++c) {
+    const double D = c == k ? 1.0 : 0.0;
+    qpp[c] = q[c] + D * dr * 2;
+    qp[c] = q[c] + D * dr;
+    qm[c] = q[c] - D * dr;
+    qmm[c] = q[c] - D * dr * 2;
+  }
+  const double f0 = f.F(m.x, q, m.spc);
+  const double fpp = f.F(m.x, qpp, m.spc), fp = f.F(m.x, qp, m.spc);
+  const double fm = f.F(m.x, qm, m.spc), fmm = f.F(m.x, qmm, m.spc);
+  return (-fpp + 16.0 * fp - 30.0 * f0 + 16.0 * fm - fmm) / (12.0 * dr * dr);
+}
+
+// Trace of block `direction` = a * ns + b of d2F/dq2 (the reference's
+// d2F_dq2 convention), analytic.  The dof tables of the pair and triplet
+// measures request the diagonal blocks and, for j1 = j2, the j1-j2 cross
+// blocks.
+double block_trace(const Term &f, int ns, int direction, const Measure &m, const double *q) {
+  const int a = direction / ns, b = direction % ns;
+  if (a == b) {
+    double H[9];
+    term_d2(f.id, a, m.x, q, m.spc, H);
+    return H[0] + H[4] + H[8];
+  }
+  if (ns == 3 && a > 0 && b > 0) return tri_cross_trace(f.id, m.x, q, m.spc);
+  return 0.0;
+}
+
+// meanfield_integral_mp (Quadrature-Multipole.cpp:97-143):
+//   f(mean) + sum_{(a, b) in dof} sigma_a^2 / 2 tr d2f/dq_a dq_b.
+double integ_mp(const Term &f, const Measure &m) {
+  double acc = f.F(m.x, m.mean, m.spc);
+  for (int a = 0; a < m.ns; ++a) {
+    const double c2 = sq(m.sigma[a]) / 2.0;
+    for (int b = 0; b < m.ns; ++b) {
+      if (m.dof[a * m.ns + b] != 1) continue;
+      if (gRule == 1)
+        for (int al = 0; al < 3; ++al) acc += c2 * fd_hess_diag(f, m.ns, a * m.ns + b, al, m, m.mean);
+      else
+        acc += c2 * block_trace(f, m.ns, a * m.ns + b, m, m.mean);
+    }
+  }
+  return acc;
+}
+
+// meanfield_integral_mp_dsq (147-196): sigma_dir sum_{b in dof row dir} tr
+// d2f/dq_dir dq_b.
+double integ_mp_dsq(int dir, const Term &f, const Measure &m) {
+  double acc = 0.0;
+  for (int b = 0; b < m.ns; ++b) {
+    if (m.dof[dir * m.ns + b] != 1) continue;
+    if (gRule == 1)
+      for (int al = 0; al < 3; ++al)
+        acc += m.sigma[dir] * fd_hess_diag(f, m.ns, dir * m.ns + b, al, m, m.mean);
+    else
+      acc += m.sigma[dir] * block_trace(f, m.ns, dir * m.ns + b, m, m.mean);
+  }
+  return acc;
+}
+
+// meanfield_integral_mp_dmq (200-286): grad_dir f(mean) plus, for every
+// site slot s and axis al, sigma_s^2 / 2 times the five-point second
+// difference (step 0.01) of grad_dir f in q_{s, al}.  Each slot moves
+// alone, also when two slots hold the same site.
+void integ_mp_dmq(int dir, const Term &f, const Measure &m, double *out) {
+  const double dr = 0.01;
+  double g0[3], gpp[3], gp[3], gm[3], gmm[3], qk[9];
+  f.dq(dir, g0, m.x, m.mean, m.spc);
+  for (int a = 0; a < 3; ++a) out[a] = g0[a];
+  for (int k = 0; k < 3 * m.ns; ++k) qk[k] = m.mean[k];
+  for (int s = 0; s < m.ns; ++s) {
+    const double c2 = sq(m.sigma[s]) / 2.0;
+    for (int al = 0; al < 3; ++al) {
+      const int k = 3 * s + al;
+      qk[k] = m.mean[k] + dr * 2;
+      f.dq(dir, gpp, m.x, qk, m.spc);
+      qk[k] = m.mean[k] + dr;
+      f.dq(dir, gp, m.x, qk, m.spc);
+      qk[k] = m.mean[k] - dr;
+      f.dq(dir, gm, m.x, qk, m.spc);
+      qk[k] = m.mean[k] - dr * 2;
+      f.dq(dir, gmm, m.x, qk, m.spc);
+      qk[k] = m.mean[k];
+      for (int b = 0; b < 3; ++b)
+        out[b] += c2 * ((-gpp[b] + 16.0 * gp[b] - 30.0 * g0[b] + 16.0 * gm[b] - gmm[b]) /
+                        (12.0 * dr * dr));
+    }
+  }
+}
+
 // evaluate_D2V0_i_Dmeanq2_u_MgHx (MgHx-mf-V-bulk.cpp:1366-1600).
 void D2V0_dq2(const View &v, int u, int i, double *out9) {
   for (int c = 0; c < 9; ++c) out9[c] = 0.0;
@@ -1077,6 +1229,8 @@ void par_for(int n, const std::function<void(int)> &fn) {
 
 // ===========================================================================
 extern "C" {
+
+void orc_set_rule(int rule) { gRule = (rule == 1 || rule == 2) ? rule : 0; }
 
 int orc_load_tables(const char *dir) {
   std::string d(dir);

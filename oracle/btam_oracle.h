@@ -22,6 +22,12 @@ extern "C" {
 /* Table ids: 0 rho_Mg, 1 rho_H, 2 F_Mg, 3 F_H, 4/5/6 phi MgMg/HH/MgH,
  * 7/8/9 u MgMg/HH/MgH, 10/11/12 w MgMg/HH/MgH. */
 int orc_load_tables(const char *dir);
+/* Integration rule of the mean-field forms: 0 the degree-3 Gauss-Hermite
+ * rule (default, the reference's shipped build); 1 the multipole rule as
+ * the reference's build flags compile it (-DMULTIPOLE_INTEGRAL with
+ * -DNUMERICAL_DERIVATIVES=0: finite-difference Hessians); 2 the multipole
+ * rule with analytic Hessians (NUMERICAL_DERIVATIVES undefined). */
+void orc_set_rule(int rule);
 double orc_spline(int table, double r, int deriv);
 int orc_table_info(int table, double *dx);
 double orc_mass(int species);

@@ -19,6 +19,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libbtam_oracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbtam_ref.so")
 REF_FAST_SO = os.path.join(HERE, "_ref", "libbtam_ref_fast.so")
+REF_MP_SO = os.path.join(HERE, "_ref", "libbtam_ref_mp.so")
+REF_MPA_SO = os.path.join(HERE, "_ref", "libbtam_ref_mpa.so")
 TABLES = os.path.join(os.path.dirname(HERE), "bt-am_b200", "data")
 
 _D = ctypes.POINTER(ctypes.c_double)
@@ -179,6 +181,12 @@ class Oracle(Lib):
         super().__init__(build_oracle(), "orc", tables)
         self._f("mass").restype = ctypes.c_double
 
+    def set_rule(self, rule):
+        """0: degree-3 Gauss-Hermite rule (the shipped build); 1: multipole
+        with finite-difference Hessians (the reference's build flags); 2:
+        multipole with analytic Hessians."""
+        self._f("set_rule")(int(rule))
+
     def mass(self, species):
         return self._f("mass")(int(species))
 
@@ -231,6 +239,15 @@ class Oracle(Lib):
 def reference(fast=False, tables=TABLES):
     """The reference's own arithmetic (shim build), or None if not built."""
     path = REF_FAST_SO if fast else REF_SO
+    if not os.path.exists(path):
+        return None
+    return Lib(path, "ref", tables)
+
+
+def reference_multipole(analytic=False, tables=TABLES):
+    """The reference built with -DMULTIPOLE_INTEGRAL (and, unless `analytic`,
+    its own -DNUMERICAL_DERIVATIVES=0), or None if not built."""
+    path = REF_MPA_SO if analytic else REF_MP_SO
     if not os.path.exists(path):
         return None
     return Lib(path, "ref", tables)

@@ -13,6 +13,8 @@ Run from the repository root, with the reference tree present:
     python tests/golden/make_golden.py            # every fixture
     python tests/golden/make_golden.py --point    # point.npz only (it reads
                                                   # the system fixtures)
+    python tests/golden/make_golden.py --multipole  # multipole.npz only (it
+                                                    # reads the system fixtures)
 """
 import os
 import sys
@@ -172,10 +174,48 @@ def point_fixture(ref):
     np.savez_compressed(os.path.join(OUT, "point.npz"), **out)
 
 
+def multipole_fixture():
+    """The mean-field forms under the multipole rule (MULTIPOLE_INTEGRAL),
+    from the reference built two ways (oracle/Makefile): with its own
+    -DNUMERICAL_DERIVATIVES=0, which selects finite-difference Hessians
+    (rule 1), and without it, analytic Hessians (rule 2).  On the stored
+    topologies of two system fixtures: rho-bar, V0, S0 of every real site
+    and the assembled residuals of a sample of sites."""
+    out = {}
+    for rule, analytic in ((1, False), (2, True)):
+        ref = pyoracle.reference_multipole(analytic)
+        if ref is None:
+            sys.exit("oracle/_ref/libbtam_ref_mp*.so missing: run `make -C oracle ref` first")
+        for name in ("sphere", "ortho_mgh"):
+            g = np.load(os.path.join(OUT, f"{name}.npz"))
+            n = len(g["x"])
+            owner, image, offs, idx = g["owner"], g["image"], g["offs"], g["idx"]
+            full = {"q": np.ascontiguousarray(g["q_all"]),
+                    "sigma": np.ascontiguousarray(g["sigma"][owner]),
+                    "x": np.ascontiguousarray(g["x"][owner]),
+                    "species": np.ascontiguousarray(g["species"][owner]),
+                    "beta": np.ascontiguousarray(g["beta"][owner]),
+                    "gamma": np.ascontiguousarray(g["gamma"][owner])}
+            real = np.arange(n, dtype=np.int32)
+            rho_real = ref.mf_rho(full, offs, idx, real)
+            rho = rho_real[owner]
+            us = np.arange(0, n, max(1, n // 40), dtype=np.int32)
+            Rq, Rs, Rx = assemble(ref, full, rho, owner, image, offs, idx, us)
+            key = f"{name}_r{rule}_"
+            out.update({key + "rho": rho_real, key + "V0": ref.V0(full, rho, offs, idx, real),
+                        key + "S0": ref.S0(full, rho, offs, idx, real), key + "res_sites": us,
+                        key + "Rq": Rq, key + "Rs": Rs, key + "Rx": Rx})
+            print(f"multipole rule {rule} {name}: {n} real, {len(us)} residual sites")
+    np.savez_compressed(os.path.join(OUT, "multipole.npz"), **out)
+
+
 def main():
     ref = pyoracle.reference()
     if ref is not None and sys.argv[1:] == ["--point"]:
         point_fixture(ref)
+        return
+    if sys.argv[1:] == ["--multipole"]:
+        multipole_fixture()
         return
     if ref is None:
         sys.exit("oracle/_ref/libbtam_ref.so missing: run `make -C oracle ref` first")
@@ -230,6 +270,7 @@ def main():
     system_fixture("ortho_mgh", ortho, ref, orc)
     system_fixture("config1", lattice.config1(), ref, orc, residual_sample=40, seed=1)
     point_fixture(ref)
+    multipole_fixture()
 
 
 if __name__ == "__main__":

@@ -184,3 +184,71 @@ def test_point_forms_match_reference_live(oracle, ref):
     q0 = full["q"] + 0.01
     assert np.array_equal(oracle.pt_DV_dF(full, q0, rho, offs, idx, real),
                           ref.pt_DV_dF(full, q0, rho, offs, idx, real))
+
+
+@pytest.mark.parametrize("rule", [1, 2])
+@pytest.mark.parametrize("name", ["sphere", "ortho_mgh"])
+def test_multipole_rule_against_golden(oracle, name, rule):
+    """The multipole rule (MULTIPOLE_INTEGRAL, Quadrature-Multipole.cpp) of
+    the restated oracle against the reference built with it: rule 1 with the
+    reference's own -DNUMERICAL_DERIVATIVES=0 (finite-difference Hessians,
+    bit-exact), rule 2 with analytic Hessians (operation order differs)."""
+    g = load(name)
+    m = load("multipole")
+    key = f"{name}_r{rule}_"
+    n = len(g["x"])
+    owner, image, offs, idx = g["owner"], g["image"], g["offs"], g["idx"]
+    full = {"q": g["q_all"], "sigma": g["sigma"][owner], "x": g["x"][owner],
+            "species": g["species"][owner], "beta": g["beta"][owner],
+            "gamma": g["gamma"][owner]}
+    real = np.arange(n, dtype=np.int32)
+    oracle.set_rule(rule)
+    try:
+        rho = oracle.mf_rho(full, offs, idx, real)
+        V0 = oracle.V0(full, rho[owner], offs, idx, real)
+        S0 = oracle.S0(full, rho[owner], offs, idx, real)
+        Rq, Rs, Rx = oracle.residuals(full, rho[owner], owner, image, offs, idx,
+                                      m[key + "res_sites"])
+    finally:
+        oracle.set_rule(0)
+    if rule == 1:
+        assert np.array_equal(rho, m[key + "rho"])
+        assert np.array_equal(V0, m[key + "V0"])
+        assert np.array_equal(S0, m[key + "S0"])
+    else:
+        for a, b in ((rho, m[key + "rho"]), (V0, m[key + "V0"]), (S0, m[key + "S0"])):
+            assert np.allclose(a, b, rtol=1e-13, atol=0)
+    for a, b in ((Rq, m[key + "Rq"]), (Rs, m[key + "Rs"]), (Rx, m[key + "Rx"])):
+        assert np.allclose(a, b, rtol=0, atol=1e-13 * max(1.0, np.abs(b).max()))
+    # the rule changes the result: rule 1 against the degree-3 rule's rho-bar
+    assert np.abs(rho - g["rho"]).max() > 1e-6 * np.abs(g["rho"]).max()
+
+
+def test_multipole_rule_matches_reference_live(oracle):
+    import pyoracle
+    from btam import lattice
+    ref = pyoracle.reference_multipole()
+    if ref is None:
+        pytest.skip("reference multipole build oracle/_ref absent (needs the reference tree)")
+    s = lattice.cluster("sphere", 6.0, x_fn=lambda g, r, n: g.uniform(0.0, 0.7, n),
+                        h_fraction=0.6, seed=12)
+    full, n, owner, image = pyoracle.expand(s, oracle)
+    offs, idx = oracle.neighbors(full["q"])
+    real = np.arange(n, dtype=np.int32)
+    us, is_ = [], []
+    for u in range(0, n, 7):
+        for i in [u, *idx[offs[u]:offs[u + 1]]]:
+            us.append(u)
+            is_.append(i)
+    oracle.set_rule(1)
+    try:
+        r1 = oracle.mf_rho(full, offs, idx, real)
+        v1 = oracle.V0(full, r1, offs, idx, real)
+        a4, ax = oracle.DV0_pairs(full, r1, offs, idx, us, is_)
+    finally:
+        oracle.set_rule(0)
+    r2 = ref.mf_rho(full, offs, idx, real)
+    assert np.array_equal(r1, r2)
+    assert np.array_equal(v1, ref.V0(full, r2, offs, idx, real))
+    b4, bx = ref.DV0_pairs(full, r2, offs, idx, us, is_)
+    assert np.array_equal(a4, b4) and np.array_equal(ax, bx)
