@@ -72,6 +72,8 @@ _PROTOS = {
     "btam_stretch_apply": (ctypes.c_int, [_V, _D]),
     "btam_pt_hessian": (ctypes.c_int, [_V, _D]),
     "btam_mf_hessian": (ctypes.c_int, [_V, _D]),
+    "btam_mf_eval_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D,
+                                              ctypes.POINTER(ctypes.c_double)]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
@@ -444,6 +446,18 @@ class System:
         _check(lib().btam_pt_hessian(self.handle, _d(H)), "btam_pt_hessian")
         return H
 
+    def mf_eval_multipole(self, rule=1):
+        """rho-bar, V0 per site and their sum under the multipole rule
+        (MULTIPOLE_INTEGRAL): rule MP_FD (1) with the finite-difference
+        Hessians of the reference's build flags, MP_ANALYTIC (2) with
+        analytic Hessians.  FP64."""
+        rho = np.zeros(self.n)
+        V0 = np.zeros(self.n)
+        E = ctypes.c_double(0.0)
+        _check(lib().btam_mf_eval_multipole(self.handle, int(rule), _d(rho), _d(V0),
+                                            ctypes.byref(E)), "btam_mf_eval_multipole")
+        return rho, V0, E.value
+
     def mf_hessian(self):
         """Mean-field Hessian blocks, (n, 3, 3): the sum over i in {u} U N(u)
         of evaluate_D2V0_i_Dmeanq2_u_MgHx (FP64)."""
@@ -576,6 +590,7 @@ class Batch:
 
 JOB_RELAX, JOB_DMD, JOB_EVAL, JOB_STRETCH = 0, 1, 2, 3
 RELAX_FP64, RELAX_MIXED, RELAX_FP32C, RELAX_NEWTON = 0, 1, 2, 3
+MP_FD, MP_ANALYTIC = 1, 2
 
 
 def estimate_bytes(sysdict):

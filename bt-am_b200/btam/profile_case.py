@@ -39,6 +39,9 @@ def main():
     ap.add_argument("--evals", type=int, default=4)
     ap.add_argument("--stretch", action="store_true",
                     help="run the bulk stretch relaxation (non-mean-field forms) instead")
+    ap.add_argument("--multipole", type=int, default=0, choices=[0, 1, 2],
+                    help="evaluate rho-bar and V0 under the multipole rule (1: FD Hessians, "
+                         "2: analytic) instead")
     args = ap.parse_args()
     prec = btam.FP32C if args.precision == "fp32c" else btam.FP64
     if args.workload == "dropin":
@@ -48,6 +51,20 @@ def main():
     tables = btam.Tables()
     S = btam.System(tables, sysd)
     S.build_neighbors()
+    if args.multipole:
+        S.mf_eval_multipole(args.multipole)  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(args.evals):
+            rho, V0, E = S.mf_eval_multipole(args.multipole)
+        dt = time.perf_counter() - t0
+        nr, ng, npairs = S.info()
+        print(json.dumps({"workload": args.workload, "multipole_rule": args.multipole,
+                          "sites": nr, "pairs": npairs, "evals": args.evals,
+                          "wall_ms_per_eval": dt * 1e3 / args.evals, "energy": E,
+                          "finite": bool(np.isfinite(V0).all())}))
+        S.close()
+        tables.close()
+        return
     if args.stretch:
         t0 = time.perf_counter()
         F, info = S.relax_stretch(atol=1e-12, rtol=1e-10, max_iter=20)

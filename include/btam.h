@@ -206,6 +206,27 @@ int btam_mf_stress(btam_system *s, int precision, double *W0, double *total);
  * state's values). */
 int btam_mf_hessian(btam_system *s, double *H);
 
+/* ---- the multipole rule (MULTIPOLE_INTEGRAL) ------------------------------
+ * The reference's alternative mean-field rule behind its compile switch
+ * (MgHx-mf-V-bulk.cpp:715-724; meanfield_integral_mp,
+ * Quadrature-Multipole.cpp:97-143): <f> = f(mean) + sum over the measure's
+ * dof table of sigma_a^2 / 2 tr d2f/dq_a dq_b.  Two Hessian variants:
+ *   BTAM_MP_FD        as the reference's build flags compile it
+ *                     (-DNUMERICAL_DERIVATIVES=0 satisfies the rule's
+ *                     #ifdef): finite-difference Hessians, step 1e-4,
+ *                     diagonal entries only (MgHx-ADP.cpp:736-812,
+ *                     1091-1167, 1605-1680, 2270-2349);
+ *   BTAM_MP_ANALYTIC  NUMERICAL_DERIVATIVES undefined: analytic Hessians.
+ * Replaces evaluate_mf_rho_i_adp_MgHx (708-787) and evaluate_V0_i_adp_MgHx
+ * (791-953) built with that rule: rho (n_real, may be NULL) the multipole
+ * rho-bar, V0 (n_real, may be NULL) the per-site V0, *energy (may be NULL)
+ * their sum.  FP64, a direct evaluation of the reference's pair and
+ * triplet sums on the system's neighbour lists (kept as built). */
+#define BTAM_MP_FD 1
+#define BTAM_MP_ANALYTIC 2
+int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0,
+                           double *energy);
+
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);
