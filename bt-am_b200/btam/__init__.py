@@ -74,6 +74,7 @@ _PROTOS = {
     "btam_mf_hessian": (ctypes.c_int, [_V, _D]),
     "btam_mf_eval_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D,
                                               ctypes.POINTER(ctypes.c_double)]),
+    "btam_mf_residuals_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
@@ -457,6 +458,15 @@ class System:
         _check(lib().btam_mf_eval_multipole(self.handle, int(rule), _d(rho), _d(V0),
                                             ctypes.byref(E)), "btam_mf_eval_multipole")
         return rho, V0, E.value
+
+    def mf_residuals_multipole(self, rule=1):
+        """(Rq (n, 3), Rs (n,), Rx (n,)) under the multipole rule, FP64."""
+        Rq = np.zeros((self.n, 3))
+        Rs = np.zeros(self.n)
+        Rx = np.zeros(self.n)
+        _check(lib().btam_mf_residuals_multipole(self.handle, int(rule), _d(Rq), _d(Rs), _d(Rx)),
+               "btam_mf_residuals_multipole")
+        return Rq, Rs, Rx
 
     def mf_hessian(self):
         """Mean-field Hessian blocks, (n, 3, 3): the sum over i in {u} U N(u)

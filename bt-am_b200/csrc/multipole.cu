@@ -34,6 +34,8 @@
 namespace btam {
 namespace {
 
+constexpr double kSqrt2d = 1.4142135623730951;  // sqrt(2) of the rule (Macros.hpp)
+
 // cubic_spline (cubic-spline.cpp:84-96) in the reference's operation order:
 // m = min((int)(x / dx), n - 1), p = min(x - m dx, dx).
 __device__ __forceinline__ int seg_ref(double x, double dx, int n, double &p) {
@@ -376,6 +378,555 @@ __global__ void __launch_bounds__(128) mp_v0_kernel(MpArgs a) {
   }
 }
 
+// ---- residuals under the rule ---------------------------------------------
+// evaluate_DV0_i_Dq_u_MgHx (MgHx-mf-V-bulk.cpp:1823-2098) with
+// meanfield_integral_mp_dmq / _dsq (Quadrature-Multipole.cpp:147-286) and
+// evaluate_DV0_i_Dxi_u_adp_MgHx (2102-2325), whose occupancy integrals stay
+// on the degree-3 rule (meanfield_integral_gh_3th_dxi) at the multipole
+// rho-bar.  Gradient and occupancy functions in the reference's operation
+// order (MgHx-ADP.cpp:557-601, 815-844, 904-949, 1170-1209, 1285-1371,
+// 1683-1758, 1835-1935, 2352-2434).
+
+__device__ __forceinline__ void tab_vd(const double *k, double p, double &v, double &d) {
+  v = cubv(k, p);
+  d = cubd(k, p);
+}
+
+// d rho_ij / dq_dir (dir 0: q_i, 1: q_j).
+__device__ void rho_dq(const RadialView<double> &T, int pk, int cj, double nj, int dir,
+                       const double *q, double *out) {
+  double r[3], r2 = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sqz(r[a]);
+  }
+  const double nr = sqrt(r2), inv = 1.0 / nr;
+  double p;
+  const int m = seg_ref(nr, T.dx, T.n, p);
+  const double g = nj * cubd(pr_rec(T, pk, m) + rho_off(pk, cj), p);
+  for (int a = 0; a < 3; ++a) out[a] = dir == 0 ? g * inv * r[a] : -g * inv * r[a];
+}
+__device__ void pair_dq(const RadialView<double> &T, int pk, double ni, double nj, int dir,
+                        const double *q, double *out) {
+  double r[3], r2 = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    r[a] = q[a] - q[3 + a];
+    r2 += sqz(r[a]);
+  }
+  const double nr = sqrt(r2), inv = 1.0 / nr;
+  double p;
+  const int m = seg_ref(nr, T.dx, T.n, p);
+  const double g = ni * nj * cubd(pr_rec(T, pk, m), p);
+  for (int a = 0; a < 3; ++a) out[a] = dir == 0 ? 0.5 * g * inv * r[a] : -0.5 * g * inv * r[a];
+}
+// d V_dipole / dq_dir and d V_quadrupole / dq_dir at one geometry.
+__device__ void tri_dq(const RadialView<double> &T, int pk1, int pk2, const double *n, int dir,
+                       const double *q, double *gd, double *gq) {
+  double r1[3], r2[3], r1sq = 0.0, r2sq = 0.0, dot = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    r1[a] = q[a] - q[3 + a];
+    r2[a] = q[a] - q[6 + a];
+    r1sq += sqz(r1[a]);
+    r2sq += sqz(r2[a]);
+    dot += r1[a] * r2[a];
+  }
+  const double n1 = sqrt(r1sq), n2 = sqrt(r2sq);
+  double p1, p2;
+  const int m1 = seg_ref(n1, T.dx, T.n, p1), m2 = seg_ref(n2, T.dx, T.n, p2);
+  double k1[8], k2[8];
+  ld8(uw_rec(T, pk1, m1), k1);
+  ld8(uw_rec(T, pk2, m2), k2);
+  const double i1 = 1.0 / n1, i2 = 1.0 / n2;
+  const double c1 = n[0] * n[1], c2 = n[0] * n[2];
+  const double u1 = c1 * cubv(k1, p1), u2 = c2 * cubv(k2, p2);
+  const double du1 = c1 * cubd(k1, p1), du2 = c2 * cubd(k2, p2);
+  const double w1 = c1 * cubv(k1 + 4, p1), w2 = c2 * cubv(k2 + 4, p2);
+  const double dw1 = c1 * cubd(k1 + 4, p1), dw2 = c2 * cubd(k2 + 4, p2);
+  const double dd = sqz(dot);
+  for (int a = 0; a < 3; ++a) {
+    if (dir == 0) {
+      gd[a] = 0.5 * (du1 * u2 * dot * i1 * r1[a] + u1 * du2 * dot * i2 * r2[a] +
+                     u1 * u2 * (r1[a] + r2[a]));
+      gq[a] = (1.0 / 2.0) * (dw1 * w2 * dd * i1 * r1[a] + w1 * dw2 * dd * i2 * r2[a] +
+                             w1 * w2 * 2 * dot * (r1[a] + r2[a])) -
+              (1.0 / 6.0) * (dw1 * w2 * n1 * r2sq * r1[a] + w1 * dw2 * r1sq * n2 * r2[a] +
+                             w1 * w2 * 2 * r2sq * r1[a] + w1 * w2 * 2 * r1sq * r2[a]);
+    } else if (dir == 1) {
+      gd[a] = -0.5 * (du1 * u2 * dot * i1 * r1[a] + u1 * u2 * r2[a]);
+      gq[a] = -0.5 * (dw1 * w2 * dd * i1 * r1[a] + w1 * w2 * 2 * dot * r2[a]) +
+              (1.0 / 6.0) * (dw1 * w2 * n1 * r2sq * r1[a] + w1 * w2 * 2 * r2sq * r1[a]);
+    } else {
+      gd[a] = -0.5 * (u1 * du2 * dot * i2 * r2[a] + u1 * u2 * r1[a]);
+      gq[a] = -0.5 * (w1 * dw2 * dd * i2 * r2[a] + w1 * w2 * 2 * dot * r1[a]) +
+              (1.0 / 6.0) * (w1 * dw2 * r1sq * n2 * r2[a] + w1 * w2 * 2 * r1sq * r2[a]);
+    }
+  }
+}
+// d / dn_dir of the four terms (occupancy derivatives).
+__device__ double rho_dn(const RadialView<double> &T, int pk, int cj, int dir, const double *q) {
+  if (dir != 1) return 0.0;
+  double r2 = 0.0;
+  for (int a = 0; a < 3; ++a) r2 += sqz(q[a] - q[3 + a]);
+  double p;
+  const int m = seg_ref(sqrt(r2), T.dx, T.n, p);
+  return cubv(pr_rec(T, pk, m) + rho_off(pk, cj), p);
+}
+__device__ double pair_dn(const RadialView<double> &T, int pk, const double *n, int dir,
+                          const double *q) {
+  double r2 = 0.0;
+  for (int a = 0; a < 3; ++a) r2 += sqz(q[a] - q[3 + a]);
+  double p;
+  const int m = seg_ref(sqrt(r2), T.dx, T.n, p);
+  const double phi = cubv(pr_rec(T, pk, m), p);
+  return dir == 0 ? 0.5 * (n[1] * phi) : 0.5 * (n[0] * phi);
+}
+__device__ void tri_dn(const RadialView<double> &T, int pk1, int pk2, const double *n, int dir,
+                       const double *q, double &vd, double &vq) {
+  double r1sq = 0.0, r2sq = 0.0, dot = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double r1 = q[a] - q[3 + a], r2 = q[a] - q[6 + a];
+    r1sq += sqz(r1);
+    r2sq += sqz(r2);
+    dot += r1 * r2;
+  }
+  double p1, p2;
+  const int m1 = seg_ref(sqrt(r1sq), T.dx, T.n, p1), m2 = seg_ref(sqrt(r2sq), T.dx, T.n, p2);
+  double k1[8], k2[8];
+  ld8(uw_rec(T, pk1, m1), k1);
+  ld8(uw_rec(T, pk2, m2), k2);
+  const double s1 = cubv(k1, p1), s2 = cubv(k2, p2);          // u
+  const double t1 = cubv(k1 + 4, p1), t2 = cubv(k2 + 4, p2);  // w
+  if (dir == 0) {
+    const double u1 = n[0] * n[1] * s1, u2 = n[0] * n[2] * s2;
+    const double d1 = n[1] * s1, d2 = n[2] * s2;
+    vd = (1.0 / 2.0) * d1 * u2 * dot + (1.0 / 2.0) * u1 * d2 * dot;
+    const double w1 = n[0] * n[1] * t1, w2 = n[0] * n[2] * t2;
+    const double e1 = n[1] * t1, e2 = n[2] * t2, dd = sqz(dot);
+    vq = (1.0 / 2.0) * e1 * w2 * dd + (1.0 / 2.0) * w1 * e2 * dd -
+         (1.0 / 6.0) * e1 * w2 * r1sq * r2sq - (1.0 / 6.0) * w1 * e2 * r1sq * r2sq;
+  } else if (dir == 1) {
+    vd = (1.0 / 2.0) * (n[0] * s1) * (n[0] * n[2] * s2) * dot;
+    const double e1 = n[0] * t1, w2 = n[0] * n[2] * t2;
+    vq = (1.0 / 2.0) * e1 * w2 * sqz(dot) - (1.0 / 6.0) * e1 * w2 * r1sq * r2sq;
+  } else {
+    vd = (1.0 / 2.0) * (n[0] * n[1] * s1) * (n[0] * s2) * dot;
+    const double w1 = n[0] * n[1] * t1, e2 = n[0] * t2;
+    vq = (1.0 / 2.0) * w1 * e2 * sqz(dot) - (1.0 / 6.0) * w1 * e2 * r1sq * r2sq;
+  }
+}
+
+// Degree-3 rule points of a measure (Quadrature-Measure.cpp:30-109,
+// Quadrature-Hermitian-3th.cpp:36-110): slots grouped (a coincident j1 = j2
+// is one group), one row per axis of each group, 2D points
+// mean +/- sqrt(2) sigma_s zeta [slot s in row l's group, axis of row l],
+// zeta = sqrt(D) / sqrt(2), weight 1 / (2D).
+struct Gh3 {
+  int ns, D, grp[3];
+};
+__device__ __forceinline__ Gh3 gh3_of(int ns, bool coincident) {
+  Gh3 m;
+  m.ns = ns;
+  m.grp[0] = 0;
+  m.grp[1] = 1;
+  m.grp[2] = coincident ? 1 : 2;
+  m.D = 3 * (ns == 2 ? 2 : (coincident ? 2 : 3));
+  return m;
+}
+template <int N>
+__device__ __forceinline__ void gh3_point(const Gh3 &m, const double (&mean)[N], const double *sig,
+                                          int l, double sgn, double (&ql)[N]) {
+  const double zeta = sqrt((double)m.D) / kSqrt2d;
+  for (int s = 0; s < m.ns; ++s)
+    for (int a = 0; a < 3; ++a) {
+      const double b = (m.grp[s] == l / 3 && a == l % 3) ? 1.0 : 0.0;
+      const double off = kSqrt2d * sig[s] * zeta * b;
+      ql[s * 3 + a] = sgn > 0 ? mean[s * 3 + a] + off : mean[s * 3 + a] - off;
+    }
+}
+
+// Five-point second difference with step 0.01 (meanfield_integral_mp_dmq).
+__device__ __forceinline__ double d2_dmq(double gpp, double gp, double g0, double gm,
+                                         double gmm) {
+  const double dr = 0.01;
+  return (-gpp + 16.0 * gp - 30.0 * g0 + 16.0 * gm - gmm) / (12.0 * dr * dr);
+}
+template <int N>
+__device__ __forceinline__ void moved(const double (&q)[N], int k, int which, double (&o)[N]) {
+  const double dr = 0.01;
+#pragma unroll
+  for (int c = 0; c < N; ++c) o[c] = q[c];
+  o[k] = which == 0 ? q[k] + dr * 2 : which == 1 ? q[k] + dr : which == 2 ? q[k] - dr
+                                                                            : q[k] - dr * 2;
+}
+
+// One pair measure (c = slot 0, nb = slot 1) for u in slot `dir`: the
+// multipole dmq and dsq of rho and of the pair term, and the degree-3 dxi.
+struct PairOut {
+  double drho_q[3], pair_q[3], drho_s, pair_s, drho_x, pair_x;
+};
+__device__ void pair_residual(const RadialView<double> &T, int rule, const PairSite &c,
+                              const PairSite &nb, int dir, PairOut &o) {
+  const int pk = pair_kind(c.code, nb.code);
+  const double q[6] = {c.q[0], c.q[1], c.q[2], nb.q[0], nb.q[1], nb.q[2]};
+  const double sig[2] = {c.sig, nb.sig}, n[2] = {c.x, nb.x};
+  // dmq: gradient at the mean plus sigma_s^2 / 2 x second differences
+  double g0r[3], g0p[3];
+  rho_dq(T, pk, nb.code, nb.x, dir, q, g0r);
+  pair_dq(T, pk, c.x, nb.x, dir, q, g0p);
+  for (int a = 0; a < 3; ++a) {
+    o.drho_q[a] = g0r[a];
+    o.pair_q[a] = g0p[a];
+  }
+  for (int s = 0; s < 2; ++s) {
+    const double c2 = sqz(sig[s]) / 2.0;
+    for (int al = 0; al < 3; ++al) {
+      double gr[4][3], gp[4][3];
+      for (int w = 0; w < 4; ++w) {
+        double qq[6];
+        moved(q, 3 * s + al, w, qq);
+        rho_dq(T, pk, nb.code, nb.x, dir, qq, gr[w]);
+        pair_dq(T, pk, c.x, nb.x, dir, qq, gp[w]);
+      }
+      for (int b = 0; b < 3; ++b) {
+        o.drho_q[b] += c2 * d2_dmq(gr[0][b], gr[1][b], g0r[b], gr[2][b], gr[3][b]);
+        o.pair_q[b] += c2 * d2_dmq(gp[0][b], gp[1][b], g0p[b], gp[2][b], gp[3][b]);
+      }
+    }
+  }
+  // dsq: sigma_dir x tr of block (dir, dir)
+  o.drho_s = 0.0;
+  o.pair_s = 0.0;
+  if (rule == 1) {
+    const double f0r = rho_F(T, pk, nb.code, nb.x, q), f0p = pair_F(T, pk, c.x, nb.x, q);
+    for (int al = 0; al < 3; ++al) {
+      double fr[4], fp[4];
+      for (int w = 0; w < 4; ++w) {
+        double qq[6];
+        shifted(q, 3 * dir + al, w, qq);
+        fr[w] = rho_F(T, pk, nb.code, nb.x, qq);
+        fp[w] = pair_F(T, pk, c.x, nb.x, qq);
+      }
+      o.drho_s += sig[dir] * d2_5(fr[0], fr[1], f0r, fr[2], fr[3]);
+      o.pair_s += sig[dir] * d2_5(fp[0], fp[1], f0p, fp[2], fp[3]);
+    }
+  } else {
+    double r2 = 0.0;
+    for (int a = 0; a < 3; ++a) r2 += sqz(q[a] - q[3 + a]);
+    const double s = sqrt(r2);
+    double p;
+    const int m = seg_ref(s, T.dx, T.n, p);
+    const double *kr = pr_rec(T, pk, m) + rho_off(pk, nb.code), *kp = pr_rec(T, pk, m);
+    o.drho_s = sig[dir] * (nb.x * (cubdd(kr, p) + 2.0 * cubd(kr, p) / s));
+    o.pair_s = sig[dir] * (0.5 * c.x * nb.x * (cubdd(kp, p) + 2.0 * cubd(kp, p) / s));
+  }
+  // dxi on the degree-3 rule
+  const Gh3 g = gh3_of(2, false);
+  const double W = 1.0 / (2.0 * g.D);
+  o.drho_x = 0.0;
+  o.pair_x = 0.0;
+  for (int sg = 0; sg < 2; ++sg)
+    for (int l = 0; l < g.D; ++l) {
+      double ql[6];
+      gh3_point(g, q, sig, l, sg == 0 ? 1.0 : -1.0, ql);
+      o.drho_x += rho_dn(T, pk, nb.code, dir, ql) * W;
+      o.pair_x += pair_dn(T, pk, n, dir, ql) * W;
+    }
+}
+
+// One triplet measure (c; j1, j2) for u in slot `dir` (1 or 2 may both
+// hold u when j1 = j2): dmq, dsq of the dipole and quadrupole terms
+// (with_q: j2 passes the gradient's x > min_occupancy test) and their
+// degree-3 dxi (with_x: j2 passes x >= min_occupancy).
+struct TriOut {
+  double dip_q[3], quad_q[3], dip_s, quad_s, dip_x, quad_x;
+};
+__device__ void tri_residual(const RadialView<double> &T, int rule, const PairSite &c,
+                             const PairSite &j1, const PairSite &j2, bool coincident, int dir,
+                             bool with_q, bool with_x, TriOut &o) {
+  const int pk1 = pair_kind(c.code, j1.code), pk2 = pair_kind(c.code, j2.code);
+  const double n[3] = {c.x, j1.x, j2.x};
+  const double q[9] = {c.q[0],  c.q[1],  c.q[2],  j1.q[0], j1.q[1],
+                       j1.q[2], j2.q[0], j2.q[1], j2.q[2]};
+  const double sig[3] = {c.sig, j1.sig, j2.sig};
+  for (int a = 0; a < 3; ++a) o.dip_q[a] = o.quad_q[a] = 0.0;
+  o.dip_s = o.quad_s = o.dip_x = o.quad_x = 0.0;
+  if (with_q) {
+    double g0d[3], g0q[3];
+    tri_dq(T, pk1, pk2, n, dir, q, g0d, g0q);
+    for (int a = 0; a < 3; ++a) {
+      o.dip_q[a] = g0d[a];
+      o.quad_q[a] = g0q[a];
+    }
+    for (int s = 0; s < 3; ++s) {
+      const double c2 = sqz(sig[s]) / 2.0;
+      for (int al = 0; al < 3; ++al) {
+        double gd[4][3], gq[4][3];
+        for (int w = 0; w < 4; ++w) {
+          double qq[9];
+          moved(q, 3 * s + al, w, qq);
+          tri_dq(T, pk1, pk2, n, dir, qq, gd[w], gq[w]);
+        }
+        for (int b = 0; b < 3; ++b) {
+          o.dip_q[b] += c2 * d2_dmq(gd[0][b], gd[1][b], g0d[b], gd[2][b], gd[3][b]);
+          o.quad_q[b] += c2 * d2_dmq(gq[0][b], gq[1][b], g0q[b], gq[2][b], gq[3][b]);
+        }
+      }
+    }
+    // dsq: sigma_dir x sum over the dof row of dir of the block traces
+    if (rule == 1) {
+      double f0d, f0q;
+      tri_F(T, pk1, pk2, n, q, f0d, f0q);
+      for (int b = 0; b < 3; ++b) {
+        if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
+        const int dirn = dir * 3 + b, slot = dirn / 4;
+        const bool diag = dirn == 0 || dirn == 4 || dirn == 8;
+        for (int al = 0; al < 3; ++al) {
+          double sd[4], sq4[4];
+          for (int w = 0; w < 4; ++w) {
+            double qq[9];
+            shifted(q, 3 * slot + al, w, qq);
+            tri_F(T, pk1, pk2, n, qq, sd[w], sq4[w]);
+          }
+          o.dip_s += sig[dir] * d2_5(sd[0], sd[1], f0d, sd[2], sd[3]);
+          if (diag) o.quad_s += sig[dir] * d2_5(sq4[0], sq4[1], f0q, sq4[2], sq4[3]);
+        }
+      }
+    } else {
+      const TriTr t = tri_traces(T, pk1, pk2, n, q);
+      for (int b = 0; b < 3; ++b) {
+        if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
+        double trd, trq;
+        if (b != dir) {
+          trd = t.d12;
+          trq = t.q12;
+        } else if (dir == 0) {
+          trd = t.d11 + t.d22 + 2.0 * t.d12;
+          trq = t.q11 + t.q22 + 2.0 * t.q12;
+        } else {
+          trd = dir == 1 ? t.d11 : t.d22;
+          trq = dir == 1 ? t.q11 : t.q22;
+        }
+        o.dip_s += sig[dir] * trd;
+        o.quad_s += sig[dir] * trq;
+      }
+    }
+  }
+  if (with_x) {
+    const Gh3 g = gh3_of(3, coincident);
+    const double W = 1.0 / (2.0 * g.D);
+    for (int sg = 0; sg < 2; ++sg)
+      for (int l = 0; l < g.D; ++l) {
+        double ql[9], vd, vq;
+        gh3_point(g, q, sig, l, sg == 0 ? 1.0 : -1.0, ql);
+        tri_dn(T, pk1, pk2, n, dir, ql, vd, vq);
+        o.dip_x += vd * W;
+        o.quad_x += vq * W;
+      }
+  }
+}
+
+struct MpResArgs {
+  MpArgs b;
+  const int *owner;
+  const double *gamma;
+  double *g5;  // 5 values (dV0/dq 3, dV0/dsigma, dV0/dx) per (u, centre)
+  double *Rq, *Rs, *Rx;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+// One warp per (u, centre i in {u} U N(u)): evaluate_DV0_i_Dq_u_MgHx and
+// evaluate_DV0_i_Dxi_u_adp_MgHx for i = the centre's owner o and u as seen
+// from o's frame, each term of the reference's loops over o's list that
+// holds u.
+__global__ void __launch_bounds__(128) mp_pairs_kernel(MpResArgs r, long long total) {
+  const MpArgs &a = r.b;
+  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= total) return;
+  // u: the last real site with offs[u] + u <= w
+  int lo = 0, hi = a.n_real - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if ((long long)a.offs[mid] + mid <= w) lo = mid;
+    else hi = mid - 1;
+  }
+  const int u = lo, c = (int)(w - ((long long)a.offs[u] + u));
+  double *out = r.g5 + 5 * w;
+  const int ic = c == 0 ? u : a.idx[a.offs[u] + c - 1];
+  const int o = r.owner[ic];
+  // u in o's frame: itself for the centre u; else the entry of o's list
+  // that is u translated as ic is
+  int uu = u, ks = -1;
+  if (c != 0) {
+    const double4 pu = a.pos[u], pc = a.pos[ic], po = a.pos[o];
+    const double d[3] = {pu.x - pc.x, pu.y - pc.y, pu.z - pc.z};
+    uu = -1;
+    for (int k = a.offs[o] + lane; k < a.offs[o + 1]; k += 32) {
+      const int j = a.idx[k];
+      if (r.owner[j] != u) continue;
+      const double4 pj = a.pos[j];
+      if (fabs(pj.x - po.x - d[0]) < 1e-8 && fabs(pj.y - po.y - d[1]) < 1e-8 &&
+          fabs(pj.z - po.z - d[2]) < 1e-8)
+        ks = k;
+    }
+    for (int off = 16; off > 0; off >>= 1) ks = max(ks, __shfl_xor_sync(0xffffffffu, ks, off));
+    if (ks >= 0) uu = a.idx[ks];
+  }
+  const PairSite so = site_of(a, o);
+  double acc[12];  // dV0/dq parts: drho 0-2, pair 3-5, dipole 6-8, quadrupole 9-11
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
+  double sq4[4] = {0, 0, 0, 0};  // drho_s, pair_s, dip_s, quad_s
+  double sx[4] = {0, 0, 0, 0};   // drho_x, pair_x, dip_x, quad_x
+  const bool live = uu >= 0 && !(a.xb[uu].x < kMinOcc) && !(so.x < kMinOcc);
+  if (live) {
+    const int nb0 = a.offs[o], nn = a.offs[o + 1] - nb0;
+    auto add_pair = [&](const PairOut &po_) {
+      for (int b = 0; b < 3; ++b) {
+        acc[b] += po_.drho_q[b];
+        acc[3 + b] += po_.pair_q[b];
+      }
+      sq4[0] += po_.drho_s;
+      sq4[1] += po_.pair_s;
+      sx[0] += po_.drho_x;
+      sx[1] += po_.pair_x;
+    };
+    auto add_tri = [&](const TriOut &t, double f) {
+      for (int b = 0; b < 3; ++b) {
+        acc[6 + b] += f * t.dip_q[b];
+        acc[9 + b] += f * t.quad_q[b];
+      }
+      sq4[2] += f * t.dip_s;
+      sq4[3] += f * t.quad_s;
+      sx[2] += f * t.dip_x;
+      sx[3] += f * t.quad_x;
+    };
+    if (c == 0) {
+      // i = u: every pair and triplet of u's list, u in slot 0
+      for (int k = lane; k < nn; k += 32) {
+        const PairSite sj = site_of(a, a.idx[nb0 + k]);
+        if (sj.x < kMinOcc) continue;
+        PairOut po_;
+        pair_residual(a.T, a.rule, so, sj, 0, po_);
+        add_pair(po_);
+      }
+      const long long ntri = (long long)nn * (nn + 1) / 2;
+      for (long long t = lane; t < ntri; t += 32) {
+        int k2 = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)k2 * (k2 + 1) / 2 > t) --k2;
+        while ((long long)(k2 + 1) * (k2 + 2) / 2 <= t) ++k2;
+        const int k1 = (int)(t - (long long)k2 * (k2 + 1) / 2);
+        const PairSite s1 = site_of(a, a.idx[nb0 + k1]);
+        if (s1.x < kMinOcc) continue;
+        const PairSite s2 = site_of(a, a.idx[nb0 + k2]);
+        const bool wq = !(s2.x <= kMinOcc), wx = !(s2.x < kMinOcc);
+        if (!wq && !wx) continue;
+        TriOut to;
+        tri_residual(a.T, a.rule, so, s1, s2, k1 == k2, 0, wq, wx, to);
+        add_tri(to, k1 == k2 ? 1.0 : 2.0);
+      }
+    } else {
+      // i = o: the pair (o, u) and the triplets of o's list that hold u
+      const PairSite su = site_of(a, uu);
+      if (lane == 0) {
+        PairOut po_;
+        pair_residual(a.T, a.rule, so, su, 1, po_);
+        add_pair(po_);
+      }
+      const int kk = ks - nb0;
+      for (int k = lane; k < nn; k += 32) {
+        const PairSite sk = site_of(a, a.idx[nb0 + k]);
+        if (k >= kk) {
+          // (j1, j2) = (u, k): u in slot 1, and in slot 2 as well for k = u
+          const bool wq = !(sk.x <= kMinOcc), wx = !(sk.x < kMinOcc);
+          if (!wq && !wx) continue;
+          const double f = k == kk ? 1.0 : 2.0;
+          for (int dir = 1; dir <= (k == kk ? 2 : 1); ++dir) {
+            TriOut to;
+            tri_residual(a.T, a.rule, so, su, sk, k == kk, dir, wq, wx, to);
+            add_tri(to, f);
+          }
+        } else {
+          // (j1, j2) = (k, u): u in slot 2
+          if (sk.x < kMinOcc) continue;
+          const bool wq = !(su.x <= kMinOcc), wx = !(su.x < kMinOcc);
+          if (!wq && !wx) continue;
+          TriOut to;
+          tri_residual(a.T, a.rule, so, sk, su, false, 2, wq, wx, to);
+          add_tri(to, 2.0);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 12; ++k) acc[k] = warp_sum(acc[k]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    sq4[k] = warp_sum(sq4[k]);
+    sx[k] = warp_sum(sx[k]);
+  }
+  if (lane == 0) {
+    double g[5] = {0, 0, 0, 0, 0};
+    if (live) {
+      double p;
+      const SplineView<double> &E = so.code == 0 ? a.emb_mg : a.emb_h;
+      const int m = seg_ref(a.rho[o], E.dx, E.n, p);
+      const Coef4<double> cf = E.c[m];
+      const double kk4[4] = {cf.a, cf.b, cf.c, cf.d};
+      const double dF = cubd(kk4, p);
+      for (int b = 0; b < 3; ++b) g[b] = so.x * dF * acc[b] + acc[3 + b] + acc[6 + b] + acc[9 + b];
+      g[3] = so.x * dF * sq4[0] + sq4[1] + sq4[2] + sq4[3];
+      // evaluate_DV0_i_Dxi_u_adp_MgHx's embedding part (2300-2315)
+      double emb = 0.0;
+      if (so.code == 1 && o == uu) emb = cubv(kk4, p);
+      if (so.code == 1 && o != uu) emb = so.x * dF * sx[0];
+      if (so.code == 0) emb = dF * sx[0];
+      g[4] = emb + sx[1] + sx[2] + sx[3];
+    }
+    for (int k = 0; k < 5; ++k) out[k] = g[k];
+  }
+}
+
+// Residual assembly per real site (the project's definition, include/btam.h):
+// R = sum over the centres of beta_o / beta_u times the per-pair values,
+// then the entropy and chemical-potential parts.
+__global__ void mp_assemble_kernel(MpResArgs r) {
+  const MpArgs &a = r.b;
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= a.n_real) return;
+  double rq[3] = {0, 0, 0}, rs = 0.0, rx = 0.0;
+  const double2 xbu = a.xb[u];
+  const double xu = xbu.x, bu = xbu.y;
+  if (!(xu < kMinOcc)) {
+    const long long base = (long long)a.offs[u] + u;
+    const int ncen = 1 + a.offs[u + 1] - a.offs[u];
+    for (int c = 0; c < ncen; ++c) {
+      const int ic = c == 0 ? u : a.idx[a.offs[u] + c - 1];
+      const int o = r.owner[ic];
+      const double wgt = a.xb[o].y / bu;
+      const double *g = r.g5 + 5 * (base + c);
+      for (int b = 0; b < 3; ++b) rq[b] += wgt * g[b];
+      rs += wgt * g[3];
+      rx += wgt * g[4];
+    }
+    rs -= 3.0 / (bu * a.pos[u].w);
+    if (a.code[u] == 1) {
+      const double dlogz = 3.0 / (2.0 * xu) + (xu < 1.0 ? 1.0 / (1.0 - xu) : 0.0);
+      rx -= dlogz / bu;
+      if (xu < 0.9999) rx -= r.gamma[u] / bu;
+    } else {
+      rx = 0.0;
+    }
+  }
+  for (int b = 0; b < 3; ++b) r.Rq[3 * (size_t)u + b] = rq[b];
+  r.Rs[u] = rs;
+  r.Rx[u] = rx;
+}
+
 }  // namespace
 }  // namespace btam
 
@@ -428,6 +979,67 @@ int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, do
   for (size_t k = 0; k < n; ++k) E += hv[k];
   if (V0) std::copy(hv.begin(), hv.end(), V0);
   if (energy) *energy = E;
+  return read_err(s);
+}
+
+int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs, double *Rx) {
+  if (!s || !Rq || !Rs || !Rx || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC))
+    return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  const size_t n = (size_t)s->n_real;
+  if (n == 0) return BTAM_OK;
+  std::vector<int> offs_n(1);
+  cudaError_t e = cudaMemcpyAsync(offs_n.data(), s->offs + n, sizeof(int),
+                                  cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  const long long total = (long long)offs_n[0] + (long long)n;
+  double *rd = nullptr, *g5 = nullptr, *out = nullptr;
+  BTAM_TRY(dalloc(rd, s->st, n));
+  int st = dalloc(g5, s->st, 5 * (size_t)total);
+  if (st == BTAM_OK) st = dalloc(out, s->st, 5 * n);
+  if (st != BTAM_OK) {
+    dfree(rd, s->st);
+    dfree(g5, s->st);
+    return st;
+  }
+  MpResArgs r;
+  MpArgs &a = r.b;
+  a.n_real = s->n_real;
+  a.rule = rule;
+  a.pos = s->pos;
+  a.xb = s->xb;
+  a.code = s->code;
+  a.offs = s->offs;
+  a.idx = s->idx;
+  a.T = s->T->r64;
+  a.emb_mg = s->T->v64.t[T_F_MG];
+  a.emb_h = s->T->v64.t[T_F_H];
+  a.rho = rd;
+  a.out = rd;
+  r.owner = s->owner;
+  r.gamma = s->gamma;
+  r.g5 = g5;
+  r.Rq = out;
+  r.Rs = out + 3 * n;
+  r.Rx = out + 4 * n;
+  const int g = (int)(((long long)n * 32 + 127) / 128);
+  mp_rho_kernel<<<g, 128, 0, s->st>>>(a);
+  const long long gp = (total * 32 + 127) / 128;
+  mp_pairs_kernel<<<(unsigned)gp, 128, 0, s->st>>>(r, total);
+  mp_assemble_kernel<<<(int)((n + 127) / 128), 128, 0, s->st>>>(r);
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(Rq, out, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(Rs, out + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(Rx, out + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  dfree(rd, s->st);
+  dfree(g5, s->st);
+  dfree(out, s->st);
+  if (e != cudaSuccess) return cuda_status(e);
   return read_err(s);
 }
 

@@ -226,6 +226,17 @@ int btam_mf_hessian(btam_system *s, double *H);
 #define BTAM_MP_ANALYTIC 2
 int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0,
                            double *energy);
+/* The residuals of every real site under the same rule: Rq (3 n_real), Rs
+ * and Rx (n_real each), assembled as btam_mf_eval's.  The per-pair parts
+ * replace evaluate_DV0_i_Dq_u_MgHx (1823-2098) built with the rule
+ * (meanfield_integral_mp_dmq: the gradient plus sigma_s^2 / 2 times its
+ * five-point second difference, step 0.01, in every coordinate of every
+ * slot; meanfield_integral_mp_dsq: sigma times the Hessian traces) and
+ * evaluate_DV0_i_Dxi_u_adp_MgHx (2102-2325), whose occupancy integrals the
+ * reference keeps on the degree-3 rule, at the multipole rho-bar.  FP64,
+ * a direct evaluation: one warp per (site, centre) pair. */
+int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs,
+                                double *Rx);
 
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
