@@ -165,16 +165,21 @@ def active_pairs(sys_, offs, idx, owner):
     return int(np.sum(act_i & (xa[idx] >= 5e-4)))
 
 
-def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1):
+def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1, multipole=False):
     """Times the reference's own arithmetic (oracle/_ref, -Ofast build, on
     `threads` host threads) on a bounded sample of one evaluation (divided
-    by `scale`) and extrapolates.  Returns (evals_per_s, description)."""
+    by `scale`) and extrapolates.  With `multipole`, the -O2 build with
+    MULTIPOLE_INTEGRAL and the reference's own -DNUMERICAL_DERIVATIVES=0
+    (the oracle's rule 1 when that build is absent).  Returns
+    (evals_per_s, description, kind, seconds per evaluation)."""
     import pyoracle
-    ref = pyoracle.reference(fast=True)
+    ref = pyoracle.reference_multipole() if multipole else pyoracle.reference(fast=True)
     kind = "reference"
     orc = pyoracle.Oracle()
     if ref is None:
         ref, kind = orc, "port"
+        if multipole:
+            orc.set_rule(1)
     os.environ["BTAM_REF_THREADS"] = str(threads)
     os.environ["BTAM_ORACLE_THREADS"] = str(threads)
     rng = np.random.default_rng(seed)
@@ -498,6 +503,44 @@ def bench_config1(args, tables):
     return out
 
 
+def bench_multipole(args, tables):
+    """The reference's other mean-field rule (MULTIPOLE_INTEGRAL) on the
+    plain drop-in workload: rho-bar + V0 and the residuals, FP64, under the
+    finite-difference Hessians of the reference's build flags (rule 1) and
+    the analytic ones (rule 2); host clock around each call (allocation and
+    the result copies included).  Beside it, the reference built with the
+    rule, timed on a bounded sample on all host threads."""
+    import torch
+    import btam
+    from btam import lattice
+
+    sys_ = lattice.config2()
+    S = btam.System(tables, sys_)
+    S.build_neighbors()
+    out = {"workload": WORKLOAD + ", multipole rule", "sites": len(sys_["x"])}
+    for rule, name in ((btam.MP_FD, "rule_fd_hessians"), (btam.MP_ANALYTIC, "rule_analytic")):
+        S.mf_eval_multipole(rule)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        _, _, E = S.mf_eval_multipole(rule)
+        t1 = time.perf_counter()
+        S.mf_residuals_multipole(rule)
+        t2 = time.perf_counter()
+        out[name] = {"energy": E, "rho_V0_ms": (t1 - t0) * 1e3, "residuals_ms": (t2 - t1) * 1e3,
+                     "evaluation_ms": (t2 - t0) * 1e3}
+    S.close()
+    if not args.no_cpu and int(os.environ.get("RANK", "0")) == 0:
+        threads = os.cpu_count() or 1
+        _, desc, kind, t_full = cpu_reference_sample(sys_, threads, seed=2, scale=4,
+                                                     multipole=True)
+        out["cpu_reference"] = {"s_per_evaluation": t_full, "threads": threads, "kind": kind,
+                                "build": "-O2 -DMULTIPOLE_INTEGRAL -DNUMERICAL_DERIVATIVES=0",
+                                "sample": desc}
+        out["gpu_over_cpu_rule_fd"] = t_full / (out["rule_fd_hessians"]["evaluation_ms"] * 1e-3)
+    out["timing"] = "host clock around each call"
+    return out
+
+
 def bench_serving(args, tables):
     """The served workload: a seeded Poisson stream (mean 200 jobs/s) of 64
     jobs, half relaxations (L-BFGS to |R| <= 1e-5 or 100 iterations) and half
@@ -711,6 +754,7 @@ def run_btam(args, ws, rank, local):
     nanowire = None if args.no_wire else bench_nanowire(args, tables)
     stretch = None if args.no_stretch else bench_bulk_stretch(args, tables)
     config1 = None if args.no_stretch else bench_config1(args, tables)
+    multipole = None if args.no_multipole else bench_multipole(args, tables)
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
@@ -747,7 +791,7 @@ def run_btam(args, ws, rank, local):
                 "gpu_launches": launches_per_eval(shapes["fp32c"]) * args.steps,
                 "clocks": clocks, "batched": batched, "serving": serving,
                 "precision_nanowire": nanowire, "bulk_stretch": stretch,
-                "config1_workflow": config1}
+                "config1_workflow": config1, "multipole": multipole}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
@@ -767,6 +811,8 @@ def main():
     ap.add_argument("--no-wire", action="store_true", help="skip the nanowire DMD workload")
     ap.add_argument("--no-stretch", action="store_true",
                     help="skip the bulk stretch relaxation and config-1 workflow workloads")
+    ap.add_argument("--no-multipole", action="store_true",
+                    help="skip the multipole-rule workload")
     ap.add_argument("--dmd-steps", type=int, default=1000,
                     help="master-equation steps of the nanowire workload")
     args = ap.parse_args()
