@@ -189,7 +189,7 @@ __device__ double pair_mp(const RadialView<double> &T, int rule, int term, const
 struct TriTr {
   double d11, d22, d12, q11, q22, q12;
 };
-__device__ TriTr tri_traces(const RadialView<double> &T, int pk1, int pk2, const double *n,
+__device__ __forceinline__ TriTr tri_traces(const RadialView<double> &T, int pk1, int pk2, const double *n,
                             const double *q) {
   double r1sq = 0.0, r2sq = 0.0, d = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -379,6 +379,27 @@ __global__ void __launch_bounds__(128) mp_v0_kernel(MpArgs a) {
 }
 
 // ---- residuals under the rule ---------------------------------------------
+// The residual kernel calls its geometry functions out of line: inlined
+// into every step of the unrolled second differences they overflow the
+// instruction cache (the kernel stalled on instruction fetch).  The
+// energy kernels keep them inline.  Rounding is the same either way.
+__device__ __noinline__ double rho_F_call(const RadialView<double> &T, int pk, int cj, double nj,
+                                          const double *q) {
+  return rho_F(T, pk, cj, nj, q);
+}
+__device__ __noinline__ double pair_F_call(const RadialView<double> &T, int pk, double ni,
+                                           double nj, const double *q) {
+  return pair_F(T, pk, ni, nj, q);
+}
+__device__ __noinline__ void tri_F_call(const RadialView<double> &T, int pk1, int pk2,
+                                        const double *n, const double *q, double &fd,
+                                        double &fq) {
+  tri_F(T, pk1, pk2, n, q, fd, fq);
+}
+__device__ __noinline__ TriTr tri_traces_call(const RadialView<double> &T, int pk1, int pk2,
+                                              const double *n, const double *q) {
+  return tri_traces(T, pk1, pk2, n, q);
+}
 // evaluate_DV0_i_Dq_u_MgHx (MgHx-mf-V-bulk.cpp:1823-2098) with
 // meanfield_integral_mp_dmq / _dsq (Quadrature-Multipole.cpp:147-286) and
 // evaluate_DV0_i_Dxi_u_adp_MgHx (2102-2325), whose occupancy integrals stay
@@ -387,13 +408,8 @@ __global__ void __launch_bounds__(128) mp_v0_kernel(MpArgs a) {
 // order (MgHx-ADP.cpp:557-601, 815-844, 904-949, 1170-1209, 1285-1371,
 // 1683-1758, 1835-1935, 2352-2434).
 
-__device__ __forceinline__ void tab_vd(const double *k, double p, double &v, double &d) {
-  v = cubv(k, p);
-  d = cubd(k, p);
-}
-
 // d rho_ij / dq_dir (dir 0: q_i, 1: q_j).
-__device__ void rho_dq(const RadialView<double> &T, int pk, int cj, double nj, int dir,
+__device__ __noinline__ void rho_dq(const RadialView<double> &T, int pk, int cj, double nj, int dir,
                        const double *q, double *out) {
   double r[3], r2 = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -406,7 +422,7 @@ __device__ void rho_dq(const RadialView<double> &T, int pk, int cj, double nj, i
   const double g = nj * cubd(pr_rec(T, pk, m) + rho_off(pk, cj), p);
   for (int a = 0; a < 3; ++a) out[a] = dir == 0 ? g * inv * r[a] : -g * inv * r[a];
 }
-__device__ void pair_dq(const RadialView<double> &T, int pk, double ni, double nj, int dir,
+__device__ __noinline__ void pair_dq(const RadialView<double> &T, int pk, double ni, double nj, int dir,
                         const double *q, double *out) {
   double r[3], r2 = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -420,7 +436,7 @@ __device__ void pair_dq(const RadialView<double> &T, int pk, double ni, double n
   for (int a = 0; a < 3; ++a) out[a] = dir == 0 ? 0.5 * g * inv * r[a] : -0.5 * g * inv * r[a];
 }
 // d V_dipole / dq_dir and d V_quadrupole / dq_dir at one geometry.
-__device__ void tri_dq(const RadialView<double> &T, int pk1, int pk2, const double *n, int dir,
+__device__ __noinline__ void tri_dq(const RadialView<double> &T, int pk1, int pk2, const double *n, int dir,
                        const double *q, double *gd, double *gq) {
   double r1[3], r2[3], r1sq = 0.0, r2sq = 0.0, dot = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -463,7 +479,7 @@ __device__ void tri_dq(const RadialView<double> &T, int pk1, int pk2, const doub
   }
 }
 // d / dn_dir of the four terms (occupancy derivatives).
-__device__ double rho_dn(const RadialView<double> &T, int pk, int cj, int dir, const double *q) {
+__device__ __noinline__ double rho_dn(const RadialView<double> &T, int pk, int cj, int dir, const double *q) {
   if (dir != 1) return 0.0;
   double r2 = 0.0;
   for (int a = 0; a < 3; ++a) r2 += sqz(q[a] - q[3 + a]);
@@ -471,7 +487,7 @@ __device__ double rho_dn(const RadialView<double> &T, int pk, int cj, int dir, c
   const int m = seg_ref(sqrt(r2), T.dx, T.n, p);
   return cubv(pr_rec(T, pk, m) + rho_off(pk, cj), p);
 }
-__device__ double pair_dn(const RadialView<double> &T, int pk, const double *n, int dir,
+__device__ __noinline__ double pair_dn(const RadialView<double> &T, int pk, const double *n, int dir,
                           const double *q) {
   double r2 = 0.0;
   for (int a = 0; a < 3; ++a) r2 += sqz(q[a] - q[3 + a]);
@@ -480,7 +496,7 @@ __device__ double pair_dn(const RadialView<double> &T, int pk, const double *n, 
   const double phi = cubv(pr_rec(T, pk, m), p);
   return dir == 0 ? 0.5 * (n[1] * phi) : 0.5 * (n[0] * phi);
 }
-__device__ void tri_dn(const RadialView<double> &T, int pk1, int pk2, const double *n, int dir,
+__device__ __noinline__ void tri_dn(const RadialView<double> &T, int pk1, int pk2, const double *n, int dir,
                        const double *q, double &vd, double &vq) {
   double r1sq = 0.0, r2sq = 0.0, dot = 0.0;
   for (int a = 0; a < 3; ++a) {
@@ -597,14 +613,14 @@ __device__ void pair_residual(const RadialView<double> &T, int rule, const PairS
   o.drho_s = 0.0;
   o.pair_s = 0.0;
   if (rule == 1) {
-    const double f0r = rho_F(T, pk, nb.code, nb.x, q), f0p = pair_F(T, pk, c.x, nb.x, q);
+    const double f0r = rho_F_call(T, pk, nb.code, nb.x, q), f0p = pair_F_call(T, pk, c.x, nb.x, q);
     for (int al = 0; al < 3; ++al) {
       double fr[4], fp[4];
       for (int w = 0; w < 4; ++w) {
         double qq[6];
         shifted(q, 3 * dir + al, w, qq);
-        fr[w] = rho_F(T, pk, nb.code, nb.x, qq);
-        fp[w] = pair_F(T, pk, c.x, nb.x, qq);
+        fr[w] = rho_F_call(T, pk, nb.code, nb.x, qq);
+        fp[w] = pair_F_call(T, pk, c.x, nb.x, qq);
       }
       o.drho_s += sig[dir] * d2_5(fr[0], fr[1], f0r, fr[2], fr[3]);
       o.pair_s += sig[dir] * d2_5(fp[0], fp[1], f0p, fp[2], fp[3]);
@@ -675,7 +691,7 @@ __device__ void tri_residual(const RadialView<double> &T, int rule, const PairSi
     // dsq: sigma_dir x sum over the dof row of dir of the block traces
     if (rule == 1) {
       double f0d, f0q;
-      tri_F(T, pk1, pk2, n, q, f0d, f0q);
+      tri_F_call(T, pk1, pk2, n, q, f0d, f0q);
       for (int b = 0; b < 3; ++b) {
         if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
         const int dirn = dir * 3 + b, slot = dirn / 4;
@@ -685,14 +701,14 @@ __device__ void tri_residual(const RadialView<double> &T, int rule, const PairSi
           for (int w = 0; w < 4; ++w) {
             double qq[9];
             shifted(q, 3 * slot + al, w, qq);
-            tri_F(T, pk1, pk2, n, qq, sd[w], sq4[w]);
+            tri_F_call(T, pk1, pk2, n, qq, sd[w], sq4[w]);
           }
           o.dip_s += sig[dir] * d2_5(sd[0], sd[1], f0d, sd[2], sd[3]);
           if (diag) o.quad_s += sig[dir] * d2_5(sq4[0], sq4[1], f0q, sq4[2], sq4[3]);
         }
       }
     } else {
-      const TriTr t = tri_traces(T, pk1, pk2, n, q);
+      const TriTr t = tri_traces_call(T, pk1, pk2, n, q);
       for (int b = 0; b < 3; ++b) {
         if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
         double trd, trq;
