@@ -72,7 +72,7 @@ _PROTOS = {
     "btam_stretch_apply": (ctypes.c_int, [_V, _D]),
     "btam_pt_hessian": (ctypes.c_int, [_V, _D]),
     "btam_mf_hessian": (ctypes.c_int, [_V, _D]),
-    "btam_mf_eval_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D,
+    "btam_mf_eval_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D,
                                               ctypes.POINTER(ctypes.c_double)]),
     "btam_mf_residuals_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
@@ -451,12 +451,15 @@ class System:
         """rho-bar, V0 per site and their sum under the multipole rule
         (MULTIPOLE_INTEGRAL): rule MP_FD (1) with the finite-difference
         Hessians of the reference's build flags, MP_ANALYTIC (2) with
-        analytic Hessians.  FP64."""
+        analytic Hessians.  FP64.  The per-site S0 of the same call is kept
+        in `last_S0`."""
         rho = np.zeros(self.n)
         V0 = np.zeros(self.n)
+        S0 = np.zeros(self.n)
         E = ctypes.c_double(0.0)
-        _check(lib().btam_mf_eval_multipole(self.handle, int(rule), _d(rho), _d(V0),
+        _check(lib().btam_mf_eval_multipole(self.handle, int(rule), _d(rho), _d(V0), _d(S0),
                                             ctypes.byref(E)), "btam_mf_eval_multipole")
+        self.last_S0 = S0
         return rho, V0, E.value
 
     def mf_residuals_multipole(self, rule=1):

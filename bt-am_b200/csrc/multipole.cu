@@ -32,6 +32,7 @@
 #include "internal.cuh"
 
 namespace btam {
+double tables_mass(const btam_tables *t, int code);
 namespace {
 
 constexpr double kSqrt2d = 1.4142135623730951;  // sqrt(2) of the rule (Macros.hpp)
@@ -294,6 +295,9 @@ struct MpArgs {
   SplineView<double> emb_mg, emb_h;
   const double *rho;  // multipole rho-bar of the real sites (V0 kernel)
   double *out;
+  double *S0;             // V0 kernel: the free entropy as well (may be null)
+  const double *gamma;    // per real site
+  double mass[2];         // Mg, H
 };
 
 __device__ __forceinline__ PairSite site_of(const MpArgs &a, int j) {
@@ -375,6 +379,20 @@ __global__ void __launch_bounds__(128) mp_v0_kernel(MpArgs a) {
       v = emb + pair + dip + quad;
     }
     a.out[i] = v;
+    if (a.S0) {
+      // evaluate_S0_i_adp_MgHx (957-1142) on this V0: -log Z0 + beta H0 -
+      // gamma x~, H0 = 1 / (2 beta) + V0; zero for x below min_occupancy
+      double S = 0.0;
+      if (!(si.x < kMinOcc)) {
+        const double beta = a.xb[i].y;
+        const double m = kUma * si.x * a.mass[si.code];
+        double logZ = 3.0 * log((si.sig * sqrt(m / beta)) / kHbar);
+        if (si.x < 1.0) logZ += log(1.0 / (1.0 - si.x));
+        const double gx = si.code == 1 ? a.gamma[i] * (si.x > 0.9999 ? 0.9999 : si.x) : 0.0;
+        S = -logZ + beta * (1.0 / (2.0 * beta) + v) - gx;
+      }
+      a.S0[i] = S;
+    }
   }
 }
 
@@ -950,15 +968,18 @@ using namespace btam;
 
 extern "C" {
 
-int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, double *energy) {
+int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, double *S0,
+                           double *energy) {
   if (!s || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC)) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   const size_t n = (size_t)s->n_real;
-  double *rd = nullptr, *vd = nullptr;
+  double *rd = nullptr, *vd = nullptr, *sd = nullptr;
   BTAM_TRY(dalloc(rd, s->st, n));
   int st = dalloc(vd, s->st, n);
+  if (st == BTAM_OK) st = dalloc(sd, s->st, n);
   if (st != BTAM_OK) {
     dfree(rd, s->st);
+    dfree(vd, s->st);
     return st;
   }
   MpArgs a;
@@ -973,23 +994,31 @@ int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, do
   a.emb_mg = s->T->v64.t[T_F_MG];
   a.emb_h = s->T->v64.t[T_F_H];
   a.rho = rd;
+  a.S0 = nullptr;
+  a.gamma = s->gamma;
+  a.mass[0] = tables_mass(s->T, 0);
+  a.mass[1] = tables_mass(s->T, 1);
   const int g = (int)(((long long)s->n_real * 32 + 127) / 128);
   cudaError_t e = cudaSuccess;
   if (g > 0) {
     a.out = rd;
     mp_rho_kernel<<<g, 128, 0, s->st>>>(a);
     a.out = vd;
+    a.S0 = sd;
     mp_v0_kernel<<<g, 128, 0, s->st>>>(a);
     e = cudaGetLastError();
   }
   std::vector<double> hv(n);
   if (e == cudaSuccess && rho && n)
     e = cudaMemcpyAsync(rho, rd, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess && S0 && n)
+    e = cudaMemcpyAsync(S0, sd, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
   if (e == cudaSuccess && n)
     e = cudaMemcpyAsync(hv.data(), vd, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   dfree(rd, s->st);
   dfree(vd, s->st);
+  dfree(sd, s->st);
   if (e != cudaSuccess) return cuda_status(e);
   double E = 0.0;
   for (size_t k = 0; k < n; ++k) E += hv[k];
@@ -1033,6 +1062,10 @@ int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs
   a.emb_h = s->T->v64.t[T_F_H];
   a.rho = rd;
   a.out = rd;
+  a.S0 = nullptr;
+  a.gamma = s->gamma;
+  a.mass[0] = tables_mass(s->T, 0);
+  a.mass[1] = tables_mass(s->T, 1);
   r.owner = s->owner;
   r.gamma = s->gamma;
   r.g5 = g5;

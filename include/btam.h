@@ -217,14 +217,15 @@ int btam_mf_hessian(btam_system *s, double *H);
  *                     diagonal entries only (MgHx-ADP.cpp:736-812,
  *                     1091-1167, 1605-1680, 2270-2349);
  *   BTAM_MP_ANALYTIC  NUMERICAL_DERIVATIVES undefined: analytic Hessians.
- * Replaces evaluate_mf_rho_i_adp_MgHx (708-787) and evaluate_V0_i_adp_MgHx
- * (791-953) built with that rule: rho (n_real, may be NULL) the multipole
- * rho-bar, V0 (n_real, may be NULL) the per-site V0, *energy (may be NULL)
- * their sum.  FP64, a direct evaluation of the reference's pair and
- * triplet sums on the system's neighbour lists (kept as built). */
+ * Replaces evaluate_mf_rho_i_adp_MgHx (708-787), evaluate_V0_i_adp_MgHx
+ * (791-953) and evaluate_S0_i_adp_MgHx (957-1142) built with that rule:
+ * rho (n_real, may be NULL) the multipole rho-bar, V0 and S0 (n_real each,
+ * may be NULL) per site, *energy (may be NULL) the sum of V0.  FP64, a
+ * direct evaluation of the reference's pair and triplet sums on the
+ * system's neighbour lists (kept as built). */
 #define BTAM_MP_FD 1
 #define BTAM_MP_ANALYTIC 2
-int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0,
+int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, double *S0,
                            double *energy);
 /* The residuals of every real site under the same rule: Rq (3 n_real), Rs
  * and Rx (n_real each), assembled as btam_mf_eval's.  The per-pair parts

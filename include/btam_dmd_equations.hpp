@@ -56,7 +56,14 @@
  *  - evaluate_D2V_i_Dq2_j (btam_pt_hessian) and evaluate_D2V0_i_Dmeanq2_j
  *    (btam_mf_hessian, FP64 whatever the bound precision) are lumped like
  *    the gradients: the whole sum over i in {u} U N(u) at site_i ==
- *    site_i_star.  Every slot of the table is served. */
+ *    site_i_star.  Every slot of the table is served.
+ *  - A caller compiled with MULTIPOLE_INTEGRAL, as the reference's rule
+ *    switch selects it, gets the mean-field values and derivatives of the
+ *    multipole rule (btam_mf_eval_multipole, btam_mf_residuals_multipole;
+ *    FP64): with finite-difference Hessians when NUMERICAL_DERIVATIVES is
+ *    defined (the reference's CMakeLists.txt defines it), analytic ones
+ *    otherwise.  The stretch derivative and the Hessian blocks stay on the
+ *    degree-3 rule. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -202,8 +209,23 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
   }
   if (!c.have_state) return;
   if ((what & kMeanField) && !c.valid) {
+#if defined(MULTIPOLE_INTEGRAL)
+    // the caller is built with the reference's other rule
+    // (MgHx-mf-V-bulk.cpp:715-724), whose Hessians follow the same
+    // `#ifdef NUMERICAL_DERIVATIVES` as Quadrature-Multipole.cpp:134
+#ifdef NUMERICAL_DERIVATIVES
+    const int rule = BTAM_MP_FD;
+#else
+    const int rule = BTAM_MP_ANALYTIC;
+#endif
+    c.status = btam_mf_eval_multipole(c.sys, rule, c.rho.data(), c.V0.data(), c.S0.data(),
+                                      nullptr);
+    if (c.status == BTAM_OK)
+      c.status = btam_mf_residuals_multipole(c.sys, rule, c.Rq.data(), c.Rs.data(), c.Rx.data());
+#else
     c.status = btam_mf_eval(c.sys, c.precision, c.rho.data(), c.V0.data(), c.S0.data(),
                             c.Rq.data(), c.Rs.data(), c.Rx.data(), nullptr);
+#endif
     c.valid = c.status == BTAM_OK;
   }
   if ((what & kPoint) && !c.pt_valid) {

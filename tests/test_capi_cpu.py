@@ -13,7 +13,9 @@ from btam import dump, lattice
 def test_library_exports_every_declared_symbol():
     names = btam.exported_symbols()
     assert len(names) >= 20
-    L = ctypes.CDLL(btam.LIB_PATH)
+    # RTLD_NOW: every symbol the library needs resolves at load, not at the
+    # first call
+    L = ctypes.CDLL(btam.LIB_PATH, mode=os.RTLD_NOW | os.RTLD_LOCAL)
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
     assert L.btam_version() >= 100

@@ -58,6 +58,38 @@ def test_plugin_table_matches_direct_evaluation(gpu_tables, tmp_path):
     assert np.abs(v[:, 7] - dx).max() <= 1e-12 * scale
 
 
+@pytest.mark.parametrize("defines,rule", [
+    (("MULTIPOLE_INTEGRAL", "NUMERICAL_DERIVATIVES=0"), btam.MP_FD),
+    (("MULTIPOLE_INTEGRAL",), btam.MP_ANALYTIC)])
+def test_plugin_table_multipole_build(gpu_tables, tmp_path, defines, rule):
+    """A caller compiled with the reference's MULTIPOLE_INTEGRAL switch (and
+    its NUMERICAL_DERIVATIVES, or without it) gets the multipole rule's
+    values and derivatives."""
+    import compat_build
+    probe = compat_build.build_probe(defines)
+    s = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.5, x_range=(0.0, 0.4),
+                          sigma_range=(0.08, 0.15), jitter=0.02, seed=29)
+    n = len(s["x"])
+    inp, out = str(tmp_path / "sys.bin"), str(tmp_path / "out.bin")
+    write_system(inp, s)
+    r = subprocess.run([probe, TABLES, inp, out], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    raw = open(out, "rb").read()
+    v = np.frombuffer(raw[:8 * 8 * n], np.float64).reshape(n, 8)
+    assert np.frombuffer(raw[8 * 8 * n:], np.int32)[0] == 0
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    rho, V0, _ = S.mf_eval_multipole(rule)
+    Rq, Rs, Rx = S.mf_residuals_multipole(rule)
+    assert np.array_equal(v[:, 0], rho) and np.array_equal(v[:, 1], V0)
+    assert np.array_equal(v[:, 2], S.last_S0) and np.array_equal(v[:, 3:6], Rq)
+    beta, sigma = s["beta"], s["sigma"]
+    dsig = Rs + 3.0 / (beta * sigma)
+    assert np.abs(v[:, 6] - dsig).max() <= 1e-12 * max(1.0, np.abs(dsig).max())
+    # and it is not the degree-3 rule
+    assert np.abs(rho - S.evaluate(btam.FP64)["rho"]).max() > 1e-8
+
+
 def test_plugin_table_point_forms_match_reference(gpu_tables, tmp_path):
     """The non-mean-field slots (evaluate_rho_i, evaluate_DV_i_Dq_j,
     evaluate_DV_i_DF) driven the way the reference's bulk residual drives

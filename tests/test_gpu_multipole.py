@@ -37,6 +37,7 @@ def test_multipole_against_reference(gpu_tables, name, rule):
     assert np.allclose(rho, m[key + "rho"], rtol=tol, atol=0)
     assert np.abs(V0 - m[key + "V0"]).max() <= tol * np.abs(m[key + "V0"]).max()
     assert abs(E - m[key + "V0"].sum()) <= tol * np.abs(m[key + "V0"]).sum()
+    assert np.abs(S.last_S0 - m[key + "S0"]).max() <= tol * np.abs(m[key + "S0"]).max()
     # reproducible, and different from the degree-3 rule
     rho2, V02, E2 = S.mf_eval_multipole(rule)
     assert np.array_equal(rho, rho2) and np.array_equal(V0, V02) and E == E2
