@@ -70,3 +70,45 @@ def test_multipole_rejects_unknown_rule(gpu_tables):
             S.mf_eval_multipole(rule)
         with pytest.raises(btam.BtamError):
             S.mf_residuals_multipole(rule)
+
+
+def test_multipole_full_size_translation_invariance(gpu_tables):
+    """Plain drop-in size (27,000 sites), rule 2: the per-site values stay
+    finite and the multipole residual R_q sums to zero over the periodic
+    cell (uniform beta; every term depends on differences of positions)."""
+    from btam import lattice
+    s = lattice.config2()
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    rho, V0, E = S.mf_eval_multipole(btam.MP_ANALYTIC)
+    assert np.isfinite(V0).all() and np.isfinite(E)
+    Rq, Rs, Rx = S.mf_residuals_multipole(btam.MP_ANALYTIC)
+    assert np.isfinite(Rq).all() and np.isfinite(Rs).all() and np.isfinite(Rx).all()
+    assert np.abs(Rq.sum(axis=0)).max() < 1e-8 * max(1.0, np.abs(Rq).max()) * len(Rq) ** 0.5
+
+
+def test_multipole_sigma_derivative_by_differences(gpu_tables):
+    """Rule 2 (analytic Hessians): R_sigma + 3 / (beta sigma) is the exact
+    derivative of sum_i V0_i in sigma_u (uniform beta), checked by central
+    differences of the device energy."""
+    g = load("ortho_mgh")
+    s = system_of(g)
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    _, _, E0 = S.mf_eval_multipole(btam.MP_ANALYTIC)
+    _, Rs, _ = S.mf_residuals_multipole(btam.MP_ANALYTIC)
+    beta, sigma, x = s["beta"], s["sigma"], s["x"]
+    assert np.ptp(beta) == 0.0
+    h = 1e-5
+    for u in np.flatnonzero(x >= 5e-4)[::37][:6]:
+        sp, sm = sigma.copy(), sigma.copy()
+        sp[u] += h
+        sm[u] -= h
+        S.set_state(sigma=sp)
+        Ep = S.mf_eval_multipole(btam.MP_ANALYTIC)[2]
+        S.set_state(sigma=sm)
+        Em = S.mf_eval_multipole(btam.MP_ANALYTIC)[2]
+        S.set_state(sigma=sigma)
+        fd = (Ep - Em) / (2 * h)
+        an = Rs[u] + 3.0 / (beta[u] * sigma[u])
+        assert abs(fd - an) <= 1e-6 * max(1.0, abs(an)), (u, fd, an)
