@@ -75,6 +75,7 @@ _PROTOS = {
     "btam_mf_eval_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D,
                                               ctypes.POINTER(ctypes.c_double)]),
     "btam_mf_residuals_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D]),
+    "btam_mf_stress_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
@@ -470,6 +471,15 @@ class System:
         _check(lib().btam_mf_residuals_multipole(self.handle, int(rule), _d(Rq), _d(Rs), _d(Rx)),
                "btam_mf_residuals_multipole")
         return Rq, Rs, Rx
+
+    def mf_stress_multipole(self, rule=1):
+        """(W0 (n, 3, 3), total (3, 3)): evaluate_DV0_i_dF_bulk_MgHx under
+        the multipole rule at q0 = q, FP64."""
+        W = np.zeros((self.n, 3, 3))
+        tot = np.zeros((3, 3))
+        _check(lib().btam_mf_stress_multipole(self.handle, int(rule), _d(W), _d(tot)),
+               "btam_mf_stress_multipole")
+        return W, tot
 
     def mf_hessian(self):
         """Mean-field Hessian blocks, (n, 3, 3): the sum over i in {u} U N(u)

@@ -593,23 +593,20 @@ __device__ __forceinline__ void moved(const double (&q)[N], int k, int which, do
                                                                             : q[k] - dr * 2;
 }
 
-// One pair measure (c = slot 0, nb = slot 1) for u in slot `dir`: the
-// multipole dmq and dsq of rho and of the pair term, and the degree-3 dxi.
-struct PairOut {
-  double drho_q[3], pair_q[3], drho_s, pair_s, drho_x, pair_x;
-};
-__device__ void pair_residual(const RadialView<double> &T, int rule, const PairSite &c,
-                              const PairSite &nb, int dir, PairOut &o) {
+// meanfield_integral_mp_dmq of rho_ij and V_pair_ij over the pair measure
+// (c, nb) for slot `dir`: the gradient at the mean plus sigma_s^2 / 2 times
+// its five-point second differences in every coordinate of both slots.
+__device__ void pair_dmq(const RadialView<double> &T, const PairSite &c, const PairSite &nb,
+                         int dir, double *drho, double *dpair) {
   const int pk = pair_kind(c.code, nb.code);
   const double q[6] = {c.q[0], c.q[1], c.q[2], nb.q[0], nb.q[1], nb.q[2]};
-  const double sig[2] = {c.sig, nb.sig}, n[2] = {c.x, nb.x};
-  // dmq: gradient at the mean plus sigma_s^2 / 2 x second differences
+  const double sig[2] = {c.sig, nb.sig};
   double g0r[3], g0p[3];
   rho_dq(T, pk, nb.code, nb.x, dir, q, g0r);
   pair_dq(T, pk, c.x, nb.x, dir, q, g0p);
   for (int a = 0; a < 3; ++a) {
-    o.drho_q[a] = g0r[a];
-    o.pair_q[a] = g0p[a];
+    drho[a] = g0r[a];
+    dpair[a] = g0p[a];
   }
   for (int s = 0; s < 2; ++s) {
     const double c2 = sqz(sig[s]) / 2.0;
@@ -622,11 +619,56 @@ __device__ void pair_residual(const RadialView<double> &T, int rule, const PairS
         pair_dq(T, pk, c.x, nb.x, dir, qq, gp[w]);
       }
       for (int b = 0; b < 3; ++b) {
-        o.drho_q[b] += c2 * d2_dmq(gr[0][b], gr[1][b], g0r[b], gr[2][b], gr[3][b]);
-        o.pair_q[b] += c2 * d2_dmq(gp[0][b], gp[1][b], g0p[b], gp[2][b], gp[3][b]);
+        drho[b] += c2 * d2_dmq(gr[0][b], gr[1][b], g0r[b], gr[2][b], gr[3][b]);
+        dpair[b] += c2 * d2_dmq(gp[0][b], gp[1][b], g0p[b], gp[2][b], gp[3][b]);
       }
     }
   }
+}
+
+// meanfield_integral_mp_dmq of V_dipole and V_quadrupole over the triplet
+// measure (c, j1, j2) for slot `dir`; every slot moves alone.
+__device__ void tri_dmq(const RadialView<double> &T, const PairSite &c, const PairSite &j1,
+                        const PairSite &j2, int dir, double *gdip, double *gquad) {
+  const int pk1 = pair_kind(c.code, j1.code), pk2 = pair_kind(c.code, j2.code);
+  const double n[3] = {c.x, j1.x, j2.x};
+  const double q[9] = {c.q[0],  c.q[1],  c.q[2],  j1.q[0], j1.q[1],
+                       j1.q[2], j2.q[0], j2.q[1], j2.q[2]};
+  const double sig[3] = {c.sig, j1.sig, j2.sig};
+  double g0d[3], g0q[3];
+  tri_dq(T, pk1, pk2, n, dir, q, g0d, g0q);
+  for (int a = 0; a < 3; ++a) {
+    gdip[a] = g0d[a];
+    gquad[a] = g0q[a];
+  }
+  for (int s = 0; s < 3; ++s) {
+    const double c2 = sqz(sig[s]) / 2.0;
+    for (int al = 0; al < 3; ++al) {
+      double gd[4][3], gq[4][3];
+      for (int w = 0; w < 4; ++w) {
+        double qq[9];
+        moved(q, 3 * s + al, w, qq);
+        tri_dq(T, pk1, pk2, n, dir, qq, gd[w], gq[w]);
+      }
+      for (int b = 0; b < 3; ++b) {
+        gdip[b] += c2 * d2_dmq(gd[0][b], gd[1][b], g0d[b], gd[2][b], gd[3][b]);
+        gquad[b] += c2 * d2_dmq(gq[0][b], gq[1][b], g0q[b], gq[2][b], gq[3][b]);
+      }
+    }
+  }
+}
+
+// One pair measure (c = slot 0, nb = slot 1) for u in slot `dir`: the
+// multipole dmq and dsq of rho and of the pair term, and the degree-3 dxi.
+struct PairOut {
+  double drho_q[3], pair_q[3], drho_s, pair_s, drho_x, pair_x;
+};
+__device__ void pair_residual(const RadialView<double> &T, int rule, const PairSite &c,
+                              const PairSite &nb, int dir, PairOut &o) {
+  const int pk = pair_kind(c.code, nb.code);
+  const double q[6] = {c.q[0], c.q[1], c.q[2], nb.q[0], nb.q[1], nb.q[2]};
+  const double sig[2] = {c.sig, nb.sig}, n[2] = {c.x, nb.x};
+  pair_dmq(T, c, nb, dir, o.drho_q, o.pair_q);
   // dsq: sigma_dir x tr of block (dir, dir)
   o.drho_s = 0.0;
   o.pair_s = 0.0;
@@ -685,27 +727,7 @@ __device__ void tri_residual(const RadialView<double> &T, int rule, const PairSi
   for (int a = 0; a < 3; ++a) o.dip_q[a] = o.quad_q[a] = 0.0;
   o.dip_s = o.quad_s = o.dip_x = o.quad_x = 0.0;
   if (with_q) {
-    double g0d[3], g0q[3];
-    tri_dq(T, pk1, pk2, n, dir, q, g0d, g0q);
-    for (int a = 0; a < 3; ++a) {
-      o.dip_q[a] = g0d[a];
-      o.quad_q[a] = g0q[a];
-    }
-    for (int s = 0; s < 3; ++s) {
-      const double c2 = sqz(sig[s]) / 2.0;
-      for (int al = 0; al < 3; ++al) {
-        double gd[4][3], gq[4][3];
-        for (int w = 0; w < 4; ++w) {
-          double qq[9];
-          moved(q, 3 * s + al, w, qq);
-          tri_dq(T, pk1, pk2, n, dir, qq, gd[w], gq[w]);
-        }
-        for (int b = 0; b < 3; ++b) {
-          o.dip_q[b] += c2 * d2_dmq(gd[0][b], gd[1][b], g0d[b], gd[2][b], gd[3][b]);
-          o.quad_q[b] += c2 * d2_dmq(gq[0][b], gq[1][b], g0q[b], gq[2][b], gq[3][b]);
-        }
-      }
-    }
+    tri_dmq(T, c, j1, j2, dir, o.dip_q, o.quad_q);
     // dsq: sigma_dir x sum over the dof row of dir of the block traces
     if (rule == 1) {
       double f0d, f0q;
@@ -961,6 +983,80 @@ __global__ void mp_assemble_kernel(MpResArgs r) {
   r.Rx[u] = rx;
 }
 
+// evaluate_DV0_i_dF_bulk_MgHx (MgHx-mf-V-bulk.cpp:2329-2552) under the rule,
+// at reference positions q0 = q: for every term of V0_i, each slot a's
+// meanfield_integral_mp_dmq (x) q_a, summed; W0_i = x_i F'(rho_i) drho +
+// pair + dipole + quadrupole (3x3, row: gradient component).  j1 and j2
+// skip empty H sites (2408-2410, 2465-2467).  A warp per real site.
+__global__ void __launch_bounds__(128) mp_stress_kernel(MpArgs a, double *W) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= a.n_real) return;
+  const PairSite si = site_of(a, i);
+  double drho[9], pair[9], dip[9], quad[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) drho[c] = pair[c] = dip[c] = quad[c] = 0.0;
+  const int nb0 = a.offs[i], nn = a.offs[i + 1] - nb0;
+  if (!(si.x < kMinOcc)) {
+    for (int k = lane; k < nn; k += 32) {
+      const PairSite sj = site_of(a, a.idx[nb0 + k]);
+      if (empty_h(sj)) continue;
+      for (int dir = 0; dir < 2; ++dir) {
+        const double *r0 = dir == 0 ? si.q : sj.q;
+        double gr[3], gp[3];
+        pair_dmq(a.T, si, sj, dir, gr, gp);
+        for (int x = 0; x < 3; ++x)
+          for (int y = 0; y < 3; ++y) {
+            drho[3 * x + y] += gr[x] * r0[y];
+            pair[3 * x + y] += gp[x] * r0[y];
+          }
+      }
+    }
+    const long long ntri = (long long)nn * (nn + 1) / 2;
+    for (long long t = lane; t < ntri; t += 32) {
+      int k2 = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+      while ((long long)k2 * (k2 + 1) / 2 > t) --k2;
+      while ((long long)(k2 + 1) * (k2 + 2) / 2 <= t) ++k2;
+      const int k1 = (int)(t - (long long)k2 * (k2 + 1) / 2);
+      const PairSite s1 = site_of(a, a.idx[nb0 + k1]);
+      if (empty_h(s1)) continue;
+      const PairSite s2 = site_of(a, a.idx[nb0 + k2]);
+      if (empty_h(s2)) continue;
+      const double f = k1 == k2 ? 1.0 : 2.0;
+      for (int dir = 0; dir < 3; ++dir) {
+        const double *r0 = dir == 0 ? si.q : (dir == 1 ? s1.q : s2.q);
+        double gd[3], gq[3];
+        tri_dmq(a.T, si, s1, s2, dir, gd, gq);
+        for (int x = 0; x < 3; ++x)
+          for (int y = 0; y < 3; ++y) {
+            dip[3 * x + y] += f * gd[x] * r0[y];
+            quad[3 * x + y] += f * gq[x] * r0[y];
+          }
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 9; ++c) {
+    drho[c] = warp_sum(drho[c]);
+    pair[c] = warp_sum(pair[c]);
+    dip[c] = warp_sum(dip[c]);
+    quad[c] = warp_sum(quad[c]);
+  }
+  if (lane == 0) {
+    double dF = 0.0;
+    if (!(si.x < kMinOcc)) {
+      const SplineView<double> &E = si.code == 0 ? a.emb_mg : a.emb_h;
+      double p;
+      const int m = seg_ref(a.rho[i], E.dx, E.n, p);
+      const Coef4<double> cf = E.c[m];
+      const double k4[4] = {cf.a, cf.b, cf.c, cf.d};
+      dF = cubd(k4, p);
+    }
+    for (int c = 0; c < 9; ++c)
+      W[9 * (size_t)i + c] =
+          si.x < kMinOcc ? 0.0 : si.x * dF * drho[c] + pair[c] + dip[c] + quad[c];
+  }
+}
+
 }  // namespace
 }  // namespace btam
 
@@ -1089,6 +1185,57 @@ int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs
   dfree(g5, s->st);
   dfree(out, s->st);
   if (e != cudaSuccess) return cuda_status(e);
+  return read_err(s);
+}
+
+int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total) {
+  if (!s || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC)) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  const size_t n = (size_t)s->n_real;
+  double *rd = nullptr, *wd = nullptr;
+  BTAM_TRY(dalloc(rd, s->st, n));
+  int st = dalloc(wd, s->st, 9 * n);
+  if (st != BTAM_OK) {
+    dfree(rd, s->st);
+    return st;
+  }
+  MpArgs a;
+  a.n_real = s->n_real;
+  a.rule = rule;
+  a.pos = s->pos;
+  a.xb = s->xb;
+  a.code = s->code;
+  a.offs = s->offs;
+  a.idx = s->idx;
+  a.T = s->T->r64;
+  a.emb_mg = s->T->v64.t[T_F_MG];
+  a.emb_h = s->T->v64.t[T_F_H];
+  a.rho = rd;
+  a.out = rd;
+  a.S0 = nullptr;
+  a.gamma = s->gamma;
+  a.mass[0] = tables_mass(s->T, 0);
+  a.mass[1] = tables_mass(s->T, 1);
+  const int g = (int)(((long long)n * 32 + 127) / 128);
+  cudaError_t e = cudaSuccess;
+  std::vector<double> hw(9 * n);
+  if (g > 0) {
+    mp_rho_kernel<<<g, 128, 0, s->st>>>(a);
+    mp_stress_kernel<<<g, 128, 0, s->st>>>(a, wd);
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(hw.data(), wd, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  dfree(rd, s->st);
+  dfree(wd, s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (W0) std::copy(hw.begin(), hw.end(), W0);
+  if (total) {
+    for (int c = 0; c < 9; ++c) total[c] = 0.0;
+    for (size_t k = 0; k < n; ++k)
+      for (int c = 0; c < 9; ++c) total[c] += hw[9 * k + c];
+  }
   return read_err(s);
 }
 

@@ -238,6 +238,11 @@ int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, do
  * a direct evaluation: one warp per (site, centre) pair. */
 int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs,
                                 double *Rx);
+/* The mean-field stress under the same rule, as btam_mf_stress: W0 (9 per
+ * real site, row-major) = evaluate_DV0_i_dF_bulk_MgHx (2329-2552) built
+ * with the rule (its meanfield_integral_mp_dmq) at reference positions q0 =
+ * q; total (9) their sum.  Either output may be NULL.  FP64, direct. */
+int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total);
 
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */

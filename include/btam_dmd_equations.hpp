@@ -62,8 +62,9 @@
  *    multipole rule (btam_mf_eval_multipole, btam_mf_residuals_multipole;
  *    FP64): with finite-difference Hessians when NUMERICAL_DERIVATIVES is
  *    defined (the reference's CMakeLists.txt defines it), analytic ones
- *    otherwise.  The stretch derivative and the Hessian blocks stay on the
- *    degree-3 rule. */
+ *    otherwise; the mean-field stretch derivative too
+ *    (btam_mf_stress_multipole).  The Hessian blocks stay on the degree-3
+ *    rule. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -234,7 +235,15 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
     c.pt_valid = c.status == BTAM_OK;
   }
   if ((what & kStress) && !c.mfs_valid) {
+#if defined(MULTIPOLE_INTEGRAL)
+#ifdef NUMERICAL_DERIVATIVES
+    c.status = btam_mf_stress_multipole(c.sys, BTAM_MP_FD, c.mf_W.data(), nullptr);
+#else
+    c.status = btam_mf_stress_multipole(c.sys, BTAM_MP_ANALYTIC, c.mf_W.data(), nullptr);
+#endif
+#else
     c.status = btam_mf_stress(c.sys, c.precision, c.mf_W.data(), nullptr);
+#endif
     c.mfs_valid = c.status == BTAM_OK;
   }
   if ((what & kHessian) && !c.pth_valid) {

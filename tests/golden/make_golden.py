@@ -179,8 +179,9 @@ def multipole_fixture():
     from the reference built two ways (oracle/Makefile): with its own
     -DNUMERICAL_DERIVATIVES=0, which selects finite-difference Hessians
     (rule 1), and without it, analytic Hessians (rule 2).  On the stored
-    topologies of two system fixtures: rho-bar, V0, S0 of every real site
-    and the assembled residuals of a sample of sites."""
+    topologies of two system fixtures: rho-bar, V0, S0 and the stretch
+    derivative evaluate_DV0_i_dF_bulk_MgHx (q0 = q) of every real site, and
+    the assembled residuals of a sample of sites."""
     out = {}
     for rule, analytic in ((1, False), (2, True)):
         ref = pyoracle.reference_multipole(analytic)
@@ -204,7 +205,8 @@ def multipole_fixture():
             key = f"{name}_r{rule}_"
             out.update({key + "rho": rho_real, key + "V0": ref.V0(full, rho, offs, idx, real),
                         key + "S0": ref.S0(full, rho, offs, idx, real), key + "res_sites": us,
-                        key + "Rq": Rq, key + "Rs": Rs, key + "Rx": Rx})
+                        key + "Rq": Rq, key + "Rs": Rs, key + "Rx": Rx,
+                        key + "W0": ref.mf_DV0_dF(full, full["q"], rho, offs, idx, real)})
             print(f"multipole rule {rule} {name}: {n} real, {len(us)} residual sites")
     np.savez_compressed(os.path.join(OUT, "multipole.npz"), **out)
 

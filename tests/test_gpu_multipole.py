@@ -61,6 +61,19 @@ def test_multipole_residuals_against_reference(gpu_tables, name, rule):
     assert np.array_equal(Rq, Rq2) and np.array_equal(Rs, Rs2) and np.array_equal(Rx, Rx2)
 
 
+@pytest.mark.parametrize("rule", [btam.MP_FD, btam.MP_ANALYTIC])
+@pytest.mark.parametrize("name", ["sphere", "ortho_mgh"])
+def test_multipole_stress_against_reference(gpu_tables, name, rule):
+    """evaluate_DV0_i_dF_bulk_MgHx under the rule, q0 = q."""
+    g, m = load(name), load("multipole")
+    b = m[f"{name}_r{rule}_W0"]
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    W, tot = S.mf_stress_multipole(rule)
+    assert np.abs(W - b).max() <= 1e-11 * max(1.0, np.abs(b).max())
+    assert np.abs(tot - b.sum(axis=0)).max() <= 1e-11 * max(1.0, np.abs(b).sum(axis=0).max())
+
+
 def test_multipole_rejects_unknown_rule(gpu_tables):
     g = load("sphere")
     S = btam.System(gpu_tables, system_of(g))
@@ -70,6 +83,8 @@ def test_multipole_rejects_unknown_rule(gpu_tables):
             S.mf_eval_multipole(rule)
         with pytest.raises(btam.BtamError):
             S.mf_residuals_multipole(rule)
+        with pytest.raises(btam.BtamError):
+            S.mf_stress_multipole(rule)
 
 
 def test_multipole_full_size_translation_invariance(gpu_tables):

@@ -209,8 +209,11 @@ def test_multipole_rule_against_golden(oracle, name, rule):
         S0 = oracle.S0(full, rho[owner], offs, idx, real)
         Rq, Rs, Rx = oracle.residuals(full, rho[owner], owner, image, offs, idx,
                                       m[key + "res_sites"])
+        W0 = oracle.mf_DV0_dF(full, full["q"], rho[owner], offs, idx, real)
     finally:
         oracle.set_rule(0)
+    b = m[key + "W0"]
+    assert np.abs(W0 - b).max() <= (0 if rule == 1 else 1e-13) * max(1.0, np.abs(b).max())
     if rule == 1:
         assert np.array_equal(rho, m[key + "rho"])
         assert np.array_equal(V0, m[key + "V0"])
