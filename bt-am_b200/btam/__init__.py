@@ -76,6 +76,7 @@ _PROTOS = {
                                               ctypes.POINTER(ctypes.c_double)]),
     "btam_mf_residuals_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D]),
     "btam_mf_stress_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
+    "btam_mf_hessian_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
@@ -480,6 +481,13 @@ class System:
         _check(lib().btam_mf_stress_multipole(self.handle, int(rule), _d(W), _d(tot)),
                "btam_mf_stress_multipole")
         return W, tot
+
+    def mf_hessian_multipole(self, rule=1):
+        """Mean-field Hessian blocks (n, 3, 3) under the multipole rule."""
+        H = np.zeros((self.n, 3, 3))
+        _check(lib().btam_mf_hessian_multipole(self.handle, int(rule), _d(H)),
+               "btam_mf_hessian_multipole")
+        return H
 
     def mf_hessian(self):
         """Mean-field Hessian blocks, (n, 3, 3): the sum over i in {u} U N(u)

@@ -106,6 +106,9 @@ int mf_rho64_enqueue(btam_system *s);
 // Enqueues the mean-field Hessian blocks of the current state into Hd (9
 // per real site) (mf_hessian.cu).
 int mf_hessian_enqueue(btam_system *s, double *Hd);
+// The same blocks on a given rho-bar and, if gmp is set, per-list-entry
+// rho gradients (3 per entry of a real site) instead of the degree-3 ones.
+int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp, double *Hd);
 
 // Enqueues the directed pass 1 and the mean-field stress of the current
 // state; *W: per-site stress (9 n), *tot: totals whose [2..10] hold the sum

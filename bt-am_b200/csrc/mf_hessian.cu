@@ -170,6 +170,11 @@ struct MfhArgs {
   const double2 *xb;
   const int *code, *owner, *offs, *idx;
   const double *rho;  // mean-field rho-bar of the real sites
+  // null: the rho gradients come from the degree-3 rule's points; else, per
+  // list entry p of a real site i, the gradient of rho_ij (j = idx[p]) in
+  // q_i that replaces them (the multipole rule's, whose gradient in q_j is
+  // its exact negative)
+  const double *gmp;
   RadialView<double> T;
   SplineView<double> emb_mg, emb_h;
   double *H;
@@ -269,7 +274,10 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
       const int c1 = a.code[j1];
       // ---- i = u: pair (u, j1), centre block
       double pair[6] = {0, 0, 0, 0, 0, 0};
-      pair_terms(a, qu, cu, xu, pu.w, q1, c1, x1, p1.w, 0, gsum, d2s, pair);
+      double gdeg3[3] = {0, 0, 0};
+      pair_terms(a, qu, cu, xu, pu.w, q1, c1, x1, p1.w, 0, a.gmp ? gdeg3 : gsum, d2s, pair);
+      if (a.gmp)
+        for (int c = 0; c < 3; ++c) gsum[c] += a.gmp[3 * (size_t)k1 + c];
       for (int c = 0; c < 6; ++c) hs[c] += pair[c];
       // triplets (u, j1, j2), j2 at or after j1 in u's list
       const double r1[3] = {qu[0] - q1[0], qu[1] - q1[1], qu[2] - q1[2]};
@@ -301,6 +309,8 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
       if (xu <= kMinOcc && cu == 1) continue;
       double gi[3] = {0, 0, 0}, d2i[6] = {0, 0, 0, 0, 0, 0}, hi[6] = {0, 0, 0, 0, 0, 0};
       pair_terms(a, q1, c1, x1, p1.w, qu, cu, xu, pu.w, 1, gi, d2i, hi);
+      if (a.gmp)
+        for (int c = 0; c < 3; ++c) gi[c] = -a.gmp[3 * (size_t)ks + c];
       const double ru[3] = {-d[0], -d[1], -d[2]};  // q_j1 - q_u
       for (int k2 = a.offs[o]; k2 < a.offs[o + 1]; ++k2) {
         const int j2 = a.idx[k2];
@@ -345,6 +355,10 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
 int mf_hessian_enqueue(btam_system *s, double *Hd) {
   int st = mf_rho64_enqueue(s);  // rho-bar of the real sites into the system's rho
   if (st != BTAM_OK) return st;
+  return mf_hessian_enqueue_with(s, s->rho, nullptr, Hd);
+}
+
+int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp, double *Hd) {
   MfhArgs a;
   a.n_real = s->n_real;
   a.pos = s->pos;
@@ -353,7 +367,8 @@ int mf_hessian_enqueue(btam_system *s, double *Hd) {
   a.owner = s->owner;
   a.offs = s->offs;
   a.idx = s->idx;
-  a.rho = s->rho;
+  a.rho = rho;
+  a.gmp = gmp;
   a.T = s->T->r64;
   a.emb_mg = s->T->v64.t[T_F_MG];
   a.emb_h = s->T->v64.t[T_F_H];

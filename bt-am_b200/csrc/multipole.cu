@@ -1057,6 +1057,22 @@ __global__ void __launch_bounds__(128) mp_stress_kernel(MpArgs a, double *W) {
   }
 }
 
+// Per list entry p of a real site i: the multipole rule's gradient of rho_ij
+// (j = idx[p]) in q_i (meanfield_integral_mp_dmq), the piece of
+// evaluate_D2V0_i_Dmeanq2_u_MgHx the rule changes (MgHx-mf-V-bulk.cpp:1476;
+// its blocks stay on meanfield_integral_gh_3th_d2mq, 1482-1566).
+__global__ void __launch_bounds__(128) mp_rho_grad_kernel(MpArgs a, double *G) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (i >= a.n_real) return;
+  const PairSite si = site_of(a, i);
+  for (int k = a.offs[i] + lane; k < a.offs[i + 1]; k += 32) {
+    const PairSite sj = site_of(a, a.idx[k]);
+    double gr[3], gp[3];
+    pair_dmq(a.T, si, sj, 0, gr, gp);
+    for (int c = 0; c < 3; ++c) G[3 * (size_t)k + c] = gr[c];
+  }
+}
+
 }  // namespace
 }  // namespace btam
 
@@ -1236,6 +1252,59 @@ int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total
     for (size_t k = 0; k < n; ++k)
       for (int c = 0; c < 9; ++c) total[c] += hw[9 * k + c];
   }
+  return read_err(s);
+}
+
+int btam_mf_hessian_multipole(btam_system *s, int rule, double *H) {
+  if (!s || !H || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC)) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  const size_t n = (size_t)s->n_real;
+  if (n == 0) return BTAM_OK;
+  int np = 0;
+  cudaError_t e = cudaMemcpyAsync(&np, s->offs + n, sizeof(int), cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  double *rd = nullptr, *G = nullptr, *Hd = nullptr;
+  BTAM_TRY(dalloc(rd, s->st, n));
+  int st = dalloc(G, s->st, 3 * (size_t)(np > 0 ? np : 1));
+  if (st == BTAM_OK) st = dalloc(Hd, s->st, 9 * n);
+  if (st != BTAM_OK) {
+    dfree(rd, s->st);
+    dfree(G, s->st);
+    return st;
+  }
+  MpArgs a;
+  a.n_real = s->n_real;
+  a.rule = rule;
+  a.pos = s->pos;
+  a.xb = s->xb;
+  a.code = s->code;
+  a.offs = s->offs;
+  a.idx = s->idx;
+  a.T = s->T->r64;
+  a.emb_mg = s->T->v64.t[T_F_MG];
+  a.emb_h = s->T->v64.t[T_F_H];
+  a.rho = rd;
+  a.out = rd;
+  a.S0 = nullptr;
+  a.gamma = s->gamma;
+  a.mass[0] = tables_mass(s->T, 0);
+  a.mass[1] = tables_mass(s->T, 1);
+  const int g = (int)(((long long)n * 32 + 127) / 128);
+  mp_rho_kernel<<<g, 128, 0, s->st>>>(a);
+  mp_rho_grad_kernel<<<g, 128, 0, s->st>>>(a, G);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) {
+    st = mf_hessian_enqueue_with(s, rd, G, Hd);
+    if (st == BTAM_OK)
+      e = cudaMemcpyAsync(H, Hd, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+    if (st == BTAM_OK && e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  }
+  dfree(rd, s->st);
+  dfree(G, s->st);
+  dfree(Hd, s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  if (st != BTAM_OK) return st;
   return read_err(s);
 }
 

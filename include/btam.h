@@ -243,6 +243,12 @@ int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs
  * with the rule (its meanfield_integral_mp_dmq) at reference positions q0 =
  * q; total (9) their sum.  Either output may be NULL.  FP64, direct. */
 int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total);
+/* The mean-field Hessian blocks under the same rule, as btam_mf_hessian:
+ * evaluate_D2V0_i_Dmeanq2_u_MgHx (1366-1600) built with the rule, which
+ * takes its rho gradient from meanfield_integral_mp_dmq (1476) and keeps
+ * the term blocks on the degree-3 rule (meanfield_integral_gh_3th_d2mq),
+ * at the multipole rho-bar.  H: 9 per real site.  FP64. */
+int btam_mf_hessian_multipole(btam_system *s, int rule, double *H);
 
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */

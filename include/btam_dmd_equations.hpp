@@ -62,9 +62,9 @@
  *    multipole rule (btam_mf_eval_multipole, btam_mf_residuals_multipole;
  *    FP64): with finite-difference Hessians when NUMERICAL_DERIVATIVES is
  *    defined (the reference's CMakeLists.txt defines it), analytic ones
- *    otherwise; the mean-field stretch derivative too
- *    (btam_mf_stress_multipole).  The Hessian blocks stay on the degree-3
- *    rule. */
+ *    otherwise; the mean-field stretch derivative and Hessian blocks too
+ *    (btam_mf_stress_multipole, btam_mf_hessian_multipole).  The
+ *    non-mean-field forms have no rule. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
 
@@ -251,7 +251,15 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
     c.pth_valid = c.status == BTAM_OK;
   }
   if ((what & kMfHessian) && !c.mfh_valid) {
+#if defined(MULTIPOLE_INTEGRAL)
+#ifdef NUMERICAL_DERIVATIVES
+    c.status = btam_mf_hessian_multipole(c.sys, BTAM_MP_FD, c.mf_H.data());
+#else
+    c.status = btam_mf_hessian_multipole(c.sys, BTAM_MP_ANALYTIC, c.mf_H.data());
+#endif
+#else
     c.status = btam_mf_hessian(c.sys, c.mf_H.data());
+#endif
     c.mfh_valid = c.status == BTAM_OK;
   }
 }

@@ -207,6 +207,14 @@ def multipole_fixture():
                         key + "S0": ref.S0(full, rho, offs, idx, real), key + "res_sites": us,
                         key + "Rq": Rq, key + "Rs": Rs, key + "Rx": Rx,
                         key + "W0": ref.mf_DV0_dF(full, full["q"], rho, offs, idx, real)})
+            # the assembled Hessian blocks (evaluate_D2V0_i_Dmeanq2_u_MgHx)
+            plan = residual_pairs(full, owner, image, offs, idx, real)
+            kk = np.array([p_[0] for p_ in plan])
+            h9 = ref.mf_D2V0_pairs(full, rho, offs, idx, np.array([p_[1] for p_ in plan], np.int32),
+                                   np.array([p_[2] for p_ in plan], np.int32))
+            H0 = np.zeros((n, 3, 3))
+            np.add.at(H0, kk, h9)
+            out[key + "H0"] = H0
             print(f"multipole rule {rule} {name}: {n} real, {len(us)} residual sites")
     np.savez_compressed(os.path.join(OUT, "multipole.npz"), **out)
 

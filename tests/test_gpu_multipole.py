@@ -74,6 +74,20 @@ def test_multipole_stress_against_reference(gpu_tables, name, rule):
     assert np.abs(tot - b.sum(axis=0)).max() <= 1e-11 * max(1.0, np.abs(b).sum(axis=0).max())
 
 
+@pytest.mark.parametrize("rule", [btam.MP_FD, btam.MP_ANALYTIC])
+@pytest.mark.parametrize("name", ["sphere", "ortho_mgh"])
+def test_multipole_hessian_against_reference(gpu_tables, name, rule):
+    """evaluate_D2V0_i_Dmeanq2_u_MgHx built with the rule, summed over
+    i in {u} U N(u)."""
+    g, m = load(name), load("multipole")
+    b = m[f"{name}_r{rule}_H0"]
+    S = btam.System(gpu_tables, system_of(g))
+    S.build_neighbors()
+    H = S.mf_hessian_multipole(rule)
+    assert np.abs(H - b).max() <= 1e-9 * max(1.0, np.abs(b).max())
+    assert np.array_equal(H, np.transpose(H, (0, 2, 1)))
+
+
 def test_multipole_rejects_unknown_rule(gpu_tables):
     g = load("sphere")
     S = btam.System(gpu_tables, system_of(g))
@@ -85,6 +99,8 @@ def test_multipole_rejects_unknown_rule(gpu_tables):
             S.mf_residuals_multipole(rule)
         with pytest.raises(btam.BtamError):
             S.mf_stress_multipole(rule)
+        with pytest.raises(btam.BtamError):
+            S.mf_hessian_multipole(rule)
 
 
 def test_multipole_full_size_translation_invariance(gpu_tables):

@@ -214,6 +214,23 @@ def test_multipole_rule_against_golden(oracle, name, rule):
         oracle.set_rule(0)
     b = m[key + "W0"]
     assert np.abs(W0 - b).max() <= (0 if rule == 1 else 1e-13) * max(1.0, np.abs(b).max())
+    # Hessian blocks, summed over i in {u} U N(u) as the fixture sums them
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import residual_pairs
+    plan = residual_pairs(full, owner, image, offs, idx, real)
+    kk = np.array([p_[0] for p_ in plan])
+    oracle.set_rule(rule)
+    try:
+        h9 = oracle.mf_D2V0_pairs(full, rho[owner], offs, idx,
+                                  np.array([p_[1] for p_ in plan], np.int32),
+                                  np.array([p_[2] for p_ in plan], np.int32))
+    finally:
+        oracle.set_rule(0)
+    H0 = np.zeros((n, 3, 3))
+    np.add.at(H0, kk, h9)
+    b = m[key + "H0"]
+    assert np.abs(H0 - b).max() <= 1e-12 * max(1.0, np.abs(b).max())
     if rule == 1:
         assert np.array_equal(rho, m[key + "rho"])
         assert np.array_equal(V0, m[key + "V0"])
