@@ -47,6 +47,8 @@ _V = ctypes.c_void_p
 _PROTOS = {
     "btam_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "btam_version": (ctypes.c_int, []),
+    "btam_pool_usage": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong),
+                                       ctypes.POINTER(ctypes.c_longlong)]),
     "btam_tables_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_V)]),
     "btam_tables_destroy": (None, [_V]),
     "btam_tables_mass": (ctypes.c_double, [_V, ctypes.c_int]),
@@ -82,6 +84,13 @@ _PROTOS = {
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_int, _D, _D]),
     "btam_mf_stress": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
+    "btam_mf_pair_terms": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, ctypes.c_longlong]),
+    "btam_mf_pair_terms_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D,
+                                                    ctypes.c_longlong]),
+    "btam_mf_hessian_pairs": (ctypes.c_int, [_V, _D, _D, ctypes.c_longlong]),
+    "btam_mf_hessian_pairs_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D, _D,
+                                                       ctypes.c_longlong]),
+    "btam_pt_pair_terms": (ctypes.c_int, [_V, _D, _D, _D, _D, ctypes.c_longlong]),
     "btam_mf_eval_profile": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_probe_fma_peak": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, _D]),
     "btam_probe_gather_peak": (ctypes.c_int, [_V, ctypes.c_double, _D]),
@@ -94,6 +103,12 @@ _PROTOS = {
     "btam_dmd_setup": (ctypes.c_int, [_V]),
     "btam_dmd_step": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D,
                                      ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_dmd_step_ctl": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D,
+                                         ctypes.POINTER(ctypes.c_longlong), _D]),
+    "btam_dmd_clip_count": (ctypes.c_int, [_V, ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_dmd_run": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_longlong), _D]),
     "btam_dmd_occupancy": (ctypes.c_int, [_V, _D, ctypes.POINTER(ctypes.c_longlong), _D]),
     "btam_dmd_graph_copy": (ctypes.c_int, [_V, _I, _I, ctypes.c_longlong]),
     "btam_batch_create": (ctypes.c_int, [ctypes.POINTER(_V), ctypes.c_int, ctypes.POINTER(_V)]),
@@ -198,6 +213,14 @@ def probe_fma_peak(fp64=False, seconds=0.5):
     _check(lib().btam_probe_fma_peak(int(fp64), float(seconds), _d(out)),
            "btam_probe_fma_peak")
     return float(out[0])
+
+
+def pool_usage():
+    """(used, reserved) bytes of the library's device-memory pool on the
+    current device."""
+    used, reserved = ctypes.c_longlong(0), ctypes.c_longlong(0)
+    _check(lib().btam_pool_usage(ctypes.byref(used), ctypes.byref(reserved)), "btam_pool_usage")
+    return used.value, reserved.value
 
 
 class Tables:
@@ -386,6 +409,40 @@ class System:
         hi, lo = tot[0], tot[1] & 0xFFFFFFFFFFFFFFFF
         return (hi << 64) + lo
 
+    def dmd_step_ctl(self, nsteps=1, precision=FP64, dt=4e-4, Df=0.045, dr=3.2, min_dx=1e-8,
+                     max_x=0.9, max_dx=0.05, max_sub=64):
+        """Master-equation steps with step control; returns (total quanta,
+        stats dict: substeps, subdivided, clipped, worst_ratio)."""
+        prm = np.array([dt, Df, dr, min_dx, max_x, max_dx, max_sub], np.float64)
+        tot = (ctypes.c_longlong * 2)()
+        st = np.zeros(4)
+        _check(lib().btam_dmd_step_ctl(self.handle, precision, nsteps, _d(prm), tot, _d(st)),
+               "btam_dmd_step_ctl")
+        hi, lo = tot[0], tot[1] & 0xFFFFFFFFFFFFFFFF
+        return (hi << 64) + lo, dict(substeps=int(st[0]), subdivided=int(st[1]),
+                                     clipped=int(st[2]), worst_ratio=float(st[3]))
+
+    def dmd_run(self, nsteps, precision=FP64, relax_every=0, relax_mode=0, relax_tol=1e-6,
+                relax_max_iter=200, dt=4e-4, Df=0.045, dr=3.2, min_dx=1e-8, max_x=0.9,
+                max_dx=0.05, max_sub=64):
+        """Controlled master-equation steps with a (q, sigma) relaxation every
+        relax_every steps; returns (total quanta, stats dict)."""
+        prm = np.array([dt, Df, dr, min_dx, max_x, max_dx, max_sub], np.float64)
+        tot = (ctypes.c_longlong * 2)()
+        st = np.zeros(6)
+        _check(lib().btam_dmd_run(self.handle, precision, nsteps, _d(prm), relax_every,
+                                  relax_mode, relax_tol, relax_max_iter, tot, _d(st)),
+               "btam_dmd_run")
+        hi, lo = tot[0], tot[1] & 0xFFFFFFFFFFFFFFFF
+        return (hi << 64) + lo, dict(substeps=int(st[0]), subdivided=int(st[1]),
+                                     clipped=int(st[2]), worst_ratio=float(st[3]),
+                                     relaxations=int(st[4]), relax_evaluations=int(st[5]))
+
+    def dmd_clip_count(self):
+        c = ctypes.c_longlong(0)
+        _check(lib().btam_dmd_clip_count(self.handle, ctypes.byref(c)), "btam_dmd_clip_count")
+        return c.value
+
     def dmd_occupancy(self):
         x = np.zeros(self.n)
         qn = np.zeros(self.n, np.int64)
@@ -519,6 +576,52 @@ class System:
         tot = np.zeros(9)
         _check(lib().btam_mf_stress(self.handle, precision, _d(W), _d(tot)), "btam_mf_stress")
         return W, tot.reshape(3, 3)
+
+    def pair_terms(self, precision=FP64):
+        """Unweighted per-pair terms of the residual assembly: (self (n, 5):
+        dV0_u/d(q_u, sigma_u, x_u); slot (entries, 5): dV0_j/d(q_u, sigma_u,
+        x_u) for every entry (u, j) of the real sites' neighbour lists)."""
+        offs, _ = self.neighbors()
+        n_slots = int(offs[self.n])
+        selfv = np.zeros((self.n, 5))
+        slot = np.zeros((max(n_slots, 1), 5))
+        _check(lib().btam_mf_pair_terms(self.handle, precision, _d(selfv), _d(slot), n_slots),
+               "btam_mf_pair_terms")
+        return selfv, slot[:n_slots]
+
+    def _n_slots(self):
+        offs, _ = self.neighbors()
+        return int(offs[self.n])
+
+    def pair_terms_multipole(self, rule=1):
+        """Per-pair terms under the multipole rule (as pair_terms)."""
+        ns = self._n_slots()
+        selfv, slot = np.zeros((self.n, 5)), np.zeros((max(ns, 1), 5))
+        _check(lib().btam_mf_pair_terms_multipole(self.handle, rule, _d(selfv), _d(slot), ns),
+               "btam_mf_pair_terms_multipole")
+        return selfv, slot[:ns]
+
+    def mf_hessian_pairs(self, rule=0):
+        """Per-pair mean-field Hessian blocks (rule 0: degree-3; 1, 2: the
+        multipole rule): (Hself (n, 3, 3), Hslot (entries, 3, 3))."""
+        ns = self._n_slots()
+        Hs, Hp = np.zeros((self.n, 3, 3)), np.zeros((max(ns, 1), 3, 3))
+        if rule:
+            code = lib().btam_mf_hessian_pairs_multipole(self.handle, rule, _d(Hs), _d(Hp), ns)
+        else:
+            code = lib().btam_mf_hessian_pairs(self.handle, _d(Hs), _d(Hp), ns)
+        _check(code, "btam_mf_hessian_pairs")
+        return Hs, Hp[:ns]
+
+    def pt_pair_terms(self):
+        """Per-pair non-mean-field terms: (self3 (n, 3), slot3 (entries, 3),
+        Hself (n, 3, 3), Hslot (entries, 3, 3))."""
+        ns = self._n_slots()
+        g, gp = np.zeros((self.n, 3)), np.zeros((max(ns, 1), 3))
+        Hs, Hp = np.zeros((self.n, 3, 3)), np.zeros((max(ns, 1), 3, 3))
+        _check(lib().btam_pt_pair_terms(self.handle, _d(g), _d(gp), _d(Hs), _d(Hp), ns),
+               "btam_pt_pair_terms")
+        return g, gp[:ns], Hs, Hp[:ns]
 
     def relax_stretch_mf(self, precision=FP64, atol=1e-12, rtol=1e-10, max_iter=20,
                          F0=(1.0, 1.0, 1.0)):

@@ -71,10 +71,24 @@ template <class R> struct TablesView {
 
 template <class R> BTAM_HD R rmin(R a, R b) { return a < b ? a : b; }
 
+// Segment index m = min(int(x / dx), n - 1) (cubic-spline.cpp:89-90).  In
+// FP64 the index is the reference's: x times 1/dx truncates to the same
+// integer as the rounded quotient unless it lies within 1e-9 of a knot, and
+// there the quotient itself is taken, so a point on a knot picks the
+// reference's segment.  The FP32 form takes the product.
+template <class R> BTAM_HD int seg_index(R x, R dx, R inv_dx, int n) {
+  const R t = x * inv_dx;
+  int m = (int)t;
+  if (sizeof(R) == 8) {
+    const R f = t - (R)m;
+    if (f < (R)1e-9 || f > (R)1 - (R)1e-9) m = (int)(x / dx);
+  }
+  return m < n - 1 ? m : n - 1;
+}
+
 template <class R>
 BTAM_HD void spline_vd(const SplineView<R> &s, R r, R &v, R &dv) {
-  int m = (int)(r * s.inv_dx);
-  m = m < s.n - 1 ? m : s.n - 1;
+  const int m = seg_index<R>(r, s.dx, s.inv_dx, s.n);
   R p = rmin(r - (R)m * s.dx, s.dx);
 #if defined(__CUDA_ARCH__)
   Coef4<R> k;
@@ -142,8 +156,7 @@ BTAM_HD int rho_off(int pk, int c) { return (pk == 2 && c == 1) ? 8 : 4; }
 // Segment of |r| = s (cubic-spline.cpp:84-96): m = min(floor(s/dx), n-1),
 // p = min(s - m dx, dx).
 template <class R> BTAM_HD int seg_of(const RadialView<R> &T, R s, R &p) {
-  int m = (int)(s * T.inv_dx);
-  m = m < T.n - 1 ? m : T.n - 1;
+  const int m = seg_index<R>(s, T.dx, T.inv_dx, T.n);
   p = rmin(s - (R)m * T.dx, T.dx);
   return m;
 }
@@ -755,11 +768,20 @@ template <class R, bool RO> struct MomRec {
   }
 };
 
+// The two parts of pair (u, j), unweighted: self = the terms of
+// dV0_u/d(q_u, sigma_u) that pair j carries, cros = dV0_j/d(q_u, sigma_u,
+// x_u), the reference's evaluate_DV0_i_Dq_u(u, j) and
+// evaluate_DV0_i_Dxi_u(u, j) (MgHx-mf-V-bulk.cpp:1823-2098, 2102-2325).
+template <class R> struct Pass2Parts {
+  R self_q[3], self_s;
+  R cros_q[3], cros_s, cros_x;
+};
+
 template <class R, class MU, class MJ>
-BTAM_HD void pass2_pair(const RadialView<R> &T, const V3<R> &r0, R sig_u,
-                        R sig_j, R xu, R xj, int cu, int cj, R embq_u,
-                        R embq_j, R embx_j, R omega, const MU &mu,
-                        const MJ &mj, Pass2Out<R> &o) {
+BTAM_HD void pass2_pair_parts(const RadialView<R> &T, const V3<R> &r0, R sig_u,
+                              R sig_j, R xu, R xj, int cu, int cj, R embq_u,
+                              R embq_j, R embx_j, const MU &mu, const MJ &mj,
+                              Pass2Parts<R> &P) {
   const int pk = pair_kind(cu, cj);
   const R X = xu * xj;
   const R w6 = (R)kW6, w9 = (R)kW9;
@@ -894,9 +916,27 @@ BTAM_HD void pass2_pair(const RadialView<R> &T, const V3<R> &r0, R sig_u,
     cros_x += (R)2 * w9 * xj * dual_f(dual_flip(Dj_h), gc);
   }
 
-  for (int k = 0; k < 3; ++k) o.gq[k] += self_q[k] + omega * cros_q[k];
-  o.gs += self_s + omega * cros_s;
-  o.gx += omega * cros_x;
+  for (int k = 0; k < 3; ++k) {
+    P.self_q[k] = self_q[k];
+    P.cros_q[k] = cros_q[k];
+  }
+  P.self_s = self_s;
+  P.cros_s = cros_s;
+  P.cros_x = cros_x;
+}
+
+// Both parts of pair (u, j) weighted into u's residual: self + omega cros,
+// omega = beta_j / beta_u.
+template <class R, class MU, class MJ>
+BTAM_HD void pass2_pair(const RadialView<R> &T, const V3<R> &r0, R sig_u,
+                        R sig_j, R xu, R xj, int cu, int cj, R embq_u,
+                        R embq_j, R embx_j, R omega, const MU &mu,
+                        const MJ &mj, Pass2Out<R> &o) {
+  Pass2Parts<R> P;
+  pass2_pair_parts(T, r0, sig_u, sig_j, xu, xj, cu, cj, embq_u, embq_j, embx_j, mu, mj, P);
+  for (int k = 0; k < 3; ++k) o.gq[k] += P.self_q[k] + omega * P.cros_q[k];
+  o.gs += P.self_s + omega * P.cros_s;
+  o.gx += omega * P.cros_x;
 }
 
 // ---------------------------------------------------------------------------

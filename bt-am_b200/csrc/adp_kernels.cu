@@ -190,8 +190,14 @@ __device__ __forceinline__ bool mbar_wait0(unsigned bar) {
   return false;
 }
 
+// `ok` is false (the same in every thread of the block) when the staging copy
+// did not complete within two bounded waits: the timeout bit is then set and
+// the block must return without touching the table; nothing recovers the
+// evaluation, whose call reports BTAM_ERR_TIMEOUT.
 template <class R, bool SM>
-__device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArgs<R> &a) {
+__device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArgs<R> &a,
+                                                                   bool &ok) {
+  ok = true;
   if constexpr (SM && sizeof(R) == 4) {
     // dynamic shared memory: the table (a multiple of 32 bytes), then an
     // 8-byte mbarrier; the kernels that stage it hold no static shared memory
@@ -223,14 +229,15 @@ __device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArg
         (void)state;
       }
       staged = __syncthreads_and(mbar_wait0(bar)) != 0;
-      if (!staged) {  // the copy did not complete in time: flag it, wait
-                      // once more, then copy with the threads
+      if (!staged) {  // the copy did not complete in time: flag it and wait
+                      // once more; the threads never write over a copy that
+                      // may still be in flight
         if (threadIdx.x == 0) atomicOr(a.err, 1 << kErrBitTimeout);
-        mbar_wait0(bar);
-        __syncthreads();
+        staged = __syncthreads_and(mbar_wait0(bar)) != 0;
+        if (!staged) ok = false;
       }
     }
-    if (!staged) {
+    if (!staged && ok) {
       // 16-byte halves c of record c / 2, stored swapped where uw_swapped says
       for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x) {
         const int dst = uw_swapped(c >> 1) ? (c ^ 1) : c;
@@ -584,6 +591,77 @@ mf_stress_kernel(const EvalArgs<R> a, double *W0) {
   }
 }
 
+// Per-pair terms of the residual assembly, unweighted (the reference's
+// per-pair functions): a warp per real site u, a lane per slot p of u's
+// list (neighbour j).  self[5u..5u+4] = dV0_u/d(q_u, sigma_u, x_u): the sum
+// over u's pairs of their self parts, and dV0_u/dx_u from pass 1;
+// slot[5p..5p+4] = dV0_j/d(q_u, sigma_u, x_u), the pair's cross part.  Zero
+// for an empty u or j.  Reads the moment records of a directed pass 1.
+template <class R, int W>
+__global__ void __launch_bounds__(W * 32)
+mf_pair_terms_kernel(const EvalArgs<R> a, double *self, double *slot) {
+  __shared__ R mu_s[W][kMomStride];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
+  const double2 xbu = a.xb[u];
+  const double xu = xbu.x;
+  const int nb0 = a.offs[u], nb1 = a.offs[u + 1];
+  if (xu < kMinOcc) {
+    for (int p = nb0 + lane; p < nb1; p += 32)
+      for (int c = 0; c < 5; ++c) slot[5 * (size_t)p + c] = 0.0;
+    if (lane < 5) self[5 * (size_t)u + lane] = 0.0;
+    continue;
+  }
+  const R *mu_g = a.mom + (size_t)u * kMomStride;
+  for (int c = lane; c < kMomStride; c += 32) mu_s[warp][c] = mu_g[c];
+  __syncwarp();
+  const MomRec<R, false> mu(mu_s[warp]);
+  const double4 qu = a.pos[u];
+  const int cu = a.code[u];
+  Acc<R> acc[4];
+  bool ok = true;
+  for (int p = nb0 + lane; p < nb1; p += 32) {
+    const int j = a.idx[p];
+    const double2 xbj = a.xb[j];
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (!(xbj.x < kMinOcc)) {
+      const int o = a.owner[j];
+      const double4 qj = a.pos[j];
+      const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
+      Pass2Parts<R> P;
+      pass2_pair_parts<R>(a.T, pair_vec<R>(qu, qj), (R)qu.w, (R)qj.w, (R)xu, (R)xbj.x, cu,
+                          a.code[j], mu.scalar(0), mj.scalar(0), mj.scalar(1), mu, mj, P);
+      acc[0].add(P.self_q[0]);
+      acc[1].add(P.self_q[1]);
+      acc[2].add(P.self_q[2]);
+      acc[3].add(P.self_s);
+      v[0] = P.cros_q[0];
+      v[1] = P.cros_q[1];
+      v[2] = P.cros_q[2];
+      v[3] = P.cros_s;
+      v[4] = P.cros_x;
+    }
+    for (int c = 0; c < 5; ++c) {
+      slot[5 * (size_t)p + c] = v[c];
+      ok = ok && finite(v[c]);
+    }
+  }
+  double t[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) t[c] = warp_sum(acc[c].get());
+  if (lane == 0) {
+    for (int c = 0; c < 4; ++c) {
+      self[5 * (size_t)u + c] = t[c];
+      ok = ok && finite(t[c]);
+    }
+    self[5 * (size_t)u + 4] = a.selfx[u];
+  }
+  if (__any_sync(0xffffffffu, !ok) && lane == 0) atomicOr(a.err, 1 << kErrBitNonFinite);
+  __syncwarp();  // mu_s is reloaded for the warp's next site
+  }
+}
+
 // One owned slot p = (u, j): both directions of the pair from its 25
 // geometries (pass2_pair_sym); u's part into slot p, j's part into the
 // reverse slot.  Pairs with an empty site give zero records, so every slot
@@ -651,7 +729,9 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
 template <int TPB>
 __global__ void __launch_bounds__(TPB, 1)
 pass2u_pair_smem_kernel(const EvalArgs<float> a) {
-  const auto T = kernel_view<float, true>(a);
+  bool ok;
+  const auto T = kernel_view<float, true>(a, ok);
+  if (!ok) return;  // the staging copy timed out (flagged)
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
     pass2u_one(a, T, t);
@@ -920,6 +1000,17 @@ cudaError_t launch_mf_stress(const EvalArgs<R> &a, double *W0, cudaStream_t st) 
     mf_stress_kernel<R, 4><<<nblocks(a.n_real, 4), 128, 0, st>>>(a, W0);
   return cudaGetLastError();
 }
+template <class R>
+cudaError_t launch_mf_pair_terms(const EvalArgs<R> &a, double *self, double *slot,
+                                 cudaStream_t st) {
+  if (a.n_real > 0)
+    mf_pair_terms_kernel<R, 4><<<nblocks(a.n_real, 4), 128, 0, st>>>(a, self, slot);
+  return cudaGetLastError();
+}
+template cudaError_t launch_mf_pair_terms<double>(const EvalArgs<double> &, double *, double *,
+                                                  cudaStream_t);
+template cudaError_t launch_mf_pair_terms<float>(const EvalArgs<float> &, double *, double *,
+                                                 cudaStream_t);
 template cudaError_t launch_mf_stress<double>(const EvalArgs<double> &, double *, cudaStream_t);
 template cudaError_t launch_mf_stress<float>(const EvalArgs<float> &, double *, cudaStream_t);
 

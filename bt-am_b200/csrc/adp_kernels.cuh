@@ -139,6 +139,12 @@ cudaError_t launch_seg_totals(int n_sys, const int *seg, const double *V0, const
 // records of a directed pass 1 (launch_pass1 with variants 0, 0).
 template <class R>
 cudaError_t launch_mf_stress(const EvalArgs<R> &a, double *W0, cudaStream_t st);
+// Unweighted per-pair terms of the residual assembly from the moment records
+// of a directed pass 1: self (5 per real site) = dV0_u/d(q_u, sigma_u, x_u),
+// slot (5 per slot of the real sites' lists) = dV0_j/d(q_u, sigma_u, x_u).
+template <class R>
+cudaError_t launch_mf_pair_terms(const EvalArgs<R> &a, double *self, double *slot,
+                                 cudaStream_t st);
 cudaError_t launch_rho_nmf(int n_real, const double4 *pos, const double2 *xb,
                            const int *code, const int *offs, const int *idx,
                            SplineView<double> rho_mg, SplineView<double> rho_h,

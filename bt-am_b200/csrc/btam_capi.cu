@@ -6,6 +6,7 @@
 // topo_kernels.cu on the current device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -367,6 +368,18 @@ const char *btam_status_string(int st) {
 }
 
 int btam_version(void) { return 100; }
+
+int btam_pool_usage(long long *used, long long *reserved) {
+  if (!used || !reserved) return BTAM_ERR_ARG;
+  cudaMemPool_t pool = btam::device_pool();
+  if (!pool) return BTAM_ERR_CUDA;
+  unsigned long long u = 0, r = 0;
+  BTAM_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &u));
+  BTAM_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &r));
+  *used = (long long)u;
+  *reserved = (long long)r;
+  return BTAM_OK;
+}
 
 int btam_tables_load(const char *dir, btam_tables **out) {
   if (!dir || !out) return BTAM_ERR_ARG;
@@ -1126,6 +1139,44 @@ int btam_mf_stress(btam_system *s, int precision, double *W0, double *total) {
   return read_err(s);
 }
 
+int btam_mf_pair_terms(btam_system *s, int precision, double *self, double *slot,
+                       long long slot_cap) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  int n_slots = 0;
+  BTAM_TRY(copy_sync(&n_slots, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  if (slot && slot_cap < n_slots) return BTAM_ERR_ARG;
+  double *d_self = nullptr, *d_slot = nullptr;
+  BTAM_TRY(dalloc(d_self, s->st, 5 * (size_t)s->n_real));
+  cudaError_t e = dalloc(d_slot, s->st, 5 * (size_t)n_slots);
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  // the directed pass 1 writes the moment records and dV0_u/dx_u
+  if (e == cudaSuccess) {
+    if (precision == BTAM_FP64) {
+      if (!s->mom64) e = dalloc(s->mom64, s->st, nm);
+      EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
+      if (e == cudaSuccess) e = launch_pass1(a, s->st, 0, 0);
+      if (e == cudaSuccess) e = launch_mf_pair_terms(a, d_self, d_slot, s->st);
+    } else {
+      if (!s->mom32) e = dalloc(s->mom32, s->st, nm);
+      EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
+      if (e == cudaSuccess) e = launch_pass1(a, s->st, 0, 0);
+      if (e == cudaSuccess) e = launch_mf_pair_terms(a, d_self, d_slot, s->st);
+    }
+  }
+  if (e == cudaSuccess && self)
+    e = cudaMemcpyAsync(self, d_self, 5 * (size_t)s->n_real * sizeof(double),
+                        cudaMemcpyDeviceToHost, s->st);
+  if (e == cudaSuccess && slot)
+    e = cudaMemcpyAsync(slot, d_slot, 5 * (size_t)n_slots * sizeof(double),
+                        cudaMemcpyDeviceToHost, s->st);
+  dfree(d_self, s->st);
+  dfree(d_slot, s->st);
+  if (e != cudaSuccess) return cuda_status(e);
+  return read_err(s);
+}
+
 int btam_rho_nmf(btam_system *s, double *rho) {
   if (!s || !rho) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
@@ -1489,6 +1540,8 @@ int btam_dmd_setup(btam_system *s) {
   for (long long **p : {&s->X, &s->X0})
     BTAM_TRY(dalloc(*p, s->st, n));
   BTAM_TRY(dalloc(s->dtot, s->st, 2));
+  BTAM_TRY(dalloc(s->dctl, s->st, 3));
+  BTAM_TRY(cudaMemsetAsync(s->dctl, 0, 3 * sizeof(unsigned long long), s->st));
   BTAM_TRY(dalloc(s->mu, s->st, n));
   BTAM_TRY(dalloc(s->dact, s->st, n));
   BTAM_TRY(dalloc(s->ddeg, s->st, n));
@@ -1502,19 +1555,22 @@ int btam_dmd_setup(btam_system *s) {
   return BTAM_OK;
 }
 
-int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *params,
-                  long long *total_quanta) {
-  if (!s || nsteps < 0) return BTAM_ERR_ARG;
-  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
-  DmdParams prm;
-  // defaults: the reference's diffusion parameters (Variables.hpp:68-92)
+}  // extern "C"
+
+namespace {
+
+// The reference's diffusion parameters (Variables.hpp:68-92) unless given.
+int dmd_params(const double *params, DmdParams &prm) {
   prm.dt = params ? params[0] : 4e-4;
   prm.Df = params ? params[1] : 0.045;
   prm.dr = params ? params[2] : 3.2;
   prm.min_dx = params ? params[3] : 1e-8;
   prm.max_x = params ? params[4] : 0.9;
-  if (!(prm.dt >= 0.0 && prm.Df >= 0.0 && prm.dr > 0.0 && prm.max_x > 0.0)) return BTAM_ERR_ARG;
-  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  return (prm.dt >= 0.0 && prm.Df >= 0.0 && prm.dr > 0.0 && prm.max_x > 0.0) ? BTAM_OK
+                                                                              : BTAM_ERR_ARG;
+}
+
+DmdArgs dmd_args(btam_system *s) {
   DmdArgs a;
   a.n = s->n_real;
   a.xb = s->xb;
@@ -1531,20 +1587,139 @@ int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *param
   a.mu = s->mu;
   a.active = s->dact;
   a.deg = s->ddeg;
-  for (int k = 0; k < nsteps; ++k) {
-    int st = btam_mf_eval_async(s, precision);  // chemical potentials at the current x
-    if (st != BTAM_OK) return st;
-    BTAM_TRY(dmd_step(a, prm, s->st));
-    if (s->n_ghost > 0)
-      BTAM_TRY(launch_ghost_refresh(s->n_real, s->n_ghost, s->pos, s->xb, s->code, s->owner,
-                                    s->image, s->box, s->st));
-  }
+  a.ctl = s->dctl;
+  return a;
+}
+
+// Images follow their owners' new occupancies.
+int dmd_refresh_images(btam_system *s) {
+  if (s->n_ghost > 0)
+    BTAM_TRY(launch_ghost_refresh(s->n_real, s->n_ghost, s->pos, s->xb, s->code, s->owner,
+                                  s->image, s->box, s->st));
+  return BTAM_OK;
+}
+
+int dmd_finish(btam_system *s, long long *total_quanta) {
   if (total_quanta) {
     BTAM_TRY(dmd_total(s->n_real, s->code, s->X, s->dtot, s->st));
     BTAM_TRY(cudaMemcpyAsync(total_quanta, s->dtot, 2 * sizeof(long long), cudaMemcpyDeviceToHost,
                              s->st));
   }
   return read_err(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *params,
+                  long long *total_quanta) {
+  if (!s || nsteps < 0) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  DmdParams prm;
+  if (dmd_params(params, prm) != BTAM_OK) return BTAM_ERR_ARG;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  const DmdArgs a = dmd_args(s);
+  for (int k = 0; k < nsteps; ++k) {
+    int st = btam_mf_eval_async(s, precision);  // chemical potentials at the current x
+    if (st != BTAM_OK) return st;
+    BTAM_TRY(dmd_step(a, prm, s->st));
+    if ((st = dmd_refresh_images(s)) != BTAM_OK) return st;
+  }
+  return dmd_finish(s, total_quanta);
+}
+
+int btam_dmd_step_ctl(btam_system *s, int precision, int nsteps, const double *params,
+                      long long *total_quanta, double *stats) {
+  if (!s || nsteps < 0) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  DmdParams prm;
+  if (dmd_params(params, prm) != BTAM_OK) return BTAM_ERR_ARG;
+  const double max_dx = params ? params[5] : 0.05;
+  const double max_sub_d = params ? params[6] : 64.0;
+  if (!(max_dx > 0.0) || !(max_sub_d >= 1.0 && max_sub_d <= 1e6)) return BTAM_ERR_ARG;
+  const long long max_sub = (long long)max_sub_d;
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  const DmdArgs a = dmd_args(s);
+  unsigned long long clip0 = 0;
+  BTAM_TRY(copy_sync(&clip0, s->dctl + 2, sizeof(clip0), cudaMemcpyDeviceToHost, s->st));
+  long long subs = 0, split = 0;
+  double worst = 0.0;
+  for (int k = 0; k < nsteps; ++k) {
+    int st = btam_mf_eval_async(s, precision);
+    if (st != BTAM_OK) return st;
+    BTAM_TRY(dmd_prepare(a, s->st));
+    BTAM_TRY(dmd_control(a, prm, max_dx, s->st));
+    unsigned long long bits[2] = {0, 0};
+    BTAM_TRY(copy_sync(bits, s->dctl, sizeof(bits), cudaMemcpyDeviceToHost, s->st));
+    double r[2];
+    std::memcpy(r, bits, sizeof(r));
+    const double need = std::max(r[0], r[1]);
+    if (!std::isfinite(need)) return BTAM_ERR_NONFINITE;
+    worst = std::max(worst, need);
+    const long long m = std::min(max_sub, std::max(1ll, (long long)std::ceil(need)));
+    DmdParams sub = prm;
+    sub.dt = prm.dt / (double)m;
+    for (long long j = 0; j < m; ++j) {
+      if (j > 0) {  // fresh chemical potentials for every later sub-step
+        if ((st = btam_mf_eval_async(s, precision)) != BTAM_OK) return st;
+        BTAM_TRY(dmd_prepare(a, s->st));
+      }
+      BTAM_TRY(dmd_apply(a, sub, s->st));
+      if ((st = dmd_refresh_images(s)) != BTAM_OK) return st;
+    }
+    subs += m;
+    split += m > 1;
+  }
+  int st = dmd_finish(s, total_quanta);
+  if (stats) {
+    unsigned long long clip1 = 0;
+    BTAM_TRY(copy_sync(&clip1, s->dctl + 2, sizeof(clip1), cudaMemcpyDeviceToHost, s->st));
+    stats[0] = (double)subs;
+    stats[1] = (double)split;
+    stats[2] = (double)(clip1 - clip0);
+    stats[3] = worst;
+  }
+  return st;
+}
+
+int btam_dmd_run(btam_system *s, int precision, int nsteps, const double *params,
+                 int relax_every, int relax_mode, double relax_tol, int relax_max_iter,
+                 long long *total_quanta, double *stats) {
+  if (!s || nsteps < 0 || relax_every < 0) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  double acc[6] = {0, 0, 0, 0, 0, 0};
+  int done = 0;
+  while (done < nsteps) {
+    const int k = relax_every > 0 ? std::min(relax_every, nsteps - done) : nsteps - done;
+    double st4[4] = {0, 0, 0, 0};
+    int st = btam_dmd_step_ctl(s, precision, k, params, nullptr, st4);
+    if (st != BTAM_OK) return st;
+    for (int c = 0; c < 3; ++c) acc[c] += st4[c];
+    acc[3] = std::max(acc[3], st4[3]);
+    done += k;
+    if (relax_every > 0 && done % relax_every == 0) {
+      // the mechanical state follows the new occupancies
+      double info[5] = {0, 0, 0, 0, 0};
+      st = btam_relax(s, relax_mode, relax_tol, relax_max_iter, 8, nullptr, info);
+      if (st != BTAM_OK) return st;
+      acc[4] += 1.0;
+      acc[5] += info[2];
+    }
+  }
+  if (stats)
+    for (int c = 0; c < 6; ++c) stats[c] = acc[c];
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  return dmd_finish(s, total_quanta);
+}
+
+int btam_dmd_clip_count(btam_system *s, long long *clipped) {
+  if (!s || !clipped) return BTAM_ERR_ARG;
+  if (!s->dmd_ready) return BTAM_ERR_NOT_BUILT;
+  unsigned long long c = 0;
+  BTAM_TRY(copy_sync(&c, s->dctl + 2, sizeof(c), cudaMemcpyDeviceToHost, s->st));
+  *clipped = (long long)c;
+  return BTAM_OK;
 }
 
 int btam_dmd_occupancy(btam_system *s, double *x, long long *quanta, double *mu) {

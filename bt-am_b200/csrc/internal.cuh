@@ -75,6 +75,7 @@ struct btam_system {
   int *doffs = nullptr, *didx = nullptr, dq_cap = 0;
   long long didx_cap = 0, d_pairs = 0;
   long long *X = nullptr, *X0 = nullptr, *dtot = nullptr;
+  unsigned long long *dctl = nullptr;  // step-control maxima and clip count (DmdArgs::ctl)
   double *mu = nullptr;
   int *dact = nullptr, *ddeg = nullptr;
   // relaxation work vectors
@@ -104,11 +105,13 @@ cudaError_t launch_pt_totals(int n, const double *V, const double *Fq, const dou
 int mf_rho64_enqueue(btam_system *s);
 
 // Enqueues the mean-field Hessian blocks of the current state into Hd (9
-// per real site) (mf_hessian.cu).
-int mf_hessian_enqueue(btam_system *s, double *Hd);
+// per real site); with Hslot (9 per entry of the real sites' lists), Hd
+// holds the i = u blocks and Hslot the per-neighbour ones (mf_hessian.cu).
+int mf_hessian_enqueue(btam_system *s, double *Hd, double *Hslot);
 // The same blocks on a given rho-bar and, if gmp is set, per-list-entry
 // rho gradients (3 per entry of a real site) instead of the degree-3 ones.
-int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp, double *Hd);
+int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp, double *Hd,
+                            double *Hslot);
 
 // Enqueues the directed pass 1 and the mean-field stress of the current
 // state; *W: per-site stress (9 n), *tot: totals whose [2..10] hold the sum

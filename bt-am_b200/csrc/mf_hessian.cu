@@ -178,6 +178,10 @@ struct MfhArgs {
   RadialView<double> T;
   SplineView<double> emb_mg, emb_h;
   double *H;
+  // null: H sums over i in {u} U N(u); else H holds the i = u block only and
+  // Hslot (9 per entry p of the real sites' lists) the block of neighbour
+  // idx[p]: the reference's per-pair values
+  double *Hslot = nullptr;
 };
 
 __device__ __forceinline__ bool skipped(const MfhArgs &a, int j) {
@@ -244,8 +248,7 @@ __device__ void triplet_terms(const MfhArgs &a, const double *r1_0, const double
 
 __device__ __forceinline__ void emb_dd(const SplineView<double> &E, double rho, double &d1,
                                        double &d2) {
-  int m = (int)(rho * E.inv_dx);
-  m = m < E.n - 1 ? m : E.n - 1;
+  const int m = seg_index(rho, E.dx, E.inv_dx, E.n);
   const double p = fmin(rho - (double)m * E.dx, E.dx);
   const double k[4] = {E.c[m].a, E.c[m].b, E.c[m].c, E.c[m].d};
   double v;
@@ -264,6 +267,9 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
   double gsum[3] = {0, 0, 0}, d2s[6] = {0, 0, 0, 0, 0, 0};
   double hn[6] = {0, 0, 0, 0, 0, 0};       // i = neighbours: everything
   const int nb0 = a.offs[u], nb1 = a.offs[u + 1];
+  if (a.Hslot)
+    for (int k1 = nb0 + lane; k1 < nb1; k1 += 32)
+      for (int c = 0; c < 9; ++c) a.Hslot[9 * (size_t)k1 + c] = 0.0;
   if (live) {
     for (int k1 = nb0 + lane; k1 < nb1; k1 += 32) {
       const int j1 = a.idx[k1];
@@ -322,6 +328,15 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
       }
       double dF, ddF;
       emb_dd(c1 == 0 ? a.emb_mg : a.emb_h, a.rho[o], dF, ddF);
+      if (a.Hslot) {
+        for (int x = 0; x < 3; ++x)
+          for (int y = 0; y < 3; ++y) {
+            const int c = s6(x < y ? x : y, x < y ? y : x);
+            a.Hslot[9 * (size_t)k1 + 3 * x + y] =
+                hi[c] + x1 * ddF * gi[x] * gi[y] + x1 * dF * d2i[c];
+          }
+        continue;
+      }
       for (int x = 0; x < 3; ++x)
         for (int y = x; y < 3; ++y)
           hn[s6(x, y)] += hi[s6(x, y)] + x1 * ddF * gi[x] * gi[y] + x1 * dF * d2i[s6(x, y)];
@@ -352,13 +367,14 @@ __global__ void __launch_bounds__(128) mf_hess_kernel(MfhArgs a) {
 }  // namespace
 }  // namespace btam
 
-int mf_hessian_enqueue(btam_system *s, double *Hd) {
+int mf_hessian_enqueue(btam_system *s, double *Hd, double *Hslot) {
   int st = mf_rho64_enqueue(s);  // rho-bar of the real sites into the system's rho
   if (st != BTAM_OK) return st;
-  return mf_hessian_enqueue_with(s, s->rho, nullptr, Hd);
+  return mf_hessian_enqueue_with(s, s->rho, nullptr, Hd, Hslot);
 }
 
-int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp, double *Hd) {
+int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp, double *Hd,
+                            double *Hslot) {
   MfhArgs a;
   a.n_real = s->n_real;
   a.pos = s->pos;
@@ -373,6 +389,7 @@ int mf_hessian_enqueue_with(btam_system *s, const double *rho, const double *gmp
   a.emb_mg = s->T->v64.t[T_F_MG];
   a.emb_h = s->T->v64.t[T_F_H];
   a.H = Hd;
+  a.Hslot = Hslot;
   const int g = (int)(((long long)s->n_real * 32 + 127) / 128);
   if (g > 0) mf_hess_kernel<<<g, 128, 0, s->st>>>(a);
   return cuda_status(cudaGetLastError());
@@ -385,7 +402,7 @@ int btam_mf_hessian(btam_system *s, double *H) {
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   double *Hd = nullptr;
   BTAM_TRY(dalloc(Hd, s->st, 9 * (size_t)s->n_real));
-  int st = mf_hessian_enqueue(s, Hd);
+  int st = mf_hessian_enqueue(s, Hd, nullptr);
   if (st != BTAM_OK) {
     dfree(Hd, s->st);
     return st;
@@ -394,6 +411,28 @@ int btam_mf_hessian(btam_system *s, double *H) {
                                         cudaMemcpyDeviceToHost, s->st);
   dfree(Hd, s->st);
   if (e != cudaSuccess) return cuda_status(e);
+  return read_err(s);
+}
+
+int btam_mf_hessian_pairs(btam_system *s, double *Hself, double *Hslot, long long slot_cap) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  int n_slots = 0;
+  BTAM_TRY(copy_sync(&n_slots, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  if (Hslot && slot_cap < n_slots) return BTAM_ERR_ARG;
+  double *Hd = nullptr, *Hs = nullptr;
+  BTAM_TRY(dalloc(Hd, s->st, 9 * (size_t)s->n_real));
+  cudaError_t e = dalloc(Hs, s->st, 9 * (size_t)n_slots);
+  int st = e == cudaSuccess ? mf_hessian_enqueue(s, Hd, Hs) : cuda_status(e);
+  if (st == BTAM_OK && Hself)
+    st = cuda_status(cudaMemcpyAsync(Hself, Hd, 9 * (size_t)s->n_real * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s->st));
+  if (st == BTAM_OK && Hslot)
+    st = cuda_status(cudaMemcpyAsync(Hslot, Hs, 9 * (size_t)n_slots * sizeof(double),
+                                     cudaMemcpyDeviceToHost, s->st));
+  dfree(Hd, s->st);
+  dfree(Hs, s->st);
+  if (st != BTAM_OK) return st;
   return read_err(s);
 }
 

@@ -1139,9 +1139,18 @@ int btam_mf_eval_multipole(btam_system *s, int rule, double *rho, double *V0, do
   return read_err(s);
 }
 
-int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs, double *Rx) {
-  if (!s || !Rq || !Rs || !Rx || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC))
-    return BTAM_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// The multipole residuals (Rq, Rs, Rx; any may be null) and, when self5 or
+// slot5 is given, their unweighted per-pair terms split out of the pairs
+// kernel's buffer (per real site u: entry 0 the pair (u, u), entries 1.. its
+// list entries in order): self5 (5 per real site), slot5 (5 per list entry;
+// slot_cap entries at least).
+int mp_residuals(btam_system *s, int rule, double *Rq, double *Rs, double *Rx, double *self5,
+                 double *slot5, long long slot_cap) {
+  if (!s || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC)) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   const size_t n = (size_t)s->n_real;
   if (n == 0) return BTAM_OK;
@@ -1150,6 +1159,7 @@ int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs
                                   cudaMemcpyDeviceToHost, s->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) return cuda_status(e);
+  if (slot5 && slot_cap < offs_n[0]) return BTAM_ERR_ARG;
   const long long total = (long long)offs_n[0] + (long long)n;
   double *rd = nullptr, *g5 = nullptr, *out = nullptr;
   BTAM_TRY(dalloc(rd, s->st, n));
@@ -1190,18 +1200,53 @@ int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs
   mp_pairs_kernel<<<(unsigned)gp, 128, 0, s->st>>>(r, total);
   mp_assemble_kernel<<<(int)((n + 127) / 128), 128, 0, s->st>>>(r);
   e = cudaGetLastError();
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && Rq)
     e = cudaMemcpyAsync(Rq, out, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && Rs)
     e = cudaMemcpyAsync(Rs, out + 3 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
-  if (e == cudaSuccess)
+  if (e == cudaSuccess && Rx)
     e = cudaMemcpyAsync(Rx, out + 4 * n, n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+  std::vector<double> g5h, offsh;
+  std::vector<int> offs_h;
+  if (e == cudaSuccess && (self5 || slot5)) {
+    g5h.resize(5 * (size_t)total);
+    offs_h.resize(n + 1);
+    e = cudaMemcpyAsync(g5h.data(), g5, g5h.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                        s->st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(offs_h.data(), s->offs, (n + 1) * sizeof(int), cudaMemcpyDeviceToHost,
+                          s->st);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e == cudaSuccess && (self5 || slot5)) {
+    for (size_t u = 0; u < n; ++u) {
+      const double *g = g5h.data() + 5 * ((size_t)offs_h[u] + u);
+      if (self5)
+        for (int c = 0; c < 5; ++c) self5[5 * u + c] = g[c];
+      if (slot5)
+        for (int p = offs_h[u]; p < offs_h[u + 1]; ++p)
+          for (int c = 0; c < 5; ++c) slot5[5 * (size_t)p + c] = g[5 * (1 + p - offs_h[u]) + c];
+    }
+  }
   dfree(rd, s->st);
   dfree(g5, s->st);
   dfree(out, s->st);
   if (e != cudaSuccess) return cuda_status(e);
   return read_err(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_mf_residuals_multipole(btam_system *s, int rule, double *Rq, double *Rs, double *Rx) {
+  if (!Rq || !Rs || !Rx) return BTAM_ERR_ARG;
+  return mp_residuals(s, rule, Rq, Rs, Rx, nullptr, nullptr, 0);
+}
+
+int btam_mf_pair_terms_multipole(btam_system *s, int rule, double *self, double *slot,
+                                 long long slot_cap) {
+  return mp_residuals(s, rule, nullptr, nullptr, nullptr, self, slot, slot_cap);
 }
 
 int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total) {
@@ -1255,8 +1300,15 @@ int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total
   return read_err(s);
 }
 
-int btam_mf_hessian_multipole(btam_system *s, int rule, double *H) {
-  if (!s || !H || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC)) return BTAM_ERR_ARG;
+}  // extern "C"
+
+namespace {
+
+// The multipole Hessian blocks: H (9 per real site, may be null) summed over
+// i in {u} U N(u), or with Hslot (9 per list entry; slot_cap entries at
+// least) the i = u blocks in H and the per-neighbour blocks in Hslot.
+int mp_hessian(btam_system *s, int rule, double *H, double *Hslot, long long slot_cap) {
+  if (!s || (rule != BTAM_MP_FD && rule != BTAM_MP_ANALYTIC)) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   const size_t n = (size_t)s->n_real;
   if (n == 0) return BTAM_OK;
@@ -1264,13 +1316,16 @@ int btam_mf_hessian_multipole(btam_system *s, int rule, double *H) {
   cudaError_t e = cudaMemcpyAsync(&np, s->offs + n, sizeof(int), cudaMemcpyDeviceToHost, s->st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   if (e != cudaSuccess) return cuda_status(e);
-  double *rd = nullptr, *G = nullptr, *Hd = nullptr;
+  if (Hslot && slot_cap < np) return BTAM_ERR_ARG;
+  double *rd = nullptr, *G = nullptr, *Hd = nullptr, *Hs = nullptr;
   BTAM_TRY(dalloc(rd, s->st, n));
   int st = dalloc(G, s->st, 3 * (size_t)(np > 0 ? np : 1));
   if (st == BTAM_OK) st = dalloc(Hd, s->st, 9 * n);
+  if (st == BTAM_OK && Hslot) st = dalloc(Hs, s->st, 9 * (size_t)(np > 0 ? np : 1));
   if (st != BTAM_OK) {
     dfree(rd, s->st);
     dfree(G, s->st);
+    dfree(Hd, s->st);
     return st;
   }
   MpArgs a;
@@ -1295,17 +1350,36 @@ int btam_mf_hessian_multipole(btam_system *s, int rule, double *H) {
   mp_rho_grad_kernel<<<g, 128, 0, s->st>>>(a, G);
   e = cudaGetLastError();
   if (e == cudaSuccess) {
-    st = mf_hessian_enqueue_with(s, rd, G, Hd);
-    if (st == BTAM_OK)
+    st = mf_hessian_enqueue_with(s, rd, G, Hd, Hs);
+    if (st == BTAM_OK && H)
       e = cudaMemcpyAsync(H, Hd, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+    if (st == BTAM_OK && e == cudaSuccess && Hslot)
+      e = cudaMemcpyAsync(Hslot, Hs, 9 * (size_t)np * sizeof(double), cudaMemcpyDeviceToHost,
+                          s->st);
     if (st == BTAM_OK && e == cudaSuccess) e = cudaStreamSynchronize(s->st);
   }
   dfree(rd, s->st);
   dfree(G, s->st);
   dfree(Hd, s->st);
+  dfree(Hs, s->st);
   if (e != cudaSuccess) return cuda_status(e);
   if (st != BTAM_OK) return st;
   return read_err(s);
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_mf_hessian_multipole(btam_system *s, int rule, double *H) {
+  if (!H) return BTAM_ERR_ARG;
+  return mp_hessian(s, rule, H, nullptr, 0);
+}
+
+int btam_mf_hessian_pairs_multipole(btam_system *s, int rule, double *Hself, double *Hslot,
+                                    long long slot_cap) {
+  if (!Hself || !Hslot) return BTAM_ERR_ARG;
+  return mp_hessian(s, rule, Hself, Hslot, slot_cap);
 }
 
 }  // extern "C"

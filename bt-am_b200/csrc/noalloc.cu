@@ -21,7 +21,10 @@
 //    serialise them;
 //  * the first call on each device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture begins.
+//    before any stream capture begins;
+//  * a call reads the kernels' error flag back to the host and waits for
+//    its stream before returning, so the host blocks until the evaluation
+//    has finished.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -151,5 +154,6 @@ extern "C" int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_r
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return noalloc_status(e);
   if (bits & (1 << kErrBitNonFinite)) return BTAM_ERR_NONFINITE;
+  if (bits & (1 << kErrBitTimeout)) return BTAM_ERR_TIMEOUT;
   return bits ? BTAM_ERR_CUDA : BTAM_OK;
 }

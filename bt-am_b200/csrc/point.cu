@@ -157,7 +157,12 @@ __device__ __forceinline__ V3<double> pt_grad(const double (&m)[kPtRec], const V
                      k * r.z + ca * mu.z + cl * Lr.z);
 }
 
-__global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a) {
+// PAIRS: the per-pair terms instead of their sum: slot3[3p..] = h(j->u) =
+// dV_j/dq_u for every entry p of u's list (0 for an empty j) and Fq_u =
+// -sum_j g(u->j) = dV_u/dq_u (evaluate_DV_i_Dq_u_adp_MgHx at (u, j) and
+// (u, u)).
+template <bool PAIRS>
+__global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a, double *slot3) {
   const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (u >= a.n_real) return;
   const double xu = a.xb[u].x;
@@ -165,6 +170,9 @@ __global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a) {
   double acc[12];
 #pragma unroll
   for (int c = 0; c < 12; ++c) acc[c] = 0.0;
+  if (PAIRS && xu < kMinOcc)
+    for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32)
+      for (int c = 0; c < 3; ++c) slot3[3 * (size_t)p + c] = 0.0;
   if (!(xu < kMinOcc)) {
     double mu_[kPtRec];
     ld_rec(a.rec + (size_t)kPtRec * u, mu_);
@@ -172,6 +180,8 @@ __global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a) {
     for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
       const int j = a.idx[p];
       const double xj = a.xb[j].x;
+      if (PAIRS && xj < kMinOcc)
+        for (int c = 0; c < 3; ++c) slot3[3 * (size_t)p + c] = 0.0;
       if (xj < kMinOcc) continue;
       const double4 qj = a.pos[j];
       const int cj = a.code[j], pk = pair_kind(cu, cj);
@@ -186,9 +196,18 @@ __global__ void __launch_bounds__(128) pt_grad_kernel(PtArgs a) {
       ld_rec12(a.rec + (size_t)kPtRec * a.owner[j], mo);
       const V3<double> rn = mk3<double>(-r.x, -r.y, -r.z);
       const V3<double> hj = pt_grad(mo, rn, g, t, xu, dru, dph);
-      acc[0] += hj.x - gu.x;
-      acc[1] += hj.y - gu.y;
-      acc[2] += hj.z - gu.z;
+      if (PAIRS) {
+        slot3[3 * (size_t)p] = hj.x;
+        slot3[3 * (size_t)p + 1] = hj.y;
+        slot3[3 * (size_t)p + 2] = hj.z;
+        acc[0] -= gu.x;
+        acc[1] -= gu.y;
+        acc[2] -= gu.z;
+      } else {
+        acc[0] += hj.x - gu.x;
+        acc[1] += hj.y - gu.y;
+        acc[2] += hj.z - gu.z;
+      }
       acc[3] += gu.x * r.x;
       acc[4] += gu.x * r.y;
       acc[5] += gu.x * r.z;
@@ -340,8 +359,7 @@ __global__ void __launch_bounds__(128) pt_hself_kernel(PtArgs a, double *hrec) {
       const double rho = a.rec[(size_t)kPtRec * i];
       double F, dF, ddF;
       const SplineView<double> &E = ci == 0 ? a.emb_mg : a.emb_h;
-      int m = (int)(rho * E.inv_dx);
-      m = m < E.n - 1 ? m : E.n - 1;
+      const int m = seg_index(rho, E.dx, E.inv_dx, E.n);
       const double pp = fmin(rho - (double)m * E.dx, E.dx);
       const double k[4] = {E.c[m].a, E.c[m].b, E.c[m].c, E.c[m].d};
       cub_vdd(k, pp, F, dF, ddF);
@@ -367,12 +385,20 @@ __global__ void __launch_bounds__(128) pt_hself_kernel(PtArgs a, double *hrec) {
 
 // Pass 2b: H_u (9 per real site) = the self products + the neighbours'
 // linear terms of both kinds.
-__global__ void __launch_bounds__(128) pt_hess_kernel(PtArgs a, const double *hrec, double *H) {
+// PAIRS: H_u holds the i = u block only and slot9[9p..] the block of
+// neighbour j's terms for every entry p of u's list (0 for an empty j):
+// evaluate_D2V_i_Dq2_u_MgHx at (u, u) and (u, j).
+template <bool PAIRS>
+__global__ void __launch_bounds__(128) pt_hess_kernel(PtArgs a, const double *hrec, double *H,
+                                                      double *slot9) {
   const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (u >= a.n_real) return;
   const double xu = a.xb[u].x;
   const int cu = a.code[u];
   double acc[6] = {0, 0, 0, 0, 0, 0};
+  if (PAIRS && xu < kMinOcc)
+    for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32)
+      for (int c = 0; c < 9; ++c) slot9[9 * (size_t)p + c] = 0.0;
   if (!(xu < kMinOcc)) {
     double mu_[kPtRec];
     ld_rec(a.rec + (size_t)kPtRec * u, mu_);
@@ -380,6 +406,8 @@ __global__ void __launch_bounds__(128) pt_hess_kernel(PtArgs a, const double *hr
     for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
       const int j = a.idx[p];
       const double xj = a.xb[j].x;
+      if (PAIRS && xj < kMinOcc)
+        for (int c = 0; c < 9; ++c) slot9[9 * (size_t)p + c] = 0.0;
       if (xj < kMinOcc) continue;
       const double4 qj = a.pos[j];
       const int cj = a.code[j], pk = pair_kind(cu, cj), o = a.owner[j];
@@ -395,9 +423,18 @@ __global__ void __launch_bounds__(128) pt_hess_kernel(PtArgs a, const double *hr
       double mo[kPtRec];
       ld_rec(a.rec + (size_t)kPtRec * o, mo);
       const double fj = hrec[8 * (size_t)o];
-      pt_hess_linear(mo, rn, S, t,
-                     fj * (xu * S.drc) * (xu * S.drc) + mo[1] * xu * S.ddrc + 0.5 * t * S.ddph,
-                     mo[1] * xu * S.drc + 0.5 * t * S.dph, acc);
+      if (PAIRS) {
+        double hj[6] = {0, 0, 0, 0, 0, 0};
+        pt_hess_linear(mo, rn, S, t,
+                       fj * (xu * S.drc) * (xu * S.drc) + mo[1] * xu * S.ddrc + 0.5 * t * S.ddph,
+                       mo[1] * xu * S.drc + 0.5 * t * S.dph, hj);
+        for (int x = 0; x < 3; ++x)
+          for (int y = 0; y < 3; ++y) slot9[9 * (size_t)p + 3 * x + y] = hj[sym6(x, y)];
+      } else {
+        pt_hess_linear(mo, rn, S, t,
+                       fj * (xu * S.drc) * (xu * S.drc) + mo[1] * xu * S.ddrc + 0.5 * t * S.ddph,
+                       mo[1] * xu * S.drc + 0.5 * t * S.dph, acc);
+      }
     }
   }
 #pragma unroll
@@ -503,7 +540,7 @@ int pt_run(btam_system *s, const PtLayout &L) {
   const PtArgs a = pt_args(s, L);
   const int g = nblk((long long)s->n_real * 32, 128);
   pt_moments_kernel<<<g, 128, 0, s->st>>>(a);
-  pt_grad_kernel<<<g, 128, 0, s->st>>>(a);
+  pt_grad_kernel<false><<<g, 128, 0, s->st>>>(a, nullptr);
   pt_totals_part_kernel<<<kPtParts, 256, 0, s->st>>>(s->n_real, L.V, L.Fq, L.W, L.part);
   pt_totals_final_kernel<<<1, 32, 0, s->st>>>(L.part, L.tot);
   return cuda_status(cudaGetLastError());
@@ -642,10 +679,52 @@ int btam_pt_hessian(btam_system *s, double *H) {
   const int g = nblk((long long)s->n_real * 32, 128);
   pt_moments_kernel<<<g, 128, 0, s->st>>>(a);
   pt_hself_kernel<<<g, 128, 0, s->st>>>(a, L.hrec);
-  pt_hess_kernel<<<g, 128, 0, s->st>>>(a, L.hrec, L.H);
+  pt_hess_kernel<false><<<g, 128, 0, s->st>>>(a, L.hrec, L.H, nullptr);
   BTAM_TRY(cudaGetLastError());
   BTAM_TRY(cudaMemcpyAsync(H, L.H, 9 * (size_t)s->n_real * sizeof(double),
                            cudaMemcpyDeviceToHost, s->st));
+  return read_err(s);
+}
+
+int btam_pt_pair_terms(btam_system *s, double *self3, double *slot3, double *Hself,
+                       double *Hslot, long long slot_cap) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  int n_slots = 0;
+  BTAM_TRY(copy_sync(&n_slots, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  if ((slot3 || Hslot) && slot_cap < n_slots) return BTAM_ERR_ARG;
+  PtLayout L;
+  int st = pt_buffers(s, L);
+  if (st != BTAM_OK) return st;
+  const size_t n = (size_t)s->n_real;
+  double *d_slot = nullptr;
+  BTAM_TRY(dalloc(d_slot, s->st, 9 * (size_t)n_slots));
+  const PtArgs a = pt_args(s, L);
+  const int g = nblk((long long)s->n_real * 32, 128);
+  pt_moments_kernel<<<g, 128, 0, s->st>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && (self3 || slot3)) {
+    pt_grad_kernel<true><<<g, 128, 0, s->st>>>(a, d_slot);
+    e = cudaGetLastError();
+    if (e == cudaSuccess && self3)
+      e = cudaMemcpyAsync(self3, L.Fq, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess && slot3)
+      e = cudaMemcpyAsync(slot3, d_slot, 3 * (size_t)n_slots * sizeof(double),
+                          cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);  // d_slot is reused below
+  }
+  if (e == cudaSuccess && (Hself || Hslot)) {
+    pt_hself_kernel<<<g, 128, 0, s->st>>>(a, L.hrec);
+    pt_hess_kernel<true><<<g, 128, 0, s->st>>>(a, L.hrec, L.H, d_slot);
+    e = cudaGetLastError();
+    if (e == cudaSuccess && Hself)
+      e = cudaMemcpyAsync(Hself, L.H, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, s->st);
+    if (e == cudaSuccess && Hslot)
+      e = cudaMemcpyAsync(Hslot, d_slot, 9 * (size_t)n_slots * sizeof(double),
+                          cudaMemcpyDeviceToHost, s->st);
+  }
+  dfree(d_slot, s->st);
+  if (e != cudaSuccess) return cuda_status(e);
   return read_err(s);
 }
 

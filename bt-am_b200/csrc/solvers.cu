@@ -256,32 +256,91 @@ __global__ void dmd_degree_kernel(int n, const int *doffs, const int *didx, cons
   deg[i] = d;
 }
 
+// Occupancy moved from i to o across an active edge in one step: dt J with
+// J = Df/dr^2 (beta_i+beta_j)/2 xm (1-xm) (mu_i - mu_o), xm = (x_i+x_o)/2
+// (exactly antisymmetric in i, o).
+__device__ __forceinline__ double dmd_move(const double2 *xb, const double *mu,
+                                           const long long *X, int i, int o,
+                                           const DmdParams &prm) {
+  const double xi = (double)X[i] * kDmdQuantum, xo = (double)X[o] * kDmdQuantum;
+  const double xm = 0.5 * (xi + xo), bm = 0.5 * (xb[i].y + xb[o].y);
+  const double J = prm.Df / (prm.dr * prm.dr) * bm * xm * (1.0 - xm) * (mu[i] - mu[o]);
+  return prm.dt * J;
+}
+
+// The room of edge (i, o) in quanta under the degree split: a move from i
+// to o of at most hi, from o to i of at most -lo (lo <= 0).
+__device__ __forceinline__ void dmd_room(const long long *X, const int *deg, int i, int o,
+                                         long long xmax, long long &hi, long long &lo) {
+  const long long di = deg[i] > 0 ? deg[i] : 1, dq = deg[o] > 0 ? deg[o] : 1;
+  const long long out_i = X[i] / di, out_o = X[o] / dq;
+  const long long in_i = xmax > X[i] ? (xmax - X[i]) / di : 0;
+  const long long in_o = xmax > X[o] ? (xmax - X[o]) / dq : 0;
+  hi = out_i < in_o ? out_i : in_o;
+  lo = -(out_o < in_i ? out_o : in_i);
+}
+
 __global__ void dmd_flux_kernel(int n, const double2 *xb, const int *doffs, const int *didx,
                                 const int *owner, const int *active, const int *deg,
                                 const double *mu, const long long *X0, long long *X,
-                                DmdParams prm) {
+                                DmdParams prm, unsigned long long *ctl) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !active[i]) return;
   const long long xmax = llrint(prm.max_x * kDmdInvQuantum);
   for (int p = doffs[i]; p < doffs[i + 1]; ++p) {
     int o = owner[didx[p]];
     if (o <= i || !active[o]) continue;  // each undirected edge once, from its lower end
-    double xi = (double)X0[i] * kDmdQuantum, xo = (double)X0[o] * kDmdQuantum;
-    double xm = 0.5 * (xi + xo), bm = 0.5 * (xb[i].y + xb[o].y);
-    double J = prm.Df / (prm.dr * prm.dr) * bm * xm * (1.0 - xm) * (mu[i] - mu[o]);
-    double dlt = prm.dt * J;  // occupancy moved from i to o
+    const double dlt = dmd_move(xb, mu, X0, i, o, prm);  // occupancy moved from i to o
     if (fabs(dlt) < prm.min_dx) continue;
     long long q = llrint(dlt * kDmdInvQuantum);
-    long long di = deg[i] > 0 ? deg[i] : 1, dq = deg[o] > 0 ? deg[o] : 1;
-    long long out_i = X0[i] / di, out_o = X0[o] / dq;
-    long long in_i = xmax > X0[i] ? (xmax - X0[i]) / di : 0;
-    long long in_o = xmax > X0[o] ? (xmax - X0[o]) / dq : 0;
-    long long hi = out_i < in_o ? out_i : in_o;
-    long long lo = -(out_o < in_i ? out_o : in_i);
+    long long hi, lo;
+    dmd_room(X0, deg, i, o, xmax, hi, lo);
+    // a move cut to a nonzero room is counted; a zero room (empty giver,
+    // full receiver) moves nothing and is not
+    if (ctl && ((q > hi && hi > 0) || (q < lo && lo < 0))) atomicAdd(ctl + 2, 1ull);
     q = q > hi ? hi : (q < lo ? lo : q);
     if (q == 0) continue;
     atomicAdd((unsigned long long *)&X[i], (unsigned long long)(-q));
     atomicAdd((unsigned long long *)&X[o], (unsigned long long)q);
+  }
+}
+
+// Step-control decision for a step of prm.dt at the current state: per
+// site, its occupancy change over max_dx (moves below min_dx skipped, as in
+// the update) and, over its edges to higher sites, each move over its
+// nonzero room; the maxima go to ctl[1] and ctl[0] (a non-negative
+// double's bits order as the double).
+__global__ void dmd_control_kernel(int n, const double2 *xb, const int *doffs, const int *didx,
+                                   const int *owner, const int *active, const int *deg,
+                                   const double *mu, const long long *X, DmdParams prm,
+                                   double max_dx, unsigned long long *ctl) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double ratio = 0.0, dx = 0.0;
+  if (i < n && active[i]) {
+    const long long xmax = llrint(prm.max_x * kDmdInvQuantum);
+    for (int p = doffs[i]; p < doffs[i + 1]; ++p) {
+      int o = owner[didx[p]];
+      if (o == i || !active[o]) continue;
+      const double dlt = dmd_move(xb, mu, X, i, o, prm);
+      if (fabs(dlt) < prm.min_dx) continue;
+      dx = __dsub_rn(dx, dlt);  // no contraction: the oracle rounds each term
+      if (o < i) continue;  // the room of each edge once
+      const long long q = llrint(dlt * kDmdInvQuantum);
+      long long hi, lo;
+      dmd_room(X, deg, i, o, xmax, hi, lo);
+      if (q > hi && hi > 0) ratio = fmax(ratio, (double)q / (double)hi);
+      if (q < lo && lo < 0) ratio = fmax(ratio, (double)q / (double)lo);
+    }
+  }
+  double r = fabs(dx) / max_dx;
+  // warp maxima (every lane of the block takes part), then one atomic per warp
+  for (int off = 16; off > 0; off >>= 1) {
+    ratio = fmax(ratio, __shfl_xor_sync(0xffffffffu, ratio, off));
+    r = fmax(r, __shfl_xor_sync(0xffffffffu, r, off));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(ctl, (unsigned long long)__double_as_longlong(ratio));
+    atomicMax(ctl + 1, (unsigned long long)__double_as_longlong(r));
   }
 }
 
@@ -326,15 +385,35 @@ cudaError_t dmd_commit_all(int n, const int *code, const long long *X, double2 *
   return cudaGetLastError();
 }
 
-cudaError_t dmd_step(const DmdArgs &a, const DmdParams &prm, cudaStream_t st) {
+cudaError_t dmd_prepare(const DmdArgs &a, cudaStream_t st) {
   dmd_mu_kernel<<<nbk(a.n), 256, 0, st>>>(a.n, a.xb, a.code, a.Rx, a.gamma, a.moffs, a.midx,
                                           a.X, a.mu, a.active);
   dmd_degree_kernel<<<nbk(a.n), 256, 0, st>>>(a.n, a.doffs, a.didx, a.owner, a.active, a.deg);
-  cudaMemcpyAsync(a.X0, a.X, (size_t)a.n * sizeof(long long), cudaMemcpyDeviceToDevice, st);
+  return cudaGetLastError();
+}
+
+cudaError_t dmd_control(const DmdArgs &a, const DmdParams &prm, double max_dx,
+                        cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(a.ctl, 0, 2 * sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  dmd_control_kernel<<<nbk(a.n), 256, 0, st>>>(a.n, a.xb, a.doffs, a.didx, a.owner, a.active,
+                                               a.deg, a.mu, a.X, prm, max_dx, a.ctl);
+  return cudaGetLastError();
+}
+
+cudaError_t dmd_apply(const DmdArgs &a, const DmdParams &prm, cudaStream_t st) {
+  cudaError_t e = cudaMemcpyAsync(a.X0, a.X, (size_t)a.n * sizeof(long long),
+                                  cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return e;
   dmd_flux_kernel<<<nbk(a.n), 256, 0, st>>>(a.n, a.xb, a.doffs, a.didx, a.owner, a.active,
-                                            a.deg, a.mu, a.X0, a.X, prm);
+                                            a.deg, a.mu, a.X0, a.X, prm, a.ctl);
   dmd_commit_kernel<<<nbk(a.n), 256, 0, st>>>(a.n, a.code, a.X, a.xb);
   return cudaGetLastError();
+}
+
+cudaError_t dmd_step(const DmdArgs &a, const DmdParams &prm, cudaStream_t st) {
+  cudaError_t e = dmd_prepare(a, st);
+  return e == cudaSuccess ? dmd_apply(a, prm, st) : e;
 }
 
 cudaError_t dmd_total(int n, const int *code, const long long *X, long long *out2,

@@ -48,6 +48,10 @@ struct DmdArgs {
   long long *X, *X0;        // occupancy quanta, snapshot
   double *mu;
   int *active, *deg;
+  // step-control counters: [0] the largest edge move over its room and [1]
+  // the largest site change over max_dx of the last decision (non-negative
+  // doubles as their bits), [2] edge moves clipped to a nonzero room
+  unsigned long long *ctl = nullptr;
 };
 
 cudaError_t dmd_init(int n, const double2 *xb, const int *code, long long *X, cudaStream_t st);
@@ -55,6 +59,13 @@ cudaError_t dmd_init(int n, const double2 *xb, const int *code, long long *X, cu
 cudaError_t dmd_commit_all(int n, const int *code, const long long *X, double2 *xb,
                            cudaStream_t st);
 cudaError_t dmd_step(const DmdArgs &a, const DmdParams &prm, cudaStream_t st);
+// The step in its parts: chemical potentials, activity and degrees of the
+// current state; then (optionally) the step-control decision for a step
+// of prm.dt into ctl[0..1]; then the occupancy update of one step of
+// prm.dt (snapshot, edge moves, commit).
+cudaError_t dmd_prepare(const DmdArgs &a, cudaStream_t st);
+cudaError_t dmd_control(const DmdArgs &a, const DmdParams &prm, double max_dx, cudaStream_t st);
+cudaError_t dmd_apply(const DmdArgs &a, const DmdParams &prm, cudaStream_t st);
 cudaError_t dmd_total(int n, const int *code, const long long *X, long long *out2,
                       cudaStream_t st);
 

@@ -81,6 +81,12 @@ typedef struct btam_batch btam_batch;
 
 const char *btam_status_string(int status);
 int btam_version(void);
+/* Bytes of the library's device-memory pool on the current device (no
+ * counterpart in the reference): in use by live systems, batches and
+ * servers, and reserved from the device.  Every device allocation of the
+ * library comes from this pool, so a call that leaves both unchanged
+ * allocated nothing that it kept. */
+int btam_pool_usage(long long *used, long long *reserved);
 
 /* Replaces init_adp_MgHx(&adp_MgMg, MgMg, dir), (&adp_HH, HH, dir),
  * (&adp_MgH, MgH, dir) (src/ADP/MgHx-ADP.cpp:366-501; called at
@@ -195,6 +201,28 @@ int btam_set_variants(btam_system *s, int precision, int pass1_variant, int pass
  * be NULL. */
 int btam_mf_stress(btam_system *s, int precision, double *W0, double *total);
 
+/* The per-pair terms of the residual assembly, unweighted, one value per
+ * call of the reference's per-pair functions (the whole assembly that
+ * btam_mf_eval returns is their beta-weighted sum):
+ *   self (5 per real site u, may be NULL):  dV0_u/dq_u (3), dV0_u/dsigma_u,
+ *        dV0_u/dx_u = evaluate_DV0_i_Dq_u_MgHx(u, u) (MgHx-mf-V-bulk.cpp:
+ *        1823-2098; its dq part also evaluate_DV0_i_Dmeanq_u_MgHx, 1146-1362,
+ *        and its dsigma part evaluate_DV0_i_Dstdvq_u_MgHx, 1603-1819) and
+ *        evaluate_DV0_i_Dxi_u_adp_MgHx(u, u) (2102-2325);
+ *   slot (5 per entry p of the real sites' neighbour lists, in the order of
+ *        btam_neighbors_copy; slot_cap entries of 5 at least, may be NULL):
+ *        for u's entry p with neighbour j, dV0_j/d(q_u, sigma_u, x_u) = the
+ *        same functions at (u, j).  For a periodic image j it is the value
+ *        of j's owner o at the image of u that neighbours o with the
+ *        opposite shift (translation invariance), the pair the reference
+ *        evaluates for that entry.
+ * Values are 0 when u or j is empty (x < min_occupancy).  The dx part is
+ * defined for every species (the assembly keeps it for H sites only).
+ * Directed kernels, in `precision`; runs the directed pass 1 first (the
+ * system's rho, V0, S0 buffers then hold the current state's values). */
+int btam_mf_pair_terms(btam_system *s, int precision, double *self, double *slot,
+                       long long slot_cap);
+
 /* Mean-field Hessian blocks: H (9 per real site, row-major) = sum over
  * i in {u} U N(u) of evaluate_D2V0_i_Dmeanq2_u_MgHx(u, i)
  * (MgHx-mf-V-bulk.cpp:1366-1600), FP64, as the reference forms each term
@@ -205,6 +233,11 @@ int btam_mf_stress(btam_system *s, int precision, double *W0, double *total);
  * pass 1 first (the system's rho, V0, S0 buffers then hold the current
  * state's values). */
 int btam_mf_hessian(btam_system *s, double *H);
+/* The same blocks one pair at a time, as the reference returns them:
+ * Hself (9 per real site, may be NULL) = evaluate_D2V0_i_Dmeanq2_u_MgHx(u, u)
+ * and Hslot (9 per entry of the real sites' lists, slot_cap entries at
+ * least, may be NULL) = the block of the entry's neighbour i, (u, i). */
+int btam_mf_hessian_pairs(btam_system *s, double *Hself, double *Hslot, long long slot_cap);
 
 /* ---- the multipole rule (MULTIPOLE_INTEGRAL) ------------------------------
  * The reference's alternative mean-field rule behind its compile switch
@@ -250,6 +283,19 @@ int btam_mf_stress_multipole(btam_system *s, int rule, double *W0, double *total
  * at the multipole rho-bar.  H: 9 per real site.  FP64. */
 int btam_mf_hessian_multipole(btam_system *s, int rule, double *H);
 
+/* The per-pair terms under the multipole rule, as btam_mf_pair_terms: self
+ * (5 per real site) and slot (5 per list entry, slot_cap entries at least),
+ * either may be NULL; evaluate_DV0_i_Dq_u_MgHx (1823-2098) and
+ * evaluate_DV0_i_Dxi_u_adp_MgHx (2102-2325) built with the rule, FP64. */
+int btam_mf_pair_terms_multipole(btam_system *s, int rule, double *self, double *slot,
+                                 long long slot_cap);
+/* Per-pair Hessian blocks: Hself (9 per real site) the block of i = u and
+ * Hslot (9 per list entry, slot_cap entries at least) the block of the
+ * entry's neighbour i, evaluate_D2V0_i_Dmeanq2_u_MgHx(u, u) and (u, i)
+ * (1366-1600) built with the rule.  Both outputs are required. */
+int btam_mf_hessian_pairs_multipole(btam_system *s, int rule, double *Hself, double *Hslot,
+                                    long long slot_cap);
+
 /* Replaces evaluate_rho_i_adp_MgHx_kokkos (src/ADP/density.cpp:44-104), the
  * non-mean-field density the shipped main-BT-AM.cpp evaluates (197-207). */
 int btam_rho_nmf(btam_system *s, double *rho);
@@ -278,6 +324,16 @@ int btam_pt_eval(btam_system *s, double *rho, double *V, double *Fq, double *W,
  * the slots u holds in V_i's terms (for j1 = j2 = u the two slot blocks
  * without their cross blocks, so this is not d2(sum V)/dq_u^2 there). */
 int btam_pt_hessian(btam_system *s, double *H);
+/* The non-mean-field gradient and Hessian terms one pair at a time, as the
+ * reference's per-pair functions return them (any output may be NULL):
+ *   self3 (3 per real site) = evaluate_DV_i_Dq_u_adp_MgHx(u, u) (147-330),
+ *   slot3 (3 per entry of the real sites' lists) = the same at (u, i) for
+ *         the entry's neighbour i,
+ *   Hself (9 per real site) = evaluate_D2V_i_Dq2_u_MgHx(u, u) (333-528),
+ *   Hslot (9 per entry) = the same at (u, i);
+ * slot_cap bounds the entries of slot3 and Hslot. */
+int btam_pt_pair_terms(btam_system *s, double *self3, double *slot3, double *Hself,
+                       double *Hslot, long long slot_cap);
 /* Stretches the system by diag(F) (F[a] > 0): q <- F q for every site, the
  * cell rows and the origin likewise; images follow; neighbour lists are
  * kept.  BTAM_ERR_BOX_TOO_SMALL (nothing changed) if a periodic cell would
@@ -370,6 +426,38 @@ int btam_relax_newton(btam_system *s, double tol, int max_newton, int max_cg,
 int btam_dmd_setup(btam_system *s);
 int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *params,
                   long long *total_quanta);
+/* The same steps with step control (no counterpart in the reference).
+ * Every step of length dt first takes the chemical potentials at the
+ * current occupancies and from them two ratios: the largest move of an
+ * edge over the room the degree split leaves it (edges whose room is zero,
+ * an empty giver or a full receiver, move nothing and do not count), and
+ * the largest change of a site's occupancy over max_dx.  The step is then
+ * taken as m = min(max_sub, max(1, ceil(the larger ratio))) sub-steps of
+ * dt / m, each with fresh chemical potentials (the first reuses the
+ * decision's): a sub-step is exactly one btam_dmd_step of dt / m.
+ * params (7, NULL = defaults): dt, Df, dr, min_dx, max_x as btam_dmd_step,
+ * then max_dx (0.05) and max_sub (64).  stats (4, may be NULL): sub-steps
+ * taken, steps that were subdivided, edge moves still cut to their room
+ * (possible when a step needs more than max_sub sub-steps or the chemical
+ * potentials change within it), the largest ratio seen.  Synchronises once
+ * per step to read the decision. */
+int btam_dmd_step_ctl(btam_system *s, int precision, int nsteps, const double *params,
+                      long long *total_quanta, double *stats);
+/* A mean-field DMD run (no counterpart in the reference, which keeps only
+ * the method's parameters): nsteps master-equation steps with step control
+ * (btam_dmd_step_ctl, params as there) and, after every relax_every steps,
+ * a relaxation of (q, sigma) at the new occupancies (btam_relax with
+ * relax_mode, relax_tol, relax_max_iter, history 8, default bounds), so the
+ * mechanical state follows the occupancy; relax_every = 0 never relaxes.
+ * Neighbour lists and the diffusive graph stay as built.  stats (6, may be
+ * NULL): sub-steps, subdivided steps, cut edge moves, the largest ratio
+ * (as btam_dmd_step_ctl), relaxations run, their residual evaluations. */
+int btam_dmd_run(btam_system *s, int precision, int nsteps, const double *params,
+                 int relax_every, int relax_mode, double relax_tol, int relax_max_iter,
+                 long long *total_quanta, double *stats);
+/* Edge moves cut to a nonzero room by every master-equation step since
+ * btam_dmd_setup (btam_dmd_step and btam_dmd_step_ctl alike). */
+int btam_dmd_clip_count(btam_system *s, long long *clipped);
 /* Current occupancies (n_real), their quanta and the last chemical
  * potentials; any pointer may be NULL. */
 int btam_dmd_occupancy(btam_system *s, double *x, long long *quanta, double *mu);
@@ -393,8 +481,9 @@ int btam_dmd_graph_copy(const btam_system *s, int *offs, int *idx, long long idx
  * per device) lives until the process exits and is shared by every call on
  * that device: calls that overlap on the GPU race; serialise them.  The
  * first call on each device looks the scratch up, so make it before any
- * stream capture.  Runs on `stream` (a cudaStream_t, NULL = default) and
- * synchronises it before returning. */
+ * stream capture.  Runs on `stream` (a cudaStream_t, NULL = default); before
+ * returning it reads the kernels' error flag back to the host and waits for
+ * `stream`, so the host blocks until the evaluation has finished. */
 int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_real,
                          const double *pos4, const double *xb, const int *code,
                          const int *owner, const double *gamma, const int *offs,

@@ -19,29 +19,34 @@
  *
  * Semantics:
  *  - Sites 0..n-1 of the caller's arrays are the real sites of the bound
- *    system, in its order; rows beyond n (the caller's ghost copies) are not
- *    read.  The caller's `mf_rho` is not read (rho-bar is recomputed with
- *    the state); `specie` is read only to tell H sites for the occupancy
- *    derivative (the system keeps its own species).
- *  - Every call compares the state of the sites it depends on (the site,
- *    the site whose derivative is asked for, and the neighbours in its
- *    AtomTopology) with the evaluated state; on any difference the whole
- *    state is taken from the caller's arrays and evaluated again.  Calls are
+ *    system, in its order; indices from n on are the system's periodic
+ *    images in its numbering (btam_ghosts_copy: the order in which the
+ *    reference's DMSwarmCreateGhostAtoms appends them).  Rows beyond n of
+ *    the caller's arrays are never read: an image takes its owner's state.
+ *    The caller's `mf_rho`/`rho` arguments are not read (rho-bar is
+ *    recomputed with the state); `specie` is not read (the system keeps its
+ *    own species).
+ *  - A value of site i depends on the state of i and of its neighbours
+ *    N(i).  Every call compares that state (the system's own lists, images
+ *    mapped to their owners, and the site u a derivative is taken for) with
+ *    the evaluated state; on any difference the whole state is taken from
+ *    the caller's arrays and the values are evaluated again.  Calls are
  *    serialised by a mutex, so OpenMP callers are safe.
- *  - The reference has no assembler of its per-pair derivatives (one term
- *    dV0_i/d(.)_u per call); the device computes the assembled residuals.
- *    So the derivative functions are lumped: for site_i == site_i_star they
- *    return the whole sum over i in {u} U N(u) of the terms the reference
- *    returns for (u, i), each weighted by beta_i / beta_u (plain sum when
- *    every site has the same beta), and zero for site_i != site_i_star.  A
- *    caller that sums over i, as every residual assembly does, gets the
- *    assembled value.  The occupancy derivative is defined for H sites
- *    (zero for Mg, as the device's R_x).
+ *  - The derivative slots return the reference's per-pair values, one term
+ *    per (u, i) call: evaluate_DV0_i_Dq_j(u, i) is dV0_i/d(q_u, sigma_u),
+ *    evaluate_DV0_i_Dxi_j(u, i) is dV0_i/dx_u, and likewise the
+ *    non-mean-field gradient and the Hessian blocks (btam_mf_pair_terms,
+ *    btam_pt_pair_terms, btam_mf_hessian_pairs).  i = u is the self term;
+ *    for i != u the pair is found in u's list as the entry whose owner is
+ *    i's owner and whose image shift is i's minus u's, so both the entry as
+ *    u's list names it and the pair the reference evaluates for it (u's
+ *    image in i's list, i real) give the same value.  A site i that does not
+ *    neighbour u gives 0, as in the reference.  A caller assembles a
+ *    residual by summing over i in {u} U N(u), images included, with its
+ *    own weights (the device's btam_mf_eval weights by beta_i / beta_u).
  *  - The non-mean-field forms (evaluate_rho_i, evaluate_DV_i_Dq_j,
- *    evaluate_DV_i_DF) come from one btam_pt_eval of the state; the
- *    gradient is lumped like the mean-field derivatives (the whole
- *    sum_{i in {u} U N(u)} dV_i/dq_u at site_i == site_i_star).  The
- *    caller's `rho` argument is not read.
+ *    evaluate_DV_i_DF, evaluate_D2V_i_Dq2_j) come from btam_pt_eval and
+ *    btam_pt_pair_terms of the state.
  *  - Stretches: when the caller's mean_q is a diagonal stretch diag(F) of the
  *    positions bound with bind() (to 1e-13 relative, every row), the system's
  *    cell is stretched with it, so periodic images follow as the caller's
@@ -52,18 +57,15 @@
  *    unstretched positions, Mechanical-Relaxation-bulk.cpp:577-579); other
  *    mean_q0 give NaN and last_status() BTAM_ERR_ARG.
  *  - evaluate_DV0_i_DF (the mean-field stretch derivative) comes from
- *    btam_mf_stress in the bound precision.
- *  - evaluate_D2V_i_Dq2_j (btam_pt_hessian) and evaluate_D2V0_i_Dmeanq2_j
- *    (btam_mf_hessian, FP64 whatever the bound precision) are lumped like
- *    the gradients: the whole sum over i in {u} U N(u) at site_i ==
- *    site_i_star.  Every slot of the table is served.
+ *    btam_mf_stress in the bound precision; evaluate_D2V0_i_Dmeanq2_j is
+ *    FP64 whatever the bound precision.  Every slot of the table is served.
  *  - A caller compiled with MULTIPOLE_INTEGRAL, as the reference's rule
  *    switch selects it, gets the mean-field values and derivatives of the
- *    multipole rule (btam_mf_eval_multipole, btam_mf_residuals_multipole;
- *    FP64): with finite-difference Hessians when NUMERICAL_DERIVATIVES is
- *    defined (the reference's CMakeLists.txt defines it), analytic ones
- *    otherwise; the mean-field stretch derivative and Hessian blocks too
- *    (btam_mf_stress_multipole, btam_mf_hessian_multipole).  The
+ *    multipole rule (btam_mf_eval_multipole, btam_mf_pair_terms_multipole,
+ *    btam_mf_hessian_pairs_multipole; FP64): with finite-difference
+ *    Hessians when NUMERICAL_DERIVATIVES is defined (the reference's
+ *    CMakeLists.txt defines it), analytic ones otherwise; the mean-field
+ *    stretch derivative too (btam_mf_stress_multipole).  The
  *    non-mean-field forms have no rule. */
 #ifndef BTAM_DMD_EQUATIONS_HPP
 #define BTAM_DMD_EQUATIONS_HPP
@@ -80,20 +82,25 @@ struct Cache {
   std::mutex mu;
   btam_system *sys = nullptr;
   int precision = BTAM_FP64;
-  int n = 0;
+  int n = 0, n_ghost = 0;
   bool have_state = false;  // q, sigma, x below are the system's state
-  bool valid = false;       // mean-field results of that state
-  bool pt_valid = false;    // non-mean-field results of that state
-  bool mfs_valid = false;   // mean-field stress of that state
-  bool pth_valid = false;   // non-mean-field Hessian blocks of that state
-  bool mfh_valid = false;   // mean-field Hessian blocks of that state
+  bool valid = false;       // mean-field per-site values of that state
+  bool pairs_valid = false; // mean-field per-pair terms
+  bool pt_valid = false;    // non-mean-field per-site values
+  bool ptp_valid = false;   // non-mean-field per-pair terms and Hessian blocks
+  bool mfs_valid = false;   // mean-field stress
+  bool mfh_valid = false;   // mean-field per-pair Hessian blocks
   int status = BTAM_OK;     // status of the last evaluation
-  std::vector<double> beta, gamma;
   std::vector<double> q, sigma, x;  // the evaluated state (q row-major)
   std::vector<double> q_bind;       // positions at bind(): the stretch reference
   double F[3] = {1.0, 1.0, 1.0};    // stretch of the system's cell against them
-  std::vector<double> rho, V0, S0, Rq, Rs, Rx;
-  std::vector<double> pt_rho, pt_Fq, pt_W, mf_W, pt_H, mf_H;
+  // the system's lists of the real sites, owners and image shifts of all
+  // sites (real sites: themselves, shift 0)
+  std::vector<int> offs, idx, owner, shift;
+  std::vector<double> rho, V0, S0;         // per site
+  std::vector<double> self5, slot5;        // dV0/d(q, sigma, x): i = u, list entries
+  std::vector<double> pt_rho, pt_W, mf_W;  // per site
+  std::vector<double> pt_self3, pt_slot3, pt_Hself, pt_Hslot, mf_Hself, mf_Hslot;
 };
 
 inline Cache &cache() {
@@ -101,11 +108,13 @@ inline Cache &cache() {
   return c;
 }
 
-/* Binds a built system: evaluations use `precision` (BTAM_FP64 or
- * BTAM_FP32C); beta and gamma (n values each, NULL = the defaults of
- * btam_system_create) must be those the system was created with: the
- * adapter removes the entropy terms from the device's residuals with them. */
+/* Binds a built system (neighbour lists built): evaluations use `precision`
+ * (BTAM_FP64 or BTAM_FP32C).  beta and gamma are accepted for the
+ * signature of earlier versions and not read: the per-pair values do not
+ * depend on them. */
 inline int bind(btam_system *s, int precision, const double *beta, const double *gamma) {
+  (void)beta;
+  (void)gamma;
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
   int n_real = 0, n_ghost = 0;
@@ -115,27 +124,44 @@ inline int bind(btam_system *s, int precision, const double *beta, const double 
   c.sys = s;
   c.precision = precision;
   c.n = n_real;
-  c.have_state = c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = c.mfh_valid = false;
+  c.n_ghost = n_ghost;
+  c.have_state = c.valid = c.pairs_valid = c.pt_valid = c.ptp_valid = c.mfs_valid =
+      c.mfh_valid = false;
   c.F[0] = c.F[1] = c.F[2] = 1.0;
-  c.beta.assign(beta ? beta : nullptr, beta ? beta + n_real : nullptr);
-  c.gamma.assign(gamma ? gamma : nullptr, gamma ? gamma + n_real : nullptr);
-  if (!beta) c.beta.assign(n_real, 1.0 / (8.617332478e-5 * 300.0));  // k_B 300 K
-  if (!gamma) c.gamma.assign(n_real, 0.0);
-  c.q.assign(3 * (size_t)n_real, 0.0);
-  c.sigma.assign(n_real, 0.0);
-  c.x.assign(n_real, 0.0);
-  c.rho.assign(n_real, 0.0);
-  c.V0.assign(n_real, 0.0);
-  c.S0.assign(n_real, 0.0);
-  c.Rq.assign(3 * (size_t)n_real, 0.0);
-  c.Rs.assign(n_real, 0.0);
-  c.Rx.assign(n_real, 0.0);
-  c.pt_rho.assign(n_real, 0.0);
-  c.pt_Fq.assign(3 * (size_t)n_real, 0.0);
-  c.pt_W.assign(9 * (size_t)n_real, 0.0);
-  c.mf_W.assign(9 * (size_t)n_real, 0.0);
-  c.pt_H.assign(9 * (size_t)n_real, 0.0);
-  c.mf_H.assign(9 * (size_t)n_real, 0.0);
+  const size_t n = (size_t)n_real, na = n + (size_t)n_ghost;
+  // the lists (btam_neighbors_copy returns every list the system holds;
+  // the real sites' come first)
+  std::vector<int> offs_all(na + 1, 0), idx_all((size_t)(n_pairs > 0 ? n_pairs : 1));
+  st = btam_neighbors_copy(s, offs_all.data(), idx_all.data(), (long long)idx_all.size());
+  if (st != BTAM_OK) return st;
+  c.offs.assign(offs_all.begin(), offs_all.begin() + n + 1);
+  c.idx.assign(idx_all.begin(), idx_all.begin() + c.offs[n]);
+  c.owner.resize(na);
+  c.shift.assign(3 * na, 0);
+  for (size_t j = 0; j < n; ++j) c.owner[j] = (int)j;
+  if (n_ghost > 0) {
+    std::vector<double> qg(3 * (size_t)n_ghost);
+    st = btam_ghosts_copy(s, qg.data(), c.owner.data() + n, c.shift.data() + 3 * n);
+    if (st != BTAM_OK) return st;
+  }
+  const size_t ns = c.idx.size();
+  c.q.assign(3 * n, 0.0);
+  c.sigma.assign(n, 0.0);
+  c.x.assign(n, 0.0);
+  c.rho.assign(n, 0.0);
+  c.V0.assign(n, 0.0);
+  c.S0.assign(n, 0.0);
+  c.self5.assign(5 * n, 0.0);
+  c.slot5.assign(5 * ns, 0.0);
+  c.pt_rho.assign(n, 0.0);
+  c.pt_W.assign(9 * n, 0.0);
+  c.mf_W.assign(9 * n, 0.0);
+  c.pt_self3.assign(3 * n, 0.0);
+  c.pt_slot3.assign(3 * ns, 0.0);
+  c.pt_Hself.assign(9 * n, 0.0);
+  c.pt_Hslot.assign(9 * ns, 0.0);
+  c.mf_Hself.assign(9 * n, 0.0);
+  c.mf_Hslot.assign(9 * ns, 0.0);
   st = btam_system_get_state(s, c.q.data(), c.sigma.data(), c.x.data());
   c.have_state = st == BTAM_OK;
   c.q_bind = c.q;
@@ -148,6 +174,11 @@ inline int last_status() { return cache().status; }
 
 namespace detail {
 
+// Real site of a caller index (a real site or an image), -1 if out of range.
+inline int owner_of(const Cache &c, unsigned j) {
+  return (size_t)j < c.owner.size() ? c.owner[j] : -1;
+}
+
 template <class M, class V>
 inline bool same_site(const Cache &c, int j, const M &mean_q, const V *stdv_q, const V &xi) {
   if (j < 0 || j >= c.n) return true;
@@ -155,6 +186,24 @@ inline bool same_site(const Cache &c, int j, const M &mean_q, const V *stdv_q, c
     if (mean_q(j, k) != c.q[3 * (size_t)j + k]) return false;
   if (stdv_q && (*stdv_q)(j) != c.sigma[j]) return false;
   return xi(j) == c.x[j];
+}
+
+// Entry of u's list that is the pair (u, i): -1 for i = u (the self term),
+// -2 when i does not neighbour u.  The entry's owner is i's owner and its
+// image shift is i's minus u's, so an image u of a real site and the entry
+// as u's owner lists it name the same pair.
+inline long long entry_of(const Cache &c, unsigned u, unsigned i) {
+  if (u == i) return -1;
+  const int u0 = owner_of(c, u), i0 = owner_of(c, i);
+  if (u0 < 0 || i0 < 0) return -2;
+  const int *su = &c.shift[3 * (size_t)u], *si = &c.shift[3 * (size_t)i];
+  for (int p = c.offs[u0]; p < c.offs[u0 + 1]; ++p) {
+    const int j = c.idx[p];
+    if (c.owner[j] != i0) continue;
+    const int *sj = &c.shift[3 * (size_t)j];
+    if (sj[0] == si[0] - su[0] && sj[1] == si[1] - su[1] && sj[2] == si[2] - su[2]) return p;
+  }
+  return -2;
 }
 
 // Diagonal stretch F with c.q = diag(F) q_bind on every row (to 1e-13
@@ -176,24 +225,30 @@ inline bool stretch_of(const Cache &c, double F[3]) {
   return true;
 }
 
-enum { kMeanField = 1, kPoint = 2, kStress = 4, kHessian = 8, kMfHessian = 16 };
+enum {
+  kMeanField = 1, kPairs = 2, kPoint = 4, kPointPairs = 8, kStress = 16, kMfHessian = 32
+};
 
-// Loads the caller's state when the sites a value depends on differ from the
-// cache, then evaluates what `what` asks for and is not yet evaluated.
+// Loads the caller's state when the state a value of site i (and its
+// derivative for site u) depends on differs from the cache: u, i and i's
+// neighbours in the system's lists (images as their owners).  Then
+// evaluates what `what` asks for and is not yet evaluated.
 template <class M, class V>
-inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *stdv_q,
-                    const V &xi, const AtomTopology &topo, int what) {
-  bool same = c.have_state && same_site(c, (int)a, mean_q, stdv_q, xi) &&
-              same_site(c, (int)b, mean_q, stdv_q, xi);
-  for (int k = 0; same && k < topo.numneigh; ++k)
-    same = same_site(c, (int)topo.mech_neighs_ptr[k], mean_q, stdv_q, xi);
+inline void refresh(Cache &c, unsigned u, unsigned i, const M &mean_q, const V *stdv_q,
+                    const V &xi, int what) {
+  const int i0 = owner_of(c, i);
+  bool same = c.have_state && same_site(c, owner_of(c, u), mean_q, stdv_q, xi) &&
+              same_site(c, i0, mean_q, stdv_q, xi);
+  if (same && i0 >= 0)
+    for (int p = c.offs[i0]; same && p < c.offs[i0 + 1]; ++p)
+      same = same_site(c, c.owner[c.idx[p]], mean_q, stdv_q, xi);
   if (!same) {
     for (int j = 0; j < c.n; ++j) {
       for (int k = 0; k < 3; ++k) c.q[3 * (size_t)j + k] = mean_q(j, k);
       if (stdv_q) c.sigma[j] = (*stdv_q)(j);
       c.x[j] = xi(j);
     }
-    c.valid = c.pt_valid = c.mfs_valid = c.pth_valid = c.mfh_valid = false;
+    c.valid = c.pairs_valid = c.pt_valid = c.ptp_valid = c.mfs_valid = c.mfh_valid = false;
     // a stretch of the bound positions takes the cell with it; any other
     // state keeps the current cell
     double F[3];
@@ -209,75 +264,92 @@ inline void refresh(Cache &c, unsigned a, unsigned b, const M &mean_q, const V *
     c.have_state = c.status == BTAM_OK;
   }
   if (!c.have_state) return;
+  const long long ns = (long long)c.idx.size();
+#if defined(MULTIPOLE_INTEGRAL)
+  // the caller is built with the reference's other rule
+  // (MgHx-mf-V-bulk.cpp:715-724), whose Hessians follow the same
+  // `#ifdef NUMERICAL_DERIVATIVES` as Quadrature-Multipole.cpp:134
+#ifdef NUMERICAL_DERIVATIVES
+  const int rule = BTAM_MP_FD;
+#else
+  const int rule = BTAM_MP_ANALYTIC;
+#endif
+#endif
   if ((what & kMeanField) && !c.valid) {
 #if defined(MULTIPOLE_INTEGRAL)
-    // the caller is built with the reference's other rule
-    // (MgHx-mf-V-bulk.cpp:715-724), whose Hessians follow the same
-    // `#ifdef NUMERICAL_DERIVATIVES` as Quadrature-Multipole.cpp:134
-#ifdef NUMERICAL_DERIVATIVES
-    const int rule = BTAM_MP_FD;
-#else
-    const int rule = BTAM_MP_ANALYTIC;
-#endif
     c.status = btam_mf_eval_multipole(c.sys, rule, c.rho.data(), c.V0.data(), c.S0.data(),
                                       nullptr);
-    if (c.status == BTAM_OK)
-      c.status = btam_mf_residuals_multipole(c.sys, rule, c.Rq.data(), c.Rs.data(), c.Rx.data());
 #else
     c.status = btam_mf_eval(c.sys, c.precision, c.rho.data(), c.V0.data(), c.S0.data(),
-                            c.Rq.data(), c.Rs.data(), c.Rx.data(), nullptr);
+                            nullptr, nullptr, nullptr, nullptr);
 #endif
     c.valid = c.status == BTAM_OK;
   }
+  if ((what & kPairs) && !c.pairs_valid) {
+#if defined(MULTIPOLE_INTEGRAL)
+    c.status = btam_mf_pair_terms_multipole(c.sys, rule, c.self5.data(), c.slot5.data(), ns);
+#else
+    c.status = btam_mf_pair_terms(c.sys, c.precision, c.self5.data(), c.slot5.data(), ns);
+#endif
+    c.pairs_valid = c.status == BTAM_OK;
+  }
   if ((what & kPoint) && !c.pt_valid) {
-    c.status = btam_pt_eval(c.sys, c.pt_rho.data(), nullptr, c.pt_Fq.data(), c.pt_W.data(),
-                            nullptr);
+    c.status = btam_pt_eval(c.sys, c.pt_rho.data(), nullptr, nullptr, c.pt_W.data(), nullptr);
     c.pt_valid = c.status == BTAM_OK;
+  }
+  if ((what & kPointPairs) && !c.ptp_valid) {
+    c.status = btam_pt_pair_terms(c.sys, c.pt_self3.data(), c.pt_slot3.data(),
+                                  c.pt_Hself.data(), c.pt_Hslot.data(), ns);
+    c.ptp_valid = c.status == BTAM_OK;
   }
   if ((what & kStress) && !c.mfs_valid) {
 #if defined(MULTIPOLE_INTEGRAL)
-#ifdef NUMERICAL_DERIVATIVES
-    c.status = btam_mf_stress_multipole(c.sys, BTAM_MP_FD, c.mf_W.data(), nullptr);
-#else
-    c.status = btam_mf_stress_multipole(c.sys, BTAM_MP_ANALYTIC, c.mf_W.data(), nullptr);
-#endif
+    c.status = btam_mf_stress_multipole(c.sys, rule, c.mf_W.data(), nullptr);
 #else
     c.status = btam_mf_stress(c.sys, c.precision, c.mf_W.data(), nullptr);
 #endif
     c.mfs_valid = c.status == BTAM_OK;
   }
-  if ((what & kHessian) && !c.pth_valid) {
-    c.status = btam_pt_hessian(c.sys, c.pt_H.data());
-    c.pth_valid = c.status == BTAM_OK;
-  }
   if ((what & kMfHessian) && !c.mfh_valid) {
 #if defined(MULTIPOLE_INTEGRAL)
-#ifdef NUMERICAL_DERIVATIVES
-    c.status = btam_mf_hessian_multipole(c.sys, BTAM_MP_FD, c.mf_H.data());
+    c.status = btam_mf_hessian_pairs_multipole(c.sys, rule, c.mf_Hself.data(),
+                                               c.mf_Hslot.data(), ns);
 #else
-    c.status = btam_mf_hessian_multipole(c.sys, BTAM_MP_ANALYTIC, c.mf_H.data());
-#endif
-#else
-    c.status = btam_mf_hessian(c.sys, c.mf_H.data());
+    c.status = btam_mf_hessian_pairs(c.sys, c.mf_Hself.data(), c.mf_Hslot.data(), ns);
 #endif
     c.mfh_valid = c.status == BTAM_OK;
   }
+}
+
+// Component c of the per-pair value (u, i) of width w: the self term of u's
+// owner, the list entry, 0 when i does not neighbour u, NaN when the values
+// are not valid or an index is out of range.
+inline double pair_value(const Cache &c, bool valid, const std::vector<double> &self,
+                         const std::vector<double> &slot, int w, unsigned u, unsigned i,
+                         int comp) {
+  const int u0 = owner_of(c, u);
+  if (!valid || u0 < 0 || owner_of(c, i) < 0) return NAN;
+  const long long e = entry_of(c, u, i);
+  if (e == -1) return self[(size_t)w * u0 + comp];
+  if (e < 0) return 0.0;
+  return slot[(size_t)w * e + comp];
 }
 
 // A stress W taken at q0 = q, at reference positions mean_q0, which must be
 // the bound positions (the cell's stretch F maps them to q): W(a, b) / F_b.
 template <class M>
 inline Eigen::Matrix3d stress_at_q0(Cache &c, const std::vector<double> &Wq, bool valid,
-                                    unsigned i, const M &mean_q0, const AtomTopology &topo) {
-  bool ok = valid && (int)i < c.n;
+                                    unsigned i, const M &mean_q0) {
+  const int i0 = owner_of(c, i);
+  bool ok = valid && i0 >= 0 && (int)i < c.n;
   auto bound = [&](int j) {
     if (j < 0 || j >= c.n) return true;
     for (int k = 0; k < 3; ++k)
       if (mean_q0(j, k) != c.q_bind[3 * (size_t)j + k]) return false;
     return true;
   };
-  ok = ok && bound((int)i);
-  for (int k = 0; ok && k < topo.numneigh; ++k) ok = bound((int)topo.mech_neighs_ptr[k]);
+  ok = ok && bound(i0);
+  for (int p = ok ? c.offs[i0] : 0; ok && p < c.offs[i0 + 1]; ++p) ok = bound(c.owner[c.idx[p]]);
   if (valid && !ok) c.status = BTAM_ERR_ARG;
   Eigen::Matrix3d W;
   for (int a = 0; a < 3; ++a)
@@ -285,162 +357,143 @@ inline Eigen::Matrix3d stress_at_q0(Cache &c, const std::vector<double> &Wq, boo
   return W;
 }
 
-// Assembled sigma derivative of V0 (the residual without its entropy term
-// -3 / (beta sigma)).
-inline double dV0_dsigma(const Cache &c, int u) {
-  return c.Rs[u] + 3.0 / (c.beta[u] * c.sigma[u]);
-}
-
-// Assembled occupancy derivative of V0 at an H site (R_x without its
-// entropy and chemical terms); Mg sites (and empty sites) carry none.
-inline double dV0_dx(const Cache &c, int u, bool hydrogen) {
-  const double xu = c.x[u];
-  if (!hydrogen || !(xu >= BTAM_MIN_OCCUPANCY)) return 0.0;
-  const double dlogz = 3.0 / (2.0 * xu) + (xu < 1.0 ? 1.0 / (1.0 - xu) : 0.0);
-  return c.Rx[u] + dlogz / c.beta[u] + (xu < 0.9999 ? c.gamma[u] / c.beta[u] : 0.0);
+inline double site_value(const Cache &c, bool valid, const std::vector<double> &v, unsigned i) {
+  const int i0 = owner_of(c, i);
+  return valid && i0 >= 0 ? v[i0] : NAN;
 }
 
 inline double rho_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::VectorXd &xi,
-                    const AtomicSpecie *, const AtomTopology topo) {
+                    const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, topo, kPoint);
-  return c.pt_valid && (int)i < c.n ? c.pt_rho[i] : NAN;
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, kPoint);
+  return site_value(c, c.pt_valid, c.pt_rho, i);
 }
 
 inline Eigen::Vector3d DV_Dq(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                              const Eigen::VectorXd &xi, const Eigen::VectorXd &,
-                             const AtomicSpecie *, const AtomTopology topo) {
+                             const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, u, i, mean_q, nullptr, xi, topo, kPoint);
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, u, i, mean_q, nullptr, xi, kPointPairs);
   Eigen::Vector3d g;
-  for (int k = 0; k < 3; ++k)
-    g(k) = !c.pt_valid || (int)u >= c.n ? NAN : (u == i ? c.pt_Fq[3 * (size_t)u + k] : 0.0);
+  for (int k = 0; k < 3; ++k) g(k) = pair_value(c, c.ptp_valid, c.pt_self3, c.pt_slot3, 3, u, i, k);
   return g;
 }
 
 inline Eigen::Matrix3d D2V_Dq2(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                                const Eigen::VectorXd &xi, const Eigen::VectorXd &,
-                               const AtomicSpecie *, const AtomTopology topo) {
+                               const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, u, i, mean_q, nullptr, xi, topo, kHessian);
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, u, i, mean_q, nullptr, xi, kPointPairs);
   Eigen::Matrix3d H;
-  const bool ok = c.pth_valid && (int)u < c.n;
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b)
-      H(a, b) = !ok ? NAN : (u == i ? c.pt_H[9 * (size_t)u + 3 * a + b] : 0.0);
+      H(a, b) = pair_value(c, c.ptp_valid, c.pt_Hself, c.pt_Hslot, 9, u, i, 3 * a + b);
   return H;
 }
 
 inline Eigen::Matrix3d D2V0_Dmeanq2(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                                     const Eigen::VectorXd &stdv_q, const Eigen::VectorXd &xi,
                                     const Eigen::VectorXd &, const AtomicSpecie *,
-                                    const AtomTopology topo) {
+                                    const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMfHessian);
+  refresh(c, u, i, mean_q, &stdv_q, xi, kMfHessian);
   Eigen::Matrix3d H;
-  const bool ok = c.mfh_valid && (int)u < c.n;
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b)
-      H(a, b) = !ok ? NAN : (u == i ? c.mf_H[9 * (size_t)u + 3 * a + b] : 0.0);
+      H(a, b) = pair_value(c, c.mfh_valid, c.mf_Hself, c.mf_Hslot, 9, u, i, 3 * a + b);
   return H;
 }
 
 inline Eigen::Matrix3d DV_DF(unsigned i, const Eigen::MatrixXd &mean_q,
                              const Eigen::MatrixXd &mean_q0, const Eigen::VectorXd &xi,
                              const Eigen::VectorXd &, const AtomicSpecie *,
-                             const AtomTopology topo) {
+                             const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, topo, kPoint);
-  return stress_at_q0(c, c.pt_W, c.pt_valid, i, mean_q0, topo);
+  refresh<Eigen::MatrixXd, Eigen::VectorXd>(c, i, i, mean_q, nullptr, xi, kPoint);
+  return stress_at_q0(c, c.pt_W, c.pt_valid, i, mean_q0);
 }
 
 inline Eigen::Matrix3d DV0_DF(unsigned i, const Eigen::MatrixXd &mean_q,
                               const Eigen::MatrixXd &mean_q0, const Eigen::VectorXd &stdv_q,
                               const Eigen::VectorXd &xi, const Eigen::VectorXd &,
-                              const AtomicSpecie *, const AtomTopology topo) {
+                              const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kStress);
-  return stress_at_q0(c, c.mf_W, c.mfs_valid, i, mean_q0, topo);
+  refresh(c, i, i, mean_q, &stdv_q, xi, kStress);
+  return stress_at_q0(c, c.mf_W, c.mfs_valid, i, mean_q0);
 }
 
 inline double mf_rho_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::VectorXd &stdv_q,
-                       const Eigen::VectorXd &xi, const AtomicSpecie *, const AtomTopology topo) {
+                       const Eigen::VectorXd &xi, const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kMeanField);
-  return c.valid && (int)i < c.n ? c.rho[i] : NAN;
+  refresh(c, i, i, mean_q, &stdv_q, xi, kMeanField);
+  return site_value(c, c.valid, c.rho, i);
 }
 
 inline double V0_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::VectorXd &stdv_q,
                    const Eigen::VectorXd &xi, const Eigen::VectorXd &, const AtomicSpecie *,
-                   const AtomTopology topo) {
+                   const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kMeanField);
-  return c.valid && (int)i < c.n ? c.V0[i] : NAN;
+  refresh(c, i, i, mean_q, &stdv_q, xi, kMeanField);
+  return site_value(c, c.valid, c.V0, i);
 }
 
 inline double S0_i(unsigned i, const Eigen::MatrixXd &mean_q, const Eigen::VectorXd &stdv_q,
                    const Eigen::VectorXd &xi, const Eigen::VectorXd &, const Eigen::VectorXd &,
-                   const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology topo) {
+                   const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, i, i, mean_q, &stdv_q, xi, topo, kMeanField);
-  return c.valid && (int)i < c.n ? c.S0[i] : NAN;
+  refresh(c, i, i, mean_q, &stdv_q, xi, kMeanField);
+  return site_value(c, c.valid, c.S0, i);
 }
 
 inline Eigen::Vector3d DV0_Dmeanq(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                                   const Eigen::VectorXd &stdv_q, const Eigen::VectorXd &xi,
                                   const Eigen::VectorXd &, const AtomicSpecie *,
-                                  const AtomTopology topo) {
+                                  const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
+  refresh(c, u, i, mean_q, &stdv_q, xi, kPairs);
   Eigen::Vector3d g;
-  for (int k = 0; k < 3; ++k)
-    g(k) = !c.valid || (int)u >= c.n ? NAN : (u == i ? c.Rq[3 * (size_t)u + k] : 0.0);
+  for (int k = 0; k < 3; ++k) g(k) = pair_value(c, c.pairs_valid, c.self5, c.slot5, 5, u, i, k);
   return g;
 }
 
 inline double DV0_Dstdvq(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                          const Eigen::VectorXd &stdv_q, const Eigen::VectorXd &xi,
-                         const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology topo) {
+                         const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
-  if (!c.valid || (int)u >= c.n) return NAN;
-  return u == i ? dV0_dsigma(c, (int)u) : 0.0;
+  refresh(c, u, i, mean_q, &stdv_q, xi, kPairs);
+  return pair_value(c, c.pairs_valid, c.self5, c.slot5, 5, u, i, 3);
 }
 
 inline Eigen::Vector4d DV0_Dq(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                               const Eigen::VectorXd &stdv_q, const Eigen::VectorXd &xi,
                               const Eigen::VectorXd &, const AtomicSpecie *,
-                              const AtomTopology topo) {
+                              const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
+  refresh(c, u, i, mean_q, &stdv_q, xi, kPairs);
   Eigen::Vector4d g;
-  const bool ok = c.valid && (int)u < c.n;
-  for (int k = 0; k < 3; ++k) g(k) = !ok ? NAN : (u == i ? c.Rq[3 * (size_t)u + k] : 0.0);
-  g(3) = !ok ? NAN : (u == i ? dV0_dsigma(c, (int)u) : 0.0);
+  for (int k = 0; k < 4; ++k) g(k) = pair_value(c, c.pairs_valid, c.self5, c.slot5, 5, u, i, k);
   return g;
 }
 
 inline double DV0_Dxi(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
                       const Eigen::VectorXd &stdv_q, const Eigen::VectorXd &xi,
-                      const Eigen::VectorXd &, const AtomicSpecie *specie,
-                      const AtomTopology topo) {
+                      const Eigen::VectorXd &, const AtomicSpecie *, const AtomTopology) {
   Cache &c = cache();
   std::lock_guard<std::mutex> lock(c.mu);
-  refresh(c, u, i, mean_q, &stdv_q, xi, topo, kMeanField);
-  if (!c.valid || (int)u >= c.n) return NAN;
-  return u == i ? dV0_dx(c, (int)u, specie && (int)specie[u] == 1) : 0.0;  // 1: H
+  refresh(c, u, i, mean_q, &stdv_q, xi, kPairs);
+  return pair_value(c, c.pairs_valid, c.self5, c.slot5, 5, u, i, 4);
 }
 
 }  // namespace detail

@@ -9,6 +9,7 @@
 // Build: oracle/Makefile (-O2 -ffp-contract=off, IEEE double).
 #include "btam_oracle.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1559,21 +1560,21 @@ void orc_residuals(int n, const double *q, const double *sigma,
 // Hydrogen master-equation update (project definition; the reference keeps
 // only the parameters, Variables.hpp:68-92).  Sequential restatement of
 // btam_dmd_step's integer update.
-void orc_dmd_update(int n, const int *code_all, const int *owner, const double *x_all,
-                    const double *beta, const double *mu, const int *moffs,
-                    const int *midx, const int *doffs, const int *didx,
-                    const double *params, long long *X) {
-  const double q = 8.8817841970012523e-16, invq = 1125899906842624.0;
-  const double dt = params[0], Df = params[1], dr = params[2], min_dx = params[3],
-               max_x = params[4];
-  std::vector<int> active(n, 0);
-  std::vector<long long> deg(n, 0), X0(X, X + n);
+// Diffusive activity and degrees of the real H sites (shared by the update
+// and the step-control decision).
+static void orc_dmd_active(int n, const int *code_all, const int *owner, const double *x_all,
+                           const int *moffs, const int *midx, const int *doffs,
+                           const int *didx, const long long *X, std::vector<int> &active,
+                           std::vector<long long> &deg) {
+  const double q = 8.8817841970012523e-16;
+  active.assign(n, 0);
+  deg.assign(n, 0);
   // diffusive activity: x_i plus the occupancy of its H mechanical
   // neighbours reaches 0.01 (list_of_active_diffusive_sites_MgHx,
   // Topology.cpp:202-364)
   for (int i = 0; i < n; ++i) {
     if (code_all[i] != 1) continue;
-    double mass = (double)X0[i] * q;
+    double mass = (double)X[i] * q;
     for (int p = moffs[i]; p < moffs[i + 1]; ++p)
       if (code_all[midx[p]] == 1) mass += x_all[midx[p]];
     active[i] = mass >= 0.01;
@@ -1581,6 +1582,65 @@ void orc_dmd_update(int n, const int *code_all, const int *owner, const double *
   for (int i = 0; i < n; ++i)
     if (active[i])
       for (int p = doffs[i]; p < doffs[i + 1]; ++p) deg[i] += active[owner[didx[p]]];
+}
+
+// The room of edge (i, o) in quanta under the degree split.
+static void orc_dmd_room(const long long *X, const std::vector<long long> &deg, int i, int o,
+                         long long xmax, long long &hi, long long &lo) {
+  long long di = deg[i] > 0 ? deg[i] : 1, dq = deg[o] > 0 ? deg[o] : 1;
+  long long out_i = X[i] / di, out_o = X[o] / dq;
+  long long in_i = xmax > X[i] ? (xmax - X[i]) / di : 0;
+  long long in_o = xmax > X[o] ? (xmax - X[o]) / dq : 0;
+  hi = out_i < in_o ? out_i : in_o;
+  lo = -(out_o < in_i ? out_o : in_i);
+}
+
+void orc_dmd_control(int n, const int *code_all, const int *owner, const double *x_all,
+                     const double *beta, const double *mu, const int *moffs, const int *midx,
+                     const int *doffs, const int *didx, const double *params, double max_dx,
+                     const long long *X, double *out2) {
+  const double q = 8.8817841970012523e-16, invq = 1125899906842624.0;
+  const double dt = params[0], Df = params[1], dr = params[2], min_dx = params[3],
+               max_x = params[4];
+  std::vector<int> active;
+  std::vector<long long> deg;
+  orc_dmd_active(n, code_all, owner, x_all, moffs, midx, doffs, didx, X, active, deg);
+  const long long xmax = llrint(max_x * invq);
+  double ratio = 0.0, worst_dx = 0.0;
+  for (int i = 0; i < n; ++i) {
+    if (!active[i]) continue;
+    double dx = 0.0;
+    for (int p = doffs[i]; p < doffs[i + 1]; ++p) {
+      int o = owner[didx[p]];
+      if (o == i || !active[o]) continue;
+      double xi = (double)X[i] * q, xo = (double)X[o] * q;
+      double xm = 0.5 * (xi + xo), bm = 0.5 * (beta[i] + beta[o]);
+      double J = Df / (dr * dr) * bm * xm * (1.0 - xm) * (mu[i] - mu[o]);
+      double dlt = dt * J;
+      if (std::fabs(dlt) < min_dx) continue;
+      dx -= dlt;
+      if (o < i) continue;
+      long long qn = llrint(dlt * invq), hi, lo;
+      orc_dmd_room(X, deg, i, o, xmax, hi, lo);
+      if (qn > hi && hi > 0) ratio = std::max(ratio, (double)qn / (double)hi);
+      if (qn < lo && lo < 0) ratio = std::max(ratio, (double)qn / (double)lo);
+    }
+    worst_dx = std::max(worst_dx, std::fabs(dx) / max_dx);
+  }
+  out2[0] = ratio;
+  out2[1] = worst_dx;
+}
+
+void orc_dmd_update(int n, const int *code_all, const int *owner, const double *x_all,
+                    const double *beta, const double *mu, const int *moffs,
+                    const int *midx, const int *doffs, const int *didx,
+                    const double *params, long long *X, long long *clipped) {
+  const double q = 8.8817841970012523e-16, invq = 1125899906842624.0;
+  const double dt = params[0], Df = params[1], dr = params[2], min_dx = params[3],
+               max_x = params[4];
+  std::vector<int> active;
+  std::vector<long long> deg, X0(X, X + n);
+  orc_dmd_active(n, code_all, owner, x_all, moffs, midx, doffs, didx, X0.data(), active, deg);
   const long long xmax = llrint(max_x * invq);
   for (int i = 0; i < n; ++i) {
     if (!active[i]) continue;
@@ -1592,13 +1652,9 @@ void orc_dmd_update(int n, const int *code_all, const int *owner, const double *
       double J = Df / (dr * dr) * bm * xm * (1.0 - xm) * (mu[i] - mu[o]);
       double dlt = dt * J;
       if (std::fabs(dlt) < min_dx) continue;
-      long long qn = llrint(dlt * invq);
-      long long di = deg[i] > 0 ? deg[i] : 1, dq = deg[o] > 0 ? deg[o] : 1;
-      long long out_i = X0[i] / di, out_o = X0[o] / dq;
-      long long in_i = xmax > X0[i] ? (xmax - X0[i]) / di : 0;
-      long long in_o = xmax > X0[o] ? (xmax - X0[o]) / dq : 0;
-      long long hi = out_i < in_o ? out_i : in_o;
-      long long lo = -(out_o < in_i ? out_o : in_i);
+      long long qn = llrint(dlt * invq), hi, lo;
+      orc_dmd_room(X0.data(), deg, i, o, xmax, hi, lo);
+      if (clipped && ((qn > hi && hi > 0) || (qn < lo && lo < 0))) ++*clipped;
       qn = qn > hi ? hi : (qn < lo ? lo : qn);
       X[i] -= qn;
       X[o] += qn;

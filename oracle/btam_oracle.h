@@ -130,11 +130,20 @@ void orc_residuals(int n, const double *q, const double *sigma,
  * potentials; x_all/code_all/owner the all-sites occupancy, species code
  * (0 Mg, 1 H) and owner; moffs/midx the mechanical neighbours and
  * doffs/didx the diffusive neighbours of the real sites; params as
- * btam_dmd_step (dt, Df, dr, min_dx, max_x). */
+ * btam_dmd_step (dt, Df, dr, min_dx, max_x).  clipped (may be NULL) counts
+ * the edge moves cut to a nonzero room. */
 void orc_dmd_update(int n, const int *code_all, const int *owner, const double *x_all,
                     const double *beta, const double *mu, const int *moffs,
                     const int *midx, const int *doffs, const int *didx,
-                    const double *params, long long *X);
+                    const double *params, long long *X, long long *clipped);
+/* The step-control decision of btam_dmd_step_ctl for a step of params[0]
+ * at the quanta X (same arguments as orc_dmd_update): out2[0] the largest
+ * edge move over its nonzero room, out2[1] the largest site change over
+ * max_dx (project definition). */
+void orc_dmd_control(int n, const int *code_all, const int *owner, const double *x_all,
+                     const double *beta, const double *mu, const int *moffs, const int *midx,
+                     const int *doffs, const int *didx, const double *params, double max_dx,
+                     const long long *X, double *out2);
 
 #ifdef __cplusplus
 }

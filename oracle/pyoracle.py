@@ -343,23 +343,44 @@ def diffusive_graph(q_all, species_all, n_real, rc=2.6, maxn=50):
     return offs, np.array(out, np.int32)
 
 
-def dmd_update(oracle, X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx, params):
-    """One master-equation update of the quanta X (copy returned)."""
-    X = np.ascontiguousarray(X, np.int64).copy()
-    n = len(X)
-    L = oracle.lib
-    f = L.orc_dmd_update
-    f.restype = None
-    code_all = np.ascontiguousarray(code_all, np.int32)
-    owner = np.ascontiguousarray(owner, np.int32)
-    x_all = np.ascontiguousarray(x_all, np.float64)
-    beta = np.ascontiguousarray(beta, np.float64)
-    mu = np.ascontiguousarray(mu, np.float64)
+def _dmd_args(X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx, params):
+    arrs = [np.ascontiguousarray(a, np.int32) for a in (code_all, owner)]
+    darr = [np.ascontiguousarray(a, np.float64) for a in (x_all, beta, mu)]
+    graph = [np.ascontiguousarray(a, np.int32) for a in (moffs, midx, doffs, didx)]
     prm = np.ascontiguousarray(params, np.float64)
-    arrs = [np.ascontiguousarray(a, np.int32) for a in (moffs, midx, doffs, didx)]
-    f(n, _i(code_all), _i(owner), _d(x_all), _d(beta), _d(mu), *[_i(a) for a in arrs],
-      _d(prm), X.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)))
-    return X
+    keep = arrs + darr + graph + [prm]
+    args = [len(X), _i(arrs[0]), _i(arrs[1]), _d(darr[0]), _d(darr[1]), _d(darr[2]),
+            *[_i(a) for a in graph], _d(prm)]
+    return args, keep
+
+
+def dmd_update(oracle, X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx, params,
+               count_clips=False):
+    """One master-equation update of the quanta X (copy returned; with
+    count_clips, also the number of edge moves cut to a nonzero room)."""
+    X = np.ascontiguousarray(X, np.int64).copy()
+    f = oracle.lib.orc_dmd_update
+    f.restype = None
+    args, keep = _dmd_args(X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx,
+                           params)
+    clipped = ctypes.c_longlong(0)
+    f(*args, X.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)), ctypes.byref(clipped))
+    return (X, clipped.value) if count_clips else X
+
+
+def dmd_control(oracle, X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx, params,
+                max_dx):
+    """The step-control ratios (edge move over room, site change over
+    max_dx) of a step of params[0] at the quanta X."""
+    X = np.ascontiguousarray(X, np.int64)
+    f = oracle.lib.orc_dmd_control
+    f.restype = None
+    args, keep = _dmd_args(X, code_all, owner, x_all, beta, mu, moffs, midx, doffs, didx,
+                           params)
+    out = np.zeros(2)
+    f(*args, ctypes.c_double(max_dx), X.ctypes.data_as(ctypes.POINTER(ctypes.c_longlong)),
+      _d(out))
+    return out
 
 
 def residuals_on_topology(oracle, real, q_ghost, owner_ghost, image_ghost, offs_real, idx,

@@ -15,6 +15,8 @@ Run from the repository root, with the reference tree present:
                                                   # the system fixtures)
     python tests/golden/make_golden.py --multipole  # multipole.npz only (it
                                                     # reads the system fixtures)
+    python tests/golden/make_golden.py --pairs    # pairs.npz only (it reads
+                                                  # the system fixtures)
 """
 import os
 import sys
@@ -27,7 +29,9 @@ import pyoracle  # noqa: E402
 from btam import dump, lattice  # noqa: E402
 
 OUT = os.path.dirname(os.path.abspath(__file__))
-REF_TREE = os.environ.get("BTAM_REFERENCE", "/root/reference")
+# the reference tree: $BTAM_REFERENCE, else a checkout named "reference" beside
+# this repository
+REF_TREE = os.environ.get("BTAM_REFERENCE", os.path.join(os.path.dirname(ROOT), "reference"))
 
 
 def residual_pairs(full, owner, image, offs, idx, us):
@@ -219,8 +223,114 @@ def multipole_fixture():
     np.savez_compressed(os.path.join(OUT, "multipole.npz"), **out)
 
 
+def pair_plan(owner, image, offs, idx, us):
+    """For each u in us, its self entry and every entry p of its list (the
+    neighbour ic = idx[p]): (k, entry, uu, o) with entry -1 for the self
+    entry and p otherwise, and (uu, o) the argument pair the reference
+    evaluates for it: o = owner(ic), uu = u for a real ic, else the image of
+    u in o's list with the opposite shift."""
+    plan = []
+    for k, u in enumerate(us):
+        plan.append((k, -1, int(u), int(u)))
+        for p in range(offs[u], offs[u + 1]):
+            ic = idx[p]
+            o = owner[ic]
+            T = image[ic]
+            uu = int(u)
+            if np.any(T != 0):
+                uu = -1
+                for cand in idx[offs[o]:offs[o + 1]]:
+                    if owner[cand] == u and np.all(image[cand] == -T):
+                        uu = int(cand)
+                        break
+                if uu < 0:
+                    raise RuntimeError("asymmetric neighbour lists")
+            plan.append((k, p, uu, int(o)))
+    return plan
+
+
+def pairs_fixture(ref, orc):
+    """The reference's per-pair functions, one (u, i) call at a time, on a
+    sample of sites of each system fixture and of a cell with per-site
+    temperatures (beta varies from site to site): evaluate_DV0_i_Dq_u_MgHx
+    and evaluate_DV0_i_Dxi_u_adp_MgHx (g4, gx), evaluate_DV_i_Dq_u_adp_MgHx
+    (pt_g3), evaluate_D2V_i_Dq2_u_MgHx (pt_h9) and
+    evaluate_D2V0_i_Dmeanq2_u_MgHx (mf_h9), for the self entry and every
+    list entry of each sampled site."""
+    out = {}
+    systems = {}
+    for name in ("sphere", "x5cube", "ortho_mgh", "config1"):
+        g = dict(np.load(os.path.join(OUT, f"{name}.npz")))
+        systems[name] = g
+    # a periodic Mg-H cell whose sites carry temperatures T ~ U[300, 600] K
+    hot = lattice.supercell(4, 3, 3, ortho=True, h_fraction=0.4, x_range=(0.0, 0.5),
+                            sigma_range=(0.08, 0.15), jitter=0.02, seed=9)
+    rng = np.random.default_rng(9)
+    hot["beta"] = 1.0 / (8.617332478e-5 * rng.uniform(300.0, 600.0, len(hot["x"])))
+    full, n, owner, image = pyoracle.expand(hot, orc)
+    offs, idx = orc.neighbors(full["q"])
+    real = np.arange(n, dtype=np.int32)
+    rho_real = ref.mf_rho(full, offs, idx, real)
+    us = np.sort(rng.choice(n, 16, replace=False)).astype(np.int32)
+    Rq, Rs, Rx = assemble(ref, full, rho_real[owner], owner, image, offs, idx, us)
+    g = {k: hot[k] for k in ("q", "sigma", "x", "species", "beta", "gamma", "origin", "cell",
+                             "periodic")}
+    g.update(q_all=full["q"], owner=owner, image=image, offs=offs, idx=idx, rho=rho_real,
+             rho_nmf=ref.rho_nmf(full, offs, idx, real), res_sites=us, Rq=Rq, Rs=Rs, Rx=Rx,
+             V0=ref.V0(full, rho_real[owner], offs, idx, real))
+    systems["hot_cell"] = g
+    for name, g in systems.items():
+        n = len(g["x"])
+        owner, image, offs, idx = g["owner"], g["image"], g["offs"], g["idx"]
+        full = {"q": np.ascontiguousarray(g["q_all"]),
+                "sigma": np.ascontiguousarray(g["sigma"][owner]),
+                "x": np.ascontiguousarray(g["x"][owner]),
+                "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+        rng = np.random.default_rng(len(name))
+        act = np.flatnonzero(g["x"] >= 5e-4)
+        pick = [act[g["species"][act] == sp] for sp in (12, 1)]
+        us = np.concatenate([rng.choice(p_, min(len(p_), 6), replace=False)
+                             for p_ in pick if len(p_)])
+        empty = np.flatnonzero(g["x"] < 5e-4)
+        if len(empty):
+            us = np.append(us, empty[0])  # an empty site: every value is 0
+        us = np.sort(us).astype(np.int32)
+        plan = pair_plan(owner, image, offs, idx, us)
+        uu = np.array([p_[2] for p_ in plan], np.int32)
+        oo = np.array([p_[3] for p_ in plan], np.int32)
+        g4, gx = ref.DV0_pairs(full, g["rho"][owner], offs, idx, uu, oo)
+        pt_g3 = ref.pt_DV_pairs(full, g["rho_nmf"][owner], offs, idx, uu, oo)
+        pt_h9 = ref.pt_D2V_pairs(full, g["rho_nmf"][owner], offs, idx, uu, oo)
+        mf_h9 = ref.mf_D2V0_pairs(full, g["rho"][owner], offs, idx, uu, oo)
+        out.update({f"{name}_us": us,
+                    f"{name}_k": np.array([p_[0] for p_ in plan], np.int32),
+                    f"{name}_entry": np.array([p_[1] for p_ in plan], np.int32),
+                    f"{name}_uu": uu, f"{name}_oo": oo,
+                    f"{name}_g4": g4, f"{name}_gx": gx, f"{name}_pt_g3": pt_g3,
+                    f"{name}_pt_h9": pt_h9, f"{name}_mf_h9": mf_h9})
+        if name == "hot_cell":
+            out.update({f"hot_cell_{k}": v for k, v in g.items()})
+        # the same pairs under the multipole rule, from the reference built
+        # with it (rule 1: the reference's own finite-difference Hessians;
+        # rule 2: analytic), at the rule's rho-bar
+        if name in ("sphere", "ortho_mgh"):
+            for rule, analytic in ((1, False), (2, True)):
+                refm = pyoracle.reference_multipole(analytic)
+                real = np.arange(n, dtype=np.int32)
+                rho_mp = refm.mf_rho(full, offs, idx, real)
+                m4, mx = refm.DV0_pairs(full, rho_mp[owner], offs, idx, uu, oo)
+                mh = refm.mf_D2V0_pairs(full, rho_mp[owner], offs, idx, uu, oo)
+                out.update({f"{name}_mp{rule}_g4": m4, f"{name}_mp{rule}_gx": mx,
+                            f"{name}_mp{rule}_h9": mh})
+        print(f"pairs {name}: {len(us)} sites, {len(plan)} pairs")
+    np.savez_compressed(os.path.join(OUT, "pairs.npz"), **out)
+
+
 def main():
     ref = pyoracle.reference()
+    if ref is not None and sys.argv[1:] == ["--pairs"]:
+        pairs_fixture(ref, pyoracle.Oracle())
+        return
     if ref is not None and sys.argv[1:] == ["--point"]:
         point_fixture(ref)
         return
@@ -281,6 +391,7 @@ def main():
     system_fixture("config1", lattice.config1(), ref, orc, residual_sample=40, seed=1)
     point_fixture(ref)
     multipole_fixture()
+    pairs_fixture(ref, orc)
 
 
 if __name__ == "__main__":

@@ -311,3 +311,39 @@ def test_full_size_config2(gpu_tables, oracle):
             E.append(S.evaluate(btam.FP64)["totals"][0])
         S.set_state(q=s["q"])
         assert abs((E[0] - E[1]) / (2 * h) - a["Rq"][site, ax]) < 1e-5
+
+
+def test_full_size_config3_nanowire(gpu_tables, oracle):
+    """Precision workload (hcp Mg nanowire R = 30 A, 20 cells, periodic along
+    the axis only, 38 040 sites with free surfaces): the FP32C form against
+    the FP64 form at the form's stated tolerance on every result, the FP64
+    form against sampled literal residuals of the oracle, and translation
+    invariance (T is uniform, so sum_u R_q(u) is the gradient of the total
+    energy under a rigid shift)."""
+    import pyoracle
+    s = lattice.config3()
+    n = len(s["x"])
+    assert n == 38040
+    S = btam.System(gpu_tables, s)
+    S.build_neighbors()
+    a = S.evaluate(btam.FP64)
+    b = S.evaluate(btam.FP32C)
+    E64, E32 = a["totals"][0], b["totals"][0]
+    assert abs(E32 - E64) <= 1e-6 * abs(E64)
+    assert np.max(np.abs(b["V0"] - a["V0"])) <= 1e-5
+    assert np.max(np.abs(b["Rq"] - a["Rq"])) <= 1e-5
+    assert np.max(np.abs(b["Rs"] - a["Rs"])) <= 1e-5
+    assert np.max(np.abs(b["Rx"] - a["Rx"])) <= 1e-5 * max(1.0, np.abs(a["Rx"]).max())
+    assert np.abs(a["Rq"].sum(axis=0)).max() < 1e-8
+    # surface and core sites of both species
+    r = np.hypot(s["q"][:, 0] - s["q"][:, 0].mean(), s["q"][:, 1] - s["q"][:, 1].mean())
+    picks = []
+    for sp in (12, 1):
+        m = s["species"] == sp
+        picks += [np.flatnonzero(m & (r < 10.0))[0], np.flatnonzero(m & (r > 27.0))[0],
+                  np.flatnonzero(m & (r > 27.0))[-1]]
+    sites = np.array(sorted(set(map(int, picks))), np.int32)
+    lit = pyoracle.sampled_residuals(s, oracle, sites)
+    assert rel(a["V0"][sites], lit["V0"]) < 1e-10
+    for k in ("Rq", "Rs", "Rx"):
+        assert np.max(np.abs(a[k][sites] - lit[k])) < 1e-10 * max(1.0, np.abs(lit[k]).max()), k

@@ -141,6 +141,102 @@ def test_master_equation_matches_oracle_and_conserves(gpu_tables, oracle):
         assert np.any(X1 != Xb)
 
 
+def dmd_context(S, s, xb):
+    """The arguments the oracle's master-equation functions take, from a
+    device system and the occupancies xb of its real sites."""
+    n = len(s["x"])
+    qg, og, _ = S.ghosts()
+    owner = np.concatenate([np.arange(n), og]).astype(np.int32)
+    code_all = (s["species"][owner] == 1).astype(np.int32)
+    moffs, midx = S.neighbors()
+    doffs, didx = S.dmd_graph()
+    return dict(code_all=code_all, owner=owner, x_all=xb[owner], beta=s["beta"], moffs=moffs,
+                midx=midx, doffs=doffs, didx=didx)
+
+
+def test_master_equation_step_control_matches_oracle(gpu_tables, oracle):
+    """A controlled step: the device's decision equals the oracle's at the
+    same chemical potentials, the step equals m plain steps of dt / m (each
+    the oracle's update of its state), the clipped moves are the oracle's,
+    and total hydrogen is exact."""
+    import pyoracle
+    s = small_mgh(h=0.6, xr=(0.0, 0.6))
+    prm = dict(dt=2e-3, Df=0.045, dr=3.2, min_dx=1e-8, max_x=0.9)
+    plist = [prm[k] for k in ("dt", "Df", "dr", "min_dx", "max_x")]
+    A, B = (btam.System(gpu_tables, s) for _ in range(2))
+    for S in (A, B):
+        S.build_neighbors()
+        S.dmd_setup()
+    # the chemical potentials at the start (a step of dt = 0 moves nothing)
+    total0 = B.dmd_step(1, btam.FP64, **dict(prm, dt=0.0))
+    x0, X0, mu0 = B.dmd_occupancy()
+    ctx = dmd_context(B, s, x0)
+    r = pyoracle.dmd_control(oracle, X0, mu=mu0, params=plist, max_dx=1.0, **ctx)
+    # a site-change bound that needs several sub-steps
+    max_dx = r[1] / 3.5
+    r = pyoracle.dmd_control(oracle, X0, mu=mu0, params=plist, max_dx=max_dx, **ctx)
+    m = int(max(1, np.ceil(max(r))))
+    assert m >= 4
+    total, st = A.dmd_step_ctl(1, btam.FP64, max_dx=max_dx, **prm)
+    assert st["substeps"] == m and st["subdivided"] == 1 and total == total0
+    assert abs(st["worst_ratio"] - max(r)) <= 1e-12 * max(r)
+    clips = 0
+    for j in range(m):
+        xb, Xb, _ = B.dmd_occupancy()
+        B.dmd_step(1, btam.FP64, **dict(prm, dt=prm["dt"] / m))
+        _, X1, mu = B.dmd_occupancy()
+        Xo, c = pyoracle.dmd_update(oracle, Xb, mu=mu, params=[prm["dt"] / m] + plist[1:],
+                                    count_clips=True, **dmd_context(B, s, xb))
+        assert np.array_equal(Xo, X1), j
+        clips += c
+    _, XA, _ = A.dmd_occupancy()
+    assert np.array_equal(XA, X1)
+    assert st["clipped"] == clips and A.dmd_clip_count() == clips
+
+
+def test_master_equation_clipping_is_counted(gpu_tables, oracle):
+    """A step long enough that moves are cut to their room: the plain step
+    counts the cut moves as the oracle does; the controlled step divides it
+    until none is cut, and conserves hydrogen exactly."""
+    import pyoracle
+    s = small_mgh(h=0.8, xr=(0.0, 0.6), seed=13)
+    prm = dict(dt=0.5, Df=0.045, dr=3.2, min_dx=1e-8, max_x=0.9)
+    plist = [prm[k] for k in ("dt", "Df", "dr", "min_dx", "max_x")]
+    A, B = (btam.System(gpu_tables, s) for _ in range(2))
+    for S in (A, B):
+        S.build_neighbors()
+        S.dmd_setup()
+    xb, Xb, _ = B.dmd_occupancy()
+    total0 = B.dmd_step(1, btam.FP64, **prm)
+    _, X1, mu = B.dmd_occupancy()
+    Xo, c = pyoracle.dmd_update(oracle, Xb, mu=mu, params=plist, count_clips=True,
+                                **dmd_context(B, s, xb))
+    assert np.array_equal(Xo, X1) and c > 0 and B.dmd_clip_count() == c
+    total, st = A.dmd_step_ctl(1, btam.FP64, max_dx=1.0, max_sub=4096, **prm)
+    assert total == total0 and st["substeps"] > 1 and st["worst_ratio"] > 1.0
+    assert A.dmd_clip_count() == st["clipped"]
+
+
+def test_dmd_run_relaxes_between_steps(gpu_tables):
+    """btam_dmd_run equals its parts run by hand (controlled steps, then a
+    relaxation every k steps), bit for bit, and conserves hydrogen."""
+    s = small_mgh(h=0.6, xr=(0.05, 0.6), seed=17)
+    A, B = (btam.System(gpu_tables, s) for _ in range(2))
+    for S in (A, B):
+        S.build_neighbors()
+        S.dmd_setup()
+    total0 = B.dmd_step(0, btam.FP64)
+    total, st = A.dmd_run(6, btam.FP64, relax_every=3, relax_tol=1e-6, relax_max_iter=100,
+                          dt=1e-3)
+    assert total == total0 and st["relaxations"] == 2 and st["relax_evaluations"] > 0
+    for _ in range(2):
+        B.dmd_step_ctl(3, btam.FP64, dt=1e-3)
+        B.relax(mode=0, tol=1e-6, max_iter=100, m=8)
+    for a, b in zip(A.get_state(), B.get_state()):
+        assert np.array_equal(a, b)
+    assert np.array_equal(A.dmd_occupancy()[1], B.dmd_occupancy()[1])
+
+
 def test_master_equation_long_run_conserves_and_bounds(gpu_tables):
     s = small_mgh(h=0.8, xr=(0.0, 0.5), seed=9)
     S = btam.System(gpu_tables, s)
@@ -173,6 +269,10 @@ def test_master_equation_nanowire_conserves(gpu_tables):
     h = s["species"] == 1
     assert np.all(X[h] >= 0) and np.all(x[h] <= 0.9 + 1e-12) and np.all(np.isfinite(mu))
     assert np.abs(x[h] - s["x"][h]).max() > 0.0  # hydrogen moved
+    # the same steps with step control report what they did
+    total, st = S.dmd_step_ctl(20, btam.FP32C, dt=1e-3)
+    assert total == total0 and st["substeps"] >= 20
+    assert st["clipped"] >= 0 and np.isfinite(st["worst_ratio"])
 
 
 def test_master_equation_checkpoint_resume_bitwise(gpu_tables, tmp_path):

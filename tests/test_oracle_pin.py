@@ -272,3 +272,38 @@ def test_multipole_rule_matches_reference_live(oracle):
     assert np.array_equal(v1, ref.V0(full, r2, offs, idx, real))
     b4, bx = ref.DV0_pairs(full, r2, offs, idx, us, is_)
     assert np.array_equal(a4, b4) and np.array_equal(ax, bx)
+
+
+PAIR_SYSTEMS = ["sphere", "x5cube", "ortho_mgh", "config1", "hot_cell"]
+
+
+def pair_system(name):
+    """The full (real + image) arrays of a per-pair fixture system."""
+    p = load("pairs")
+    g = {k[len("hot_cell_"):]: v for k, v in p.items() if k.startswith("hot_cell_")} \
+        if name == "hot_cell" else load(name)
+    owner = g["owner"]
+    full = {"q": np.ascontiguousarray(g["q_all"]),
+            "sigma": np.ascontiguousarray(g["sigma"][owner]),
+            "x": np.ascontiguousarray(g["x"][owner]),
+            "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+    return p, g, full
+
+
+@pytest.mark.parametrize("name", PAIR_SYSTEMS)
+def test_pair_terms_against_golden(oracle, name):
+    """The oracle's per-pair functions, one (u, i) call at a time, reproduce
+    the reference's (evaluate_DV0_i_Dq_u, evaluate_DV0_i_Dxi_u,
+    evaluate_DV_i_Dq_u, evaluate_D2V_i_Dq2_u, evaluate_D2V0_i_Dmeanq2_u)."""
+    p, g, full = pair_system(name)
+    owner, offs, idx = g["owner"], g["offs"], g["idx"]
+    uu, oo = p[f"{name}_uu"], p[f"{name}_oo"]
+    g4, gx = oracle.DV0_pairs(full, g["rho"][owner], offs, idx, uu, oo)
+    assert np.array_equal(g4, p[f"{name}_g4"]) and np.array_equal(gx, p[f"{name}_gx"])
+    g3 = oracle.pt_DV_pairs(full, g["rho_nmf"][owner], offs, idx, uu, oo)
+    assert np.array_equal(g3, p[f"{name}_pt_g3"])
+    for key, fn, rho in (("pt_h9", oracle.pt_D2V_pairs, g["rho_nmf"]),
+                         ("mf_h9", oracle.mf_D2V0_pairs, g["rho"])):
+        h = fn(full, rho[owner], offs, idx, uu, oo)
+        ref_h = p[f"{name}_{key}"]
+        assert np.max(np.abs(h - ref_h)) <= 1e-14 * max(1.0, np.abs(ref_h).max()), key
