@@ -7,13 +7,15 @@ hexagonal cells (9000 Mg) with H on all 18000 tetrahedral sites
 T = 400 K; synthetic, seeded.  Neighbour lists are built once before timing
 (the reference also builds them once, main-BT-AM.cpp:100-104).
 
-Default arm (--impl btam): the FP32-compensated form is the headline
-`value`; the plain FP64 drop-in on the same system is reported beside it.
-`e2e` times the same evaluation through the C ABI with host buffers
-(pinned), including the host->device state copy and the device->host
-residual read.  Reference arm (--impl reference): the reference's own CPU
-arithmetic (oracle/_ref, -Ofast, all host threads) on a bounded sample of the
-same workload, extrapolated to one full evaluation.
+Default arm (--impl btam): the headline `value` is the FP64 drop-in (the
+reference's arithmetic type, autotuned kernels); `e2e` times the same FP64
+evaluation through the C ABI with host buffers (pinned), including the
+host->device state copy and the device->host residual read.  The
+FP32-compensated form is reported in its own `fp32c` record (value, e2e,
+error against the FP64 form, ratios), beside the plain two-pass FP64 kernel
+pair.  Reference arm (--impl reference): the reference's own CPU arithmetic
+(oracle/_ref, -Ofast, all host threads) on a bounded sample of the same
+workload, extrapolated to one full evaluation and labelled as such.
 
 Multi-GPU (torchrun): every rank evaluates its own replica (independent
 systems, no data-path collective); value = evaluations of all ranks / max
@@ -54,6 +56,9 @@ NCU_L1_SECTORS = {"pass1 pair-rule kernel": 51.73e6, "pass1 site kernel": 54.59e
                   "pass2 pair kernel": 28.55e6, "pass2 site kernel": 2.56e6}
 NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.71,
                "pass2 pair kernel": 0.69, "pass2 site kernel": 0.31}
+# DRAM bytes (read + write) per launch of the FP64 kernels on this workload
+# (autotuned variants), from one ncu capture; empty until captured
+NCU_DRAM_BYTES_FP64 = {}
 # shared-memory wavefronts per launch: the pass-2 pair kernel reads its u/w
 # spline records from shared memory (its global sectors are the moment and
 # pair records only)
@@ -165,13 +170,16 @@ def active_pairs(sys_, offs, idx, owner):
     return int(np.sum(act_i & (xa[idx] >= 5e-4)))
 
 
-def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1, multipole=False):
+def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1, multipole=False,
+                         info=None):
     """Times the reference's own arithmetic (oracle/_ref, -Ofast build, on
     `threads` host threads) on a bounded sample of one evaluation (divided
     by `scale`) and extrapolates.  With `multipole`, the -O2 build with
     MULTIPOLE_INTEGRAL and the reference's own -DNUMERICAL_DERIVATIVES=0
     (the oracle's rule 1 when that build is absent).  Returns
-    (evals_per_s, description, kind, seconds per evaluation)."""
+    (evals_per_s, description, kind, seconds per evaluation); `info`, when
+    given, receives the sample sizes and the wall time the sample took."""
+    t_start = time.perf_counter()
     import pyoracle
     ref = pyoracle.reference_multipole() if multipole else pyoracle.reference(fast=True)
     kind = "reference"
@@ -221,6 +229,10 @@ def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1, multipol
     ref.DV0_pairs(full, rho, offs, idx, us, is_)
     t_res = (time.perf_counter() - t0) / len(sample_res)
     t_full = n * (t_rho + t_v0 + t_res)
+    if info is not None:
+        info.update({"rho_sites": len(query), "V0_sites": len(sample_v0),
+                     "residual_sites": len(sample_res), "total_sites": n,
+                     "sample_wall_s": time.perf_counter() - t_start})
     desc = (f"{kind} arithmetic on {threads} threads: rho-bar of {len(query)} sites, V0 of "
             f"{len(sample_v0)} sites, residual assembly (dV0_i/d(q,sigma,x) over i in "
             f"{{u}}+N(u)) of {len(sample_res)} sites, each scaled to all {n} sites")
@@ -228,22 +240,36 @@ def cpu_reference_sample(sys_, threads, budget_s=12.0, seed=0, scale=1, multipol
 
 
 def run_reference(args, ws, rank):
+    """The reference's own CPU arithmetic on the plain drop-in workload.  A
+    full evaluation would take about 25 minutes on 16 host threads (the
+    reference's residual assembly is O(N_nb^3) per site), so each step times
+    a bounded, seeded sample of sites and extrapolates it to all sites; the
+    line says so ("extrapolated", the sample sizes, and the wall time each
+    sampled step really took)."""
     if rank != 0:
         return
     from btam import lattice
     sys_ = lattice.config2()
     threads = os.cpu_count() or 1
-    vals = []
+    vals, walls, info = [], [], {}
     for k in range(args.warmup + args.steps):
-        v, desc, kind, _ = cpu_reference_sample(sys_, threads, seed=k)
+        v, desc, kind, _ = cpu_reference_sample(sys_, threads, seed=k, info=info)
         if k >= args.warmup:
             vals.append(v)
+            walls.append(info["sample_wall_s"])
     value = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "evals/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "sites": len(sys_["x"])},
+            "extrapolated": True,
+            "steps_meaning": ("each step is one seeded site sample of a full evaluation, timed "
+                              "and scaled to all sites; ms_per_step is that extrapolated full "
+                              "evaluation, sample_wall_ms_per_step the time a step really took"),
+            "sample_wall_ms_per_step": 1e3 * float(np.mean(walls)),
+            "sampled_sites": {k: info[k] for k in ("rho_sites", "V0_sites", "residual_sites",
+                                                   "total_sites")},
             "cpu_baseline": {"value": value, "unit": "evals/s", "cores": threads,
                              "kind": kind, "sample": desc},
             "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
@@ -366,6 +392,20 @@ def bench_nanowire(args, tables):
     h = sys_["species"] == 1
     steps = args.dmd_steps
     out, xs = {}, {}
+    # error of the FP32C residual evaluation against the FP64 one on the
+    # wire's initial state
+    S = btam.System(tables, sys_)
+    S.build_neighbors()
+    a, b = S.evaluate(btam.FP64), S.evaluate(btam.FP32C)
+    S.close()
+    err = {"vs": "FP64 form, initial state",
+           "energy_rel": abs(b["totals"][0] - a["totals"][0]) / abs(a["totals"][0]),
+           "V0_max_abs": float(np.abs(b["V0"] - a["V0"]).max()),
+           "Rq_max_abs": float(np.abs(b["Rq"] - a["Rq"]).max()),
+           "Rs_max_abs": float(np.abs(b["Rs"] - a["Rs"]).max()),
+           "Rx_max_abs": float(np.abs(b["Rx"] - a["Rx"]).max()),
+           "sum_Rq_fp64": float(np.abs(a["Rq"].sum(axis=0)).max()),
+           "tolerance": "energy <= 1e-6 relative, residuals <= 1e-5 eV/A"}
     for prec, name in ((btam.FP32C, "fp32c"), (btam.FP64, "fp64")):
         S = btam.System(tables, sys_)
         S.build_neighbors()
@@ -381,12 +421,31 @@ def bench_nanowire(args, tables):
         xs[name] = x
         out[name] = {"steps_per_s": steps / t, "ms_per_step": t * 1e3 / steps,
                      "total_h_conserved": bool(total == total0),
+                     "clipped_edge_moves": S.dmd_clip_count(),
                      "x_min": float(x[h].min()), "x_max": float(x[h].max())}
         S.close()
+    # the same FP32C run with step control (sub-steps where a move would be
+    # cut to its room or a site would change by more than 0.05)
+    S = btam.System(tables, sys_)
+    S.build_neighbors()
+    S.autotune(btam.FP32C)
+    S.dmd_setup()
+    total0 = S.dmd_step(0, btam.FP32C, dt=1e-3)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    total, st = S.dmd_step_ctl(steps, btam.FP32C, dt=1e-3)
+    t = time.perf_counter() - t0
+    x, X, mu = S.dmd_occupancy()
+    out["fp32c_step_control"] = dict(st, steps_per_s=steps / t, ms_per_step=t * 1e3 / steps,
+                                     total_h_conserved=bool(total == total0),
+                                     max_abs_dx_vs_fixed_steps=float(
+                                         np.abs(x - xs["fp32c"]).max()))
+    S.close()
     nr = len(sys_["x"])
     return {"workload": "hcp Mg nanowire R = 30 A along c, 20 cells, periodic along the axis, "
                         "x ~ U[0, 0.5] beyond 20 A, 0.02 inside, seed 3",
             "sites": nr, "h_sites": int(h.sum()), "steps": steps, "dt": 1e-3,
+            "fp32c_error": err,
             "timing": "host clock around one call of all steps (device-resident loop)",
             **out,
             "fp32c_vs_fp64_max_abs_dx": float(np.abs(xs["fp32c"] - xs["fp64"]).max())}
@@ -602,7 +661,11 @@ def bench_serving(args, tables):
             "plain_fp64_one_at_a_time": dict(plain, kernels="plain two-pass pair, variants (0, 0)"),
             "fp64_one_at_a_time": dict(fp64_one, kernels="the server's undirected kernels"),
             "served_over_plain_jobs_per_s": served["jobs_per_s"] / plain["jobs_per_s"],
-            "served_over_fp64_one_at_a_time": served["jobs_per_s"] / fp64_one["jobs_per_s"]}
+            "served_over_fp64_one_at_a_time": served["jobs_per_s"] / fp64_one["jobs_per_s"],
+            "summary": {"served_jobs_per_s": served["jobs_per_s"], "p50_s": served["p50_s"],
+                        "p99_s": served["p99_s"],
+                        "over_plain_fp64": served["jobs_per_s"] / plain["jobs_per_s"],
+                        "over_fp64_one_at_a_time": served["jobs_per_s"] / fp64_one["jobs_per_s"]}}
 
 
 def run_btam(args, ws, rank, local):
@@ -654,7 +717,9 @@ def run_btam(args, ws, rank, local):
 
     results = {}
     clocks = None
-    for prec, name in ((btam.FP32C, "fp32c"), (btam.FP64, "fp64"), (btam.FP64, "fp64_two_pass")):
+    # the headline first: the FP64 drop-in (the reference's arithmetic type),
+    # then the FP32-compensated form and the plain two-pass FP64 kernel pair
+    for prec, name in ((btam.FP64, "fp64"), (btam.FP32C, "fp32c"), (btam.FP64, "fp64_two_pass")):
         if name == "fp64_two_pass":
             # the plain two-pass kernel pair: one warp per site in each pass,
             # every directed pair evaluated by its own site, default shapes
@@ -664,51 +729,57 @@ def run_btam(args, ws, rank, local):
         with ClockSampler(local) as cs:
             ms = timed_steps(prec, args.steps)
             barrier()
-        if name == "fp32c":
+        if name == "fp64":
             clocks = cs.summary()
         step_ms = max_over_ranks(float(np.mean(ms)))
         results[name] = dict(ms=step_ms, value=replica_value(ws, step_ms))
     S.set_variants(btam.FP64, *shapes["fp64"])
-    # per-kernel times for the roofline (FP32C form)
-    prof = np.median(np.array([S.profile(btam.FP32C) for _ in range(7)]), axis=0)
+    # per-kernel times for the rooflines (median of 7 profiled evaluations)
     prof64 = np.median(np.array([S.profile(btam.FP64) for _ in range(7)]), axis=0)
+    prof32 = np.median(np.array([S.profile(btam.FP32C) for _ in range(7)]), axis=0)
     fp32_peak = btam.probe_fma_peak(False, 0.5)
     fp64_peak = btam.probe_fma_peak(True, 0.5)
     gather_peak = btam.probe_gather_peak(tables, 0.5)
-    und = bool(shapes["fp32c"][1] & 16)
-    flops = kernel_flops(und)
     names = ["pass1 pair-rule kernel", "pass1 site kernel", "pass2 pair kernel",
              "pass2 site kernel", "totals"]
-    dom = int(np.argmax(prof))
-    achieved = flops[dom] * P / (prof[dom] * 1e-3) / 1e12
-    eval_rate = (FLOP_PASS1 + FLOP_PASS2) * P / (results["fp32c"]["ms"] * 1e-3) / 1e12
-    roofline = {"bound": "fp32", "kernel": names[dom] + " (FP32C)", "achieved": achieved,
-                "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                "traffic": NCU_DRAM_BYTES.get(names[dom]) if und else None,
+    eval_flops = (FLOP_PASS1 + FLOP_PASS2) * P
+
+    def kernel_roofline(prof, shape, peak, form, ncu_bytes):
+        und = bool((shape[0] | shape[1]) & 16)
+        flops = kernel_flops(und)
+        dom = int(np.argmax(prof))
+        achieved = flops[dom] * P / (prof[dom] * 1e-3) / 1e12
+        return {"bound": form, "kernel": f"{names[dom]} ({'FP64' if form == 'fp64' else 'FP32C'})",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": ncu_bytes.get(names[dom]) if und else None,
                 "traffic_unit": "bytes per launch (ncu dram read + write)",
-                "peak_source": "measured live: btam_probe_fma_peak FP32 FMA loop on all SMs",
+                "peak_source": f"measured live: btam_probe_fma_peak {form.upper()} FMA loop on "
+                               "all SMs (no vector-FMA figure in the measured peaks file)",
                 "flops_per_launch": flops[dom] * P,
                 "kernel_ms": dict(zip(names, map(float, prof))),
-                "kernel_flops_per_directed_pair": dict(zip(names, flops)),
-                "evaluation": {"flops": (FLOP_PASS1 + FLOP_PASS2) * P, "achieved": eval_rate,
-                               "frac": eval_rate / fp32_peak},
-                "l1_gather": {
-                    "bound": "L1 data pipe (random 32-byte record gathers)",
-                    "peak_gbs": gather_peak,
-                    "peak_source": "measured live: btam_probe_gather_peak, random 32-byte "
-                                   "spline-record gathers on all SMs",
-                    "kernels": {k: {"sector_gbs": NCU_L1_SECTORS[k] * 32 / (prof[i] * 1e-3) / 1e9,
-                                    "frac": NCU_L1_SECTORS[k] * 32 / (prof[i] * 1e-3) / 1e9 /
-                                    gather_peak,
-                                    "ncu_data_pipe_frac": NCU_L1_PIPE[k],
-                                    "ncu_shared_wavefronts": NCU_SHARED_WAVEFRONTS[k]}
-                                for i, k in enumerate(names) if k in NCU_L1_SECTORS} if und
-                    else None,
-                    "sectors_source": "L1 global-load sectors per launch from one ncu capture"},
-                "fp64_form": {"kernel_ms": dict(zip(names, map(float, prof64))),
-                              "fp64_peak": fp64_peak,
-                              "evaluation_frac": (FLOP_PASS1 + FLOP_PASS2) * P /
-                              (results["fp64"]["ms"] * 1e-3) / 1e12 / fp64_peak}}
+                "kernel_flops_per_directed_pair": dict(zip(names, flops))}, und
+
+    roofline, _ = kernel_roofline(prof64, shapes["fp64"], fp64_peak, "fp64", NCU_DRAM_BYTES_FP64)
+    eval64 = eval_flops / (results["fp64"]["ms"] * 1e-3) / 1e12
+    roofline["evaluation"] = {"flops": eval_flops, "achieved": eval64, "frac": eval64 / fp64_peak,
+                              "dram_bytes_ncu": sum(NCU_DRAM_BYTES_FP64.values()) or None,
+                              "algorithmic_bytes": 81 * n + 4 * P}
+    roof32, und32 = kernel_roofline(prof32, shapes["fp32c"], fp32_peak, "fp32", NCU_DRAM_BYTES)
+    eval32 = eval_flops / (results["fp32c"]["ms"] * 1e-3) / 1e12
+    roof32["evaluation"] = {"flops": eval_flops, "achieved": eval32, "frac": eval32 / fp32_peak,
+                            "dram_bytes_ncu": sum(NCU_DRAM_BYTES.values()),
+                            "algorithmic_bytes": 45 * n + 4 * P}
+    roof32["l1_gather"] = {
+        "bound": "L1 data pipe (random 32-byte record gathers)",
+        "peak_gbs": gather_peak,
+        "peak_source": "measured live: btam_probe_gather_peak, random 32-byte "
+                       "spline-record gathers on all SMs",
+        "kernels": {k: {"sector_gbs": NCU_L1_SECTORS[k] * 32 / (prof32[i] * 1e-3) / 1e9,
+                        "frac": NCU_L1_SECTORS[k] * 32 / (prof32[i] * 1e-3) / 1e9 / gather_peak,
+                        "ncu_data_pipe_frac": NCU_L1_PIPE[k],
+                        "ncu_shared_wavefronts": NCU_SHARED_WAVEFRONTS[k]}
+                    for i, k in enumerate(names) if k in NCU_L1_SECTORS} if und32 else None,
+        "sectors_source": "L1 global-load sectors per launch from one ncu capture"}
     # e2e through the C ABI with pinned host buffers
     qh = torch.from_numpy(sys_["q"]).pin_memory().numpy()
     sh = torch.from_numpy(sys_["sigma"]).pin_memory().numpy()
@@ -717,24 +788,28 @@ def run_btam(args, ws, rank, local):
             for k, sh_ in (("Rq", (n, 3)), ("Rs", (n,)), ("Rx", (n,)), ("totals", (4,)))}
     lib = btam.lib()
 
-    def e2e_step():
+    def e2e_step(prec):
         # new (q, sigma, x) from host buffers, evaluation, residuals back to
         # host buffers: one C-ABI call
-        code = lib.btam_mf_eval_state(S.handle, btam.FP32C, btam._d(qh), btam._d(sh),
+        code = lib.btam_mf_eval_state(S.handle, prec, btam._d(qh), btam._d(sh),
                                       btam._d(xh), None, None, None, btam._d(outs["Rq"]),
                                       btam._d(outs["Rs"]), btam._d(outs["Rx"]),
                                       btam._d(outs["totals"]))
         if code:
             raise btam.BtamError(code, "btam_mf_eval_state")
 
-    for _ in range(args.warmup):
-        e2e_step()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    barrier()
-    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+    def e2e_ms(prec):
+        for _ in range(args.warmup):
+            e2e_step(prec)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step(prec)
+        barrier()
+        return max_over_ranks((time.perf_counter() - t0) * 1e3 / args.steps)
+
+    e2e64 = e2e_ms(btam.FP64)
+    e2e32 = e2e_ms(btam.FP32C)
     h2d = n * (24 + 8 + 8)
     d2h = n * (24 + 8 + 8) + 32
     # error of the FP32C form against the FP64 form (the FP64 form agrees with
@@ -759,39 +834,60 @@ def run_btam(args, ws, rank, local):
     if rank == 0 and not args.no_cpu:
         v, desc, kind, _ = cpu_reference_sample(sys_, os.cpu_count() or 1)
         cpu = {"value": v, "unit": "evals/s", "cores": os.cpu_count() or 1, "kind": kind,
-               "sample": desc}
+               "sample": desc, "extrapolated": True}
         # the same arithmetic on one thread, on a quarter of the sample
         v1, desc1, _, _ = cpu_reference_sample(sys_, 1, seed=1, scale=4)
         cpu["single_thread"] = {"value": v1, "unit": "evals/s", "cores": 1, "sample": desc1}
     if rank == 0:
-        line = {"metric": METRIC, "value": results["fp32c"]["value"], "unit": "evals/s",
+        r64, r32, r2p = results["fp64"], results["fp32c"], results["fp64_two_pass"]
+        fp32c = {"value": r32["value"], "unit": "evals/s", "ms_per_step": r32["ms"],
+                 "kernels": "autotuned variants " + str(shapes["fp32c"]),
+                 "e2e": {"value": ws * 1e3 / e2e32, "unit": "evals/s", "ms_per_step": e2e32,
+                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                 "error_vs_fp64": precision, "roofline": roof32,
+                 "over_fp64_drop_in": r32["value"] / r64["value"],
+                 "over_fp64_two_pass": r32["value"] / r2p["value"],
+                 "e2e_over_fp64_e2e": e2e64 / e2e32}
+        summary = {"fp64_evals_per_s": r64["value"], "fp64_e2e_evals_per_s": ws * 1e3 / e2e64,
+                   "fp32c_evals_per_s": r32["value"], "fp32c_e2e_evals_per_s": ws * 1e3 / e2e32,
+                   "fp32c_energy_rel_err": precision["energy_rel"],
+                   "fp32c_max_residual_err": max(precision["Rq_max_abs"], precision["Rs_max_abs"],
+                                                 precision["Rx_max_abs"]),
+                   "fp32c_over_fp64_drop_in": fp32c["over_fp64_drop_in"],
+                   "fp32c_over_fp64_two_pass": fp32c["over_fp64_two_pass"]}
+        if batched:
+            summary["batched_system_evals_per_s"] = batched["graph_fp32c"]["value"]
+            summary["batched_over_fp64_autotuned_launches"] = batched["graph_fp32c_over_plain_fp64"]
+            summary["batched_over_fp64_two_pass_launches"] = \
+                batched["graph_fp32c_over_plain_fp64_two_pass"]
+        if serving:
+            summary["serving"] = serving.get("summary")
+        line = {"metric": METRIC, "value": r64["value"], "unit": "evals/s",
                 "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": results["fp32c"]["ms"], "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "fp32c",
+                "ms_per_step": r64["ms"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "sites": n, "images": ng,
-                           "directed_active_pairs": P, "precision": "fp32c",
-                           "l2": "flushed between steps (256 MiB write, outside step events)",
-                           "parallelism": f"{ws} independent replica(s), no collective",
-                           "kernel_shapes": shapes},
-                "fp64_drop_in": {"value": results["fp64"]["value"], "unit": "evals/s",
-                                 "ms_per_step": results["fp64"]["ms"],
-                                 "kernels": "autotuned variants " + str(shapes["fp64"])},
-                "fp64_two_pass": {"value": results["fp64_two_pass"]["value"], "unit": "evals/s",
-                                  "ms_per_step": results["fp64_two_pass"]["ms"],
-                                  "kernels": "plain two-pass pair (directed, variants (0, 0))"},
-                "fp32c_error": precision,
-                "fp32c_over_fp64": results["fp32c"]["value"] / results["fp64"]["value"],
-                "fp32c_over_fp64_two_pass": (results["fp32c"]["value"] /
-                                             results["fp64_two_pass"]["value"]),
+                "config": {"workload": WORKLOAD, "sites": n},
+                "setup": {"images": ng, "directed_active_pairs": P, "precision": "fp64",
+                          "l2": "flushed between steps (256 MiB write, outside step events)",
+                          "parallelism": f"{ws} independent replica(s), no collective",
+                          "kernel_shapes": shapes},
                 "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": {"value": ws * 1e3 / e2e_ms, "unit": "evals/s",
+                "e2e": {"value": ws * 1e3 / e2e64, "unit": "evals/s",
                         "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                        "ms_per_step": e2e_ms},
-                "gpu_launches": launches_per_eval(shapes["fp32c"]) * args.steps,
-                "clocks": clocks, "batched": batched, "serving": serving,
+                        "ms_per_step": e2e64,
+                        "call": "btam_mf_eval_state(BTAM_FP64) with pinned host buffers"},
+                "gpu_launches": launches_per_eval(shapes["fp64"]) * args.steps,
+                "clocks": clocks,
+                "fp64_two_pass": {"value": r2p["value"], "unit": "evals/s",
+                                  "ms_per_step": r2p["ms"],
+                                  "kernels": "plain two-pass pair (directed, variants (0, 0))"},
+                "fp32c": fp32c,
+                "batched": batched, "serving": serving,
                 "precision_nanowire": nanowire, "bulk_stretch": stretch,
-                "config1_workflow": config1, "multipole": multipole}
+                "config1_workflow": config1, "multipole": multipole,
+                # last, so that it is inside any tail of the line
+                "summary": summary}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
