@@ -133,6 +133,9 @@ _PROTOS = {
                                          ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.POINTER(ctypes.c_longlong)]),
     "btam_server_destroy": (ctypes.c_int, [_V]),
+    "btam_server_batch_stats": (ctypes.c_int, [_V, ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.POINTER(ctypes.c_longlong),
+                                               ctypes.POINTER(ctypes.c_longlong)]),
     "btam_mf_eval_noalloc": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _V, _V, _V, _V,
                                             _V, _V, _V, _V, _V, _V, _V, _V, _V]),
 }
@@ -748,7 +751,7 @@ class Server:
     def submit(self, sysdict, kind, precision=FP32C, mode=RELAX_FP32C, tol=1e-5, max_iter=300,
                nsteps=100, dmd=(1e-3, 0.045, 3.2, 1e-8, 0.9), plain=False):
         """Queues a job; plain=True runs it on the plain two-pass kernel pair
-        instead of the server's undirected kernels."""
+        on its own instead of through the server's batched evaluations."""
         s = sysdict
         arrs = dict(q=np.ascontiguousarray(s["q"], np.float64),
                     sigma=np.ascontiguousarray(s["sigma"], np.float64),
@@ -800,6 +803,14 @@ class Server:
                "btam_server_stats")
         return dict(waiting=w.value, running=r.value, completed=c.value, failed=f.value,
                     bytes_in_use=b.value)
+
+    def batch_stats(self):
+        """Continuous batching counters: rounds, job evaluations served,
+        rebuilds of the shared batch."""
+        r, e, b = (ctypes.c_longlong() for _ in range(3))
+        _check(lib().btam_server_batch_stats(self.handle, ctypes.byref(r), ctypes.byref(e),
+                                             ctypes.byref(b)), "btam_server_batch_stats")
+        return dict(rounds=r.value, evaluations=e.value, rebuilds=b.value)
 
     def close(self):
         if getattr(self, "handle", None):

@@ -717,6 +717,24 @@ BTAM_HD void pass1_pair_part2(const TV &T, const V3<R> &r0, R sig_i, R X, int pk
   acc[0] += X * X * ss;
 }
 
+// Part II for one axis k only (the FP64 form runs three of these, so that
+// 19 accumulators are live instead of 55): G(d) for d = 2k, 2k + 1 at part
+// index 1 + 9 (d - 2k) + c and the axis' share of sself at part index 0.
+template <class R, class TV>
+BTAM_HD void pass1_pair_part2_axis(const TV &T, const V3<R> &r0, R sig_i, R X, int pk, int k,
+                                   R *acc) {
+  const R amt_i = sig_i * (R)kDelta9;
+  R ss = (R)0, p;
+#pragma unroll
+  for (int sg = 0; sg < 2; ++sg) {
+    Geo<R> g;
+    geo_uw<R, false>(g, disp(r0, k, sg ? -amt_i : amt_i), T, pk, p);
+    feat_acc(acc, 1 + 9 * sg, g, X);
+    ss += bff(g);
+  }
+  acc[0] += X * X * ss;
+}
+
 // Flat pass-1 value of part II's local index t.
 BTAM_HD int p1_part2_value(int t) { return t == 0 ? kP1Sself : kP1Gd + (t - 1); }
 

@@ -424,7 +424,7 @@ pass1_kernel(const EvalArgs<R> a) {
       if (act && v0 + k < kP1Gd && v0 + k != kP1Sself)
         site[p1_site_slot(v0 + k)] = tree_total(acc[k], lo[k]);
   }
-  {  // part II: centre-displaced points
+  if constexpr (sizeof(R) == 4) {  // part II: centre-displaced points
     R acc[kP1PartII], lo[kP1PartII];
 #pragma unroll
     for (int c = 0; c < kP1PartII; ++c) acc[c] = (R)0;
@@ -441,6 +441,35 @@ pass1_kernel(const EvalArgs<R> a) {
     for (int k = 0; k < kP1PartII / G; ++k)
       if (act && t0 + k < 1 + 54)
         site[p1_site_slot(p1_part2_value(t0 + k))] = tree_total(acc[k], lo[k]);
+  } else {
+    // FP64: part II one axis at a time (19 live accumulators instead of 55;
+    // each displaced point is still evaluated once), sself summed over the
+    // three axes in axis order
+    double sself = 0.0;
+#pragma unroll 1
+    for (int ax = 0; ax < 3; ++ax) {
+      R acc[kP1PartI], lo[kP1PartI];
+#pragma unroll
+      for (int c = 0; c < kP1PartI; ++c) acc[c] = (R)0;
+#pragma unroll 1
+      for (int p = nb0 + sl; p < nb1; p += G) {
+        const NbSite<R> sj = nb_site(a, a.idx[p]);
+        if (!sj.active) continue;
+        pass1_pair_part2_axis<R>(T, pair_vec<R>(qi, sj), (R)qi.w, (R)xi * sj.occ,
+                                 pair_kind(ci, sj.code), ax, acc);
+      }
+      lane_tree<G>(acc, lo, lane);
+      const int t0 = tree_base<kP1PartI, G>(sl);
+#pragma unroll
+      for (int k = 0; k < kP1PartI / G; ++k) {
+        const int t = t0 + k;
+        if (t == 0) sself += tree_total(acc[k], lo[k]);
+        else if (act && t < 1 + 18)
+          site[p1_site_slot(p1_part2_value(1 + 18 * ax + (t - 1)))] = tree_total(acc[k], lo[k]);
+      }
+    }
+    // lane 0 of the group held part index 0 in every axis
+    if (act && sl == 0) site[p1_site_slot(kP1Sself)] = sself;
   }
   __syncwarp();
   // epilogue: lanes 0..7 of the group form the record's eight duals, lane 0

@@ -16,6 +16,7 @@
 // per-system totals use the same reduction tree as a single system.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "../../include/btam.h"
@@ -65,6 +66,40 @@ __global__ void shift_slot_own_kernel(long long n, const int *src, int *dst, int
 }
 
 inline int blocks_of(long long n, int per) { return (int)((n + per - 1) / per); }
+
+// Copies the site rows (real, then images) of the systems in the table into
+// their batch rows: blockIdx.y picks the system, the x dimension strides rows.
+__global__ void batch_gather_kernel(BatchXfer t, double4 *pos, double2 *xb) {
+  const BatchXfer::Sys &d = t.sys[blockIdx.y];
+  const int rows = d.n + d.g;
+  for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const int dst = r < d.n ? d.R + r : d.G + (r - d.n);
+    pos[dst] = d.pos[r];
+    xb[dst] = d.xb[r];
+  }
+}
+
+// Copies the results of the systems in the table from their batch rows into
+// their own buffers, with their totals (4 each) and the batch's error bits.
+__global__ void batch_scatter_kernel(BatchXfer t, const double *rho, const double *V0,
+                                     const double *S0, const double *Rq, const double *Rs,
+                                     const double *Rx, const double *totals, const int *err) {
+  const BatchXfer::Sys &d = t.sys[blockIdx.y];
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int r = tid; r < d.n; r += gridDim.x * blockDim.x) {
+    const int src = d.R + r;
+    d.rho[r] = rho[src];
+    d.V0[r] = V0[src];
+    d.S0[r] = S0[src];
+    d.Rq[3 * (size_t)r] = Rq[3 * (size_t)src];
+    d.Rq[3 * (size_t)r + 1] = Rq[3 * (size_t)src + 1];
+    d.Rq[3 * (size_t)r + 2] = Rq[3 * (size_t)src + 2];
+    d.Rs[r] = Rs[src];
+    d.Rx[r] = Rx[src];
+  }
+  if (tid < 4) d.totals[tid] = totals[4 * (size_t)d.k + tid];
+  if (tid == 0 && *err) atomicOr(d.err, *err);
+}
 
 }  // namespace
 
@@ -479,6 +514,38 @@ int btam_batch_eval_async(btam_batch *b, int precision) {
   if (st != BTAM_OK) return st;
   return cuda_status(cudaGraphLaunch(b->exec[precision == BTAM_FP64 ? 0 : 1], b->st));
 }
+
+}  // extern "C"
+
+// ---- evaluation rounds of the job server (server.cu) -----------------------
+// The systems in a round's table: their site rows are copied in after
+// everything already enqueued on their streams (ready events), the batch is
+// evaluated, and their results are copied back into their own buffers.
+int batch_round(btam_batch *b, const BatchXfer &t, const cudaEvent_t *ready, int precision) {
+  if (t.n <= 0) return BTAM_OK;
+  for (int k = 0; k < t.n; ++k) BTAM_TRY(cudaStreamWaitEvent(b->st, ready[k], 0));
+  int rows = 0;
+  for (int k = 0; k < t.n; ++k) rows = std::max(rows, t.sys[k].n + t.sys[k].g);
+  const dim3 grid(std::max(1, std::min(64, blocks_of(rows, 256))), t.n);
+  batch_gather_kernel<<<grid, 256, 0, b->st>>>(t, b->pos, b->xb);
+  BTAM_TRY(cudaGetLastError());
+  BTAM_TRY(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
+  int st = btam_batch_eval_async(b, precision);
+  if (st != BTAM_OK) return st;
+  batch_scatter_kernel<<<grid, 256, 0, b->st>>>(t, b->rho, b->V0, b->S0, b->Rq, b->Rs, b->Rx,
+                                                 b->totals, b->err);
+  return cuda_status(cudaGetLastError());
+}
+
+// Row bases of system k in the batch layout.
+void batch_bases(const btam_batch *b, int k, int *R, int *G) {
+  *R = b->base_real[k];
+  *G = b->base_img[k];
+}
+
+cudaStream_t batch_stream_of(const btam_batch *b) { return b->st; }
+
+extern "C" {
 
 int btam_batch_sync(btam_batch *b) {
   if (!b) return BTAM_ERR_ARG;

@@ -598,6 +598,7 @@ void btam_system_destroy(btam_system *s) {
   dfree(s->S0, s->st); dfree(s->selfx, s->st); dfree(s->Rq, s->st); dfree(s->Rs, s->st); dfree(s->Rx, s->st); dfree(s->totals, s->st);
   dfree(s->mom64, s->st); dfree(s->mom32, s->st); dfree(s->err, s->st);
   dfree(s->doffs, s->st); dfree(s->didx, s->st); dfree(s->X, s->st); dfree(s->X0, s->st); dfree(s->dtot, s->st); dfree(s->mu, s->st);
+  dfree(s->dctl, s->st);
   dfree(s->dact, s->st); dfree(s->ddeg, s->st); dfree(s->rv, s->st);
   dfree(s->rev, s->st); dfree(s->slot_own, s->st); dfree(s->own_off, s->st); dfree(s->own_p, s->st); dfree(s->own_u, s->st);
   dfree(s->pbuf, s->st);
@@ -819,6 +820,7 @@ int btam_mf_eval_async(btam_system *s, int precision) {
   if (!s) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
   if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  if (s->batcher) return batcher_eval(s, precision);  // a served job: one shared launch
   const size_t nm = (size_t)s->n_real * kMomStride;
   if (precision == BTAM_FP64) {
     if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));

@@ -14,6 +14,9 @@
 
 using namespace btam;
 
+// The job server's evaluation batcher (server.cu).
+struct EvalBatcher;
+
 struct btam_tables {
   HostTables host;
   int device = 0;
@@ -91,7 +94,37 @@ struct btam_system {
   // non-mean-field forms: site records, outputs and totals (point.cu)
   double *pt = nullptr;
   size_t pt_cap = 0;
+  // the job server's evaluation batcher this system's evaluations go to
+  // (null: its own kernels), and the events that order them
+  EvalBatcher *batcher = nullptr;
+  cudaEvent_t batch_ready = nullptr, batch_done = nullptr;
 };
+
+// ---- evaluation rounds of the job server ----------------------------------
+// A table of systems whose evaluations one batch launch serves: each
+// system's device buffers and its rows in the batch layout (batch.cu).
+struct BatchXfer {
+  static constexpr int kMax = 96;  // systems per round (kernel-argument table)
+  struct Sys {
+    const double4 *pos;
+    const double2 *xb;
+    double *rho, *V0, *S0, *Rq, *Rs, *Rx, *totals;
+    int *err;
+    int n, g;  // real sites, images
+    int R, G;  // their first rows in the batch
+    int k;     // the system's index in the batch
+  } sys[kMax];
+  int n = 0;
+};
+// Enqueues on the batch's stream: after each system's ready event, its site
+// rows into the batch; one evaluation of the batch; the results back.
+int batch_round(btam_batch *b, const BatchXfer &t, const cudaEvent_t *ready, int precision);
+void batch_bases(const btam_batch *b, int k, int *R, int *G);
+cudaStream_t batch_stream_of(const btam_batch *b);
+
+// btam_mf_eval_async of a system attached to the job server's batcher
+// hands the evaluation to it (server.cu).
+int batcher_eval(btam_system *s, int precision);
 
 // Point-form buffers reused by the mean-field stress, and the fixed-order
 // totals over per-site V, Fq, W (V, Fq may be NULL) into tot[12]

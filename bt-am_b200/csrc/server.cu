@@ -7,13 +7,25 @@
 // (sched.hpp), then run by one of the worker threads on its own
 // btam_system, i.e. its own CUDA stream, with q, sigma, x, the images and
 // the neighbour lists resident on the device from creation to the last step.
-// Workers never synchronise the device (stream-ordered allocation, one
-// stream per job), so the kernels of every running job overlap on the GPU;
-// a job that arrives while others run starts as soon as a worker and its
-// memory are free.  Results are the same as the job run alone: every kernel
-// is deterministic and a job's work touches only its own buffers.
+// A job that arrives while others run starts as soon as a worker slot and
+// its memory are free.
+//
+// Continuous batching: the residual evaluations of all running jobs go
+// through one batcher (EvalBatcher below).  A job's solver (L-BFGS steps,
+// master-equation steps) runs on its own thread and stream as before; each
+// time it needs an evaluation it hands its system to the batcher and waits.
+// The batcher collects the requests of every running job (or those that
+// arrive within a short window), copies their states into one batch layout
+// (batch.cu: every job's sites renumbered into one device layout, rebuilt
+// when a job joins), evaluates them all with one graph launch, and copies
+// each job's results back into its own buffers; the job's stream waits for
+// that and carries on.  So the jobs in flight share every evaluation launch
+// instead of each launching its own kernels, and a job's results are the
+// same alone and in the mix (every kernel is deterministic, a system's rows
+// never mix with another's, and the batch's kernel shapes are fixed).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -26,6 +38,7 @@
 
 #include "../../include/btam.h"
 #include "adp_kernels.cuh"
+#include "internal.cuh"
 #include "sched.hpp"
 
 namespace {
@@ -53,6 +66,198 @@ double since(Clock::time_point t0) {
 
 }  // namespace
 
+// ---- the evaluation batcher -------------------------------------------------
+// Launch variants of served evaluations (index 0 FP64, 1 FP32C): undirected,
+// persistent grid, and the block shapes the autotuner picks for the plain
+// drop-in workload on a B200.
+constexpr int kServeVariant1[2] = {btam::kUndirected | btam::kPersistent | 3,
+                                   btam::kUndirected | btam::kPersistent | 4};
+constexpr int kServeVariant2[2] = {btam::kUndirected | btam::kPersistent | 0,
+                                   btam::kUndirected | btam::kPersistent | 2};
+// How long a round waits for the running jobs that have not asked yet.
+constexpr int kRoundWaitUs = 400;
+
+struct EvalBatcher {
+  int device = 0;
+  std::mutex mu;
+  std::condition_variable cv;
+  bool stop = false;
+  struct Req {
+    btam_system *s;
+    int precision;
+    bool done = false;
+    int status = BTAM_OK;
+  };
+  std::vector<btam_system *> members;  // systems of the running jobs
+  bool joined = false;                 // a member is missing from the batch layout
+  std::vector<Req *> pending;
+  Clock::time_point first_pending;
+  // the batch and the systems of its layout (a system that left keeps its
+  // rows until the next rebuild; they are evaluated but nobody reads them)
+  btam_batch *batch = nullptr;
+  std::map<btam_system *, int> layout;
+  long long layout_sites = 0, departed_sites = 0;  // real sites in the layout; of jobs gone
+  std::thread thr;
+  long long rounds = 0, evals = 0, rebuilds = 0;
+};
+
+namespace {
+
+// Builds the batch over the current members, with the served launch shapes.
+int batcher_rebuild(EvalBatcher *B, const std::vector<btam_system *> &members) {
+  if (B->batch) btam_batch_destroy(B->batch);
+  B->batch = nullptr;
+  B->layout.clear();
+  if (members.empty()) return BTAM_OK;
+  int st = btam_batch_create(members.data(), (int)members.size(), &B->batch);
+  for (int f = 0; f < 2 && st == BTAM_OK; ++f)
+    st = btam_batch_set_variants(B->batch, f == 0 ? BTAM_FP64 : BTAM_FP32C, kServeVariant1[f],
+                                 kServeVariant2[f]);
+  if (st != BTAM_OK) return st;
+  B->layout_sites = 0;
+  for (size_t k = 0; k < members.size(); ++k) {
+    B->layout[members[k]] = (int)k;
+    B->layout_sites += members[k]->n_real;
+  }
+  ++B->rebuilds;
+  return BTAM_OK;
+}
+
+// One round: the requests of each precision in tables of at most
+// BatchXfer::kMax systems, each table one gather, one batch evaluation and
+// one scatter on the batch's stream; then every requester's done event.
+int batcher_round(EvalBatcher *B, const std::vector<EvalBatcher::Req *> &round,
+                  const std::vector<btam_system *> &members, bool rebuild) {
+  if (rebuild) {
+    int st = batcher_rebuild(B, members);
+    if (st != BTAM_OK) return st;
+  }
+  for (int prec : {BTAM_FP32C, BTAM_FP64}) {
+    std::vector<btam_system *> sys;
+    for (auto *r : round)
+      if (r->precision == prec) sys.push_back(r->s);
+    for (size_t at = 0; at < sys.size(); at += BatchXfer::kMax) {
+      BatchXfer t;
+      cudaEvent_t ready[BatchXfer::kMax];
+      const size_t end = std::min(sys.size(), at + BatchXfer::kMax);
+      for (size_t j = at; j < end; ++j) {
+        btam_system *s = sys[j];
+        auto it = B->layout.find(s);
+        if (it == B->layout.end()) return BTAM_ERR_ARG;  // not in the batch: cannot happen
+        BatchXfer::Sys &d = t.sys[t.n];
+        d.pos = s->pos;
+        d.xb = s->xb;
+        d.rho = s->rho;
+        d.V0 = s->V0;
+        d.S0 = s->S0;
+        d.Rq = s->Rq;
+        d.Rs = s->Rs;
+        d.Rx = s->Rx;
+        d.totals = s->totals;
+        d.err = s->err;
+        d.n = s->n_real;
+        d.g = s->n_ghost;
+        d.k = it->second;
+        batch_bases(B->batch, d.k, &d.R, &d.G);
+        ready[t.n] = s->batch_ready;
+        ++t.n;
+      }
+      int st = batch_round(B->batch, t, ready, prec);
+      if (st != BTAM_OK) return st;
+      for (int j = 0; j < t.n; ++j)
+        BTAM_TRY(cudaEventRecord(sys[at + j]->batch_done, batch_stream_of(B->batch)));
+      B->evals += t.n;
+    }
+  }
+  ++B->rounds;
+  return BTAM_OK;
+}
+
+void batcher_main(EvalBatcher *B) {
+  cudaSetDevice(B->device);
+  std::unique_lock<std::mutex> lock(B->mu);
+  for (;;) {
+    // a round starts when every running job has asked, or when the first
+    // request has waited kRoundWaitUs
+    for (;;) {
+      if (B->pending.empty()) {
+        if (B->stop) break;
+        B->cv.wait(lock);
+        continue;
+      }
+      if (B->pending.size() >= B->members.size() || B->stop) break;
+      const auto deadline = B->first_pending + std::chrono::microseconds(kRoundWaitUs);
+      if (B->cv.wait_until(lock, deadline) == std::cv_status::timeout) break;
+    }
+    if (B->pending.empty()) return;  // stopping
+    std::vector<EvalBatcher::Req *> round;
+    round.swap(B->pending);
+    const std::vector<btam_system *> members = B->members;
+    // rebuild when a job joined, or when the rows of jobs that left are more
+    // than a quarter of the batch (they are evaluated for nothing)
+    bool rebuild = B->joined || !B->batch || 4 * B->departed_sites > B->layout_sites;
+    for (auto *r : round)
+      if (!B->layout.count(r->s)) rebuild = true;
+    B->joined = false;
+    if (rebuild) B->departed_sites = 0;
+    lock.unlock();
+    const int st = batcher_round(B, round, members, rebuild);
+    lock.lock();
+    for (auto *r : round) {
+      r->status = st;
+      r->done = true;
+    }
+    B->cv.notify_all();
+  }
+}
+
+// Attaches a built system to the batcher (its evaluations then go there).
+int batcher_attach(EvalBatcher *B, btam_system *s) {
+  BTAM_TRY(cudaEventCreateWithFlags(&s->batch_ready, cudaEventDisableTiming));
+  BTAM_TRY(cudaEventCreateWithFlags(&s->batch_done, cudaEventDisableTiming));
+  std::lock_guard<std::mutex> lock(B->mu);
+  B->members.push_back(s);
+  B->joined = true;
+  s->batcher = B;
+  return BTAM_OK;
+}
+
+// Detaches a system whose work has finished (its stream is idle, so no round
+// still reads or writes its buffers).
+void batcher_detach(EvalBatcher *B, btam_system *s) {
+  {
+    std::lock_guard<std::mutex> lock(B->mu);
+    B->members.erase(std::find(B->members.begin(), B->members.end(), s));
+    // its rows stay in the batch until the next rebuild
+    if (B->layout.erase(s)) B->departed_sites += s->n_real;
+    s->batcher = nullptr;
+  }
+  B->cv.notify_all();  // a round may have been waiting for this job
+  if (s->batch_ready) cudaEventDestroy(s->batch_ready);
+  if (s->batch_done) cudaEventDestroy(s->batch_done);
+  s->batch_ready = s->batch_done = nullptr;
+}
+
+}  // namespace
+
+// The served job's side: its state is ready once everything enqueued on its
+// stream has run; the evaluation joins the next round, and the job's stream
+// waits for that round's results.
+int batcher_eval(btam_system *s, int precision) {
+  EvalBatcher *B = s->batcher;
+  BTAM_TRY(cudaEventRecord(s->batch_ready, s->st));
+  EvalBatcher::Req r{s, precision};
+  {
+    std::unique_lock<std::mutex> lock(B->mu);
+    if (B->pending.empty()) B->first_pending = Clock::now();
+    B->pending.push_back(&r);
+    B->cv.notify_all();
+    B->cv.wait(lock, [&] { return r.done; });
+  }
+  if (r.status != BTAM_OK) return r.status;
+  return cuda_status(cudaStreamWaitEvent(s->st, s->batch_done, 0));
+}
+
 struct btam_server {
   const btam_tables *T = nullptr;
   int device = 0;
@@ -66,17 +271,10 @@ struct btam_server {
   bool stop = false;
   std::vector<std::thread> workers;
   long long completed = 0, failed = 0;
+  EvalBatcher batcher;
 };
 
 namespace {
-
-// Launch variants of served jobs (index 0 FP64, 1 FP32C): undirected,
-// persistent grid, and the block shapes the autotuner picks for the plain
-// drop-in workload on a B200.
-constexpr int kServeVariant1[2] = {btam::kUndirected | btam::kPersistent | 3,
-                                   btam::kUndirected | btam::kPersistent | 4};
-constexpr int kServeVariant2[2] = {btam::kUndirected | btam::kPersistent | 0,
-                                   btam::kUndirected | btam::kPersistent | 2};
 
 // Runs one job on the calling worker thread; fills job->res and the outputs.
 void run_job(btam_server *srv, Job *job) {
@@ -89,14 +287,14 @@ void run_job(btam_server *srv, Job *job) {
                               job->gamma.empty() ? nullptr : job->gamma.data(), job->origin,
                               job->cell, job->periodic, &s);
   if (st == BTAM_OK) st = btam_neighbors_build(s, 0);
-  // jobs run the undirected kernels (each neighbour pair evaluated once for
-  // both directions) on persistent grids, in both arithmetic forms, unless
-  // they ask for the plain two-pass pair; the pair buffers are part of
-  // btam_estimate_bytes
-  if (st == BTAM_OK && !sp.plain)
-    st = btam_set_variants(s, BTAM_FP32C, kServeVariant1[1], kServeVariant2[1]);
-  if (st == BTAM_OK && !sp.plain)
-    st = btam_set_variants(s, BTAM_FP64, kServeVariant1[0], kServeVariant2[0]);
+  // jobs hand their evaluations to the batcher (the undirected kernels on
+  // persistent grids, in the batch's buffers, which btam_estimate_bytes
+  // counts), unless they ask for the plain two-pass pair on their own
+  bool attached = false;
+  if (st == BTAM_OK && !sp.plain) {
+    st = batcher_attach(&srv->batcher, s);
+    attached = st == BTAM_OK;
+  }
   if (st == BTAM_OK) {
     r.t_start = since(srv->t0);
     if (sp.kind == BTAM_JOB_RELAX) {
@@ -144,6 +342,8 @@ void run_job(btam_server *srv, Job *job) {
     job->x_out.resize(n);
     st = btam_system_get_state(s, job->q_out.data(), job->sigma_out.data(), job->x_out.data());
   }
+  if (s) cudaStreamSynchronize(s->st);
+  if (attached) batcher_detach(&srv->batcher, s);
   if (s) btam_system_destroy(s);
   r.status = st;
 }
@@ -232,6 +432,8 @@ int btam_server_create(const btam_tables *t, int n_workers, long long budget_byt
     budget_bytes = (long long)(0.8 * (double)free_b);
   }
   srv->queue = btam::AdmissionQueue((size_t)budget_bytes);
+  srv->batcher.device = srv->device;
+  srv->batcher.thr = std::thread(batcher_main, &srv->batcher);
   for (int w = 0; w < n_workers; ++w) srv->workers.emplace_back(worker_main, srv);
   *out = srv;
   return BTAM_OK;
@@ -320,7 +522,24 @@ int btam_server_destroy(btam_server *srv) {
   }
   srv->work_cv.notify_all();
   for (auto &w : srv->workers) w.join();
+  {
+    std::lock_guard<std::mutex> lock(srv->batcher.mu);
+    srv->batcher.stop = true;
+  }
+  srv->batcher.cv.notify_all();
+  srv->batcher.thr.join();
+  if (srv->batcher.batch) btam_batch_destroy(srv->batcher.batch);
   delete srv;
+  return BTAM_OK;
+}
+
+int btam_server_batch_stats(btam_server *srv, long long *rounds, long long *evaluations,
+                            long long *rebuilds) {
+  if (!srv) return BTAM_ERR_ARG;
+  std::lock_guard<std::mutex> lock(srv->batcher.mu);
+  if (rounds) *rounds = srv->batcher.rounds;
+  if (evaluations) *evaluations = srv->batcher.evals;
+  if (rebuilds) *rebuilds = srv->batcher.rebuilds;
   return BTAM_OK;
 }
 

@@ -534,9 +534,12 @@ int btam_batch_totals_copy(btam_batch *b, double *totals);
  * (btam_estimate_bytes) fits the memory budget next to the running jobs (a
  * job may overtake the head of the queue only if it leaves room for the
  * head).  Each running job owns a system and its stream: its state and
- * neighbour lists stay resident on the device until it ends, and the work of
- * all running jobs overlaps on the GPU.  A job's results equal those of the
- * same job run alone (deterministic kernels, private buffers). */
+ * neighbour lists stay resident on the device until it ends.  Continuous
+ * batching: the residual evaluations of all running jobs are merged, round
+ * by round, into one batched launch (one graph over every running job's
+ * sites); jobs join at the next round after they start and leave when they
+ * end.  A job's results equal those of the same job run alone
+ * (deterministic kernels, fixed kernel shapes, rows never shared). */
 typedef struct btam_server btam_server;
 
 #define BTAM_JOB_RELAX 0  /* btam_relax(mode, tol, max_iter, lbfgs_m, bounds) */
@@ -592,6 +595,11 @@ int btam_server_stats(btam_server *srv, long long *waiting, int *running,
                       long long *completed, long long *failed, long long *bytes_in_use);
 /* Lets running jobs finish, drops the jobs still queued, joins the workers. */
 int btam_server_destroy(btam_server *srv);
+/* Continuous batching counters: evaluation rounds run, job evaluations
+ * they served (each round serves every running job that asked), and
+ * rebuilds of the shared batch layout (when jobs joined or left). */
+int btam_server_batch_stats(btam_server *srv, long long *rounds, long long *evaluations,
+                            long long *rebuilds);
 
 /* ---- measurement (no counterpart in the reference, which has only PETSc's
  * SNES monitor for tracing) ------------------------------------------------ */

@@ -1,8 +1,10 @@
 """Job server: results of every job alone and in a concurrent mix.
 
-Tolerance: none.  A job's kernels are deterministic and touch only its own
-buffers, so its final state, residual norm, objective and hydrogen total must
-be bitwise the same whether it ran alone or overlapped with others."""
+Tolerance: none.  The server merges the evaluations of the running jobs into
+shared batched launches (continuous batching); every kernel is
+deterministic, a job's rows never mix with another's and the kernel shapes
+are fixed, so a job's final state, residual norm, objective and hydrogen
+total must be bitwise the same whether it ran alone or in a mix."""
 import numpy as np
 import pytest
 
@@ -52,8 +54,11 @@ def test_server_results_alone_equal_in_mix(gpu_tables):
     ids = [srv.submit(s, **kw) for s, kw in jobs for _ in range(2)]
     mixed = [srv.wait(i) for i in ids]
     st = srv.stats()
+    bs = srv.batch_stats()
     srv.close()
     assert st["completed"] >= len(ids) and st["failed"] == 0
+    # evaluations were shared: rounds served several jobs at once
+    assert bs["evaluations"] > bs["rounds"] > 0 and bs["rebuilds"] > 0
     for k, r in enumerate(mixed):
         same(alone[k // 2], r)
     # the jobs did overlap: some job started before another had ended
