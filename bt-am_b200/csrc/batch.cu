@@ -530,8 +530,14 @@ int batch_round(btam_batch *b, const BatchXfer &t, const cudaEvent_t *ready, int
   batch_gather_kernel<<<grid, 256, 0, b->st>>>(t, b->pos, b->xb);
   BTAM_TRY(cudaGetLastError());
   BTAM_TRY(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
-  int st = btam_batch_eval_async(b, precision);
+  // the kernels are launched directly, not replayed from a captured graph:
+  // the other jobs' threads keep making CUDA calls meanwhile (their
+  // neighbour builds free scratch memory with cudaFree, which synchronises
+  // implicitly and must never meet a stream in capture)
+  int st = ensure_moments(b, precision);
   if (st != BTAM_OK) return st;
+  BTAM_TRY(precision == BTAM_FP64 ? enqueue_eval<double>(b, 0, b->mom64, b->T->r64)
+                                  : enqueue_eval<float>(b, 1, b->mom32, b->T->r32));
   batch_scatter_kernel<<<grid, 256, 0, b->st>>>(t, b->rho, b->V0, b->S0, b->Rq, b->Rs, b->Rx,
                                                  b->totals, b->err);
   return cuda_status(cudaGetLastError());

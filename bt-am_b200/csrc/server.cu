@@ -17,7 +17,7 @@
 // The batcher collects the requests of every running job (or those that
 // arrive within a short window), copies their states into one batch layout
 // (batch.cu: every job's sites renumbered into one device layout, rebuilt
-// when a job joins), evaluates them all with one graph launch, and copies
+// when a job joins), evaluates them all with one set of launches, and copies
 // each job's results back into its own buffers; the job's stream waits for
 // that and carries on.  So the jobs in flight share every evaluation launch
 // instead of each launching its own kernels, and a job's results are the
@@ -92,6 +92,9 @@ struct EvalBatcher {
   bool joined = false;                 // a member is missing from the batch layout
   std::vector<Req *> pending;
   Clock::time_point first_pending;
+  // a round is running on a copy of the members: a job must not leave (and
+  // destroy its system) until it ends
+  bool in_round = false;
   // the batch and the systems of its layout (a system that left keeps its
   // rows until the next rebuild; they are evaluated but nobody reads them)
   btam_batch *batch = nullptr;
@@ -200,9 +203,11 @@ void batcher_main(EvalBatcher *B) {
       if (!B->layout.count(r->s)) rebuild = true;
     B->joined = false;
     if (rebuild) B->departed_sites = 0;
+    B->in_round = true;
     lock.unlock();
     const int st = batcher_round(B, round, members, rebuild);
     lock.lock();
+    B->in_round = false;
     for (auto *r : round) {
       r->status = st;
       r->done = true;
@@ -223,10 +228,13 @@ int batcher_attach(EvalBatcher *B, btam_system *s) {
 }
 
 // Detaches a system whose work has finished (its stream is idle, so no round
-// still reads or writes its buffers).
+// still reads or writes its buffers), once no round is running: a round
+// works on a copy of the members and may be rebuilding the batch from it.
 void batcher_detach(EvalBatcher *B, btam_system *s) {
   {
-    std::lock_guard<std::mutex> lock(B->mu);
+    std::unique_lock<std::mutex> lock(B->mu);
+    // a running round may be rebuilding the batch from this system
+    B->cv.wait(lock, [&] { return !B->in_round; });
     B->members.erase(std::find(B->members.begin(), B->members.end(), s));
     // its rows stay in the batch until the next rebuild
     if (B->layout.erase(s)) B->departed_sites += s->n_real;

@@ -536,9 +536,9 @@ int btam_batch_totals_copy(btam_batch *b, double *totals);
  * head).  Each running job owns a system and its stream: its state and
  * neighbour lists stay resident on the device until it ends.  Continuous
  * batching: the residual evaluations of all running jobs are merged, round
- * by round, into one batched launch (one graph over every running job's
- * sites); jobs join at the next round after they start and leave when they
- * end.  A job's results equal those of the same job run alone
+ * by round, into one batched evaluation (one set of launches over every
+ * running job's sites); jobs join at the next round after they start and
+ * leave when they end.  A job's results equal those of the same job run alone
  * (deterministic kernels, fixed kernel shapes, rows never shared). */
 typedef struct btam_server btam_server;
 
