@@ -272,8 +272,12 @@ int batch_build(btam_batch *b) {
   std::vector<int> seg(ns + 1);
   for (int k = 0; k < ns; ++k) {
     btam_system *s = b->sys[k];
-    int last = 0;  // real sites' pairs: offs[n_real] (the list may also cover images)
-    BTAM_TRY(copy_sync(&last, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    // real sites' pairs: offs[n_real]; when the lists cover the real sites
+    // only that is every entry, known on the host (no wait on the system's
+    // stream); when they also cover the images it is read back
+    int last = (int)s->n_pairs;
+    if (s->n_list != s->n_real)
+      BTAM_TRY(copy_sync(&last, s->offs + s->n_real, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     n_list_pairs[k] = last;
     if (n_real + n_img + s->n_real + s->n_ghost > 0x7fffffffLL || n_pairs + last > 0x7fffffffLL)
       return BTAM_ERR_TOO_LARGE;

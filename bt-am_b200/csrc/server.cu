@@ -10,8 +10,10 @@
 // A job that arrives while others run starts as soon as a worker slot and
 // its memory are free.
 //
-// Continuous batching: the residual evaluations of all running jobs go
-// through one batcher (EvalBatcher below).  A job's solver (L-BFGS steps,
+// Continuous batching: the residual evaluations of all running jobs of up
+// to kBatchMaxSites sites go through one batcher (EvalBatcher below); larger
+// jobs run their own kernels on their own streams, overlapping with the
+// rounds.  A job's solver (L-BFGS steps,
 // master-equation steps) runs on its own thread and stream as before; each
 // time it needs an evaluation it hands its system to the batcher and waits.
 // The batcher collects the requests of every running job (or those that
@@ -76,6 +78,12 @@ constexpr int kServeVariant2[2] = {btam::kUndirected | btam::kPersistent | 0,
                                    btam::kUndirected | btam::kPersistent | 2};
 // How long a round waits for the running jobs that have not asked yet.
 constexpr int kRoundWaitUs = 400;
+// Jobs of at most this many sites share the batched evaluations; larger
+// jobs fill the GPU on their own and run their own kernels on their own
+// streams (their launch and synchronisation overheads are a small part of
+// their evaluations, and a shared round would make the small jobs wait for
+// them).
+constexpr int kBatchMaxSites = 8192;
 
 struct EvalBatcher {
   int device = 0;
@@ -295,13 +303,17 @@ void run_job(btam_server *srv, Job *job) {
                               job->gamma.empty() ? nullptr : job->gamma.data(), job->origin,
                               job->cell, job->periodic, &s);
   if (st == BTAM_OK) st = btam_neighbors_build(s, 0);
-  // jobs hand their evaluations to the batcher (the undirected kernels on
-  // persistent grids, in the batch's buffers, which btam_estimate_bytes
-  // counts), unless they ask for the plain two-pass pair on their own
+  // small jobs hand their evaluations to the batcher (the undirected
+  // kernels on persistent grids, in the batch's buffers, which
+  // btam_estimate_bytes counts); large jobs run the same kernels on their
+  // own stream; a job that asks for the plain two-pass pair runs it alone
   bool attached = false;
-  if (st == BTAM_OK && !sp.plain) {
+  if (st == BTAM_OK && !sp.plain && n <= kBatchMaxSites) {
     st = batcher_attach(&srv->batcher, s);
     attached = st == BTAM_OK;
+  } else if (st == BTAM_OK && !sp.plain) {
+    st = btam_set_variants(s, BTAM_FP32C, kServeVariant1[1], kServeVariant2[1]);
+    if (st == BTAM_OK) st = btam_set_variants(s, BTAM_FP64, kServeVariant1[0], kServeVariant2[0]);
   }
   if (st == BTAM_OK) {
     r.t_start = since(srv->t0);

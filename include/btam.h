@@ -535,10 +535,11 @@ int btam_batch_totals_copy(btam_batch *b, double *totals);
  * job may overtake the head of the queue only if it leaves room for the
  * head).  Each running job owns a system and its stream: its state and
  * neighbour lists stay resident on the device until it ends.  Continuous
- * batching: the residual evaluations of all running jobs are merged, round
- * by round, into one batched evaluation (one set of launches over every
- * running job's sites); jobs join at the next round after they start and
- * leave when they end.  A job's results equal those of the same job run alone
+ * batching: the residual evaluations of the running jobs of up to 8192
+ * sites are merged, round by round, into one batched evaluation (one set of
+ * launches over those jobs' sites); jobs join at the next round after they
+ * start and leave when they end.  Larger jobs run their own kernels on
+ * their own streams, overlapping with the rounds.  A job's results equal those of the same job run alone
  * (deterministic kernels, fixed kernel shapes, rows never shared). */
 typedef struct btam_server btam_server;
 
