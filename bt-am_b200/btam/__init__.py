@@ -53,6 +53,10 @@ _PROTOS = {
     "btam_tables_destroy": (None, [_V]),
     "btam_tables_mass": (ctypes.c_double, [_V, ctypes.c_int]),
     "btam_tables_spline": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, _D, _D, _D]),
+    "btam_term_eval": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, _D, _D, _I, _D]),
+    "btam_term_quadrature": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                            ctypes.c_int, ctypes.c_int, _D, _D, _D, _I, _D]),
     "btam_system_create": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _I, _D, _D, _D, _D,
                                           _I, ctypes.POINTER(_V)]),
     "btam_system_destroy": (None, [_V]),
@@ -245,6 +249,40 @@ class Tables:
         _check(lib().btam_tables_spline(self.handle, table, len(r), _d(r), _d(v), _d(dv)),
                "btam_tables_spline")
         return v, dv
+
+    def term(self, term, fn, direction, q, x, species):
+        """One slot of the per-term plugin table (potential_function) at n
+        geometries: term 0 rho_ij, 1 V_pair_ij, 2 V_dipole_ij1j2,
+        3 V_quadrupole_ij1j2; fn 0 F, 1 dF_dq, 2 d2F_dq2, 3 dF_dq_FD,
+        4 d2F_dq2_FD, 5 dF_dn.  q (n, 9), x and species (n, 3); returns
+        (n, 9), the slot's values first."""
+        q = np.ascontiguousarray(np.asarray(q, np.float64).reshape(-1, 9))
+        x = np.ascontiguousarray(np.asarray(x, np.float64).reshape(-1, 3))
+        sp = np.ascontiguousarray(np.asarray(species, np.int32).reshape(-1, 3))
+        n = len(q)
+        if len(x) != n or len(sp) != n:
+            raise ValueError("q, x and species need one row per geometry")
+        out = np.zeros((n, 9))
+        _check(lib().btam_term_eval(self.handle, int(term), int(fn), int(direction), n, _d(q),
+                                    _d(x), _i(sp), _d(out)), "btam_term_eval")
+        return out
+
+    def term_quadrature(self, term, mode, slot, q, sigma, x, species, coincident=False):
+        """A term averaged over the mean-field measure with the degree-3
+        rule: mode 0 the value, 1 d/d mean q of slot (3 values), 2 d/d
+        sigma of slot, 3 d/dx of slot.  Returns (n, 9), the values first."""
+        q = np.ascontiguousarray(np.asarray(q, np.float64).reshape(-1, 9))
+        sg = np.ascontiguousarray(np.asarray(sigma, np.float64).reshape(-1, 3))
+        x = np.ascontiguousarray(np.asarray(x, np.float64).reshape(-1, 3))
+        sp = np.ascontiguousarray(np.asarray(species, np.int32).reshape(-1, 3))
+        n = len(q)
+        if len(sg) != n or len(x) != n or len(sp) != n:
+            raise ValueError("q, sigma, x and species need one row per geometry")
+        out = np.zeros((n, 9))
+        _check(lib().btam_term_quadrature(self.handle, int(term), int(mode), int(slot),
+                                          int(bool(coincident)), n, _d(q), _d(sg), _d(x),
+                                          _i(sp), _d(out)), "btam_term_quadrature")
+        return out
 
     def close(self):
         if self.handle:

@@ -1073,6 +1073,287 @@ __global__ void __launch_bounds__(128) mp_rho_grad_kernel(MpArgs a, double *G) {
   }
 }
 
+// ---- the per-term plugin interface ------------------------------------------
+// The reference's potential_function table (Macros.hpp:252-278) of its four
+// ADP terms, rho_ij (MgHx-ADP.cpp:526-844), V_pair_ij (869-1209),
+// V_dipole_ij1j2 (1233-1758) and V_quadrupole_ij1j2 (1781-2434), one
+// geometry per thread: F, dF_dq, d2F_dq2, dF_dq_FD, d2F_dq2_FD and dF_dn,
+// and their averages over the reference's measure with the degree-3 rule.
+// Values, gradients, occupancy derivatives and the finite differences use
+// the restated functions above (the reference's operation order, no
+// contraction); the analytic Hessian blocks are formed here from the
+// terms' radial, vector and tensor parts.
+struct TermArgs {
+  RadialView<double> T;
+  int term, fn, dir, ns, n;
+  int mode, coincident;   // quadratures
+  const double *q, *x, *sigma;
+  const int *code;        // 3 per geometry: 0 Mg, 1 H
+  double *out;            // 9 per geometry
+};
+
+__device__ double term_F(const RadialView<double> &T, int term, const int *c, const double *n,
+                         const double (&q)[9]) {
+  const int pk1 = pair_kind(c[0], c[1]);
+  if (term == 0) return rho_F(T, pk1, c[1], n[1], q);
+  if (term == 1) return pair_F(T, pk1, n[0], n[1], q);
+  double fd, fq;
+  tri_F(T, pk1, pair_kind(c[0], c[2]), n, q, fd, fq);
+  return term == 2 ? fd : fq;
+}
+__device__ void term_dq(const RadialView<double> &T, int term, const int *c, const double *n,
+                        int dir, const double *q, double *g) {
+  const int pk1 = pair_kind(c[0], c[1]);
+  if (term == 0) {
+    rho_dq(T, pk1, c[1], n[1], dir, q, g);
+  } else if (term == 1) {
+    pair_dq(T, pk1, n[0], n[1], dir, q, g);
+  } else {
+    double gd[3], gq[3];
+    tri_dq(T, pk1, pair_kind(c[0], c[2]), n, dir, q, gd, gq);
+    for (int a = 0; a < 3; ++a) g[a] = term == 2 ? gd[a] : gq[a];
+  }
+}
+__device__ double term_dn(const RadialView<double> &T, int term, const int *c, const double *n,
+                          int dir, const double *q) {
+  const int pk1 = pair_kind(c[0], c[1]);
+  if (term == 0) return rho_dn(T, pk1, c[1], dir, q);
+  if (term == 1) return pair_dn(T, pk1, n, dir, q);
+  double vd, vq;
+  tri_dn(T, pk1, pair_kind(c[0], c[2]), n, dir, q, vd, vq);
+  return term == 2 ? vd : vq;
+}
+
+// Spline value and first and second derivatives of four coefficients.
+__device__ __forceinline__ void cub3(const double *k, double p, double (&f)[3]) {
+  f[0] = cubv(k, p);
+  f[1] = cubd(k, p);
+  f[2] = cubdd(k, p);
+}
+// H (3x3) += c (f'' P + f' (I - P) / s), P = r r^T / s^2: the Hessian of
+// c f(|r|) in r.
+__device__ void hess_radial(const double *r, double s, double d1, double d2, double c,
+                            double *H) {
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      const double P = r[a] * r[b] / (s * s);
+      H[3 * a + b] += c * (d2 * P + d1 * ((a == b ? 1.0 : 0.0) - P) / s);
+    }
+}
+
+// The analytic Hessian block `dir` of a term at one geometry, as the
+// reference's d2F_dq2 numbers them: pairs 0 (i i), 1 and 2 (i j, j i), 3
+// (j j); triplets 3 a + b for slots (a, b), of which the reference forms 0,
+// 4, 5, 7 and 8 and leaves the others zero.  With r_k = q_0 - q_k, the
+// blocks follow from H11 = d2V/dr1^2, H22 and H12 = d2V/dr1 dr2:
+// (0, 0) = H11 + H22 + H12 + H12^T, (1, 1) = H11, (2, 2) = H22,
+// (1, 2) = H12, (2, 1) = H12^T.
+__device__ void term_d2(const RadialView<double> &T, int term, const int *c, const double *n,
+                        int dir, const double *q, double *out) {
+  for (int e = 0; e < 9; ++e) out[e] = 0.0;
+  if (term < 2) {
+    const int pk = pair_kind(c[0], c[1]);
+    double r[3];
+    for (int a = 0; a < 3; ++a) r[a] = q[a] - q[3 + a];
+    const double s = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    double p, f[3];
+    const int m = seg_ref(s, T.dx, T.n, p);
+    cub3(term == 0 ? pr_rec(T, pk, m) + rho_off(pk, c[1]) : pr_rec(T, pk, m), p, f);
+    const double cf = term == 0 ? n[1] : 0.5 * n[0] * n[1];
+    hess_radial(r, s, f[1], f[2], (dir == 1 || dir == 2) ? -cf : cf, out);
+    return;
+  }
+  if (!(dir == 0 || dir == 4 || dir == 5 || dir == 7 || dir == 8)) return;
+  double r1[3], r2[3];
+  for (int a = 0; a < 3; ++a) {
+    r1[a] = q[a] - q[3 + a];
+    r2[a] = q[a] - q[6 + a];
+  }
+  const double s1 = sqrt(r1[0] * r1[0] + r1[1] * r1[1] + r1[2] * r1[2]);
+  const double s2 = sqrt(r2[0] * r2[0] + r2[1] * r2[1] + r2[2] * r2[2]);
+  const double dd = r1[0] * r2[0] + r1[1] * r2[1] + r1[2] * r2[2];
+  const double c1 = n[0] * n[1], c2 = n[0] * n[2];
+  double p1, p2, f1[3], f2[3];
+  const int m1 = seg_ref(s1, T.dx, T.n, p1), m2 = seg_ref(s2, T.dx, T.n, p2);
+  const int off = term == 2 ? 0 : 4;  // u or w in the segment record
+  cub3(uw_rec(T, pair_kind(c[0], c[1]), m1) + off, p1, f1);
+  cub3(uw_rec(T, pair_kind(c[0], c[2]), m2) + off, p2, f2);
+  double H11[9] = {0}, H22[9] = {0}, H12[9] = {0};
+  if (term == 2) {
+    // 1/2 A1.A2 with A_k = c_k u(s_k) r_k
+    double A1[3], A2[3];
+    for (int a = 0; a < 3; ++a) {
+      A1[a] = c1 * f1[0] * r1[a];
+      A2[a] = c2 * f2[0] * r2[a];
+    }
+    auto vec = [&](const double *mv, const double *r, double s, const double (&f)[3], double cc,
+                   double *H) {
+      const double mr = mv[0] * r[0] + mv[1] * r[1] + mv[2] * r[2];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          const double P = r[a] * r[b] / (s * s);
+          H[3 * a + b] += cc * (f[1] * (mv[a] * r[b] + r[a] * mv[b]) / s +
+                                mr * (f[2] * P + f[1] * ((a == b ? 1.0 : 0.0) - P) / s));
+        }
+    };
+    vec(A2, r1, s1, f1, 0.5 * c1, H11);
+    vec(A1, r2, s2, f2, 0.5 * c2, H22);
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) {
+        double acc = 0.0;
+        for (int z = 0; z < 3; ++z)
+          acc += c1 * ((z == x ? f1[0] : 0.0) + f1[1] * r1[z] * r1[x] / s1) * c2 *
+                 ((z == y ? f2[0] : 0.0) + f2[1] * r2[z] * r2[y] / s2);
+        H12[3 * x + y] = 0.5 * acc;
+      }
+  } else {
+    // 1/2 B1:B2 - 1/6 t1 t2 with B_k = c_k w(s_k) r_k r_k^T, t_k = c_k w(s_k) s_k^2
+    const double t1 = c1 * f1[0] * s1 * s1, t2 = c2 * f2[0] * s2 * s2;
+    const double hp1 = f1[1] * s1 * s1 + 2.0 * f1[0] * s1;
+    const double hpp1 = f1[2] * s1 * s1 + 4.0 * f1[1] * s1 + 2.0 * f1[0];
+    const double hp2 = f2[1] * s2 * s2 + 2.0 * f2[0] * s2;
+    const double hpp2 = f2[2] * s2 * s2 + 4.0 * f2[1] * s2 + 2.0 * f2[0];
+    auto ten = [&](const double *r_o, double c_o, double w_o, const double *r, double s,
+                   const double (&f)[3], double cc, double *H) {
+      // sum_ab M_ab d2 (w(s) r_a r_b) with M = c_o w_o r_o r_o^T
+      double Mr[3];
+      const double ro_r = r_o[0] * r[0] + r_o[1] * r[1] + r_o[2] * r[2];
+      for (int a = 0; a < 3; ++a) Mr[a] = c_o * w_o * r_o[a] * ro_r;
+      const double rMr = r[0] * Mr[0] + r[1] * Mr[1] + r[2] * Mr[2];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) {
+          const double P = r[a] * r[b] / (s * s);
+          H[3 * a + b] += cc * (rMr * (f[2] * P + f[1] * ((a == b ? 1.0 : 0.0) - P) / s) +
+                                2.0 * f[1] * (r[a] * Mr[b] + Mr[a] * r[b]) / s +
+                                2.0 * f[0] * c_o * w_o * r_o[a] * r_o[b]);
+        }
+    };
+    ten(r2, c2, f2[0], r1, s1, f1, 0.5 * c1, H11);
+    hess_radial(r1, s1, hp1, hpp1, -t2 * c1 / 6.0, H11);
+    ten(r1, c1, f1[0], r2, s2, f2, 0.5 * c2, H22);
+    hess_radial(r2, s2, hp2, hpp2, -t1 * c2 / 6.0, H22);
+    for (int x = 0; x < 3; ++x)
+      for (int y = 0; y < 3; ++y) {
+        const double G =
+            c1 * c2 *
+            (f1[1] * f2[1] * (r1[x] / s1) * (r2[y] / s2) * dd * dd +
+             2.0 * f1[1] * f2[0] * (r1[x] / s1) * r1[y] * dd +
+             2.0 * f1[0] * f2[1] * r2[x] * (r2[y] / s2) * dd +
+             2.0 * f1[0] * f2[0] * ((x == y ? dd : 0.0) + r2[x] * r1[y]));
+        const double g1 = c1 * hp1 * r1[x] / s1, g2 = c2 * hp2 * r2[y] / s2;
+        H12[3 * x + y] = 0.5 * G - g1 * g2 / 6.0;
+      }
+  }
+  for (int x = 0; x < 3; ++x)
+    for (int y = 0; y < 3; ++y) {
+      const int e = 3 * x + y, et = 3 * y + x;
+      out[e] = dir == 0 ? H11[e] + H22[e] + H12[e] + H12[et]
+               : dir == 4 ? H11[e] : dir == 8 ? H22[e] : dir == 5 ? H12[e] : H12[et];
+    }
+}
+
+__global__ void __launch_bounds__(128) term_eval_kernel(TermArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n) return;
+  double q[9], n[3];
+  int c[3];
+  for (int e = 0; e < 9; ++e) q[e] = e < 3 * a.ns ? a.q[9 * (size_t)k + e] : 0.0;
+  for (int s = 0; s < 3; ++s) {
+    n[s] = s < a.ns ? a.x[3 * (size_t)k + s] : 0.0;
+    c[s] = s < a.ns ? a.code[3 * (size_t)k + s] : 0;
+  }
+  double out[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (a.fn == 0) {
+    out[0] = term_F(a.T, a.term, c, n, q);
+  } else if (a.fn == 1) {
+    term_dq(a.T, a.term, c, n, a.dir, q, out);
+  } else if (a.fn == 2) {
+    term_d2(a.T, a.term, c, n, a.dir, q, out);
+  } else if (a.fn == 3) {
+    // dF_dq_FD: five points with step 1e-4 (1e-5 for the pair term,
+    // dV_pair_ij_dq_FD) along each coordinate of slot dir; the moved
+    // coordinate keeps its last position (+2 dr) while the next one moves,
+    // as the reference's shared work array does
+    const double dr = a.term == 1 ? 0.00001 : 0.0001;
+    const double f0 = term_F(a.T, a.term, c, n, q);
+    double qn[9];
+    for (int e = 0; e < 9; ++e) qn[e] = q[e];
+    for (int al = 0; al < 3; ++al) {
+      const int d = a.dir * 3 + al;
+      qn[d] = q[d] - dr * 2;
+      const double fmm = term_F(a.T, a.term, c, n, qn);
+      qn[d] = q[d] - dr;
+      const double fm = term_F(a.T, a.term, c, n, qn);
+      qn[d] = q[d] + dr;
+      const double fp = term_F(a.T, a.term, c, n, qn);
+      qn[d] = q[d] + dr * 2;
+      const double fpp = term_F(a.T, a.term, c, n, qn);
+      out[al] = ((fmm - f0) - 8.0 * (fm - f0) + 8.0 * (fp - f0) - (fpp - f0)) / (12.0 * dr);
+    }
+  } else if (a.fn == 4) {
+    // d2F_dq2_FD: the diagonal entries only, second differences along the
+    // coordinates of slot dir / (ns + 1); the quadrupole's fills blocks 0,
+    // 4 and 8 only (dV2_quadrupole_ij1j2_dq2_FD)
+    const double f0 = term_F(a.T, a.term, c, n, q);
+    for (int al = 0; al < 3 && !(a.term == 3 && a.dir % 4 != 0); ++al) {
+      const int d = a.dir / (1 + a.ns) * 3 + al;
+      double s4[4];
+      for (int w = 0; w < 4; ++w) {
+        double qq[9];
+        shifted(q, d, w, qq);
+        s4[w] = term_F(a.T, a.term, c, n, qq);
+      }
+      out[4 * al] = d2_5(s4[0], s4[1], f0, s4[2], s4[3]);
+    }
+  } else {
+    out[0] = term_dn(a.T, a.term, c, n, a.dir, q);
+  }
+  for (int e = 0; e < 9; ++e) a.out[9 * (size_t)k + e] = out[e];
+}
+
+// The same terms averaged over the reference's measure with the degree-3
+// rule (meanfield_integral_gh3th, _gh_3th_dmq, _gh3th_dsq, _gh_3th_dxi,
+// Quadrature-Hermitian-3th.cpp:36-378): mode 0 the value, 1 d/d mean q of
+// slot dir (3 values), 2 d/d sigma of slot dir, 3 d/dx of slot dir.
+__global__ void __launch_bounds__(128) term_quad_kernel(TermArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n) return;
+  double q[9], n[3], sig[3];
+  int c[3];
+  for (int e = 0; e < 9; ++e) q[e] = e < 3 * a.ns ? a.q[9 * (size_t)k + e] : 0.0;
+  for (int s = 0; s < 3; ++s) {
+    n[s] = s < a.ns ? a.x[3 * (size_t)k + s] : 0.0;
+    sig[s] = s < a.ns ? a.sigma[3 * (size_t)k + s] : 0.0;
+    c[s] = s < a.ns ? a.code[3 * (size_t)k + s] : 0;
+  }
+  const Gh3 m = gh3_of(a.ns, a.coincident != 0);
+  const double W = 1.0 / (2.0 * m.D), zeta = sqrt((double)m.D) / kSqrt2d;
+  double out[3] = {0, 0, 0};
+  for (int sg = 0; sg < 2; ++sg)
+    for (int l = 0; l < m.D; ++l) {
+      const double sgn = sg == 0 ? 1.0 : -1.0;
+      double ql[9];
+      gh3_point(m, q, sig, l, sgn, ql);
+      if (a.mode == 0) {
+        out[0] += term_F(a.T, a.term, c, n, ql) * W;
+      } else if (a.mode == 3) {
+        out[0] += term_dn(a.T, a.term, c, n, a.dir, ql) * W;
+      } else {
+        double g[3];
+        term_dq(a.T, a.term, c, n, a.dir, ql, g);
+        for (int al = 0; al < 3; ++al) {
+          if (a.mode == 1) {
+            out[al] += g[al] * W;
+          } else {
+            const double b = (m.grp[a.dir] == l / 3 && al == l % 3) ? 1.0 : 0.0;
+            out[0] += g[al] * (sgn * kSqrt2d * zeta * b) * W;
+          }
+        }
+      }
+    }
+  for (int e = 0; e < 9; ++e) a.out[9 * (size_t)k + e] = e < 3 ? out[e] : 0.0;
+}
+
 }  // namespace
 }  // namespace btam
 
@@ -1380,6 +1661,95 @@ int btam_mf_hessian_pairs_multipole(btam_system *s, int rule, double *Hself, dou
                                     long long slot_cap) {
   if (!Hself || !Hslot) return BTAM_ERR_ARG;
   return mp_hessian(s, rule, Hself, Hslot, slot_cap);
+}
+
+}  // extern "C"
+
+// ---- the per-term plugin interface (C ABI) ----------------------------------
+namespace {
+
+int term_launch(const btam_tables *t, bool quad, int term, int fn_or_mode, int dir, int slot_ns,
+                int coincident, int n, const double *q, const double *sigma, const double *x,
+                const int *species, double *out) {
+  if (!t || n < 0 || !q || !x || !species || !out || (quad && !sigma)) return BTAM_ERR_ARG;
+  if (term < 0 || term > 3) return BTAM_ERR_ARG;
+  const int ns = term < 2 ? 2 : 3;
+  if (slot_ns != ns) return BTAM_ERR_ARG;
+  if (quad ? (fn_or_mode < 0 || fn_or_mode > 3) : (fn_or_mode < 0 || fn_or_mode > 5))
+    return BTAM_ERR_ARG;
+  const bool block = !quad && (fn_or_mode == 2 || fn_or_mode == 4);
+  if (fn_or_mode != 0 && (dir < 0 || dir >= (block ? ns * ns : ns))) return BTAM_ERR_ARG;
+  if (n == 0) return BTAM_OK;
+  std::vector<int> code(3 * (size_t)n, 0);
+  for (size_t k = 0; k < 3 * (size_t)n; ++k) {
+    if (k % 3 >= (size_t)ns) continue;
+    if (species[k] == 12) code[k] = 0;
+    else if (species[k] == 1) code[k] = 1;
+    else return BTAM_ERR_SPECIES;
+  }
+  cudaStream_t st = cudaStreamPerThread;
+  double *dq = nullptr, *dx = nullptr, *ds = nullptr, *dout = nullptr;
+  int *dc = nullptr;
+  cudaError_t e = dalloc(dq, st, 9 * (size_t)n);
+  if (e == cudaSuccess) e = dalloc(dx, st, 3 * (size_t)n);
+  if (e == cudaSuccess) e = dalloc(ds, st, 3 * (size_t)n);
+  if (e == cudaSuccess) e = dalloc(dout, st, 9 * (size_t)n);
+  if (e == cudaSuccess) e = dalloc(dc, st, 3 * (size_t)n);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dq, q, 9 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && quad)
+    e = cudaMemcpyAsync(ds, sigma, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dc, code.data(), 3 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    TermArgs a;
+    a.T = t->r64;
+    a.term = term;
+    a.fn = quad ? 0 : fn_or_mode;
+    a.mode = quad ? fn_or_mode : 0;
+    a.dir = dir;
+    a.ns = ns;
+    a.n = n;
+    a.coincident = coincident;
+    a.q = dq;
+    a.x = dx;
+    a.sigma = ds;
+    a.code = dc;
+    a.out = dout;
+    const int g = (n + 127) / 128;
+    if (quad) term_quad_kernel<<<g, 128, 0, st>>>(a);
+    else term_eval_kernel<<<g, 128, 0, st>>>(a);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(out, dout, 9 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  dfree(dq, st);
+  dfree(dx, st);
+  dfree(ds, st);
+  dfree(dout, st);
+  dfree(dc, st);
+  return cuda_status(e);
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_term_eval(const btam_tables *t, int term, int fn, int direction, int n,
+                   const double *q, const double *x, const int *species, double *out) {
+  return term_launch(t, false, term, fn, direction, term < 2 ? 2 : 3, 0, n, q, nullptr, x,
+                     species, out);
+}
+
+int btam_term_quadrature(const btam_tables *t, int term, int mode, int slot, int coincident,
+                         int n, const double *q, const double *sigma, const double *x,
+                         const int *species, double *out) {
+  if (coincident && term < 2) return BTAM_ERR_ARG;
+  return term_launch(t, true, term, mode, slot, term < 2 ? 2 : 3, coincident, n, q, sigma, x,
+                     species, out);
 }
 
 }  // extern "C"

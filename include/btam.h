@@ -103,6 +103,37 @@ double btam_tables_mass(const btam_tables *t, int species);
 int btam_tables_spline(const btam_tables *t, int table, int n, const double *r,
                        double *value, double *deriv);
 
+/* The per-term plugin table (potential_function, Macros.hpp:252-278) of
+ * the four ADP terms: term 0 rho_ij (MgHx-ADP.cpp:526-844), 1 V_pair_ij
+ * (869-1209), 2 V_dipole_ij1j2 (1233-1758), 3 V_quadrupole_ij1j2
+ * (1781-2434), for n geometries at once on the device, FP64.  fn selects
+ * the slot: 0 F, 1 dF_dq, 2 d2F_dq2, 3 dF_dq_FD, 4 d2F_dq2_FD, 5 dF_dn;
+ * direction is the slot's direction argument (a site for 1, 3 and 5; a
+ * block ns * a + b for 2 and 4).  q: 9 per geometry (site-major, 6 used
+ * by the pair terms), x and species: 3 per geometry (species 12 = Mg,
+ * 1 = H; 2 used by the pair terms), out: 9 per geometry, the slot's
+ * values first (1 for F and dF_dn, 3 for dF_dq, a 3x3 row-major block for
+ * the Hessians) and zeros after.  Where the reference leaves a value
+ * unset (the triplet Hessian blocks other than 0, 4, 5, 7 and 8, the
+ * off-diagonal entries of the FD Hessians, the quadrupole's FD blocks other
+ * than 0, 4 and 8) out holds 0, as the reference's zeroed outputs do.  The
+ * finite-difference gradient steps by 1e-4, by 1e-5 for V_pair_ij, as the
+ * reference's do.  BTAM_ERR_SPECIES for a species other
+ * than 12 and 1. */
+int btam_term_eval(const btam_tables *t, int term, int fn, int direction, int n,
+                   const double *q, const double *x, const int *species, double *out);
+/* The same terms averaged over the mean-field measure of each geometry
+ * (means q, widths sigma: 3 per geometry) with the degree-3 rule:
+ * mode 0 meanfield_integral_gh3th, 1 _gh_3th_dmq (d/d mean q of slot,
+ * 3 values), 2 _gh3th_dsq (d/d sigma of slot), 3 _gh_3th_dxi (d/dx of
+ * slot) (Quadrature-Hermitian-3th.cpp:36-378) over the pair or triplet
+ * measure (Quadrature-Measure.cpp:30-109); coincident != 0 (triplets
+ * only) is the measure with j1 = j2, one group for both.  out: 9 per
+ * geometry, the 1 or 3 values first. */
+int btam_term_quadrature(const btam_tables *t, int term, int mode, int slot, int coincident,
+                         int n, const double *q, const double *sigma, const double *x,
+                         const int *species, double *out);
+
 /* Replaces read_dump_information + init_DMD_simulation (dump-input.cpp:
  * 51-214, Atom.cpp:80-431): one system of n sites with its DMSwarm fields
  * (coordinates, "stdv-q", "molar-fraction", "specie", "beta", "gamma").

@@ -497,7 +497,72 @@ inline double DV0_Dxi(unsigned u, unsigned i, const Eigen::MatrixXd &mean_q,
 }
 
 }  // namespace detail
+
+/* The per-term table (potential_function, Macros.hpp:252-278) of the four
+ * ADP terms, served by btam_term_eval on the tables bound here.  The
+ * functions keep the reference's signatures and write what the reference's
+ * write (MgHx-ADP.cpp:509-2434): 1 value for F and dF_dn, 3 for the
+ * gradients, a zeroed 3x3 block for the Hessians.  Each call is one device
+ * evaluation of one geometry; a caller with many geometries calls
+ * btam_term_eval once for all of them instead. */
+inline const btam_tables *&term_tables() {
+  static const btam_tables *t = nullptr;
+  return t;
+}
+inline void bind_tables(const btam_tables *t) { term_tables() = t; }
+
+namespace detail {
+template <int Term, int Fn>
+void term_slot(int direction, double *out, const double *xi, const double *q,
+               const AtomicSpecie *spc) {
+  const int ns = Term < 2 ? 2 : 3;
+  const int width = (Fn == 0 || Fn == 5) ? 1 : (Fn == 2 || Fn == 4) ? 9 : 3;
+  double qq[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, xx[3] = {0, 0, 0}, r[9];
+  int sp[3] = {0, 0, 0};
+  for (int k = 0; k < 3 * ns; ++k) qq[k] = q[k];
+  for (int k = 0; k < ns; ++k) {
+    xx[k] = xi[k];
+    sp[k] = (int)spc[k];
+  }
+  Cache &c = cache();
+  std::lock_guard<std::mutex> lock(c.mu);
+  c.status = btam_term_eval(term_tables(), Term, Fn, direction, 1, qq, xx, sp, r);
+  for (int k = 0; k < width; ++k) out[k] = c.status == BTAM_OK ? r[k] : std::nan("");
+}
+template <int Term>
+void term_value(double *out, const double *xi, const double *q, const AtomicSpecie *spc) {
+  term_slot<Term, 0>(0, out, xi, q, spc);
+}
+template <int Term>
+potential_function term_table() {
+  potential_function f;
+  f.F = term_value<Term>;
+  f.dF_dq = term_slot<Term, 1>;
+  f.d2F_dq2 = term_slot<Term, 2>;
+  f.dF_dq_FD = term_slot<Term, 3>;
+  f.d2F_dq2_FD = term_slot<Term, 4>;
+  f.dF_dn = term_slot<Term, 5>;
+  return f;
+}
+}  // namespace detail
 }  // namespace btam_compat
+
+/* Drop-ins for rho_ij_adp_MgHx_constructor (MgHx-ADP.cpp:509-522),
+ * V_pair_ij_adp_MgHx_constructor (848-865), V_dipole_ij1j2_adp_MgHx_
+ * constructor (1213-1230) and V_quadrupole_ij1j2_adp_MgHx_constructor
+ * (1762-1777), served by the tables bound with btam_compat::bind_tables. */
+inline potential_function btam_rho_ij_adp_MgHx_constructor() {
+  return btam_compat::detail::term_table<0>();
+}
+inline potential_function btam_V_pair_ij_adp_MgHx_constructor() {
+  return btam_compat::detail::term_table<1>();
+}
+inline potential_function btam_V_dipole_ij1j2_adp_MgHx_constructor() {
+  return btam_compat::detail::term_table<2>();
+}
+inline potential_function btam_V_quadrupole_ij1j2_adp_MgHx_constructor() {
+  return btam_compat::detail::term_table<3>();
+}
 
 /* Drop-in for DMD_MgHx_constructor() (MgHx-mf-V-bulk.cpp:46-79), served by
  * the system bound with btam_compat::bind. */

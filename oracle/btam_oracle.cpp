@@ -1662,4 +1662,69 @@ void orc_dmd_update(int n, const int *code_all, const int *owner, const double *
   }
 }
 
+// One slot of the reference's per-term table (potential_function,
+// Macros.hpp:252-278) at one geometry: fn 0 F, 1 dF_dq, 2 d2F_dq2 (the
+// diagonal blocks a (ns + 1) only; other blocks return 1), 3 dF_dq_FD
+// (d_rho_ij_dq_FD, MgHx-ADP.cpp:605-661, and its three twins: five points,
+// step 1e-4, 1e-5 for the pair term, the moved coordinate left at +2 dr
+// while the next one moves), 4 d2F_dq2_FD (736-812: the diagonal of the
+// slot direction / (ns + 1)),
+// 5 dF_dn.  out: 9 values, unused ones 0.
+int orc_term_eval(int term, int fn, int dir, int ns, const double *q, const double *x,
+                  const int *spc, double *out) {
+  const Term *t = term == 0 ? &kRho : term == 1 ? &kPair : term == 2 ? &kDip
+                : term == 3 ? &kQuad : nullptr;
+  if (!t || ns != (term < 2 ? 2 : 3)) return 1;
+  for (int e = 0; e < 9; ++e) out[e] = 0.0;
+  const double dr = 0.0001;
+  if (fn == 0) {
+    out[0] = t->F(x, q, spc);
+  } else if (fn == 1) {
+    t->dq(dir, out, x, q, spc);
+  } else if (fn == 2) {
+    if (dir % (ns + 1) != 0) return 1;
+    term_d2(term, dir / (ns + 1), x, q, spc, out);
+  } else if (fn == 3) {
+    // the pair term's twin steps by 1e-5 (dV_pair_ij_dq_FD, 953-1008)
+    const double h = term == 1 ? 0.00001 : dr;
+    const double f0 = t->F(x, q, spc);
+    double qn[9];
+    for (int e = 0; e < 3 * ns; ++e) qn[e] = q[e];
+    for (int a = 0; a < 3; ++a) {
+      const int d = 3 * dir + a;
+      qn[d] = q[d] - h * 2;
+      const double fmm = t->F(x, qn, spc);
+      qn[d] = q[d] - h;
+      const double fm = t->F(x, qn, spc);
+      qn[d] = q[d] + h;
+      const double fp = t->F(x, qn, spc);
+      qn[d] = q[d] + h * 2;
+      const double fpp = t->F(x, qn, spc);
+      out[a] = ((fmm - f0) - 8.0 * (fm - f0) + 8.0 * (fp - f0) - (fpp - f0)) / (12.0 * h);
+    }
+  } else if (fn == 4) {
+    // the quadrupole's fills the diagonal blocks 0, 4 and 8 only
+    // (dV2_quadrupole_ij1j2_dq2_FD, 2270-2349)
+    if (term == 3 && dir % (ns + 1) != 0) return 0;
+    const double f0 = t->F(x, q, spc);
+    for (int a = 0; a < 3; ++a) {
+      const int d = dir / (1 + ns) * 3 + a;
+      double qs[4][9], f[4];
+      for (int w = 0; w < 4; ++w) {
+        for (int e = 0; e < 3 * ns; ++e) qs[w][e] = q[e];
+        const double D = 1.0;
+        qs[w][d] = w == 0 ? q[d] + D * dr * 2 : w == 1 ? q[d] + D * dr
+                 : w == 2 ? q[d] - D * dr : q[d] - D * dr * 2;
+        f[w] = t->F(x, qs[w], spc);
+      }
+      out[4 * a] = (-f[0] + 16.0 * f[1] - 30.0 * f0 + 16.0 * f[2] - f[3]) / (12.0 * dr * dr);
+    }
+  } else if (fn == 5) {
+    out[0] = t->dn(dir, x, q, spc);
+  } else {
+    return 1;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -52,6 +52,10 @@ int orc_neighbors(int n, const double *q, double rc, int maxn, const int *query,
 int orc_quadrature(int term, int mode, int slot, int nsites, int coincident,
                    const double *q, const double *sigma, const double *x,
                    const int *spc, double *out);
+/* One slot of the per-term table at one geometry (fn 0 F, 1 dF_dq, 2 the
+ * diagonal Hessian blocks, 3 dF_dq_FD, 4 d2F_dq2_FD, 5 dF_dn); 9 outputs. */
+int orc_term_eval(int term, int fn, int dir, int ns, const double *q, const double *x,
+                  const int *spc, double *out);
 
 /* Literal per-site drivers over a system of n sites (real + ghost) with CSR
  * neighbour lists for every site. */

@@ -74,6 +74,19 @@ class Lib:
                               _d(sigma), _d(x), _i(spc), _d(out))
         return out if mode == 1 else out[0]
 
+    def term_eval(self, term, fn, direction, q, x, spc):
+        """One slot of the per-term plugin table at one geometry (reference
+        build only: ref_term_eval); 9 values, unused ones 0."""
+        q = np.ascontiguousarray(q, np.float64).ravel()
+        x = np.ascontiguousarray(x, np.float64)
+        spc = np.ascontiguousarray(spc, np.int32)
+        out = np.zeros(9)
+        rc = self._f("term_eval")(int(term), int(fn), int(direction), len(x), _d(q), _d(x),
+                                  _i(spc), _d(out))
+        if rc:
+            raise ValueError("term_eval")
+        return out
+
     # --- per-site drivers over a system with CSR neighbour lists ----------
     def mf_rho(self, s, offs, idx, sites):
         sites = np.ascontiguousarray(sites, np.int32)

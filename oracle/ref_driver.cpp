@@ -198,6 +198,35 @@ int ref_quadrature(int term, int mode, int slot, int nsites, int coincident,
   return 0;
 }
 
+// One slot of the per-term plugin table (potential_function, Macros.hpp:
+// 252-278) of one ADP term at one geometry, through the reference's own
+// constructor: fn 0 = F, 1 = dF_dq, 2 = d2F_dq2, 3 = dF_dq_FD,
+// 4 = d2F_dq2_FD, 5 = dF_dn; out holds up to 9 values.
+int ref_term_eval(int term, int fn, int direction, int nsites, const double *q,
+                  const double *x, const int *spc, double *out) {
+  potential_function f;
+  switch (term) {
+  case 0: f = rho_ij_adp_MgHx_constructor(); break;
+  case 1: f = V_pair_ij_adp_MgHx_constructor(); break;
+  case 2: f = V_dipole_ij1j2_adp_MgHx_constructor(); break;
+  case 3: f = V_quadrupole_ij1j2_adp_MgHx_constructor(); break;
+  default: return 1;
+  }
+  AtomicSpecie sp[3];
+  for (int k = 0; k < nsites; ++k) sp[k] = (AtomicSpecie)spc[k];
+  for (int k = 0; k < 9; ++k) out[k] = 0.0;
+  switch (fn) {
+  case 0: f.F(out, x, q, sp); break;
+  case 1: f.dF_dq(direction, out, x, q, sp); break;
+  case 2: f.d2F_dq2(direction, out, x, q, sp); break;
+  case 3: f.dF_dq_FD(direction, out, x, q, sp); break;
+  case 4: f.d2F_dq2_FD(direction, out, x, q, sp); break;
+  case 5: f.dF_dn(direction, out, x, q, sp); break;
+  default: return 1;
+  }
+  return 0;
+}
+
 // evaluate_mf_rho_i_adp_MgHx (MgHx-mf-V-bulk.cpp:708-787) for each listed site.
 void ref_mf_rho(int n, const double *q, const double *sigma, const double *x,
                 const int *spc, const int *offs, const int *idx,

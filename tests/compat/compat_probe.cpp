@@ -33,6 +33,15 @@
 // reads evaluate_DV0_i_Dq_j and evaluate_DV0_i_Dxi_j of the pair (u, i),
 // moves site j by dq along x in its own mean_q array, and reads the pair
 // again: output 5 + 5 values, then the status.
+//
+// With `terms` as the only argument after the output path, the second
+// argument is a file of term geometries instead of a system: count (int),
+// then per row term, fn, direction (ints), q (9), x (3), species (3 ints).
+// The probe calls the per-term table the reference's term constructors
+// return (potential_function: F, dF_dq, d2F_dq2, dF_dq_FD, d2F_dq2_FD,
+// dF_dn of rho_ij, V_pair_ij, V_dipole_ij1j2, V_quadrupole_ij1j2) through
+// the btam_ drop-ins, one geometry per call, into a zeroed 9-value buffer
+// per row, and writes the buffers; then the status.
 #include "Macros.hpp"
 #include "btam_dmd_equations.hpp"
 
@@ -41,7 +50,51 @@
 #include <string>
 #include <vector>
 
+static int run_terms(char **argv) {
+  FILE *f = fopen(argv[2], "rb");
+  if (!f) return 2;
+  int m = 0;
+  if (fread(&m, sizeof(int), 1, f) != 1) return 2;
+  btam_tables *T = nullptr;
+  int st = btam_tables_load(argv[1], &T);
+  if (st != BTAM_OK) return 3;
+  btam_compat::bind_tables(T);
+  const potential_function tab[4] = {
+      btam_rho_ij_adp_MgHx_constructor(), btam_V_pair_ij_adp_MgHx_constructor(),
+      btam_V_dipole_ij1j2_adp_MgHx_constructor(),
+      btam_V_quadrupole_ij1j2_adp_MgHx_constructor()};
+  std::vector<double> out(9 * (size_t)m, 0.0);
+  for (int r = 0; r < m && st == BTAM_OK; ++r) {
+    int h[3], sp[3];
+    double q[9], x[3];
+    if (fread(h, sizeof(int), 3, f) != 3 || fread(q, sizeof(double), 9, f) != 9 ||
+        fread(x, sizeof(double), 3, f) != 3 || fread(sp, sizeof(int), 3, f) != 3)
+      return 2;
+    AtomicSpecie spc[3] = {(AtomicSpecie)sp[0], (AtomicSpecie)sp[1], (AtomicSpecie)sp[2]};
+    const potential_function &pf = tab[h[0]];
+    double *o = out.data() + 9 * (size_t)r;
+    switch (h[1]) {
+      case 0: pf.F(o, x, q, spc); break;
+      case 1: pf.dF_dq(h[2], o, x, q, spc); break;
+      case 2: pf.d2F_dq2(h[2], o, x, q, spc); break;
+      case 3: pf.dF_dq_FD(h[2], o, x, q, spc); break;
+      case 4: pf.d2F_dq2_FD(h[2], o, x, q, spc); break;
+      default: pf.dF_dn(h[2], o, x, q, spc); break;
+    }
+    st = btam_compat::last_status();
+  }
+  fclose(f);
+  FILE *o = fopen(argv[3], "wb");
+  if (!o) return 2;
+  fwrite(out.data(), sizeof(double), out.size(), o);
+  fwrite(&st, sizeof(int), 1, o);
+  fclose(o);
+  btam_tables_destroy(T);
+  return 0;
+}
+
 int main(int argc, char **argv) {
+  if (argc == 5 && std::string(argv[4]) == "terms") return run_terms(argv);
   const bool pt = argc == 8 && std::string(argv[4]) == "pt";
   const bool pairs = argc == 6 && std::string(argv[4]) == "pairs";
   const bool perturb = argc == 9 && std::string(argv[4]) == "perturb";

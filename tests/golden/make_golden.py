@@ -17,6 +17,7 @@ Run from the repository root, with the reference tree present:
                                                     # reads the system fixtures)
     python tests/golden/make_golden.py --pairs    # pairs.npz only (it reads
                                                   # the system fixtures)
+    python tests/golden/make_golden.py --termfns  # termfns.npz only
 """
 import os
 import sys
@@ -326,8 +327,48 @@ def pairs_fixture(ref, orc):
     np.savez_compressed(os.path.join(OUT, "pairs.npz"), **out)
 
 
+# Slots of the per-term plugin table: (fn, directions) per number of sites;
+# fn 0 F, 1 dF_dq, 2 d2F_dq2, 3 dF_dq_FD, 4 d2F_dq2_FD, 5 dF_dn.
+TERM_FNS = {2: [(0, [0]), (1, [0, 1]), (2, [0, 1, 2, 3]), (3, [0, 1]), (4, [0, 1, 2, 3]),
+                (5, [0, 1])],
+            3: [(0, [0]), (1, [0, 1, 2]), (2, list(range(9))), (3, [0, 1, 2]),
+                (4, list(range(9))), (5, [0, 1, 2])]}
+
+
+def termfns_fixture(ref, per=12):
+    """Every slot of the reference's per-term plugin table (potential_function:
+    F, dF_dq, d2F_dq2, their finite-difference twins and dF_dn) of the four ADP
+    terms, each direction, at seeded geometries: sites 1.6-6.5 A from the
+    centre (some past the table end), species mixed, occupancies in [0.05, 1]."""
+    rng = np.random.default_rng(17)
+    rows = []
+    for term in range(4):
+        ns = 2 if term < 2 else 3
+        for fn, dirs in TERM_FNS[ns]:
+            for d in dirs:
+                for _ in range(per):
+                    q = np.zeros(9)
+                    q[:3] = rng.uniform(-1.0, 1.0, 3)
+                    for k in range(1, ns):
+                        v = rng.normal(size=3)
+                        q[3 * k:3 * k + 3] = q[:3] + v / np.linalg.norm(v) * rng.uniform(1.6, 6.5)
+                    x = rng.uniform(0.05, 1.0, 3)
+                    spc = rng.choice([12, 1], 3).astype(np.int32)
+                    out = ref.term_eval(term, fn, d, q[:3 * ns], x[:ns], spc[:ns])
+                    rows.append((term, fn, d, ns, q, x, spc, out))
+    np.savez_compressed(
+        os.path.join(OUT, "termfns.npz"),
+        meta=np.array([r_[:4] for r_ in rows], np.int32), q=np.array([r_[4] for r_ in rows]),
+        x=np.array([r_[5] for r_ in rows]), species=np.array([r_[6] for r_ in rows]),
+        out=np.array([r_[7] for r_ in rows]))
+    print(f"termfns: {len(rows)} evaluations")
+
+
 def main():
     ref = pyoracle.reference()
+    if ref is not None and sys.argv[1:] == ["--termfns"]:
+        termfns_fixture(ref)
+        return
     if ref is not None and sys.argv[1:] == ["--pairs"]:
         pairs_fixture(ref, pyoracle.Oracle())
         return
@@ -392,6 +433,7 @@ def main():
     point_fixture(ref)
     multipole_fixture()
     pairs_fixture(ref, orc)
+    termfns_fixture(ref)
 
 
 if __name__ == "__main__":

@@ -307,3 +307,26 @@ def test_pair_terms_against_golden(oracle, name):
         h = fn(full, rho[owner], offs, idx, uu, oo)
         ref_h = p[f"{name}_{key}"]
         assert np.max(np.abs(h - ref_h)) <= 1e-14 * max(1.0, np.abs(ref_h).max()), key
+
+
+def test_term_table_against_golden(oracle):
+    """The oracle's per-term functions reproduce the reference's per-term
+    table (F, dF_dq, dF_dq_FD with its stale-coordinate steps, d2F_dq2_FD,
+    dF_dn, and the diagonal d2F_dq2 blocks the oracle forms) at the
+    fixture's geometries.  Values, gradients and occupancy derivatives are
+    bit-exact; the analytic blocks are derived in another order (1e-13)."""
+    d = load("termfns")
+    n_checked = 0
+    for r in range(len(d["meta"])):
+        term, fn, direction, ns = (int(v) for v in d["meta"][r])
+        if fn == 2 and direction % (ns + 1):
+            continue  # off-diagonal blocks: not formed by the oracle
+        out = oracle.term_eval(term, fn, direction, d["q"][r][:3 * ns], d["x"][r][:ns],
+                               d["species"][r][:ns])
+        gold = d["out"][r]
+        if fn == 2:
+            assert np.abs(out - gold).max() <= 1e-13 * max(1.0, np.abs(gold).max()), r
+        else:
+            assert np.array_equal(out, gold), (r, term, fn, direction)
+        n_checked += 1
+    assert n_checked == 840
