@@ -144,8 +144,8 @@ template <class R> BTAM_HD const R *uw_rec(const RadialView<R> &T, int pk, int m
   return T.uw + (size_t)kUWStride * ((size_t)T.n * pk + m);
 }
 // The same tables with the uw block staged in shared memory by the kernel
-// (FP32 only: 3 pair kinds x n segments x 32 bytes = 115 KB at n = 1194);
-// the pr block stays in global memory.
+// (3 pair kinds x n segments x 32 bytes = 115 KB at n = 1194 in FP32,
+// x 64 bytes = 229 KB in FP64); the pr block stays in global memory.
 template <class R> struct RadialViewS : RadialView<R> {};
 template <class R> BTAM_HD const R *pr_rec(const RadialView<R> &T, int pk, int m) {
   return T.pr + (size_t)8 * T.n * pk + (size_t)pr_stride(pk) * m;
@@ -240,6 +240,30 @@ BTAM_HD void lds8(const float *p, bool swap, float (&v)[8]) {
 }
 // Whether record r (= n pk + m) of a staged uw block has its halves swapped.
 BTAM_HD bool uw_swapped(int r) { return ((r >> 2) & 1) != 0; }
+// FP64: the 16-byte quarter k of record r sits at quarter k ^ uw_xor64(r)
+// of the record in a staged uw block.  A record is 64 bytes, so its
+// quarters start on bank groups 16 (r & 1) + 4 k'; with the XOR over bits
+// 1-2 of r the same quarter of records r mod 8 = 0..7 falls on eight
+// different 4-bank groups, and the 128-bit shared loads of random records
+// spread over all 32 banks.
+BTAM_HD int uw_xor64(int r) { return (r >> 1) & 3; }
+// 8 doubles of a 64-byte record in shared memory, quarters placed by x =
+// uw_xor64(r) (four 128-bit shared loads; host: plain copy).
+BTAM_HD void lds8(const double *p, int x, double (&v)[8]) {
+#if defined(__CUDA_ARCH__)
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    asm volatile("ld.shared.v2.f64 {%0,%1}, [%2];"
+                 : "=d"(v[2 * k]), "=d"(v[2 * k + 1])
+                 : "r"(a + 16u * (unsigned)(k ^ x)));
+#else
+  for (int k = 0; k < 4; ++k) {
+    v[2 * k] = p[2 * (k ^ x)];
+    v[2 * k + 1] = p[2 * (k ^ x) + 1];
+  }
+#endif
+}
 
 template <class R> struct V3 {
   R x, y, z;
@@ -340,6 +364,9 @@ template <class R> BTAM_HD void ld_uw(const RadialView<R> &T, int pk, int m, R (
 }
 BTAM_HD void ld_uw(const RadialViewS<float> &T, int pk, int m, float (&k)[8]) {
   lds8(uw_rec<float>(T, pk, m), uw_swapped(T.n * pk + m), k);
+}
+BTAM_HD void ld_uw(const RadialViewS<double> &T, int pk, int m, double (&k)[8]) {
+  lds8(uw_rec<double>(T, pk, m), uw_xor64(T.n * pk + m), k);
 }
 
 // u, w of pair kind pk at one geometry (values and, when D, derivatives);

@@ -173,7 +173,12 @@ template <> __device__ __forceinline__ void st_rec4<double>(double *p, const dou
 // memory.
 template <class R, bool SM> struct KView { using type = RadialView<R>; };
 template <> struct KView<float, true> { using type = RadialViewS<float>; };
-constexpr int kUWSharedMax = 3 * kUWStride * 1200;  // floats: up to 1200 segments
+template <> struct KView<double, true> { using type = RadialViewS<double>; };
+constexpr int kUWSharedMax = 3 * kUWStride * 1200;  // values: up to 1200 segments
+// Dynamic shared memory of a staging kernel: the table and its mbarrier.
+template <class R> constexpr size_t uw_shared_bytes(int n) {
+  return (size_t)3 * kUWStride * (size_t)n * sizeof(R) + 16;
+}
 // Bounded wait on phase 0 of a shared-memory mbarrier (true: completed).
 __device__ __forceinline__ bool mbar_wait0(unsigned bar) {
   for (int it = 0; it < (1 << 22); ++it) {
@@ -198,18 +203,19 @@ template <class R, bool SM>
 __device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArgs<R> &a,
                                                                    bool &ok) {
   ok = true;
-  if constexpr (SM && sizeof(R) == 4) {
+  if constexpr (SM) {
     // dynamic shared memory: the table (a multiple of 32 bytes), then an
     // 8-byte mbarrier; the kernels that stage it hold no static shared memory
-    extern __shared__ __align__(128) float uw_dyn[];
-    const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 floats
+    extern __shared__ __align__(128) unsigned char uw_raw[];
+    R *uw_dyn = reinterpret_cast<R *>(uw_raw);
+    const int nuw = 3 * kUWStride * a.T.n;  // a multiple of 8 values
     bool staged = false;
     if (a.T.uws) {
       // one bulk copy of the pre-laid-out table (the tile is regular: one
       // contiguous, 16-byte aligned block), completion on the mbarrier
       const unsigned dst = (unsigned)__cvta_generic_to_shared(uw_dyn);
-      const unsigned bar = dst + 4u * (unsigned)nuw;
-      const unsigned bytes = 4u * (unsigned)nuw;
+      const unsigned bytes = (unsigned)sizeof(R) * (unsigned)nuw;
+      const unsigned bar = dst + bytes;
       if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -238,15 +244,19 @@ __device__ __forceinline__ typename KView<R, SM>::type kernel_view(const EvalArg
       }
     }
     if (!staged && ok) {
-      // 16-byte halves c of record c / 2, stored swapped where uw_swapped says
-      for (int c = threadIdx.x; c < nuw / 4; c += blockDim.x) {
-        const int dst = uw_swapped(c >> 1) ? (c ^ 1) : c;
+      // 16-byte pieces c of the table, placed as ld_uw reads them: FP32
+      // halves c of record c / 2, swapped where uw_swapped says; FP64
+      // quarters c of record c / 4, permuted by uw_xor64
+      const int npieces = nuw * (int)sizeof(R) / 16;
+      for (int c = threadIdx.x; c < npieces; c += blockDim.x) {
+        const int dst = sizeof(R) == 4 ? (uw_swapped(c >> 1) ? (c ^ 1) : c)
+                                       : ((c & ~3) | ((c & 3) ^ uw_xor64(c >> 2)));
         reinterpret_cast<float4 *>(uw_dyn)[dst] =
             __ldg(reinterpret_cast<const float4 *>(a.T.uw) + c);
       }
       __syncthreads();
     }
-    RadialViewS<float> T;
+    RadialViewS<R> T;
     T.uw = uw_dyn;
     T.pr = a.T.pr;
     T.dx = a.T.dx;
@@ -752,14 +762,15 @@ pass2u_pair_kernel(const EvalArgs<R> a) {
     pass2u_one(a, a.T, t);
 }
 
-// The same with the uw block of the tables staged in shared memory (FP32,
-// 115 KB, one block of TPB threads per SM): the 13 triplet geometries of a
-// pair then gather their spline records from shared memory instead of L1.
-template <int TPB>
+// The same with the uw block of the tables staged in shared memory (115 KB
+// in FP32, 229 KB in FP64; one block of TPB threads per SM): the triplet
+// geometries of a pair then gather their spline records from shared memory
+// instead of L1.
+template <class R, int TPB>
 __global__ void __launch_bounds__(TPB, 1)
-pass2u_pair_smem_kernel(const EvalArgs<float> a) {
+pass2u_pair_smem_kernel(const EvalArgs<R> a) {
   bool ok;
-  const auto T = kernel_view<float, true>(a, ok);
+  const auto T = kernel_view<R, true>(a, ok);
   if (!ok) return;  // the staging copy timed out (flagged)
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
@@ -920,8 +931,7 @@ void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers, bool und, cudaEvent_t
 // memory (the uw tables): as many blocks as fit on the device at once, at
 // most `full`.
 template <class K> int smem_grid(K kernel, int threads, size_t smem, int full) {
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(sizeof(float) * kUWSharedMax + 16));
+  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, sms = 0, per = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -972,26 +982,23 @@ void go2u(const EvalArgs<R> &a, cudaStream_t st, bool pers, cudaEvent_t mid) {
   ks<<<grid_of(ks, a.n_real, 4, pers), 128, 0, st>>>(a);
 }
 
-// Shared-memory variant of the undirected pass-2 pair kernel: FP32 tables
-// of up to 1200 segments, one block of 512 threads per SM (always a
-// persistent grid); otherwise (FP64, larger tables) the default shape.
-inline void go2u_smem(const EvalArgs<float> &a, cudaStream_t st, cudaEvent_t mid) {
-  constexpr int TPB = 512;
+// Shared-memory variant of the undirected pass-2 pair kernel: tables of up
+// to 1200 segments (115 KB in FP32, 230 KB in FP64, within the 227 KB a
+// block may hold), one block of TPB threads per SM (always a persistent
+// grid); larger tables take the default shape.
+template <class R, int TPB>
+void go2u_smem(const EvalArgs<R> &a, cudaStream_t st, cudaEvent_t mid) {
   if (a.T.n > kUWSharedMax / (3 * kUWStride)) {
-    go2u<float, 128, 1>(a, st, false, mid);
+    go2u<R, 128, 1>(a, st, false, mid);
     return;
   }
-  // the table and its 8-byte mbarrier (kernel_view)
-  const size_t bytes = (size_t)3 * kUWStride * a.T.n * sizeof(float) + 16;
-  auto k = pass2u_pair_smem_kernel<TPB>;
+  const size_t bytes = uw_shared_bytes<R>(a.T.n);
+  auto k = pass2u_pair_smem_kernel<R, TPB>;
   const int g = smem_grid(k, TPB, bytes, nblocks(a.n_own, TPB));
   if (g > 0) k<<<g, TPB, bytes, st>>>(a);
   if (mid) cudaEventRecord(mid, st);
-  auto ks = pass2u_site_kernel<float, 4>;
+  auto ks = pass2u_site_kernel<R, 4>;
   ks<<<grid_of(ks, a.n_real, 4, true), 128, 0, st>>>(a);
-}
-inline void go2u_smem(const EvalArgs<double> &a, cudaStream_t st, cudaEvent_t mid) {
-  go2u<double, 128, 1>(a, st, false, mid);
 }
 
 template <class R>
@@ -1003,7 +1010,8 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent
     case 1: go2u<R, 128, 5>(a, st, pers, mid); break;
     case 2: go2u<R, 128, 4>(a, st, pers, mid); break;
     case 3: go2u<R, 256, 2>(a, st, pers, mid); break;
-    case 4: go2u_smem(a, st, mid); break;
+    case 4: go2u_smem<R, 512>(a, st, mid); break;
+    case 5: go2u_smem<R, 384>(a, st, mid); break;
     default: go2u<R, 128, 1>(a, st, pers, mid); break;
     }
     return cudaGetLastError();

@@ -78,7 +78,10 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0,
 // (4,-,32), (4,5,8), (4,4,16), (8,2,16), (4,5,16)
 constexpr int kPass1Variants = 5;
 constexpr int kPass2Variants = 6;  // shapes (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
-constexpr int kPass2UVariants = 5;  // undirected pair kernel (threads, min blocks): (128,-), (128,5), (128,4), (256,2), (512,1) with the uw tables in shared memory (FP32; always persistent)
+// undirected pair kernel (threads, min blocks): (128,-), (128,5), (128,4),
+// (256,2), then one block of 512 or 384 threads per SM with the uw tables in
+// shared memory (always persistent)
+constexpr int kPass2UVariants = 6;
 constexpr int kPersistent = 8;
 constexpr int kUndirected = 16;
 inline bool valid_variants(int v1, int v2) {

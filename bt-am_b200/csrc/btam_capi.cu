@@ -470,6 +470,26 @@ int btam_tables_load(const char *dir, btam_tables **out) {
     }
     t->r32.uws = t->uws32;
   }
+  {  // the FP64 uw block with its 16-byte quarters placed as the
+     // shared-memory kernels read them (uw_xor64)
+    const size_t nrec = (size_t)3 * rn;
+    std::vector<double> sw(nrec * kUWStride);
+    const double *src = r64.data() + uw64[0];
+    for (size_t r = 0; r < nrec; ++r)
+      for (int k = 0; k < 4; ++k) {
+        const int pk = k ^ uw_xor64((int)r);
+        sw[kUWStride * r + 2 * pk] = src[kUWStride * r + 2 * k];
+        sw[kUWStride * r + 2 * pk + 1] = src[kUWStride * r + 2 * k + 1];
+      }
+    e = cudaMalloc(&t->uws64, sw.size() * sizeof(double));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(t->uws64, sw.data(), sw.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      btam_tables_destroy(t);
+      return cuda_status(e);
+    }
+    t->r64.uws = t->uws64;
+  }
   *out = t;
   return BTAM_OK;
 }
@@ -481,6 +501,7 @@ void btam_tables_destroy(btam_tables *t) {
   if (t->rad64) cudaFree(t->rad64);
   if (t->rad32) cudaFree(t->rad32);
   if (t->uws32) cudaFree(t->uws32);
+  if (t->uws64) cudaFree(t->uws64);
   delete t;
 }
 

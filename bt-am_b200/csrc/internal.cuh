@@ -28,6 +28,7 @@ struct btam_tables {
   double *rad64 = nullptr;
   float *rad32 = nullptr;
   float *uws32 = nullptr;  // the FP32 uw block in its shared-memory layout
+  double *uws64 = nullptr;  // the FP64 uw block in its shared-memory layout
   RadialView<double> r64;
   RadialView<float> r32;
 };
