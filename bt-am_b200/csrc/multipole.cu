@@ -663,7 +663,7 @@ __device__ void tri_dmq(const RadialView<double> &T, const PairSite &c, const Pa
 struct PairOut {
   double drho_q[3], pair_q[3], drho_s, pair_s, drho_x, pair_x;
 };
-__device__ void pair_residual(const RadialView<double> &T, int rule, const PairSite &c,
+__device__ __noinline__ void pair_residual(const RadialView<double> &T, int rule, const PairSite &c,
                               const PairSite &nb, int dir, PairOut &o) {
   const int pk = pair_kind(c.code, nb.code);
   const double q[6] = {c.q[0], c.q[1], c.q[2], nb.q[0], nb.q[1], nb.q[2]};
@@ -709,83 +709,344 @@ __device__ void pair_residual(const RadialView<double> &T, int rule, const PairS
     }
 }
 
-// One triplet measure (c; j1, j2) for u in slot `dir` (1 or 2 may both
-// hold u when j1 = j2): dmq, dsq of the dipole and quadrupole terms
-// (with_q: j2 passes the gradient's x > min_occupancy test) and their
-// degree-3 dxi (with_x: j2 passes x >= min_occupancy).
-struct TriOut {
-  double dip_q[3], quad_q[3], dip_s, quad_s, dip_x, quad_x;
+// ---- triplets: every slot direction from one set of leg evaluations ------
+// One leg (i, j_k) of a triplet geometry: r = q_i - q_jk, |r|^2, |r|, 1/|r|
+// and the raw spline values (D: and first derivatives) of u and w at |r|,
+// each formed in the operations of tri_F, tri_dq and tri_dn, so a term
+// assembled from legs equals theirs bit for bit.  A finite-difference or
+// rule point that moves one slot recomputes only the legs that slot ends.
+struct Leg {
+  double r[3], rsq, nr, inv, u, du, w, dw;
 };
-__device__ void tri_residual(const RadialView<double> &T, int rule, const PairSite &c,
-                             const PairSite &j1, const PairSite &j2, bool coincident, int dir,
-                             bool with_q, bool with_x, TriOut &o) {
+template <bool D>
+__device__ __forceinline__ void leg_of(const RadialView<double> &T, int pk, const double *qi,
+                                       const double *qj, Leg &L) {
+  L.rsq = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    L.r[a] = qi[a] - qj[a];
+    L.rsq += sqz(L.r[a]);
+  }
+  L.nr = sqrt(L.rsq);
+  double p;
+  const int m = seg_ref(L.nr, T.dx, T.n, p);
+  double k[8];
+  ld8(uw_rec(T, pk, m), k);
+  L.u = cubv(k, p);
+  L.w = cubv(k + 4, p);
+  if (D) {
+    L.inv = 1.0 / L.nr;
+    L.du = cubd(k, p);
+    L.dw = cubd(k + 4, p);
+  }
+}
+// A leg parked in shared memory (10 doubles) while other work holds the
+// registers.
+__device__ __forceinline__ void st_leg(double *p, const Leg &L) {
+  p[0] = L.r[0]; p[1] = L.r[1]; p[2] = L.r[2]; p[3] = L.rsq; p[4] = L.nr;
+  p[5] = L.inv; p[6] = L.u; p[7] = L.du; p[8] = L.w; p[9] = L.dw;
+}
+__device__ __forceinline__ Leg ld_leg(const double *p) {
+  Leg L;
+  L.r[0] = p[0]; L.r[1] = p[1]; L.r[2] = p[2]; L.rsq = p[3]; L.nr = p[4];
+  L.inv = p[5]; L.u = p[6]; L.du = p[7]; L.w = p[8]; L.dw = p[9];
+  return L;
+}
+__device__ __forceinline__ double leg_dot(const Leg &L1, const Leg &L2) {
+  double dot = 0.0;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) dot += L1.r[a] * L2.r[a];
+  return dot;
+}
+// tri_dq of all three slots, component e = 6 dir + a (dipole) or
+// 6 dir + 3 + a (quadrupole), each handed to sink(e, value) as it is formed.
+template <class Sink>
+__device__ __forceinline__ void dq_all(const Leg &L1, const Leg &L2, double c1, double c2,
+                                       Sink &&sink) {
+  const double dot = leg_dot(L1, L2);
+  const double i1 = L1.inv, i2 = L2.inv, n1 = L1.nr, n2 = L2.nr;
+  const double r1sq = L1.rsq, r2sq = L2.rsq;
+  const double u1 = c1 * L1.u, u2 = c2 * L2.u;
+  const double du1 = c1 * L1.du, du2 = c2 * L2.du;
+  const double w1 = c1 * L1.w, w2 = c2 * L2.w;
+  const double dw1 = c1 * L1.dw, dw2 = c2 * L2.dw;
+  const double dd = sqz(dot);
+  const double *r1 = L1.r, *r2 = L2.r;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    sink(a, 0.5 * (du1 * u2 * dot * i1 * r1[a] + u1 * du2 * dot * i2 * r2[a] +
+                   u1 * u2 * (r1[a] + r2[a])));
+    sink(3 + a, (1.0 / 2.0) * (dw1 * w2 * dd * i1 * r1[a] + w1 * dw2 * dd * i2 * r2[a] +
+                               w1 * w2 * 2 * dot * (r1[a] + r2[a])) -
+                    (1.0 / 6.0) * (dw1 * w2 * n1 * r2sq * r1[a] + w1 * dw2 * r1sq * n2 * r2[a] +
+                                   w1 * w2 * 2 * r2sq * r1[a] + w1 * w2 * 2 * r1sq * r2[a]));
+    sink(6 + a, -0.5 * (du1 * u2 * dot * i1 * r1[a] + u1 * u2 * r2[a]));
+    sink(9 + a, -0.5 * (dw1 * w2 * dd * i1 * r1[a] + w1 * w2 * 2 * dot * r2[a]) +
+                    (1.0 / 6.0) * (dw1 * w2 * n1 * r2sq * r1[a] + w1 * w2 * 2 * r2sq * r1[a]));
+    sink(12 + a, -0.5 * (u1 * du2 * dot * i2 * r2[a] + u1 * u2 * r1[a]));
+    sink(15 + a, -0.5 * (w1 * dw2 * dd * i2 * r2[a] + w1 * w2 * 2 * dot * r1[a]) +
+                     (1.0 / 6.0) * (w1 * dw2 * r1sq * n2 * r2[a] + w1 * w2 * 2 * r1sq * r2[a]));
+  }
+}
+// tri_F from legs.
+__device__ __forceinline__ void f_legs(const Leg &L1, const Leg &L2, double c1, double c2,
+                                       double &fd, double &fq) {
+  const double dot = leg_dot(L1, L2);
+  const double u1 = c1 * L1.u, u2 = c2 * L2.u;
+  const double w1 = c1 * L1.w, w2 = c2 * L2.w;
+  fd = (1.0 / 2.0) * u1 * u2 * dot;
+  fq = (1.0 / 2.0) * w1 * w2 * sqz(dot) - (1.0 / 6.0) * w1 * w2 * L1.rsq * L2.rsq;
+}
+// tri_dn of all three slots: v[2 dir] dipole, v[2 dir + 1] quadrupole.
+__device__ __forceinline__ void dn_all(const Leg &L1, const Leg &L2, const double *n,
+                                       double (&v)[6]) {
+  const double dot = leg_dot(L1, L2);
+  const double r1sq = L1.rsq, r2sq = L2.rsq;
+  const double s1 = L1.u, s2 = L2.u, t1 = L1.w, t2 = L2.w;
+  {
+    const double u1 = n[0] * n[1] * s1, u2 = n[0] * n[2] * s2;
+    const double d1 = n[1] * s1, d2 = n[2] * s2;
+    v[0] = (1.0 / 2.0) * d1 * u2 * dot + (1.0 / 2.0) * u1 * d2 * dot;
+    const double w1 = n[0] * n[1] * t1, w2 = n[0] * n[2] * t2;
+    const double e1 = n[1] * t1, e2 = n[2] * t2, dd = sqz(dot);
+    v[1] = (1.0 / 2.0) * e1 * w2 * dd + (1.0 / 2.0) * w1 * e2 * dd -
+           (1.0 / 6.0) * e1 * w2 * r1sq * r2sq - (1.0 / 6.0) * w1 * e2 * r1sq * r2sq;
+  }
+  {
+    v[2] = (1.0 / 2.0) * (n[0] * s1) * (n[0] * n[2] * s2) * dot;
+    const double e1 = n[0] * t1, w2 = n[0] * n[2] * t2;
+    v[3] = (1.0 / 2.0) * e1 * w2 * sqz(dot) - (1.0 / 6.0) * e1 * w2 * r1sq * r2sq;
+  }
+  {
+    v[4] = (1.0 / 2.0) * (n[0] * n[1] * s1) * (n[0] * s2) * dot;
+    const double w1 = n[0] * n[1] * t1, e2 = n[0] * t2;
+    v[5] = (1.0 / 2.0) * w1 * e2 * sqz(dot) - (1.0 / 6.0) * w1 * e2 * r1sq * r2sq;
+  }
+}
+
+// dmq of slot S's three coordinates: for each, the five-point second
+// difference (step 0.01) of all slots' gradients, times sigma_S^2 / 2, added
+// to acc (g0: the gradients at the mean).  g0 and acc are the lane's
+// shared-memory scratch.
+template <int S>
+__device__ __forceinline__ void dmq_slot(const RadialView<double> &T, int pk1, int pk2,
+                                         const double (&q)[9], const double *legs,
+                                         double c1, double c2, double c2s, const double *g0,
+                                         double *acc) {
+#pragma unroll 1
+  for (int al = 0; al < 3; ++al) {
+    const double dr = 0.01;
+    const double x0 = al == 0 ? q[3 * S] : al == 1 ? q[3 * S + 1] : q[3 * S + 2];
+    double t[18];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const double v = w == 0 ? x0 + dr * 2 : w == 1 ? x0 + dr : w == 2 ? x0 - dr : x0 - dr * 2;
+      double pm[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) pm[a] = a == al ? v : q[3 * S + a];
+      // the five-point combination -gpp + 16 gp - 30 g0 + 16 gm - gmm,
+      // formed in that order as the points arrive (pp, p, m, mm)
+      auto step = [&](int e, double g) {
+        if (w == 0) t[e] = -g;
+        else if (w == 1) t[e] = (t[e] + 16.0 * g) - 30.0 * g0[e];
+        else if (w == 2) t[e] = t[e] + 16.0 * g;
+        else t[e] = t[e] - g;
+      };
+      if (S == 0) {
+        Leg M1, M2;
+        leg_of<true>(T, pk1, pm, q + 3, M1);
+        leg_of<true>(T, pk2, pm, q + 6, M2);
+        dq_all(M1, M2, c1, c2, step);
+      } else if (S == 1) {
+        Leg M1;
+        leg_of<true>(T, pk1, q, pm, M1);
+        dq_all(M1, ld_leg(legs + 10), c1, c2, step);
+      } else {
+        Leg M2;
+        leg_of<true>(T, pk2, q, pm, M2);
+        dq_all(ld_leg(legs), M2, c1, c2, step);
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < 18; ++e) acc[e] += c2s * (t[e] / (12.0 * dr * dr));
+  }
+}
+
+// Second differences (step 1e-4) of the dipole and quadrupole values along
+// slot S's three coordinates (the reference's d2F_dq2_FD diagonal).
+template <int S>
+__device__ __forceinline__ void fd_slot(const RadialView<double> &T, int pk1, int pk2,
+                                        const double (&q)[9], const double *legs,
+                                        double c1, double c2, double f0d, double f0q,
+                                        double *dd, double *dq) {
+#pragma unroll 1
+  for (int al = 0; al < 3; ++al) {
+    const double dr = 0.0001;
+    const double x0 = al == 0 ? q[3 * S] : al == 1 ? q[3 * S + 1] : q[3 * S + 2];
+    double fd4[4], fq4[4];
+#pragma unroll 1
+    for (int w = 0; w < 4; ++w) {
+      const double D = 1.0;
+      const double v = w == 0 ? x0 + D * dr * 2 : w == 1 ? x0 + D * dr
+                     : w == 2 ? x0 - D * dr : x0 - D * dr * 2;
+      double pm[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) pm[a] = a == al ? v : q[3 * S + a];
+      double fd, fq;
+      if (S == 0) {
+        Leg M1, M2;
+        leg_of<false>(T, pk1, pm, q + 3, M1);
+        leg_of<false>(T, pk2, pm, q + 6, M2);
+        f_legs(M1, M2, c1, c2, fd, fq);
+      } else if (S == 1) {
+        Leg M1;
+        leg_of<false>(T, pk1, q, pm, M1);
+        f_legs(M1, ld_leg(legs + 10), c1, c2, fd, fq);
+      } else {
+        Leg M2;
+        leg_of<false>(T, pk2, q, pm, M2);
+        f_legs(ld_leg(legs), M2, c1, c2, fd, fq);
+      }
+      if (w == 0) { fd4[0] = fd; fq4[0] = fq; }
+      else if (w == 1) { fd4[1] = fd; fq4[1] = fq; }
+      else if (w == 2) { fd4[2] = fd; fq4[2] = fq; }
+      else { fd4[3] = fd; fq4[3] = fq; }
+    }
+    const double vd = d2_5(fd4[0], fd4[1], f0d, fd4[2], fd4[3]);
+    const double vq = d2_5(fq4[0], fq4[1], f0q, fq4[2], fq4[3]);
+    if (al == 0) { dd[0] = vd; dq[0] = vq; }
+    else if (al == 1) { dd[1] = vd; dq[1] = vq; }
+    else { dd[2] = vd; dq[2] = vq; }
+  }
+}
+
+// One triplet measure (c; j1, j2) for u in each slot (dir 0: c, 1: j1,
+// 2: j2; with j1 = j2 the coincident measure), evaluate_DV0_i_Dq_u_MgHx's
+// meanfield_integral_mp_dmq and _dsq of the dipole and quadrupole terms
+// (with_q: j2 passes the gradient's x > min_occupancy test) and
+// evaluate_DV0_i_Dxi_u_adp_MgHx's degree-3 dxi (j2 passes x >=
+// min_occupancy, as every triplet here does).  Each slot's values are the
+// reference's, term for term: the same points, the same differences, the
+// same per-slot sums; only the geometry is shared between the slots.
+// out[5 dir + 0..2] = dmq dipole + quadrupole, [3] dsq, [4] dxi, times f
+// (the lane's shared-memory stage); sc: 56 doubles of its scratch.
+__device__ __forceinline__ void tri_all(const RadialView<double> &T, int rule, const PairSite &c,
+                                        const PairSite &j1, const PairSite &j2,
+                                        bool coincident, bool with_q, double f, double *sc,
+                                        double *out) {
   const int pk1 = pair_kind(c.code, j1.code), pk2 = pair_kind(c.code, j2.code);
   const double n[3] = {c.x, j1.x, j2.x};
+  const double c1 = n[0] * n[1], c2 = n[0] * n[2];
   const double q[9] = {c.q[0],  c.q[1],  c.q[2],  j1.q[0], j1.q[1],
                        j1.q[2], j2.q[0], j2.q[1], j2.q[2]};
   const double sig[3] = {c.sig, j1.sig, j2.sig};
-  for (int a = 0; a < 3; ++a) o.dip_q[a] = o.quad_q[a] = 0.0;
-  o.dip_s = o.quad_s = o.dip_x = o.quad_x = 0.0;
+  // the legs at the mean, parked in the scratch (sc[36..55])
+  double *legs = sc + 36;
+  {
+    Leg L1, L2;
+    leg_of<true>(T, pk1, q, q + 3, L1);
+    leg_of<true>(T, pk2, q, q + 6, L2);
+    st_leg(legs, L1);
+    st_leg(legs + 10, L2);
+  }
+#pragma unroll
+  for (int e = 0; e < 15; ++e) out[e] = 0.0;
   if (with_q) {
-    tri_dmq(T, c, j1, j2, dir, o.dip_q, o.quad_q);
-    // dsq: sigma_dir x sum over the dof row of dir of the block traces
+    // dmq: the gradients at the mean plus sigma_s^2 / 2 times their
+    // second differences along every coordinate of every slot
+    double *g0 = sc, *acc = sc + 18;
+    dq_all(ld_leg(legs), ld_leg(legs + 10), c1, c2,
+           [&](int e, double g) { g0[e] = acc[e] = g; });
+    dmq_slot<0>(T, pk1, pk2, q, legs, c1, c2, sqz(sig[0]) / 2.0, g0, acc);
+    dmq_slot<1>(T, pk1, pk2, q, legs, c1, c2, sqz(sig[1]) / 2.0, g0, acc);
+    dmq_slot<2>(T, pk1, pk2, q, legs, c1, c2, sqz(sig[2]) / 2.0, g0, acc);
+#pragma unroll
+    for (int d = 0; d < 3; ++d)
+#pragma unroll
+      for (int a = 0; a < 3; ++a) out[5 * d + a] = f * acc[6 * d + a] + f * acc[6 * d + 3 + a];
+    // dsq: sigma_dir x the block traces of the dof row of dir
+    double sd_[3] = {0, 0, 0}, sq_[3] = {0, 0, 0};
     if (rule == 1) {
       double f0d, f0q;
-      tri_F_call(T, pk1, pk2, n, q, f0d, f0q);
-      for (int b = 0; b < 3; ++b) {
-        if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
-        const int dirn = dir * 3 + b, slot = dirn / 4;
-        const bool diag = dirn == 0 || dirn == 4 || dirn == 8;
-        for (int al = 0; al < 3; ++al) {
-          double sd[4], sq4[4];
-          for (int w = 0; w < 4; ++w) {
-            double qq[9];
-            shifted(q, 3 * slot + al, w, qq);
-            tri_F_call(T, pk1, pk2, n, qq, sd[w], sq4[w]);
+      f_legs(ld_leg(legs), ld_leg(legs + 10), c1, c2, f0d, f0q);
+      // the second differences in the scratch: Dd[slot][al] at sc[3 slot +
+      // al], Dq at sc[9 + 3 slot + al]
+      double *Dd = sc, *Dq = sc + 9;
+      fd_slot<0>(T, pk1, pk2, q, legs, c1, c2, f0d, f0q, Dd, Dq);
+      fd_slot<1>(T, pk1, pk2, q, legs, c1, c2, f0d, f0q, Dd + 3, Dq + 3);
+      fd_slot<2>(T, pk1, pk2, q, legs, c1, c2, f0d, f0q, Dd + 6, Dq + 6);
+      // rows of the dof table in the reference's (dir, b) order; direction
+      // dir * 3 + b reads slot (dir * 3 + b) / 4
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
+          const int dirn = dir * 3 + b, slot = dirn / 4;
+          const bool diag = dirn == 0 || dirn == 4 || dirn == 8;
+#pragma unroll
+          for (int al = 0; al < 3; ++al) {
+            sd_[dir] += sig[dir] * Dd[3 * slot + al];
+            if (diag) sq_[dir] += sig[dir] * Dq[3 * slot + al];
           }
-          o.dip_s += sig[dir] * d2_5(sd[0], sd[1], f0d, sd[2], sd[3]);
-          if (diag) o.quad_s += sig[dir] * d2_5(sq4[0], sq4[1], f0q, sq4[2], sq4[3]);
         }
-      }
     } else {
       const TriTr t = tri_traces_call(T, pk1, pk2, n, q);
-      for (int b = 0; b < 3; ++b) {
-        if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
-        double trd, trq;
-        if (b != dir) {
-          trd = t.d12;
-          trq = t.q12;
-        } else if (dir == 0) {
-          trd = t.d11 + t.d22 + 2.0 * t.d12;
-          trq = t.q11 + t.q22 + 2.0 * t.q12;
-        } else {
-          trd = dir == 1 ? t.d11 : t.d22;
-          trq = dir == 1 ? t.q11 : t.q22;
+#pragma unroll
+      for (int dir = 0; dir < 3; ++dir)
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+          if (!(b == dir || (coincident && dir > 0 && b > 0))) continue;
+          double trd, trq;
+          if (b != dir) {
+            trd = t.d12;
+            trq = t.q12;
+          } else if (dir == 0) {
+            trd = t.d11 + t.d22 + 2.0 * t.d12;
+            trq = t.q11 + t.q22 + 2.0 * t.q12;
+          } else {
+            trd = dir == 1 ? t.d11 : t.d22;
+            trq = dir == 1 ? t.q11 : t.q22;
+          }
+          sd_[dir] += sig[dir] * trd;
+          sq_[dir] += sig[dir] * trq;
         }
-        o.dip_s += sig[dir] * trd;
-        o.quad_s += sig[dir] * trq;
-      }
     }
+#pragma unroll
+    for (int d = 0; d < 3; ++d) out[5 * d + 3] = f * sd_[d] + f * sq_[d];
   }
-  if (with_x) {
-    const Gh3 g = gh3_of(3, coincident);
-    const double W = 1.0 / (2.0 * g.D);
-    for (int sg = 0; sg < 2; ++sg)
-      for (int l = 0; l < g.D; ++l) {
-        double ql[9], vd, vq;
-        gh3_point(g, q, sig, l, sg == 0 ? 1.0 : -1.0, ql);
-        tri_dn(T, pk1, pk2, n, dir, ql, vd, vq);
-        o.dip_x += vd * W;
-        o.quad_x += vq * W;
-      }
-  }
+  // dxi on the degree-3 rule: the rows of a group move the group's slots
+  const Gh3 g = gh3_of(3, coincident);
+  const double W = 1.0 / (2.0 * g.D);
+  double vx[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll 1
+  for (int sg = 0; sg < 2; ++sg)
+#pragma unroll 1
+    for (int l = 0; l < g.D; ++l) {
+      double ql[9];
+      gh3_point(g, q, sig, l, sg == 0 ? 1.0 : -1.0, ql);
+      const int grp = l / 3;
+      Leg M1, M2;
+      if (grp == 0 || grp == g.grp[1]) leg_of<false>(T, pk1, ql, ql + 3, M1);
+      else M1 = ld_leg(legs);
+      if (grp == 0 || grp == g.grp[2]) leg_of<false>(T, pk2, ql, ql + 6, M2);
+      else M2 = ld_leg(legs + 10);
+      double v[6];
+      dn_all(M1, M2, n, v);
+#pragma unroll
+      for (int e = 0; e < 6; ++e) vx[e] += v[e] * W;
+    }
+#pragma unroll
+  for (int d = 0; d < 3; ++d) out[5 * d + 4] = f * vx[2 * d] + f * vx[2 * d + 1];
 }
 
 struct MpResArgs {
   MpArgs b;
   const int *owner;
+  const int *rev;      // reverse slot of every real list entry (-1: none)
   const double *gamma;
-  double *g5;  // 5 values (dV0/dq 3, dV0/dsigma, dV0/dx) per (u, centre)
+  double *gk;  // 5 values per (centre o, slot): slot 0 the pair (o, o), 1 + k list entry k
+  double *g5;  // the same per (u, centre): centre 0 u itself, 1 + k u's list entry k
   double *Rq, *Rs, *Rx;
 };
 
@@ -794,156 +1055,136 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// One warp per (u, centre i in {u} U N(u)): evaluate_DV0_i_Dq_u_MgHx and
-// evaluate_DV0_i_Dxi_u_adp_MgHx for i = the centre's owner o and u as seen
-// from o's frame, each term of the reference's loops over o's list that
-// holds u.
-__global__ void __launch_bounds__(128) mp_pairs_kernel(MpResArgs r, long long total) {
+// One warp per centre o: every term of evaluate_DV0_i_Dq_u_MgHx and
+// evaluate_DV0_i_Dxi_u_adp_MgHx (i = o) for u = o and for u = each entry of
+// o's list, the pairs (o, j) and the triplets (o; j1 <= j2) of o's active
+// entries (x >= min_occupancy; an empty site takes part in nothing), one
+// pair or triplet per lane.  A triplet gives its slots' values to u = o
+// (slot 0), u = j1 (slot 1) and u = j2 (slot 2) at once.  The per-(o, u)
+// totals gather in shared memory in a fixed order (the lanes stage their
+// values, then one lane per value adds them in lane order), so every
+// evaluation gives the same bits.
+constexpr int kMpW = 1;              // warps per block
+constexpr int kMpSlots = 256;        // maxneigh + 1
+__global__ void __launch_bounds__(kMpW * 32) mp_centre_kernel(MpResArgs r) {
   const MpArgs &a = r.b;
-  const long long w = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (w >= total) return;
-  // u: the last real site with offs[u] + u <= w
-  int lo = 0, hi = a.n_real - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if ((long long)a.offs[mid] + mid <= w) lo = mid;
-    else hi = mid - 1;
+  __shared__ double acc_s[kMpW][kMpSlots][5];
+  __shared__ double stage_s[kMpW][32][15];  // per lane: its triplet's 15 values
+  __shared__ int key_s[kMpW][32][2];
+  __shared__ int act_s[kMpW][kMpSlots];
+  __shared__ double scr_s[kMpW][32][57];  // tri_all's per-lane scratch (odd stride)
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int o = blockIdx.x * kMpW + warp;
+  if (o >= a.n_real) return;
+  double(*acc)[5] = acc_s[warp];
+  int *act = act_s[warp];
+  const int nb0 = a.offs[o], nn = a.offs[o + 1] - nb0;
+  if (nn >= kMpSlots) {  // longer than maxneigh lists are refused when built
+    for (int e = lane; e < 5 * (1 + nn); e += 32) r.gk[5 * ((size_t)nb0 + o) + e] = nan("");
+    return;
   }
-  const int u = lo, c = (int)(w - ((long long)a.offs[u] + u));
-  double *out = r.g5 + 5 * w;
-  const int ic = c == 0 ? u : a.idx[a.offs[u] + c - 1];
-  const int o = r.owner[ic];
-  // u in o's frame: itself for the centre u; else the entry of o's list
-  // that is u translated as ic is
-  int uu = u, ks = -1;
-  if (c != 0) {
-    const double4 pu = a.pos[u], pc = a.pos[ic], po = a.pos[o];
-    const double d[3] = {pu.x - pc.x, pu.y - pc.y, pu.z - pc.z};
-    uu = -1;
-    for (int k = a.offs[o] + lane; k < a.offs[o + 1]; k += 32) {
-      const int j = a.idx[k];
-      if (r.owner[j] != u) continue;
-      const double4 pj = a.pos[j];
-      if (fabs(pj.x - po.x - d[0]) < 1e-8 && fabs(pj.y - po.y - d[1]) < 1e-8 &&
-          fabs(pj.z - po.z - d[2]) < 1e-8)
-        ks = k;
-    }
-    for (int off = 16; off > 0; off >>= 1) ks = max(ks, __shfl_xor_sync(0xffffffffu, ks, off));
-    if (ks >= 0) uu = a.idx[ks];
-  }
+  for (int k = lane; k < 1 + nn; k += 32)
+    for (int c = 0; c < 5; ++c) acc[k][c] = 0.0;
   const PairSite so = site_of(a, o);
-  double acc[12];  // dV0/dq parts: drho 0-2, pair 3-5, dipole 6-8, quadrupole 9-11
-#pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = 0.0;
-  double sq4[4] = {0, 0, 0, 0};  // drho_s, pair_s, dip_s, quad_s
-  double sx[4] = {0, 0, 0, 0};   // drho_x, pair_x, dip_x, quad_x
-  const bool live = uu >= 0 && !(a.xb[uu].x < kMinOcc) && !(so.x < kMinOcc);
+  const bool live = !(so.x < kMinOcc);
+  // active entries in list order
+  int na = 0;
+  for (int base = 0; base < nn; base += 32) {
+    const int k = base + lane;
+    const bool on = live && k < nn && !(a.xb[a.idx[nb0 + k]].x < kMinOcc);
+    const unsigned m = __ballot_sync(0xffffffffu, on);
+    if (on) act[na + __popc(m & ((1u << lane) - 1u))] = k;
+    na += __popc(m);
+  }
+  __syncwarp();
+  double dF = 0.0, Fv = 0.0;
   if (live) {
-    const int nb0 = a.offs[o], nn = a.offs[o + 1] - nb0;
-    auto add_pair = [&](const PairOut &po_) {
-      for (int b = 0; b < 3; ++b) {
-        acc[b] += po_.drho_q[b];
-        acc[3 + b] += po_.pair_q[b];
-      }
-      sq4[0] += po_.drho_s;
-      sq4[1] += po_.pair_s;
-      sx[0] += po_.drho_x;
-      sx[1] += po_.pair_x;
-    };
-    auto add_tri = [&](const TriOut &t, double f) {
-      for (int b = 0; b < 3; ++b) {
-        acc[6 + b] += f * t.dip_q[b];
-        acc[9 + b] += f * t.quad_q[b];
-      }
-      sq4[2] += f * t.dip_s;
-      sq4[3] += f * t.quad_s;
-      sx[2] += f * t.dip_x;
-      sx[3] += f * t.quad_x;
-    };
-    if (c == 0) {
-      // i = u: every pair and triplet of u's list, u in slot 0
-      for (int k = lane; k < nn; k += 32) {
-        const PairSite sj = site_of(a, a.idx[nb0 + k]);
-        if (sj.x < kMinOcc) continue;
-        PairOut po_;
-        pair_residual(a.T, a.rule, so, sj, 0, po_);
-        add_pair(po_);
-      }
-      const long long ntri = (long long)nn * (nn + 1) / 2;
-      for (long long t = lane; t < ntri; t += 32) {
-        int k2 = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
-        while ((long long)k2 * (k2 + 1) / 2 > t) --k2;
-        while ((long long)(k2 + 1) * (k2 + 2) / 2 <= t) ++k2;
-        const int k1 = (int)(t - (long long)k2 * (k2 + 1) / 2);
-        const PairSite s1 = site_of(a, a.idx[nb0 + k1]);
-        if (s1.x < kMinOcc) continue;
-        const PairSite s2 = site_of(a, a.idx[nb0 + k2]);
-        const bool wq = !(s2.x <= kMinOcc), wx = !(s2.x < kMinOcc);
-        if (!wq && !wx) continue;
-        TriOut to;
-        tri_residual(a.T, a.rule, so, s1, s2, k1 == k2, 0, wq, wx, to);
-        add_tri(to, k1 == k2 ? 1.0 : 2.0);
-      }
-    } else {
-      // i = o: the pair (o, u) and the triplets of o's list that hold u
-      const PairSite su = site_of(a, uu);
-      if (lane == 0) {
-        PairOut po_;
-        pair_residual(a.T, a.rule, so, su, 1, po_);
-        add_pair(po_);
-      }
-      const int kk = ks - nb0;
-      for (int k = lane; k < nn; k += 32) {
-        const PairSite sk = site_of(a, a.idx[nb0 + k]);
-        if (k >= kk) {
-          // (j1, j2) = (u, k): u in slot 1, and in slot 2 as well for k = u
-          const bool wq = !(sk.x <= kMinOcc), wx = !(sk.x < kMinOcc);
-          if (!wq && !wx) continue;
-          const double f = k == kk ? 1.0 : 2.0;
-          for (int dir = 1; dir <= (k == kk ? 2 : 1); ++dir) {
-            TriOut to;
-            tri_residual(a.T, a.rule, so, su, sk, k == kk, dir, wq, wx, to);
-            add_tri(to, f);
-          }
-        } else {
-          // (j1, j2) = (k, u): u in slot 2
-          if (sk.x < kMinOcc) continue;
-          const bool wq = !(su.x <= kMinOcc), wx = !(su.x < kMinOcc);
-          if (!wq && !wx) continue;
-          TriOut to;
-          tri_residual(a.T, a.rule, so, sk, su, false, 2, wq, wx, to);
-          add_tri(to, 2.0);
-        }
-      }
-    }
+    double p;
+    const SplineView<double> &E = so.code == 0 ? a.emb_mg : a.emb_h;
+    const int m = seg_ref(a.rho[o], E.dx, E.n, p);
+    const Coef4<double> cf = E.c[m];
+    const double kk4[4] = {cf.a, cf.b, cf.c, cf.d};
+    dF = cubd(kk4, p);
+    Fv = cubv(kk4, p);
+  }
+  const double fx = so.x * dF;  // the embedding factor of the rho terms
+  // pairs: slot 0 (u = o) summed over lanes, slot 1 + k (u = entry k) once
+  double ps[5] = {0, 0, 0, 0, 0};
+  for (int m = lane; m < na; m += 32) {
+    const int k = act[m];
+    const PairSite sj = site_of(a, a.idx[nb0 + k]);
+    PairOut p0, p1;
+    pair_residual(a.T, a.rule, so, sj, 0, p0);
+    pair_residual(a.T, a.rule, so, sj, 1, p1);
+    for (int b = 0; b < 3; ++b) ps[b] += fx * p0.drho_q[b] + p0.pair_q[b];
+    ps[3] += fx * p0.drho_s + p0.pair_s;
+    ps[4] += (so.code == 0 ? dF * p0.drho_x : 0.0) + p0.pair_x;
+    for (int b = 0; b < 3; ++b) acc[1 + k][b] = fx * p1.drho_q[b] + p1.pair_q[b];
+    acc[1 + k][3] = fx * p1.drho_s + p1.pair_s;
+    acc[1 + k][4] = (so.code == 1 ? so.x * dF : dF) * p1.drho_x + p1.pair_x;
   }
 #pragma unroll
-  for (int k = 0; k < 12; ++k) acc[k] = warp_sum(acc[k]);
-#pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    sq4[k] = warp_sum(sq4[k]);
-    sx[k] = warp_sum(sx[k]);
-  }
+  for (int c = 0; c < 5; ++c) ps[c] = warp_sum(ps[c]);
+  __syncwarp();
   if (lane == 0) {
-    double g[5] = {0, 0, 0, 0, 0};
-    if (live) {
-      double p;
-      const SplineView<double> &E = so.code == 0 ? a.emb_mg : a.emb_h;
-      const int m = seg_ref(a.rho[o], E.dx, E.n, p);
-      const Coef4<double> cf = E.c[m];
-      const double kk4[4] = {cf.a, cf.b, cf.c, cf.d};
-      const double dF = cubd(kk4, p);
-      for (int b = 0; b < 3; ++b) g[b] = so.x * dF * acc[b] + acc[3 + b] + acc[6 + b] + acc[9 + b];
-      g[3] = so.x * dF * sq4[0] + sq4[1] + sq4[2] + sq4[3];
-      // evaluate_DV0_i_Dxi_u_adp_MgHx's embedding part (2300-2315)
-      double emb = 0.0;
-      if (so.code == 1 && o == uu) emb = cubv(kk4, p);
-      if (so.code == 1 && o != uu) emb = so.x * dF * sx[0];
-      if (so.code == 0) emb = dF * sx[0];
-      g[4] = emb + sx[1] + sx[2] + sx[3];
+    for (int c = 0; c < 5; ++c) acc[0][c] = ps[c];
+    if (live && so.code == 1) acc[0][4] += Fv;  // d(x_o F(rho_o))/dx_o's F part
+  }
+  __syncwarp();
+  // triplets (m1 <= m2) of the active entries, 32 per round
+  const long long ntri = (long long)na * (na + 1) / 2;
+  for (long long t0 = 0; t0 < ntri; t0 += 32) {
+    const long long t = t0 + lane;
+    int k1 = -1, k2 = -1;
+    double *out = stage_s[warp][lane];
+    if (t < ntri) {
+      int m2 = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+      while ((long long)m2 * (m2 + 1) / 2 > t) --m2;
+      while ((long long)(m2 + 1) * (m2 + 2) / 2 <= t) ++m2;
+      const int m1 = (int)(t - (long long)m2 * (m2 + 1) / 2);
+      k1 = act[m1];
+      k2 = act[m2];
+      const PairSite s1 = site_of(a, a.idx[nb0 + k1]);
+      const PairSite s2 = site_of(a, a.idx[nb0 + k2]);
+      tri_all(a.T, a.rule, so, s1, s2, m1 == m2, !(s2.x <= kMinOcc), m1 == m2 ? 1.0 : 2.0,
+              scr_s[warp][lane], out);
     }
-    for (int k = 0; k < 5; ++k) out[k] = g[k];
+    key_s[warp][lane][0] = k1;
+    key_s[warp][lane][1] = k2;
+    __syncwarp();
+    if (lane < 5) {
+      for (int l = 0; l < 32; ++l) {
+        const int q1 = key_s[warp][l][0], q2 = key_s[warp][l][1];
+        if (q1 < 0) break;
+        acc[0][lane] += stage_s[warp][l][lane];
+        acc[1 + q1][lane] += stage_s[warp][l][5 + lane];
+        acc[1 + q2][lane] += stage_s[warp][l][10 + lane];
+      }
+    }
+    __syncwarp();
+  }
+  double *g = r.gk + 5 * ((size_t)nb0 + o);
+  for (int e = lane; e < 5 * (1 + nn); e += 32) g[e] = (&acc[0][0])[e];
+}
+
+// The per-(u, centre) layout of the pairs' values: centre 0 is u's own slot
+// 0; centre 1 + k (list entry p = offs[u] + k, owner o) is the slot of o's
+// entry that is u, seen from o (the reverse slot of p).
+__global__ void __launch_bounds__(128) mp_gather_kernel(MpResArgs r) {
+  const MpArgs &a = r.b;
+  const int u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (u >= a.n_real) return;
+  const int nb0 = a.offs[u], nn = a.offs[u + 1] - nb0;
+  double *dst = r.g5 + 5 * ((size_t)nb0 + u);
+  for (int c = lane; c < 1 + nn; c += 32) {
+    const double *src = nullptr;
+    if (c == 0) {
+      src = r.gk + 5 * ((size_t)nb0 + u);
+    } else {
+      const int p = nb0 + c - 1, rv = r.rev[p];
+      if (rv >= 0) src = r.gk + 5 * ((size_t)rv + r.owner[a.idx[p]] + 1);
+    }
+    for (int e = 0; e < 5; ++e) dst[5 * c + e] = src ? src[e] : 0.0;
   }
 }
 
@@ -1442,13 +1683,15 @@ int mp_residuals(btam_system *s, int rule, double *Rq, double *Rs, double *Rx, d
   if (e != cudaSuccess) return cuda_status(e);
   if (slot5 && slot_cap < offs_n[0]) return BTAM_ERR_ARG;
   const long long total = (long long)offs_n[0] + (long long)n;
-  double *rd = nullptr, *g5 = nullptr, *out = nullptr;
+  double *rd = nullptr, *g5 = nullptr, *gk = nullptr, *out = nullptr;
   BTAM_TRY(dalloc(rd, s->st, n));
   int st = dalloc(g5, s->st, 5 * (size_t)total);
+  if (st == BTAM_OK) st = dalloc(gk, s->st, 5 * (size_t)total);
   if (st == BTAM_OK) st = dalloc(out, s->st, 5 * n);
   if (st != BTAM_OK) {
     dfree(rd, s->st);
     dfree(g5, s->st);
+    dfree(gk, s->st);
     return st;
   }
   MpResArgs r;
@@ -1470,15 +1713,17 @@ int mp_residuals(btam_system *s, int rule, double *Rq, double *Rs, double *Rx, d
   a.mass[0] = tables_mass(s->T, 0);
   a.mass[1] = tables_mass(s->T, 1);
   r.owner = s->owner;
+  r.rev = s->rev;
   r.gamma = s->gamma;
+  r.gk = gk;
   r.g5 = g5;
   r.Rq = out;
   r.Rs = out + 3 * n;
   r.Rx = out + 4 * n;
   const int g = (int)(((long long)n * 32 + 127) / 128);
   mp_rho_kernel<<<g, 128, 0, s->st>>>(a);
-  const long long gp = (total * 32 + 127) / 128;
-  mp_pairs_kernel<<<(unsigned)gp, 128, 0, s->st>>>(r, total);
+  mp_centre_kernel<<<(int)((n + kMpW - 1) / kMpW), kMpW * 32, 0, s->st>>>(r);
+  mp_gather_kernel<<<g, 128, 0, s->st>>>(r);
   mp_assemble_kernel<<<(int)((n + 127) / 128), 128, 0, s->st>>>(r);
   e = cudaGetLastError();
   if (e == cudaSuccess && Rq)
@@ -1511,6 +1756,7 @@ int mp_residuals(btam_system *s, int rule, double *Rq, double *Rs, double *Rx, d
   }
   dfree(rd, s->st);
   dfree(g5, s->st);
+  dfree(gk, s->st);
   dfree(out, s->st);
   if (e != cudaSuccess) return cuda_status(e);
   return read_err(s);
