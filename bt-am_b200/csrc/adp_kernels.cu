@@ -65,14 +65,19 @@ __device__ __forceinline__ V3<R> pair_vec(const double4 &a, const double4 &b) {
 __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
 // What the pair kernels read about a neighbour: one 32-byte load from the
-// packed Site32 rows in the FP32C form, the separate arrays otherwise.
+// packed Site32 rows in the FP32C form, two 32-byte loads from the Site64 rows
+// in the FP64 form, the separate arrays otherwise.  BO: also beta and owner
+// (the pass-2 pair kernel), from the same FP64 row.
 template <class R> struct NbSite {
   double x, y, z;
   R sigma, occ;
   int code;
   bool active;
+  double beta;
+  int owner;
 };
-template <class R> __device__ __forceinline__ NbSite<R> nb_site(const EvalArgs<R> &a, int j) {
+template <class R, bool BO = false>
+__device__ __forceinline__ NbSite<R> nb_site(const EvalArgs<R> &a, int j) {
   NbSite<R> n;
   if (sizeof(R) == 4 && a.s32) {
     double4 h;
@@ -89,6 +94,30 @@ template <class R> __device__ __forceinline__ NbSite<R> nb_site(const EvalArgs<R
     n.code = sig_code < 0.0f ? 1 : 0;
     n.occ = (R)occ;
     n.active = occ >= 0.0f;
+    if (BO) {
+      const SiteB e = a.sb[j];
+      n.beta = e.beta;
+      n.owner = e.owner;
+    }
+  } else if (sizeof(R) == 8 && a.s64) {
+    double4 h, t;
+    const double *row = reinterpret_cast<const double *>(a.s64 + j);
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"(h.x), "=d"(h.y), "=d"(h.z), "=d"(h.w)
+        : "l"(row));
+    asm("ld.global.nc.v4.f64 {%0,%1,%2,%3}, [%4];"
+        : "=d"(t.x), "=d"(t.y), "=d"(t.z), "=d"(t.w)
+        : "l"(row + 4));
+    const long long co = __double_as_longlong(t.y);  // (code, owner), low word first
+    n.x = h.x;
+    n.y = h.y;
+    n.z = h.z;
+    n.sigma = (R)h.w;
+    n.occ = (R)t.x;
+    n.code = (int)(co & 0xffffffffll);
+    n.active = !(t.x < kMinOcc);
+    n.beta = t.z;
+    n.owner = (int)(co >> 32);
   } else {
     const double4 q = a.pos[j];
     const double2 xb = a.xb[j];
@@ -99,14 +128,12 @@ template <class R> __device__ __forceinline__ NbSite<R> nb_site(const EvalArgs<R
     n.occ = (R)xb.x;
     n.code = a.code[j];
     n.active = !(xb.x < kMinOcc);
+    if (BO) {
+      n.beta = xb.y;
+      n.owner = a.owner[j];
+    }
   }
   return n;
-}
-template <class R> __device__ __forceinline__ double nb_beta(const EvalArgs<R> &a, int j) {
-  return (sizeof(R) == 4 && a.sb) ? a.sb[j].beta : a.xb[j].y;
-}
-template <class R> __device__ __forceinline__ int nb_owner(const EvalArgs<R> &a, int j) {
-  return (sizeof(R) == 4 && a.sb) ? a.sb[j].owner : a.owner[j];
 }
 template <class R> __device__ __forceinline__ V3<R> pair_vec(const double4 &a, const NbSite<R> &b) {
   return mk3<R>((R)(a.x - b.x), (R)(a.y - b.y), (R)(a.z - b.z));
@@ -135,6 +162,26 @@ __global__ void pack_sites_kernel(int n, const double4 *pos, const double2 *xb, 
   e.owner = owner[i];
   e.pad = 0;
   sb[i] = e;
+}
+
+// Packs the FP64 neighbour rows (Site64) of all sites.
+__global__ void pack_sites64_kernel(int n, const double4 *pos, const double2 *xb,
+                                    const int *code, const int *owner, Site64 *s64) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double4 q = pos[i];
+  const double2 b = xb[i];
+  Site64 r;
+  r.x = q.x;
+  r.y = q.y;
+  r.z = q.z;
+  r.sigma = q.w;
+  r.occ = b.x;
+  r.code = code[i];
+  r.owner = owner[i];
+  r.beta = b.y;
+  r.pad = 0.0;
+  s64[i] = r;
 }
 
 // ---- record stores of the undirected kernels -------------------------------
@@ -709,13 +756,13 @@ template <class R, class TV>
 __device__ __forceinline__ void pass2u_one(const EvalArgs<R> &a, const TV &T, int t) {
   const int p = a.own_p[t], u = a.own_u[t];
   const int j = a.idx[p], r = a.rev[p];
-  const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
+  const NbSite<R> su = nb_site<R, true>(a, u), sj = nb_site<R, true>(a, j);
   R vu[8], vj[8];
 #pragma unroll
   for (int c = 0; c < 8; ++c) vu[c] = vj[c] = (R)0;
   if (su.active && sj.active) {
-    const int o = nb_owner(a, j);
-    const double bu = nb_beta(a, u), bj = nb_beta(a, j);
+    const int o = sj.owner;
+    const double bu = su.beta, bj = sj.beta;
     const MomRec<R, true> mu(a.mom + (size_t)u * kMomStride);
     const MomRec<R, true> mj(a.mom + (size_t)o * kMomStride);
     Pass2Out<R> ou, oj;
@@ -955,6 +1002,9 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2, c
   if (a.s32 && a.n_all > 0)
     pack_sites_kernel<<<nblocks(a.n_all, 256), 256, 0, st>>>(a.n_all, a.pos, a.xb, a.code,
                                                              a.owner, a.s32, a.sb);
+  if (a.s64 && a.n_all > 0)
+    pack_sites64_kernel<<<nblocks(a.n_all, 256), 256, 0, st>>>(a.n_all, a.pos, a.xb, a.code,
+                                                               a.owner, a.s64);
   switch (v & (kPersistent - 1)) {
   case 1: go1<R, 4, 5, 8>(a, st, pers, und, mid); break;
   case 2: go1<R, 4, 4, 16>(a, st, pers, und, mid); break;

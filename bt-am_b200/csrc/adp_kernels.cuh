@@ -21,6 +21,15 @@ struct __align__(16) SiteB {
   double beta;
   int owner, pad;
 };
+// Packed copy of what the FP64 kernels read about a neighbour, one 64-byte
+// row (two sectors) per site (made by launch_pass1 from pos / xb / code /
+// owner): position and sigma, then occupancy, species, owner and beta.
+struct __align__(64) Site64 {
+  double x, y, z, sigma;
+  double occ;
+  int code, owner;
+  double beta, pad;
+};
 
 // Device view of one system for an evaluation.  Site arrays cover real sites
 // then periodic images ("all sites"); per-site outputs cover real sites.
@@ -29,6 +38,7 @@ template <class R> struct EvalArgs {
   int n_all = 0;        // real sites + images (rows of the site arrays)
   Site32 *s32 = nullptr;  // FP32C: packed neighbour data [all] (nullptr: unpacked)
   SiteB *sb = nullptr;    // FP32C: beta and owner [all]
+  Site64 *s64 = nullptr;  // FP64: packed neighbour rows [all] (nullptr: unpacked)
   const double4 *pos;   // x, y, z, sigma            [all]
   const double2 *xb;    // occupancy x, beta         [all]
   const int *code;      // 0 = Mg, 1 = H             [all]

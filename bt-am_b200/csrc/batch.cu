@@ -122,6 +122,7 @@ struct btam_batch {
   // undirected pass 2: reverse slots, owned slots and their sites, slot buffer
   Site32 *s32 = nullptr;  // packed neighbour rows of the FP32C kernels [all]
   SiteB *sb = nullptr;
+  Site64 *s64 = nullptr;  // packed neighbour rows of the FP64 kernels [all]
   int *rev = nullptr, *slot_own = nullptr, *own_p = nullptr, *own_u = nullptr;
   int n_own = 0;
   char *pbuf = nullptr;
@@ -149,6 +150,8 @@ template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const RadialVie
   if (sizeof(R) == 4) {
     a.s32 = b->s32;
     a.sb = b->sb;
+  } else {
+    a.s64 = b->s64;
   }
   a.pos = b->pos;
   a.xb = b->xb;
@@ -252,6 +255,7 @@ void free_batch(btam_batch *b) {
   dfree(b->rev, b->st);
   dfree(b->s32, b->st);
   dfree(b->sb, b->st);
+  dfree(b->s64, b->st);
   dfree(b->slot_own, b->st);
   dfree(b->own_p, b->st);
   dfree(b->own_u, b->st);
@@ -307,6 +311,7 @@ int batch_build(btam_batch *b) {
   BTAM_TRY(dalloc(b->owner, b->st, na));
   BTAM_TRY(dalloc(b->s32, b->st, na));
   BTAM_TRY(dalloc(b->sb, b->st, na));
+  BTAM_TRY(dalloc(b->s64, b->st, na));
   BTAM_TRY(dalloc(b->gamma, b->st, nr));
   BTAM_TRY(dalloc(b->offs, b->st, nr + 1));
   BTAM_TRY(dalloc(b->idx, b->st, (size_t)n_pairs));

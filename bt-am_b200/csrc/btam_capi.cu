@@ -239,6 +239,7 @@ int ensure_sites(btam_system *s, int n_all) {
   // packed neighbour rows of the FP32C kernels (rewritten by every pass 1)
   BTAM_TRY(dalloc(s->s32, s->st, cap));
   BTAM_TRY(dalloc(s->sb, s->st, cap));
+  BTAM_TRY(dalloc(s->s64, s->st, cap));
   s->cap_all = cap;
   return BTAM_OK;
 }
@@ -250,6 +251,8 @@ template <class R> EvalArgs<R> eval_args(btam_system *s, R *mom, const RadialVie
   if (sizeof(R) == 4) {
     a.s32 = s->s32;
     a.sb = s->sb;
+  } else {
+    a.s64 = s->s64;
   }
   a.pos = s->pos;
   a.xb = s->xb;
@@ -612,7 +615,7 @@ void btam_system_destroy(btam_system *s) {
   if (s->st) cudaStreamSynchronize(s->st);
   dfree(s->pos, s->st); dfree(s->xb, s->st); dfree(s->code, s->st); dfree(s->owner, s->st); dfree(s->image, s->st);
   dfree(s->pt, s->st);
-  dfree(s->s32, s->st); dfree(s->sb, s->st);
+  dfree(s->s32, s->st); dfree(s->sb, s->st); dfree(s->s64, s->st);
   dfree(s->gamma, s->st); dfree(s->stage, s->st); dfree(s->offs, s->st); dfree(s->idx, s->st); dfree(s->cnt, s->st);
   dfree(s->tmp, s->st); dfree(s->bbox, s->st); dfree(s->grid, s->st); dfree(s->cell_of, s->st); dfree(s->cell_cnt, s->st);
   dfree(s->cell_start, s->st); dfree(s->cursor, s->st); dfree(s->cell_sites, s->st); dfree(s->rho, s->st); dfree(s->V0, s->st);

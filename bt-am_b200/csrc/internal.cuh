@@ -48,6 +48,7 @@ struct btam_system {
   double *gamma = nullptr;
   Site32 *s32 = nullptr;  // packed neighbour rows of the FP32C kernels [all]
   SiteB *sb = nullptr;
+  Site64 *s64 = nullptr;  // packed neighbour rows of the FP64 kernels [all]
   // staging for host updates
   double *stage = nullptr;  // 5 n_real doubles: q (3n), sigma, x
   // neighbour lists
