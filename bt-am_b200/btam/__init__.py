@@ -69,6 +69,7 @@ _PROTOS = {
     "btam_mf_rho": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_mf_eval": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D]),
     "btam_mf_eval_async": (ctypes.c_int, [_V, ctypes.c_int]),
+    "btam_mf_eval_x": (ctypes.c_int, [_V, ctypes.c_int]),
     "btam_mf_eval_state": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D,
                                           _D, _D]),
     "btam_results_copy": (ctypes.c_int, [_V, _D, _D, _D, _D, _D, _D, _D]),
@@ -391,6 +392,12 @@ class System:
 
     def evaluate_async(self, precision=FP64):
         _check(lib().btam_mf_eval_async(self.handle, precision), "btam_mf_eval_async")
+
+    def evaluate_x(self, precision=FP64):
+        """The occupancy gradients alone (btam_mf_eval_x): rho, V0, S0, Rx and
+        totals of the state, Rq and Rs 0; synchronises."""
+        _check(lib().btam_mf_eval_x(self.handle, precision), "btam_mf_eval_x")
+        return self.results(want=("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals"))
 
     def sync(self):
         _check(lib().btam_system_sync(self.handle), "btam_system_sync")

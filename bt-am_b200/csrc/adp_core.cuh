@@ -453,6 +453,16 @@ BTAM_HD void dual_ax_at(const DualAx<R> &P, int k, R a, const Geo<R> &g, V3<R> &
   f = g.u * dar + g.w * rLr;
 }
 
+// D . f(r) alone at r = r0 + a e_k, formed as dual_ax_at forms it.
+template <class R>
+BTAM_HD R dual_ax_f(const DualAx<R> &P, int k, R a, const Geo<R> &g) {
+  const Dual<R> &D = P.D;
+  R lkk = k == 0 ? D.d[0] : (k == 1 ? D.d[1] : D.d[2]);
+  R rLr = P.rLr0 + a * ((R)2 * comp(P.Lr0, k) + a * lkk);
+  R dar = P.dar0 + a * D.a[k];
+  return g.u * dar + g.w * rLr;
+}
+
 // D . f(r) with f(r) = (u r, w r r^T):  u (Da.r) + w (r^T Lambda r)
 template <class R> BTAM_HD R dual_f(const Dual<R> &D, const Geo<R> &g) {
   V3<R> Da = mk3<R>(D.a[0], D.a[1], D.a[2]);
@@ -625,6 +635,38 @@ BTAM_HD void pair_rule_record(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R 
         rec[o] += A * sd;
         rec[o + 1] += B * sd;
         rec[o + 2] += C * sd;
+      }
+  }
+}
+
+// The four pass-1 sums of pair_rule_record alone ([0] sum rho_{s_u},
+// [1] sum rho_{s_j}, [2] sum phi, [3] sum B(f, f)), from the same points
+// and operations without their derivatives.  They depend on positions and
+// widths only, so a run of evaluations at fixed positions and widths (the
+// master equation's steps) can keep them.
+template <class R, class TV>
+BTAM_HD void pair_rule_sums(const TV &T, const V3<R> &r0, R sig_u, R sig_j, int cu, int cj,
+                            R (&rec)[kPr1]) {
+  const int pk = pair_kind(cu, cj);
+#pragma unroll
+  for (int c = 0; c < kPr1; ++c) rec[c] = (R)0;
+#pragma unroll
+  for (int side = 0; side < 2; ++side) {
+    const R amt = (side == 0 ? sig_u : -sig_j) * (R)kDelta6;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int sg = 0; sg < 2; ++sg) {
+        const R a = sg ? -amt : amt;
+        Geo<R> g;
+        R p;
+        const int m = geo_uw<R, false>(g, disp(r0, k, a), T, pk, p);
+        R rj, drj, ru, dru, ph, dph;
+        pr_at<R, false, true>(T, pk, cu, cj, m, p, ph, dph, rj, drj, ru, dru);
+        rec[0] += ru;
+        rec[1] += rj;
+        rec[2] += ph;
+        rec[3] += bff(g);
       }
   }
 }
@@ -999,7 +1041,11 @@ BTAM_HD void pass2_pair(const RadialView<R> &T, const V3<R> &r0, R sig_u,
 // beta_j / beta_u, omega_ju = beta_u / beta_j; pr: the pair's record from
 // pair_rule_record (its 12 pair-rule points were evaluated once, in pass 1;
 // only the 13 triplet geometries are evaluated here).
-template <class R, class MU, class MJ, class TV>
+// XO: the occupancy gradients only (ou.gx, oj.gx), the chemical potentials
+// of the master equation: the same x terms from the same operations, the
+// values at the 13 geometries without their derivatives, no position or
+// width terms (ou.gq, ou.gs, oj.gq, oj.gs are left as they are).
+template <class R, class MU, class MJ, class TV, bool XO = false>
 BTAM_HD void pass2_pair_sym(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu,
                             R xj, int cu, int cj, R embq_u, R embx_u, R embq_j, R embx_j,
                             R omega_uj, R omega_ju, const MU &mu, const MJ &mj,
@@ -1016,16 +1062,18 @@ BTAM_HD void pass2_pair_sym(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu
 
   // ---- 12-point pair rule, from the pair's record (pair_rule_record)
   {
-    const R ku = embq_u * xj, kj = embq_j * xu;
+    if constexpr (!XO) {
+      const R ku = embq_u * xj, kj = embq_j * xu;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      self_q[c] = w6 * (ku * pr[4 + c] + pr[10 + c]);
-      cros_q[c] = w6 * (kj * pr[7 + c] + pr[10 + c]);
+      for (int c = 0; c < 3; ++c) {
+        self_q[c] = w6 * (ku * pr[4 + c] + pr[10 + c]);
+        cros_q[c] = w6 * (kj * pr[7 + c] + pr[10 + c]);
+      }
+      self_s = w6 * (ku * pr[13] + pr[15]);
+      cros_s = w6 * (kj * pr[14] + pr[15]);
+      rself_s = w6 * (kj * pr[17] + pr[18]);
+      rcros_s = w6 * (ku * pr[16] + pr[18]);
     }
-    self_s = w6 * (ku * pr[13] + pr[15]);
-    cros_s = w6 * (kj * pr[14] + pr[15]);
-    rself_s = w6 * (kj * pr[17] + pr[18]);
-    rcros_s = w6 * (ku * pr[16] + pr[18]);
     cros_x = w6 * (embx_j * pr[0] + (R)0.5 * xj * pr[2] + (R)2 * X * xj * pr[3]);
     rcros_x = w6 * (embx_u * pr[1] + (R)0.5 * xu * pr[2] + (R)2 * X * xu * pr[3]);
   }
@@ -1034,7 +1082,7 @@ BTAM_HD void pass2_pair_sym(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu
   Geo<R> gc;
   {
     R p;
-    geo_uw<R, true>(gc, r0, T, pk, p);
+    geo_uw<R, !XO>(gc, r0, T, pk, p);
   }
   const Dual<R> Xf0 = dual_feat(gc, X);
   const R sfac = (R)2 * w9 * X;
@@ -1053,25 +1101,32 @@ BTAM_HD void pass2_pair_sym(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu
         const R a = sg ? -amt : amt;
         Geo<R> g;
         R p;
-        geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
-        feat_add(FA, g);
-        R hb = (R)0.5 * X * bff_grad_coef(g);
-        V3<R> v4;
-        R f4u;
-        dual_Jf(mu.dual(kDualGd + 2 * k + sg), g, v4, f4u);  // S4
-        V3<R> v5, vx;
-        R f5, fx;
-        dual_ax_at(c5, k, a, g, v5, f5);  // C5
-        dual_ax_at(x5, k, a, g, vx, fx);  // X5
-        V3<R> s4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
-        self_q[0] += sfac * s4.x; self_q[1] += sfac * s4.y; self_q[2] += sfac * s4.z;
-        cros_q[0] += sfac * v5.x; cros_q[1] += sfac * v5.y; cros_q[2] += sfac * v5.z;
-        R sd = sg ? -(R)kDelta9 : (R)kDelta9;
-        self_s += sfac * comp(s4, k) * sd;
-        cros_s += sfac * comp(v5, k) * sd;
-        cros_x += (R)2 * w9 * xj * fx;
-        // j's view: u's centre-displaced term as a function of x_j
-        rcros_x += (R)2 * w9 * xu * (f4u - X * bff(g));
+        geo_uw<R, !XO>(g, disp(r0, k, a), T, pk, p);
+        if constexpr (XO) {
+          const R fx = dual_ax_f(x5, k, a, g);
+          const R f4u = dual_f(mu.dual(kDualGd + 2 * k + sg), g);
+          cros_x += (R)2 * w9 * xj * fx;
+          rcros_x += (R)2 * w9 * xu * (f4u - X * bff(g));
+        } else {
+          feat_add(FA, g);
+          R hb = (R)0.5 * X * bff_grad_coef(g);
+          V3<R> v4;
+          R f4u;
+          dual_Jf(mu.dual(kDualGd + 2 * k + sg), g, v4, f4u);  // S4
+          V3<R> v5, vx;
+          R f5, fx;
+          dual_ax_at(c5, k, a, g, v5, f5);  // C5
+          dual_ax_at(x5, k, a, g, vx, fx);  // X5
+          V3<R> s4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
+          self_q[0] += sfac * s4.x; self_q[1] += sfac * s4.y; self_q[2] += sfac * s4.z;
+          cros_q[0] += sfac * v5.x; cros_q[1] += sfac * v5.y; cros_q[2] += sfac * v5.z;
+          R sd = sg ? -(R)kDelta9 : (R)kDelta9;
+          self_s += sfac * comp(s4, k) * sd;
+          cros_s += sfac * comp(v5, k) * sd;
+          cros_x += (R)2 * w9 * xj * fx;
+          // j's view: u's centre-displaced term as a function of x_j
+          rcros_x += (R)2 * w9 * xu * (f4u - X * bff(g));
+        }
       }
   }
   // B: j displaced by -+3 sigma_j e_k (j's centre-displaced points)
@@ -1088,54 +1143,67 @@ BTAM_HD void pass2_pair_sym(const TV &T, const V3<R> &r0, R sig_u, R sig_j, R xu
         const R a = sg ? amt : -amt;
         Geo<R> g;
         R p;
-        geo_uw<R, true>(g, disp(r0, k, a), T, pk, p);
-        feat_add(FB, g);
-        V3<R> v5, vxf;
-        R f5, fxf;
-        dual_ax_at(s5, k, a, g, v5, f5);  // S5
-        dual_ax_at(xf, k, a, g, vxf, fxf);
-        self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
-        const Dual<R> Pj = dual_flip(mj.dual(kDualGd + 2 * k + sg));
-        V3<R> v4;
-        R f4;
-        dual_Jf(Pj, g, v4, f4);  // C4
-        R hb = (R)0.5 * X * bff_grad_coef(g);
-        V3<R> c4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
-        cros_q[0] += sfac * c4.x; cros_q[1] += sfac * c4.y; cros_q[2] += sfac * c4.z;
-        R bffg = bff(g);
-        cros_x += (R)2 * w9 * xj * (f4 - X * bffg);
-        R sd = sg ? (R)kDelta9 : -(R)kDelta9;
-        rself_s += sfac * comp(c4, k) * sd;
-        rcros_s += sfac * comp(v5, k) * sd;
-        // j's view: u's neighbour-displaced term as a function of x_j
-        rcros_x += (R)2 * w9 * xu * (f5 - fxf);
+        geo_uw<R, !XO>(g, disp(r0, k, a), T, pk, p);
+        if constexpr (XO) {
+          const R f5 = dual_ax_f(s5, k, a, g);
+          const R fxf = dual_ax_f(xf, k, a, g);
+          const R f4 = dual_f(dual_flip(mj.dual(kDualGd + 2 * k + sg)), g);
+          R bffg = bff(g);
+          cros_x += (R)2 * w9 * xj * (f4 - X * bffg);
+          rcros_x += (R)2 * w9 * xu * (f5 - fxf);
+        } else {
+          feat_add(FB, g);
+          V3<R> v5, vxf;
+          R f5, fxf;
+          dual_ax_at(s5, k, a, g, v5, f5);  // S5
+          dual_ax_at(xf, k, a, g, vxf, fxf);
+          self_q[0] += sfac * v5.x; self_q[1] += sfac * v5.y; self_q[2] += sfac * v5.z;
+          const Dual<R> Pj = dual_flip(mj.dual(kDualGd + 2 * k + sg));
+          V3<R> v4;
+          R f4;
+          dual_Jf(Pj, g, v4, f4);  // C4
+          R hb = (R)0.5 * X * bff_grad_coef(g);
+          V3<R> c4 = mk3<R>(v4.x - hb * g.r.x, v4.y - hb * g.r.y, v4.z - hb * g.r.z);
+          cros_q[0] += sfac * c4.x; cros_q[1] += sfac * c4.y; cros_q[2] += sfac * c4.z;
+          R bffg = bff(g);
+          cros_x += (R)2 * w9 * xj * (f4 - X * bffg);
+          R sd = sg ? (R)kDelta9 : -(R)kDelta9;
+          rself_s += sfac * comp(c4, k) * sd;
+          rcros_s += sfac * comp(v5, k) * sd;
+          // j's view: u's neighbour-displaced term as a function of x_j
+          rcros_x += (R)2 * w9 * xu * (f5 - fxf);
+        }
       }
   }
   // centre-geometry pieces
   {
-    Dual<R> dFB = dual_of<R, R>(FB.a, FB.l);
-    Dual<R> dFA = dual_of<R, R>(FA.a, FA.l);
-    for (int k = 0; k < 3; ++k) {
-      dFB.a[k] *= X; dFB.d[k] *= X; dFB.o[k] *= X;
-      dFA.a[k] *= X; dFA.d[k] *= X; dFA.o[k] *= X;
-    }
     const Dual<R> Dj_h = mj.dual(kDualH);
     const Dual<R> Du_h = mu.dual(kDualH);
-    V3<R> vs = dual_J(dual_sub(Du_h, dFB), gc);
-    V3<R> vc = dual_J(dual_sub(dual_flip(Dj_h), dFA), gc);
-    self_q[0] += sfac * vs.x; self_q[1] += sfac * vs.y; self_q[2] += sfac * vs.z;
-    cros_q[0] += sfac * vc.x; cros_q[1] += sfac * vc.y; cros_q[2] += sfac * vc.z;
+    if constexpr (!XO) {
+      Dual<R> dFB = dual_of<R, R>(FB.a, FB.l);
+      Dual<R> dFA = dual_of<R, R>(FA.a, FA.l);
+      for (int k = 0; k < 3; ++k) {
+        dFB.a[k] *= X; dFB.d[k] *= X; dFB.o[k] *= X;
+        dFA.a[k] *= X; dFA.d[k] *= X; dFA.o[k] *= X;
+      }
+      V3<R> vs = dual_J(dual_sub(Du_h, dFB), gc);
+      V3<R> vc = dual_J(dual_sub(dual_flip(Dj_h), dFA), gc);
+      self_q[0] += sfac * vs.x; self_q[1] += sfac * vs.y; self_q[2] += sfac * vs.z;
+      cros_q[0] += sfac * vc.x; cros_q[1] += sfac * vc.y; cros_q[2] += sfac * vc.z;
+    }
     cros_x += (R)2 * w9 * xj * dual_f(dual_flip(Dj_h), gc);
     rcros_x += (R)2 * w9 * xu * dual_f(Du_h, gc);
   }
 
-  for (int k = 0; k < 3; ++k) {
-    ou.gq[k] += self_q[k] + omega_uj * cros_q[k];
-    oj.gq[k] += -cros_q[k] - omega_ju * self_q[k];
+  if constexpr (!XO) {
+    for (int k = 0; k < 3; ++k) {
+      ou.gq[k] += self_q[k] + omega_uj * cros_q[k];
+      oj.gq[k] += -cros_q[k] - omega_ju * self_q[k];
+    }
+    ou.gs += self_s + omega_uj * cros_s;
+    oj.gs += rself_s + omega_ju * rcros_s;
   }
-  ou.gs += self_s + omega_uj * cros_s;
   ou.gx += omega_uj * cros_x;
-  oj.gs += rself_s + omega_ju * rcros_s;
   oj.gx += omega_ju * rcros_x;
 }
 

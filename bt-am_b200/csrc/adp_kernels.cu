@@ -324,6 +324,12 @@ pass1u_pair_kernel(const EvalArgs<R> a) {
     const int p = a.own_p[t], u = a.own_u[t];
     const int j = a.idx[p];
     const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
+    if (a.x_only) {  // the four pass-1 sums, occupied or not
+      R s4[kPr1];
+      pair_rule_sums<R>(T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.code, sj.code, s4);
+      st_rec4(a.prec1 + (size_t)kPr1 * t, s4);
+      continue;
+    }
     R rec[kPrRec];
     if (su.active && sj.active) {
       pair_rule_record<R>(T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
@@ -752,7 +758,9 @@ mf_pair_terms_kernel(const EvalArgs<R> a, double *self, double *slot) {
 // geometries (pass2_pair_sym); u's part into slot p, j's part into the
 // reverse slot.  Pairs with an empty site give zero records, so every slot
 // of the real sites' lists is written exactly once per evaluation.
-template <class R, class TV>
+// XO: the occupancy gradients alone (EvalArgs::x_only): only prec1 is read
+// and only the gx slot values are written.
+template <class R, class TV, bool XO = false>
 __device__ __forceinline__ void pass2u_one(const EvalArgs<R> &a, const TV &T, int t) {
   const int p = a.own_p[t], u = a.own_u[t];
   const int j = a.idx[p], r = a.rev[p];
@@ -775,25 +783,31 @@ __device__ __forceinline__ void pass2u_one(const EvalArgs<R> &a, const TV &T, in
 #pragma unroll
       for (int c = 0; c < kPr1; ++c) pr[c] = v4[c];
     }
-    const R *src = a.prec2 + (size_t)kPr2 * t;
+    if constexpr (XO) {
 #pragma unroll
-    for (int h = 0; h < kPr2 / 8; ++h) {
-      R v[8];
-      ld8(src + 8 * h, v);
+      for (int c = kPr1; c < kPrRec; ++c) pr[c] = (R)0;
+    } else {
+      const R *src = a.prec2 + (size_t)kPr2 * t;
 #pragma unroll
-      for (int c = 0; c < 8; ++c) pr[kPr1 + 8 * h + c] = v[c];
+      for (int h = 0; h < kPr2 / 8; ++h) {
+        R v[8];
+        ld8(src + 8 * h, v);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) pr[kPr1 + 8 * h + c] = v[c];
+      }
     }
-    pass2_pair_sym<R>(T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code,
-                      sj.code, mu.scalar(0), mu.scalar(1), mj.scalar(0), mj.scalar(1),
-                      (R)(bj / bu), (R)(bu / bj), mu, mj, pr, ou, oj);
+    pass2_pair_sym<R, MomRec<R, true>, MomRec<R, true>, TV, XO>(
+        T, pair_vec<R>(su, sj), su.sigma, sj.sigma, su.occ, sj.occ, su.code, sj.code,
+        mu.scalar(0), mu.scalar(1), mj.scalar(0), mj.scalar(1), (R)(bj / bu), (R)(bu / bj), mu,
+        mj, pr, ou, oj);
     vu[0] = ou.gq[0]; vu[1] = ou.gq[1]; vu[2] = ou.gq[2]; vu[3] = ou.gs; vu[4] = ou.gx;
     vj[0] = oj.gq[0]; vj[1] = oj.gq[1]; vj[2] = oj.gq[2]; vj[3] = oj.gs; vj[4] = oj.gx;
   }
   // slot records: (gq, gs) as one 4-vector, gx in its own array
-  st_rec4(a.pbuf + 4 * (size_t)p, vu);
+  if (!XO) st_rec4(a.pbuf + 4 * (size_t)p, vu);
   a.pgx[p] = vu[4];
   if (r >= 0) {
-    st_rec4(a.pbuf + 4 * (size_t)r, vj);
+    if (!XO) st_rec4(a.pbuf + 4 * (size_t)r, vj);
     a.pgx[r] = vj[4];
   }
 }
@@ -804,6 +818,12 @@ __global__ void __launch_bounds__(TPB, MB)
 pass2u_pair_kernel(const EvalArgs<R> a) {
   // one copy of the body for every trip: a site or pair gives the same bits
   // whichever trip of whichever grid computes it
+  if (a.x_only) {
+#pragma unroll 1
+    for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
+      pass2u_one<R, RadialView<R>, true>(a, a.T, t);
+    return;
+  }
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
     pass2u_one(a, a.T, t);
@@ -819,6 +839,12 @@ pass2u_pair_smem_kernel(const EvalArgs<R> a) {
   bool ok;
   const auto T = kernel_view<R, true>(a, ok);
   if (!ok) return;  // the staging copy timed out (flagged)
+  if (a.x_only) {
+#pragma unroll 1
+    for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
+      pass2u_one<R, decltype(T), true>(a, T, t);
+    return;
+  }
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB)
     pass2u_one(a, T, t);
@@ -844,6 +870,19 @@ pass2u_site_kernel(const EvalArgs<R> a) {
       continue;
     }
     Acc<R> acc[5];
+    if (a.x_only) {  // the occupancy gradients alone; R_q and R_sigma are 0
+      for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) acc[4].add(ld_ro(a.pgx + p));
+      const double tx = warp_sum(acc[4].get());
+      if (lane == 0) {
+        double gs = 0.0, gx = tx;
+        residual_epilogue(a.pos[u].w, xu, a.code[u], xbu.y, a.gamma[u], a.selfx[u], gs, gx);
+        a.Rq[3 * u] = a.Rq[3 * u + 1] = a.Rq[3 * u + 2] = 0.0;
+        a.Rs[u] = 0.0;
+        a.Rx[u] = gx;
+        if (!finite(gx)) atomicOr(a.err, 1 << kErrBitNonFinite);
+      }
+      continue;
+    }
     for (int p = a.offs[u] + lane; p < a.offs[u + 1]; p += 32) {
       R v[4];
       ld4(a.pbuf + 4 * (size_t)p, v);
@@ -955,8 +994,8 @@ void go1(const EvalArgs<R> &a, cudaStream_t st, bool pers, bool und, cudaEvent_t
   const int n_groups = (a.n_real + 32 / G - 1) / (32 / G);
   if (und) {
     auto kp = pass1u_pair_kernel<R, 128>;
-    int g = nblocks(a.n_own, 128);
-    if (pers) {
+    int g = a.recs_ready ? 0 : nblocks(a.n_own, 128);  // kept sums: no pair-rule kernel
+    if (pers && g > 0) {
       int dev = 0, sms = 0, per = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -53,6 +53,15 @@ template <class R> struct EvalArgs {
   double *rho, *V0, *S0, *selfx;  // [real]
   double *Rq, *Rs, *Rx;           // [3*real], [real], [real]
   int *err;
+  // Occupancy gradients only (the master equation's chemical potentials):
+  // with the undirected variants, pass 2 forms R_x alone and writes R_q and
+  // R_sigma as 0, and the pair-rule kernel forms only the four pass-1 sums
+  // of each pair (every pair, occupied or not: they do not depend on the
+  // occupancies).  recs_ready: those sums are already in prec1 from an
+  // earlier launch at the same positions and widths, so pass 1 skips the
+  // pair-rule kernel.  Both are ignored by the directed variants.
+  int x_only = 0;
+  int recs_ready = 0;
   // undirected pass 2 (optional; nullptr / 0 when absent)
   const int *rev = nullptr;    // reverse slot of each real-site slot, -1 if none
   const int *own_p = nullptr;  // owned slots

@@ -306,6 +306,38 @@ int ensure_pbuf(btam_system *s, size_t elem) {
 
 }  // namespace
 
+// One evaluation enqueued on the system's stream.  x_only: the occupancy
+// gradients alone with the undirected variants (EvalArgs::x_only); recs_ready:
+// the pair-rule kernel's four pass-1 sums are still those of the current
+// positions and widths (an earlier x_only evaluation in the same run of
+// master-equation steps made them), so pass 1 skips that kernel.  A served
+// job's evaluation goes to the server's batcher in full.
+static int enqueue_eval(btam_system *s, int precision, bool x_only, bool recs_ready) {
+  if (!s) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  if (s->batcher) return batcher_eval(s, precision);  // a served job: one shared launch
+  const size_t nm = (size_t)s->n_real * kMomStride;
+  if (precision == BTAM_FP64) {
+    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
+    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
+    a.x_only = x_only;
+    a.recs_ready = x_only && recs_ready;
+    BTAM_TRY(launch_pass1(a, s->st, s->variant1[0], s->variant2[0]));
+    BTAM_TRY(launch_pass2(a, s->st, s->variant2[0]));
+  } else {
+    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
+    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
+    a.x_only = x_only;
+    a.recs_ready = x_only && recs_ready;
+    BTAM_TRY(launch_pass1(a, s->st, s->variant1[1], s->variant2[1]));
+    BTAM_TRY(launch_pass2(a, s->st, s->variant2[1]));
+  }
+  BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->totals + 4,
+                          s->st));
+  return BTAM_OK;
+}
+
 // Table views for the allocation-free entry point (noalloc.cu).
 namespace btam {
 // One pool per device, created on first use and kept for the life of the
@@ -841,25 +873,11 @@ int btam_ghosts_copy(const btam_system *s, double *q, int *owner, int *image) {
 }
 
 int btam_mf_eval_async(btam_system *s, int precision) {
-  if (!s) return BTAM_ERR_ARG;
-  if (!s->built) return BTAM_ERR_NOT_BUILT;
-  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
-  if (s->batcher) return batcher_eval(s, precision);  // a served job: one shared launch
-  const size_t nm = (size_t)s->n_real * kMomStride;
-  if (precision == BTAM_FP64) {
-    if (!s->mom64) BTAM_TRY(dalloc(s->mom64, s->st, nm));
-    EvalArgs<double> a = eval_args<double>(s, s->mom64, s->T->r64);
-    BTAM_TRY(launch_pass1(a, s->st, s->variant1[0], s->variant2[0]));
-    BTAM_TRY(launch_pass2(a, s->st, s->variant2[0]));
-  } else {
-    if (!s->mom32) BTAM_TRY(dalloc(s->mom32, s->st, nm));
-    EvalArgs<float> a = eval_args<float>(s, s->mom32, s->T->r32);
-    BTAM_TRY(launch_pass1(a, s->st, s->variant1[1], s->variant2[1]));
-    BTAM_TRY(launch_pass2(a, s->st, s->variant2[1]));
-  }
-  BTAM_TRY(launch_totals(s->n_real, s->V0, s->S0, s->Rq, s->Rs, s->Rx, s->totals, s->totals + 4,
-                          s->st));
-  return BTAM_OK;
+  return enqueue_eval(s, precision, false, false);
+}
+
+int btam_mf_eval_x(btam_system *s, int precision) {
+  return enqueue_eval(s, precision, true, false);
 }
 
 }  // extern "C"
@@ -1647,7 +1665,9 @@ int btam_dmd_step(btam_system *s, int precision, int nsteps, const double *param
   BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
   const DmdArgs a = dmd_args(s);
   for (int k = 0; k < nsteps; ++k) {
-    int st = btam_mf_eval_async(s, precision);  // chemical potentials at the current x
+    // chemical potentials at the current x; positions and widths do not
+    // move during the steps, so the pair-rule sums of the first are kept
+    int st = enqueue_eval(s, precision, true, k > 0);
     if (st != BTAM_OK) return st;
     BTAM_TRY(dmd_step(a, prm, s->st));
     if ((st = dmd_refresh_images(s)) != BTAM_OK) return st;
@@ -1671,9 +1691,11 @@ int btam_dmd_step_ctl(btam_system *s, int precision, int nsteps, const double *p
   BTAM_TRY(copy_sync(&clip0, s->dctl + 2, sizeof(clip0), cudaMemcpyDeviceToHost, s->st));
   long long subs = 0, split = 0;
   double worst = 0.0;
+  bool recs = false;  // the pair-rule sums of this call's positions are made
   for (int k = 0; k < nsteps; ++k) {
-    int st = btam_mf_eval_async(s, precision);
+    int st = enqueue_eval(s, precision, true, recs);
     if (st != BTAM_OK) return st;
+    recs = true;
     BTAM_TRY(dmd_prepare(a, s->st));
     BTAM_TRY(dmd_control(a, prm, max_dx, s->st));
     unsigned long long bits[2] = {0, 0};
@@ -1688,7 +1710,7 @@ int btam_dmd_step_ctl(btam_system *s, int precision, int nsteps, const double *p
     sub.dt = prm.dt / (double)m;
     for (long long j = 0; j < m; ++j) {
       if (j > 0) {  // fresh chemical potentials for every later sub-step
-        if ((st = btam_mf_eval_async(s, precision)) != BTAM_OK) return st;
+        if ((st = enqueue_eval(s, precision, true, true)) != BTAM_OK) return st;
         BTAM_TRY(dmd_prepare(a, s->st));
       }
       BTAM_TRY(dmd_apply(a, sub, s->st));

@@ -268,6 +268,14 @@ __device__ __forceinline__ double dmd_move(const double2 *xb, const double *mu,
   return prm.dt * J;
 }
 
+// A move in quanta, rounded to nearest from a value first held within
+// +-4e18 (far outside any room, which is at most max_x in quanta), so that a
+// move whose quanta overflow 64 bits (an empty site's chemical potential
+// against an occupied one) is cut to the room like any other large move.
+__device__ __forceinline__ long long dmd_quanta(double dlt) {
+  return llrint(fmin(fmax(dlt * kDmdInvQuantum, -4e18), 4e18));
+}
+
 // The room of edge (i, o) in quanta under the degree split: a move from i
 // to o of at most hi, from o to i of at most -lo (lo <= 0).
 __device__ __forceinline__ void dmd_room(const long long *X, const int *deg, int i, int o,
@@ -292,7 +300,7 @@ __global__ void dmd_flux_kernel(int n, const double2 *xb, const int *doffs, cons
     if (o <= i || !active[o]) continue;  // each undirected edge once, from its lower end
     const double dlt = dmd_move(xb, mu, X0, i, o, prm);  // occupancy moved from i to o
     if (fabs(dlt) < prm.min_dx) continue;
-    long long q = llrint(dlt * kDmdInvQuantum);
+    long long q = dmd_quanta(dlt);
     long long hi, lo;
     dmd_room(X0, deg, i, o, xmax, hi, lo);
     // a move cut to a nonzero room is counted; a zero room (empty giver,
@@ -325,7 +333,7 @@ __global__ void dmd_control_kernel(int n, const double2 *xb, const int *doffs, c
       if (fabs(dlt) < prm.min_dx) continue;
       dx = __dsub_rn(dx, dlt);  // no contraction: the oracle rounds each term
       if (o < i) continue;  // the room of each edge once
-      const long long q = llrint(dlt * kDmdInvQuantum);
+      const long long q = dmd_quanta(dlt);
       long long hi, lo;
       dmd_room(X, deg, i, o, xmax, hi, lo);
       if (q > hi && hi > 0) ratio = fmax(ratio, (double)q / (double)hi);

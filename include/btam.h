@@ -205,6 +205,17 @@ int btam_mf_eval_state(btam_system *s, int precision, const double *q, const dou
  * outputs resident on the device; results stay in the system's buffers
  * (btam_results_copy reads them).  Does not synchronise. */
 int btam_mf_eval_async(btam_system *s, int precision);
+/* The occupancy gradients alone, enqueued like btam_mf_eval_async: rho-bar,
+ * V0, S0 and R_x of the state (rho-bar, V0, S0 bit for bit the full
+ * evaluation's, R_x to its last bits: a multiply-add of the shared
+ * expressions may fuse differently without the derivative terms), with
+ * R_q and R_sigma written as 0; evaluate_DV0_i_Dxi_u_adp_MgHx
+ * (MgHx-mf-V-bulk.cpp:2102-2325) assembled as in btam_mf_eval.  These are
+ * the master equation's chemical potentials; btam_dmd_step takes them this
+ * way and keeps the pair rule's position-only sums between its steps.  The
+ * directed kernel variants and a served job's evaluations compute the full
+ * residuals instead. */
+int btam_mf_eval_x(btam_system *s, int precision);
 int btam_results_copy(btam_system *s, double *rho, double *V0, double *S0,
                       double *Rq, double *Rs, double *Rx, double *totals);
 /* Waits for the system's stream and returns the first error it raised. */
@@ -442,7 +453,9 @@ int btam_relax_newton(btam_system *s, double tol, int max_newton, int max_cg,
  * list_of_diffusive_neighs, Neighbors.cpp:139-275).  Setup builds the H-H
  * graph (pairs within 2.6 A, at most 50 per site) and carries every H
  * occupancy as an integer number of 2^-50 quanta from then on.  A step:
- * evaluates the residuals (precision), forms the chemical potential
+ * evaluates the occupancy gradients (btam_mf_eval_x; after the steps the
+ * system's stored R_q and R_sigma are 0 until the next full evaluation),
+ * forms the chemical potential
  *   mu_i = R_x(i) + [x_i<0.9999] gamma_i/beta_i     (x_i >= 5e-4)
  *   mu_i = -(3/(2x) + 1/(1-x))/beta_i, x = max(x_i, 1e-12)   (emptier sites)
  * of every H site that is diffusively active (x_i plus the x of its H

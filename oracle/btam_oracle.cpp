@@ -1595,6 +1595,11 @@ static void orc_dmd_room(const long long *X, const std::vector<long long> &deg, 
   lo = -(out_o < in_i ? out_o : in_i);
 }
 
+// A move in quanta (v = the move times 2^50), rounded to nearest from a
+// value first held within +-4e18, so that a move whose quanta overflow 64
+// bits is cut to the edge's room like any other large move.
+long long orc_dmd_quanta(double v) { return llrint(std::fmin(std::fmax(v, -4e18), 4e18)); }
+
 void orc_dmd_control(int n, const int *code_all, const int *owner, const double *x_all,
                      const double *beta, const double *mu, const int *moffs, const int *midx,
                      const int *doffs, const int *didx, const double *params, double max_dx,
@@ -1620,7 +1625,7 @@ void orc_dmd_control(int n, const int *code_all, const int *owner, const double 
       if (std::fabs(dlt) < min_dx) continue;
       dx -= dlt;
       if (o < i) continue;
-      long long qn = llrint(dlt * invq), hi, lo;
+      long long qn = orc_dmd_quanta(dlt * invq), hi, lo;
       orc_dmd_room(X, deg, i, o, xmax, hi, lo);
       if (qn > hi && hi > 0) ratio = std::max(ratio, (double)qn / (double)hi);
       if (qn < lo && lo < 0) ratio = std::max(ratio, (double)qn / (double)lo);
@@ -1652,7 +1657,7 @@ void orc_dmd_update(int n, const int *code_all, const int *owner, const double *
       double J = Df / (dr * dr) * bm * xm * (1.0 - xm) * (mu[i] - mu[o]);
       double dlt = dt * J;
       if (std::fabs(dlt) < min_dx) continue;
-      long long qn = llrint(dlt * invq), hi, lo;
+      long long qn = orc_dmd_quanta(dlt * invq), hi, lo;
       orc_dmd_room(X0.data(), deg, i, o, xmax, hi, lo);
       if (clipped && ((qn > hi && hi > 0) || (qn < lo && lo < 0))) ++*clipped;
       qn = qn > hi ? hi : (qn < lo ? lo : qn);
