@@ -824,51 +824,58 @@ __device__ __forceinline__ void dn_all(const Leg &L1, const Leg &L2, const doubl
   }
 }
 
-// dmq of slot S's three coordinates: for each, the five-point second
+// dmq of every slot's three coordinates: for each, the five-point second
 // difference (step 0.01) of all slots' gradients, times sigma_S^2 / 2, added
-// to acc (g0: the gradients at the mean).  g0 and acc are the lane's
-// shared-memory scratch.
-template <int S>
-__device__ __forceinline__ void dmq_slot(const RadialView<double> &T, int pk1, int pk2,
-                                         const double (&q)[9], const double *legs,
-                                         double c1, double c2, double c2s, const double *g0,
-                                         double *acc) {
+// to acc (g0: the gradients at the mean).  g0, acc and the legs at the mean
+// are the lane's shared-memory scratch.  One body serves the three slots (a
+// moved slot recomputes the legs it ends, the others come from the
+// scratch), which keeps the unrolled differences small enough for the
+// instruction cache.
+__device__ __forceinline__ void dmq_slots(const RadialView<double> &T, int pk1, int pk2,
+                                          const double (&q)[9], const double (&sig)[3],
+                                          const double *legs, double c1, double c2,
+                                          const double *g0, double *acc) {
 #pragma unroll 1
-  for (int al = 0; al < 3; ++al) {
-    const double dr = 0.01;
-    const double x0 = al == 0 ? q[3 * S] : al == 1 ? q[3 * S + 1] : q[3 * S + 2];
-    double t[18];
+  for (int S = 0; S < 3; ++S) {
+    const double c2s = sqz(S == 0 ? sig[0] : S == 1 ? sig[1] : sig[2]) / 2.0;
+    double base[3];
 #pragma unroll
-    for (int w = 0; w < 4; ++w) {
-      const double v = w == 0 ? x0 + dr * 2 : w == 1 ? x0 + dr : w == 2 ? x0 - dr : x0 - dr * 2;
-      double pm[3];
+    for (int a = 0; a < 3; ++a) base[a] = S == 0 ? q[a] : S == 1 ? q[3 + a] : q[6 + a];
+#pragma unroll 1
+    for (int al = 0; al < 3; ++al) {
+      const double dr = 0.01;
+      const double x0 = al == 0 ? base[0] : al == 1 ? base[1] : base[2];
+      double t[18];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) pm[a] = a == al ? v : q[3 * S + a];
-      // the five-point combination -gpp + 16 gp - 30 g0 + 16 gm - gmm,
-      // formed in that order as the points arrive (pp, p, m, mm)
-      auto step = [&](int e, double g) {
-        if (w == 0) t[e] = -g;
-        else if (w == 1) t[e] = (t[e] + 16.0 * g) - 30.0 * g0[e];
-        else if (w == 2) t[e] = t[e] + 16.0 * g;
-        else t[e] = t[e] - g;
-      };
-      if (S == 0) {
+      for (int w = 0; w < 4; ++w) {
+        const double v = w == 0 ? x0 + dr * 2 : w == 1 ? x0 + dr : w == 2 ? x0 - dr
+                                                                          : x0 - dr * 2;
+        double pc[3], p1[3], p2[3];  // the three positions with slot S moved
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double m = a == al ? v : base[a];
+          pc[a] = S == 0 ? m : q[a];
+          p1[a] = S == 1 ? m : q[3 + a];
+          p2[a] = S == 2 ? m : q[6 + a];
+        }
+        // the five-point combination -gpp + 16 gp - 30 g0 + 16 gm - gmm,
+        // formed in that order as the points arrive (pp, p, m, mm)
+        auto step = [&](int e, double g) {
+          if (w == 0) t[e] = -g;
+          else if (w == 1) t[e] = (t[e] + 16.0 * g) - 30.0 * g0[e];
+          else if (w == 2) t[e] = t[e] + 16.0 * g;
+          else t[e] = t[e] - g;
+        };
         Leg M1, M2;
-        leg_of<true>(T, pk1, pm, q + 3, M1);
-        leg_of<true>(T, pk2, pm, q + 6, M2);
+        if (S != 2) leg_of<true>(T, pk1, pc, p1, M1);
+        else M1 = ld_leg(legs);
+        if (S != 1) leg_of<true>(T, pk2, pc, p2, M2);
+        else M2 = ld_leg(legs + 10);
         dq_all(M1, M2, c1, c2, step);
-      } else if (S == 1) {
-        Leg M1;
-        leg_of<true>(T, pk1, q, pm, M1);
-        dq_all(M1, ld_leg(legs + 10), c1, c2, step);
-      } else {
-        Leg M2;
-        leg_of<true>(T, pk2, q, pm, M2);
-        dq_all(ld_leg(legs), M2, c1, c2, step);
       }
-    }
 #pragma unroll
-    for (int e = 0; e < 18; ++e) acc[e] += c2s * (t[e] / (12.0 * dr * dr));
+      for (int e = 0; e < 18; ++e) acc[e] += c2s * (t[e] / (12.0 * dr * dr));
+    }
   }
 }
 
@@ -957,9 +964,7 @@ __device__ __forceinline__ void tri_all(const RadialView<double> &T, int rule, c
     double *g0 = sc, *acc = sc + 18;
     dq_all(ld_leg(legs), ld_leg(legs + 10), c1, c2,
            [&](int e, double g) { g0[e] = acc[e] = g; });
-    dmq_slot<0>(T, pk1, pk2, q, legs, c1, c2, sqz(sig[0]) / 2.0, g0, acc);
-    dmq_slot<1>(T, pk1, pk2, q, legs, c1, c2, sqz(sig[1]) / 2.0, g0, acc);
-    dmq_slot<2>(T, pk1, pk2, q, legs, c1, c2, sqz(sig[2]) / 2.0, g0, acc);
+    dmq_slots(T, pk1, pk2, q, sig, legs, c1, c2, g0, acc);
 #pragma unroll
     for (int d = 0; d < 3; ++d)
 #pragma unroll
