@@ -488,6 +488,19 @@ def bench_bulk_stretch(args, tables, cpu_budget_s=6.0):
            "status": info["status"], "ms_total": t * 1e3,
            "ms_per_residual": t * 1e3 / max(info["evaluations"], 1),
            "timing": "host clock around the call (each residual ends in a 96-byte read)"}
+    # the solver the reference's main program configures for this relaxation:
+    # N-GMRES(m = 3) with the critical-point line search
+    S = btam.System(tables, sys_)
+    S.build_neighbors()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    Fg, ig = S.relax_stretch_ngmres(m=3, atol=1e-12, rtol=1e-10, max_iter=60)
+    tg = time.perf_counter() - t0
+    S.close()
+    out["ngmres_m3_cp"] = {"F": [float(f) for f in Fg], "iterations": ig["iterations"],
+                           "residual_evaluations": ig["evaluations"], "final_norm": ig["norm"],
+                           "status": ig["status"], "ms_total": tg * 1e3,
+                           "max_abs_F_vs_newton": float(np.max(np.abs(Fg - F)))}
     if not args.no_cpu:
         ref = pyoracle.reference(fast=True)
         kind = "reference"

@@ -86,6 +86,8 @@ _PROTOS = {
     "btam_mf_hessian_multipole": (ctypes.c_int, [_V, ctypes.c_int, _D]),
     "btam_relax_stretch": (ctypes.c_int, [_V, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                           _D, _D]),
+    "btam_relax_stretch_ngmres": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
+                                                 ctypes.c_double, ctypes.c_int, _D, _D]),
     "btam_relax_stretch_mf": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_int, _D, _D]),
     "btam_mf_stress": (ctypes.c_int, [_V, ctypes.c_int, _D, _D]),
@@ -614,6 +616,17 @@ class System:
         info = np.zeros(5)
         _check(lib().btam_relax_stretch(self.handle, atol, rtol, max_iter, _d(F), _d(info)),
                "btam_relax_stretch")
+        return F, dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
+                       status=int(info[3]), volume=info[4])
+
+    def relax_stretch_ngmres(self, m=3, atol=1e-12, rtol=1e-10, max_iter=50,
+                             F0=(1.0, 1.0, 1.0)):
+        """The same relaxation with N-GMRES(m) and the critical-point line
+        search, the reference's configured solver.  Returns (F, info)."""
+        F = np.ascontiguousarray(F0, np.float64).copy()
+        info = np.zeros(5)
+        _check(lib().btam_relax_stretch_ngmres(self.handle, int(m), atol, rtol, max_iter, _d(F),
+                                               _d(info)), "btam_relax_stretch_ngmres")
         return F, dict(norm=info[0], iterations=int(info[1]), evaluations=int(info[2]),
                        status=int(info[3]), volume=info[4])
 

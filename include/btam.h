@@ -400,6 +400,15 @@ int btam_stretch_apply(btam_system *s, const double F[3]);
  * here, and any solver that converges finds the same F. */
 int btam_relax_stretch(btam_system *s, double atol, double rtol, int max_iter, double F[3],
                        double *info);
+/* The same relaxation with the solver the reference's main program
+ * configures for it (main-BT-AM.cpp:64-67: -minV_dF_snes_type ngmres,
+ * -minV_dF_snes_ngmres_m 3, -minV_dF_snes_linesearch_type cp): N-GMRES(m)
+ * with the critical-point line search, PETSc SNESNGMRES's difference
+ * selection and restart with their defaults; three residual evaluations per
+ * iteration.  m = 1..3 (the stretch has three unknowns); info as
+ * btam_relax_stretch. */
+int btam_relax_stretch_ngmres(btam_system *s, int m, double atol, double rtol, int max_iter,
+                              double F[3], double *info);
 /* The same relaxation on the mean-field stress (btam_mf_stress: the
  * reference's evaluate_DV0_i_dF_bulk_MgHx, whose table slot
  * evaluate_DV0_i_DF no reference solver calls) at fixed sigma and x, in

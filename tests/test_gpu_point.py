@@ -138,6 +138,38 @@ def test_relax_stretch_zeroes_reference_stress(gpu_tables, oracle, name):
     assert np.max(np.abs(Yd)) <= 1e-11
 
 
+@pytest.mark.parametrize("name", ["x5cube", "ortho_mgh"])
+@pytest.mark.parametrize("m", [3, 2, 1])
+def test_relax_stretch_ngmres_reaches_the_same_stretch(gpu_tables, oracle, name, m):
+    """The reference's configured solver (N-GMRES(m = 3) with the
+    critical-point line search; m = 1, 2 as well) converges to |Y| <= 1e-12
+    at the stretch the Newton solve finds (1e-9), three residual evaluations
+    per iteration, and the oracle's residual vanishes there."""
+    g = load(name)
+    s = system_of(g)
+    A = btam.System(gpu_tables, s)
+    A.build_neighbors()
+    Fn, _ = A.relax_stretch(atol=1e-12, rtol=1e-10, max_iter=20)
+    B = btam.System(gpu_tables, s)
+    B.build_neighbors()
+    F, info = B.relax_stretch_ngmres(m=m, atol=1e-12, rtol=1e-10, max_iter=60)
+    assert info["status"] == 1 and info["norm"] <= 1e-12, info
+    assert info["evaluations"] <= 1 + 3 * info["iterations"], info
+    assert np.max(np.abs(F - Fn)) <= 1e-9, (F, Fn)
+    q, _, _ = B.get_state()
+    assert np.array_equal(q, s["q"] * F)
+    n = len(g["x"])
+    owner = g["owner"]
+    full = {"q": np.ascontiguousarray(g["q_all"] * F), "x": np.ascontiguousarray(g["x"][owner]),
+            "species": np.ascontiguousarray(g["species"][owner].astype(np.int32))}
+    real = np.arange(n, dtype=np.int32)
+    rho = oracle.rho_nmf(full, g["offs"], g["idx"], real)
+    W = oracle.pt_DV_dF(full, g["q_all"], rho[owner], g["offs"], g["idx"], real)
+    vol = abs(np.linalg.det(s["cell"].reshape(3, 3)))
+    Y = np.array([W[:, a, a].sum() for a in range(3)]) / vol
+    assert np.max(np.abs(Y)) <= 1e-9, Y
+
+
 def test_relax_stretch_rejections(gpu_tables):
     g = load("sphere")
     S = btam.System(gpu_tables, system_of(g))
