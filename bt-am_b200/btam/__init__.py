@@ -57,6 +57,8 @@ _PROTOS = {
                                       ctypes.c_int, _D, _D, _I, _D]),
     "btam_term_quadrature": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                             ctypes.c_int, ctypes.c_int, _D, _D, _D, _I, _D]),
+    "btam_term_quadrature5": (ctypes.c_int, [_V, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                             ctypes.c_int, _D, _D, _D, _I, _D]),
     "btam_system_create": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _I, _D, _D, _D, _D,
                                           _I, ctypes.POINTER(_V)]),
     "btam_system_destroy": (None, [_V]),
@@ -285,6 +287,22 @@ class Tables:
         _check(lib().btam_term_quadrature(self.handle, int(term), int(mode), int(slot),
                                           int(bool(coincident)), n, _d(q), _d(sg), _d(x),
                                           _i(sp), _d(out)), "btam_term_quadrature")
+        return out
+
+    def term_quadrature5(self, term, mode, direction, q, sigma, x, species):
+        """The 5th-degree rule over the pair measure of a pair term: mode 0
+        the average of F, 1 of dF_dq(direction), 2 of d2F_dq2(direction).
+        q (n, 6), sigma, x, species (n, 2); returns (n, 9)."""
+        n = len(q)
+        qq = np.zeros((n, 9))
+        qq[:, :6] = np.asarray(q, np.float64).reshape(n, 6)
+        pad = lambda v, dt: np.ascontiguousarray(
+            np.pad(np.asarray(v, dt).reshape(n, 2), ((0, 0), (0, 1))))
+        sg, x, sp = pad(sigma, np.float64), pad(x, np.float64), pad(species, np.int32)
+        out = np.zeros((n, 9))
+        _check(lib().btam_term_quadrature5(self.handle, int(term), int(mode), int(direction), n,
+                                           _d(qq), _d(sg), _d(x), _i(sp), _d(out)),
+               "btam_term_quadrature5")
         return out
 
     def close(self):

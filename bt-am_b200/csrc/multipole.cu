@@ -1600,6 +1600,60 @@ __global__ void __launch_bounds__(128) term_quad_kernel(TermArgs a) {
   for (int e = 0; e < 9; ++e) a.out[9 * (size_t)k + e] = e < 3 ? out[e] : 0.0;
 }
 
+// The reference's 5th-degree rule over the pair measure (Quadrature-
+// Hermitian-5th.cpp:31-432; no caller in the reference selects it) of a
+// pair term: mode 0 the average of F, 1 of dF_dq(dir), 2 of d2F_dq2(dir).
+// 44 points, the 22 of its table and their negatives: z = (1, ..., 1)
+// (weight 1/128), sqrt(2) e_k (k = 0..5; 1/16), (1, ..., 1) with entries a < b
+// set to -1 (1/128); q = mean +- sqrt(2) sigma_s z, each value weighted
+// W c0 with c0 = pi^(3/2), the sum scaled by pi^(-3/2), in that order.
+__global__ void __launch_bounds__(128) term_quad5_kernel(TermArgs a) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= a.n) return;
+  constexpr double kPi = 3.14159265358979323846;
+  double q[9], n[3], sig[2];
+  int c[3];
+  for (int e = 0; e < 9; ++e) q[e] = e < 6 ? a.q[9 * (size_t)k + e] : 0.0;
+  for (int s = 0; s < 3; ++s) {
+    n[s] = s < 2 ? a.x[3 * (size_t)k + s] : 0.0;
+    c[s] = s < 2 ? a.code[3 * (size_t)k + s] : 0;
+  }
+  sig[0] = a.sigma[3 * (size_t)k];
+  sig[1] = a.sigma[3 * (size_t)k + 1];
+  const double c0 = pow(sqrt(kPi), 6.0 / 2.0);
+  const int nv = a.mode == 0 ? 1 : a.mode == 1 ? 3 : 9;
+  double out[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int sg = 0; sg < 2; ++sg)
+    for (int gp = 0; gp < 22; ++gp) {
+      // the point's entry z_m (m = 3 s + axis) and weight
+      int pa = -1, pb = -1;
+      if (gp >= 7) {  // pairs a < b in order
+        int t = gp - 7;
+        for (pa = 0; t >= 5 - pa; ++pa) t -= 5 - pa;
+        pb = pa + 1 + t;
+      }
+      const double W = (gp >= 1 && gp <= 6) ? 0.0625 : 0.0078125;
+      double ql[9];
+      for (int e = 0; e < 9; ++e) ql[e] = 0.0;
+      for (int al = 0; al < 3; ++al)
+        for (int s = 0; s < 2; ++s) {
+          const int m = 3 * s + al;
+          const double z = gp == 0 ? 1.0
+                         : gp <= 6 ? (m == gp - 1 ? kSqrt2d : 0.0)
+                                   : ((m == pa || m == pb) ? -1.0 : 1.0);
+          const double off = kSqrt2d * sig[s] * z;
+          ql[m] = sg == 0 ? q[m] + off : q[m] - off;
+        }
+      double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      if (a.mode == 0) v[0] = term_F(a.T, a.term, c, n, ql);
+      else if (a.mode == 1) term_dq(a.T, a.term, c, n, a.dir, ql, v);
+      else term_d2(a.T, a.term, c, n, a.dir, ql, v);
+      for (int e = 0; e < nv; ++e) out[e] += v[e] * W * c0;
+    }
+  const double sc = pow(1.0 / sqrt(kPi), 6.0 / 2.0);
+  for (int e = 0; e < 9; ++e) a.out[9 * (size_t)k + e] = e < nv ? out[e] * sc : 0.0;
+}
+
 }  // namespace
 }  // namespace btam
 
@@ -1921,8 +1975,9 @@ namespace {
 
 int term_launch(const btam_tables *t, bool quad, int term, int fn_or_mode, int dir, int slot_ns,
                 int coincident, int n, const double *q, const double *sigma, const double *x,
-                const int *species, double *out) {
-  if (!t || n < 0 || !q || !x || !species || !out || (quad && !sigma)) return BTAM_ERR_ARG;
+                const int *species, double *out, bool fifth = false) {
+  if (!t || n < 0 || !q || !x || !species || !out || ((quad || fifth) && !sigma))
+    return BTAM_ERR_ARG;
   if (term < 0 || term > 3) return BTAM_ERR_ARG;
   const int ns = term < 2 ? 2 : 3;
   if (slot_ns != ns) return BTAM_ERR_ARG;
@@ -1950,7 +2005,7 @@ int term_launch(const btam_tables *t, bool quad, int term, int fn_or_mode, int d
     e = cudaMemcpyAsync(dq, q, 9 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(dx, x, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
-  if (e == cudaSuccess && quad)
+  if (e == cudaSuccess && (quad || fifth))
     e = cudaMemcpyAsync(ds, sigma, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(dc, code.data(), 3 * (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st);
@@ -1959,7 +2014,7 @@ int term_launch(const btam_tables *t, bool quad, int term, int fn_or_mode, int d
     a.T = t->r64;
     a.term = term;
     a.fn = quad ? 0 : fn_or_mode;
-    a.mode = quad ? fn_or_mode : 0;
+    a.mode = (quad || fifth) ? fn_or_mode : 0;
     a.dir = dir;
     a.ns = ns;
     a.n = n;
@@ -1970,7 +2025,8 @@ int term_launch(const btam_tables *t, bool quad, int term, int fn_or_mode, int d
     a.code = dc;
     a.out = dout;
     const int g = (n + 127) / 128;
-    if (quad) term_quad_kernel<<<g, 128, 0, st>>>(a);
+    if (fifth) term_quad5_kernel<<<g, 128, 0, st>>>(a);
+    else if (quad) term_quad_kernel<<<g, 128, 0, st>>>(a);
     else term_eval_kernel<<<g, 128, 0, st>>>(a);
     e = cudaGetLastError();
   }
@@ -1993,6 +2049,16 @@ int btam_term_eval(const btam_tables *t, int term, int fn, int direction, int n,
                    const double *q, const double *x, const int *species, double *out) {
   return term_launch(t, false, term, fn, direction, term < 2 ? 2 : 3, 0, n, q, nullptr, x,
                      species, out);
+}
+
+int btam_term_quadrature5(const btam_tables *t, int term, int mode, int direction, int n,
+                          const double *q, const double *sigma, const double *x,
+                          const int *species, double *out) {
+  if (term < 0 || term > 1 || mode < 0 || mode > 2) return BTAM_ERR_ARG;
+  if (mode > 0 && (direction < 0 || direction >= (mode == 1 ? 2 : 4))) return BTAM_ERR_ARG;
+  // the term evaluator's argument checks with the slot function of the mode
+  return term_launch(t, false, term, mode == 0 ? 0 : mode == 1 ? 1 : 2, mode == 0 ? 0 : direction,
+                     2, 0, n, q, sigma, x, species, out, true);
 }
 
 int btam_term_quadrature(const btam_tables *t, int term, int mode, int slot, int coincident,

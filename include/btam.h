@@ -133,6 +133,17 @@ int btam_term_eval(const btam_tables *t, int term, int fn, int direction, int n,
 int btam_term_quadrature(const btam_tables *t, int term, int mode, int slot, int coincident,
                          int n, const double *q, const double *sigma, const double *x,
                          const int *species, double *out);
+/* The reference's 5th-degree rule over the pair measure
+ * (Quadrature-Hermitian-5th.cpp:31-432: moment_1th_Vij_gaussian_measure_5th,
+ * moment_1th_grad_f_ and moment_1th_hess_f_gaussian_measure_5th_6d) of a
+ * pair term (0 rho_ij, 1 V_pair_ij) for n geometries: mode 0 the average of
+ * F, 1 of dF_dq(direction), 2 of d2F_dq2(direction).  q: 9 per geometry (6
+ * used), sigma, x, species: 3 per geometry (2 used); out: 9 per geometry,
+ * the 1, 3 or 9 values first.  No caller in the reference selects this rule
+ * (its integrator switch offers the degree-3 and multipole rules only). */
+int btam_term_quadrature5(const btam_tables *t, int term, int mode, int direction, int n,
+                          const double *q, const double *sigma, const double *x,
+                          const int *species, double *out);
 
 /* Replaces read_dump_information + init_DMD_simulation (dump-input.cpp:
  * 51-214, Atom.cpp:80-431): one system of n sites with its DMSwarm fields

@@ -1667,6 +1667,59 @@ void orc_dmd_update(int n, const int *code_all, const int *owner, const double *
   }
 }
 
+// The 5th-degree rule over the pair measure (Quadrature-Hermitian-5th.cpp:
+// 31-432) of pair term `term` (0 rho, 1 pair): mode 0 the average of F,
+// 1 of dF_dq(direction), 2 of d2F_dq2(direction) (a pair's blocks: 0 and 3
+// the Hessian H of the radial term, 1 and 2 -H).  44 points, the 22 of the
+// table and their negatives: z = (1, ..., 1) with weight 1/128, sqrt(2)
+// e_k (k = 0..5) with weight 1/16, and (1, ..., 1) with two entries -1
+// (pairs a < b in order) with weight 1/128; q = mean +- sqrt(2) sigma_s z
+// (sigma of the site of each coordinate); each value weighted W c0,
+// c0 = pi^(3/2), the sum scaled by pi^(-3/2).
+int orc_quad5(int term, int mode, int direction, const double *q, const double *sigma,
+              const double *x, const int *spc, double *out) {
+  if (term < 0 || term > 1 || mode < 0 || mode > 2) return 1;
+  const Term &t = term == 0 ? kRho : kPair;
+  const double s2 = 1.4142135623730951, PI = 3.14159265358979323846;
+  double z[22][6], W[22];
+  for (int k = 0; k < 6; ++k) z[0][k] = 1.0;
+  W[0] = 0.0078125;
+  for (int g = 1; g <= 6; ++g) {
+    for (int k = 0; k < 6; ++k) z[g][k] = k == g - 1 ? s2 : 0.0;
+    W[g] = 0.0625;
+  }
+  int g = 7;
+  for (int a = 0; a < 6; ++a)
+    for (int b = a + 1; b < 6; ++b, ++g) {
+      for (int k = 0; k < 6; ++k) z[g][k] = (k == a || k == b) ? -1.0 : 1.0;
+      W[g] = 0.0078125;
+    }
+  const double c0 = std::pow(std::sqrt(PI), 6.0 / 2.0);
+  const int nv = mode == 0 ? 1 : mode == 1 ? 3 : 9;
+  for (int e = 0; e < 9; ++e) out[e] = 0.0;
+  for (int sg = 0; sg < 2; ++sg)
+    for (int gp = 0; gp < 22; ++gp) {
+      double ql[6], v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int a = 0; a < 3; ++a)
+        for (int s = 0; s < 2; ++s) {
+          const double off = s2 * sigma[s] * z[gp][s * 3 + a];
+          ql[s * 3 + a] = sg == 0 ? q[s * 3 + a] + off : q[s * 3 + a] - off;
+        }
+      if (mode == 0) {
+        v[0] = t.F(x, ql, spc);
+      } else if (mode == 1) {
+        t.dq(direction, v, x, ql, spc);
+      } else {
+        term_d2(term, 0, x, ql, spc, v);
+        if (direction == 1 || direction == 2)
+          for (int e = 0; e < 9; ++e) v[e] = -v[e];
+      }
+      for (int e = 0; e < nv; ++e) out[e] += v[e] * W[gp] * c0;
+    }
+  for (int e = 0; e < nv; ++e) out[e] = out[e] * std::pow(1.0 / std::sqrt(PI), 6.0 / 2.0);
+  return 0;
+}
+
 // One slot of the reference's per-term table (potential_function,
 // Macros.hpp:252-278) at one geometry: fn 0 F, 1 dF_dq, 2 d2F_dq2 (the
 // diagonal blocks a (ns + 1) only; other blocks return 1), 3 dF_dq_FD

@@ -56,6 +56,10 @@ int orc_quadrature(int term, int mode, int slot, int nsites, int coincident,
  * diagonal Hessian blocks, 3 dF_dq_FD, 4 d2F_dq2_FD, 5 dF_dn); 9 outputs. */
 int orc_term_eval(int term, int fn, int dir, int ns, const double *q, const double *x,
                   const int *spc, double *out);
+/* The 5th-degree rule over the pair measure of a pair term (mode 0 F, 1
+ * dF_dq, 2 d2F_dq2 of direction); 9 outputs. */
+int orc_quad5(int term, int mode, int direction, const double *q, const double *sigma,
+              const double *x, const int *spc, double *out);
 
 /* Literal per-site drivers over a system of n sites (real + ghost) with CSR
  * neighbour lists for every site. */

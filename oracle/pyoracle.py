@@ -87,6 +87,20 @@ class Lib:
             raise ValueError("term_eval")
         return out
 
+    def quad5(self, term, mode, direction, q, sigma, x, spc):
+        """The reference's 5th-degree rule over the pair measure of a pair
+        term (reference build: ref_quad5; oracle: orc_quad5); 9 values."""
+        q = np.ascontiguousarray(q, np.float64).ravel()
+        sigma = np.ascontiguousarray(sigma, np.float64)
+        x = np.ascontiguousarray(x, np.float64)
+        spc = np.ascontiguousarray(spc, np.int32)
+        out = np.zeros(9)
+        rc = self._f("quad5")(int(term), int(mode), int(direction), _d(q), _d(sigma), _d(x),
+                              _i(spc), _d(out))
+        if rc:
+            raise ValueError("quad5")
+        return out
+
     # --- per-site drivers over a system with CSR neighbour lists ----------
     def mf_rho(self, s, offs, idx, sites):
         sites = np.ascontiguousarray(sites, np.int32)

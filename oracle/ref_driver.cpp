@@ -24,6 +24,7 @@
 #include "ADP/density.hpp"
 #include "Macros.hpp"
 #include "Numerical/Quadrature-Hermitian-3th.hpp"
+#include "Numerical/Quadrature-Hermitian-5th.hpp"
 #include "Numerical/Quadrature-Measure.hpp"
 #include "Numerical/cubic-spline.hpp"
 
@@ -224,6 +225,37 @@ int ref_term_eval(int term, int fn, int direction, int nsites, const double *q,
   case 5: f.dF_dn(direction, out, x, q, sp); break;
   default: return 1;
   }
+  return 0;
+}
+
+// The reference's 5th-degree rule over the pair measure (Quadrature-Hermitian-
+// 5th.cpp:31-432) of a pair term (0 rho_ij, 1 V_pair_ij) at one geometry:
+// mode 0 moment_1th_Vij_gaussian_measure_5th (1 value),
+// 1 moment_1th_grad_f_gaussian_measure_5th_6d (dF_dq of direction, 3),
+// 2 moment_1th_hess_f_gaussian_measure_5th_6d (d2F_dq2 of direction, 9).
+int ref_quad5(int term, int mode, int direction, const double *q, const double *sigma,
+              const double *x, const int *spc, double *out) {
+  potential_function f;
+  switch (term) {
+  case 0: f = rho_ij_adp_MgHx_constructor(); break;
+  case 1: f = V_pair_ij_adp_MgHx_constructor(); break;
+  default: return 1;
+  }
+  double qq[6], ss[2], xx[2];
+  AtomicSpecie sp[2];
+  for (int k = 0; k < 6; ++k) qq[k] = q[k];
+  for (int k = 0; k < 2; ++k) {
+    ss[k] = sigma[k];
+    xx[k] = x[k];
+    sp[k] = (AtomicSpecie)spc[k];
+  }
+  int dof[4] = {1, 0, 0, 1};
+  gaussian_measure_ctx ctx = fill_out_gaussian_measure(qq, ss, xx, sp, dof, 2);
+  for (int k = 0; k < 9; ++k) out[k] = 0.0;
+  if (mode == 0) moment_1th_Vij_gaussian_measure_5th(out, f, &ctx);
+  else if (mode == 1) moment_1th_grad_f_gaussian_measure_5th_6d(direction, out, f, &ctx);
+  else moment_1th_hess_f_gaussian_measure_5th_6d(direction, out, f, &ctx);
+  destroy_gaussian_measure(&ctx);
   return 0;
 }
 

@@ -364,8 +364,39 @@ def termfns_fixture(ref, per=12):
     print(f"termfns: {len(rows)} evaluations")
 
 
+def quad5_fixture(ref, per=8):
+    """The reference's 5th-degree rule (Quadrature-Hermitian-5th.cpp) of the
+    two pair terms: the average, the averaged gradient of each site and the
+    averaged Hessian blocks, at seeded pair geometries (sites 1.6-6.5 A
+    apart, widths 0.05-0.2 A, species mixed, occupancies in [0.05, 1])."""
+    rng = np.random.default_rng(23)
+    rows = []
+    for term in (0, 1):
+        for mode, dirs in ((0, [0]), (1, [0, 1]), (2, [0, 1, 2, 3])):
+            for d in dirs:
+                for _ in range(per):
+                    q = np.zeros(6)
+                    q[:3] = rng.uniform(-1.0, 1.0, 3)
+                    v = rng.normal(size=3)
+                    q[3:] = q[:3] + v / np.linalg.norm(v) * rng.uniform(1.6, 6.5)
+                    sig = rng.uniform(0.05, 0.2, 2)
+                    x = rng.uniform(0.05, 1.0, 2)
+                    spc = rng.choice([12, 1], 2).astype(np.int32)
+                    out = ref.quad5(term, mode, d, q, sig, x, spc)
+                    rows.append((term, mode, d, q, sig, x, spc, out))
+    np.savez_compressed(
+        os.path.join(OUT, "quad5.npz"),
+        meta=np.array([r_[:3] for r_ in rows], np.int32), q=np.array([r_[3] for r_ in rows]),
+        sigma=np.array([r_[4] for r_ in rows]), x=np.array([r_[5] for r_ in rows]),
+        species=np.array([r_[6] for r_ in rows]), out=np.array([r_[7] for r_ in rows]))
+    print(f"quad5: {len(rows)} quadratures")
+
+
 def main():
     ref = pyoracle.reference()
+    if ref is not None and sys.argv[1:] == ["--quad5"]:
+        quad5_fixture(ref)
+        return
     if ref is not None and sys.argv[1:] == ["--termfns"]:
         termfns_fixture(ref)
         return

@@ -136,3 +136,23 @@ def test_reference_style_caller_of_the_term_table(tmp_path):
         tol = 1e-4 if fn == 4 else TOL[fn]
         gold = d["out"][r]
         assert np.abs(vals[k] - gold).max() <= tol * max(1.0, np.abs(gold).max()), r
+
+
+def test_fifth_degree_rule(gpu_tables):
+    """The reference's 5th-degree rule over the pair measure
+    (Quadrature-Hermitian-5th.cpp:31-432) on the device against the
+    reference build's values (tests/golden/quad5.npz): averages of F and
+    dF_dq within 1e-12, of d2F_dq2 within 1e-10 (the analytic blocks'
+    tolerance)."""
+    d = dict(np.load(os.path.join(GOLD, "quad5.npz")))
+    for key in sorted({tuple(m) for m in d["meta"]}):
+        term, mode, direction = key
+        sel = np.all(d["meta"] == key, axis=1)
+        out = gpu_tables.term_quadrature5(term, mode, direction, d["q"][sel], d["sigma"][sel],
+                                          d["x"][sel], d["species"][sel])
+        gold = d["out"][sel]
+        tol = 1e-10 if mode == 2 else 1e-12
+        assert np.abs(out - gold).max() <= tol * max(1.0, np.abs(gold).max()), key
+    with pytest.raises(btam.BtamError):
+        gpu_tables.term_quadrature5(2, 0, 0, d["q"][:1], d["sigma"][:1], d["x"][:1],
+                                    d["species"][:1])  # pair terms only

@@ -330,3 +330,20 @@ def test_term_table_against_golden(oracle):
             assert np.array_equal(out, gold), (r, term, fn, direction)
         n_checked += 1
     assert n_checked == 840
+
+
+def test_fifth_degree_rule_against_golden(oracle):
+    """The oracle's restatement of the reference's 5th-degree rule over the
+    pair measure (Quadrature-Hermitian-5th.cpp:31-432) reproduces the
+    reference build's averages of F and dF_dq bit for bit and of d2F_dq2 to
+    1e-14 (the oracle's Hessian blocks are derived in another order)."""
+    d = load("quad5")
+    for r in range(len(d["meta"])):
+        term, mode, direction = (int(v) for v in d["meta"][r])
+        out = oracle.quad5(term, mode, direction, d["q"][r], d["sigma"][r], d["x"][r],
+                           d["species"][r])
+        gold = d["out"][r]
+        if mode == 2:
+            assert np.abs(out - gold).max() <= 1e-14 * np.abs(gold).max(), r
+        else:
+            assert np.array_equal(out, gold), r
