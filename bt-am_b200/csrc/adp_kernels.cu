@@ -68,6 +68,10 @@ __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 // packed Site32 rows in the FP32C form, two 32-byte loads from the Site64 rows
 // in the FP64 form, the separate arrays otherwise.  BO: also beta and owner
 // (the pass-2 pair kernel), from the same FP64 row.
+template <class R> __device__ __forceinline__ bool site_off(const EvalArgs<R> &a, int i) {
+  return a.site_on && !a.site_on[i];
+}
+
 template <class R> struct NbSite {
   double x, y, z;
   R sigma, occ;
@@ -322,6 +326,7 @@ pass1u_pair_kernel(const EvalArgs<R> a) {
 #pragma unroll 1
   for (int t = blockIdx.x * TPB + threadIdx.x; t < a.n_own; t += gridDim.x * TPB) {
     const int p = a.own_p[t], u = a.own_u[t];
+    if (site_off(a, u)) continue;
     const int j = a.idx[p];
     const NbSite<R> su = nb_site(a, u), sj = nb_site(a, j);
     if (a.x_only) {  // the four pass-1 sums, occupied or not
@@ -443,7 +448,7 @@ pass1_kernel(const EvalArgs<R> a) {
 #pragma unroll 1
   for (int wi = blockIdx.x * W + warp; wi * SPW < a.n_real; wi += gridDim.x * W) {
   const int i = wi * SPW + half;
-  const bool live = i < a.n_real;
+  const bool live = i < a.n_real && !site_off(a, i);
   const double2 xbi = live ? a.xb[i] : make_double2(0.0, 1.0);
   const double xi = xbi.x;
   const bool act = live && !(xi < kMinOcc);
@@ -570,6 +575,7 @@ pass2_kernel(const EvalArgs<R> a) {
   // whichever trip of whichever grid computes it
 #pragma unroll 1
   for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
+  if (site_off(a, u)) continue;
   const double2 xbu = a.xb[u];
   const double xu = xbu.x;
   if (xu < kMinOcc) {
@@ -763,6 +769,7 @@ mf_pair_terms_kernel(const EvalArgs<R> a, double *self, double *slot) {
 template <class R, class TV, bool XO = false>
 __device__ __forceinline__ void pass2u_one(const EvalArgs<R> &a, const TV &T, int t) {
   const int p = a.own_p[t], u = a.own_u[t];
+  if (site_off(a, u)) return;
   const int j = a.idx[p], r = a.rev[p];
   const NbSite<R> su = nb_site<R, true>(a, u), sj = nb_site<R, true>(a, j);
   R vu[8], vj[8];
@@ -860,6 +867,7 @@ pass2u_site_kernel(const EvalArgs<R> a) {
   // whichever trip of whichever grid computes it
 #pragma unroll 1
   for (int u = blockIdx.x * W + warp; u < a.n_real; u += gridDim.x * W) {
+    if (site_off(a, u)) continue;
     const double2 xbu = a.xb[u];
     const double xu = xbu.x;
     if (xu < kMinOcc) {

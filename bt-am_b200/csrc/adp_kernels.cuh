@@ -62,6 +62,10 @@ template <class R> struct EvalArgs {
   // pair-rule kernel.  Both are ignored by the directed variants.
   int x_only = 0;
   int recs_ready = 0;
+  // Sites to evaluate (1 per real site; nullptr: all): a served round of a
+  // batch evaluates only the systems that asked.  Every pair and triplet of
+  // a system lies within it, so a site that is off is skipped whole.
+  const unsigned char *site_on = nullptr;
   // undirected pass 2 (optional; nullptr / 0 when absent)
   const int *rev = nullptr;    // reverse slot of each real-site slot, -1 if none
   const int *own_p = nullptr;  // owned slots

@@ -69,13 +69,15 @@ inline int blocks_of(long long n, int per) { return (int)((n + per - 1) / per); 
 
 // Copies the site rows (real, then images) of the systems in the table into
 // their batch rows: blockIdx.y picks the system, the x dimension strides rows.
-__global__ void batch_gather_kernel(BatchXfer t, double4 *pos, double2 *xb) {
+__global__ void batch_gather_kernel(BatchXfer t, double4 *pos, double2 *xb,
+                                    unsigned char *site_on) {
   const BatchXfer::Sys &d = t.sys[blockIdx.y];
   const int rows = d.n + d.g;
   for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
     const int dst = r < d.n ? d.R + r : d.G + (r - d.n);
     pos[dst] = d.pos[r];
     xb[dst] = d.xb[r];
+    if (r < d.n) site_on[dst] = 1;  // this system is evaluated in the round
   }
 }
 
@@ -123,6 +125,9 @@ struct btam_batch {
   Site32 *s32 = nullptr;  // packed neighbour rows of the FP32C kernels [all]
   SiteB *sb = nullptr;
   Site64 *s64 = nullptr;  // packed neighbour rows of the FP64 kernels [all]
+  // the systems a served round evaluates (1 per real site), used while masked
+  unsigned char *site_on = nullptr;
+  bool masked = false;
   int *rev = nullptr, *slot_own = nullptr, *own_p = nullptr, *own_u = nullptr;
   int n_own = 0;
   char *pbuf = nullptr;
@@ -153,6 +158,7 @@ template <class R> EvalArgs<R> batch_args(btam_batch *b, R *mom, const RadialVie
   } else {
     a.s64 = b->s64;
   }
+  if (b->masked) a.site_on = b->site_on;
   a.pos = b->pos;
   a.xb = b->xb;
   a.code = b->code;
@@ -256,6 +262,7 @@ void free_batch(btam_batch *b) {
   dfree(b->s32, b->st);
   dfree(b->sb, b->st);
   dfree(b->s64, b->st);
+  dfree(b->site_on, b->st);
   dfree(b->slot_own, b->st);
   dfree(b->own_p, b->st);
   dfree(b->own_u, b->st);
@@ -312,6 +319,7 @@ int batch_build(btam_batch *b) {
   BTAM_TRY(dalloc(b->s32, b->st, na));
   BTAM_TRY(dalloc(b->sb, b->st, na));
   BTAM_TRY(dalloc(b->s64, b->st, na));
+  BTAM_TRY(dalloc(b->site_on, b->st, nr));
   BTAM_TRY(dalloc(b->gamma, b->st, nr));
   BTAM_TRY(dalloc(b->offs, b->st, nr + 1));
   BTAM_TRY(dalloc(b->idx, b->st, (size_t)n_pairs));
@@ -536,7 +544,10 @@ int batch_round(btam_batch *b, const BatchXfer &t, const cudaEvent_t *ready, int
   int rows = 0;
   for (int k = 0; k < t.n; ++k) rows = std::max(rows, t.sys[k].n + t.sys[k].g);
   const dim3 grid(std::max(1, std::min(64, blocks_of(rows, 256))), t.n);
-  batch_gather_kernel<<<grid, 256, 0, b->st>>>(t, b->pos, b->xb);
+  // only the systems in the table are evaluated: the others' rows keep
+  // their last results, which nobody reads
+  BTAM_TRY(cudaMemsetAsync(b->site_on, 0, (size_t)b->n_real, b->st));
+  batch_gather_kernel<<<grid, 256, 0, b->st>>>(t, b->pos, b->xb, b->site_on);
   BTAM_TRY(cudaGetLastError());
   BTAM_TRY(cudaMemsetAsync(b->err, 0, sizeof(int), b->st));
   // the kernels are launched directly, not replayed from a captured graph:
@@ -545,8 +556,11 @@ int batch_round(btam_batch *b, const BatchXfer &t, const cudaEvent_t *ready, int
   // implicitly and must never meet a stream in capture)
   int st = ensure_moments(b, precision);
   if (st != BTAM_OK) return st;
-  BTAM_TRY(precision == BTAM_FP64 ? enqueue_eval<double>(b, 0, b->mom64, b->T->r64)
-                                  : enqueue_eval<float>(b, 1, b->mom32, b->T->r32));
+  b->masked = true;
+  const cudaError_t ev = precision == BTAM_FP64 ? enqueue_eval<double>(b, 0, b->mom64, b->T->r64)
+                                                : enqueue_eval<float>(b, 1, b->mom32, b->T->r32);
+  b->masked = false;
+  BTAM_TRY(ev);
   batch_scatter_kernel<<<grid, 256, 0, b->st>>>(t, b->rho, b->V0, b->S0, b->Rq, b->Rs, b->Rx,
                                                  b->totals, b->err);
   return cuda_status(cudaGetLastError());
