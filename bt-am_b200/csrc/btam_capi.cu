@@ -995,9 +995,23 @@ int btam_mf_eval_state(btam_system *s, int precision, const double *q, const dou
   }
   int st = btam_mf_eval_async(s, precision);
   if (st != BTAM_OK) return st;
-  int flags = 0;
-  BTAM_TRY(cudaMemcpyAsync(&flags, s->err + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
-  st = btam_results_copy(s, rho, V0, S0, Rq, Rs, Rx, totals);
+  // the result copies, then the validation flags and error bits behind
+  // them, and one wait for all of it
+  const size_t nb = (size_t)n * sizeof(double);
+  const struct {
+    double *dst;
+    const double *src;
+    size_t bytes;
+  } cp[7] = {{rho, s->rho, nb}, {V0, s->V0, nb}, {S0, s->S0, nb}, {Rq, s->Rq, 3 * nb},
+             {Rs, s->Rs, nb},   {Rx, s->Rx, nb}, {totals, s->totals, 4 * sizeof(double)}};
+  for (const auto &c : cp)
+    if (c.dst) BTAM_TRY(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, s->st));
+  int bits[2] = {0, 0};
+  BTAM_TRY(cudaMemcpyAsync(bits, s->err, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  BTAM_TRY(cudaStreamSynchronize(s->st));
+  const int flags = bits[1];
+  st = status_from_bits(bits[0]);
   if (flags & 1) return BTAM_ERR_NONFINITE;
   if (flags & 2) return BTAM_ERR_OCCUPANCY;
   if (flags & 4) return BTAM_ERR_OUT_OF_BOX;
