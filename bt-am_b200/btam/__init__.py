@@ -47,6 +47,7 @@ _V = ctypes.c_void_p
 _PROTOS = {
     "btam_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "btam_version": (ctypes.c_int, []),
+    "btam_last_cuda_error": (ctypes.c_char_p, []),
     "btam_pool_usage": (ctypes.c_int, [ctypes.POINTER(ctypes.c_longlong),
                                        ctypes.POINTER(ctypes.c_longlong)]),
     "btam_tables_load": (ctypes.c_int, [ctypes.c_char_p, ctypes.POINTER(_V)]),
@@ -207,6 +208,10 @@ def _i(a):
 
 def _check(code, what):
     if code != 0:
+        if code in (7, 8):  # BTAM_ERR_OOM, BTAM_ERR_CUDA: name the runtime error
+            name = lib().btam_last_cuda_error().decode()
+            if name:
+                what = f"{what} ({name})"
         raise BtamError(code, what)
 
 
@@ -441,9 +446,10 @@ class System:
     # -- consumers: relaxation and the hydrogen master equation
     def relax(self, mode=0, tol=1e-8, max_iter=500, m=8, sigma_min=0.001, sigma_max=0.4,
               x_min=0.01):
-        """L-BFGS relaxation of (q, sigma) on the device.  Returns a dict with
-        the final projected residual norm, iterations, evaluations, objective
-        and status (1 converged, 0 iteration limit, -1 stalled)."""
+        """Relaxation of (q, sigma) on the device: L-BFGS (modes 0-2, m pairs)
+        or N-GMRES(m) with the critical-point line search (mode 4).  Returns a
+        dict with the final projected residual norm, iterations, evaluations,
+        objective and status (1 converged, 0 iteration limit, -1 stalled)."""
         info = np.zeros(5)
         bd = np.array([sigma_min, sigma_max, x_min], np.float64)
         _check(lib().btam_relax(self.handle, mode, tol, max_iter, m, _d(bd), _d(info)),
@@ -802,7 +808,7 @@ class Batch:
 
 
 JOB_RELAX, JOB_DMD, JOB_EVAL, JOB_STRETCH = 0, 1, 2, 3
-RELAX_FP64, RELAX_MIXED, RELAX_FP32C, RELAX_NEWTON = 0, 1, 2, 3
+RELAX_FP64, RELAX_MIXED, RELAX_FP32C, RELAX_NEWTON, RELAX_NGMRES = 0, 1, 2, 3, 4
 MP_FD, MP_ANALYTIC = 1, 2
 
 

@@ -75,7 +75,11 @@ template <class R> BTAM_HD R rmin(R a, R b) { return a < b ? a : b; }
 // FP64 the index is the reference's: x times 1/dx truncates to the same
 // integer as the rounded quotient unless it lies within 1e-9 of a knot, and
 // there the quotient itself is taken, so a point on a knot picks the
-// reference's segment.  The FP32 form takes the product.
+// reference's segment.  The FP32 form takes the product.  A negative
+// argument (an embedding density below 0, which the reference would index
+// before its table with) takes segment 0, whose cubic is then extrapolated;
+// on the device a NaN argument converts to 0 as well, so no argument reads
+// outside the table.
 template <class R> BTAM_HD int seg_index(R x, R dx, R inv_dx, int n) {
   const R t = x * inv_dx;
   int m = (int)t;
@@ -83,7 +87,8 @@ template <class R> BTAM_HD int seg_index(R x, R dx, R inv_dx, int n) {
     const R f = t - (R)m;
     if (f < (R)1e-9 || f > (R)1 - (R)1e-9) m = (int)(x / dx);
   }
-  return m < n - 1 ? m : n - 1;
+  m = m < n - 1 ? m : n - 1;
+  return m > 0 ? m : 0;
 }
 
 template <class R>

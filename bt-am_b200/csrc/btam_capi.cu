@@ -16,6 +16,7 @@
 
 #include "../../include/btam.h"
 #include "adp_core.cuh"
+#include "linalg.hpp"
 #include "adp_kernels.cuh"
 #include "solvers.cuh"
 #include "tables_io.hpp"
@@ -403,6 +404,11 @@ const char *btam_status_string(int st) {
 }
 
 int btam_version(void) { return 100; }
+
+const char *btam_last_cuda_error(void) {
+  const cudaError_t e = last_cuda_error();
+  return e == cudaSuccess ? "" : cudaGetErrorName(e);
+}
 
 int btam_pool_usage(long long *used, long long *reserved) {
   if (!used || !reserved) return BTAM_ERR_ARG;
@@ -1284,6 +1290,12 @@ __global__ void fill_kernel(int n, double v, double *a) {
   if (i < n) a[i] = v;
 }
 
+// g / beta per site: the N-GMRES residual in energy units
+__global__ void unbeta_kernel(int n4, const double2 *xb, double *g) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n4) g[i] /= xb[i >> 2].y;
+}
+
 // max over sites and components of |p| in unscaled units (p / sqrt(max(x, 1e-3)))
 __global__ void absmax_kernel(int n4, const double2 *xb, const double *a, double *out) {
   __shared__ double sh[256];
@@ -1299,6 +1311,226 @@ __global__ void absmax_kernel(int n4, const double2 *xb, const double *a, double
   if (threadIdx.x == 0) *out = sh[0];
 }
 
+// The relaxation with the reference's option set for its SNES (main-BT-AM.cpp:
+// 64-67: -snes_type ngmres, -snes_ngmres_m 3, -snes_linesearch_type cp):
+// N-GMRES(m) on the variables z = (q, log sigma) scaled by the occupancies
+// (the same z and bounds as the L-BFGS schedule) with the residual
+// g(z) = (R_q, sigma R_sigma) / sqrt(x), the gradient of F in energy units
+// (the L-BFGS gradient over beta), FP64, every vector on the device.  The
+// energy units make the line search's first trial (lambda = 1) move a site
+// by its force over its occupancy in A per eV/A instead of beta times that.
+// As PETSc's SNESNGMRES with its defaults forms it: each iteration takes
+// z^M = z - lambda g(z), lambda from the critical-point line search (one
+// secant step on g(z - lambda g) . g from lambda = 0 and the first trial,
+// lambda = 1 damped to a 0.05 move), then the
+// combination z^A of z^M and the last m
+// iterates minimising the linearised |g|; z^A is kept when |g(z^A)| < 2
+// min|g| and either 0.1 |z^A - z^M| < min_i |z^A - z_i| or sqrt|g(z)| < 0.9
+// sqrt(min|g|), else z^M; the subspace restarts after two consecutive
+// iterations with (0.1 |z^A - z^M| > min_i |z^A - z_i| and sqrt|g(z^A)| >
+// 0.9 sqrt(min|g|)) or |g(z^A)| > 2 min|g|.  Three evaluations per
+// iteration; converged on the projected residual norm as btam_relax.
+int relax_ngmres(btam_system *s, double tol, int max_iter, int m, const double *bounds,
+                 double *info) {
+  constexpr double gammaA = 2.0, gammaC = 2.0, epsilonB = 0.1, deltaB = 0.9;
+  constexpr double kTrialMove = 0.05, kMaxMove = 0.5;
+  constexpr int restart_it = 2;
+  const double sig_lo = bounds ? bounds[0] : 0.001, sig_hi = bounds ? bounds[1] : 0.4,
+               x_min = bounds ? bounds[2] : 0.01;
+  if (!(sig_lo > 0.0 && sig_hi > sig_lo && x_min >= 0.0)) return BTAM_ERR_ARG;
+  const int n = s->n_real, n4 = 4 * n;
+  // X F XM FM XA FA D, Xd[m] Fd[m] (n4 each), fterm rterm ones (n), scalars
+  double *buf = nullptr;
+  BTAM_TRY(dalloc(buf, s->st, (size_t)(7 + 2 * m) * n4 + 3 * (size_t)n + 64));
+  double *X = buf, *F = buf + n4, *XM = buf + 2 * (size_t)n4, *FM = buf + 3 * (size_t)n4,
+         *XA = buf + 4 * (size_t)n4, *FA = buf + 5 * (size_t)n4, *D = buf + 6 * (size_t)n4;
+  std::vector<double *> Xd(m), Fd(m);
+  for (int k = 0; k < m; ++k) {
+    Xd[k] = buf + (size_t)(7 + k) * n4;
+    Fd[k] = buf + (size_t)(7 + m + k) * n4;
+  }
+  RelaxVecs v;
+  v.fterm = buf + (size_t)(7 + 2 * m) * n4;
+  v.rterm = v.fterm + n;
+  v.ones = v.rterm + n;
+  v.scal = v.ones + n;
+  v.tmp = v.scal + 2;  // 8 scratch scalars
+  double *dots = v.tmp + 8;  // up to 40 dot products
+  v.bd.ls_lo = std::log(sig_lo);
+  v.bd.ls_hi = std::log(sig_hi);
+  v.bd.x_min = x_min;
+  fill_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(n, 1.0, v.ones);
+  int st = cuda_status(cudaGetLastError());
+  // state at z (with the bounds), then its evaluation into (Z, G)
+  auto eval_at = [&](const double *z, double *Z, double *G, double &r2) -> int {
+    if (z) {
+      BTAM_TRY(relax_apply(n, s->xb, z, z, 0.0, v.bd, s->pos, s->st));
+      if (s->n_ghost > 0)
+        BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                      s->box, s->st));
+    }
+    v.z = Z;
+    v.g = G;
+    double f = 0.0;
+    const int r = relax_eval(s, BTAM_FP64, v, f, r2);
+    if (r != BTAM_OK) return r;
+    unbeta_kernel<<<(n4 + 255) / 256, 256, 0, s->st>>>(n4, s->xb, G);
+    return cuda_status(cudaGetLastError());
+  };
+  // dot products of a with each b[k], in one wait
+  auto mdot = [&](const double *a, const std::vector<const double *> &bs, double *out) -> int {
+    for (size_t k = 0; k < bs.size(); ++k) BTAM_TRY(vec_dot(n4, a, bs[k], dots + k, s->st));
+    BTAM_TRY(cudaMemcpyAsync(out, dots, bs.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                             s->st));
+    return cuda_status(cudaStreamSynchronize(s->st));
+  };
+  auto nrm = [&](const double *a, double &out) -> int {
+    double d2 = 0.0;
+    const int r = mdot(a, {a}, &d2);
+    out = std::sqrt(d2);
+    return r;
+  };
+  int evals = 0, it = 0, status = 0;
+  double r2 = 0.0, fnorm = 0.0;
+  if (st == BTAM_OK) st = eval_at(nullptr, X, F, r2);
+  ++evals;
+  if (st == BTAM_OK) st = nrm(F, fnorm);
+  std::vector<double> Q((size_t)m * m, 0.0), xi(m), beta(m), H((size_t)m * m);
+  double fminnorm = fnorm;
+  int k_restart = 1, l = 1, ivec = 0, restart_count = 0;
+  auto put = [&](int iv, const double *x, const double *f) -> int {
+    BTAM_TRY(cudaMemcpyAsync(Xd[iv], x, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    BTAM_TRY(cudaMemcpyAsync(Fd[iv], f, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    return BTAM_OK;
+  };
+  if (st == BTAM_OK) st = put(0, X, F);
+  if (st == BTAM_OK && std::sqrt(r2) <= tol) status = 1;
+  for (int k = 1; st == BTAM_OK && status == 0 && k <= max_iter; ++k) {
+    // z^M: the critical-point line search along -g from z.  Its first trial
+    // is lambda = 1 damped so that no q moves by more than 0.05 A nor log
+    // sigma by more than 0.05, and its result moves neither by more than
+    // 0.5 (the reference's maxstep bound of 1e8 on lambda, in displacement)
+    double pmax = 0.0;
+    absmax_kernel<<<1, 256, 0, s->st>>>(n4, s->xb, F, v.tmp + 6);
+    st = cuda_status(cudaMemcpyAsync(&pmax, v.tmp + 6, sizeof(double), cudaMemcpyDeviceToHost,
+                                     s->st));
+    if (st == BTAM_OK) st = cuda_status(cudaStreamSynchronize(s->st));
+    if (st != BTAM_OK) break;
+    const double lam_max = pmax > 0.0 ? std::min(1e8, kMaxMove / pmax) : 1e8;
+    double lambda = pmax > kTrialMove ? kTrialMove / pmax : 1.0, r2M = 0.0, fty = 0.0;
+    const double fty0 = fnorm * fnorm;
+    if (fty0 >= 1e-15 * fnorm) {
+      if ((st = cuda_status(vec_axpby(n4, 1.0, X, -lambda, F, D, s->st))) != BTAM_OK) break;
+      if ((st = eval_at(D, XM, FM, r2M)) != BTAM_OK) break;
+      ++evals;
+      if ((st = mdot(FM, {F}, &fty)) != BTAM_OK) break;
+      double sl = (fty - fty0) / lambda;  // secant slope from lambda_old = 0
+      if (sl > 0.0) sl = -sl;
+      if (sl != 0.0 && !(std::fabs(fty) / std::fabs(fty0) < 1e-8)) {
+        double lu = lambda - fty / sl;
+        if (lu < 1e-12) lu = lambda + fty / sl;
+        if (std::isfinite(lu)) lambda = std::min(lu, lam_max);
+      }
+    }
+    if ((st = cuda_status(vec_axpby(n4, 1.0, X, -lambda, F, D, s->st))) != BTAM_OK) break;
+    if ((st = eval_at(D, XM, FM, r2M)) != BTAM_OK) break;
+    ++evals;
+    double fMnorm = 0.0;
+    if ((st = nrm(FM, fMnorm)) != BTAM_OK) break;
+    // z^A: the combination minimising |(1 - sum beta) g^M + sum beta g_i|
+    {
+      std::vector<const double *> fs(l);
+      for (int i = 0; i < l; ++i) fs[i] = Fd[i];
+      std::vector<double> col(l);
+      if ((st = mdot(FM, fs, xi.data())) != BTAM_OK) break;
+      if ((st = mdot(Fd[ivec], fs, col.data())) != BTAM_OK) break;
+      for (int i = 0; i < l; ++i) Q[(size_t)i * m + ivec] = Q[(size_t)ivec * m + i] = col[i];
+    }
+    const double nu = fMnorm * fMnorm;
+    for (int i = 0; i < l; ++i) beta[i] = nu - xi[i];
+    for (int j = 0; j < l; ++j)
+      for (int i = 0; i < l; ++i)
+        H[(size_t)i * l + j] = Q[(size_t)i * m + j] - xi[i] - xi[j] + nu;
+    if (l == 1) beta[0] = H[0] != 0.0 ? beta[0] / H[0] : 0.0;
+    else lsq_sym(l, H.data(), beta.data());
+    double alph = 0.0;
+    for (int i = 0; i < l; ++i) alph += beta[i];
+    if ((st = cuda_status(vec_axpby(n4, 1.0 - alph, XM, 0.0, XM, D, s->st))) != BTAM_OK) break;
+    for (int i = 0; i < l && st == BTAM_OK; ++i)
+      st = cuda_status(vec_axpby(n4, 1.0, D, beta[i], Xd[i], D, s->st));
+    if (st != BTAM_OK) break;
+    double r2A = 0.0;
+    if ((st = eval_at(D, XA, FA, r2A)) != BTAM_OK) break;
+    ++evals;
+    if (fminnorm > fMnorm) fminnorm = fMnorm;
+    double fAnorm = 0.0, dnorm = 0.0, dminnorm = -1.0;
+    if ((st = nrm(FA, fAnorm)) != BTAM_OK) break;
+    if ((st = cuda_status(vec_axpby(n4, 1.0, XA, -1.0, XM, D, s->st))) != BTAM_OK) break;
+    if ((st = nrm(D, dnorm)) != BTAM_OK) break;
+    for (int i = 0; i < l && st == BTAM_OK; ++i) {
+      double dc = 0.0;
+      st = cuda_status(vec_axpby(n4, 1.0, Xd[i], -1.0, XA, D, s->st));
+      if (st == BTAM_OK) st = nrm(D, dc);
+      if (dc < dminnorm || dminnorm < 0.0) dminnorm = dc;
+    }
+    if (st != BTAM_OK) break;
+    // selection
+    bool selA = fAnorm < gammaA * fminnorm;
+    if (!(epsilonB * dnorm < dminnorm || std::sqrt(fnorm) < deltaB * std::sqrt(fminnorm)))
+      selA = false;
+    const double *xs = selA ? XA : XM, *fsel = selA ? FA : FM;
+    st = cuda_status(cudaMemcpyAsync(X, xs, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    if (st == BTAM_OK)
+      st = cuda_status(
+          cudaMemcpyAsync(F, fsel, n4 * sizeof(double), cudaMemcpyDeviceToDevice, s->st));
+    if (st != BTAM_OK) break;
+    fnorm = selA ? fAnorm : fMnorm;
+    r2 = selA ? r2A : r2M;
+    // restart
+    bool rs = false;
+    if (epsilonB * dnorm > dminnorm && std::sqrt(fAnorm) > deltaB * std::sqrt(fminnorm)) rs = true;
+    if (fAnorm > gammaC * fminnorm) rs = true;
+    restart_count = rs ? restart_count + 1 : 0;
+    ivec = k_restart % m;
+    if (restart_count >= restart_it) {
+      restart_count = 0;
+      k_restart = 1;
+      l = 1;
+      ivec = 0;
+      st = put(0, XM, FM);
+    } else {
+      if (l < m) ++l;
+      ++k_restart;
+      if (fminnorm > fnorm) fminnorm = fnorm;
+      st = put(ivec, X, F);
+    }
+    it = k;
+    if (!std::isfinite(fnorm)) st = BTAM_ERR_NONFINITE;
+    if (std::sqrt(r2) <= tol) status = 1;
+  }
+  // leave the system at the selected iterate, evaluated; relax_eval has
+  // read its objective and residual norm before the scratch is released
+  double r2f = r2, ff = 0.0;
+  if (st == BTAM_OK) {
+    v.z = XM;
+    v.g = FM;
+    st = cuda_status(relax_apply(n, s->xb, X, X, 0.0, v.bd, s->pos, s->st));
+    if (st == BTAM_OK && s->n_ghost > 0)
+      st = cuda_status(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner,
+                                            s->image, s->box, s->st));
+    if (st == BTAM_OK) st = relax_eval(s, BTAM_FP64, v, ff, r2f);
+  }
+  dfree(buf, s->st);
+  if (info) {
+    info[0] = std::sqrt(r2f);
+    info[1] = it;
+    info[2] = evals;
+    info[3] = ff;
+    info[4] = status;
+  }
+  return st;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1307,7 +1539,8 @@ int btam_relax(btam_system *s, int mode, double tol, int max_iter, int m, const 
                double *info) {
   if (!s || !(tol > 0.0) || max_iter < 0 || m < 1 || m > 16) return BTAM_ERR_ARG;
   if (!s->built) return BTAM_ERR_NOT_BUILT;
-  if (mode < 0 || mode > 3) return BTAM_ERR_ARG;
+  if (mode < 0 || mode > 4) return BTAM_ERR_ARG;
+  if (mode == BTAM_RELAX_NGMRES) return relax_ngmres(s, tol, max_iter, m, bounds, info);
   if (mode == BTAM_RELAX_NEWTON) {  // max_iter Newton steps, m unused
     double inf6[6];
     const int st = btam_relax_newton(s, tol, max_iter, 300, bounds, inf6);

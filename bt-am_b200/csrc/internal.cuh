@@ -170,8 +170,16 @@ inline int status_from_bits(int bits) {
   return BTAM_OK;
 }
 
+// The CUDA runtime error that this thread last turned into a status
+// (btam_last_cuda_error reports it).
+inline cudaError_t &last_cuda_error() {
+  static thread_local cudaError_t e = cudaSuccess;
+  return e;
+}
+
 inline int cuda_status(cudaError_t e) {
   if (e == cudaSuccess) return BTAM_OK;
+  last_cuda_error() = e;
   if (e == cudaErrorMemoryAllocation) return BTAM_ERR_OOM;
   return BTAM_ERR_CUDA;
 }

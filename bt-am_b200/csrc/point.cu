@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "internal.cuh"
+#include "linalg.hpp"
 
 namespace btam {
 namespace {
@@ -755,57 +756,6 @@ int btam_stretch_apply(btam_system *s, const double F[3]) {
 
 namespace {
 
-// Symmetric 3x3 (or smaller, n <= 3) least squares H beta = b with the
-// minimum-norm solution: eigenvalues below 2.2e-16 times the largest are
-// dropped (Jacobi rotations), as an SVD solve with machine-precision cutoff
-// does for a symmetric positive semi-definite H.
-void lsq_sym(int n, double H[3][3], double b[3]) {
-  double A[3][3], V[3][3];
-  for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) {
-      A[i][j] = (i < n && j < n) ? H[i][j] : 0.0;
-      V[i][j] = i == j ? 1.0 : 0.0;
-    }
-  for (int sweep = 0; sweep < 50; ++sweep) {
-    double off = 0.0;
-    for (int i = 0; i < n; ++i)
-      for (int j = i + 1; j < n; ++j) off += A[i][j] * A[i][j];
-    if (off < 1e-300) break;
-    for (int p = 0; p < n; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        if (A[p][q] == 0.0) continue;
-        const double th = (A[q][q] - A[p][p]) / (2.0 * A[p][q]);
-        const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
-        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
-        for (int k = 0; k < n; ++k) {  // A <- A J
-          const double akp = A[k][p], akq = A[k][q];
-          A[k][p] = c * akp - sn * akq;
-          A[k][q] = sn * akp + c * akq;
-        }
-        for (int k = 0; k < n; ++k) {  // A <- J^T A
-          const double apk = A[p][k], aqk = A[q][k];
-          A[p][k] = c * apk - sn * aqk;
-          A[q][k] = sn * apk + c * aqk;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double vkp = V[k][p], vkq = V[k][q];
-          V[k][p] = c * vkp - sn * vkq;
-          V[k][q] = sn * vkp + c * vkq;
-        }
-      }
-  }
-  double lmax = 0.0;
-  for (int i = 0; i < n; ++i) lmax = std::max(lmax, std::fabs(A[i][i]));
-  double y[3] = {0.0, 0.0, 0.0};
-  for (int k = 0; k < n; ++k) {
-    if (!(std::fabs(A[k][k]) > 2.220446049250313e-16 * lmax)) continue;
-    double vb = 0.0;
-    for (int i = 0; i < n; ++i) vb += V[i][k] * b[i];
-    for (int i = 0; i < n; ++i) y[i] += V[i][k] * vb / A[k][k];
-  }
-  for (int i = 0; i < n; ++i) b[i] = y[i];
-}
-
 // The reference's configured solver for the stretch equations: SNES type
 // "ngmres" with m = 3 and line search "cp" (main-BT-AM.cpp:64-67, the
 // options of the "minV_dF_" solver that Mechanical-Relaxation-bulk.cpp:296-341
@@ -872,8 +822,14 @@ int ngmres_stretch(const std::function<int(const double *, double *)> &residual,
     for (int i = 0; i < l; ++i) beta[i] = nu - xi[i];
     for (int j = 0; j < l; ++j)
       for (int i = 0; i < l; ++i) H[i][j] = Q[i][j] - xi[i] - xi[j] + nu;
-    if (l == 1) beta[0] = H[0][0] != 0.0 ? beta[0] / H[0][0] : 0.0;
-    else lsq_sym(l, H, beta);
+    if (l == 1) {
+      beta[0] = H[0][0] != 0.0 ? beta[0] / H[0][0] : 0.0;
+    } else {
+      double Hf[9];
+      for (int i = 0; i < l; ++i)
+        for (int j = 0; j < l; ++j) Hf[i * l + j] = H[i][j];
+      lsq_sym(l, Hf, beta);
+    }
     double alph = 0.0;
     for (int i = 0; i < l; ++i) alph += beta[i];
     double XA[3], FA[3];

@@ -74,6 +74,8 @@ extern "C" {
 #define BTAM_RELAX_MIXED 1       /* FP32C until |R| < 1e-5, then FP64 */
 #define BTAM_RELAX_FP32C 2       /* FP32C only (stops at its ~1e-6 noise floor) */
 #define BTAM_RELAX_NEWTON 3      /* btam_relax_newton (FP64): max_iter Newton steps, m unused */
+#define BTAM_RELAX_NGMRES 4      /* N-GMRES(m) with the critical-point line search (FP64): the
+                                    reference's SNES options (main-BT-AM.cpp:64-67, m = 3) */
 
 typedef struct btam_tables btam_tables;
 typedef struct btam_system btam_system;
@@ -81,6 +83,9 @@ typedef struct btam_batch btam_batch;
 
 const char *btam_status_string(int status);
 int btam_version(void);
+/* Name of the CUDA runtime error behind the calling thread's last
+ * BTAM_ERR_CUDA or BTAM_ERR_OOM ("cudaErrorInvalidValue", ...; "" if none). */
+const char *btam_last_cuda_error(void);
 /* Bytes of the library's device-memory pool on the current device (no
  * counterpart in the reference): in use by live systems, batches and
  * servers, and reserved from the device.  Every device allocation of the
