@@ -831,9 +831,11 @@ class Server:
         self.sizes = {}
 
     def submit(self, sysdict, kind, precision=FP32C, mode=RELAX_FP32C, tol=1e-5, max_iter=300,
-               nsteps=100, dmd=(1e-3, 0.045, 3.2, 1e-8, 0.9), plain=False):
+               nsteps=100, dmd=(1e-3, 0.045, 3.2, 1e-8, 0.9), plain=False, history=0):
         """Queues a job; plain=True runs it on the plain two-pass kernel pair
-        on its own instead of through the server's batched evaluations."""
+        on its own instead of through the server's batched evaluations.
+        history: the relaxation's L-BFGS history or N-GMRES subspace size
+        (0: 8, or 3 for N-GMRES)."""
         s = sysdict
         arrs = dict(q=np.ascontiguousarray(s["q"], np.float64),
                     sigma=np.ascontiguousarray(s["sigma"], np.float64),
@@ -853,6 +855,7 @@ class Server:
         sp.species = _i(arrs["species"])
         sp.periodic = _i(arrs["periodic"])
         sp.tol, sp.max_iter, sp.nsteps = float(tol), int(max_iter), int(nsteps)
+        sp.lbfgs_m = int(history)
         sp.plain = int(bool(plain))
         for c in range(5):
             sp.dmd_params[c] = float(dmd[c])

@@ -1996,7 +1996,8 @@ int btam_dmd_run(btam_system *s, int precision, int nsteps, const double *params
     if (relax_every > 0 && done % relax_every == 0) {
       // the mechanical state follows the new occupancies
       double info[5] = {0, 0, 0, 0, 0};
-      st = btam_relax(s, relax_mode, relax_tol, relax_max_iter, 8, nullptr, info);
+      st = btam_relax(s, relax_mode, relax_tol, relax_max_iter,
+                      relax_mode == BTAM_RELAX_NGMRES ? 3 : 8, nullptr, info);
       if (st != BTAM_OK) return st;
       acc[4] += 1.0;
       acc[5] += info[2];

@@ -322,8 +322,8 @@ void run_job(btam_server *srv, Job *job) {
       const double bounds[3] = {sp.sigma_min > 0 ? sp.sigma_min : 0.001,
                                 sp.sigma_max > 0 ? sp.sigma_max : 0.4,
                                 sp.x_min > 0 ? sp.x_min : 0.01};
-      st = btam_relax(s, sp.mode, sp.tol, sp.max_iter, sp.lbfgs_m > 0 ? sp.lbfgs_m : 8, bounds,
-                      info);
+      const int hist = sp.lbfgs_m > 0 ? sp.lbfgs_m : (sp.mode == BTAM_RELAX_NGMRES ? 3 : 8);
+      st = btam_relax(s, sp.mode, sp.tol, sp.max_iter, hist, bounds, info);
       r.norm = info[0];
       r.iterations = (int)info[1];
       r.evaluations = (int)info[2];

@@ -516,8 +516,9 @@ int btam_dmd_step_ctl(btam_system *s, int precision, int nsteps, const double *p
  * the method's parameters): nsteps master-equation steps with step control
  * (btam_dmd_step_ctl, params as there) and, after every relax_every steps,
  * a relaxation of (q, sigma) at the new occupancies (btam_relax with
- * relax_mode, relax_tol, relax_max_iter, history 8, default bounds), so the
- * mechanical state follows the occupancy; relax_every = 0 never relaxes.
+ * relax_mode, relax_tol, relax_max_iter, history 8 (N-GMRES: 3), default
+ * bounds), so the mechanical state follows the occupancy; relax_every = 0
+ * never relaxes.
  * Neighbour lists and the diffusive graph stay as built.  stats (6, may be
  * NULL): sub-steps, subdivided steps, cut edge moves, the largest ratio
  * (as btam_dmd_step_ctl), relaxations run, their residual evaluations. */
@@ -631,7 +632,7 @@ typedef struct btam_job_spec {
   const double *origin, *cell;  /* [3], [9] */
   const int *periodic;          /* [3] */
   double tol;                   /* relaxation tolerance */
-  int max_iter, lbfgs_m;        /* relaxation iterations, history (0: 8) */
+  int max_iter, lbfgs_m;        /* relaxation iterations, history m (0: 8; N-GMRES 3) */
   double sigma_min, sigma_max, x_min;  /* relaxation bounds (0: defaults) */
   int nsteps;                   /* master-equation steps */
   double dmd_params[5];         /* dt, Df, dr, min_dx, max_x */

@@ -30,6 +30,7 @@ def job_mix():
         (sph2, dict(kind=btam.JOB_EVAL, precision=btam.FP64)),
         (cell, dict(kind=btam.JOB_STRETCH, tol=1e-12, max_iter=20)),
         (sph, dict(kind=btam.JOB_RELAX, mode=btam.RELAX_NEWTON, tol=1e-7, max_iter=40)),
+        (cell, dict(kind=btam.JOB_RELAX, mode=btam.RELAX_NGMRES, tol=1e-7, max_iter=150)),
     ]
 
 
@@ -96,16 +97,28 @@ def test_server_admission_by_memory(gpu_tables):
     srv.close()
 
 
-def test_stretch_and_newton_jobs_equal_direct_calls(gpu_tables):
-    """A bulk stretch job and a Newton relaxation job give the final state,
-    residual and counts of the same calls made directly on a system."""
+def test_stretch_newton_and_ngmres_jobs_equal_direct_calls(gpu_tables):
+    """A bulk stretch job, a Newton relaxation job and an N-GMRES(3)
+    relaxation job give the final state, residual and counts of the same
+    calls made directly on a system."""
     jobs = job_mix()
     cell, kw_s = jobs[6]
     sph, kw_n = jobs[7]
+    cell_g, kw_g = jobs[8]
     srv = btam.Server(gpu_tables, workers=2)
     rs = srv.wait(srv.submit(cell, **kw_s))
     rn = srv.wait(srv.submit(sph, **kw_n))
+    rg = srv.wait(srv.submit(cell_g, **kw_g))
     srv.close()
+    G = btam.System(gpu_tables, cell_g)
+    G.build_neighbors()
+    G.set_variants(btam.FP64, 16 | 8 | 3, 16 | 8 | 0)
+    info = G.relax(mode=btam.RELAX_NGMRES, tol=1e-7, max_iter=150, m=3)
+    qg, sg, _ = G.get_state()
+    assert rg["status"] == 0 and rg["converged"] == info["status"], (rg, info)
+    assert rg["iterations"] == info["iterations"] == 150 or info["status"] == 1
+    assert rg["norm"] == info["norm"] and rg["evaluations"] == info["evaluations"]
+    assert np.array_equal(rg["q"], qg) and np.array_equal(rg["sigma"], sg)
     S = btam.System(gpu_tables, cell)
     S.build_neighbors()
     F, info = S.relax_stretch(atol=1e-12, rtol=1e-10, max_iter=20)
