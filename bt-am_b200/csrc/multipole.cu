@@ -38,10 +38,13 @@ namespace {
 constexpr double kSqrt2d = 1.4142135623730951;  // sqrt(2) of the rule (Macros.hpp)
 
 // cubic_spline (cubic-spline.cpp:84-96) in the reference's operation order:
-// m = min((int)(x / dx), n - 1), p = min(x - m dx, dx).
+// m = min((int)(x / dx), n - 1), p = min(x - m dx, dx); a negative x (an
+// embedding density below 0) takes segment 0 instead of an index before
+// the table.
 __device__ __forceinline__ int seg_ref(double x, double dx, int n, double &p) {
   int m = (int)(x / dx);
   m = m < n - 1 ? m : n - 1;
+  m = m > 0 ? m : 0;
   p = (double)m * dx;
   p = x - p;
   p = fmin(p, dx);
