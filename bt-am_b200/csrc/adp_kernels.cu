@@ -1057,6 +1057,7 @@ cudaError_t launch_pass1(const EvalArgs<R> &a, cudaStream_t st, int v, int v2, c
   case 2: go1<R, 4, 4, 16>(a, st, pers, und, mid); break;
   case 3: go1<R, 8, 2, 16>(a, st, pers, und, mid); break;
   case 4: go1<R, 4, 5, 16>(a, st, pers, und, mid); break;
+  case 5: go1<R, 4, 3, 16>(a, st, pers, und, mid); break;
   default: go1<R, 4, 1, 32>(a, st, pers, und, mid); break;
   }
   return cudaGetLastError();
@@ -1109,6 +1110,7 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int v, cudaEvent
     case 3: go2u<R, 256, 2>(a, st, pers, mid); break;
     case 4: go2u_smem<R, 512>(a, st, mid); break;
     case 5: go2u_smem<R, 384>(a, st, mid); break;
+    case 6: go2u<R, 128, 3>(a, st, pers, mid); break;
     default: go2u<R, 128, 1>(a, st, pers, mid); break;
     }
     return cudaGetLastError();

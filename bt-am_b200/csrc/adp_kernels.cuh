@@ -98,13 +98,13 @@ cudaError_t launch_pass2(const EvalArgs<R> &a, cudaStream_t st, int variant = 0,
 //           [| kUndirected: pass 1 takes its pair-rule sums, pass 2 its
 //            whole per-pair work, from one evaluation per undirected pair]
 // pass-1 shapes (warps per block, min blocks per SM, lanes per site):
-// (4,-,32), (4,5,8), (4,4,16), (8,2,16), (4,5,16)
-constexpr int kPass1Variants = 5;
+// (4,-,32), (4,5,8), (4,4,16), (8,2,16), (4,5,16), (4,3,16)
+constexpr int kPass1Variants = 6;
 constexpr int kPass2Variants = 6;  // shapes (4,-), (4,3), (4,4), (4,5), (8,2), (2,8)
 // undirected pair kernel (threads, min blocks): (128,-), (128,5), (128,4),
 // (256,2), then one block of 512 or 384 threads per SM with the uw tables in
-// shared memory (always persistent)
-constexpr int kPass2UVariants = 6;
+// shared memory (always persistent), then (128,3)
+constexpr int kPass2UVariants = 7;
 constexpr int kPersistent = 8;
 constexpr int kUndirected = 16;
 inline bool valid_variants(int v1, int v2) {

@@ -129,9 +129,9 @@ def test_launch_variants(gpu_tables):
     S.build_neighbors()
     for prec, tol in ((btam.FP64, 1e-12), (btam.FP32C, 1e-6)):
         base = S.evaluate(prec)
-        for shape1, shape2 in ([(v, v) for v in range(5)] + [(0, 5)] +
-                               [(0, 16 | v) for v in range(5)] +
-                               [(16 | v, 16 | v) for v in range(5)]):
+        for shape1, shape2 in ([(v, v) for v in range(6)] +
+                               [(0, 16 | v) for v in range(7)] +
+                               [(16 | v, 16 | v) for v in range(6)] + [(16 | 5, 16 | 6)]):
             for pers in (0, 8):
                 S.set_variants(prec, shape1 | pers, shape2 | pers)
                 out = S.evaluate(prec)
@@ -148,10 +148,10 @@ def test_launch_variants(gpu_tables):
                 for k in ("Rq", "Rs", "Rx"):
                     assert np.abs(out[k] - base[k]).max() < 10 * tol, (prec, shape1, k)
         v1, v2 = S.autotune(prec)
-        assert (v1 & 7) < 5 and v1 < 32 and v2 < 32
-        assert (v2 & 7) < (5 if v2 & 16 else 6)
+        assert (v1 & 7) < 6 and v1 < 32 and v2 < 32
+        assert (v2 & 7) < (7 if v2 & 16 else 6)
     with pytest.raises(btam.BtamError):
-        S.set_variants(btam.FP64, 5, 0)
+        S.set_variants(btam.FP64, 6, 0)
 
 
 def test_state_update_rejections(gpu_tables):
