@@ -75,6 +75,9 @@ _PROTOS = {
     "btam_mf_eval_x": (ctypes.c_int, [_V, ctypes.c_int]),
     "btam_mf_eval_state": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D, _D,
                                           _D, _D]),
+    "btam_mf_eval_state_async": (ctypes.c_int, [_V, ctypes.c_int, _D, _D, _D, _D, _D, _D, _D,
+                                                _D, _D, _D, ctypes.POINTER(ctypes.c_longlong)]),
+    "btam_mf_eval_state_wait": (ctypes.c_int, [_V, ctypes.c_longlong]),
     "btam_results_copy": (ctypes.c_int, [_V, _D, _D, _D, _D, _D, _D, _D]),
     "btam_system_sync": (ctypes.c_int, [_V]),
     "btam_rho_nmf": (ctypes.c_int, [_V, _D]),
@@ -344,6 +347,7 @@ class System:
                                         _i(per), ctypes.byref(h)), "btam_system_create")
         self.handle = h
         self.all_sites = None
+        self._inflight = {}  # evaluate_state_async tickets -> their arrays
 
     # -- state and topology
     def set_state(self, q=None, sigma=None, x=None):
@@ -414,6 +418,31 @@ class System:
                                         _d(out["Rq"]), _d(out["Rs"]), _d(out["Rx"]),
                                         _d(out["totals"])), "btam_mf_eval_state")
         return out
+
+    def evaluate_state_async(self, precision=FP64, q=None, sigma=None, x=None, out=None):
+        """btam_mf_eval_state_async: enqueues the new state, its evaluation
+        and the copies of the results into `out` (a dict of float64 arrays
+        named as evaluate_state's; pin them for overlapped copies) and
+        returns a ticket for wait_state.  The arrays (inputs included) must
+        stay alive and untouched until then."""
+        cv = lambda a: None if a is None else np.ascontiguousarray(a, np.float64)
+        q, sigma, x = cv(q), cv(sigma), cv(x)
+        out = out or {}
+        for k, v in out.items():
+            assert v.dtype == np.float64 and v.flags["C_CONTIGUOUS"], k
+        tk = ctypes.c_longlong()
+        args = [_d(out.get(k)) for k in ("rho", "V0", "S0", "Rq", "Rs", "Rx", "totals")]
+        _check(lib().btam_mf_eval_state_async(self.handle, precision, _d(q), _d(sigma), _d(x),
+                                              *args, ctypes.byref(tk)),
+               "btam_mf_eval_state_async")
+        self._inflight[tk.value] = (q, sigma, x, out)  # kept alive until the wait
+        return tk.value
+
+    def wait_state(self, ticket):
+        """Waits for a btam_mf_eval_state_async call; raises on its status."""
+        keep = self._inflight.pop(ticket, None)
+        _check(lib().btam_mf_eval_state_wait(self.handle, int(ticket)), "btam_mf_eval_state_wait")
+        return keep[3] if keep else None
 
     def evaluate_async(self, precision=FP64):
         _check(lib().btam_mf_eval_async(self.handle, precision), "btam_mf_eval_async")

@@ -305,6 +305,10 @@ int ensure_pbuf(btam_system *s, size_t elem) {
   return BTAM_OK;
 }
 
+// the pipelined state evaluations' buffers, events and copy streams
+// (defined beside btam_mf_eval_state_async)
+void release_state_slots(btam_system *s);
+
 }  // namespace
 
 // One evaluation enqueued on the system's stream.  x_only: the occupancy
@@ -651,6 +655,7 @@ int btam_system_create(const btam_tables *t, int n, const double *q, const doubl
 void btam_system_destroy(btam_system *s) {
   if (!s) return;
   if (s->st) cudaStreamSynchronize(s->st);
+  release_state_slots(s);
   dfree(s->pos, s->st); dfree(s->xb, s->st); dfree(s->code, s->st); dfree(s->owner, s->st); dfree(s->image, s->st);
   dfree(s->pt, s->st);
   dfree(s->s32, s->st); dfree(s->sb, s->st); dfree(s->s64, s->st);
@@ -1022,6 +1027,162 @@ int btam_mf_eval_state(btam_system *s, int precision, const double *q, const dou
   if (flags & 2) return BTAM_ERR_OCCUPANCY;
   if (flags & 4) return BTAM_ERR_OUT_OF_BOX;
   return st;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Status of a completed pipelined call from its flags (error bits, then the
+// validation flags of its update), with btam_mf_eval_state's precedence.
+int state_status(const int *f) {
+  if (f[1] & 1) return BTAM_ERR_NONFINITE;
+  if (f[1] & 2) return BTAM_ERR_OCCUPANCY;
+  if (f[1] & 4) return BTAM_ERR_OUT_OF_BOX;
+  return status_from_bits(f[0]);
+}
+
+// Waits until the call in slot b has delivered its results, frees the slot
+// and returns the call's status.
+int retire_state_slot(btam_system *s, int b) {
+  auto &sl = s->slot[b];
+  const cudaError_t e = cudaEventSynchronize(sl.out);
+  sl.ticket = 0;
+  return e == cudaSuccess ? state_status(sl.hflags) : cuda_status(e);
+}
+
+// The two slots' buffers, events and the copy streams, made on first use.
+int ensure_state_slots(btam_system *s) {
+  if (s->cp_in && s->cp_out) return BTAM_OK;
+  const size_t n = (size_t)s->n_real;
+  for (auto &sl : s->slot) {
+    BTAM_TRY(dalloc(sl.stage, s->st, 5 * n));
+    BTAM_TRY(dalloc(sl.res, s->st, 8 * n + 4));
+    BTAM_TRY(dalloc(sl.flags, s->st, 2));
+    if (!sl.hflags) BTAM_TRY(cudaMallocHost((void **)&sl.hflags, 2 * sizeof(int)));
+    sl.hflags[0] = sl.hflags[1] = 0;
+    for (cudaEvent_t *ev : {&sl.in, &sl.used, &sl.done, &sl.out})
+      if (!*ev) BTAM_TRY(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    sl.ticket = 0;
+  }
+  if (!s->cp_in) BTAM_TRY(cudaStreamCreateWithFlags(&s->cp_in, cudaStreamNonBlocking));
+  if (!s->cp_out) BTAM_TRY(cudaStreamCreateWithFlags(&s->cp_out, cudaStreamNonBlocking));
+  // the slot buffers come from the pool in the order of `st`: the copy
+  // streams use them only after that
+  cudaEvent_t ev = nullptr;
+  BTAM_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, s->st);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s->cp_in, ev, 0);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(s->cp_out, ev, 0);
+  cudaEventDestroy(ev);
+  return cuda_status(e);
+}
+
+void release_state_slots(btam_system *s) {
+  if (s->cp_in) cudaStreamSynchronize(s->cp_in);
+  if (s->cp_out) cudaStreamSynchronize(s->cp_out);
+  for (auto &sl : s->slot) {
+    dfree(sl.stage, s->st);
+    dfree(sl.res, s->st);
+    dfree(sl.flags, s->st);
+    if (sl.hflags) cudaFreeHost(sl.hflags);
+    sl.hflags = nullptr;
+    for (cudaEvent_t *ev : {&sl.in, &sl.used, &sl.done, &sl.out})
+      if (*ev) cudaEventDestroy(*ev);
+    sl.in = sl.used = sl.done = sl.out = nullptr;
+  }
+  if (s->cp_in) cudaStreamDestroy(s->cp_in);
+  if (s->cp_out) cudaStreamDestroy(s->cp_out);
+  s->cp_in = s->cp_out = nullptr;
+}
+
+}  // namespace
+
+extern "C" {
+
+int btam_mf_eval_state_async(btam_system *s, int precision, const double *q,
+                             const double *sigma, const double *x, double *rho, double *V0,
+                             double *S0, double *Rq, double *Rs, double *Rx, double *totals,
+                             long long *ticket) {
+  if (!s || !ticket) return BTAM_ERR_ARG;
+  if (!s->built) return BTAM_ERR_NOT_BUILT;
+  if (precision != BTAM_FP64 && precision != BTAM_FP32C) return BTAM_ERR_ARG;
+  if (s->batcher) return BTAM_ERR_ARG;  // a served system evaluates in the server's rounds
+  int st = ensure_state_slots(s);
+  if (st != BTAM_OK) return st;
+  const long long tk = s->next_ticket;
+  const int b = (int)(tk & 1);
+  auto &sl = s->slot[b];
+  if (sl.ticket) {  // the call two back still holds this slot: let it finish
+    const long long old = sl.ticket;
+    s->finished.emplace_back(old, retire_state_slot(s, b));
+  }
+  const int n = s->n_real;
+  const size_t nb = (size_t)n * sizeof(double);
+  double *dq = sl.stage, *ds = sl.stage + 3 * (size_t)n, *dx = sl.stage + 4 * (size_t)n;
+  // copies in on their own stream, once the slot's staging was last read
+  BTAM_TRY(cudaStreamWaitEvent(s->cp_in, sl.used, 0));
+  if (q) BTAM_TRY(cudaMemcpyAsync(dq, q, 3 * nb, cudaMemcpyHostToDevice, s->cp_in));
+  if (sigma) BTAM_TRY(cudaMemcpyAsync(ds, sigma, nb, cudaMemcpyHostToDevice, s->cp_in));
+  if (x) BTAM_TRY(cudaMemcpyAsync(dx, x, nb, cudaMemcpyHostToDevice, s->cp_in));
+  BTAM_TRY(cudaEventRecord(sl.in, s->cp_in));
+  // validation, the update and the evaluation on the system's stream
+  BTAM_TRY(cudaStreamWaitEvent(s->st, sl.in, 0));
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, 2 * sizeof(int), s->st));
+  if (q || sigma || x) {
+    validate_stage_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(
+        n, q ? dq : nullptr, sigma ? ds : nullptr, x ? dx : nullptr, s->code, s->box, s->err + 1);
+    BTAM_TRY(cudaGetLastError());
+    pack_state_kernel<<<(n + 127) / 128, 128, 0, s->st>>>(
+        n, q ? dq : nullptr, sigma ? ds : nullptr, x ? dx : nullptr, s->pos, s->xb, s->err + 1);
+    BTAM_TRY(cudaGetLastError());
+    if (s->n_ghost > 0)
+      BTAM_TRY(launch_ghost_refresh(n, s->n_ghost, s->pos, s->xb, s->code, s->owner, s->image,
+                                    s->box, s->st));
+  }
+  BTAM_TRY(cudaEventRecord(sl.used, s->st));
+  if ((st = btam_mf_eval_async(s, precision)) != BTAM_OK) return st;
+  // the requested results and the flags into the slot (device copies), so
+  // that the next call may overwrite the system's result arrays while
+  // these go to the host on the copy-out stream
+  const struct {
+    double *dst;
+    const double *src;
+    size_t off, bytes;
+  } cp[7] = {{rho, s->rho, 0, nb},          {V0, s->V0, (size_t)n, nb},
+             {S0, s->S0, 2 * (size_t)n, nb}, {Rq, s->Rq, 3 * (size_t)n, 3 * nb},
+             {Rs, s->Rs, 6 * (size_t)n, nb}, {Rx, s->Rx, 7 * (size_t)n, nb},
+             {totals, s->totals, 8 * (size_t)n, 4 * sizeof(double)}};
+  for (const auto &c : cp)
+    if (c.dst)
+      BTAM_TRY(cudaMemcpyAsync(sl.res + c.off, c.src, c.bytes, cudaMemcpyDeviceToDevice, s->st));
+  BTAM_TRY(cudaMemcpyAsync(sl.flags, s->err, 2 * sizeof(int), cudaMemcpyDeviceToDevice, s->st));
+  BTAM_TRY(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
+  BTAM_TRY(cudaEventRecord(sl.done, s->st));
+  BTAM_TRY(cudaStreamWaitEvent(s->cp_out, sl.done, 0));
+  for (const auto &c : cp)
+    if (c.dst)
+      BTAM_TRY(cudaMemcpyAsync(c.dst, sl.res + c.off, c.bytes, cudaMemcpyDeviceToHost, s->cp_out));
+  BTAM_TRY(cudaMemcpyAsync(sl.hflags, sl.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                           s->cp_out));
+  BTAM_TRY(cudaEventRecord(sl.out, s->cp_out));
+  sl.ticket = tk;
+  s->next_ticket = tk + 1;
+  *ticket = tk;
+  return BTAM_OK;
+}
+
+int btam_mf_eval_state_wait(btam_system *s, long long ticket) {
+  if (!s || ticket <= 0) return BTAM_ERR_ARG;
+  for (int b = 0; b < 2; ++b)
+    if (s->slot[b].ticket == ticket) return retire_state_slot(s, b);
+  for (size_t k = 0; k < s->finished.size(); ++k)
+    if (s->finished[k].first == ticket) {
+      const int st = s->finished[k].second;
+      s->finished.erase(s->finished.begin() + (long)k);
+      return st;
+    }
+  return BTAM_ERR_ARG;  // unknown, or already waited for
 }
 
 int btam_mf_rho(btam_system *s, int precision, double *rho) {

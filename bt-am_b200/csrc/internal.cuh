@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <utility>
 #include <vector>
 
 #include "../../include/btam.h"
@@ -100,6 +101,20 @@ struct btam_system {
   // (null: its own kernels), and the events that order them
   EvalBatcher *batcher = nullptr;
   cudaEvent_t batch_ready = nullptr, batch_done = nullptr;
+  // pipelined state evaluations (btam_mf_eval_state_async): two slots, each
+  // with its own staging and result buffers, so that one call's host copies
+  // run on the copy streams while the next call evaluates on `st`
+  struct StateSlot {
+    double *stage = nullptr;  // q (3n), sigma (n), x (n)
+    double *res = nullptr;    // rho, V0, S0, Rq (3n), Rs, Rx (8n), totals (4)
+    int *flags = nullptr;     // error bits, validation flags (device)
+    int *hflags = nullptr;    // their host copy (pinned)
+    cudaEvent_t in = nullptr, used = nullptr, done = nullptr, out = nullptr;
+    long long ticket = 0;     // the call in the slot (0: free)
+  } slot[2];
+  cudaStream_t cp_in = nullptr, cp_out = nullptr;  // host-to-device, device-to-host
+  long long next_ticket = 1;
+  std::vector<std::pair<long long, int>> finished;  // calls retired before their wait
 };
 
 // ---- evaluation rounds of the job server ----------------------------------

@@ -217,6 +217,25 @@ int btam_mf_eval(btam_system *s, int precision, double *rho, double *V0,
 int btam_mf_eval_state(btam_system *s, int precision, const double *q, const double *sigma,
                        const double *x, double *rho, double *V0, double *S0, double *Rq,
                        double *Rs, double *Rx, double *totals);
+/* btam_mf_eval_state without the wait (no counterpart in the reference):
+ * enqueues the copy of the new state, its check and update, the evaluation
+ * and the copies of the results, and returns a ticket.  The host copies run
+ * on two copy streams of the system, so a call's results travel to the host
+ * while the next call evaluates: with pinned host buffers, a stream of
+ * states costs about the evaluations alone.  Two calls may be in flight; a
+ * third waits for the first to finish (its status is kept for its wait).
+ * The host buffers of a call must stay untouched until its wait returns.
+ * Other calls on the system are ordered after the evaluations but not after
+ * the copies out: wait for every ticket first.  Not for systems of the job
+ * server (BTAM_ERR_ARG). */
+int btam_mf_eval_state_async(btam_system *s, int precision, const double *q,
+                             const double *sigma, const double *x, double *rho, double *V0,
+                             double *S0, double *Rq, double *Rs, double *Rx, double *totals,
+                             long long *ticket);
+/* Waits for the call of `ticket` to deliver its results; returns its status
+ * (the statuses of btam_mf_eval_state).  BTAM_ERR_ARG for a ticket unknown
+ * or already waited for. */
+int btam_mf_eval_state_wait(btam_system *s, long long ticket);
 /* The same evaluation enqueued on the system's stream with inputs and
  * outputs resident on the device; results stay in the system's buffers
  * (btam_results_copy reads them).  Does not synchronise. */
