@@ -568,11 +568,11 @@ int btam_dmd_graph_copy(const btam_system *s, int *offs, int *idx, long long idx
  * Rx per real site, Rq 3 per real site, totals[4] as btam_mf_eval.
  * Limit: n_real <= 16384 (BTAM_ERR_TOO_LARGE beyond).  The scratch (~10.9 MB
  * per device) lives until the process exits and is shared by every call on
- * that device: calls that overlap on the GPU race; serialise them.  The
- * first call on each device looks the scratch up, so make it before any
- * stream capture.  Runs on `stream` (a cudaStream_t, NULL = default); before
- * returning it reads the kernels' error flag back to the host and waits for
- * `stream`, so the host blocks until the evaluation has finished. */
+ * that device: calls that overlap on the GPU race; serialise them.  Runs
+ * on `stream` (a cudaStream_t, NULL = default); before returning it reads
+ * the kernels' error flag back to the host and waits for `stream`, so the
+ * host blocks until the evaluation has finished, and the call can never be
+ * recorded into a CUDA graph (stream capture). */
 int btam_mf_eval_noalloc(const btam_tables *t, int precision, int n_real,
                          const double *pos4, const double *xb, const int *code,
                          const int *owner, const double *gamma, const int *offs,
