@@ -159,6 +159,22 @@ def replica_value(ws, step_ms):
     return ws * 1e3 / step_ms
 
 
+def time_replicas(timed_steps, warmup, steps, barrier, max_over_ranks, ws, sampler=None):
+    """The timed region of one form on every rank: `warmup` untimed steps, a
+    barrier, `steps` timed steps (timed_steps returns their device times in
+    ms) closed by a barrier, then the mean step time's maximum over ranks
+    and the whole-job value.  sampler: a context manager held around the
+    timed steps (the clock sampler)."""
+    from contextlib import nullcontext
+    timed_steps(warmup)
+    barrier()
+    with (sampler if sampler is not None else nullcontext()):
+        ms = timed_steps(steps)
+        barrier()
+    step_ms = max_over_ranks(float(np.mean(ms)))
+    return step_ms, replica_value(ws, step_ms)
+
+
 def launches_per_eval(shape):
     """Kernel launches of one evaluation with launch variants (v1, v2): pass 1
     (plus the pair-rule kernel when either pass is undirected), pass 2 (pair
@@ -772,15 +788,12 @@ def run_btam(args, ws, rank, local):
             # the plain two-pass kernel pair: one warp per site in each pass,
             # every directed pair evaluated by its own site, default shapes
             S.set_variants(btam.FP64, 0, 0)
-        timed_steps(prec, args.warmup)
-        barrier()
-        with ClockSampler(local) as cs:
-            ms = timed_steps(prec, args.steps)
-            barrier()
+        cs = ClockSampler(local)
+        step_ms, value = time_replicas(lambda k: timed_steps(prec, k), args.warmup, args.steps,
+                                       barrier, max_over_ranks, ws, cs)
         if name == "fp64":
             clocks = cs.summary()
-        step_ms = max_over_ranks(float(np.mean(ms)))
-        results[name] = dict(ms=step_ms, value=replica_value(ws, step_ms))
+        results[name] = dict(ms=step_ms, value=value)
     S.set_variants(btam.FP64, *shapes["fp64"])
     # per-kernel times for the rooflines (median of 7 profiled evaluations)
     prof64 = np.median(np.array([S.profile(btam.FP64) for _ in range(7)]), axis=0)
