@@ -58,13 +58,13 @@ NCU_L1_SECTORS = {"pass1 pair-rule kernel": 51.73e6, "pass1 site kernel": 54.59e
 NCU_L1_PIPE = {"pass1 pair-rule kernel": 0.91, "pass1 site kernel": 0.71,
                "pass2 pair kernel": 0.69, "pass2 site kernel": 0.31}
 # DRAM bytes (read + write) per launch of the FP64 kernels on this workload
-# (autotuned variants (18, 30)), from one ncu capture
-NCU_DRAM_BYTES_FP64 = {"pass1 pair-rule kernel": 265.3e6, "pass1 site kernel": 112.3e6,
-                       "pass2 pair kernel": 486.4e6}
+# (autotuned variants (26, 30)), from one ncu capture
+NCU_DRAM_BYTES_FP64 = {"pass1 pair-rule kernel": 264.1e6, "pass1 site kernel": 107.8e6,
+                       "pass2 pair kernel": 486.3e6}
 # L1 data-pipe wavefront utilisation of the same FP64 launches (ncu
 # l1tex__data_pipe_lsu_wavefronts, share of peak): the binding unit
-NCU_L1_PIPE_FP64 = {"pass1 pair-rule kernel": 0.907, "pass1 site kernel": 0.787,
-                    "pass2 pair kernel": 0.697}
+NCU_L1_PIPE_FP64 = {"pass1 pair-rule kernel": 0.902, "pass1 site kernel": 0.769,
+                    "pass2 pair kernel": 0.711}
 # shared-memory wavefronts per launch: the pass-2 pair kernel reads its u/w
 # spline records from shared memory (its global sectors are the moment and
 # pair records only)
@@ -829,7 +829,7 @@ def run_btam(args, ws, rank, local):
     roofline["l1_data_pipe"] = {
         "bound": "L1 data pipe (random 32-byte halves of the 64-byte FP64 spline records)",
         "ncu_wavefront_frac": NCU_L1_PIPE_FP64,
-        "source": "one ncu capture of the autotuned FP64 shapes (18, 30) on this workload"}
+        "source": "one ncu capture of the autotuned FP64 shapes (26, 30) on this workload"}
     roof32, und32 = kernel_roofline(prof32, shapes["fp32c"], fp32_peak, "fp32", NCU_DRAM_BYTES)
     eval32 = eval_flops / (results["fp32c"]["ms"] * 1e-3) / 1e12
     roof32["evaluation"] = {"flops": eval_flops, "achieved": eval32, "frac": eval32 / fp32_peak,
