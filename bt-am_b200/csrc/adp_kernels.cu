@@ -436,11 +436,11 @@ template <class R> __device__ __forceinline__ double tree_total(R hi, R lo) {
 // FP64: the first pass over a site's slots keeps each active slot's pair
 // vector and weight X (and its pair kind) in shared memory, up to kCap slots
 // per site, for the three axis sweeps of part II, which then skip the
-// neighbour's row and the vector (the same values, so the same bits); the
-// cache is sized to keep the block's static shared memory under 40 KB.
+// neighbour's row and the vector; the cache holds a whole neighbour list
+// (136 slots) where the block's static shared memory stays under 47 KB.
 template <int NSITES> __host__ __device__ constexpr int p1_cache_cap() {
-  constexpr int room = (40960 - NSITES * (int)sizeof(SiteSums)) / (NSITES * 33);
-  return room > 96 ? 96 : (room < 0 ? 0 : room);
+  constexpr int room = (47000 - NSITES * (int)sizeof(SiteSums)) / (NSITES * 33);
+  return room > 136 ? 136 : (room < 0 ? 0 : room);
 }
 
 template <class R, int W, int MB, int G, bool UND>
