@@ -1522,6 +1522,7 @@ int relax_ngmres(btam_system *s, double tol, int max_iter, int m, const double *
   v.bd.x_min = x_min;
   fill_kernel<<<(n + 255) / 256, 256, 0, s->st>>>(n, 1.0, v.ones);
   int st = cuda_status(cudaGetLastError());
+  if (st == BTAM_OK) st = cuda_status(cudaMemsetAsync(s->err, 0, sizeof(int), s->st));
   // state at z (with the bounds), then its evaluation into (Z, G)
   auto eval_at = [&](const double *z, double *Z, double *G, double &r2) -> int {
     if (z) {
