@@ -21,6 +21,9 @@ def test_library_exports_every_declared_symbol():
     assert L.btam_version() >= 100
     L.btam_status_string.restype = ctypes.c_char_p
     assert L.btam_status_string(3) == b"more than maxneigh neighbours"
+    # no CUDA error has been turned into a status on this thread
+    L.btam_last_cuda_error.restype = ctypes.c_char_p
+    assert L.btam_last_cuda_error() == b""
 
 
 def test_bindings_cover_header():
