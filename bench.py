@@ -95,7 +95,10 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons, streamed every 50 ms by one
+    `nvidia-smi -lms` process from before the warm-up; the summary keeps the
+    samples read between begin() and end() (the timed region) and falls back
+    to all samples when the region was shorter than the sampling period."""
 
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -103,43 +106,68 @@ class ClockSampler:
 
     def __init__(self, device):
         self.device = device
-        self.samples = []
-        self._stop = threading.Event()
+        self.samples = []  # (host time, fields)
+        self.t0 = self.t1 = None
+        self._proc = None
         self._t = None
 
-    def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device),
-                                      f"--query-gpu={self.Q}", "--format=csv,noheader,nounits"],
-                                     capture_output=True, text=True, timeout=5).stdout
-                f = [v.strip() for v in out.strip().split(",")]
-                if len(f) == 6:
-                    self.samples.append(f)
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+    def _read(self):
+        for line in self._proc.stdout:
+            f = [v.strip() for v in line.strip().split(",")]
+            if len(f) == 6:
+                self.samples.append((time.perf_counter(), f))
 
-    def __enter__(self):
-        self._t = threading.Thread(target=self._run, daemon=True)
+    def start(self):
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "50"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self._proc = None
+            return self
+        self._t = threading.Thread(target=self._read, daemon=True)
         self._t.start()
         return self
 
+    def begin(self):
+        self.t0 = time.perf_counter()
+
+    def end(self):
+        self.t1 = time.perf_counter()
+
+    def stop(self):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=10)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+        if self._t is not None:
+            self._t.join(timeout=10)
+
+    def __enter__(self):
+        return self.start()
+
     def __exit__(self, *a):
-        self._stop.set()
-        self._t.join(timeout=10)
+        self.stop()
 
     def summary(self):
-        if not self.samples:
+        inside = [f for t, f in self.samples
+                  if self.t0 is not None and self.t1 is not None and self.t0 <= t <= self.t1]
+        window = "timed region"
+        if not inside:
+            inside, window = [f for _, f in self.samples], "whole run (timed region too short)"
+        if not inside:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in inside if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in inside if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4)
+        reasons = sorted({names[k] for s in inside for k in range(4)
                           if s[2 + k].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.samples)}
+                "samples": len(inside), "window": window}
 
 
 def reduce_max(v, dist, device):
@@ -163,14 +191,22 @@ def time_replicas(timed_steps, warmup, steps, barrier, max_over_ranks, ws, sampl
     """The timed region of one form on every rank: `warmup` untimed steps, a
     barrier, `steps` timed steps (timed_steps returns their device times in
     ms) closed by a barrier, then the mean step time's maximum over ranks
-    and the whole-job value.  sampler: a context manager held around the
-    timed steps (the clock sampler)."""
-    from contextlib import nullcontext
-    timed_steps(warmup)
-    barrier()
-    with (sampler if sampler is not None else nullcontext()):
+    and the whole-job value.  sampler: the clock sampler, started before the
+    warm-up and told where the timed region begins and ends."""
+    if sampler is not None:
+        sampler.start()
+    try:
+        timed_steps(warmup)
+        barrier()
+        if sampler is not None:
+            sampler.begin()
         ms = timed_steps(steps)
         barrier()
+        if sampler is not None:
+            sampler.end()
+    finally:
+        if sampler is not None:
+            sampler.stop()
     step_ms = max_over_ranks(float(np.mean(ms)))
     return step_ms, replica_value(ws, step_ms)
 
